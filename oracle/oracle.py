@@ -1,0 +1,407 @@
+"""CPU ORACLE of the pyfp3d element-loop hot path (test infrastructure).
+
+Python face of ``up3d_oracle.c``: the reference's operator objects
+(``PicardOperator``, ``UpwindOperator``, the isentropic field functions)
+restated over the C kernels, plus ``chain`` -- the residual + Jacobian
+composition of ``NewtonWorkspace.eval_residual`` / ``assemble_coupled``
+(``pyfp3d/solve/newton.py:345-372``, ``:430-452``) without a wake.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU baseline use
+this module; the CUDA product never imports it.  The glue follows the
+reference's own host code: numpy for per-array arithmetic and scipy's
+COO -> CSR summation for the Term-3 merge (``kernels/jacobian.py:344-358``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+
+GAMMA = 1.4
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile liboracle.so (needs gcc with OpenMP)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+_d = ctypes.c_double
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int32
+_p = ctypes.c_void_p
+
+
+def _declare(L):
+    sig = {
+        "orc_q2_at_mach": (_d, [_d, _d, _d]),
+        "orc_density_field": (None, [_p, _i64, _d, _d, _p]),
+        "orc_mach2_field": (None, [_p, _i64, _d, _d, _p]),
+        "orc_limit_q2_field": (None, [_p, _i64, _d, _d, _d, _p]),
+        "orc_drho_field": (None, [_p, _i64, _d, _d, _p]),
+        "orc_element_geometry": (_i64, [_p, _p, _i64, _p, _p]),
+        "orc_face_adjacency": (None, [_p, _i64, _p]),
+        "orc_centroids": (None, [_p, _p, _i64, _p]),
+        "orc_node_to_element": (None, [_p, _i64, _i64, _p, _p]),
+        "orc_greedy_coloring": (_i32, [_p, _i64, _i64, _p]),
+        "orc_color_partition": (None, [_p, _i64, _i32, _p, _p]),
+        "orc_csr_pattern": (_i64, [_p, _i64, _i64, _p, _p]),
+        "orc_elem_to_csr": (None, [_p, _i64, _p, _p, _p]),
+        "orc_velocities": (None, [_p, _p, _p, _i64, _p, _p]),
+        "orc_upstream": (None, [_p, _p, _p, _p, _p, _i64, ctypes.c_int, _p]),
+        "orc_rho_tilde": (None, [_p, _p, _p, _i64, _d, _d, _d, _d, _d, _p, _p]),
+        "orc_classify": (None, [_p, _p, _p, _i64, _d, _d, _d, _d, _d, _p]),
+        "orc_rho_tilde_frozen": (None, [_p, _p, _p, _p, _i64, _d, _d, _d, _d, _d, _p, _p]),
+        "orc_sens_frozen": (None, [_p, _p, _p, _p, _i64, _d, _d, _d, _d, _d, _p, _p]),
+        "orc_sens": (None, [_p, _p, _p, _i64, _d, _d, _d, _d, _d, _p, _p]),
+        "orc_residual": (None, [_p, _p, _i32, _p, _p, _p, _p, _p, _i64, _p]),
+        "orc_matrix_data": (None, [_p, _p, _i32, _p, _p, _p, _p, _i64, _p]),
+        "orc_jacobian_data": (None, [_p, _p, _i32, _p, _p, _p, _p, _p, _p, _d, _i64, _p]),
+        "orc_term3_coo": (None, [_p, _i64, _p, _p, _p, _p, _p, _p, _d, _p, _p, _p]),
+        "orc_spmv": (None, [_p, _p, _p, _p, _i64, _p]),
+        "orc_num_threads": (ctypes.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    return a.ctypes.data
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+# ---------------------------------------------------------------- physics
+
+def q2_at_mach(mach, m_inf, gamma=GAMMA):
+    return float(lib().orc_q2_at_mach(mach, m_inf, gamma))
+
+
+def density_field(q2, m_inf, gamma=GAMMA):
+    q2 = _c(q2, np.float64)
+    out = np.empty_like(q2)
+    lib().orc_density_field(_ptr(q2), q2.size, m_inf, gamma, _ptr(out))
+    return out
+
+
+def mach_squared_field(q2, m_inf, gamma=GAMMA):
+    q2 = _c(q2, np.float64)
+    out = np.empty_like(q2)
+    lib().orc_mach2_field(_ptr(q2), q2.size, m_inf, gamma, _ptr(out))
+    return out
+
+
+def limit_q2_field(q2, m_inf, m_cap, gamma=GAMMA):
+    q2 = _c(q2, np.float64)
+    out = np.empty_like(q2)
+    lib().orc_limit_q2_field(_ptr(q2), q2.size, m_inf, m_cap, gamma, _ptr(out))
+    return out
+
+
+def density_derivative_field(q2, m_inf, gamma=GAMMA):
+    q2 = _c(q2, np.float64)
+    out = np.empty_like(q2)
+    lib().orc_drho_field(_ptr(q2), q2.size, m_inf, gamma, _ptr(out))
+    return out
+
+
+# ------------------------------------------------------------------- mesh
+
+def element_geometry(nodes, elements):
+    nodes = _c(nodes, np.float64)
+    el = _c(elements, np.int32)
+    E = len(el)
+    B = np.empty((E, 4, 3))
+    V = np.empty(E)
+    bad = lib().orc_element_geometry(_ptr(nodes), _ptr(el), E, _ptr(B), _ptr(V))
+    if bad >= 0:
+        raise ValueError(f"element_gradients: degenerate tetrahedron {bad}")
+    return B, V
+
+
+def face_adjacency(elements):
+    el = _c(elements, np.int32)
+    fn = np.empty((len(el), 4), dtype=np.int32)
+    lib().orc_face_adjacency(_ptr(el), len(el), _ptr(fn))
+    return fn
+
+
+def centroids(nodes, elements):
+    nodes = _c(nodes, np.float64)
+    el = _c(elements, np.int32)
+    out = np.empty((len(el), 3))
+    lib().orc_centroids(_ptr(nodes), _ptr(el), len(el), _ptr(out))
+    return out
+
+
+def greedy_coloring(elements, n_nodes):
+    el = _c(elements, np.int32)
+    colors = np.empty(len(el), dtype=np.int32)
+    nc = lib().orc_greedy_coloring(_ptr(el), len(el), n_nodes, _ptr(colors))
+    if nc < 0:
+        raise ValueError("greedy coloring exceeded 256 colors")
+    return colors, int(nc)
+
+
+def color_partition_csr(elements, n_nodes):
+    colors, nc = greedy_coloring(elements, n_nodes)
+    off = np.empty(nc + 1, dtype=np.int64)
+    elems = np.empty(len(colors), dtype=np.int64)
+    lib().orc_color_partition(_ptr(colors), len(colors), nc, _ptr(off), _ptr(elems))
+    return off, elems, nc
+
+
+def csr_pattern(elements, n_nodes):
+    el = _c(elements, np.int32)
+    indptr = np.empty(n_nodes + 1, dtype=np.int64)
+    nnz = lib().orc_csr_pattern(_ptr(el), len(el), n_nodes, _ptr(indptr), None)
+    indices = np.empty(nnz, dtype=np.int32)
+    lib().orc_csr_pattern(_ptr(el), len(el), n_nodes, _ptr(indptr), _ptr(indices))
+    return indptr, indices
+
+
+def elem_to_csr(elements, indptr, indices):
+    el = _c(elements, np.int32)
+    indptr = _c(indptr, np.int64)
+    indices = _c(indices, np.int32)
+    out = np.empty((len(el), 4, 4), dtype=np.int64)
+    lib().orc_elem_to_csr(_ptr(el), len(el), _ptr(indptr), _ptr(indices), _ptr(out))
+    return out
+
+
+# -------------------------------------------------------------- operators
+
+class PicardOperator:
+    """Oracle restatement of ``kernels/jacobian.py:231-375``."""
+
+    def __init__(self, nodes, elements):
+        self.nodes = _c(nodes, np.float64)
+        self.elements = _c(elements, np.int32)
+        self.n_nodes = len(self.nodes)
+        self.n_tets = len(self.elements)
+        self.B, self.V = element_geometry(self.nodes, self.elements)
+        self.color_offsets, self.color_elems, self.n_colors = color_partition_csr(
+            self.elements, self.n_nodes)
+        self.indptr, self.indices = csr_pattern(self.elements, self.n_nodes)
+        self.nnz = len(self.indices)
+        self.elem_to_csr = elem_to_csr(self.elements, self.indptr, self.indices)
+        self._grad = np.empty((self.n_tets, 3))
+        self._q2 = np.empty(self.n_tets)
+        self._R = np.empty(self.n_nodes)
+        self.rho_ones = np.ones(self.n_tets)
+        self.newton_nnz = None
+        self.n_term3_active = None
+
+    def _csr(self, data):
+        return sp.csr_matrix((data, self.indices, self.indptr),
+                             shape=(self.n_nodes, self.n_nodes))
+
+    def velocities(self, phi):
+        phi = _c(phi, np.float64)
+        lib().orc_velocities(_ptr(self.elements), _ptr(self.B), _ptr(phi),
+                             self.n_tets, _ptr(self._grad), _ptr(self._q2))
+        return self._grad, self._q2
+
+    def assemble_matrix(self, rho_tilde=None):
+        rt = self.rho_ones if rho_tilde is None else _c(rho_tilde, np.float64)
+        data = np.empty(self.nnz)
+        lib().orc_matrix_data(_ptr(self.color_offsets), _ptr(self.color_elems),
+                              self.n_colors, _ptr(self.elem_to_csr), _ptr(self.B),
+                              _ptr(self.V), _ptr(rt), self.nnz, _ptr(data))
+        return self._csr(data)
+
+    def assemble_residual(self, phi, rho_tilde=None):
+        rt = self.rho_ones if rho_tilde is None else _c(rho_tilde, np.float64)
+        grad, _ = self.velocities(phi)
+        lib().orc_residual(_ptr(self.color_offsets), _ptr(self.color_elems),
+                           self.n_colors, _ptr(self.elements), _ptr(self.B),
+                           _ptr(self.V), _ptr(rt), _ptr(grad), self.n_nodes,
+                           _ptr(self._R))
+        return self._R
+
+    def assemble_newton_jacobian(self, phi, rho_tilde, s_e, s_u, upstream,
+                                 u_inf=1.0, lim_mask=None):
+        upstream = _c(upstream, np.int64)
+        if lim_mask is not None:
+            s_e = s_e * lim_mask
+            s_u = s_u * lim_mask[upstream]
+        s_e = _c(s_e, np.float64)
+        s_u = _c(s_u, np.float64)
+        rt = _c(rho_tilde, np.float64)
+        inv_u2 = 1.0 / (u_inf * u_inf)
+        phi = _c(phi, np.float64)
+        grad = np.empty((self.n_tets, 3))
+        q2 = np.empty(self.n_tets)
+        lib().orc_velocities(_ptr(self.elements), _ptr(self.B), _ptr(phi),
+                             self.n_tets, _ptr(grad), _ptr(q2))
+        data = np.empty(self.nnz)
+        lib().orc_jacobian_data(_ptr(self.color_offsets), _ptr(self.color_elems),
+                                self.n_colors, _ptr(self.elem_to_csr), _ptr(self.B),
+                                _ptr(self.V), _ptr(rt), _ptr(grad), _ptr(s_e),
+                                inv_u2, self.nnz, _ptr(data))
+        J = self._csr(data)
+        active = np.nonzero(s_u)[0].astype(np.int64)
+        self.n_term3_active = int(len(active))
+        if len(active) > 0:
+            n = 16 * len(active)
+            rows = np.empty(n, dtype=np.int64)
+            cols = np.empty(n, dtype=np.int64)
+            vals = np.empty(n)
+            lib().orc_term3_coo(_ptr(active), len(active), _ptr(self.elements),
+                                _ptr(self.B), _ptr(self.V), _ptr(grad), _ptr(upstream),
+                                _ptr(s_u), inv_u2, _ptr(rows), _ptr(cols), _ptr(vals))
+            J = (J + sp.coo_matrix((vals, (rows, cols)), shape=J.shape).tocsr()).tocsr()
+        self.newton_nnz = int(J.nnz)
+        return J
+
+
+class UpwindOperator:
+    """Oracle restatement of ``kernels/upwind.py:733-920`` (walk flux)."""
+
+    def __init__(self, nodes, elements):
+        self.nodes = _c(nodes, np.float64)
+        self.elements = _c(elements, np.int32)
+        self.face_neighbors = face_adjacency(self.elements)
+        self.centroids = centroids(self.nodes, self.elements)
+        n = len(self.elements)
+        self._upstream = np.empty(n, dtype=np.int64)
+        self.nu = np.empty(n)
+        self._rho_tilde = np.empty(n)
+        self._se = np.empty(n)
+        self._su = np.empty(n)
+        self._branch = np.empty(n, dtype=np.int8)
+        self.nu_max = 0.0
+        self.n_supersonic = 0
+        self.n_floored = 0
+
+    def upstream(self, grad, max_hops=4):
+        grad = _c(grad, np.float64)
+        fn = _c(self.face_neighbors, np.int32)
+        lib().orc_upstream(_ptr(fn), _ptr(self.centroids), _ptr(self.nodes),
+                           _ptr(self.elements), _ptr(grad), len(self.elements),
+                           max_hops, _ptr(self._upstream))
+        return self._upstream
+
+    def _monitors(self, rho_floor, branch=None):
+        self.nu_max = float(self.nu.max())
+        self.n_supersonic = int(np.count_nonzero(self.nu > 0.0))
+        if branch is None:
+            self.n_floored = int(np.count_nonzero(self._rho_tilde == rho_floor))
+        else:
+            self.n_floored = int(np.count_nonzero(branch == 3))
+
+    def rho_tilde(self, grad, q2, rho, m_inf, C, m_crit, gamma=GAMMA, rho_floor=0.05):
+        up = self.upstream(grad)
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        lib().orc_rho_tilde(_ptr(q2), _ptr(rho), _ptr(up), len(q2), m_inf, m_crit, C,
+                            gamma, rho_floor, _ptr(self.nu), _ptr(self._rho_tilde))
+        self._monitors(rho_floor)
+        return self._rho_tilde
+
+    def freeze_upwind_state(self, grad, q2, rho, m_inf, C, m_crit, gamma=GAMMA,
+                            rho_floor=0.05):
+        up = self.upstream(grad)
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        lib().orc_classify(_ptr(q2), _ptr(rho), _ptr(up), len(q2), m_inf, m_crit, C,
+                           gamma, rho_floor, _ptr(self._branch))
+        return up.copy(), self._branch.copy()
+
+    def rho_tilde_frozen(self, q2, rho, upstream, branch, m_inf, C, m_crit,
+                         gamma=GAMMA, rho_floor=0.05):
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        up, br = _c(upstream, np.int64), _c(branch, np.int8)
+        lib().orc_rho_tilde_frozen(_ptr(q2), _ptr(rho), _ptr(up), _ptr(br), len(q2),
+                                   m_inf, m_crit, C, gamma, rho_floor, _ptr(self.nu),
+                                   _ptr(self._rho_tilde))
+        self._monitors(rho_floor, branch=br)
+        return self._rho_tilde
+
+    def rho_tilde_frozen_sensitivities(self, q2, rho, upstream, branch, m_inf, C,
+                                       m_crit, gamma=GAMMA, rho_floor=0.05):
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        up, br = _c(upstream, np.int64), _c(branch, np.int8)
+        lib().orc_sens_frozen(_ptr(q2), _ptr(rho), _ptr(up), _ptr(br), len(q2), m_inf,
+                              m_crit, C, gamma, rho_floor, _ptr(self._se), _ptr(self._su))
+        return self._se, self._su
+
+    def rho_tilde_sensitivities(self, grad, q2, rho, m_inf, C, m_crit, gamma=GAMMA,
+                                rho_floor=0.05):
+        up = self.upstream(grad)
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        lib().orc_sens(_ptr(q2), _ptr(rho), _ptr(up), len(q2), m_inf, m_crit, C, gamma,
+                       rho_floor, _ptr(self._se), _ptr(self._su))
+        return self._se, self._su, self._upstream
+
+
+def spmv(indptr, indices, data, x):
+    indptr, indices = _c(indptr, np.int64), _c(indices, np.int32)
+    data, x = _c(data, np.float64), _c(x, np.float64)
+    y = np.empty(len(indptr) - 1)
+    lib().orc_spmv(_ptr(indptr), _ptr(indices), _ptr(data), _ptr(x), len(y), _ptr(y))
+    return y
+
+
+# ------------------------------------------------------------------ chain
+
+M_CRIT = 0.95
+UPWIND_C = 1.5
+RHO_FLOOR = 0.05
+M_CAP = 3.0
+
+
+def chain(op: PicardOperator, upw: UpwindOperator, phi, m_inf, u_inf=1.0,
+          m_cap=M_CAP, C=UPWIND_C, m_crit=M_CRIT, rho_floor=RHO_FLOOR,
+          gamma=GAMMA, jacobian=True):
+    """Residual + Jacobian at phi, composed like eval_residual and
+    assemble_coupled (pyfp3d/solve/newton.py:345-372, :435-452)."""
+    out = {}
+    grad, q2 = op.velocities(phi)
+    grad, q2 = grad.copy(), q2.copy()
+    q2n = q2 / u_inf ** 2
+    q2l = limit_q2_field(q2n, m_inf, m_cap, gamma)
+    lim = q2l == q2n
+    rho = density_field(q2l, m_inf, gamma)
+    rt = upw.rho_tilde(grad, q2l, rho, m_inf, C, m_crit, gamma, rho_floor).copy()
+    out.update(grad=grad, q2=q2, q2l=q2l, lim=lim, rho=rho, rho_tilde=rt,
+               nu=upw.nu.copy(), upstream=upw._upstream.copy(),
+               nu_max=upw.nu_max, n_supersonic=upw.n_supersonic,
+               n_floored=upw.n_floored, n_limited=int(np.count_nonzero(~lim)))
+    out["R"] = op.assemble_residual(phi, rt).copy()
+    if jacobian:
+        s_e, s_u, up = upw.rho_tilde_sensitivities(grad, q2l, rho, m_inf, C, m_crit,
+                                                   gamma, rho_floor)
+        s_e, s_u, up = s_e.copy(), s_u.copy(), up.copy()
+        J = op.assemble_newton_jacobian(phi, rt, s_e, s_u, up, u_inf=u_inf,
+                                        lim_mask=None if lim.all() else lim)
+        out.update(s_e=s_e, s_u=s_u, J=J, n_term3_active=op.n_term3_active,
+                   newton_nnz=op.newton_nnz)
+    return out

@@ -1,0 +1,215 @@
+"""Generate the golden fixtures of the element-loop hot path by running the
+reference (pyfp3d, pure Python + Numba) on synthetic Kuhn bump meshes.
+
+Usage (needs the reference source tree; it cannot run where that tree is
+absent, which is why its outputs are committed):
+
+    python tests/golden/make_golden.py /path/to/UP3D
+
+Every array is produced by the reference's own public entry points, composed
+exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
+them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
+(T = I):
+
+  PicardOperator(nodes, elements)                     kernels/jacobian.py:246
+  UpwindOperator(nodes, elements, weighted=False)     kernels/upwind.py:744
+  op.velocities(phi)                                  kernels/jacobian.py:264
+  limit_q2_field / density_field / mach_squared_field physics/isentropic.py:293,236,318
+  upw.rho_tilde / freeze_upwind_state / rho_tilde_frozen /
+  rho_tilde_sensitivities / rho_tilde_frozen_sensitivities
+                                                      kernels/upwind.py:783-920
+  op.assemble_residual / assemble_matrix / assemble_newton_jacobian
+                                                      kernels/jacobian.py:272-375
+  solve_subsonic (pyamg swapped for scipy spilu)      solve/picard.py:271-417
+
+The optional reference dependencies that are absent here (meshio, pyamg) are
+replaced by empty modules before import; neither is on the hot path.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+sys.path.insert(0, str(REPO))
+
+from up3d_b200.mesh.kuhn import bump_channel, pocket_state, seeded_state  # noqa: E402
+
+M_CRIT = 0.95
+UPWIND_C = 1.5
+RHO_FLOOR = 0.05
+M_CAP = 3.0
+GAMMA = 1.4
+
+
+def import_reference(ref_root: str):
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/up3d_numba_cache")
+    for name in ("meshio", "pyamg"):
+        if name not in sys.modules:
+            sys.modules[name] = types.ModuleType(name)
+    sys.path.insert(0, ref_root)
+    import pyfp3d.kernels.jacobian as jac
+    import pyfp3d.kernels.upwind as upw
+    import pyfp3d.physics.isentropic as isen
+    return jac, upw, isen
+
+
+def chain(jac, upw_mod, isen, op, upw, phi, m_inf, u_inf=1.0):
+    """Residual + Jacobian chain of eval_residual/assemble_coupled."""
+    out = {"phi": phi, "m_inf": np.float64(m_inf), "u_inf": np.float64(u_inf)}
+    grad, q2 = op.velocities(phi)
+    grad, q2 = grad.copy(), q2.copy()
+    q2n = q2 / u_inf ** 2
+    q2l = isen.limit_q2_field(q2n, m_inf, M_CAP, GAMMA)
+    lim = q2l == q2n
+    rho = isen.density_field(q2l, m_inf, GAMMA)
+    out.update(grad=grad, q2=q2, q2l=q2l, lim=lim, rho=rho,
+               mach2=isen.mach_squared_field(q2l, m_inf, GAMMA))
+    rho_t = upw.rho_tilde(grad, q2l, rho, m_inf, UPWIND_C, M_CRIT, GAMMA,
+                          RHO_FLOOR).copy()
+    out.update(rho_tilde=rho_t, nu=upw.nu.copy(),
+               upstream=upw._upstream.copy(),
+               nu_max=np.float64(upw.nu_max),
+               n_supersonic=np.int64(upw.n_supersonic),
+               n_floored=np.int64(upw.n_floored))
+    up, br = upw.freeze_upwind_state(grad, q2l, rho, m_inf, UPWIND_C,
+                                     M_CRIT, GAMMA, RHO_FLOOR)
+    rt_f = upw.rho_tilde_frozen(q2l, rho, up, br, m_inf, UPWIND_C, M_CRIT,
+                                GAMMA, RHO_FLOOR).copy()
+    se_f, su_f = upw.rho_tilde_frozen_sensitivities(
+        q2l, rho, up, br, m_inf, UPWIND_C, M_CRIT, GAMMA, RHO_FLOOR)
+    out.update(branch=br, rho_tilde_frozen=rt_f, nu_frozen=upw.nu.copy(),
+               s_e_frozen=se_f.copy(), s_u_frozen=su_f.copy())
+    s_e, s_u, upstream = upw.rho_tilde_sensitivities(
+        grad, q2l, rho, m_inf, UPWIND_C, M_CRIT, GAMMA, RHO_FLOOR)
+    s_e, s_u, upstream = s_e.copy(), s_u.copy(), upstream.copy()
+    out.update(s_e=s_e, s_u=s_u)
+    R = op.assemble_residual(phi, rho_t).copy()
+    A = op.assemble_matrix(rho_t)
+    J = op.assemble_newton_jacobian(phi, rho_t, s_e, s_u, upstream,
+                                    u_inf=u_inf,
+                                    lim_mask=None if lim.all() else lim)
+    out.update(R=R, A_data=A.data.copy(), J_data=J.data.copy(),
+               J_indices=J.indices.astype(np.int32),
+               J_indptr=J.indptr.astype(np.int64),
+               n_term3_active=np.int64(op.n_term3_active),
+               newton_nnz=np.int64(op.newton_nnz))
+    return out
+
+
+def mesh_arrays(op, upw, mesh, full=True):
+    out = {"nodes": mesh.nodes, "elements": mesh.elements,
+           "dirichlet_nodes": mesh.dirichlet_nodes,
+           "shape": np.array(mesh.shape, dtype=np.int64),
+           "B": op.B, "V": op.V,
+           "face_neighbors": upw.face_neighbors,
+           "centroids": upw.centroids,
+           "color_offsets": op.color_offsets, "color_elems": op.color_elems,
+           "indptr": op._pattern.indptr.astype(np.int64),
+           "indices": op._pattern.indices.astype(np.int32),
+           "laplace_data": op.assemble_matrix().data.copy()}
+    if full:
+        out["elem_to_csr"] = op.elem_to_csr
+    return out
+
+
+# Arrays dropped from the large-mesh fixture: each is either recomputed from
+# the kept ones in the tests or pinned on the small mesh.
+_LARGE_DROP = {"mesh/B", "mesh/centroids", "mesh/color_elems", "grad", "q2",
+               "mach2", "nu", "nu_frozen", "rho_tilde_frozen", "s_e_frozen",
+               "s_u_frozen", "lim", "q2l", "rho"}
+
+
+def _compact(v):
+    v = np.asarray(v)
+    if v.dtype == np.int64 and v.size > 1 and np.abs(v).max() < 2**31:
+        return v.astype(np.int32)
+    return v
+
+
+def make_case(jac, upw_mod, isen, name, mesh, states, full=True):
+    op = jac.PicardOperator(mesh.nodes, mesh.elements)
+    upw = upw_mod.UpwindOperator(mesh.nodes, mesh.elements, weighted=False)
+    arrays = {f"mesh/{k}": v for k, v in mesh_arrays(op, upw, mesh, full).items()}
+    if not full:
+        arrays["mesh/B_checksum"] = np.array([op.B.sum(), np.abs(op.B).sum()])
+    for label, (phi, m_inf) in states.items():
+        res = chain(jac, upw_mod, isen, op, upw, phi, m_inf)
+        for k, v in res.items():
+            if not full and (k in _LARGE_DROP):
+                continue
+            arrays[f"{label}/{k}"] = v
+    arrays = {k: _compact(v) for k, v in arrays.items()
+              if full or k not in _LARGE_DROP}
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
+def make_picard(name, mesh, m_inf):
+    """Converged subsonic Picard solution of the reference driver."""
+    import scipy.sparse.linalg as spla
+    import pyfp3d.solve.linear as lin
+    from pyfp3d.solve.picard import solve_subsonic
+    import pyfp3d.physics.isentropic as isen
+
+    def _ilu_preconditioner(A):
+        ilu = spla.spilu(A.tocsc(), drop_tol=1e-5, fill_factor=20.0)
+        return None, spla.LinearOperator(A.shape, matvec=ilu.solve)
+
+    saved = lin.build_amg_preconditioner
+    lin.build_amg_preconditioner = _ilu_preconditioner
+    try:
+        vals = mesh.nodes[mesh.dirichlet_nodes, 0].copy()
+        res = solve_subsonic(mesh.nodes, mesh.elements, mesh.dirichlet_nodes,
+                             vals, m_inf)
+    finally:
+        lin.build_amg_preconditioner = saved
+    jac_mod = sys.modules["pyfp3d.kernels.jacobian"]
+    op = jac_mod.PicardOperator(mesh.nodes, mesh.elements)
+    _, q2 = op.velocities(res["phi"])
+    cp = np.array([isen.pressure_coefficient(q, m_inf, GAMMA) for q in q2])
+    np.savez_compressed(
+        HERE / f"{name}.npz", phi=res["phi"], rho=res["rho"], cp=cp,
+        m_inf=np.float64(m_inf),
+        residual_history=np.array(res["residual_history"]),
+        drho_history=np.array(res["drho_history"]),
+        n_picard=np.int64(res["n_picard"]), converged=res["converged"],
+        nodes=mesh.nodes, elements=mesh.elements,
+        dirichlet_nodes=mesh.dirichlet_nodes)
+    print(f"wrote {name}: n_picard={res['n_picard']} "
+          f"|R|={res['residual_history'][-1]:.2e}")
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    jac, upw_mod, isen = import_reference(ref_root)
+
+    small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
+    s_states = {
+        "freestream_m05": (small.freestream(), 0.5),
+        "seed0_m085": (seeded_state(small, 0), 0.85),
+        "accelerating_m08": (pocket_state(small, "accelerating"), 0.8),
+        "shockpoint_m08": (pocket_state(small, "shockpoint"), 0.8),
+        "mixed_m08": (pocket_state(small, "mixed"), 0.8),
+        "limited_m08": (2.5 * pocket_state(small, "mixed"), 0.8),
+    }
+    make_case(jac, upw_mod, isen, "small_bump", small, s_states, full=True)
+
+    c1 = bump_channel(40, 10, 10, amplitude=0.05, seed=0)
+    c1_states = {
+        "seed0_m05": (seeded_state(c1, 0), 0.5),
+        "mixed_m08": (pocket_state(c1, "mixed"), 0.8),
+    }
+    make_case(jac, upw_mod, isen, "c1_bump", c1, c1_states, full=False)
+    make_picard("c1_picard", c1, 0.5)
+
+
+if __name__ == "__main__":
+    main()
