@@ -1,0 +1,372 @@
+"""Benchmark of the B200 element-loop hot path (one JSON line on rank 0).
+
+Workload (the transonic bump channel): a 200 x 60 x 50 Kuhn-split box
+(3.6 M tets, 625,311 nodes), bump amplitude 0.08, M_inf = 0.85, evaluated at
+the five seeded potentials phi = U x + 0.01 U (smooth random modes), cycled
+one per step.  A step is one fused residual + Newton Jacobian evaluation
+(velocities, limiter, density, walk, upwinded density, sensitivities,
+residual R and the Jacobian on the P1 pattern, plus Term 3) -- the work of
+``NewtonWorkspace.eval_residual`` + ``assemble_coupled`` without a wake.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value: device-timed Melem/s with inputs resident in HBM (the mesh data is
+~1.3 GB, larger than L2, so no flush is needed between steps).
+e2e:   the same through the public API with host buffers: each step copies
+phi host->device and R + the Jacobian data device->host.
+--impl reference: the CPU oracle (C/OpenMP restatement of the reference's
+Numba kernels) on all host cores, same workload, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+MESH = (200, 60, 50)
+AMPLITUDE = 0.08
+M_INF = 0.85
+N_STATES = 5
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mesh", default="x".join(map(str, MESH)))
+    p.add_argument("--e2e-steps", type=int, default=100)
+    p.add_argument("--cpu-states", type=int, default=5)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(shape):
+    from up3d_b200.mesh.kuhn import bump_channel, seeded_state
+    mesh = bump_channel(*shape, amplitude=AMPLITUDE, seed=0)
+    phis = [seeded_state(mesh, s) for s in range(N_STATES)]
+    return mesh, phis
+
+
+def config_dict(shape, mesh, nnz=None):
+    nx, ny, nz = shape
+    d = {"workload": f"transonic bump channel {nx}x{ny}x{nz} Kuhn-split "
+                     f"({mesh.n_tets} tets), M_inf {M_INF}, fused residual + Newton Jacobian "
+                     f"at {N_STATES} seeded phi states",
+         "mesh": f"{nx}x{ny}x{nz}", "n_tets": mesh.n_tets, "n_nodes": mesh.n_nodes,
+         "m_inf": M_INF, "bump_amplitude": AMPLITUDE, "states": N_STATES,
+         "l2": "inputs larger than L2 (mesh data ~1.3 GB >> 126 MB); no flush",
+         "parallelism": "replicas"}
+    if nnz is not None:
+        d["nnz"] = nnz
+    return d
+
+
+# ---------------------------------------------------------------- CPU side
+
+def cpu_chain_timing(mesh, phis, n_states, threads):
+    """The oracle's residual + Jacobian chain (its restatement of the
+    reference kernels), timed on the host cores."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    op = O.PicardOperator(mesh.nodes, mesh.elements)
+    upw = O.UpwindOperator(mesh.nodes, mesh.elements)
+    O.chain(op, upw, phis[0], M_INF)          # warm (page-in, thread pool)
+    t0 = time.perf_counter()
+    for k in range(n_states):
+        O.chain(op, upw, phis[k % len(phis)], M_INF)
+    dt = time.perf_counter() - t0
+    return mesh.n_tets * n_states / dt / 1e6, dt, O.num_threads()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    shape = tuple(int(v) for v in args.mesh.split("x"))
+    threads = os.cpu_count() or 1
+    mesh, phis = workload(shape)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    op = O.PicardOperator(mesh.nodes, mesh.elements)
+    upw = O.UpwindOperator(mesh.nodes, mesh.elements)
+    for w in range(min(max(args.warmup, 1), 3)):
+        O.chain(op, upw, phis[w % N_STATES], M_INF)
+    steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for k in range(steps):
+        O.chain(op, upw, phis[k % N_STATES], M_INF)
+    dt = time.perf_counter() - t0
+    value = mesh.n_tets * steps / dt / 1e6
+    sample = (f"{steps} full-mesh residual+Jacobian chains (oracle restatement of the reference "
+              f"Numba kernels, colour-ordered OpenMP) on {O.num_threads()} threads")
+    line = {"impl": "reference", "metric": "residual+Jacobian Melem/s", "value": round(value, 4),
+            "unit": "Melem/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * dt / steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(shape, mesh),
+            "cpu_baseline": {"value": round(value, 4), "unit": "Melem/s",
+                             "cores": O.num_threads(), "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "Melem/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = bus_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                   "-lms", "100"]
+            if self.bus_id:
+                cmd += ["-i", self.bus_id]
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.25)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        sm = [r[0] for r in rows]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------- GPU side
+
+def bytes_model(info, n_active=0):
+    """Algorithmic bytes of one launch of each kernel (every input read once,
+    every output written once, in the library's storage formats)."""
+    E, N, Z = info["n_tets"], info["n_nodes"], info["nnz"]
+    elem = (E * (16 + 96 + 8 + 16 + 24)      # conn, B, V, face neighbours, centroid
+            + N * (24 + 8)                   # node coordinates, phi
+            + E * (6 * 8 + 4)                # record (gB, w1, w2, w3... 6 used doubles), upstream
+            + n_active * 32)                 # Term-3 upstream factors
+    row = (4 * E * 4 + 12 * E * 2            # node->element entries, row plan
+           + 4 * (Z + 1) + 4 * (N + 1) * 2 + 4 * N   # plan offsets, indptr, entry offsets, diag
+           + E * (80 + 48)                   # packed B_i.B_j, record (gB, w1, w2)
+           + 8 * N + 8 * Z)                  # R, J data
+    return {"elem_sweep": elem, "row_gather": row}
+
+
+def read_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    for f in sorted((REPO / "profiles").glob(f"{kernel}*.md")):
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from up3d_b200 import _lib as L
+    from up3d_b200.mesh.device import DeviceMesh
+    from up3d_b200.solve.fused import FlowParams, ResidualJacobian
+
+    shape = tuple(int(v) for v in args.mesh.split("x"))
+    mesh, phis = workload(shape)
+    dmesh = DeviceMesh(mesh.nodes, mesh.elements)
+    info = {"n_tets": dmesh.n_tets, "n_nodes": dmesh.n_nodes, "nnz": dmesh.nnz}
+    ev = ResidualJacobian(dmesh)
+    flow = FlowParams(m_inf=M_INF)
+    d_phis = [torch.from_numpy(p).cuda() for p in phis]
+    stream = torch.cuda.current_stream()
+
+    def step(k):
+        ev.evaluate(d_phis[k % N_STATES], flow, jacobian=True, keep_state=False)
+
+    for w in range(max(args.warmup, 3)):
+        step(w)
+    torch.cuda.synchronize()
+    mon = ev.read_monitors()
+
+    props = torch.cuda.get_device_properties(local)
+    bus = None
+    try:
+        bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+    except Exception:
+        bus = None
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-timed region
+    with ClockSampler(bus) as clocks:
+        L.profile(True)
+        launches0 = L.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_stop = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(k)
+        t_stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        launches = L.launch_count() - launches0
+        prof = L.profile_read()
+        L.profile(False)
+        ms = t_start.elapsed_time(t_stop)
+
+        # ---- end-to-end through the public API with host buffers
+        h_phis = [torch.from_numpy(p).pin_memory() for p in phis]
+        h_R = torch.empty(dmesh.n_nodes, dtype=torch.float64).pin_memory()
+        h_J = torch.empty(dmesh.nnz, dtype=torch.float64).pin_memory()
+        d_phi = torch.empty(dmesh.n_nodes, dtype=torch.float64, device="cuda")
+        n_e2e = max(1, args.e2e_steps)
+        barrier()
+        torch.cuda.synchronize()
+        e_start = torch.cuda.Event(enable_timing=True)
+        e_stop = torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        for k in range(n_e2e):
+            d_phi.copy_(h_phis[k % N_STATES], non_blocking=True)
+            ev.evaluate(d_phi, flow, jacobian=True, keep_state=False)
+            h_R.copy_(ev.R, non_blocking=True)
+            h_J.copy_(ev.data, non_blocking=True)
+            stream.synchronize()
+        e_stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = e_start.elapsed_time(e_stop)
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
+    e2e_value = dmesh.n_tets * n_e2e * world / (e2e_ms * 1e-3) / 1e6
+
+    # roofline of the dominant kernel, timed live over the timed region
+    bm = bytes_model(info, n_active=int(mon["n_term3_active"]))
+    dom = max(("elem_sweep", "row_gather"), key=lambda s: prof[s]["ms"])
+    per_launch_ms = prof[dom]["ms"] / max(prof[dom]["calls"], 1)
+    achieved = bm[dom] / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = read_peaks()
+    traffic = read_traffic(dom)
+    step_bytes = bm["elem_sweep"] + bm["row_gather"]
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and args.cpu_states > 0:
+            threads = os.cpu_count() or 1
+            v, dt, used = cpu_chain_timing(mesh, phis, args.cpu_states, threads)
+            cpu = {"value": round(v, 4), "unit": "Melem/s", "cores": used, "kind": "port",
+                   "sample": f"{args.cpu_states} full-mesh residual+Jacobian chains of the oracle "
+                             f"(C/OpenMP restatement of the reference kernels), {dt:.1f} s"}
+        line = {
+            "metric": "residual+Jacobian Melem/s", "value": round(value, 3), "unit": "Melem/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(shape, mesh, dmesh.nnz),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "traffic": traffic,
+                         "algorithmic_bytes": bm[dom],
+                         "ms_per_launch": round(per_launch_ms, 5)},
+            "step_roofline": {"algorithmic_bytes": step_bytes,
+                              "achieved_gbs": round(step_bytes / (ms / args.steps * 1e-3) / 1e9, 1),
+                              "frac": round(step_bytes / (ms / args.steps * 1e-3) / 1e9 / peak, 4),
+                              "phases_ms_per_step": {k: round(v["ms"] / max(args.steps, 1), 5)
+                                                     for k, v in prof.items() if v["calls"]}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 3), "unit": "Melem/s",
+                    "h2d_bytes_per_step": 8 * dmesh.n_nodes,
+                    "d2h_bytes_per_step": 8 * dmesh.n_nodes + 8 * dmesh.nnz},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

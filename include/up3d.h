@@ -1,0 +1,300 @@
+/*
+ * up3d.h -- C ABI of the B200 (sm_100a) element-loop hot path of the pyfp3d
+ * full-potential solver.
+ *
+ * Conventions
+ *   - Every array argument of a per-step call is a DEVICE pointer on the
+ *     mesh's device; `stream` is a cudaStream_t (NULL = legacy default).
+ *   - Calls are asynchronous on `stream` unless they return a host value
+ *     (documented per call), in which case they synchronise that stream.
+ *   - Every call returns an up3d status; up3d_last_error() gives the message
+ *     of the last failure on the calling thread.
+ *   - A mesh handle is not thread-safe: one host thread (and one stream at a
+ *     time) per handle, like the reference's per-mesh workspaces.
+ *   - Element connectivity is int32 (n_tets, 4); node coordinates are f64
+ *     (n_nodes, 3); CSR indices are int32.
+ *
+ * Each declaration names the reference interface it replaces
+ * (file:line in swayli94/UP3D).
+ */
+#ifndef UP3D_H
+#define UP3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct up3d_mesh up3d_mesh; /* opaque per-mesh device state */
+typedef void* up3d_stream;          /* cudaStream_t */
+
+/* Status codes; the Python layer maps them to the reference's exceptions. */
+enum up3d_status {
+    UP3D_OK = 0,
+    UP3D_ERR_VALUE = -1,           /* ValueError: degenerate tet, > 256 colours, bad shapes */
+    UP3D_ERR_RUNTIME = -2,         /* RuntimeError: CUDA failure, Krylov non-convergence */
+    UP3D_ERR_NOT_IMPLEMENTED = -3, /* NotImplementedError */
+    UP3D_ERR_ARGUMENT = -4,        /* null pointer, wrong size, misuse */
+    UP3D_ERR_TIMEOUT = -5          /* a bounded device-side wait gave up */
+};
+
+/* Flow / upwind parameters shared by the per-step calls.  Defaults of the
+ * reference drivers: gamma 1.4, u_inf 1, m_cap 3, m_crit 0.95, C 1.5,
+ * rho_floor 0.05 (pyfp3d/solve/newton.py:525-528, physics/isentropic.py:21-26). */
+typedef struct {
+    double m_inf;
+    double gamma;
+    double u_inf;
+    double m_cap;
+    double m_crit;
+    double upwind_c;
+    double rho_floor;
+} up3d_flow;
+
+/* Monitors of one residual evaluation (device-resident struct written by the
+ * calls that take it; the reference keeps them as UpwindOperator attributes,
+ * pyfp3d/kernels/upwind.py:816-818, and eval_residual locals,
+ * pyfp3d/solve/newton.py:349-371). */
+typedef struct {
+    double nu_max;
+    int64_t n_supersonic;
+    int64_t n_floored;
+    int64_t n_limited;
+    int64_t n_term3_active;
+    int64_t n_term3_extra; /* Term-3 entries outside the P1 pattern */
+} up3d_monitors;
+
+typedef struct {
+    int64_t n_nodes;
+    int64_t n_tets;
+    int64_t nnz;             /* P1 pattern */
+    int32_t max_row_len;
+    int32_t max_node_degree; /* incident elements per node */
+    int32_t n_colors;        /* -1 until up3d_mesh_coloring ran */
+    int32_t device;
+} up3d_mesh_info;
+
+const char* up3d_last_error(void);
+int up3d_version(void);
+
+/* ---------------------------------------------------------------- setup */
+
+/* PicardOperator.__init__ (pyfp3d/kernels/jacobian.py:246-262) and
+ * UpwindOperator.__init__ (pyfp3d/kernels/upwind.py:744-781): element
+ * geometry B_e, V_e (mesh/metrics.py:177-204), face adjacency
+ * (mesh/metrics.py:208-278), centroids (kernels/upwind.py:750), the P1 CSR
+ * pattern (kernels/jacobian.py:60-75) and the row-gather maps.  `nodes` and
+ * `elements` are HOST arrays.  UP3D_ERR_VALUE on a degenerate tet
+ * (mesh/metrics.py:155-164) or an out-of-range node index. */
+int up3d_mesh_create(const double* nodes, const int32_t* elements, int64_t n_nodes,
+                     int64_t n_tets, int device, up3d_stream stream, up3d_mesh** out);
+int up3d_mesh_destroy(up3d_mesh* mesh);
+int up3d_mesh_get_info(const up3d_mesh* mesh, up3d_mesh_info* info);
+
+/* PicardOperator._pattern.indptr / .indices (device views, valid for the
+ * mesh's lifetime). */
+int up3d_mesh_pattern(const up3d_mesh* mesh, const int32_t** indptr, const int32_t** indices);
+
+/* PicardOperator.B (n_tets,4,3), .V (n_tets) into caller device buffers. */
+int up3d_mesh_geometry(const up3d_mesh* mesh, double* B, double* V, up3d_stream stream);
+
+/* UpwindOperator.centroids (n_tets,3) into a caller device buffer. */
+int up3d_mesh_centroids(const up3d_mesh* mesh, double* centroids, up3d_stream stream);
+
+/* UpwindOperator.face_neighbors (n_tets,4) int32: read, and overwrite (the
+ * per-side masking of pyfp3d/wake/multivalued.py:463-467). */
+int up3d_mesh_face_neighbors(const up3d_mesh* mesh, int32_t* out, up3d_stream stream);
+int up3d_mesh_set_face_neighbors(up3d_mesh* mesh, const int32_t* in, up3d_stream stream);
+
+/* color_partition_csr (pyfp3d/mesh/coloring.py:129-145): greedy colouring
+ * identical to the reference's (same visit order, smallest free colour).
+ * HOST outputs: color_offsets (n_colors+1), color_elems (n_tets); pass NULL
+ * for both to only compute and cache n_colors.  UP3D_ERR_VALUE past 256
+ * colours.  Synchronous. */
+int up3d_mesh_coloring(up3d_mesh* mesh, int64_t* color_offsets, int64_t* color_elems,
+                       int32_t* n_colors);
+
+/* PicardOperator.elem_to_csr (kernels/jacobian.py:78-103), int64
+ * (n_tets,4,4) device buffer. */
+int up3d_mesh_elem_to_csr(const up3d_mesh* mesh, int64_t* out, up3d_stream stream);
+
+/* ------------------------------------------------------ element sweeps */
+
+/* PicardOperator.velocities -> element_velocity_q2
+ * (kernels/jacobian.py:264-270, kernels/gradient.py:33-64). */
+int up3d_velocities(const up3d_mesh* mesh, const double* phi, double* grad, double* q2,
+                    up3d_stream stream);
+
+/* element_velocity_q2 on raw arrays (kernels/gradient.py:33-64): elements
+ * int32 (n_tets,4), B (n_tets,4,3), all device pointers. */
+int up3d_element_velocity_q2(const int32_t* elements, const double* B, const double* phi, int64_t n_tets,
+                             double* grad, double* q2, up3d_stream stream);
+
+/* limit_q2_field (physics/isentropic.py:293-314); if n_limited is non-NULL
+ * it receives (device int64) the count of elements with out != q2. */
+int up3d_limit_q2(const double* q2, int64_t n, double m_inf, double m_cap, double gamma,
+                  double* out, int64_t* n_limited, up3d_stream stream);
+/* density_field (physics/isentropic.py:236-258). */
+int up3d_density(const double* q2, int64_t n, double m_inf, double gamma, double* out,
+                 up3d_stream stream);
+/* mach_squared_field (physics/isentropic.py:318-334). */
+int up3d_mach_squared(const double* q2, int64_t n, double m_inf, double gamma, double* out,
+                      up3d_stream stream);
+/* density_derivative_wrt_q_sq_field (physics/isentropic.py:338-354). */
+int up3d_density_derivative(const double* q2, int64_t n, double m_inf, double gamma,
+                            double* out, up3d_stream stream);
+/* mach_squared_derivative_wrt_q_sq_field (physics/isentropic.py:358-374). */
+int up3d_mach_squared_derivative(const double* q2, int64_t n, double m_inf, double gamma,
+                                 double* out, up3d_stream stream);
+/* pressure_coefficient, elementwise (physics/isentropic.py:122-143). */
+int up3d_pressure_coefficient(const double* q2, int64_t n, double m_inf, double gamma,
+                              double* out, up3d_stream stream);
+
+/* upstream_elements (kernels/upwind.py:69-125), max_hops 4.  `grad` is
+ * (n_tets,3); `upstream` is int64 (n_tets). */
+int up3d_upwind_walk(const up3d_mesh* mesh, const double* grad, int64_t* upstream,
+                     up3d_stream stream);
+
+/* rho_tilde_sweep + monitors (kernels/upwind.py:457-500, :816-818).
+ * `monitors` (device) may be NULL. */
+int up3d_rho_tilde(const double* q2, const double* rho, const int64_t* upstream, int64_t n,
+                   const up3d_flow* flow, double* nu, double* rho_tilde,
+                   up3d_monitors* monitors, up3d_stream stream);
+/* classify_upwind_branches (kernels/upwind.py:504-541); branch int8. */
+int up3d_classify_branches(const double* q2, const double* rho, const int64_t* upstream,
+                           int64_t n, const up3d_flow* flow, int8_t* branch,
+                           up3d_stream stream);
+/* rho_tilde_frozen_sweep + monitors (kernels/upwind.py:545-593, :861-863). */
+int up3d_rho_tilde_frozen(const double* q2, const double* rho, const int64_t* upstream,
+                          const int8_t* branch, int64_t n, const up3d_flow* flow, double* nu,
+                          double* rho_tilde, up3d_monitors* monitors, up3d_stream stream);
+/* rho_tilde_sensitivities_sweep (kernels/upwind.py:647-730). */
+int up3d_rho_tilde_sens(const double* q2, const double* rho, const int64_t* upstream,
+                        int64_t n, const up3d_flow* flow, double* s_e, double* s_u,
+                        up3d_stream stream);
+/* rho_tilde_frozen_sensitivities_sweep (kernels/upwind.py:597-643). */
+int up3d_rho_tilde_frozen_sens(const double* q2, const double* rho, const int64_t* upstream,
+                               const int8_t* branch, int64_t n, const up3d_flow* flow,
+                               double* s_e, double* s_u, up3d_stream stream);
+
+/* ------------------------------------------------------------ assembly */
+
+/* PicardOperator.assemble_residual (kernels/jacobian.py:361-375 ->
+ * kernels/residual.py:44-76).  rho_tilde NULL means rho == 1.  Like the
+ * reference, the call also leaves grad(phi) (n_tets,3) and q^2 in the
+ * velocity workspace: `grad_out` / `q2_out` when given, else a
+ * library-internal buffer. */
+int up3d_residual(up3d_mesh* mesh, const double* phi, const double* rho_tilde, double* R,
+                  double* grad_out, double* q2_out, up3d_stream stream);
+
+/* PicardOperator.assemble_matrix (kernels/jacobian.py:272-286 ->
+ * :106-130): CSR data on the P1 pattern.  rho_tilde NULL means rho == 1. */
+int up3d_picard_matrix(up3d_mesh* mesh, const double* rho_tilde, double* data,
+                       up3d_stream stream);
+
+/* PicardOperator.assemble_newton_jacobian (kernels/jacobian.py:288-359):
+ * Terms 1+2 (+ the in-pattern part of Term 3) into `data` on the P1
+ * pattern; Term-3 entries outside the pattern are kept in the mesh
+ * workspace for up3d_jacobian_export.  lim_mask (uint8, NULL = none) gates
+ * s_e by lim[e] and s_u by lim[upstream[e]].  Inputs are not modified.
+ * Host outputs (synchronous): n_term3_active, n_extra, newton_nnz (nnz of
+ * the merged matrix, exact zeros dropped when Term 3 is active, as scipy's
+ * CSR addition does). */
+int up3d_jacobian(up3d_mesh* mesh, const double* phi, const double* rho_tilde,
+                  const double* s_e, const double* s_u, const int64_t* upstream, double u_inf,
+                  const uint8_t* lim_mask, double* data, int64_t* n_term3_active,
+                  int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream);
+
+/* The merged CSR (P1 pattern data + Term-3 extras) of the last up3d_jacobian
+ * or up3d_residual_jacobian call into caller device buffers of sizes
+ * n_nodes+1 and newton_nnz. */
+int up3d_jacobian_export(up3d_mesh* mesh, const double* data, int32_t* indptr,
+                         int32_t* indices, double* merged, up3d_stream stream);
+
+/* newton_nnz of the last Jacobian (kernels/jacobian.py:358): the P1 nnz, or,
+ * when Term 3 is active, the non-zeros of the merged matrix.  Synchronous. */
+int up3d_jacobian_nnz(up3d_mesh* mesh, const double* data, int64_t* newton_nnz,
+                      up3d_stream stream);
+
+/* Fused eval_residual + assemble_coupled without a wake
+ * (pyfp3d/solve/newton.py:345-372 and :435-452 with T = I): velocities,
+ * limiter, density, walk, live flux (or the frozen flux when `upstream_frozen`
+ * and `branch_frozen` are non-NULL), sensitivities, residual R (n_nodes) and
+ * the Newton Jacobian data on the P1 pattern (NULL skips the Jacobian).
+ * Monitors (device, may be NULL).  rho_tilde_out / upstream_out (device,
+ * may be NULL) receive the flux and the walk. */
+int up3d_residual_jacobian(up3d_mesh* mesh, const double* phi, const up3d_flow* flow,
+                           const int64_t* upstream_frozen, const int8_t* branch_frozen,
+                           double* R, double* data, double* rho_tilde_out,
+                           int32_t* upstream_out, up3d_monitors* monitors,
+                           up3d_stream stream);
+
+/* ------------------------------------------------------ accounting */
+
+/* Number of library kernel launches since the library was loaded (the
+ * reference has no counterpart; used to report device launches per step). */
+int up3d_launch_count(int64_t* out);
+/* Enable (1) / disable (0) per-phase CUDA-event timing and reset it. */
+int up3d_profile(int enable);
+/* Per phase slot (0 element sweep, 1 row gather, 2 Term-3 build, 3 SpMV,
+ * 4 Krylov vector work): summed milliseconds, timed calls and kernel
+ * launches since up3d_profile(1).  Synchronises the recorded events. */
+int up3d_profile_read(double* ms, int64_t* calls, int64_t* launches, int n_slots);
+
+/* ------------------------------------------------------ linear algebra */
+
+/* CSR SpMV y = A x (the scipy product inside spla.cg / spla.gmres,
+ * solve/picard.py:375-380, solve/linear.py:182).  `dirichlet` (uint8 per
+ * row, NULL = none) makes constrained rows act as identity and drops
+ * constrained columns: the free-DOF operator A[free][:, free] embedded in
+ * full size (solve/linear.py:20-58). */
+int up3d_spmv(int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+              const double* data, const double* x, double* y, const uint8_t* dirichlet,
+              up3d_stream stream);
+/* FP32 variant (mixed precision). */
+int up3d_spmv_f32(int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+                  const float* data, const float* x, float* y, const uint8_t* dirichlet,
+                  up3d_stream stream);
+
+/* A device CSR operand of the solvers.  `dirichlet` (NULL = none) embeds the
+ * free-DOF system A[free][:, free] in full size (identity rows, dropped
+ * columns); right-hand sides must then be zero on constrained rows. */
+typedef struct {
+    int64_t n;
+    const int32_t* indptr;
+    const int32_t* indices;
+    const double* data;
+    const uint8_t* dirichlet;
+} up3d_csr;
+
+typedef struct up3d_precond up3d_precond; /* opaque preconditioner */
+
+/* Point-Jacobi preconditioner z = D^{-1} r (constrained rows: identity). */
+int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream);
+/* z = M r */
+int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream stream);
+int up3d_precond_destroy(up3d_precond* M);
+
+/* Preconditioned CG (scipy.sparse.linalg.cg as called by solve_cg_amg,
+ * solve/linear.py:204-239, and solve_subsonic, solve/picard.py:375-380):
+ * x holds x0 on entry and the iterate on exit; converged when
+ * ||b - A x|| <= max(rtol ||b||, atol).  info = 0 converged, else maxiter.
+ * Synchronous. */
+int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double atol,
+            int maxiter, up3d_precond* M, int64_t* iters, double* resid, int* info,
+            up3d_stream stream);
+
+/* Restarted left-preconditioned GMRES (scipy.sparse.linalg.gmres as called
+ * by solve_gmres, solve/linear.py:134-201): operator A (+ `extra`, the
+ * Term-3 entries outside the P1 pattern, may be NULL); `maxiter` counts
+ * restart cycles; inner = total Arnoldi steps.  Synchronous. */
+int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double* x,
+               double rtol, double atol, int restart, int maxiter, up3d_precond* M,
+               int64_t* inner, double* resid, int* info, up3d_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UP3D_H */

@@ -1,0 +1,727 @@
+// Residual, Picard matrix and Newton Jacobian assembly of the up3d library.
+//
+// Scatter-free design: every CSR row (and residual entry) is produced by one
+// warp that gathers the contributions of the row node's incident elements
+// from a per-element record (gB_j = grad . B_j and the Term-1/2/3 weights)
+// and writes the row once.  The summation order of every entry is fixed by
+// the mesh-setup plan, so results are bit-reproducible run to run with no
+// atomics, as the reference's colour-ordered scatter is
+// (kernels/jacobian.py:1-33, kernels/residual.py:44-76).
+//
+// Term 3 (upstream coupling, off the element pattern) is built per call
+// from the active elements in ascending order as COO triplets, stably
+// sorted and summed per (row, column) -- the reference's fill_term3_coo +
+// COO -> CSR merge (kernels/jacobian.py:184-229, :344-358).
+
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include "elem.cuh"
+#include "internal.cuh"
+
+namespace up3d {
+
+namespace {
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+constexpr int RG_WARPS = 8;   // warps per block of the row gather
+constexpr int RG_MAXE = 64;   // incident elements per row staged in shared memory
+constexpr int WIDE_MAXE = 1024;
+
+struct RecView {
+    double gB[4];
+    double w1, w2;
+};
+
+__device__ __forceinline__ RecView load_rec(const ElemRecord* __restrict__ rec, int64_t e) {
+    const double2* p = reinterpret_cast<const double2*>(rec + e);
+    double2 a = p[0], b = p[1], c = p[2];
+    RecView r;
+    r.gB[0] = a.x;
+    r.gB[1] = a.y;
+    r.gB[2] = b.x;
+    r.gB[3] = b.y;
+    r.w1 = c.x;
+    r.w2 = c.y;
+    return r;
+}
+
+__device__ __forceinline__ double pick4(int i, double a, double b, double c, double d) {
+    return i == 0 ? a : (i == 1 ? b : (i == 2 ? c : d));
+}
+
+// Row i of the packed symmetric element matrix B B^T
+// (storage order 00,01,02,03,11,12,13,22,23,33).
+__device__ __forceinline__ void bb_row(const double* __restrict__ BB, int64_t e, int i, double out[4]) {
+    const double2* p = reinterpret_cast<const double2*>(BB + 10 * e);
+    double2 v0 = p[0], v1 = p[1], v2 = p[2], v3 = p[3], v4 = p[4];
+    // v0=(00,01) v1=(02,03) v2=(11,12) v3=(13,22) v4=(23,33)
+    out[0] = pick4(i, v0.x, v0.y, v1.x, v1.y);
+    out[1] = pick4(i, v0.y, v2.x, v2.y, v3.x);
+    out[2] = pick4(i, v1.x, v2.y, v3.y, v4.x);
+    out[3] = pick4(i, v1.y, v3.x, v4.x, v4.y);
+}
+
+// One warp per row: R_n = sum_e w1_e gB_e,i and the row of
+//   J_nm = sum_e w1_e (B_i . B_j) + [w2_e != 0] w2_e gB_i gB_j
+// (kernels/jacobian.py:406-433: Term 2 only when its weight is non-zero, so
+// J reduces to the Picard matrix bitwise at s_e = 0).
+template <bool DO_R, bool DO_J, int MAXE, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
+                 const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
+                 const uint16_t* __restrict__ plan, const int32_t* __restrict__ diag,
+                 const double* __restrict__ BB, const ElemRecord* __restrict__ rec, double* __restrict__ R,
+                 double* __restrict__ J, bool wide_pass) {
+    extern __shared__ double smem_vals[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* vals = smem_vals + (size_t)w * MAXE * 4;
+    for (int64_t n = (int64_t)blockIdx.x * WARPS + w; n < N; n += (int64_t)gridDim.x * WARPS) {
+        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
+        // the narrow pass skips rows that need the wide buffer and vice versa
+        if (wide_pass ? deg <= RG_MAXE : deg > RG_MAXE) continue;
+        double r = 0.0, d = 0.0;
+        for (int k = lane; k < deg; k += 32) {
+            uint32_t x = ent[eb + k];
+            int64_t e = x >> 2;
+            int i = x & 3;
+            RecView q = load_rec(rec, e);
+            double gBi = pick4(i, q.gB[0], q.gB[1], q.gB[2], q.gB[3]);
+            if (DO_R) r += q.w1 * gBi;
+            if (DO_J) {
+                double bij[4];
+                bb_row(BB, e, i, bij);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    double c = q.w1 * bij[j];
+                    if (q.w2 != 0.0) c += q.w2 * gBi * q.gB[j];
+                    vals[j * MAXE + k] = c;
+                    if (j == i) d += c;
+                }
+            }
+        }
+        if (DO_R) r = warp_sum(r);
+        if (DO_J) {
+            d = warp_sum(d);
+            __syncwarp();
+            const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
+            for (int s = lane; s < L; s += 32) {
+                double v = d;
+                if (s != ds) {
+                    v = 0.0;
+                    const int32_t p1 = plan_off[rb + s + 1];
+                    for (int32_t p = plan_off[rb + s]; p < p1; ++p) {
+                        uint32_t c = plan[p];
+                        v += vals[(c & 3) * MAXE + (c >> 2)];
+                    }
+                }
+                J[rb + s] = v;
+            }
+            __syncwarp();
+        }
+        if (DO_R && lane == 0) R[n] = r;
+    }
+}
+
+template <bool DO_R, bool DO_J>
+void launch_row_gather(const up3d_mesh* m, const ElemRecord* rec, double* R, double* J, cudaStream_t s) {
+    {
+        const size_t sm = sizeof(double) * RG_WARPS * RG_MAXE * 4;
+        auto kern = k_row_gather<DO_R, DO_J, RG_MAXE, RG_WARPS>;
+        const unsigned grid = grid_for(m->N, RG_WARPS, (int64_t)148 * 64);
+        kern<<<grid, RG_WARPS * 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
+                                              m->plan_off.get(), m->plan.get(), m->diag.get(), m->BB.get(), rec,
+                                              R, J, false);
+        UP3D_CHECK_LAUNCH();
+    }
+    if (m->max_deg > RG_MAXE) {
+        UP3D_REQUIRE(m->max_deg <= WIDE_MAXE, UP3D_ERR_VALUE,
+                     "a node is shared by more than 1024 elements; unsupported by the row gather");
+        const size_t sm = sizeof(double) * WIDE_MAXE * 4;
+        auto kern = k_row_gather<DO_R, DO_J, WIDE_MAXE, 1>;
+        UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<148 * 4, 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(),
+                                     m->plan.get(), m->diag.get(), m->BB.get(), rec, R, J, true);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+// ------------------------------------------------------------ prep kernels
+
+__device__ __forceinline__ void store_rec(ElemRecord* __restrict__ rec, int64_t e, const double gB[4], double w1,
+                                          double w2, double w3, double flag) {
+    double2* p = reinterpret_cast<double2*>(rec + e);
+    p[0] = make_double2(gB[0], gB[1]);
+    p[1] = make_double2(gB[2], gB[3]);
+    p[2] = make_double2(w1, w2);
+    p[3] = make_double2(w3, flag);
+}
+
+__device__ __forceinline__ void gB_of(const double g[3], const double* __restrict__ b, double gB[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) gB[j] = g[0] * b[3 * j] + g[1] * b[3 * j + 1] + g[2] * b[3 * j + 2];
+}
+
+// assemble_residual: velocities into the workspace (kernels/jacobian.py:623)
+// and the per-element record with w1 = rho_tilde V.
+__global__ void k_prep_residual(const int4* __restrict__ conn, const double* __restrict__ B,
+                                const double* __restrict__ V, const double* __restrict__ phi,
+                                const double* __restrict__ rt, int64_t E, double* __restrict__ grad,
+                                double* __restrict__ q2, ElemRecord* __restrict__ rec) {
+    GRID_STRIDE(e, E) {
+        double g[3], b[12];
+        int4 c;
+        elem_grad_B(conn, B, phi, e, g, b, c);
+        grad[3 * e] = g[0];
+        grad[3 * e + 1] = g[1];
+        grad[3 * e + 2] = g[2];
+        q2[e] = dot3r(g[0], g[1], g[2], g[0], g[1], g[2]);
+        double gB[4];
+        gB_of(g, b, gB);
+        double w1 = (rt ? rt[e] : 1.0) * V[e];
+        store_rec(rec, e, gB, w1, 0.0, 0.0, 0.0);
+    }
+}
+
+// assemble_matrix: w1 = rho_tilde V only.
+__global__ void k_prep_matrix(const double* __restrict__ V, const double* __restrict__ rt, int64_t E,
+                              ElemRecord* __restrict__ rec) {
+    GRID_STRIDE(e, E) {
+        double z[4] = {0.0, 0.0, 0.0, 0.0};
+        store_rec(rec, e, z, (rt ? rt[e] : 1.0) * V[e], 0.0, 0.0, 0.0);
+    }
+}
+
+// assemble_newton_jacobian (kernels/jacobian.py:323-338, :410-414): the
+// limiter mask gates s_e by lim[e] and s_u by lim[upstream[e]]; Term-2 and
+// Term-3 weights 2 inv_u2 s V; the upstream factor grad_u . B_u,k of active
+// elements (s_u != 0).  `grad` holds grad(phi) of every element.
+__global__ void k_prep_jacobian(const int4* __restrict__ conn, const double* __restrict__ B,
+                                const double* __restrict__ V, const double* __restrict__ grad,
+                                const double* __restrict__ rt, const double* __restrict__ se,
+                                const double* __restrict__ su, const int64_t* __restrict__ up,
+                                const uint8_t* __restrict__ lim, double inv_u2, int64_t E,
+                                ElemRecord* __restrict__ rec, double* __restrict__ t3b,
+                                int32_t* __restrict__ up32) {
+    GRID_STRIDE(e, E) {
+        const double* b = B + 12 * e;
+        double g[3] = {grad[3 * e], grad[3 * e + 1], grad[3 * e + 2]};
+        double gB[4];
+        gB_of(g, b, gB);
+        int64_t u = safe_up(up[e], e, E);
+        double s_e = se[e], s_u = su[e];
+        if (lim) {
+            s_e = s_e * (lim[e] ? 1.0 : 0.0);
+            s_u = s_u * (lim[u] ? 1.0 : 0.0);
+        }
+        double Ve = V[e];
+        double w2 = 2.0 * inv_u2 * s_e * Ve;
+        double w3 = 2.0 * inv_u2 * s_u * Ve;
+        bool active = s_u != 0.0;
+        if (active) {
+            const double* bu = B + 12 * u;
+            double gu[3] = {grad[3 * u], grad[3 * u + 1], grad[3 * u + 2]};
+            double f[4];
+            gB_of(gu, bu, f);
+            reinterpret_cast<double2*>(t3b + 4 * e)[0] = make_double2(f[0], f[1]);
+            reinterpret_cast<double2*>(t3b + 4 * e)[1] = make_double2(f[2], f[3]);
+        }
+        up32[e] = (int32_t)u;
+        store_rec(rec, e, gB, rt[e] * Ve, w2, w3, active ? 1.0 : 0.0);
+    }
+}
+
+// ------------------------------------------------------------ fused sweep
+
+struct MonAcc {
+    double nu_max = 0.0;
+    unsigned long long sup = 0, flo = 0, lim = 0, act = 0;
+};
+
+__device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
+    double nm = warp_max(a.nu_max);
+    unsigned long long s = warp_sum_u64(a.sup), f = warp_sum_u64(a.flo), l = warp_sum_u64(a.lim),
+                       t = warp_sum_u64(a.act);
+    if ((threadIdx.x & 31) == 0) {
+        if (nm > 0.0) atomic_max_nonneg(&mon->nu_max, nm);
+        if (s) atomicAdd(reinterpret_cast<unsigned long long*>(&mon->n_supersonic), s);
+        if (f) atomicAdd(reinterpret_cast<unsigned long long*>(&mon->n_floored), f);
+        if (l) atomicAdd(reinterpret_cast<unsigned long long*>(&mon->n_limited), l);
+        if (t) atomicAdd(reinterpret_cast<unsigned long long*>(&mon->n_term3_active), t);
+    }
+}
+
+// eval_residual + assemble_coupled, per element (pyfp3d/solve/newton.py:
+// 345-372, :435-452): gradient, limiter, density, upstream walk (or the
+// frozen selection), the upstream element's state recomputed in place, the
+// flux, its sensitivities and the element record.
+template <bool FROZEN, bool JAC>
+__global__ void __launch_bounds__(256)
+    k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
+                 const int4* __restrict__ fn, const double4* __restrict__ cen, const double4* __restrict__ X,
+                 const double* __restrict__ phi, Flow F, double u2, const int64_t* __restrict__ up_fz,
+                 const int8_t* __restrict__ br_fz, int64_t E, ElemRecord* __restrict__ rec,
+                 double* __restrict__ t3b, int32_t* __restrict__ up_out, double* __restrict__ rt_out,
+                 up3d_monitors* mon) {
+    MonAcc acc;
+    GRID_STRIDE(e, E) {
+        double g[3], b[12];
+        int4 c;
+        elem_grad_B(conn, B, phi, e, g, b, c);
+        double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), u2);
+        double q2l = q2n < F.q2cap ? q2n : F.q2cap;
+        bool lim_e = q2l == q2n;
+        double rho_e, drho_e;
+        rho_drho(q2l, F, rho_e, drho_e);
+
+        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, cen, X, conn, e, E, g);
+        double q2lu = q2l, rho_u = rho_e;
+        bool lim_u = lim_e;
+        double gu[3] = {g[0], g[1], g[2]};
+        double bu[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) bu[k] = b[k];
+        if (u != e) {
+            int4 cu;
+            elem_grad_B(conn, B, phi, u, gu, bu, cu);
+            double q2nu = __ddiv_rn(dot3r(gu[0], gu[1], gu[2], gu[0], gu[1], gu[2]), u2);
+            q2lu = q2nu < F.q2cap ? q2nu : F.q2cap;
+            lim_u = q2lu == q2nu;
+            rho_u = rho_of(q2lu, F);
+        }
+        acc.lim += !lim_e;
+
+        double nu, rt, s_e = 0.0, s_u = 0.0;
+        if (FROZEN) {
+            int br = br_fz[e];
+            if (br == 3) {
+                nu = 0.0;
+                rt = F.floor_;
+                acc.flo += 1;
+            } else if (br == 0) {
+                nu = 0.0;
+                rt = rho_e;
+            } else {
+                nu = switch_of(mach2_of(br == 1 ? q2l : q2lu, F), F);
+                rt = rho_e - nu * (rho_e - rho_u);
+            }
+            if (JAC) frozen_sensitivities(br, q2l, rho_e, q2lu, rho_u, F, s_e, s_u);
+        } else {
+            nu = fmax(switch_of(mach2_of(q2l, F), F), switch_of(mach2_of(q2lu, F), F));
+            rt = rho_e - nu * (rho_e - rho_u);
+            rt = rt > F.floor_ ? rt : F.floor_;
+            acc.flo += (rt == F.floor_);
+            if (JAC) live_sensitivities(q2l, rho_e, q2lu, rho_u, u == e, F, s_e, s_u);
+        }
+        acc.nu_max = fmax(acc.nu_max, nu);
+        acc.sup += (nu > 0.0);
+
+        double gB[4];
+        gB_of(g, b, gB);
+        double Ve = V[e];
+        double w2 = 0.0, w3 = 0.0;
+        bool active = false;
+        if (JAC) {
+            s_e = s_e * (lim_e ? 1.0 : 0.0);
+            s_u = s_u * (lim_u ? 1.0 : 0.0);
+            w2 = 2.0 * F.inv_u2 * s_e * Ve;
+            w3 = 2.0 * F.inv_u2 * s_u * Ve;
+            active = s_u != 0.0;
+            if (active) {
+                double f[4];
+                gB_of(gu, bu, f);
+                reinterpret_cast<double2*>(t3b + 4 * e)[0] = make_double2(f[0], f[1]);
+                reinterpret_cast<double2*>(t3b + 4 * e)[1] = make_double2(f[2], f[3]);
+                acc.act += 1;
+            }
+        }
+        store_rec(rec, e, gB, rt * Ve, w2, w3, active ? 1.0 : 0.0);
+        up_out[e] = (int32_t)u;
+        if (rt_out) rt_out[e] = rt;
+    }
+    flush(acc, mon);
+}
+
+// ------------------------------------------------------------ Term 3
+
+__global__ void k_t3_flags(const ElemRecord* __restrict__ rec, int64_t E, uint8_t* __restrict__ flag) {
+    GRID_STRIDE(e, E) flag[e] = rec[e].pad != 0.0;
+}
+
+// fill_term3_coo (kernels/jacobian.py:184-229): 16 entries per active
+// element, rows nodes(e) x cols nodes(u(e)), slot 16a + 4i + k.
+__global__ void k_t3_coo(const int32_t* __restrict__ active, const int64_t* __restrict__ n_active,
+                         const int4* __restrict__ conn, const int32_t* __restrict__ up,
+                         const ElemRecord* __restrict__ rec, const double* __restrict__ t3b,
+                         uint64_t* __restrict__ keys, double* __restrict__ vals, int32_t* __restrict__ perm) {
+    const int64_t A = *n_active;
+    GRID_STRIDE(a, A) {
+        int64_t e = active[a];
+        int64_t u = up[e];
+        int4 ce = conn[e], cu = conn[u];
+        int re[4] = {ce.x, ce.y, ce.z, ce.w};
+        int cl[4] = {cu.x, cu.y, cu.z, cu.w};
+        const ElemRecord& q = rec[e];
+        for (int i = 0; i < 4; ++i) {
+            double wi = q.w3 * q.gB[i];
+            for (int k = 0; k < 4; ++k) {
+                int64_t idx = 16 * a + 4 * i + k;
+                keys[idx] = ((uint64_t)(uint32_t)re[i] << 32) | (uint32_t)cl[k];
+                vals[idx] = wi * t3b[4 * e + k];
+                perm[idx] = (int32_t)idx;
+            }
+        }
+    }
+}
+
+__global__ void k_t3_heads(const uint64_t* __restrict__ keys, int64_t n, int32_t* __restrict__ head) {
+    GRID_STRIDE(i, n) head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// One thread per unique (row, col): the run's values in stable-sorted
+// (= COO) order, then the in-pattern part folded into the P1 data and the
+// rest kept as extras.
+__global__ void k_t3_reduce(const uint64_t* __restrict__ keys, const double* __restrict__ vals,
+                            const int32_t* __restrict__ perm, const int32_t* __restrict__ seg, int64_t n,
+                            const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                            double* __restrict__ data, int32_t* __restrict__ xrow, int32_t* __restrict__ xcol,
+                            double* __restrict__ xval, int32_t* __restrict__ xflag) {
+    GRID_STRIDE(i, n) {
+        if (!(i == 0 || keys[i] != keys[i - 1])) continue;
+        int64_t j = i;
+        double v = 0.0;
+        while (j < n && keys[j] == keys[i]) {
+            v += vals[perm[j]];
+            ++j;
+        }
+        int32_t row = (int32_t)(keys[i] >> 32), col = (int32_t)(keys[i] & 0xffffffffu);
+        int32_t rb = indptr[row], L = indptr[row + 1] - rb;
+        int32_t lo = 0, hi = L;
+        while (lo < hi) {
+            int32_t mid = (lo + hi) >> 1;
+            if (indices[rb + mid] < col) lo = mid + 1; else hi = mid;
+        }
+        int32_t s = seg[i];
+        if (lo < L && indices[rb + lo] == col) {
+            data[rb + lo] += v;
+            xflag[s] = 0;
+        } else {
+            xflag[s] = 1;
+        }
+        xrow[s] = row;
+        xcol[s] = col;
+        xval[s] = v;
+    }
+}
+
+__global__ void k_count_nonzero(const double* __restrict__ v, int64_t n, unsigned long long* out) {
+    unsigned long long c = 0;
+    GRID_STRIDE(i, n) c += (v[i] != 0.0);
+    c = warp_sum_u64(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+// Merged row lengths / fill of (P1 data + extras), optionally dropping
+// exact zeros (scipy's CSR addition does, kernels/jacobian.py:355-357).
+template <bool FILL>
+__global__ void k_merge_rows(int64_t N, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                             const double* __restrict__ data, const int32_t* __restrict__ xptr,
+                             const int32_t* __restrict__ xcol, const double* __restrict__ xval, bool drop_zeros,
+                             int32_t* __restrict__ out_ptr, int32_t* __restrict__ out_idx,
+                             double* __restrict__ out_val) {
+    GRID_STRIDE(n, N) {
+        int32_t a = indptr[n], ae = indptr[n + 1];
+        int32_t b = xptr ? xptr[n] : 0, be = xptr ? xptr[n + 1] : 0;
+        int32_t pos = FILL ? out_ptr[n] : 0;
+        int32_t cnt = 0;
+        while (a < ae || b < be) {
+            int32_t col;
+            double v;
+            if (b >= be || (a < ae && indices[a] < xcol[b])) {
+                col = indices[a];
+                v = data[a++];
+            } else {
+                col = xcol[b];
+                v = xval[b++];
+            }
+            if (drop_zeros && v == 0.0) continue;
+            if (FILL) {
+                out_idx[pos + cnt] = col;
+                out_val[pos + cnt] = v;
+            }
+            ++cnt;
+        }
+        if (!FILL) out_ptr[n] = cnt;
+    }
+}
+
+__global__ void k_rows_from_extras(const int32_t* __restrict__ xrow, int64_t n, int32_t* __restrict__ cnt) {
+    GRID_STRIDE(i, n) atomicAdd(&cnt[xrow[i]], 1);
+}
+
+template <class T>
+void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
+    size_t bytes = 0;
+    UP3D_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+    m->cub_tmp.alloc(bytes);
+    UP3D_CUDA(cub::DeviceScan::ExclusiveSum(m->cub_tmp.get(), bytes, in, out, n, s));
+}
+
+}  // namespace
+
+// Builds Term 3 from the element records (flag = pad != 0): folds the
+// in-pattern part into `data`, keeps the extras (sorted by row, col) in the
+// mesh workspace, and returns (n_active, n_extra).  Synchronises the stream.
+static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra) {
+        const int64_t E = m->E;
+    m->t3_flag.alloc(E);
+    m->t3_active.alloc(E);
+    m->i64_ws.alloc(8);
+    k_t3_flags<<<grid_for(E, 256), 256, 0, s>>>(m->rec.get(), E, m->t3_flag.get());
+    UP3D_CHECK_LAUNCH();
+    size_t bytes = 0;
+    thrust::counting_iterator<int32_t> it(0);
+    UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(), E, s));
+    m->cub_tmp.alloc(bytes);
+    UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(),
+                                         E, s));
+    UP3D_CUDA(cudaMemcpyAsync(&n_active, m->i64_ws.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    n_extra = 0;
+    m->last_active = n_active;
+    m->last_extra = 0;
+    if (n_active == 0) return;
+    const int64_t n = 16 * n_active;
+    m->t3_keys.alloc(n);
+    m->t3_keys_s.alloc(n);
+    m->t3_vals.alloc(n);
+    m->t3_perm.alloc(n);
+    m->t3_perm_s.alloc(n);
+    m->t3_head.alloc(n);
+    m->t3_seg.alloc(n);
+    k_t3_coo<<<grid_for(n_active, 128), 128, 0, s>>>(m->t3_active.get(), m->i64_ws.get(), m->conn.get(), m->up32.get(),
+                                                     m->rec.get(), m->t3b.get(), m->t3_keys.get(), m->t3_vals.get(),
+                                                     m->t3_perm.get());
+    UP3D_CHECK_LAUNCH();
+    int end_bit = 32;
+    {
+        int b = 1;
+        while ((1ll << b) < m->N) ++b;
+        end_bit = 32 + b;
+    }
+    bytes = 0;
+    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, m->t3_keys.get(), m->t3_keys_s.get(), m->t3_perm.get(),
+                                              m->t3_perm_s.get(), n, 0, end_bit, s));
+    m->cub_tmp.alloc(bytes);
+    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(m->cub_tmp.get(), bytes, m->t3_keys.get(), m->t3_keys_s.get(), m->t3_perm.get(),
+                                              m->t3_perm_s.get(), n, 0, end_bit, s));
+    k_t3_heads<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), n, m->t3_head.get());
+    UP3D_CHECK_LAUNCH();
+    scan(m, m->t3_head.get(), m->t3_seg.get(), n, s);
+    int32_t last_seg = 0, last_head = 0;
+    UP3D_CUDA(cudaMemcpyAsync(&last_seg, m->t3_seg.get() + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(&last_head, m->t3_head.get() + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    const int64_t n_uniq = (int64_t)last_seg + last_head;
+    m->x_row.alloc(n_uniq);
+    m->x_col.alloc(n_uniq);
+    m->x_val.alloc(n_uniq);
+    m->x_flag.alloc(n_uniq + 1);
+    k_t3_reduce<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), m->t3_vals.get(), m->t3_perm_s.get(), m->t3_seg.get(), n,
+                                                 m->indptr.get(), m->indices.get(), data, m->x_row.get(), m->x_col.get(),
+                                                 m->x_val.get(), m->x_flag.get());
+    UP3D_CHECK_LAUNCH();
+    // compact the extras (keeps the (row, col) order)
+    m->x_row_c.alloc(n_uniq);
+    m->x_col_c.alloc(n_uniq);
+    m->x_val_c.alloc(n_uniq);
+    auto compact = [&](auto* in, auto* out) {
+        size_t b2 = 0;
+        UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, b2, in, m->x_flag.get(), out, m->i64_ws.get() + 1, n_uniq, s));
+        m->cub_tmp.alloc(b2);
+        UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), b2, in, m->x_flag.get(), out, m->i64_ws.get() + 1,
+                                             n_uniq, s));
+    };
+    compact(m->x_row.get(), m->x_row_c.get());
+    compact(m->x_col.get(), m->x_col_c.get());
+    compact(m->x_val.get(), m->x_val_c.get());
+    UP3D_CUDA(cudaMemcpyAsync(&n_extra, m->i64_ws.get() + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    m->last_extra = n_extra;
+    // extras row pointer
+    m->x_ptr.alloc(m->N + 1);
+    UP3D_CUDA(cudaMemsetAsync(m->x_ptr.get(), 0, sizeof(int32_t) * (m->N + 1), s));
+    if (n_extra > 0) {
+        DBuf<int32_t> cnt;
+        cnt.alloc(m->N + 1);
+        UP3D_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
+        k_rows_from_extras<<<grid_for(n_extra, 256), 256, 0, s>>>(m->x_row_c.get(), n_extra, cnt.get());
+        UP3D_CHECK_LAUNCH();
+        scan(m, cnt.get(), m->x_ptr.get(), m->N + 1, s);
+        UP3D_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+static int64_t merged_nnz(up3d_mesh* m, const double* data, cudaStream_t s) {
+    if (m->last_active == 0) return m->nnz;
+        DBuf<unsigned long long> c;
+    c.alloc(1);
+    UP3D_CUDA(cudaMemsetAsync(c.get(), 0, sizeof(unsigned long long), s));
+    k_count_nonzero<<<grid_for(m->nnz, 256), 256, 0, s>>>(data, m->nnz, c.get());
+    UP3D_CHECK_LAUNCH();
+    if (m->last_extra > 0) {
+        k_count_nonzero<<<grid_for(m->last_extra, 256), 256, 0, s>>>(m->x_val_c.get(), m->last_extra, c.get());
+        UP3D_CHECK_LAUNCH();
+    }
+    unsigned long long h = 0;
+    UP3D_CUDA(cudaMemcpyAsync(&h, c.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    return (int64_t)h;
+}
+
+// launchers used by other translation units
+void row_gather_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
+    launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
+}
+
+}  // namespace up3d
+
+using namespace up3d;
+
+extern "C" {
+
+int up3d_residual(up3d_mesh* m, const double* phi, const double* rt, double* R, double* grad_out, double* q2_out,
+                  up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && R, UP3D_ERR_ARGUMENT, "up3d_residual: null argument");
+        cudaStream_t s = S(stream);
+        if (!grad_out) {
+            m->grad_ws.alloc(3 * m->E);
+            grad_out = m->grad_ws.get();
+        }
+        if (!q2_out) {
+            m->q2_ws.alloc(m->E);
+            q2_out = m->q2_ws.get();
+        }
+        k_prep_residual<<<grid_for(m->E, 256), 256, 0, s>>>(m->conn.get(), m->B.get(), m->V.get(), phi, rt, m->E,
+                                                           grad_out, q2_out, m->rec.get());
+        UP3D_CHECK_LAUNCH();
+        launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
+    });
+}
+
+int up3d_picard_matrix(up3d_mesh* m, const double* rt, double* data, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && data, UP3D_ERR_ARGUMENT, "up3d_picard_matrix: null argument");
+        cudaStream_t s = S(stream);
+        k_prep_matrix<<<grid_for(m->E, 256), 256, 0, s>>>(m->V.get(), rt, m->E, m->rec.get());
+        UP3D_CHECK_LAUNCH();
+        launch_row_gather<false, true>(m, m->rec.get(), nullptr, data, s);
+    });
+}
+
+int up3d_jacobian(up3d_mesh* m, const double* phi, const double* rt, const double* se, const double* su,
+                  const int64_t* upstream, double u_inf, const uint8_t* lim, double* data, int64_t* n_active,
+                  int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && rt && se && su && upstream && data, UP3D_ERR_ARGUMENT,
+                     "up3d_jacobian: null argument");
+        cudaStream_t s = S(stream);
+        DBuf<double> grad, q2;
+        grad.alloc(3 * m->E);
+        q2.alloc(m->E);
+        launch_velocities(m, phi, grad.get(), q2.get(), s);
+        const double inv_u2 = 1.0 / (u_inf * u_inf);
+        k_prep_jacobian<<<grid_for(m->E, 256), 256, 0, s>>>(m->conn.get(), m->B.get(), m->V.get(), grad.get(), rt, se,
+                                                           su, upstream, lim, inv_u2, m->E, m->rec.get(),
+                                                           m->t3b.get(), m->up32.get());
+        UP3D_CHECK_LAUNCH();
+        launch_row_gather<false, true>(m, m->rec.get(), nullptr, data, s);
+        int64_t na = 0, nx = 0;
+        build_term3(m, data, s, na, nx);
+        m->last_drop_zeros = na > 0;
+        if (n_active) *n_active = na;
+        if (n_extra) *n_extra = nx;
+        if (newton_nnz) *newton_nnz = merged_nnz(m, data, s);
+    });
+}
+
+int up3d_jacobian_export(up3d_mesh* m, const double* data, int32_t* indptr, int32_t* indices, double* merged,
+                         up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && data && indptr && indices && merged, UP3D_ERR_ARGUMENT,
+                     "up3d_jacobian_export: null argument");
+        cudaStream_t s = S(stream);
+                const bool has_x = m->last_extra > 0;
+        const int32_t* xptr = has_x ? m->x_ptr.get() : nullptr;
+        DBuf<int32_t> cnt;
+        cnt.alloc(m->N + 1);
+        UP3D_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
+        k_merge_rows<false><<<grid_for(m->N, 256), 256, 0, s>>>(m->N, m->indptr.get(), m->indices.get(), data, xptr,
+                                                               m->x_col_c.get(), m->x_val_c.get(), m->last_drop_zeros,
+                                                               cnt.get(), nullptr, nullptr);
+        UP3D_CHECK_LAUNCH();
+        scan(m, cnt.get(), indptr, m->N + 1, s);
+        k_merge_rows<true><<<grid_for(m->N, 256), 256, 0, s>>>(m->N, m->indptr.get(), m->indices.get(), data, xptr,
+                                                              m->x_col_c.get(), m->x_val_c.get(), m->last_drop_zeros,
+                                                              indptr, indices, merged);
+        UP3D_CHECK_LAUNCH();
+    });
+}
+
+int up3d_jacobian_nnz(up3d_mesh* m, const double* data, int64_t* newton_nnz, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && data && newton_nnz, UP3D_ERR_ARGUMENT, "up3d_jacobian_nnz: null argument");
+        *newton_nnz = merged_nnz(m, data, S(stream));
+    });
+}
+
+int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flow, const int64_t* up_fz,
+                           const int8_t* br_fz, double* R, double* data, double* rt_out, int32_t* up_out,
+                           up3d_monitors* mon, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && flow && R, UP3D_ERR_ARGUMENT, "up3d_residual_jacobian: null argument");
+        UP3D_REQUIRE((up_fz == nullptr) == (br_fz == nullptr), UP3D_ERR_ARGUMENT,
+                     "up3d_residual_jacobian: frozen upstream and branch go together");
+        cudaStream_t s = S(stream);
+        Flow F = make_flow(*flow);
+        const double u2 = flow->u_inf * flow->u_inf;
+        up3d_monitors* mo = mon ? mon : m->mon_ws.get();
+        UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
+        const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
+#define FUSED_ARGS                                                                                               \
+    m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->cen.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
+        m->E, m->rec.get(), m->t3b.get(), m->up32.get(), rt_out, mo
+        const bool jac = data != nullptr;
+        prof_begin(PROF_ELEM, s);
+        if (up_fz) {
+            if (jac) k_fused_elem<true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            else k_fused_elem<true, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
+        } else {
+            if (jac) k_fused_elem<false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            else k_fused_elem<false, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
+        }
+#undef FUSED_ARGS
+        UP3D_CHECK_LAUNCH();
+        prof_end(PROF_ELEM, s, 1);
+        if (up_out)
+            UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
+        prof_begin(PROF_ROW, s);
+        if (jac) launch_row_gather<true, true>(m, m->rec.get(), R, data, s);
+        else launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
+        prof_end(PROF_ROW, s, m->max_deg > RG_MAXE ? 2 : 1);
+        if (jac) {
+            int64_t na = 0, nx = 0;
+            prof_begin(PROF_TERM3, s);
+            build_term3(m, data, s, na, nx);
+            prof_end(PROF_TERM3, s, 0);
+            m->last_drop_zeros = na > 0;
+            UP3D_CUDA(cudaMemcpyAsync(&mo->n_term3_extra, &nx, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            UP3D_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+}  // extern "C"

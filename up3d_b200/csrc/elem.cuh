@@ -1,0 +1,164 @@
+// Device building blocks of the element sweeps, shared by the single-purpose
+// kernels (elem.cu) and the fused residual/Jacobian sweep (assemble.cu).
+#pragma once
+
+#include "internal.cuh"
+
+namespace up3d {
+
+// grad(phi)_e = sum_i phi_i B_e[i,:] in the reference's order
+// (kernels/gradient.py:52-60), IEEE-rounded.
+__device__ __forceinline__ void elem_grad(const int4* __restrict__ conn, const double* __restrict__ B,
+                                          const double* __restrict__ phi, int64_t e, double g[3]) {
+    int4 c = conn[e];
+    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
+    double2 b01 = b2[0], b23 = b2[1], b45 = b2[2], b67 = b2[3], b89 = b2[4], bab = b2[5];
+    double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
+    g[0] = radd(radd(radd(rmul(p0, b01.x), rmul(p1, b23.y)), rmul(p2, b67.x)), rmul(p3, b89.y));
+    g[1] = radd(radd(radd(rmul(p0, b01.y), rmul(p1, b45.x)), rmul(p2, b67.y)), rmul(p3, bab.x));
+    g[2] = radd(radd(radd(rmul(p0, b23.x), rmul(p1, b45.y)), rmul(p2, b89.x)), rmul(p3, bab.y));
+}
+
+// Same, also returning B_e (12 values) for reuse.
+__device__ __forceinline__ void elem_grad_B(const int4* __restrict__ conn, const double* __restrict__ B,
+                                            const double* __restrict__ phi, int64_t e, double g[3],
+                                            double b[12], int4& c) {
+    c = conn[e];
+    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double2 v = b2[k];
+        b[2 * k] = v.x;
+        b[2 * k + 1] = v.y;
+    }
+    double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        g[d] = radd(radd(radd(rmul(p0, b[d]), rmul(p1, b[3 + d])), rmul(p2, b[6 + d])), rmul(p3, b[9 + d]));
+}
+
+// upstream_elements (kernels/upwind.py:69-125): hop to the face neighbour
+// with the most negative centroid displacement along grad until the reach
+// covers 0.8 of the element's streamwise extent, at most 4 hops; u(e) = e
+// when nothing is upstream.  IEEE-rounded dot products so ties resolve as
+// in the CPU restatement.  Neighbour entries outside [0, E) count as
+// boundary faces.
+__device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, const double4* __restrict__ cen,
+                                                 const double4* __restrict__ X, const int4* __restrict__ conn,
+                                                 int64_t e, int64_t E, const double g[3]) {
+    const double gx = g[0], gy = g[1], gz = g[2];
+    int4 c = conn[e];
+    int nd[4] = {c.x, c.y, c.z, c.w};
+    double pmin = 1e300, pmax = -1e300;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double4 x = X[nd[k]];
+        double p = dot3r(x.x, x.y, x.z, gx, gy, gz);
+        if (p < pmin) pmin = p;
+        if (p > pmax) pmax = p;
+    }
+    const double target = rmul(0.8, rsub(pmax, pmin));
+    int64_t cur = e;
+    double reach = 0.0;
+    double4 cc = cen[e];
+    for (int hops = 0; hops < 4 && reach < target; ++hops) {
+        int4 f = fn[cur];
+        int nb[4] = {f.x, f.y, f.z, f.w};
+        int64_t best = -1;
+        double best_disp = 0.0;
+        double4 bestc = cc;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (nb[k] >= 0 && nb[k] < E) {
+                double4 cn = cen[nb[k]];
+                double d = dot3r(rsub(cn.x, cc.x), rsub(cn.y, cc.y), rsub(cn.z, cc.z), gx, gy, gz);
+                if (d < best_disp) {
+                    best_disp = d;
+                    best = nb[k];
+                    bestc = cn;
+                }
+            }
+        }
+        if (best < 0) break;
+        cur = best;
+        cc = bestc;
+        reach = radd(reach, -best_disp);
+    }
+    return cur;
+}
+
+// rho_tilde_sensitivities_sweep, one element (kernels/upwind.py:687-730).
+__device__ __forceinline__ void live_sensitivities(double q2e, double rho_e, double q2u, double rho_u, bool self_up,
+                                                   const Flow& F, double& se, double& su) {
+    double r_tmp, drho_e;
+    rho_drho(q2e, F, r_tmp, drho_e);
+    if (self_up) {
+        se = rho_e <= F.floor_ ? 0.0 : drho_e;
+        su = 0.0;
+        return;
+    }
+    double m2 = mach2_of(q2e, F), m2u = mach2_of(q2u, F);
+    double nu_e = switch_of(m2, F), nu_u = switch_of(m2u, F);
+    double nu = fmax(nu_e, nu_u);
+    double rt = rho_e - nu * (rho_e - rho_u);
+    if (rt <= F.floor_) {
+        se = 0.0;
+        su = 0.0;
+        return;
+    }
+    if (nu == 0.0) {
+        se = drho_e;
+        su = 0.0;
+        return;
+    }
+    double drho_u;
+    rho_drho(q2u, F, r_tmp, drho_u);
+    double djump = rho_e - rho_u;
+    if (nu_e >= nu_u) {
+        double dnu_e = m2 > F.mc2 ? dswitch_of(q2e, m2, F) : 0.0;
+        se = drho_e * (1.0 - nu) - djump * dnu_e;
+        su = nu * drho_u;
+    } else {
+        double dnu_u = dswitch_of(q2u, m2u, F);
+        se = drho_e * (1.0 - nu);
+        su = nu * drho_u - djump * dnu_u;
+    }
+}
+
+// rho_tilde_frozen_sensitivities_sweep, one element (kernels/upwind.py:616-643).
+__device__ __forceinline__ void frozen_sensitivities(int b, double q2e, double rho_e, double q2u, double rho_u,
+                                                     const Flow& F, double& se, double& su) {
+    if (b == 3) {
+        se = 0.0;
+        su = 0.0;
+        return;
+    }
+    double r_tmp, drho_e;
+    rho_drho(q2e, F, r_tmp, drho_e);
+    if (b == 0) {
+        se = drho_e;
+        su = 0.0;
+        return;
+    }
+    double drho_u;
+    rho_drho(q2u, F, r_tmp, drho_u);
+    double djump = rho_e - rho_u;
+    if (b == 1) {
+        double m2 = mach2_of(q2e, F);
+        double nu = switch_of(m2, F);
+        double dnu_e = m2 > F.mc2 ? dswitch_of(q2e, m2, F) : 0.0;
+        se = drho_e * (1.0 - nu) - djump * dnu_e;
+        su = nu * drho_u;
+    } else {
+        double m2u = mach2_of(q2u, F);
+        double nu = switch_of(m2u, F);
+        double dnu_u = m2u > F.mc2 ? dswitch_of(q2u, m2u, F) : 0.0;
+        se = drho_e * (1.0 - nu);
+        su = nu * drho_u - djump * dnu_u;
+    }
+}
+
+void launch_velocities(const up3d_mesh* m, const double* phi, double* grad, double* q2, cudaStream_t s);
+void launch_walk32(const up3d_mesh* m, const double* grad, int32_t* up, cudaStream_t s);
+
+}  // namespace up3d

@@ -1,0 +1,511 @@
+// Krylov solvers of the up3d library: preconditioned CG for the SPD Picard
+// systems and restarted, left-preconditioned GMRES for the nonsymmetric
+// Newton Jacobian (reference: solve/linear.py:134-239, which calls
+// scipy.sparse.linalg.cg / gmres).
+//
+// Vectors live on the device; each iteration's scalars (dots, norms) are
+// reduced on the device with a fixed two-pass tree (bit-reproducible) and
+// read back once per iteration for the convergence test.  GMRES follows
+// scipy's algorithm (left preconditioning, Givens rotations, adaptive inner
+// tolerance, true-residual test after every cycle) with classical
+// Gram-Schmidt applied twice (CGS2) in place of modified Gram-Schmidt, so
+// each Arnoldi step is two batched multi-dot / multi-axpy passes.
+
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+#include "krylov.cuh"
+
+namespace up3d {
+
+template <class T>
+void launch_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const T* x, T* y,
+                 const uint8_t* dir, cudaStream_t s);
+
+namespace {
+
+constexpr int RB = 256;      // reduction block
+constexpr int RGRID = 592;   // fixed partial count (4 x 148 SMs): reproducible sums
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    __syncthreads();
+    return t;
+}
+
+// partial[b*K + k] = sum over this block's slice of x_k . y   (K vectors of V)
+__global__ void __launch_bounds__(RB)
+    k_multidot(const double* __restrict__ V, int64_t ldv, int K, const double* __restrict__ y, int64_t n,
+               double* __restrict__ partial) {
+    __shared__ double sh[32];
+    for (int k = 0; k < K; ++k) {
+        const double* x = V + k * ldv;
+        double acc = 0.0;
+        GRID_STRIDE(i, n) acc += x[i] * y[i];
+        double t = block_sum(acc, sh);
+        if (threadIdx.x == 0) partial[blockIdx.x * K + k] = t;
+    }
+}
+
+// out[k] = sum_b partial[b*K + k], fixed order.
+__global__ void k_finish(const double* __restrict__ partial, int nb, int K, double* __restrict__ out) {
+    __shared__ double sh[32];
+    for (int k = 0; k < K; ++k) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[b * K + k];
+        double t = block_sum(acc, sh);
+        if (threadIdx.x == 0) out[k] = t;
+    }
+}
+
+// y -= sum_k h[k] V_k  (h on the device)
+__global__ void k_multiaxpy(const double* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h,
+                            double* __restrict__ y, int64_t n) {
+    GRID_STRIDE(i, n) {
+        double acc = y[i];
+        for (int k = 0; k < K; ++k) acc -= h[k] * V[k * ldv + i];
+        y[i] = acc;
+    }
+}
+
+__global__ void k_axpby(double a, const double* __restrict__ x, double b, double* __restrict__ y, int64_t n) {
+    GRID_STRIDE(i, n) y[i] = a * x[i] + b * y[i];
+}
+
+__global__ void k_scale(double* __restrict__ x, double a, int64_t n) {
+    GRID_STRIDE(i, n) x[i] *= a;
+}
+
+__global__ void k_sub(const double* __restrict__ b, const double* __restrict__ ax, double* __restrict__ r,
+                      int64_t n) {
+    GRID_STRIDE(i, n) r[i] = b[i] - ax[i];
+}
+
+__global__ void k_add_to(double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
+    GRID_STRIDE(i, n) out[i] = a[i] + b[i];
+}
+
+// CG updates: x += alpha p, r -= alpha q (alpha = num/den from the device)
+__global__ void k_cg_update(const double* __restrict__ sc, double* __restrict__ x, double* __restrict__ r,
+                            const double* __restrict__ p, const double* __restrict__ q, int64_t n) {
+    const double alpha = sc[0] / sc[1];
+    GRID_STRIDE(i, n) {
+        x[i] += alpha * p[i];
+        r[i] -= alpha * q[i];
+    }
+}
+
+// p = z + beta p (beta = rz_new / rz_old)
+__global__ void k_cg_dir(const double* __restrict__ sc, const double* __restrict__ z, double* __restrict__ p,
+                         int64_t n) {
+    const double beta = sc[2] / sc[0];
+    GRID_STRIDE(i, n) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void k_jacobi_diag(int64_t n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                              const double* __restrict__ data, const uint8_t* __restrict__ dir,
+                              double* __restrict__ dinv) {
+    GRID_STRIDE(r, n) {
+        double d = 0.0;
+        for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k)
+            if (indices[k] == r) d = data[k];
+        if (dir && dir[r]) d = 1.0;
+        dinv[r] = d != 0.0 ? 1.0 / d : 1.0;
+    }
+}
+
+__global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
+    GRID_STRIDE(i, n) out[i] = a[i] * b[i];
+}
+
+__global__ void k_mask(double* __restrict__ x, const uint8_t* __restrict__ dir, int64_t n) {
+    GRID_STRIDE(i, n) if (dir[i]) x[i] = 0.0;
+}
+
+__global__ void k_copy_scalar(const double* __restrict__ src, double* __restrict__ dst) { *dst = *src; }
+
+}  // namespace
+
+// ------------------------------------------------------------ Vec helper
+
+Blas::Blas(cudaStream_t s) : s(s) {
+    partial.alloc((size_t)RGRID * 64);
+    scal.alloc(128);
+    UP3D_CUDA(cudaMallocHost(&host, 128 * sizeof(double)));
+}
+Blas::~Blas() {
+    if (host) cudaFreeHost(host);
+}
+
+void Blas::multidot(const double* V, int64_t ldv, int K, const double* y, int64_t n, double* out_dev) {
+    for (int k0 = 0; k0 < K; k0 += 64) {
+        int kk = std::min(64, K - k0);
+        k_multidot<<<RGRID, RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n, partial.get());
+        UP3D_CHECK_LAUNCH();
+        k_finish<<<1, 1024, 0, s>>>(partial.get(), RGRID, kk, out_dev + k0);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+double Blas::dot(const double* x, const double* y, int64_t n) {
+    multidot(x, 0, 1, y, n, scal.get());
+    UP3D_CUDA(cudaMemcpyAsync(host, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    return host[0];
+}
+
+double Blas::nrm2(const double* x, int64_t n) { return std::sqrt(dot(x, x, n)); }
+
+void Blas::axpby(double a, const double* x, double b, double* y, int64_t n) {
+    k_axpby<<<grid_for(n, 256), 256, 0, s>>>(a, x, b, y, n);
+    UP3D_CHECK_LAUNCH();
+}
+
+void Blas::scale(double* x, double a, int64_t n) {
+    k_scale<<<grid_for(n, 256), 256, 0, s>>>(x, a, n);
+    UP3D_CHECK_LAUNCH();
+}
+
+void Blas::multiaxpy(const double* V, int64_t ldv, int K, const double* h_dev, double* y, int64_t n) {
+    k_multiaxpy<<<grid_for(n, 256), 256, 0, s>>>(V, ldv, K, h_dev, y, n);
+    UP3D_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------ operators
+
+void Operator::apply(const double* x, double* y, cudaStream_t s) const {
+    launch_spmv<double>(A.n, A.indptr, A.indices, A.data, x, y, A.dirichlet, s);
+    if (extra.indptr) {
+        // y += extra x (Term-3 entries outside the P1 pattern)
+        tmp.alloc(A.n);
+        launch_spmv<double>(A.n, extra.indptr, extra.indices, extra.data, x, tmp.get(), A.dirichlet, s);
+        if (A.dirichlet) {
+            k_mask<<<grid_for(A.n, 256), 256, 0, s>>>(tmp.get(), A.dirichlet, A.n);
+            UP3D_CHECK_LAUNCH();
+        }
+        k_add_to<<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), y, A.n);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace up3d
+
+// ------------------------------------------------------------ preconditioners
+
+struct up3d_precond {
+    int kind = 0;  // 0 identity, 1 Jacobi, 2 AMG
+    int64_t n = 0;
+    up3d::DBuf<double> dinv;
+    void* amg = nullptr;
+    up3d_precond() = default;
+    ~up3d_precond();
+    void apply(const double* r, double* z, cudaStream_t s);
+};
+
+namespace up3d {
+void amg_apply(void* amg, const double* r, double* z, cudaStream_t s);
+void amg_destroy(void* amg);
+}  // namespace up3d
+
+up3d_precond::~up3d_precond() {
+    if (amg) up3d::amg_destroy(amg);
+}
+
+void up3d_precond::apply(const double* r, double* z, cudaStream_t s) {
+    using namespace up3d;
+    if (kind == 1) {
+        k_mul<<<grid_for(n, 256), 256, 0, s>>>(dinv.get(), r, z, n);
+        UP3D_CHECK_LAUNCH();
+    } else if (kind == 2) {
+        amg_apply(amg, r, z, s);
+    } else {
+        UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+namespace up3d {
+
+void precond_apply(up3d_precond* M, const double* r, double* z, int64_t n, cudaStream_t s) {
+    if (M) {
+        M->apply(r, z, s);
+    } else {
+        UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+// scipy-convention effective absolute tolerance: max(atol, rtol * ||b||)
+static double eff_atol(double atol, double rtol, double bnrm) { return std::max(atol, rtol * bnrm); }
+
+// ------------------------------------------------------------ CG
+
+// scipy.sparse.linalg.cg (solve/linear.py:232, solve/picard.py:375-380):
+// preconditioned CG, converged when ||r|| <= max(rtol ||b||, atol).
+int cg_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int maxiter, up3d_precond* M,
+             int64_t* iters, double* resid, cudaStream_t s) {
+    const int64_t n = op.A.n;
+    Blas bl(s);
+    DBuf<double> r, z, p, q;
+    r.alloc(n);
+    z.alloc(n);
+    p.alloc(n);
+    q.alloc(n);
+    DBuf<double> sc;
+    sc.alloc(4);
+    const double bnrm = bl.nrm2(b, n);
+    const double tol = eff_atol(atol, rtol, bnrm);
+    op.apply(x, q.get(), s);
+    k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, q.get(), r.get(), n);
+    UP3D_CHECK_LAUNCH();
+    double rn = bl.nrm2(r.get(), n);
+    int64_t it = 0;
+    if (bnrm == 0.0) {
+        UP3D_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+        rn = 0.0;
+    }
+    if (rn > tol) {
+        precond_apply(M, r.get(), z.get(), n, s);
+        UP3D_CUDA(cudaMemcpyAsync(p.get(), z.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        bl.multidot(r.get(), 0, 1, z.get(), n, sc.get() + 0);  // rz
+        for (it = 1; it <= maxiter; ++it) {
+            op.apply(p.get(), q.get(), s);
+            bl.multidot(p.get(), 0, 1, q.get(), n, sc.get() + 1);  // pq
+            k_cg_update<<<grid_for(n, 256), 256, 0, s>>>(sc.get(), x, r.get(), p.get(), q.get(), n);
+            UP3D_CHECK_LAUNCH();
+            rn = bl.nrm2(r.get(), n);
+            if (rn <= tol || !std::isfinite(rn)) break;
+            precond_apply(M, r.get(), z.get(), n, s);
+            bl.multidot(r.get(), 0, 1, z.get(), n, sc.get() + 2);  // rz_new
+            k_cg_dir<<<grid_for(n, 256), 256, 0, s>>>(sc.get(), z.get(), p.get(), n);
+            UP3D_CHECK_LAUNCH();
+            k_copy_scalar<<<1, 1, 0, s>>>(sc.get() + 2, sc.get() + 0);
+            UP3D_CHECK_LAUNCH();
+        }
+        if (it > maxiter) it = maxiter;
+    }
+    if (iters) *iters = it;
+    if (resid) *resid = rn;
+    return rn <= tol ? 0 : (int)maxiter;
+}
+
+// ------------------------------------------------------------ GMRES
+
+// Givens rotation as LAPACK xLARTG: c*f + s*g = r, -s*f + c*g = 0.
+static void lartg(double f, double g, double& c, double& sn, double& r) {
+    if (g == 0.0) {
+        c = 1.0;
+        sn = 0.0;
+        r = f;
+    } else if (f == 0.0) {
+        c = 0.0;
+        sn = g > 0 ? 1.0 : -1.0;
+        r = std::fabs(g);
+    } else {
+        double d = std::sqrt(f * f + g * g);
+        c = std::fabs(f) / d;
+        r = f > 0 ? d : -d;
+        sn = g / r;
+    }
+}
+
+// scipy.sparse.linalg.gmres (solve/linear.py:182-201): restarted,
+// left-preconditioned; `maxiter` counts restart cycles.
+int gmres_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart, int maxiter,
+                up3d_precond* M, int64_t* inner, double* resid, cudaStream_t s) {
+    const int64_t n = op.A.n;
+    Blas bl(s);
+    restart = (int)std::min<int64_t>(restart, n);
+    DBuf<double> V, w, r, tmp;
+    V.alloc((size_t)(restart + 1) * n);
+    w.alloc(n);
+    r.alloc(n);
+    tmp.alloc(n);
+    DBuf<double> hdev;
+    hdev.alloc(2 * (restart + 2));
+    std::vector<double> H((size_t)restart * (restart + 1), 0.0), gc(restart), gs(restart), S(restart + 1);
+    const double bnrm = bl.nrm2(b, n);
+    double atol_eff = eff_atol(atol, rtol, bnrm);
+    if (bnrm == 0.0) {
+        UP3D_CUDA(cudaMemcpyAsync(x, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if (inner) *inner = 0;
+        if (resid) *resid = 0.0;
+        return 0;
+    }
+    const double eps = 2.220446049250313e-16;
+    precond_apply(M, b, tmp.get(), n, s);
+    const double Mb = bl.nrm2(tmp.get(), n);
+    double ptol_max = 1.0;
+    double ptol = Mb * std::min(ptol_max, atol_eff / bnrm);
+    double presid = 0.0, rnorm = 0.0;
+    int64_t total = 0;
+    bool done = false;
+    auto Hat = [&](int col, int k) -> double& { return H[(size_t)col * (restart + 1) + k]; };
+    for (int cycle = 0; cycle < maxiter && !done; ++cycle) {
+        if (cycle == 0) {
+            op.apply(x, tmp.get(), s);
+            k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+            UP3D_CHECK_LAUNCH();
+            rnorm = bl.nrm2(r.get(), n);
+            if (rnorm < atol_eff) {
+                done = true;
+                break;
+            }
+        }
+        precond_apply(M, r.get(), V.get(), n, s);
+        double beta = bl.nrm2(V.get(), n);
+        bl.scale(V.get(), 1.0 / beta, n);
+        std::fill(S.begin(), S.end(), 0.0);
+        S[0] = beta;
+        bool breakdown = false;
+        int col = 0;
+        for (col = 0; col < restart; ++col) {
+            op.apply(V.get() + (size_t)col * n, tmp.get(), s);
+            precond_apply(M, tmp.get(), w.get(), n, s);
+            const double h0 = bl.nrm2(w.get(), n);
+            // CGS2: two projections onto V_0..V_col
+            std::vector<double> hsum(col + 1, 0.0);
+            for (int pass = 0; pass < 2; ++pass) {
+                bl.multidot(V.get(), n, col + 1, w.get(), n, hdev.get());
+                bl.multiaxpy(V.get(), n, col + 1, hdev.get(), w.get(), n);
+                std::vector<double> hh(col + 1);
+                UP3D_CUDA(cudaMemcpyAsync(hh.data(), hdev.get(), sizeof(double) * (col + 1), cudaMemcpyDeviceToHost,
+                                          s));
+                UP3D_CUDA(cudaStreamSynchronize(s));
+                for (int k = 0; k <= col; ++k) hsum[k] += hh[k];
+            }
+            for (int k = 0; k <= col; ++k) Hat(col, k) = hsum[k];
+            const double h1 = bl.nrm2(w.get(), n);
+            Hat(col, col + 1) = h1;
+            UP3D_CUDA(cudaMemcpyAsync(V.get() + (size_t)(col + 1) * n, w.get(), sizeof(double) * n,
+                                      cudaMemcpyDeviceToDevice, s));
+            if (h1 <= eps * h0) {
+                Hat(col, col + 1) = 0.0;
+                breakdown = true;
+            } else {
+                bl.scale(V.get() + (size_t)(col + 1) * n, 1.0 / h1, n);
+            }
+            for (int k = 0; k < col; ++k) {
+                double c = gc[k], sn = gs[k];
+                double n0 = Hat(col, k), n1 = Hat(col, k + 1);
+                Hat(col, k) = c * n0 + sn * n1;
+                Hat(col, k + 1) = -sn * n0 + c * n1;
+            }
+            double c, sn, mag;
+            lartg(Hat(col, col), Hat(col, col + 1), c, sn, mag);
+            gc[col] = c;
+            gs[col] = sn;
+            Hat(col, col) = mag;
+            Hat(col, col + 1) = 0.0;
+            double t = -sn * S[col];
+            S[col] = c * S[col];
+            S[col + 1] = t;
+            presid = std::fabs(t);
+            ++total;
+            if (presid <= ptol || breakdown) break;
+        }
+        if (col == restart) col = restart - 1;
+        if (Hat(col, col) == 0.0) S[col] = 0.0;
+        std::vector<double> y(S.begin(), S.begin() + col + 1);
+        for (int k = col; k > 0; --k) {
+            if (y[k] != 0.0) {
+                y[k] /= Hat(k, k);
+                double tk = y[k];
+                for (int j = 0; j < k; ++j) y[j] -= tk * Hat(k, j);
+            }
+        }
+        if (y[0] != 0.0) y[0] /= Hat(0, 0);
+        // x += V^T y  (as x -= V (-y))
+        for (auto& v : y) v = -v;
+        UP3D_CUDA(cudaMemcpyAsync(hdev.get(), y.data(), sizeof(double) * (col + 1), cudaMemcpyHostToDevice, s));
+        bl.multiaxpy(V.get(), n, col + 1, hdev.get(), x, n);
+        op.apply(x, tmp.get(), s);
+        k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+        UP3D_CHECK_LAUNCH();
+        rnorm = bl.nrm2(r.get(), n);
+        if (rnorm <= atol_eff || breakdown || !std::isfinite(rnorm)) break;
+        if (presid <= ptol) ptol_max = std::max(eps, 0.25 * ptol_max);
+        else ptol_max = std::min(1.0, 1.5 * ptol_max);
+        ptol = presid * std::min(ptol_max, atol_eff / rnorm);
+    }
+    if (inner) *inner = total;
+    if (resid) *resid = rnorm;
+    return rnorm <= atol_eff ? 0 : maxiter;
+}
+
+}  // namespace up3d
+
+using namespace up3d;
+
+namespace {
+Operator make_op(const up3d_csr* A, const up3d_csr* extra) {
+    Operator op;
+    UP3D_REQUIRE(A && A->indptr && A->indices && A->data && A->n >= 0, UP3D_ERR_ARGUMENT, "bad CSR operand");
+    op.A = *A;
+    if (extra && extra->indptr) {
+        UP3D_REQUIRE(extra->n == A->n, UP3D_ERR_ARGUMENT, "extra operand size mismatch");
+        op.extra = *extra;
+    }
+    return op;
+}
+}  // namespace
+
+extern "C" {
+
+int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(A && out, UP3D_ERR_ARGUMENT, "up3d_precond_jacobi: null argument");
+        auto* M = new up3d_precond();
+        M->kind = 1;
+        M->n = A->n;
+        M->dinv.alloc(A->n);
+        k_jacobi_diag<<<grid_for(A->n, 256), 256, 0, S(stream)>>>(A->n, A->indptr, A->indices, A->data, A->dirichlet,
+                                                                 M->dinv.get());
+        UP3D_CHECK_LAUNCH();
+        *out = M;
+    });
+}
+
+int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(M && r && z, UP3D_ERR_ARGUMENT, "up3d_precond_apply: null argument");
+        M->apply(r, z, S(stream));
+    });
+}
+
+int up3d_precond_destroy(up3d_precond* M) {
+    return guarded([&] { delete M; });
+}
+
+int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double atol, int maxiter, up3d_precond* M,
+            int64_t* iters, double* resid, int* info, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(b && x, UP3D_ERR_ARGUMENT, "up3d_cg: null argument");
+        Operator op = make_op(A, nullptr);
+        int inf = cg_solve(op, b, x, rtol, atol, maxiter, M, iters, resid, S(stream));
+        if (info) *info = inf;
+    });
+}
+
+int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double* x, double rtol, double atol,
+               int restart, int maxiter, up3d_precond* M, int64_t* inner, double* resid, int* info,
+               up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(b && x && restart > 0 && maxiter > 0, UP3D_ERR_ARGUMENT, "up3d_gmres: bad argument");
+        Operator op = make_op(A, extra);
+        int inf = gmres_solve(op, b, x, rtol, atol, restart, maxiter, M, inner, resid, S(stream));
+        if (info) *info = inf;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,1 @@
+"""Mesh generation (synthetic channels) and device mesh handles."""

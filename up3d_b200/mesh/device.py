@@ -1,0 +1,203 @@
+"""Device-resident mesh handle (owner of an ``up3d_mesh``) and a device CSR.
+
+One handle serves every operator built on the same (nodes, elements): the
+handles are cached by content digest, so ``PicardOperator`` and
+``UpwindOperator`` on one mesh share a single device copy of the geometry,
+adjacency and pattern, and the per-mesh setup runs once.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+from collections import OrderedDict
+
+import numpy as np
+
+from .. import _lib as L
+
+
+class _DevView:
+    """__cuda_array_interface__ over library-owned device memory."""
+
+    def __init__(self, addr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": typestr, "data": (int(addr), False),
+            "version": 3, "strides": None,
+        }
+
+
+def device_view(addr: int, shape, dtype):
+    """Zero-copy torch view of library-owned device memory."""
+    t = L.torch()
+    typestr = {np.int32: "<i4", np.int64: "<i8", np.float64: "<f8", np.uint8: "|u1"}[dtype]
+    return t.as_tensor(_DevView(addr, shape, typestr), device="cuda")
+
+
+def _as_numpy(x, dtype):
+    if L.is_torch(x):
+        x = x.detach().cpu().numpy()
+    return np.ascontiguousarray(np.asarray(x), dtype=dtype)
+
+
+class DeviceMesh:
+    """Owner of one up3d_mesh handle on one device."""
+
+    def __init__(self, nodes, elements, device: int | None = None):
+        t = L.require_cuda()
+        nodes = _as_numpy(nodes, np.float64)
+        elements = _as_numpy(elements, np.int32)
+        if nodes.ndim != 2 or nodes.shape[1] != 3:
+            raise ValueError(f"nodes must be (n_nodes, 3), got {nodes.shape}")
+        if elements.ndim != 2 or elements.shape[1] != 4:
+            raise ValueError(f"elements must be (n_tets, 4), got {elements.shape}")
+        self.device = t.cuda.current_device() if device is None else int(device)
+        handle = ctypes.c_void_p()
+        with t.cuda.device(self.device):
+            L.call("up3d_mesh_create", nodes.ctypes.data, elements.ctypes.data, len(nodes),
+                   len(elements), self.device, L.stream_ptr(), ctypes.byref(handle))
+        self.handle = handle.value
+        info = L.MeshInfo()
+        L.call("up3d_mesh_get_info", self.handle, ctypes.byref(info))
+        self.n_nodes = int(info.n_nodes)
+        self.n_tets = int(info.n_tets)
+        self.nnz = int(info.nnz)
+        self.max_row_len = int(info.max_row_len)
+        self.max_node_degree = int(info.max_node_degree)
+        self.nodes = nodes
+        self.elements = elements
+        ip, ix = ctypes.c_void_p(), ctypes.c_void_p()
+        L.call("up3d_mesh_pattern", self.handle, ctypes.byref(ip), ctypes.byref(ix))
+        # torch-owned copies of the pattern (valid independent of the handle)
+        self.indptr = device_view(ip.value, (self.n_nodes + 1,), np.int32).clone()
+        self.indices = device_view(ix.value, (self.nnz,), np.int32).clone()
+        self._colors = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                L.lib().up3d_mesh_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    # ---------------------------------------------------------- exports
+
+    def geometry(self):
+        t = L.torch()
+        B = t.empty((self.n_tets, 4, 3), dtype=t.float64, device="cuda")
+        V = t.empty(self.n_tets, dtype=t.float64, device="cuda")
+        L.call("up3d_mesh_geometry", self.handle, B.data_ptr(), V.data_ptr(), L.stream_ptr())
+        return B, V
+
+    def centroids(self):
+        t = L.torch()
+        c = t.empty((self.n_tets, 3), dtype=t.float64, device="cuda")
+        L.call("up3d_mesh_centroids", self.handle, c.data_ptr(), L.stream_ptr())
+        return c
+
+    def face_neighbors(self):
+        t = L.torch()
+        f = t.empty((self.n_tets, 4), dtype=t.int32, device="cuda")
+        L.call("up3d_mesh_face_neighbors", self.handle, f.data_ptr(), L.stream_ptr())
+        return f
+
+    def set_face_neighbors(self, fn):
+        t = L.torch()
+        d = L.to_device(fn, t.int32)
+        if tuple(d.shape) != (self.n_tets, 4):
+            raise ValueError(f"face_neighbors must be ({self.n_tets}, 4), got {tuple(d.shape)}")
+        if int(d.max()) >= self.n_tets or int(d.min()) < -1:
+            raise ValueError("face_neighbors entries must be -1 or element indices")
+        L.call("up3d_mesh_set_face_neighbors", self.handle, d.data_ptr(), L.stream_ptr())
+        t.cuda.current_stream().synchronize()
+
+    def coloring(self):
+        if self._colors is None:
+            nc = ctypes.c_int32()
+            L.call("up3d_mesh_coloring", self.handle, None, None, ctypes.byref(nc))
+            off = np.empty(nc.value + 1, dtype=np.int64)
+            el = np.empty(self.n_tets, dtype=np.int64)
+            L.call("up3d_mesh_coloring", self.handle, off.ctypes.data, el.ctypes.data,
+                   ctypes.byref(nc))
+            self._colors = (off, el, int(nc.value))
+        return self._colors
+
+    def elem_to_csr(self):
+        t = L.torch()
+        out = t.empty((self.n_tets, 4, 4), dtype=t.int64, device="cuda")
+        L.call("up3d_mesh_elem_to_csr", self.handle, out.data_ptr(), L.stream_ptr())
+        return out
+
+
+_CACHE: "OrderedDict[tuple, DeviceMesh]" = OrderedDict()
+_CACHE_SIZE = 4
+
+
+def _digest(nodes: np.ndarray, elements: np.ndarray) -> str:
+    h = hashlib.blake2b(digest_size=20)
+    h.update(np.asarray(nodes.shape, dtype=np.int64).tobytes())
+    h.update(nodes.tobytes())
+    h.update(np.asarray(elements.shape, dtype=np.int64).tobytes())
+    h.update(elements.tobytes())
+    return h.hexdigest()
+
+
+def get_mesh(nodes, elements, device: int | None = None) -> DeviceMesh:
+    """Shared DeviceMesh for (nodes, elements) on `device` (cached)."""
+    t = L.require_cuda()
+    nodes = _as_numpy(nodes, np.float64)
+    elements = _as_numpy(elements, np.int32)
+    dev = t.cuda.current_device() if device is None else int(device)
+    key = (_digest(nodes, elements), dev)
+    m = _CACHE.get(key)
+    if m is None:
+        m = DeviceMesh(nodes, elements, dev)
+        _CACHE[key] = m
+        while len(_CACHE) > _CACHE_SIZE:
+            _CACHE.popitem(last=False)
+    else:
+        _CACHE.move_to_end(key)
+    return m
+
+
+def clear_cache():
+    _CACHE.clear()
+
+
+class DeviceCSR:
+    """CSR matrix whose arrays are CUDA tensors (int32 indices, f64/f32 data).
+
+    ``to_scipy()`` makes the host copy the reference's callers expect
+    (``scipy.sparse.csr_matrix``)."""
+
+    def __init__(self, indptr, indices, data, shape):
+        self.indptr = indptr
+        self.indices = indices
+        self.data = data
+        self.shape = tuple(shape)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.indices.numel())
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.data.detach().cpu().numpy(),
+                              self.indices.detach().cpu().numpy(),
+                              self.indptr.detach().cpu().numpy()), shape=self.shape)
+
+    def matvec(self, x, y=None, dirichlet=None):
+        """y = A x on the device (FP64 or FP32 by data dtype)."""
+        t = L.torch()
+        if y is None:
+            y = t.empty_like(x)
+        fn = "up3d_spmv" if self.data.dtype == t.float64 else "up3d_spmv_f32"
+        L.call(fn, self.shape[0], self.indptr.data_ptr(), self.indices.data_ptr(),
+               self.data.data_ptr(), x.data_ptr(), y.data_ptr(),
+               None if dirichlet is None else dirichlet.data_ptr(), L.stream_ptr())
+        return y
+
+    def __matmul__(self, x):
+        return self.matvec(x)

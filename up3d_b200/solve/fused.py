@@ -1,0 +1,91 @@
+"""Fused residual + Newton Jacobian evaluation on the device.
+
+One call does what ``NewtonWorkspace.eval_residual`` followed by
+``assemble_coupled`` do without a wake (pyfp3d/solve/newton.py:345-372,
+:430-457 with T = I): velocities, speed limiter, density, upstream walk (or
+the frozen selection), upwinded density, its sensitivities, the residual R
+and the Newton Jacobian (Terms 1-3) -- two passes over the mesh (an element
+sweep and a row gather) plus the Term-3 sort/merge when supersonic elements
+exist.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+from .. import _lib as L
+from ..mesh.device import DeviceCSR, DeviceMesh
+
+
+@dataclass
+class FlowParams:
+    m_inf: float
+    gamma: float = 1.4
+    u_inf: float = 1.0
+    m_cap: float = 3.0
+    m_crit: float = 0.95
+    upwind_c: float = 1.5
+    rho_floor: float = 0.05
+
+    def c(self) -> L.Flow:
+        return L.flow(self.m_inf, self.gamma, self.u_inf, self.m_cap, self.m_crit, self.upwind_c,
+                      self.rho_floor)
+
+
+class ResidualJacobian:
+    """Device workspace of the fused evaluation on one mesh."""
+
+    def __init__(self, mesh: DeviceMesh):
+        t = L.require_cuda()
+        self.mesh = mesh
+        self.R = t.empty(mesh.n_nodes, dtype=t.float64, device="cuda")
+        self.data = t.empty(mesh.nnz, dtype=t.float64, device="cuda")
+        self.rho_tilde = t.empty(mesh.n_tets, dtype=t.float64, device="cuda")
+        self.upstream = t.empty(mesh.n_tets, dtype=t.int32, device="cuda")
+        self.monitors = L.monitors_buffer()
+        self._n_extra = 0
+
+    def evaluate(self, phi, flow: FlowParams, jacobian: bool = True, frozen=None,
+                 keep_state: bool = True):
+        """R(phi) (and the Jacobian data on the P1 pattern).  `frozen` =
+        (upstream int64, branch int8) selects the frozen flux."""
+        up_fz = br_fz = None
+        if frozen is not None:
+            t = L.torch()
+            up_fz = L.to_device(frozen[0], t.int64)
+            br_fz = L.to_device(frozen[1], t.int8)
+        L.call("up3d_residual_jacobian", self.mesh.handle, phi.data_ptr(), flow.c(),
+               L.ptr(up_fz), L.ptr(br_fz), self.R.data_ptr(),
+               self.data.data_ptr() if jacobian else None,
+               self.rho_tilde.data_ptr() if keep_state else None,
+               self.upstream.data_ptr() if keep_state else None,
+               self.monitors.data_ptr(), L.stream_ptr())
+        return self.R
+
+    def read_monitors(self) -> dict:
+        return L.read_monitors(self.monitors)
+
+    def jacobian(self, newton_nnz: int | None = None) -> DeviceCSR:
+        """The merged Newton Jacobian of the last evaluate(jacobian=True)."""
+        t = L.torch()
+        mon = self.read_monitors()
+        if mon["n_term3_active"] == 0:
+            return DeviceCSR(self.mesh.indptr, self.mesh.indices, self.data,
+                             (self.mesh.n_nodes, self.mesh.n_nodes))
+        if newton_nnz is None:
+            newton_nnz = self.newton_nnz()
+        indptr = t.empty(self.mesh.n_nodes + 1, dtype=t.int32, device="cuda")
+        indices = t.empty(newton_nnz, dtype=t.int32, device="cuda")
+        data = t.empty(newton_nnz, dtype=t.float64, device="cuda")
+        L.call("up3d_jacobian_export", self.mesh.handle, self.data.data_ptr(), indptr.data_ptr(),
+               indices.data_ptr(), data.data_ptr(), L.stream_ptr())
+        return DeviceCSR(indptr, indices, data, (self.mesh.n_nodes, self.mesh.n_nodes))
+
+    def newton_nnz(self) -> int:
+        """nnz of the merged Jacobian (exact zeros dropped when Term 3 is
+        active, like scipy's CSR addition)."""
+        out = ctypes.c_int64()
+        L.call("up3d_jacobian_nnz", self.mesh.handle, self.data.data_ptr(), ctypes.byref(out),
+               L.stream_ptr())
+        return int(out.value)
