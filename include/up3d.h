@@ -270,6 +270,31 @@ typedef struct {
 
 typedef struct up3d_precond up3d_precond; /* opaque preconditioner */
 
+/* Smoothed-aggregation AMG (build_amg_preconditioner, solve/linear.py:61-81,
+ * pyamg.smoothed_aggregation_solver defaults: theta 0, standard aggregation,
+ * Jacobi-smoothed prolongator with omega 4/3 / rho(D^-1 A), Galerkin
+ * coarsening).  The V-cycle smooths with damped Jacobi on the device; fp32
+ * selects FP32 level operators and cycle with an FP64 coarsest solve. */
+typedef struct {
+    int max_levels;     /* default 10 */
+    int64_t max_coarse; /* dense FP64 solve at or below this size (default 500) */
+    int presmooth;      /* Jacobi sweeps (default 2) */
+    int postsmooth;     /* Jacobi sweeps (default 2) */
+    int fp32;           /* 0 FP64 cycle, 1 FP32 cycle */
+} up3d_amg_options;
+
+typedef struct {
+    int32_t n_levels;
+    int64_t n_coarse;
+    double operator_complexity;
+    int64_t level_rows[16];
+} up3d_amg_info;
+
+/* Builds the hierarchy of A (setup on the host, cycle on the device). */
+int up3d_amg_setup(const up3d_csr* A, const up3d_amg_options* options, up3d_precond** out,
+                   up3d_stream stream);
+int up3d_amg_get_info(const up3d_precond* M, up3d_amg_info* info);
+
 /* Point-Jacobi preconditioner z = D^{-1} r (constrained rows: identity). */
 int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream);
 /* z = M r */

@@ -1,0 +1,129 @@
+"""Device Krylov solvers and the AMG preconditioner against scipy's direct
+solve of the same reduced systems (the reference solves them with
+spla.cg / spla.gmres + pyamg, solve/linear.py:134-239)."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from conftest import has_cuda, rel_err
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
+
+
+@pytest.fixture(scope="module")
+def c1_system(c1_golden):
+    """Picard matrix and Newton Jacobian of the C1 mesh at the mixed state,
+    on device and as scipy, with the inflow/outflow Dirichlet split."""
+    import torch
+    from up3d_b200.kernels.jacobian import PicardOperator
+    g = c1_golden
+    op = PicardOperator(g.mesh("nodes"), g.mesh("elements"))
+    label = "mixed_m08"
+    rt = torch.from_numpy(g.state(label, "rho_tilde")).cuda()
+    A = op.assemble_matrix(rt)
+    phi = torch.from_numpy(g.state(label, "phi")).cuda()
+    J = op.assemble_newton_jacobian(phi, rt, torch.from_numpy(g.state(label, "s_e")).cuda(),
+                                    torch.from_numpy(g.state(label, "s_u")).cuda(),
+                                    torch.from_numpy(g.state(label, "upstream").astype(np.int64)).cuda())
+    dn = g.mesh("dirichlet_nodes")
+    n = op.n_nodes
+    free = np.setdiff1d(np.arange(n), dn)
+    mask = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    mask[torch.from_numpy(dn).cuda()] = 1
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(n)
+    b[dn] = 0.0
+    return {"A": A, "J": J, "mask": mask, "free": free, "b": b, "n": n}
+
+
+def _embedded(M, mask):
+    from up3d_b200.solve.linear import with_dirichlet
+    return with_dirichlet(M, mask)
+
+
+def _direct(M, free, b):
+    Ms = M.to_scipy()
+    x = np.zeros(len(b))
+    x[free] = spla.spsolve(Ms[free][:, free].tocsc(), b[free])
+    return x
+
+
+def test_cg_jacobi_matches_direct(c1_system):
+    import torch
+    from up3d_b200.solve.linear import build_jacobi_preconditioner, solve_cg
+    s = c1_system
+    A = _embedded(s["A"], s["mask"])
+    M = build_jacobi_preconditioner(A)
+    x, it, info = solve_cg(A, torch.from_numpy(s["b"]).cuda(), M=M, rtol=1e-12, maxiter=5000)
+    assert info == 0
+    ref = _direct(s["A"], s["free"], s["b"])
+    assert rel_err(x.cpu().numpy(), ref) < 1e-9
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_cg_amg_matches_direct(c1_system, fp32):
+    import torch
+    from up3d_b200.solve.linear import build_amg_preconditioner, build_jacobi_preconditioner, solve_cg
+    s = c1_system
+    A = _embedded(s["A"], s["mask"])
+    ml, M = build_amg_preconditioner(A, fp32=fp32)
+    assert ml.n_levels >= 2 and ml.operator_complexity < 3.0
+    b = torch.from_numpy(s["b"]).cuda()
+    x, it_amg, info = solve_cg(A, b, M=M, rtol=1e-12, maxiter=500)
+    assert info == 0
+    ref = _direct(s["A"], s["free"], s["b"])
+    assert rel_err(x.cpu().numpy(), ref) < 1e-9
+    _, it_jac, _ = solve_cg(A, b, M=build_jacobi_preconditioner(A), rtol=1e-12, maxiter=5000)
+    assert it_amg < it_jac / 3, (it_amg, it_jac)
+
+
+def test_amg_setup_is_deterministic(c1_system):
+    import torch
+    from up3d_b200.solve.linear import build_amg_preconditioner
+    s = c1_system
+    A = _embedded(s["A"], s["mask"])
+    r = torch.from_numpy(s["b"]).cuda()
+    z1 = build_amg_preconditioner(A)[1].matvec(r)
+    z2 = build_amg_preconditioner(A)[1].matvec(r)
+    assert torch.equal(z1, z2)
+
+
+def test_gmres_amg_on_newton_jacobian(c1_system):
+    import torch
+    from up3d_b200.solve.linear import build_amg_preconditioner, solve_gmres, with_dirichlet
+    s = c1_system
+    J = with_dirichlet(s["J"], s["mask"])
+    A = with_dirichlet(s["A"], s["mask"])
+    _, M = build_amg_preconditioner(A)
+    b = torch.from_numpy(s["b"]).cuda()
+    x, n_inner, info = solve_gmres(J, b, M=M, rtol=1e-11, restart=60, maxiter=20)
+    assert info == 0
+    ref = _direct(s["J"], s["free"], s["b"])
+    assert rel_err(x.cpu().numpy(), ref) < 1e-8
+    assert n_inner > 0
+
+
+def test_solve_gmres_scipy_inputs_return_numpy(c1_system):
+    from up3d_b200.solve.linear import solve_gmres
+    s = c1_system
+    free = s["free"]
+    Js = s["J"].to_scipy()[free][:, free].tocsr()
+    b = s["b"][free]
+    x, n_inner, info = solve_gmres(Js, b, rtol=1e-10, restart=200, maxiter=50, on_fail="return")
+    assert isinstance(x, np.ndarray)
+    r = np.linalg.norm(Js @ x - b) / np.linalg.norm(b)
+    assert (info == 0 and r < 1e-9) or info != 0
+
+
+def test_cg_amg_drop_in(c1_system):
+    from up3d_b200.solve.linear import solve_cg_amg
+    s = c1_system
+    free = s["free"]
+    As = s["A"].to_scipy()[free][:, free].tocsr()
+    b = s["b"][free]
+    x, n_it = solve_cg_amg(As, b, rtol=1e-10)
+    assert isinstance(x, np.ndarray)
+    assert np.linalg.norm(As @ x - b) <= 1e-10 * np.linalg.norm(b) * 1.01

@@ -88,7 +88,33 @@ SIGNATURES = {
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),
     "up3d_spmv": (_int, [_i64, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_spmv_f32": (_int, [_i64, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_amg_setup": (_int, [_p, _p, ctypes.POINTER(_p), _p]),
+    "up3d_amg_get_info": (_int, [_p, _p]),
+    "up3d_precond_jacobi": (_int, [_p, ctypes.POINTER(_p), _p]),
+    "up3d_precond_apply": (_int, [_p, _p, _p, _p]),
+    "up3d_precond_destroy": (_int, [_p]),
+    "up3d_cg": (_int, [_p, _p, _p, _d, _d, _int, _p, ctypes.POINTER(_i64), ctypes.POINTER(_d),
+                       ctypes.POINTER(_int), _p]),
+    "up3d_gmres": (_int, [_p, _p, _p, _p, _d, _d, _int, _int, _p, ctypes.POINTER(_i64),
+                          ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
 }
+
+
+class CSR(ctypes.Structure):
+    """up3d_csr"""
+    _fields_ = [("n", _i64), ("indptr", _p), ("indices", _p), ("data", _p), ("dirichlet", _p)]
+
+
+class AmgOptions(ctypes.Structure):
+    """up3d_amg_options"""
+    _fields_ = [("max_levels", _int), ("max_coarse", _i64), ("presmooth", _int),
+                ("postsmooth", _int), ("fp32", _int)]
+
+
+class AmgInfo(ctypes.Structure):
+    """up3d_amg_info"""
+    _fields_ = [("n_levels", _i32), ("n_coarse", _i64), ("operator_complexity", _d),
+                ("level_rows", _i64 * 16)]
 
 STATUS_EXC = {-1: ValueError, -2: RuntimeError, -3: NotImplementedError, -4: TypeError,
               -5: TimeoutError}

@@ -19,8 +19,9 @@ CSRC = HERE / "csrc"
 LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libup3d.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-         "-Xptxas", "-warn-spills"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
+         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+LINK = ["-Xcompiler", "-fopenmp", "-lgomp"]
 
 
 def sources():
@@ -61,7 +62,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     if failed:
         raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), *LINK]
     subprocess.run(cmd, check=True)
     tmp.replace(LIB)
     return LIB

@@ -68,20 +68,42 @@ __device__ __forceinline__ void bb_row(const double* __restrict__ BB, int64_t e,
 //   J_nm = sum_e w1_e (B_i . B_j) + [w2_e != 0] w2_e gB_i gB_j
 // (kernels/jacobian.py:406-433: Term 2 only when its weight is non-zero, so
 // J reduces to the Picard matrix bitwise at s_e = 0).
+#ifndef UP3D_ROW_MINB
+#define UP3D_ROW_MINB 6
+#endif
+
+// Shared memory of one warp: MAXE*4 doubles of contributions, then the
+// row's plan (at most 3 off-diagonal contributors per incident element).
+template <int MAXE>
+constexpr size_t row_smem_per_warp() {
+    return sizeof(double) * MAXE * 4 + ((sizeof(uint16_t) * 3 * MAXE + 15) / 16) * 16;
+}
+
 template <bool DO_R, bool DO_J, int MAXE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 1 ? 1 : UP3D_ROW_MINB)
     k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
                  const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
                  const uint16_t* __restrict__ plan, const int32_t* __restrict__ diag,
                  const double* __restrict__ BB, const ElemRecord* __restrict__ rec, double* __restrict__ R,
                  double* __restrict__ J, bool wide_pass) {
-    extern __shared__ double smem_vals[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double* vals = smem_vals + (size_t)w * MAXE * 4;
+    double* vals = reinterpret_cast<double*>(smem_raw + (size_t)w * row_smem_per_warp<MAXE>());
+    uint16_t* splan = reinterpret_cast<uint16_t*>(vals + MAXE * 4);
     for (int64_t n = (int64_t)blockIdx.x * WARPS + w; n < N; n += (int64_t)gridDim.x * WARPS) {
         const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
         // the narrow pass skips rows that need the wide buffer and vice versa
         if (wide_pass ? deg <= RG_MAXE : deg > RG_MAXE) continue;
+        int32_t rb = 0, L = 0, pbase = 0;
+        if (DO_J) {
+            // stage the row's contributor plan (contiguous) with one
+            // coalesced pass, overlapped with the element loads below
+            rb = indptr[n];
+            L = indptr[n + 1] - rb;
+            pbase = plan_off[rb];
+            const int32_t pcnt = plan_off[rb + L] - pbase;
+            for (int t = lane; t < pcnt; t += 32) splan[t] = plan[pbase + t];
+        }
         double r = 0.0, d = 0.0;
         for (int k = lane; k < deg; k += 32) {
             uint32_t x = ent[eb + k];
@@ -106,14 +128,14 @@ __global__ void __launch_bounds__(WARPS * 32)
         if (DO_J) {
             d = warp_sum(d);
             __syncwarp();
-            const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
+            const int32_t ds = diag[n];
             for (int s = lane; s < L; s += 32) {
                 double v = d;
                 if (s != ds) {
                     v = 0.0;
-                    const int32_t p1 = plan_off[rb + s + 1];
-                    for (int32_t p = plan_off[rb + s]; p < p1; ++p) {
-                        uint32_t c = plan[p];
+                    const int32_t p1 = plan_off[rb + s + 1] - pbase;
+                    for (int32_t p = plan_off[rb + s] - pbase; p < p1; ++p) {
+                        uint32_t c = splan[p];
                         v += vals[(c & 3) * MAXE + (c >> 2)];
                     }
                 }
@@ -128,7 +150,7 @@ __global__ void __launch_bounds__(WARPS * 32)
 template <bool DO_R, bool DO_J>
 void launch_row_gather(const up3d_mesh* m, const ElemRecord* rec, double* R, double* J, cudaStream_t s) {
     {
-        const size_t sm = sizeof(double) * RG_WARPS * RG_MAXE * 4;
+        const size_t sm = RG_WARPS * row_smem_per_warp<RG_MAXE>();
         auto kern = k_row_gather<DO_R, DO_J, RG_MAXE, RG_WARPS>;
         const unsigned grid = grid_for(m->N, RG_WARPS, (int64_t)148 * 64);
         kern<<<grid, RG_WARPS * 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
@@ -139,7 +161,7 @@ void launch_row_gather(const up3d_mesh* m, const ElemRecord* rec, double* R, dou
     if (m->max_deg > RG_MAXE) {
         UP3D_REQUIRE(m->max_deg <= WIDE_MAXE, UP3D_ERR_VALUE,
                      "a node is shared by more than 1024 elements; unsupported by the row gather");
-        const size_t sm = sizeof(double) * WIDE_MAXE * 4;
+        const size_t sm = row_smem_per_warp<WIDE_MAXE>();
         auto kern = k_row_gather<DO_R, DO_J, WIDE_MAXE, 1>;
         UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         kern<<<148 * 4, 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(),
@@ -257,19 +279,29 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // 345-372, :435-452): gradient, limiter, density, upstream walk (or the
 // frozen selection), the upstream element's state recomputed in place, the
 // flux, its sensitivities and the element record.
+#ifndef UP3D_ELEM_MINB
+#define UP3D_ELEM_MINB 3
+#endif
+
 template <bool FROZEN, bool JAC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, UP3D_ELEM_MINB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
                  const int4* __restrict__ fn, const double4* __restrict__ cen, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F, double u2, const int64_t* __restrict__ up_fz,
                  const int8_t* __restrict__ br_fz, int64_t E, ElemRecord* __restrict__ rec,
-                 double* __restrict__ t3b, int32_t* __restrict__ up_out, double* __restrict__ rt_out,
-                 up3d_monitors* mon) {
+                 double* __restrict__ t3b, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
+                 double* __restrict__ rt_out, up3d_monitors* mon) {
     MonAcc acc;
     GRID_STRIDE(e, E) {
-        double g[3], b[12];
-        int4 c;
-        elem_grad_B(conn, B, phi, e, g, b, c);
+        // own state; B_e is reduced to gB_j = grad . B_j at once so that
+        // only 7 values stay live through the walk
+        double g[3], gB[4];
+        {
+            double b[12];
+            int4 c;
+            elem_grad_B(conn, B, phi, e, g, b, c);
+            gB_of(g, b, gB);
+        }
         double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), u2);
         double q2l = q2n < F.q2cap ? q2n : F.q2cap;
         bool lim_e = q2l == q2n;
@@ -277,15 +309,15 @@ __global__ void __launch_bounds__(256)
         rho_drho(q2l, F, rho_e, drho_e);
 
         int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, cen, X, conn, e, E, g);
+        // upstream state, and its Term-3 factors grad_u . B_u,k
         double q2lu = q2l, rho_u = rho_e;
         bool lim_u = lim_e;
-        double gu[3] = {g[0], g[1], g[2]};
-        double bu[12];
-#pragma unroll
-        for (int k = 0; k < 12; ++k) bu[k] = b[k];
+        double f[4] = {gB[0], gB[1], gB[2], gB[3]};
         if (u != e) {
+            double gu[3], bu[12];
             int4 cu;
             elem_grad_B(conn, B, phi, u, gu, bu, cu);
+            if (JAC) gB_of(gu, bu, f);
             double q2nu = __ddiv_rn(dot3r(gu[0], gu[1], gu[2], gu[0], gu[1], gu[2]), u2);
             q2lu = q2nu < F.q2cap ? q2nu : F.q2cap;
             lim_u = q2lu == q2nu;
@@ -318,8 +350,6 @@ __global__ void __launch_bounds__(256)
         acc.nu_max = fmax(acc.nu_max, nu);
         acc.sup += (nu > 0.0);
 
-        double gB[4];
-        gB_of(g, b, gB);
         double Ve = V[e];
         double w2 = 0.0, w3 = 0.0;
         bool active = false;
@@ -330,14 +360,13 @@ __global__ void __launch_bounds__(256)
             w3 = 2.0 * F.inv_u2 * s_u * Ve;
             active = s_u != 0.0;
             if (active) {
-                double f[4];
-                gB_of(gu, bu, f);
                 reinterpret_cast<double2*>(t3b + 4 * e)[0] = make_double2(f[0], f[1]);
                 reinterpret_cast<double2*>(t3b + 4 * e)[1] = make_double2(f[2], f[3]);
                 acc.act += 1;
             }
         }
         store_rec(rec, e, gB, rt * Ve, w2, w3, active ? 1.0 : 0.0);
+        if (JAC) t3flag[e] = active ? 1 : 0;
         up_out[e] = (int32_t)u;
         if (rt_out) rt_out[e] = rt;
     }
@@ -474,13 +503,24 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 // Builds Term 3 from the element records (flag = pad != 0): folds the
 // in-pattern part into `data`, keeps the extras (sorted by row, col) in the
 // mesh workspace, and returns (n_active, n_extra).  Synchronises the stream.
-static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra) {
-        const int64_t E = m->E;
+// `known_active` >= 0 is the active count already known to the caller (0
+// skips everything); `flags_ready` means m->t3_flag already holds the
+// active flags.
+static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
+                        int64_t known_active = -1, bool flags_ready = false) {
+    const int64_t E = m->E;
+    if (known_active == 0) {
+        n_active = n_extra = 0;
+        m->last_active = m->last_extra = 0;
+        return;
+    }
     m->t3_flag.alloc(E);
     m->t3_active.alloc(E);
     m->i64_ws.alloc(8);
-    k_t3_flags<<<grid_for(E, 256), 256, 0, s>>>(m->rec.get(), E, m->t3_flag.get());
-    UP3D_CHECK_LAUNCH();
+    if (!flags_ready) {
+        k_t3_flags<<<grid_for(E, 256), 256, 0, s>>>(m->rec.get(), E, m->t3_flag.get());
+        UP3D_CHECK_LAUNCH();
+    }
     size_t bytes = 0;
     thrust::counting_iterator<int32_t> it(0);
     UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(), E, s));
@@ -693,8 +733,9 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
 #define FUSED_ARGS                                                                                               \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->cen.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
-        m->E, m->rec.get(), m->t3b.get(), m->up32.get(), rt_out, mo
+        m->E, m->rec.get(), m->t3b.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo
         const bool jac = data != nullptr;
+        if (jac) m->t3_flag.alloc(m->E);
         prof_begin(PROF_ELEM, s);
         if (up_fz) {
             if (jac) k_fused_elem<true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
@@ -713,13 +754,20 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         else launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
         prof_end(PROF_ROW, s, m->max_deg > RG_MAXE ? 2 : 1);
         if (jac) {
+            // the element sweep counted the active elements: Term 3 is
+            // built only when there are any (flags already written)
+            int64_t known = 0;
+            UP3D_CUDA(cudaMemcpyAsync(&known, &mo->n_term3_active, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaStreamSynchronize(s));
             int64_t na = 0, nx = 0;
             prof_begin(PROF_TERM3, s);
-            build_term3(m, data, s, na, nx);
+            build_term3(m, data, s, na, nx, known, true);
             prof_end(PROF_TERM3, s, 0);
             m->last_drop_zeros = na > 0;
-            UP3D_CUDA(cudaMemcpyAsync(&mo->n_term3_extra, &nx, sizeof(int64_t), cudaMemcpyHostToDevice, s));
-            UP3D_CUDA(cudaStreamSynchronize(s));
+            if (nx) {
+                UP3D_CUDA(cudaMemcpyAsync(&mo->n_term3_extra, &nx, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+                UP3D_CUDA(cudaStreamSynchronize(s));
+            }
         }
     });
 }

@@ -204,25 +204,6 @@ void Operator::apply(const double* x, double* y, cudaStream_t s) const {
 
 // ------------------------------------------------------------ preconditioners
 
-struct up3d_precond {
-    int kind = 0;  // 0 identity, 1 Jacobi, 2 AMG
-    int64_t n = 0;
-    up3d::DBuf<double> dinv;
-    void* amg = nullptr;
-    up3d_precond() = default;
-    ~up3d_precond();
-    void apply(const double* r, double* z, cudaStream_t s);
-};
-
-namespace up3d {
-void amg_apply(void* amg, const double* r, double* z, cudaStream_t s);
-void amg_destroy(void* amg);
-}  // namespace up3d
-
-up3d_precond::~up3d_precond() {
-    if (amg) up3d::amg_destroy(amg);
-}
-
 void up3d_precond::apply(const double* r, double* z, cudaStream_t s) {
     using namespace up3d;
     if (kind == 1) {
@@ -448,15 +429,13 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
 using namespace up3d;
 
 namespace {
-Operator make_op(const up3d_csr* A, const up3d_csr* extra) {
-    Operator op;
+void make_op(Operator& op, const up3d_csr* A, const up3d_csr* extra) {
     UP3D_REQUIRE(A && A->indptr && A->indices && A->data && A->n >= 0, UP3D_ERR_ARGUMENT, "bad CSR operand");
     op.A = *A;
     if (extra && extra->indptr) {
         UP3D_REQUIRE(extra->n == A->n, UP3D_ERR_ARGUMENT, "extra operand size mismatch");
         op.extra = *extra;
     }
-    return op;
 }
 }  // namespace
 
@@ -491,7 +470,8 @@ int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double a
             int64_t* iters, double* resid, int* info, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(b && x, UP3D_ERR_ARGUMENT, "up3d_cg: null argument");
-        Operator op = make_op(A, nullptr);
+        Operator op;
+        make_op(op, A, nullptr);
         int inf = cg_solve(op, b, x, rtol, atol, maxiter, M, iters, resid, S(stream));
         if (info) *info = inf;
     });
@@ -502,7 +482,8 @@ int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double
                up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(b && x && restart > 0 && maxiter > 0, UP3D_ERR_ARGUMENT, "up3d_gmres: bad argument");
-        Operator op = make_op(A, extra);
+        Operator op;
+        make_op(op, A, extra);
         int inf = gmres_solve(op, b, x, rtol, atol, restart, maxiter, M, inner, resid, S(stream));
         if (info) *info = inf;
     });

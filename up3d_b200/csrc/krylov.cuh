@@ -29,4 +29,22 @@ struct Operator {
     void apply(const double* x, double* y, cudaStream_t s) const;
 };
 
+void amg_apply(void* amg, const double* r, double* z, cudaStream_t s);
+void amg_destroy(void* amg);
+void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s);
+const up3d_amg_info* amg_info(void* amg);
+
 }  // namespace up3d
+
+// Preconditioner handle: identity, point Jacobi or an AMG hierarchy.
+struct up3d_precond {
+    int kind = 0;  // 0 identity, 1 Jacobi, 2 AMG
+    int64_t n = 0;
+    up3d::DBuf<double> dinv;
+    void* amg = nullptr;
+    up3d_precond() = default;
+    ~up3d_precond() {
+        if (amg) up3d::amg_destroy(amg);
+    }
+    void apply(const double* r, double* z, cudaStream_t s);
+};
