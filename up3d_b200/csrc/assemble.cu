@@ -1,11 +1,14 @@
 // Residual, Picard matrix and Newton Jacobian assembly of the up3d library.
 //
-// Scatter-free design: every CSR row (and residual entry) is produced by one
-// warp that gathers the contributions of the row node's incident elements
-// from a per-element record (gB_j = grad . B_j and the Term-1/2/3 weights)
-// and writes the row once.  The summation order of every entry is fixed by
-// the mesh-setup plan, so results are bit-reproducible run to run with no
-// atomics, as the reference's colour-ordered scatter is
+// Two passes, no atomics:
+//   1. an element sweep computes, per element, its residual contributions
+//      R_i and its symmetric local matrix J_ij (Terms 1 + 2) -- all the
+//      floating-point work, once per element, with coalesced loads;
+//   2. a row gather: one warp per CSR row sums the contributions of the row
+//      node's incident elements in a fixed order (the mesh-setup plan) and
+//      writes the row once, coalesced.
+// Every entry's summation order is fixed by the mesh, so results are
+// bit-reproducible run to run, as the reference's colour-ordered scatter is
 // (kernels/jacobian.py:1-33, kernels/residual.py:44-76).
 //
 // Term 3 (upstream coupling, off the element pattern) is built per call
@@ -30,168 +33,167 @@ constexpr int RG_WARPS = 8;   // warps per block of the row gather
 constexpr int RG_MAXE = 64;   // incident elements per row staged in shared memory
 constexpr int WIDE_MAXE = 1024;
 
-struct RecView {
-    double gB[4];
-    double w1, w2;
-};
-
-__device__ __forceinline__ RecView load_rec(const ElemRecord* __restrict__ rec, int64_t e) {
-    const double2* p = reinterpret_cast<const double2*>(rec + e);
-    double2 a = p[0], b = p[1], c = p[2];
-    RecView r;
-    r.gB[0] = a.x;
-    r.gB[1] = a.y;
-    r.gB[2] = b.x;
-    r.gB[3] = b.y;
-    r.w1 = c.x;
-    r.w2 = c.y;
-    return r;
-}
-
-__device__ __forceinline__ double pick4(int i, double a, double b, double c, double d) {
-    return i == 0 ? a : (i == 1 ? b : (i == 2 ? c : d));
-}
-
-// Row i of the packed symmetric element matrix B B^T
-// (storage order 00,01,02,03,11,12,13,22,23,33).
-__device__ __forceinline__ void bb_row(const double* __restrict__ BB, int64_t e, int i, double out[4]) {
-    const double2* p = reinterpret_cast<const double2*>(BB + 10 * e);
-    double2 v0 = p[0], v1 = p[1], v2 = p[2], v3 = p[3], v4 = p[4];
-    // v0=(00,01) v1=(02,03) v2=(11,12) v3=(13,22) v4=(23,33)
-    out[0] = pick4(i, v0.x, v0.y, v1.x, v1.y);
-    out[1] = pick4(i, v0.y, v2.x, v2.y, v3.x);
-    out[2] = pick4(i, v1.x, v2.y, v3.y, v4.x);
-    out[3] = pick4(i, v1.y, v3.x, v4.x, v4.y);
-}
-
-// One warp per row: R_n = sum_e w1_e gB_e,i and the row of
-//   J_nm = sum_e w1_e (B_i . B_j) + [w2_e != 0] w2_e gB_i gB_j
-// (kernels/jacobian.py:406-433: Term 2 only when its weight is non-zero, so
-// J reduces to the Picard matrix bitwise at s_e = 0).
 #ifndef UP3D_ROW_MINB
-#define UP3D_ROW_MINB 6
+#define UP3D_ROW_MINB 8
+#endif
+#ifndef UP3D_ELEM_MINB
+#define UP3D_ELEM_MINB 3
+#endif
+#ifndef UP3D_ELEM_MINB_JAC
+#define UP3D_ELEM_MINB_JAC 3
 #endif
 
-// Shared memory of one warp: MAXE*4 doubles of contributions, then the
-// row's plan (at most 3 off-diagonal contributors per incident element).
-template <int MAXE>
-constexpr size_t row_smem_per_warp() {
-    return sizeof(double) * MAXE * 4 + ((sizeof(uint16_t) * 3 * MAXE + 15) / 16) * 16;
-}
-
-template <bool DO_R, bool DO_J, int MAXE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 1 ? 1 : UP3D_ROW_MINB)
-    k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
-                 const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
-                 const uint16_t* __restrict__ plan, const int32_t* __restrict__ diag,
-                 const double* __restrict__ BB, const ElemRecord* __restrict__ rec, double* __restrict__ R,
-                 double* __restrict__ J, bool wide_pass) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double* vals = reinterpret_cast<double*>(smem_raw + (size_t)w * row_smem_per_warp<MAXE>());
-    uint16_t* splan = reinterpret_cast<uint16_t*>(vals + MAXE * 4);
-    for (int64_t n = (int64_t)blockIdx.x * WARPS + w; n < N; n += (int64_t)gridDim.x * WARPS) {
-        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
-        // the narrow pass skips rows that need the wide buffer and vice versa
-        if (wide_pass ? deg <= RG_MAXE : deg > RG_MAXE) continue;
-        int32_t rb = 0, L = 0, pbase = 0;
-        if (DO_J) {
-            // stage the row's contributor plan (contiguous) with one
-            // coalesced pass, overlapped with the element loads below
-            rb = indptr[n];
-            L = indptr[n + 1] - rb;
-            pbase = plan_off[rb];
-            const int32_t pcnt = plan_off[rb + L] - pbase;
-            for (int t = lane; t < pcnt; t += 32) splan[t] = plan[pbase + t];
-        }
-        double r = 0.0, d = 0.0;
-        for (int k = lane; k < deg; k += 32) {
-            uint32_t x = ent[eb + k];
-            int64_t e = x >> 2;
-            int i = x & 3;
-            RecView q = load_rec(rec, e);
-            double gBi = pick4(i, q.gB[0], q.gB[1], q.gB[2], q.gB[3]);
-            if (DO_R) r += q.w1 * gBi;
-            if (DO_J) {
-                double bij[4];
-                bb_row(BB, e, i, bij);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    double c = q.w1 * bij[j];
-                    if (q.w2 != 0.0) c += q.w2 * gBi * q.gB[j];
-                    vals[j * MAXE + k] = c;
-                    if (j == i) d += c;
-                }
-            }
-        }
-        if (DO_R) r = warp_sum(r);
-        if (DO_J) {
-            d = warp_sum(d);
-            __syncwarp();
-            const int32_t ds = diag[n];
-            for (int s = lane; s < L; s += 32) {
-                double v = d;
-                if (s != ds) {
-                    v = 0.0;
-                    const int32_t p1 = plan_off[rb + s + 1] - pbase;
-                    for (int32_t p = plan_off[rb + s] - pbase; p < p1; ++p) {
-                        uint32_t c = splan[p];
-                        v += vals[(c & 3) * MAXE + (c >> 2)];
-                    }
-                }
-                J[rb + s] = v;
-            }
-            __syncwarp();
-        }
-        if (DO_R && lane == 0) R[n] = r;
-    }
-}
-
-template <bool DO_R, bool DO_J>
-void launch_row_gather(const up3d_mesh* m, const ElemRecord* rec, double* R, double* J, cudaStream_t s) {
-    {
-        const size_t sm = RG_WARPS * row_smem_per_warp<RG_MAXE>();
-        auto kern = k_row_gather<DO_R, DO_J, RG_MAXE, RG_WARPS>;
-        const unsigned grid = grid_for(m->N, RG_WARPS, (int64_t)148 * 64);
-        kern<<<grid, RG_WARPS * 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
-                                              m->plan_off.get(), m->plan.get(), m->diag.get(), m->BB.get(), rec,
-                                              R, J, false);
-        UP3D_CHECK_LAUNCH();
-    }
-    if (m->max_deg > RG_MAXE) {
-        UP3D_REQUIRE(m->max_deg <= WIDE_MAXE, UP3D_ERR_VALUE,
-                     "a node is shared by more than 1024 elements; unsupported by the row gather");
-        const size_t sm = row_smem_per_warp<WIDE_MAXE>();
-        auto kern = k_row_gather<DO_R, DO_J, WIDE_MAXE, 1>;
-        UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        kern<<<148 * 4, 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(),
-                                     m->plan.get(), m->diag.get(), m->BB.get(), rec, R, J, true);
-        UP3D_CHECK_LAUNCH();
-    }
-}
-
-// ------------------------------------------------------------ prep kernels
-
-__device__ __forceinline__ void store_rec(ElemRecord* __restrict__ rec, int64_t e, const double gB[4], double w1,
-                                          double w2, double w3, double flag) {
-    double2* p = reinterpret_cast<double2*>(rec + e);
-    p[0] = make_double2(gB[0], gB[1]);
-    p[1] = make_double2(gB[2], gB[3]);
-    p[2] = make_double2(w1, w2);
-    p[3] = make_double2(w3, flag);
-}
+// ------------------------------------------------------------ element math
 
 __device__ __forceinline__ void gB_of(const double g[3], const double* __restrict__ b, double gB[4]) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) gB[j] = g[0] * b[3 * j] + g[1] * b[3 * j + 1] + g[2] * b[3 * j + 2];
 }
 
+// Index of the off-diagonal pair (a, b), a < b, in (01,02,03,12,13,23).
+__host__ __device__ __forceinline__ int off_index(int a, int b) { return a * (7 - a) / 2 - 1 + b - a; }
+
+// Local matrix of one element (kernels/jacobian.py:406-433):
+//   J_ij = w1 (B_i . B_j)  [+ w2 gB_i gB_j when w2 != 0]
+// Term 2 only when its weight is non-zero, so J reduces to the Picard
+// matrix bitwise at s_e = 0.  Explicit fma pins the rounding, so every
+// kernel that builds a local matrix produces identical bits.
+__device__ __forceinline__ double bbij(const double* b, int i, int j) {
+    return fma(b[3 * i + 2], b[3 * j + 2], fma(b[3 * i + 1], b[3 * j + 1], b[3 * i] * b[3 * j]));
+}
+__device__ __forceinline__ double jij(const double* b, const double gB[4], double w1, double w2, int i, int j) {
+    double v = w1 * bbij(b, i, j);
+    if (w2 != 0.0) v = fma(w2 * gB[i], gB[j], v);
+    return v;
+}
+
+// Writes [R_0, J_00, ..., R_3, J_33, J_01, J_02, J_03, J_12, J_13, J_23].
+__device__ __forceinline__ void store_local(double* __restrict__ loc, int64_t e, const double* b,
+                                            const double gB[4], double w1, double w2, bool with_r) {
+    double2* p = reinterpret_cast<double2*>(loc + (size_t)LOC_STRIDE * e);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        p[i] = make_double2(with_r ? w1 * gB[i] : 0.0, jij(b, gB, w1, w2, i, i));
+    p[4] = make_double2(jij(b, gB, w1, w2, 0, 1), jij(b, gB, w1, w2, 0, 2));
+    p[5] = make_double2(jij(b, gB, w1, w2, 0, 3), jij(b, gB, w1, w2, 1, 2));
+    p[6] = make_double2(jij(b, gB, w1, w2, 1, 3), jij(b, gB, w1, w2, 2, 3));
+}
+
+__device__ __forceinline__ void store_res(double* __restrict__ res, int64_t e, const double gB[4], double w1) {
+    double2* p = reinterpret_cast<double2*>(res + 4 * e);
+    p[0] = make_double2(w1 * gB[0], w1 * gB[1]);
+    p[1] = make_double2(w1 * gB[2], w1 * gB[3]);
+}
+
+// Term-3 vectors of an active element: a_i = w3 gB_i (the reference's
+// wi = w * gi), b_k = grad_u . B_u,k (kernels/jacobian.py:469-481).
+__device__ __forceinline__ void store_t3(double* __restrict__ t3v, int64_t e, double w3, const double gB[4],
+                                         const double f[4]) {
+    double2* p = reinterpret_cast<double2*>(t3v + 8 * e);
+    p[0] = make_double2(w3 * gB[0], w3 * gB[1]);
+    p[1] = make_double2(w3 * gB[2], w3 * gB[3]);
+    p[2] = make_double2(f[0], f[1]);
+    p[3] = make_double2(f[2], f[3]);
+}
+
+__device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, double b[12]) {
+    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double2 v = b2[k];
+        b[2 * k] = v.x;
+        b[2 * k + 1] = v.y;
+    }
+}
+
+// ------------------------------------------------------------ row gather
+
+template <int MAXE>
+constexpr size_t row_smem_per_warp() {
+    // entries (uint32) then the plan (uint16, 3 per entry), 16-B aligned
+    return ((sizeof(uint32_t) * MAXE + sizeof(uint16_t) * 3 * MAXE + 15) / 16) * 16;
+}
+
+// Jacobian rows (and, when R != null, the residual) from the local
+// matrices: R_n = sum_e R_e,i ; J_nn = sum_e J_e,ii ; J_nm = sum over the
+// plan's contributors (e, i, j) of J_e,ij.
+template <int MAXE, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 1 ? 1 : UP3D_ROW_MINB)
+    k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
+                 const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
+                 const uint16_t* __restrict__ plan, const int32_t* __restrict__ diag, const double* __restrict__ loc,
+                 double* __restrict__ R, double* __restrict__ J, bool wide_pass) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* sent = reinterpret_cast<uint32_t*>(smem_raw + (size_t)w * row_smem_per_warp<MAXE>());
+    uint16_t* splan = reinterpret_cast<uint16_t*>(sent + MAXE);
+    for (int64_t n = (int64_t)blockIdx.x * WARPS + w; n < N; n += (int64_t)gridDim.x * WARPS) {
+        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
+        if (wide_pass ? deg <= RG_MAXE : deg > RG_MAXE) continue;
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb;
+        const int32_t pbase = plan_off[rb];
+        const int32_t pcnt = plan_off[rb + L] - pbase;
+        for (int t = lane; t < pcnt; t += 32) splan[t] = plan[pbase + t];
+        double r = 0.0, d = 0.0;
+        for (int k = lane; k < deg; k += 32) {
+            const uint32_t x = ent[eb + k];
+            sent[k] = x;
+            const double2 v = reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
+            r += v.x;
+            d += v.y;
+        }
+        d = warp_sum(d);
+        if (R) r = warp_sum(r);
+        __syncwarp();
+        const int32_t ds = diag[n];
+        for (int s = lane; s < L; s += 32) {
+            double v = d;
+            if (s != ds) {
+                v = 0.0;
+                const int32_t p1 = plan_off[rb + s + 1] - pbase;
+                for (int32_t p = plan_off[rb + s] - pbase; p < p1; ++p) {
+                    const uint32_t c = splan[p];
+                    const uint32_t x = sent[c >> 2];
+                    const int i = x & 3, j = c & 3;
+                    const int q = i < j ? off_index(i, j) : off_index(j, i);
+                    v += loc[(size_t)LOC_STRIDE * (x >> 2) + 8 + q];
+                }
+            }
+            J[rb + s] = v;
+        }
+        if (R && lane == 0) R[n] = r;
+        __syncwarp();
+    }
+}
+
+// Residual rows only: R_n = sum_e R_e,i from the compact residual array.
+__global__ void __launch_bounds__(256)
+    k_row_residual(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
+                   const double* __restrict__ res, double* __restrict__ R) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < N; n += n_warps) {
+        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
+        double r = 0.0;
+        for (int k = lane; k < deg; k += 32) {
+            const uint32_t x = ent[eb + k];
+            r += res[4 * (size_t)(x >> 2) + (x & 3)];
+        }
+        r = warp_sum(r);
+        if (lane == 0) R[n] = r;
+    }
+}
+
+// ------------------------------------------------------------ prep kernels
+// Element sweeps of the single-purpose entry points.
+
 // assemble_residual: velocities into the workspace (kernels/jacobian.py:623)
-// and the per-element record with w1 = rho_tilde V.
+// and the residual contributions w1 gB_i with w1 = rho_tilde V.
 __global__ void k_prep_residual(const int4* __restrict__ conn, const double* __restrict__ B,
                                 const double* __restrict__ V, const double* __restrict__ phi,
                                 const double* __restrict__ rt, int64_t E, double* __restrict__ grad,
-                                double* __restrict__ q2, ElemRecord* __restrict__ rec) {
+                                double* __restrict__ q2, double* __restrict__ res) {
     GRID_STRIDE(e, E) {
         double g[3], b[12];
         int4 c;
@@ -202,33 +204,34 @@ __global__ void k_prep_residual(const int4* __restrict__ conn, const double* __r
         q2[e] = dot3r(g[0], g[1], g[2], g[0], g[1], g[2]);
         double gB[4];
         gB_of(g, b, gB);
-        double w1 = (rt ? rt[e] : 1.0) * V[e];
-        store_rec(rec, e, gB, w1, 0.0, 0.0, 0.0);
+        store_res(res, e, gB, (rt ? rt[e] : 1.0) * V[e]);
     }
 }
 
-// assemble_matrix: w1 = rho_tilde V only.
-__global__ void k_prep_matrix(const double* __restrict__ V, const double* __restrict__ rt, int64_t E,
-                              ElemRecord* __restrict__ rec) {
+// assemble_matrix: J_ij = rho_tilde V (B_i . B_j).
+__global__ void k_prep_matrix(const double* __restrict__ B, const double* __restrict__ V,
+                              const double* __restrict__ rt, int64_t E, double* __restrict__ loc) {
     GRID_STRIDE(e, E) {
-        double z[4] = {0.0, 0.0, 0.0, 0.0};
-        store_rec(rec, e, z, (rt ? rt[e] : 1.0) * V[e], 0.0, 0.0, 0.0);
+        double b[12];
+        load_B(B, e, b);
+        const double z[4] = {0.0, 0.0, 0.0, 0.0};
+        store_local(loc, e, b, z, (rt ? rt[e] : 1.0) * V[e], 0.0, false);
     }
 }
 
 // assemble_newton_jacobian (kernels/jacobian.py:323-338, :410-414): the
 // limiter mask gates s_e by lim[e] and s_u by lim[upstream[e]]; Term-2 and
-// Term-3 weights 2 inv_u2 s V; the upstream factor grad_u . B_u,k of active
-// elements (s_u != 0).  `grad` holds grad(phi) of every element.
-__global__ void k_prep_jacobian(const int4* __restrict__ conn, const double* __restrict__ B,
-                                const double* __restrict__ V, const double* __restrict__ grad,
-                                const double* __restrict__ rt, const double* __restrict__ se,
-                                const double* __restrict__ su, const int64_t* __restrict__ up,
-                                const uint8_t* __restrict__ lim, double inv_u2, int64_t E,
-                                ElemRecord* __restrict__ rec, double* __restrict__ t3b,
-                                int32_t* __restrict__ up32) {
+// Term-3 weights 2 inv_u2 s V; Term-3 vectors of active elements
+// (s_u != 0).  `grad` holds grad(phi) of every element.
+__global__ void k_prep_jacobian(const double* __restrict__ B, const double* __restrict__ V,
+                                const double* __restrict__ grad, const double* __restrict__ rt,
+                                const double* __restrict__ se, const double* __restrict__ su,
+                                const int64_t* __restrict__ up, const uint8_t* __restrict__ lim, double inv_u2,
+                                int64_t E, double* __restrict__ loc, double* __restrict__ t3v,
+                                uint8_t* __restrict__ t3flag, int32_t* __restrict__ up32) {
     GRID_STRIDE(e, E) {
-        const double* b = B + 12 * e;
+        double b[12];
+        load_B(B, e, b);
         double g[3] = {grad[3 * e], grad[3 * e + 1], grad[3 * e + 2]};
         double gB[4];
         gB_of(g, b, gB);
@@ -238,20 +241,20 @@ __global__ void k_prep_jacobian(const int4* __restrict__ conn, const double* __r
             s_e = s_e * (lim[e] ? 1.0 : 0.0);
             s_u = s_u * (lim[u] ? 1.0 : 0.0);
         }
-        double Ve = V[e];
-        double w2 = 2.0 * inv_u2 * s_e * Ve;
-        double w3 = 2.0 * inv_u2 * s_u * Ve;
-        bool active = s_u != 0.0;
+        const double Ve = V[e];
+        const double w2 = 2.0 * inv_u2 * s_e * Ve;
+        const double w3 = 2.0 * inv_u2 * s_u * Ve;
+        const bool active = s_u != 0.0;
         if (active) {
-            const double* bu = B + 12 * u;
+            double bu[12], f[4];
+            load_B(B, u, bu);
             double gu[3] = {grad[3 * u], grad[3 * u + 1], grad[3 * u + 2]};
-            double f[4];
             gB_of(gu, bu, f);
-            reinterpret_cast<double2*>(t3b + 4 * e)[0] = make_double2(f[0], f[1]);
-            reinterpret_cast<double2*>(t3b + 4 * e)[1] = make_double2(f[2], f[3]);
+            store_t3(t3v, e, w3, gB, f);
         }
+        t3flag[e] = active ? 1 : 0;
         up32[e] = (int32_t)u;
-        store_rec(rec, e, gB, rt[e] * Ve, w2, w3, active ? 1.0 : 0.0);
+        store_local(loc, e, b, gB, rt[e] * Ve, w2, false);
     }
 }
 
@@ -278,18 +281,15 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // eval_residual + assemble_coupled, per element (pyfp3d/solve/newton.py:
 // 345-372, :435-452): gradient, limiter, density, upstream walk (or the
 // frozen selection), the upstream element's state recomputed in place, the
-// flux, its sensitivities and the element record.
-#ifndef UP3D_ELEM_MINB
-#define UP3D_ELEM_MINB 3
-#endif
-
+// flux, its sensitivities, and the element's residual contributions and
+// local matrix (JAC) or residual contributions only.
 template <bool FROZEN, bool JAC>
-__global__ void __launch_bounds__(256, UP3D_ELEM_MINB)
+__global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
                  const int4* __restrict__ fn, const double4* __restrict__ cen, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F, double u2, const int64_t* __restrict__ up_fz,
-                 const int8_t* __restrict__ br_fz, int64_t E, ElemRecord* __restrict__ rec,
-                 double* __restrict__ t3b, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
+                 const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
+                 double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
                  double* __restrict__ rt_out, up3d_monitors* mon) {
     MonAcc acc;
     GRID_STRIDE(e, E) {
@@ -350,23 +350,25 @@ __global__ void __launch_bounds__(256, UP3D_ELEM_MINB)
         acc.nu_max = fmax(acc.nu_max, nu);
         acc.sup += (nu > 0.0);
 
-        double Ve = V[e];
-        double w2 = 0.0, w3 = 0.0;
-        bool active = false;
+        const double Ve = V[e];
+        const double w1 = rt * Ve;
         if (JAC) {
             s_e = s_e * (lim_e ? 1.0 : 0.0);
             s_u = s_u * (lim_u ? 1.0 : 0.0);
-            w2 = 2.0 * F.inv_u2 * s_e * Ve;
-            w3 = 2.0 * F.inv_u2 * s_u * Ve;
-            active = s_u != 0.0;
+            const double w2 = 2.0 * F.inv_u2 * s_e * Ve;
+            const double w3 = 2.0 * F.inv_u2 * s_u * Ve;
+            const bool active = s_u != 0.0;
             if (active) {
-                reinterpret_cast<double2*>(t3b + 4 * e)[0] = make_double2(f[0], f[1]);
-                reinterpret_cast<double2*>(t3b + 4 * e)[1] = make_double2(f[2], f[3]);
+                store_t3(t3v, e, w3, gB, f);
                 acc.act += 1;
             }
+            t3flag[e] = active ? 1 : 0;
+            double b[12];
+            load_B(B, e, b);  // second touch of B_e: an L2 hit
+            store_local(loc, e, b, gB, w1, w2, true);
+        } else {
+            store_res(res, e, gB, w1);
         }
-        store_rec(rec, e, gB, rt * Ve, w2, w3, active ? 1.0 : 0.0);
-        if (JAC) t3flag[e] = active ? 1 : 0;
         up_out[e] = (int32_t)u;
         if (rt_out) rt_out[e] = rt;
     }
@@ -375,16 +377,12 @@ __global__ void __launch_bounds__(256, UP3D_ELEM_MINB)
 
 // ------------------------------------------------------------ Term 3
 
-__global__ void k_t3_flags(const ElemRecord* __restrict__ rec, int64_t E, uint8_t* __restrict__ flag) {
-    GRID_STRIDE(e, E) flag[e] = rec[e].pad != 0.0;
-}
-
 // fill_term3_coo (kernels/jacobian.py:184-229): 16 entries per active
 // element, rows nodes(e) x cols nodes(u(e)), slot 16a + 4i + k.
 __global__ void k_t3_coo(const int32_t* __restrict__ active, const int64_t* __restrict__ n_active,
                          const int4* __restrict__ conn, const int32_t* __restrict__ up,
-                         const ElemRecord* __restrict__ rec, const double* __restrict__ t3b,
-                         uint64_t* __restrict__ keys, double* __restrict__ vals, int32_t* __restrict__ perm) {
+                         const double* __restrict__ t3v, uint64_t* __restrict__ keys, double* __restrict__ vals,
+                         int32_t* __restrict__ perm) {
     const int64_t A = *n_active;
     GRID_STRIDE(a, A) {
         int64_t e = active[a];
@@ -392,13 +390,13 @@ __global__ void k_t3_coo(const int32_t* __restrict__ active, const int64_t* __re
         int4 ce = conn[e], cu = conn[u];
         int re[4] = {ce.x, ce.y, ce.z, ce.w};
         int cl[4] = {cu.x, cu.y, cu.z, cu.w};
-        const ElemRecord& q = rec[e];
+        const double* t = t3v + 8 * e;
         for (int i = 0; i < 4; ++i) {
-            double wi = q.w3 * q.gB[i];
+            const double wi = t[i];
             for (int k = 0; k < 4; ++k) {
                 int64_t idx = 16 * a + 4 * i + k;
                 keys[idx] = ((uint64_t)(uint32_t)re[i] << 32) | (uint32_t)cl[k];
-                vals[idx] = wi * t3b[4 * e + k];
+                vals[idx] = wi * t[4 + k];
                 perm[idx] = (int32_t)idx;
             }
         }
@@ -500,38 +498,64 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 
 }  // namespace
 
-// Builds Term 3 from the element records (flag = pad != 0): folds the
-// in-pattern part into `data`, keeps the extras (sorted by row, col) in the
-// mesh workspace, and returns (n_active, n_extra).  Synchronises the stream.
-// `known_active` >= 0 is the active count already known to the caller (0
-// skips everything); `flags_ready` means m->t3_flag already holds the
-// active flags.
-static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
-                        int64_t known_active = -1, bool flags_ready = false) {
-    const int64_t E = m->E;
-    if (known_active == 0) {
-        n_active = n_extra = 0;
-        m->last_active = m->last_extra = 0;
-        return;
-    }
-    m->t3_flag.alloc(E);
-    m->t3_active.alloc(E);
-    m->i64_ws.alloc(8);
-    if (!flags_ready) {
-        k_t3_flags<<<grid_for(E, 256), 256, 0, s>>>(m->rec.get(), E, m->t3_flag.get());
+// ------------------------------------------------------------ launchers
+
+// Jacobian (+ residual) rows from m->loc.
+void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
+    {
+        const size_t sm = RG_WARPS * row_smem_per_warp<RG_MAXE>();
+        const unsigned grid = grid_for(m->N, RG_WARPS, (int64_t)148 * 64);
+        k_row_gather<RG_MAXE, RG_WARPS><<<grid, RG_WARPS * 32, sm, s>>>(
+            m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(), m->plan.get(), m->diag.get(),
+            m->loc.get(), R, J, false);
         UP3D_CHECK_LAUNCH();
     }
+    if (m->max_deg > RG_MAXE) {
+        UP3D_REQUIRE(m->max_deg <= WIDE_MAXE, UP3D_ERR_VALUE,
+                     "a node is shared by more than 1024 elements; unsupported by the row gather");
+        const size_t sm = row_smem_per_warp<WIDE_MAXE>();
+        auto kern = k_row_gather<WIDE_MAXE, 1>;
+        UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<148 * 4, 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(),
+                                     m->plan.get(), m->diag.get(), m->loc.get(), R, J, true);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+// Residual rows from m->res.
+void launch_row_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
+    k_row_residual<<<grid_for(32 * m->N, 256, (int64_t)148 * 64), 256, 0, s>>>(m->N, m->ent_off.get(),
+                                                                             m->ent.get(), m->res.get(), R);
+    UP3D_CHECK_LAUNCH();
+}
+
+// Builds Term 3 from the active flags and vectors: folds the in-pattern
+// part into `data`, keeps the extras (sorted by row, col) in the mesh
+// workspace, and returns (n_active, n_extra).  Synchronises the stream.
+// `known_active` >= 0 is the active count already known to the caller (0
+// skips everything).
+static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
+                        int64_t known_active = -1) {
+    const int64_t E = m->E;
+    n_extra = 0;
+    m->last_extra = 0;
+    if (known_active == 0) {
+        n_active = 0;
+        m->last_active = 0;
+        return;
+    }
+    m->t3_active.alloc(E);
+    m->i64_ws.alloc(8);
     size_t bytes = 0;
     thrust::counting_iterator<int32_t> it(0);
-    UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(), E, s));
-    m->cub_tmp.alloc(bytes);
-    UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(),
+    UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(),
                                          E, s));
+    m->cub_tmp.alloc(bytes);
+    UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), bytes, it, m->t3_flag.get(), m->t3_active.get(),
+                                         m->i64_ws.get(), E, s));
     UP3D_CUDA(cudaMemcpyAsync(&n_active, m->i64_ws.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaStreamSynchronize(s));
-    n_extra = 0;
     m->last_active = n_active;
-    m->last_extra = 0;
     if (n_active == 0) return;
     const int64_t n = 16 * n_active;
     m->t3_keys.alloc(n);
@@ -541,9 +565,9 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
     m->t3_perm_s.alloc(n);
     m->t3_head.alloc(n);
     m->t3_seg.alloc(n);
-    k_t3_coo<<<grid_for(n_active, 128), 128, 0, s>>>(m->t3_active.get(), m->i64_ws.get(), m->conn.get(), m->up32.get(),
-                                                     m->rec.get(), m->t3b.get(), m->t3_keys.get(), m->t3_vals.get(),
-                                                     m->t3_perm.get());
+    k_t3_coo<<<grid_for(n_active, 128), 128, 0, s>>>(m->t3_active.get(), m->i64_ws.get(), m->conn.get(),
+                                                     m->up32.get(), m->t3v.get(), m->t3_keys.get(),
+                                                     m->t3_vals.get(), m->t3_perm.get());
     UP3D_CHECK_LAUNCH();
     int end_bit = 32;
     {
@@ -552,11 +576,11 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
         end_bit = 32 + b;
     }
     bytes = 0;
-    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, m->t3_keys.get(), m->t3_keys_s.get(), m->t3_perm.get(),
-                                              m->t3_perm_s.get(), n, 0, end_bit, s));
+    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, m->t3_keys.get(), m->t3_keys_s.get(),
+                                              m->t3_perm.get(), m->t3_perm_s.get(), n, 0, end_bit, s));
     m->cub_tmp.alloc(bytes);
-    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(m->cub_tmp.get(), bytes, m->t3_keys.get(), m->t3_keys_s.get(), m->t3_perm.get(),
-                                              m->t3_perm_s.get(), n, 0, end_bit, s));
+    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(m->cub_tmp.get(), bytes, m->t3_keys.get(), m->t3_keys_s.get(),
+                                              m->t3_perm.get(), m->t3_perm_s.get(), n, 0, end_bit, s));
     k_t3_heads<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), n, m->t3_head.get());
     UP3D_CHECK_LAUNCH();
     scan(m, m->t3_head.get(), m->t3_seg.get(), n, s);
@@ -569,9 +593,9 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
     m->x_col.alloc(n_uniq);
     m->x_val.alloc(n_uniq);
     m->x_flag.alloc(n_uniq + 1);
-    k_t3_reduce<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), m->t3_vals.get(), m->t3_perm_s.get(), m->t3_seg.get(), n,
-                                                 m->indptr.get(), m->indices.get(), data, m->x_row.get(), m->x_col.get(),
-                                                 m->x_val.get(), m->x_flag.get());
+    k_t3_reduce<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), m->t3_vals.get(), m->t3_perm_s.get(),
+                                                 m->t3_seg.get(), n, m->indptr.get(), m->indices.get(), data,
+                                                 m->x_row.get(), m->x_col.get(), m->x_val.get(), m->x_flag.get());
     UP3D_CHECK_LAUNCH();
     // compact the extras (keeps the (row, col) order)
     m->x_row_c.alloc(n_uniq);
@@ -594,36 +618,30 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
     m->x_ptr.alloc(m->N + 1);
     UP3D_CUDA(cudaMemsetAsync(m->x_ptr.get(), 0, sizeof(int32_t) * (m->N + 1), s));
     if (n_extra > 0) {
-        DBuf<int32_t> cnt;
-        cnt.alloc(m->N + 1);
-        UP3D_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
-        k_rows_from_extras<<<grid_for(n_extra, 256), 256, 0, s>>>(m->x_row_c.get(), n_extra, cnt.get());
+        m->extra_cnt.alloc(m->N + 1);
+        UP3D_CUDA(cudaMemsetAsync(m->extra_cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
+        k_rows_from_extras<<<grid_for(n_extra, 256), 256, 0, s>>>(m->x_row_c.get(), n_extra, m->extra_cnt.get());
         UP3D_CHECK_LAUNCH();
-        scan(m, cnt.get(), m->x_ptr.get(), m->N + 1, s);
+        scan(m, m->extra_cnt.get(), m->x_ptr.get(), m->N + 1, s);
         UP3D_CUDA(cudaStreamSynchronize(s));
     }
 }
 
 static int64_t merged_nnz(up3d_mesh* m, const double* data, cudaStream_t s) {
     if (m->last_active == 0) return m->nnz;
-        DBuf<unsigned long long> c;
-    c.alloc(1);
-    UP3D_CUDA(cudaMemsetAsync(c.get(), 0, sizeof(unsigned long long), s));
-    k_count_nonzero<<<grid_for(m->nnz, 256), 256, 0, s>>>(data, m->nnz, c.get());
+    m->i64_ws.alloc(8);
+    unsigned long long* c = reinterpret_cast<unsigned long long*>(m->i64_ws.get() + 2);
+    UP3D_CUDA(cudaMemsetAsync(c, 0, sizeof(unsigned long long), s));
+    k_count_nonzero<<<grid_for(m->nnz, 256), 256, 0, s>>>(data, m->nnz, c);
     UP3D_CHECK_LAUNCH();
     if (m->last_extra > 0) {
-        k_count_nonzero<<<grid_for(m->last_extra, 256), 256, 0, s>>>(m->x_val_c.get(), m->last_extra, c.get());
+        k_count_nonzero<<<grid_for(m->last_extra, 256), 256, 0, s>>>(m->x_val_c.get(), m->last_extra, c);
         UP3D_CHECK_LAUNCH();
     }
     unsigned long long h = 0;
-    UP3D_CUDA(cudaMemcpyAsync(&h, c.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(&h, c, sizeof(h), cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaStreamSynchronize(s));
     return (int64_t)h;
-}
-
-// launchers used by other translation units
-void row_gather_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
-    launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
 }
 
 }  // namespace up3d
@@ -646,9 +664,9 @@ int up3d_residual(up3d_mesh* m, const double* phi, const double* rt, double* R, 
             q2_out = m->q2_ws.get();
         }
         k_prep_residual<<<grid_for(m->E, 256), 256, 0, s>>>(m->conn.get(), m->B.get(), m->V.get(), phi, rt, m->E,
-                                                           grad_out, q2_out, m->rec.get());
+                                                           grad_out, q2_out, m->res.get());
         UP3D_CHECK_LAUNCH();
-        launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
+        launch_row_residual(m, R, s);
     });
 }
 
@@ -656,9 +674,9 @@ int up3d_picard_matrix(up3d_mesh* m, const double* rt, double* data, up3d_stream
     return guarded([&] {
         UP3D_REQUIRE(m && data, UP3D_ERR_ARGUMENT, "up3d_picard_matrix: null argument");
         cudaStream_t s = S(stream);
-        k_prep_matrix<<<grid_for(m->E, 256), 256, 0, s>>>(m->V.get(), rt, m->E, m->rec.get());
+        k_prep_matrix<<<grid_for(m->E, 256), 256, 0, s>>>(m->B.get(), m->V.get(), rt, m->E, m->loc.get());
         UP3D_CHECK_LAUNCH();
-        launch_row_gather<false, true>(m, m->rec.get(), nullptr, data, s);
+        launch_row_gather(m, nullptr, data, s);
     });
 }
 
@@ -669,16 +687,20 @@ int up3d_jacobian(up3d_mesh* m, const double* phi, const double* rt, const doubl
         UP3D_REQUIRE(m && phi && rt && se && su && upstream && data, UP3D_ERR_ARGUMENT,
                      "up3d_jacobian: null argument");
         cudaStream_t s = S(stream);
+        m->grad_ws.alloc(3 * m->E);
+        m->q2_ws.alloc(m->E);
+        // scratch velocities (the reference recomputes grad into a fresh array,
+        // kernels/jacobian.py:328-332)
         DBuf<double> grad, q2;
         grad.alloc(3 * m->E);
         q2.alloc(m->E);
         launch_velocities(m, phi, grad.get(), q2.get(), s);
         const double inv_u2 = 1.0 / (u_inf * u_inf);
-        k_prep_jacobian<<<grid_for(m->E, 256), 256, 0, s>>>(m->conn.get(), m->B.get(), m->V.get(), grad.get(), rt, se,
-                                                           su, upstream, lim, inv_u2, m->E, m->rec.get(),
-                                                           m->t3b.get(), m->up32.get());
+        k_prep_jacobian<<<grid_for(m->E, 256), 256, 0, s>>>(m->B.get(), m->V.get(), grad.get(), rt, se, su, upstream,
+                                                           lim, inv_u2, m->E, m->loc.get(), m->t3v.get(),
+                                                           m->t3_flag.get(), m->up32.get());
         UP3D_CHECK_LAUNCH();
-        launch_row_gather<false, true>(m, m->rec.get(), nullptr, data, s);
+        launch_row_gather(m, nullptr, data, s);
         int64_t na = 0, nx = 0;
         build_term3(m, data, s, na, nx);
         m->last_drop_zeros = na > 0;
@@ -694,19 +716,19 @@ int up3d_jacobian_export(up3d_mesh* m, const double* data, int32_t* indptr, int3
         UP3D_REQUIRE(m && data && indptr && indices && merged, UP3D_ERR_ARGUMENT,
                      "up3d_jacobian_export: null argument");
         cudaStream_t s = S(stream);
-                const bool has_x = m->last_extra > 0;
+        const bool has_x = m->last_extra > 0;
         const int32_t* xptr = has_x ? m->x_ptr.get() : nullptr;
-        DBuf<int32_t> cnt;
-        cnt.alloc(m->N + 1);
-        UP3D_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
+        m->extra_cnt.alloc(m->N + 1);
+        int32_t* cnt = m->extra_cnt.get();
+        UP3D_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (m->N + 1), s));
         k_merge_rows<false><<<grid_for(m->N, 256), 256, 0, s>>>(m->N, m->indptr.get(), m->indices.get(), data, xptr,
-                                                               m->x_col_c.get(), m->x_val_c.get(), m->last_drop_zeros,
-                                                               cnt.get(), nullptr, nullptr);
+                                                               m->x_col_c.get(), m->x_val_c.get(),
+                                                               m->last_drop_zeros, cnt, nullptr, nullptr);
         UP3D_CHECK_LAUNCH();
-        scan(m, cnt.get(), indptr, m->N + 1, s);
+        scan(m, cnt, indptr, m->N + 1, s);
         k_merge_rows<true><<<grid_for(m->N, 256), 256, 0, s>>>(m->N, m->indptr.get(), m->indices.get(), data, xptr,
-                                                              m->x_col_c.get(), m->x_val_c.get(), m->last_drop_zeros,
-                                                              indptr, indices, merged);
+                                                              m->x_col_c.get(), m->x_val_c.get(),
+                                                              m->last_drop_zeros, indptr, indices, merged);
         UP3D_CHECK_LAUNCH();
     });
 }
@@ -731,11 +753,10 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         up3d_monitors* mo = mon ? mon : m->mon_ws.get();
         UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
         const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
-#define FUSED_ARGS                                                                                               \
+#define FUSED_ARGS                                                                                                \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->cen.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
-        m->E, m->rec.get(), m->t3b.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo
+        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo
         const bool jac = data != nullptr;
-        if (jac) m->t3_flag.alloc(m->E);
         prof_begin(PROF_ELEM, s);
         if (up_fz) {
             if (jac) k_fused_elem<true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
@@ -750,9 +771,9 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         if (up_out)
             UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
         prof_begin(PROF_ROW, s);
-        if (jac) launch_row_gather<true, true>(m, m->rec.get(), R, data, s);
-        else launch_row_gather<true, false>(m, m->rec.get(), R, nullptr, s);
-        prof_end(PROF_ROW, s, m->max_deg > RG_MAXE ? 2 : 1);
+        if (jac) launch_row_gather(m, R, data, s);
+        else launch_row_residual(m, R, s);
+        prof_end(PROF_ROW, s, jac && m->max_deg > RG_MAXE ? 2 : 1);
         if (jac) {
             // the element sweep counted the active elements: Term 3 is
             // built only when there are any (flags already written)
@@ -761,7 +782,7 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
             UP3D_CUDA(cudaStreamSynchronize(s));
             int64_t na = 0, nx = 0;
             prof_begin(PROF_TERM3, s);
-            build_term3(m, data, s, na, nx, known, true);
+            build_term3(m, data, s, na, nx, known);
             prof_end(PROF_TERM3, s, 0);
             m->last_drop_zeros = na > 0;
             if (nx) {

@@ -93,16 +93,14 @@ struct DBuf {
 
 // ------------------------------------------------------------ mesh handle
 
-// Per-element record produced by the element sweep and consumed by the row
-// gather (64 B, one cache sector pair): gB_j = grad(phi)_e . B_e,j, the
-// Term-1/2/3 weights, and padding.
-struct __align__(16) ElemRecord {
-    double gB[4];
-    double w1;  // rho_tilde_e V_e
-    double w2;  // 2 inv_u2 s_e V_e (0 when Term 2 is absent)
-    double w3;  // 2 inv_u2 s_u V_e (0 when Term 3 is absent)
-    double pad;
-};
+// Local element data written by the element sweeps and gathered by rows:
+//   LOC (E, 14): [R_0, J_00, R_1, J_11, R_2, J_22, R_3, J_33,
+//                 J_01, J_02, J_03, J_12, J_13, J_23]
+//     R_i  = rho~_e V_e (grad . B_i)                   residual contribution
+//     J_ij = rho~_e V_e (B_i . B_j) [+ w2 gB_i gB_j]   Terms 1 + 2 (symmetric)
+//   RES (E, 4): R_i only (residual-only evaluations)
+//   T3V (E, 8): a_i = w3 gB_i, b_k = grad_u . B_u,k (Term-3 active elements)
+constexpr int LOC_STRIDE = 14;
 
 }  // namespace up3d
 
@@ -117,7 +115,6 @@ struct up3d_mesh {
     up3d::DBuf<int4> conn;       // (E)
     up3d::DBuf<double> B;        // (E, 12) AoS
     up3d::DBuf<double> V;        // (E)
-    up3d::DBuf<double> BB;       // (E, 10) packed B_i . B_j, i <= j
     up3d::DBuf<int4> fnbr;       // (E) face neighbours (-1 = boundary)
     up3d::DBuf<double4> cen;     // (E) centroids
 
@@ -131,8 +128,9 @@ struct up3d_mesh {
     up3d::DBuf<int32_t> diag;     // (N) slot of the diagonal within its row
 
     // workspaces (device)
-    up3d::DBuf<up3d::ElemRecord> rec;  // (E)
-    up3d::DBuf<double> t3b;            // (E, 4) Term-3 upstream factors
+    up3d::DBuf<double> loc;            // (E, LOC_STRIDE) local matrices + residual
+    up3d::DBuf<double> res;            // (E, 4) residual contributions
+    up3d::DBuf<double> t3v;            // (E, 8) Term-3 vectors of active elements
     up3d::DBuf<int32_t> up32;          // (E) upstream (internal)
     up3d::DBuf<double> grad_ws;        // (E, 3)
     up3d::DBuf<double> q2_ws;          // (E)

@@ -41,13 +41,13 @@ __global__ void k_pad_nodes(const double* __restrict__ nodes, int64_t N, double4
         out[n] = make_double4(nodes[3 * n], nodes[3 * n + 1], nodes[3 * n + 2], 0.0);
 }
 
-// B_e, V_e, packed B_i . B_j and centroids (mesh/metrics.py:27-70, :130-204;
+// B_e, V_e and centroids (mesh/metrics.py:27-70, :130-204;
 // kernels/upwind.py:750).  Rows of J^{-1} are the cross products of J's
 // columns over det J; B_0 = -(B_1 + B_2 + B_3).  `bad` receives the smallest
 // degenerate element index (|det J| < 1e-12 * |v1||v2||v3|).
 __global__ void k_geometry(const double4* __restrict__ X, const int4* __restrict__ conn, int64_t E,
-                           double* __restrict__ B, double* __restrict__ V, double* __restrict__ BB,
-                           double4* __restrict__ cen, unsigned long long* bad) {
+                           double* __restrict__ B, double* __restrict__ V, double4* __restrict__ cen,
+                           unsigned long long* bad) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
          e += (int64_t)gridDim.x * blockDim.x) {
         int4 c = conn[e];
@@ -82,12 +82,6 @@ __global__ void k_geometry(const double4* __restrict__ X, const int4* __restrict
             for (int d = 0; d < 3; ++d) b[d] = -radd(radd(b[3 + d], b[6 + d]), b[9 + d]);
         }
         for (int k = 0; k < 12; ++k) B[12 * e + k] = b[k];
-        // packed symmetric products, order (00,01,02,03,11,12,13,22,23,33)
-        int p = 0;
-        for (int i = 0; i < 4; ++i)
-            for (int j = i; j < 4; ++j)
-                BB[10 * e + p++] = b[3 * i] * b[3 * j] + b[3 * i + 1] * b[3 * j + 1] +
-                                   b[3 * i + 2] * b[3 * j + 2];
         double cx = radd(radd(radd(x0.x, x1.x), x2.x), x3.x);
         double cy = radd(radd(radd(x0.y, x1.y), x2.y), x3.y);
         double cz = radd(radd(radd(x0.z, x1.z), x2.z), x3.z);
@@ -310,7 +304,6 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
     // geometry
     m->B.alloc(12 * E);
     m->V.alloc(E);
-    m->BB.alloc(10 * E);
     m->cen.alloc(E);
     {
         DBuf<unsigned long long> bad;
@@ -318,7 +311,7 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
         unsigned long long init = ~0ull;
         UP3D_CUDA(cudaMemcpyAsync(bad.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s));
         k_geometry<<<grid_for(E, block), block, 0, s>>>(m->nodes4.get(), m->conn.get(), E, m->B.get(),
-                                                         m->V.get(), m->BB.get(), m->cen.get(), bad.get());
+                                                         m->V.get(), m->cen.get(), bad.get());
         UP3D_CHECK_LAUNCH();
         unsigned long long hbad = 0;
         UP3D_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(hbad), cudaMemcpyDeviceToHost, s));
@@ -418,9 +411,11 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
 }
 
 void ensure_workspaces(up3d_mesh* m) {
-    m->rec.alloc(m->E);
+    m->loc.alloc((size_t)LOC_STRIDE * m->E);
+    m->res.alloc(4 * m->E);
     m->up32.alloc(m->E);
-    m->t3b.alloc(4 * m->E);
+    m->t3v.alloc(8 * m->E);
+    m->t3_flag.alloc(m->E);
     m->mon_ws.alloc(1);
     m->i64_ws.alloc(8);
 }

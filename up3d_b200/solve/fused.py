@@ -47,21 +47,24 @@ class ResidualJacobian:
         self._n_extra = 0
 
     def evaluate(self, phi, flow: FlowParams, jacobian: bool = True, frozen=None,
-                 keep_state: bool = True):
-        """R(phi) (and the Jacobian data on the P1 pattern).  `frozen` =
+                 keep_state: bool = True, R_out=None, data_out=None):
+        """R(phi) (and the Jacobian data on the P1 pattern) into this
+        workspace, or into R_out / data_out when given.  `frozen` =
         (upstream int64, branch int8) selects the frozen flux."""
         up_fz = br_fz = None
         if frozen is not None:
             t = L.torch()
             up_fz = L.to_device(frozen[0], t.int64)
             br_fz = L.to_device(frozen[1], t.int8)
+        R = self.R if R_out is None else R_out
+        data = self.data if data_out is None else data_out
         L.call("up3d_residual_jacobian", self.mesh.handle, phi.data_ptr(), flow.c(),
-               L.ptr(up_fz), L.ptr(br_fz), self.R.data_ptr(),
-               self.data.data_ptr() if jacobian else None,
+               L.ptr(up_fz), L.ptr(br_fz), R.data_ptr(),
+               data.data_ptr() if jacobian else None,
                self.rho_tilde.data_ptr() if keep_state else None,
                self.upstream.data_ptr() if keep_state else None,
                self.monitors.data_ptr(), L.stream_ptr())
-        return self.R
+        return R
 
     def read_monitors(self) -> dict:
         return L.read_monitors(self.monitors)
@@ -82,6 +85,19 @@ class ResidualJacobian:
                indices.data_ptr(), data.data_ptr(), L.stream_ptr())
         return DeviceCSR(indptr, indices, data, (self.mesh.n_nodes, self.mesh.n_nodes))
 
+    def evaluate_host(self, phi_host, flow: FlowParams, R_host, J_host) -> None:
+        """One evaluation on host buffers (pinned CPU tensors): copy phi in,
+        evaluate R and the Jacobian data on the P1 pattern, copy both back;
+        returns when R_host / J_host hold the result."""
+        t = L.torch()
+        if not hasattr(self, "_phi_in"):
+            self._phi_in = t.empty(self.mesh.n_nodes, dtype=t.float64, device="cuda")
+        self._phi_in.copy_(phi_host, non_blocking=True)
+        self.evaluate(self._phi_in, flow, jacobian=True, keep_state=False)
+        R_host.copy_(self.R, non_blocking=True)
+        J_host.copy_(self.data, non_blocking=True)
+        t.cuda.current_stream().synchronize()
+
     def newton_nnz(self) -> int:
         """nnz of the merged Jacobian (exact zeros dropped when Term 3 is
         active, like scipy's CSR addition)."""
@@ -89,3 +105,52 @@ class ResidualJacobian:
         L.call("up3d_jacobian_nnz", self.mesh.handle, self.data.data_ptr(), ctypes.byref(out),
                L.stream_ptr())
         return int(out.value)
+
+
+class HostPipeline:
+    """Residual + Jacobian evaluations on host buffers, double-buffered:
+    step k's phi upload and result download run on a copy stream while the
+    evaluation of the neighbouring step runs on the compute stream.  Every
+    step still copies its phi host -> device and its R and Jacobian data
+    device -> host; ``finish()`` returns when all requested results are in
+    their host buffers."""
+
+    def __init__(self, ev: ResidualJacobian):
+        t = L.require_cuda()
+        self.ev = ev
+        m = ev.mesh
+        self.compute = t.cuda.current_stream()
+        self.copy = t.cuda.Stream()
+        self.slots = []
+        for _ in range(2):
+            self.slots.append({
+                "phi": t.empty(m.n_nodes, dtype=t.float64, device="cuda"),
+                "R": t.empty(m.n_nodes, dtype=t.float64, device="cuda"),
+                "J": t.empty(m.nnz, dtype=t.float64, device="cuda"),
+                "free": t.cuda.Event(), "loaded": t.cuda.Event(), "done": t.cuda.Event(),
+            })
+            self.slots[-1]["free"].record(self.copy)
+        self.k = 0
+
+    def submit(self, phi_host, flow: FlowParams, R_host, J_host) -> None:
+        t = L.torch()
+        s = self.slots[self.k % 2]
+        self.k += 1
+        with t.cuda.stream(self.copy):
+            self.copy.wait_event(s["free"])
+            s["phi"].copy_(phi_host, non_blocking=True)
+            s["loaded"].record(self.copy)
+        self.compute.wait_event(s["loaded"])
+        with t.cuda.stream(self.compute):
+            self.ev.evaluate(s["phi"], flow, jacobian=True, keep_state=False, R_out=s["R"],
+                             data_out=s["J"])
+            s["done"].record(self.compute)
+        with t.cuda.stream(self.copy):
+            self.copy.wait_event(s["done"])
+            R_host.copy_(s["R"], non_blocking=True)
+            J_host.copy_(s["J"], non_blocking=True)
+            s["free"].record(self.copy)
+
+    def finish(self) -> None:
+        self.copy.synchronize()
+        self.compute.synchronize()
