@@ -224,9 +224,10 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from up3d_b200.replicas import max_over_ranks
+    from up3d_b200.replicas import world as world_env
+
+    rank, world, local = world_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -309,10 +310,7 @@ def run_ours(args):
         barrier()
         e2e_ms = e_start.elapsed_time(e_stop)
 
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
     e2e_value = dmesh.n_tets * n_e2e * world / (e2e_ms * 1e-3) / 1e6
 

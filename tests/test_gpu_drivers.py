@@ -30,3 +30,27 @@ def test_subsonic_picard_matches_reference(picard_golden):
     err = np.abs(cp - g["cp"]).max()
     assert err < 1e-8, f"converged Cp error {err:.2e}"
     assert np.abs(res["phi"] - g["phi"]).max() < 1e-8
+
+
+def test_transonic_newton_converges_on_reference_equations():
+    """Mach continuation 0.70 -> 0.85 on a 40x12x10 bump channel (bump 0.08):
+    the device Newton (exact Jacobian, GMRES + AMG, line search, frozen
+    finish) reaches |R_free| < 1e-10 with a supersonic pocket, and the
+    converged potential satisfies the reference's discrete equations (the
+    oracle residual at that potential)."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    mesh = bump_channel(40, 12, 10, amplitude=0.08, seed=0)
+    ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+    res = solve_newton_transonic(ws, 0.85, m_start=0.70, dm=0.05)
+    assert res["converged"], res["level_history"]
+    assert res["residual_history"][-1] < 1e-10
+    assert res["n_supersonic"] > 0
+    phi = res["phi"].cpu().numpy()
+    r = O.chain(O.PicardOperator(mesh.nodes, mesh.elements),
+                O.UpwindOperator(mesh.nodes, mesh.elements), phi, 0.85, jacobian=False)
+    free = np.setdiff1d(np.arange(mesh.n_nodes), mesh.dirichlet_nodes)
+    assert np.abs(r["R"][free]).max() < 2e-10
+    assert r["n_supersonic"] == res["n_supersonic"]
