@@ -30,8 +30,6 @@ namespace {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
 constexpr int RG_WARPS = 8;   // warps per block of the row gather
-constexpr int RG_MAXE = 64;   // incident elements per row staged in shared memory
-constexpr int WIDE_MAXE = 1024;
 
 #ifndef UP3D_ROW_MINB
 #define UP3D_ROW_MINB 8
@@ -49,9 +47,6 @@ __device__ __forceinline__ void gB_of(const double g[3], const double* __restric
 #pragma unroll
     for (int j = 0; j < 4; ++j) gB[j] = g[0] * b[3 * j] + g[1] * b[3 * j + 1] + g[2] * b[3 * j + 2];
 }
-
-// Index of the off-diagonal pair (a, b), a < b, in (01,02,03,12,13,23).
-__host__ __device__ __forceinline__ int off_index(int a, int b) { return a * (7 - a) / 2 - 1 + b - a; }
 
 // Local matrix of one element (kernels/jacobian.py:406-433):
 //   J_ij = w1 (B_i . B_j)  [+ w2 gB_i gB_j when w2 != 0]
@@ -108,61 +103,58 @@ __device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, 
 
 // ------------------------------------------------------------ row gather
 
-template <int MAXE>
-constexpr size_t row_smem_per_warp() {
-    // entries (uint32) then the plan (uint16, 3 per entry), 16-B aligned
-    return ((sizeof(uint32_t) * MAXE + sizeof(uint16_t) * 3 * MAXE + 15) / 16) * 16;
-}
-
 // Jacobian rows (and, when R != null, the residual) from the local
-// matrices: R_n = sum_e R_e,i ; J_nn = sum_e J_e,ii ; J_nm = sum over the
-// plan's contributors (e, i, j) of J_e,ij.
-template <int MAXE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 1 ? 1 : UP3D_ROW_MINB)
+// matrices, one warp per row n:
+//   R_n  = sum_e R_e,i        J_nn = sum_e J_e,ii      (lanes = incident
+//   entries, butterfly sum)
+//   J_nm = sum_e J_e,ij  for the upper slots m > n (lanes = slots, the plan's
+//   contributors in ascending element order), written to (n, m) and, since
+//   the element matrices are symmetric and row m lists the same elements in
+//   the same order, to its transposed slot (m, n) as well.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
                  const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
-                 const uint16_t* __restrict__ plan, const int32_t* __restrict__ diag, const double* __restrict__ loc,
-                 double* __restrict__ R, double* __restrict__ J, bool wide_pass) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t* sent = reinterpret_cast<uint32_t*>(smem_raw + (size_t)w * row_smem_per_warp<MAXE>());
-    uint16_t* splan = reinterpret_cast<uint16_t*>(sent + MAXE);
-    for (int64_t n = (int64_t)blockIdx.x * WARPS + w; n < N; n += (int64_t)gridDim.x * WARPS) {
+                 const uint32_t* __restrict__ plan, const int32_t* __restrict__ diag,
+                 const int32_t* __restrict__ zt, const double* __restrict__ loc, double* __restrict__ R,
+                 double* __restrict__ J) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < N; n += n_warps) {
         const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
-        if (wide_pass ? deg <= RG_MAXE : deg > RG_MAXE) continue;
-        const int32_t rb = indptr[n], L = indptr[n + 1] - rb;
-        const int32_t pbase = plan_off[rb];
-        const int32_t pcnt = plan_off[rb + L] - pbase;
-        for (int t = lane; t < pcnt; t += 32) splan[t] = plan[pbase + t];
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
         double r = 0.0, d = 0.0;
         for (int k = lane; k < deg; k += 32) {
             const uint32_t x = ent[eb + k];
-            sent[k] = x;
             const double2 v = reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
             r += v.x;
             d += v.y;
         }
-        d = warp_sum(d);
-        if (R) r = warp_sum(r);
-        __syncwarp();
-        const int32_t ds = diag[n];
-        for (int s = lane; s < L; s += 32) {
-            double v = d;
-            if (s != ds) {
-                v = 0.0;
-                const int32_t p1 = plan_off[rb + s + 1] - pbase;
-                for (int32_t p = plan_off[rb + s] - pbase; p < p1; ++p) {
-                    const uint32_t c = splan[p];
-                    const uint32_t x = sent[c >> 2];
-                    const int i = x & 3, j = c & 3;
-                    const int q = i < j ? off_index(i, j) : off_index(j, i);
-                    v += loc[(size_t)LOC_STRIDE * (x >> 2) + 8 + q];
-                }
+        for (int s = ds + 1 + lane; s < L; s += 32) {
+            int32_t p = plan_off[rb + s];
+            const int32_t p1 = plan_off[rb + s + 1];
+            double v = 0.0;
+            for (; p + 1 < p1; p += 2) {
+                const uint32_t c0 = plan[p], c1 = plan[p + 1];
+                const double a0 = loc[(size_t)LOC_STRIDE * (c0 >> 3) + 8 + (c0 & 7)];
+                const double a1 = loc[(size_t)LOC_STRIDE * (c1 >> 3) + 8 + (c1 & 7)];
+                v += a0;
+                v += a1;
+            }
+            if (p < p1) {
+                const uint32_t c0 = plan[p];
+                v += loc[(size_t)LOC_STRIDE * (c0 >> 3) + 8 + (c0 & 7)];
             }
             J[rb + s] = v;
+            J[zt[rb + s]] = v;
         }
-        if (R && lane == 0) R[n] = r;
-        __syncwarp();
+        d = warp_sum(d);
+        if (R) r = warp_sum(r);
+        if (lane == 0) {
+            if (deg > 0) J[rb + ds] = d;  // a node of no element has an empty row
+            if (R) R[n] = r;
+        }
     }
 }
 
@@ -502,24 +494,11 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 
 // Jacobian (+ residual) rows from m->loc.
 void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
-    {
-        const size_t sm = RG_WARPS * row_smem_per_warp<RG_MAXE>();
-        const unsigned grid = grid_for(m->N, RG_WARPS, (int64_t)148 * 64);
-        k_row_gather<RG_MAXE, RG_WARPS><<<grid, RG_WARPS * 32, sm, s>>>(
-            m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(), m->plan.get(), m->diag.get(),
-            m->loc.get(), R, J, false);
-        UP3D_CHECK_LAUNCH();
-    }
-    if (m->max_deg > RG_MAXE) {
-        UP3D_REQUIRE(m->max_deg <= WIDE_MAXE, UP3D_ERR_VALUE,
-                     "a node is shared by more than 1024 elements; unsupported by the row gather");
-        const size_t sm = row_smem_per_warp<WIDE_MAXE>();
-        auto kern = k_row_gather<WIDE_MAXE, 1>;
-        UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        kern<<<148 * 4, 32, sm, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(),
-                                     m->plan.get(), m->diag.get(), m->loc.get(), R, J, true);
-        UP3D_CHECK_LAUNCH();
-    }
+    const unsigned grid = grid_for(32 * m->N, RG_WARPS * 32, (int64_t)148 * 64);
+    k_row_gather<RG_WARPS><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
+                                                          m->plan_off.get(), m->plan.get(), m->diag.get(),
+                                                          m->zt.get(), m->loc.get(), R, J);
+    UP3D_CHECK_LAUNCH();
 }
 
 // Residual rows from m->res.
@@ -773,7 +752,7 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         prof_begin(PROF_ROW, s);
         if (jac) launch_row_gather(m, R, data, s);
         else launch_row_residual(m, R, s);
-        prof_end(PROF_ROW, s, jac && m->max_deg > RG_MAXE ? 2 : 1);
+        prof_end(PROF_ROW, s, 1);
         if (jac) {
             // the element sweep counted the active elements: Term 3 is
             // built only when there are any (flags already written)

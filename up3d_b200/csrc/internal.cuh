@@ -124,8 +124,9 @@ struct up3d_mesh {
     up3d::DBuf<int32_t> ent_off;  // (N+1) node -> incident entries
     up3d::DBuf<uint32_t> ent;     // (4E) (e << 2) | local i, ascending e per node
     up3d::DBuf<int32_t> plan_off; // (nnz+1) contributor list offset per nnz
-    up3d::DBuf<uint16_t> plan;    // (12E) off-diagonal contributors (k << 2) | j
+    up3d::DBuf<uint32_t> plan;    // (6E) upper-slot contributors (e << 3) | pair index
     up3d::DBuf<int32_t> diag;     // (N) slot of the diagonal within its row
+    up3d::DBuf<int32_t> zt;       // (nnz) slot of the transposed entry
 
     // workspaces (device)
     up3d::DBuf<double> loc;            // (E, LOC_STRIDE) local matrices + residual

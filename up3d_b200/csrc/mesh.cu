@@ -133,14 +133,19 @@ __device__ __forceinline__ int32_t lower_bound(const int32_t* __restrict__ a, in
     return lo;
 }
 
-// Row-gather plan, pass 1 (count) / pass 2 (fill): for row n, the
-// off-diagonal contributors of every slot in (entry k, local column j)
-// order, and the slot of the diagonal.
+// Index of the off-diagonal pair (a, b), a < b, in (01,02,03,12,13,23).
+__device__ __forceinline__ int pair_index(int a, int b) { return a * (7 - a) / 2 - 1 + b - a; }
+
+// Row-gather plan, pass 1 (count) / pass 2 (fill).  The P1 element
+// matrices are symmetric, so only upper-triangle slots (col > row) get a
+// contributor list: for slot (n, m), the elements holding edge (n, m) in
+// ascending element order, each as (e << 3) | (pair index of its local
+// (i, j)).  Also the slot of the diagonal.
 template <bool FILL>
 __global__ void k_plan(int64_t N, const int4* __restrict__ conn, const int32_t* __restrict__ ent_off,
                        const uint32_t* __restrict__ ent, const int32_t* __restrict__ indptr,
                        const int32_t* __restrict__ indices, int32_t* __restrict__ cursor,
-                       const int32_t* __restrict__ plan_off, uint16_t* __restrict__ plan,
+                       const int32_t* __restrict__ plan_off, uint32_t* __restrict__ plan,
                        int32_t* __restrict__ diag) {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N;
          n += (int64_t)gridDim.x * blockDim.x) {
@@ -155,15 +160,29 @@ __global__ void k_plan(int64_t N, const int4* __restrict__ conn, const int32_t* 
             int4 c = conn[e];
             int nd[4] = {c.x, c.y, c.z, c.w};
             for (int j = 0; j < 4; ++j) {
-                if (j == i) continue;
+                if (j == i || nd[j] <= n) continue;
                 int32_t s = lower_bound(cols, L, nd[j]);
                 if (FILL) {
                     int32_t pos = plan_off[rb + s] + cursor[rb + s]++;
-                    plan[pos] = (uint16_t)((k << 2) | j);
+                    const int q = i < j ? pair_index(i, j) : pair_index(j, i);
+                    plan[pos] = (uint32_t)((e << 3) | q);
                 } else {
                     cursor[rb + s]++;
                 }
             }
+        }
+    }
+}
+
+// Transposed slot of every non-zero: for (n, m) at z, the position of (m, n).
+__global__ void k_transpose_slots(int64_t N, const int32_t* __restrict__ indptr,
+                                  const int32_t* __restrict__ indices, int32_t* __restrict__ zt) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        for (int32_t z = indptr[n]; z < indptr[n + 1]; ++z) {
+            const int32_t m = indices[z];
+            const int32_t mb = indptr[m], mL = indptr[m + 1] - mb;
+            zt[z] = mb + lower_bound(indices + mb, mL, (int32_t)n);
         }
     }
 }
@@ -385,8 +404,11 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
     }
     // row-gather plan
     m->plan_off.alloc(m->nnz + 1);
-    m->plan.alloc(12 * E);
+    m->plan.alloc(6 * E);
     m->diag.alloc(N);
+    m->zt.alloc(m->nnz);
+    k_transpose_slots<<<grid_for(N, 128), 128, 0, s>>>(N, m->indptr.get(), m->indices.get(), m->zt.get());
+    UP3D_CHECK_LAUNCH();
     {
         DBuf<int32_t> cursor;
         cursor.alloc(m->nnz + 1);

@@ -282,6 +282,7 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
             "residual_history": residual_history, "eta_history": eta_history,
             "newton_orders": newton_orders, "n_gmres_total": n_gmres_total,
             "n_gmres_stalled": n_gmres_stalled, "froze": frozen is not None,
+            "frozen_state": frozen,
             "n_freeze_refresh": n_freeze_refresh, "residual_unfrozen": residual_unfrozen,
             "n_freeze_reverts": n_freeze_reverts, "nu_max": mon["nu_max"],
             "n_supersonic": mon["n_supersonic"], "n_limited": mon["n_limited"],
