@@ -318,6 +318,27 @@ int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double
                double rtol, double atol, int restart, int maxiter, up3d_precond* M,
                int64_t* inner, double* resid, int* info, up3d_stream stream);
 
+/* ------------------------------------------------ allocation-free solve */
+
+/* CG with point-Jacobi preconditioning that allocates no device or pinned
+ * memory: for callers that cannot let this library call cudaMalloc /
+ * cudaFree (a process whose device memory belongs to another allocator or a
+ * fixed pre-reserved pool, or a time-critical loop that cannot take the
+ * implicit synchronisation of those calls).  Working vectors live in one
+ * static device array of UP3D_NOALLOC_MAX_ROWS rows (about 10.5 MB, resident
+ * on every GPU that loads the library until exit).  Same arguments and
+ * result as up3d_cg with an up3d_precond_jacobi preconditioner.
+ * UP3D_ERR_VALUE for more rows than the limit.  The first call on a device
+ * resolves the array's device address (cudaGetSymbolAddress) with that
+ * device current; make it before capturing any stream.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Synchronous.  This entry point has no counterpart in the
+ * reference. */
+#define UP3D_NOALLOC_MAX_ROWS (1 << 18)
+int up3d_cg_jacobi_noalloc(const up3d_csr* A, const double* b, double* x, double rtol,
+                           double atol, int maxiter, int64_t* iters, double* resid,
+                           int* info, up3d_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

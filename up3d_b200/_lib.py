@@ -97,7 +97,11 @@ SIGNATURES = {
                        ctypes.POINTER(_int), _p]),
     "up3d_gmres": (_int, [_p, _p, _p, _p, _d, _d, _int, _int, _p, ctypes.POINTER(_i64),
                           ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
+    "up3d_cg_jacobi_noalloc": (_int, [_p, _p, _p, _d, _d, _int, ctypes.POINTER(_i64),
+                                      ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
 }
+
+NOALLOC_MAX_ROWS = 1 << 18  # UP3D_NOALLOC_MAX_ROWS
 
 
 class CSR(ctypes.Structure):

@@ -1,0 +1,215 @@
+// CG with point-Jacobi preconditioning that allocates nothing.
+//
+// For callers that cannot let this library call cudaMalloc/cudaFree: a
+// process whose device memory is already handed to another allocator (a
+// framework's caching allocator, a fixed pre-reserved pool), where a
+// library-side cudaMalloc would fail or fragment that pool, or a
+// time-critical host loop that cannot afford the implicit device
+// synchronisation of cudaMalloc/cudaFree.  All working vectors and the
+// reduction partials live in one file-scope device array; the caller passes
+// only its inputs and outputs.  The result equals up3d_cg with an
+// up3d_precond_jacobi preconditioner (same kernels, same reduction order).
+//
+// The array holds UP3D_NOALLOC_MAX_ROWS rows (see up3d.h) and stays
+// resident on every GPU that loads the library until the process exits.
+// All calls share it: calls that overlap on the GPU (other streams or
+// threads) race on it and must be serialised by the caller.
+
+#include <cmath>
+#include <mutex>
+
+#include "internal.cuh"
+
+namespace up3d {
+
+template <class T>
+void launch_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const T* x, T* y,
+                 const uint8_t* dir, cudaStream_t s);
+
+namespace {
+
+constexpr int NA_RB = 256;     // reduction block (as in krylov.cu)
+constexpr int NA_RGRID = 592;  // fixed partial count (as in krylov.cu)
+constexpr int64_t NA_ROWS = UP3D_NOALLOC_MAX_ROWS;
+// r, z, p, q, D^-1, then the reduction partials and the scalars
+constexpr int64_t NA_DOUBLES = 5 * NA_ROWS + NA_RGRID + 8;
+
+static __device__ __align__(256) double g_scratch[NA_DOUBLES];
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double na_block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    __syncthreads();
+    return t;
+}
+
+__global__ void __launch_bounds__(NA_RB) k_na_dot(const double* __restrict__ x, const double* __restrict__ y,
+                                                  int64_t n, double* __restrict__ partial) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    GRID_STRIDE(i, n) acc += x[i] * y[i];
+    double t = na_block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+__global__ void k_na_finish(const double* __restrict__ partial, int nb, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[b];
+    double t = na_block_sum(acc, sh);
+    if (threadIdx.x == 0) *out = t;
+}
+
+__global__ void k_na_diag(int64_t n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                          const double* __restrict__ data, const uint8_t* __restrict__ dir,
+                          double* __restrict__ dinv) {
+    GRID_STRIDE(r, n) {
+        double d = 0.0;
+        for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k)
+            if (indices[k] == r) d = data[k];
+        if (dir && dir[r]) d = 1.0;
+        dinv[r] = d != 0.0 ? 1.0 / d : 1.0;
+    }
+}
+
+__global__ void k_na_sub(const double* __restrict__ b, const double* __restrict__ ax, double* __restrict__ r,
+                         int64_t n) {
+    GRID_STRIDE(i, n) r[i] = b[i] - ax[i];
+}
+
+__global__ void k_na_mul(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
+                         int64_t n) {
+    GRID_STRIDE(i, n) out[i] = a[i] * b[i];
+}
+
+__global__ void k_na_update(const double* __restrict__ sc, double* __restrict__ x, double* __restrict__ r,
+                            const double* __restrict__ p, const double* __restrict__ q, int64_t n) {
+    const double alpha = sc[0] / sc[1];
+    GRID_STRIDE(i, n) {
+        x[i] += alpha * p[i];
+        r[i] -= alpha * q[i];
+    }
+}
+
+__global__ void k_na_dir(const double* __restrict__ sc, const double* __restrict__ z, double* __restrict__ p,
+                         int64_t n) {
+    const double beta = sc[2] / sc[0];
+    GRID_STRIDE(i, n) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void k_na_copy_scalar(const double* __restrict__ src, double* __restrict__ dst) { *dst = *src; }
+
+// Device address of g_scratch per device, resolved once per device with
+// that device current (the host-side name is only a stand-in).
+std::mutex g_na_mu;
+double* g_na_ptr[64] = {nullptr};
+
+double* scratch_for_current_device() {
+    int dev = 0;
+    UP3D_CUDA(cudaGetDevice(&dev));
+    UP3D_REQUIRE(dev >= 0 && dev < 64, UP3D_ERR_RUNTIME, "up3d_cg_jacobi_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_ptr[dev]) {
+        void* p = nullptr;
+        UP3D_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+        g_na_ptr[dev] = static_cast<double*>(p);
+    }
+    return g_na_ptr[dev];
+}
+
+}  // namespace
+}  // namespace up3d
+
+using namespace up3d;
+
+extern "C" int up3d_cg_jacobi_noalloc(const up3d_csr* A, const double* b, double* x, double rtol, double atol,
+                                      int maxiter, int64_t* iters, double* resid, int* info,
+                                      up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(A && A->indptr && A->indices && A->data && b && x && A->n >= 0 && maxiter >= 0,
+                     UP3D_ERR_ARGUMENT, "up3d_cg_jacobi_noalloc: bad argument");
+        UP3D_REQUIRE(A->n <= NA_ROWS, UP3D_ERR_VALUE,
+                     "up3d_cg_jacobi_noalloc: " + std::to_string(A->n) + " rows exceed the static limit of " +
+                         std::to_string(NA_ROWS) + " (UP3D_NOALLOC_MAX_ROWS); use up3d_cg");
+        cudaStream_t s = S(stream);
+        const int64_t n = A->n;
+        double* base = scratch_for_current_device();
+        double* r = base;
+        double* z = base + NA_ROWS;
+        double* p = base + 2 * NA_ROWS;
+        double* q = base + 3 * NA_ROWS;
+        double* dinv = base + 4 * NA_ROWS;
+        double* partial = base + 5 * NA_ROWS;
+        double* sc = partial + NA_RGRID;  // rz, pq, rz_new, norm
+        // previous calls leave their values behind: start the scalars at 0
+        UP3D_CUDA(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
+        auto dot = [&](const double* u, const double* v, double* out) {
+            k_na_dot<<<NA_RGRID, NA_RB, 0, s>>>(u, v, n, partial);
+            UP3D_CHECK_LAUNCH();
+            k_na_finish<<<1, 1024, 0, s>>>(partial, NA_RGRID, out);
+            UP3D_CHECK_LAUNCH();
+        };
+        auto nrm = [&](const double* u) {
+            dot(u, u, sc + 3);
+            double h = 0.0;
+            UP3D_CUDA(cudaMemcpyAsync(&h, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaStreamSynchronize(s));
+            return std::sqrt(h);
+        };
+        int64_t it = 0;
+        double rn = 0.0;
+        if (n > 0) {
+            k_na_diag<<<grid_for(n, 256), 256, 0, s>>>(n, A->indptr, A->indices, A->data, A->dirichlet, dinv);
+            UP3D_CHECK_LAUNCH();
+            const double bnrm = nrm(b);
+            const double tol = std::max(atol, rtol * bnrm);
+            launch_spmv<double>(n, A->indptr, A->indices, A->data, x, q, A->dirichlet, s);
+            k_na_sub<<<grid_for(n, 256), 256, 0, s>>>(b, q, r, n);
+            UP3D_CHECK_LAUNCH();
+            rn = nrm(r);
+            if (bnrm == 0.0) {
+                UP3D_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+                rn = 0.0;
+            }
+            if (rn > tol) {
+                k_na_mul<<<grid_for(n, 256), 256, 0, s>>>(dinv, r, z, n);
+                UP3D_CHECK_LAUNCH();
+                UP3D_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+                dot(r, z, sc + 0);
+                for (it = 1; it <= maxiter; ++it) {
+                    launch_spmv<double>(n, A->indptr, A->indices, A->data, p, q, A->dirichlet, s);
+                    dot(p, q, sc + 1);
+                    k_na_update<<<grid_for(n, 256), 256, 0, s>>>(sc, x, r, p, q, n);
+                    UP3D_CHECK_LAUNCH();
+                    rn = nrm(r);
+                    if (rn <= tol || !std::isfinite(rn)) break;
+                    k_na_mul<<<grid_for(n, 256), 256, 0, s>>>(dinv, r, z, n);
+                    UP3D_CHECK_LAUNCH();
+                    dot(r, z, sc + 2);
+                    k_na_dir<<<grid_for(n, 256), 256, 0, s>>>(sc, z, p, n);
+                    UP3D_CHECK_LAUNCH();
+                    k_na_copy_scalar<<<1, 1, 0, s>>>(sc + 2, sc + 0);
+                    UP3D_CHECK_LAUNCH();
+                }
+                if (it > maxiter) it = maxiter;
+            }
+            if (iters) *iters = it;
+            if (resid) *resid = rn;
+            if (info) *info = rn <= tol ? 0 : maxiter;
+        } else {
+            if (iters) *iters = 0;
+            if (resid) *resid = 0.0;
+            if (info) *info = 0;
+        }
+    });
+}
