@@ -31,6 +31,8 @@ namespace {
 
 constexpr int RG_WARPS = 8;   // warps per block of the row gather
 
+// Minimum resident blocks per SM (launch bounds), tuned at 3.6M tets on
+// B200: the Jacobian sweep runs fastest at 2 (128 registers, no spills).
 #ifndef UP3D_ROW_MINB
 #define UP3D_ROW_MINB 8
 #endif
@@ -38,7 +40,7 @@ constexpr int RG_WARPS = 8;   // warps per block of the row gather
 #define UP3D_ELEM_MINB 3
 #endif
 #ifndef UP3D_ELEM_MINB_JAC
-#define UP3D_ELEM_MINB_JAC 3
+#define UP3D_ELEM_MINB_JAC 2
 #endif
 
 // ------------------------------------------------------------ element math
@@ -104,54 +106,76 @@ __device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, 
 // ------------------------------------------------------------ row gather
 
 // Jacobian rows (and, when R != null, the residual) from the local
-// matrices, one warp per row n:
-//   R_n  = sum_e R_e,i        J_nn = sum_e J_e,ii      (lanes = incident
-//   entries, butterfly sum)
-//   J_nm = sum_e J_e,ij  for the upper slots m > n (lanes = slots, the plan's
-//   contributors in ascending element order), written to (n, m) and, since
-//   the element matrices are symmetric and row m lists the same elements in
-//   the same order, to its transposed slot (m, n) as well.
-template <int WARPS>
+// matrices, LPR lanes per row (32 / LPR rows per warp in flight):
+//   R_n  = sum_e R_e,i        J_nn = sum_e J_e,ii      (lanes stride the
+//   incident entries, then a butterfly over the row's lanes)
+//   J_nm = sum_e J_e,ij  for the upper slots m > n (lanes stride the slots;
+//   each slot sums its plan's contributors in ascending element order) and
+//   is written to (n, m) and, the element matrices being symmetric and row m
+//   listing the same elements in the same order, to its transposed slot.
+#ifndef UP3D_ROW_LPR
+#define UP3D_ROW_LPR 8
+#endif
+template <int WARPS, int LPR>
 __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
                  const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
                  const uint32_t* __restrict__ plan, const int32_t* __restrict__ diag,
                  const int32_t* __restrict__ zt, const double* __restrict__ loc, double* __restrict__ R,
                  double* __restrict__ J) {
-    const int lane = threadIdx.x & 31;
+    static_assert(LPR >= 1 && LPR <= 32 && (LPR & (LPR - 1)) == 0, "LPR: power of two <= 32");
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t n = warp; n < N; n += n_warps) {
-        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
-        const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
+    // warp-uniform trip count: every lane reaches the shuffles
+    for (int64_t base = warp * RPW; base < N; base += n_warps * RPW) {
+        const int64_t n = base + lane / LPR;
+        const bool valid = n < N;
+        int32_t eb = 0, deg = 0, rb = 0, L = 0, ds = -1;
+        if (valid) {
+            eb = ent_off[n];
+            deg = ent_off[n + 1] - eb;
+            rb = indptr[n];
+            L = indptr[n + 1] - rb;
+            ds = diag[n];
+        }
         double r = 0.0, d = 0.0;
-        for (int k = lane; k < deg; k += 32) {
+        for (int k = sub; k < deg; k += LPR) {
             const uint32_t x = ent[eb + k];
             const double2 v = reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
             r += v.x;
             d += v.y;
         }
-        for (int s = ds + 1 + lane; s < L; s += 32) {
+        for (int s = ds + 1 + sub; s < L; s += LPR) {
             int32_t p = plan_off[rb + s];
             const int32_t p1 = plan_off[rb + s + 1];
             double v = 0.0;
-            for (; p + 1 < p1; p += 2) {
-                const uint32_t c0 = plan[p], c1 = plan[p + 1];
+            for (; p + 3 < p1; p += 4) {
+                const uint32_t c0 = plan[p], c1 = plan[p + 1], c2 = plan[p + 2], c3 = plan[p + 3];
                 const double a0 = loc[(size_t)LOC_STRIDE * (c0 >> 3) + 8 + (c0 & 7)];
                 const double a1 = loc[(size_t)LOC_STRIDE * (c1 >> 3) + 8 + (c1 & 7)];
+                const double a2 = loc[(size_t)LOC_STRIDE * (c2 >> 3) + 8 + (c2 & 7)];
+                const double a3 = loc[(size_t)LOC_STRIDE * (c3 >> 3) + 8 + (c3 & 7)];
                 v += a0;
                 v += a1;
+                v += a2;
+                v += a3;
             }
-            if (p < p1) {
+            for (; p < p1; ++p) {
                 const uint32_t c0 = plan[p];
                 v += loc[(size_t)LOC_STRIDE * (c0 >> 3) + 8 + (c0 & 7)];
             }
             J[rb + s] = v;
             J[zt[rb + s]] = v;
         }
-        d = warp_sum(d);
-        if (R) r = warp_sum(r);
-        if (lane == 0) {
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (R) {
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        }
+        if (valid && sub == 0) {
             if (deg > 0) J[rb + ds] = d;  // a node of no element has an empty row
             if (R) R[n] = r;
         }
@@ -278,7 +302,7 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 template <bool FROZEN, bool JAC>
 __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
-                 const int4* __restrict__ fn, const double4* __restrict__ cen, const double4* __restrict__ X,
+                 const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F, double u2, const int64_t* __restrict__ up_fz,
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
@@ -300,7 +324,7 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
         double rho_e, drho_e;
         rho_drho(q2l, F, rho_e, drho_e);
 
-        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, cen, X, conn, e, E, g);
+        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, disp, X, conn, e, E, g);
         // upstream state, and its Term-3 factors grad_u . B_u,k
         double q2lu = q2l, rho_u = rho_e;
         bool lim_u = lim_e;
@@ -494,8 +518,9 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 
 // Jacobian (+ residual) rows from m->loc.
 void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
-    const unsigned grid = grid_for(32 * m->N, RG_WARPS * 32, (int64_t)148 * 64);
-    k_row_gather<RG_WARPS><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
+    constexpr int rows_per_block = RG_WARPS * 32 / UP3D_ROW_LPR;
+    const unsigned grid = grid_for(m->N, rows_per_block, (int64_t)148 * 64);
+    k_row_gather<RG_WARPS, UP3D_ROW_LPR><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
                                                           m->plan_off.get(), m->plan.get(), m->diag.get(),
                                                           m->zt.get(), m->loc.get(), R, J);
     UP3D_CHECK_LAUNCH();
@@ -733,7 +758,7 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
         const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
 #define FUSED_ARGS                                                                                                \
-    m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->cen.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
+    m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
         m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo
         const bool jac = data != nullptr;
         prof_begin(PROF_ELEM, s);

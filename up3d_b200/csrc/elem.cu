@@ -93,12 +93,12 @@ __global__ void k_field(const double* __restrict__ q2, int64_t n, Flow F, double
 }
 
 template <class IDX>
-__global__ void k_walk(const int4* __restrict__ fn, const double4* __restrict__ cen,
+__global__ void k_walk(const int4* __restrict__ fn, const double* __restrict__ disp,
                        const double4* __restrict__ X, const int4* __restrict__ conn,
                        const double* __restrict__ grad, int64_t E, IDX* __restrict__ out) {
     GRID_STRIDE(e, E) {
         double g[3] = {grad[3 * e], grad[3 * e + 1], grad[3 * e + 2]};
-        out[e] = (IDX)upstream_walk(fn, cen, X, conn, e, E, g);
+        out[e] = (IDX)upstream_walk(fn, disp, X, conn, e, E, g);
     }
 }
 
@@ -215,7 +215,7 @@ void launch_velocities(const up3d_mesh* m, const double* phi, double* grad, doub
 }
 
 void launch_walk32(const up3d_mesh* m, const double* grad, int32_t* up, cudaStream_t s) {
-    k_walk<int32_t><<<grid_for(m->E, 256), 256, 0, s>>>(m->fnbr.get(), m->cen.get(), m->nodes4.get(),
+    k_walk<int32_t><<<grid_for(m->E, 256), 256, 0, s>>>(m->fnbr.get(), m->disp.get(), m->nodes4.get(),
                                                        m->conn.get(), grad, m->E, up);
     UP3D_CHECK_LAUNCH();
 }
@@ -273,7 +273,7 @@ FIELD_ENTRY(up3d_pressure_coefficient, 4)
 int up3d_upwind_walk(const up3d_mesh* m, const double* grad, int64_t* upstream, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(m && grad && upstream, UP3D_ERR_ARGUMENT, "up3d_upwind_walk: null argument");
-        k_walk<int64_t><<<grid_for(m->E, 256), 256, 0, S(stream)>>>(m->fnbr.get(), m->cen.get(), m->nodes4.get(),
+        k_walk<int64_t><<<grid_for(m->E, 256), 256, 0, S(stream)>>>(m->fnbr.get(), m->disp.get(), m->nodes4.get(),
                                                                    m->conn.get(), grad, m->E, upstream);
         UP3D_CHECK_LAUNCH();
     });

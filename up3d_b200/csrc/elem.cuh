@@ -40,10 +40,12 @@ __device__ __forceinline__ void elem_grad_B(const int4* __restrict__ conn, const
 // upstream_elements (kernels/upwind.py:69-125): hop to the face neighbour
 // with the most negative centroid displacement along grad until the reach
 // covers 0.8 of the element's streamwise extent, at most 4 hops; u(e) = e
-// when nothing is upstream.  IEEE-rounded dot products so ties resolve as
-// in the CPU restatement.  Neighbour entries outside [0, E) count as
-// boundary faces.
-__device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, const double4* __restrict__ cen,
+// when nothing is upstream.  The displacements cen(nbr) - cen(cur) come
+// precomputed per element and face (IEEE-rounded like every other walk
+// operation), so a hop is one dependent load of (fn, disp)[cur] instead of
+// fn[cur] followed by four centroid gathers.  Neighbour entries outside
+// [0, E) count as boundary faces.
+__device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, const double* __restrict__ disp,
                                                  const double4* __restrict__ X, const int4* __restrict__ conn,
                                                  int64_t e, int64_t E, const double g[3]) {
     const double gx = g[0], gy = g[1], gz = g[2];
@@ -60,28 +62,24 @@ __device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, co
     const double target = rmul(0.8, rsub(pmax, pmin));
     int64_t cur = e;
     double reach = 0.0;
-    double4 cc = cen[e];
     for (int hops = 0; hops < 4 && reach < target; ++hops) {
-        int4 f = fn[cur];
-        int nb[4] = {f.x, f.y, f.z, f.w};
+        const int4 f = fn[cur];
+        const double2* dp = reinterpret_cast<const double2*>(disp + 12 * cur);
+        const double2 a0 = dp[0], a1 = dp[1], a2 = dp[2], a3 = dp[3], a4 = dp[4], a5 = dp[5];
+        const int nb[4] = {f.x, f.y, f.z, f.w};
+        const double d[4] = {dot3r(a0.x, a0.y, a1.x, gx, gy, gz), dot3r(a1.y, a2.x, a2.y, gx, gy, gz),
+                             dot3r(a3.x, a3.y, a4.x, gx, gy, gz), dot3r(a4.y, a5.x, a5.y, gx, gy, gz)};
         int64_t best = -1;
         double best_disp = 0.0;
-        double4 bestc = cc;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (nb[k] >= 0 && nb[k] < E) {
-                double4 cn = cen[nb[k]];
-                double d = dot3r(rsub(cn.x, cc.x), rsub(cn.y, cc.y), rsub(cn.z, cc.z), gx, gy, gz);
-                if (d < best_disp) {
-                    best_disp = d;
-                    best = nb[k];
-                    bestc = cn;
-                }
+            if (nb[k] >= 0 && nb[k] < E && d[k] < best_disp) {
+                best_disp = d[k];
+                best = nb[k];
             }
         }
         if (best < 0) break;
         cur = best;
-        cc = bestc;
         reach = radd(reach, -best_disp);
     }
     return cur;

@@ -117,6 +117,7 @@ struct up3d_mesh {
     up3d::DBuf<double> V;        // (E)
     up3d::DBuf<int4> fnbr;       // (E) face neighbours (-1 = boundary)
     up3d::DBuf<double4> cen;     // (E) centroids
+    up3d::DBuf<double> disp;     // (E, 12) cen(face neighbour k) - cen(e), k = 0..3 (0 at boundary faces)
 
     // pattern + row-gather maps (device)
     up3d::DBuf<int32_t> indptr;   // (N+1)

@@ -216,6 +216,36 @@ __global__ void k_face_neighbors(const int4* __restrict__ conn, int64_t E,
     }
 }
 
+// Walk displacements: for every element and face k, cen(fn[k]) - cen(e)
+// (IEEE-rounded), zero at boundary faces and out-of-range entries.
+__global__ void k_face_disp(const int4* __restrict__ fn, const double4* __restrict__ cen, int64_t E,
+                            double* __restrict__ disp) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int4 f = fn[e];
+        const int nb[4] = {f.x, f.y, f.z, f.w};
+        const double4 c = cen[e];
+        for (int k = 0; k < 4; ++k) {
+            double dx = 0.0, dy = 0.0, dz = 0.0;
+            if (nb[k] >= 0 && nb[k] < E) {
+                const double4 cn = cen[nb[k]];
+                dx = __dsub_rn(cn.x, c.x);
+                dy = __dsub_rn(cn.y, c.y);
+                dz = __dsub_rn(cn.z, c.z);
+            }
+            disp[12 * e + 3 * k] = dx;
+            disp[12 * e + 3 * k + 1] = dy;
+            disp[12 * e + 3 * k + 2] = dz;
+        }
+    }
+}
+
+void refresh_disp(up3d_mesh* m, cudaStream_t s) {
+    m->disp.alloc(12 * m->E);
+    k_face_disp<<<grid_for(m->E, 256), 256, 0, s>>>(m->fnbr.get(), m->cen.get(), m->E, m->disp.get());
+    UP3D_CHECK_LAUNCH();
+}
+
 __global__ void k_elem_to_csr(const int4* __restrict__ conn, int64_t E, const int32_t* __restrict__ indptr,
                               const int32_t* __restrict__ indices, int64_t* __restrict__ out) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
@@ -429,6 +459,7 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
     k_face_neighbors<<<grid_for(E, block), block, 0, s>>>(m->conn.get(), E, m->ent_off.get(), m->ent.get(),
                                                           m->fnbr.get());
     UP3D_CHECK_LAUNCH();
+    refresh_disp(m, s);
     UP3D_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -543,6 +574,7 @@ int up3d_mesh_set_face_neighbors(up3d_mesh* m, const int32_t* in, up3d_stream st
         UP3D_REQUIRE(m && in, UP3D_ERR_ARGUMENT, "up3d_mesh_set_face_neighbors: null argument");
         DeviceGuard g(m->device);
         UP3D_CUDA(cudaMemcpyAsync(m->fnbr.get(), in, sizeof(int4) * m->E, cudaMemcpyDeviceToDevice, S(stream)));
+        refresh_disp(m, S(stream));
     });
 }
 
