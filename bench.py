@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=100)
     p.add_argument("--cpu-states", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--pocket-steps", type=int, default=300)
     return p.parse_args()
 
 
@@ -186,18 +187,24 @@ class ClockSampler:
 # ---------------------------------------------------------------- GPU side
 
 def bytes_model(info, n_active=0):
-    """Algorithmic bytes of one launch of each kernel (every input read once,
-    every output written once, in the library's storage formats)."""
+    """Compulsory bytes per launch of the fused residual + Jacobian, Layout A
+    (the reference's stored geometry: B, V, int32 maps): every API input read
+    once and every output written once, intermediates free.  The element
+    sweep's share is its inputs (conn, B, V, face neighbours, centroids,
+    node coordinates, phi) and the upstream output; the row gather's share is
+    the scatter map (elem_to_csr as int32) and the outputs R and J.  Term 3
+    adds 16 COO triplets (8 + 4 + 4 bytes) per active element.
+
+    `design` counts what this library's layout moves on top: the walk's face
+    displacements and the local-matrix round trip between the two kernels."""
     E, N, Z = info["n_tets"], info["n_nodes"], info["nnz"]
-    elem = (E * (16 + 96 + 8 + 16 + 24)      # conn, B, V, face neighbours, centroid
-            + N * (24 + 8)                   # node coordinates, phi
-            + E * (14 * 8 + 4 + 1)           # local matrix + residual, upstream, Term-3 flag
-            + n_active * 64)                 # Term-3 vectors
-    row = (4 * E * 4 + 12 * E * 2            # node->element entries, row plan
-           + 4 * (Z + 1) + 4 * (N + 1) * 2 + 4 * N   # plan offsets, indptr, entry offsets, diag
-           + E * 14 * 8                      # local matrices + residual contributions
-           + 8 * N + 8 * Z)                  # R, J data
-    return {"elem_sweep": elem, "row_gather": row}
+    elem = E * (16 + 96 + 8 + 16 + 24 + 4) + N * (24 + 8)
+    row = E * 64 + N * 8 + Z * 8
+    t3 = n_active * 16 * 16
+    design_elem = (E * (16 + 96 + 8 + 16 + 96 + 4 + 14 * 8 + 1) + N * (24 + 8))
+    design_row = (E * (16 + 24 + 14 * 8) + Z * (4 + 4 + 8) + N * (4 * 3 + 8))
+    return {"elem_sweep": elem, "row_gather": row, "term3": t3, "fused": elem + row + t3,
+            "design": {"elem_sweep": design_elem, "row_gather": design_row}}
 
 
 def read_peaks():
@@ -310,6 +317,39 @@ def run_ours(args):
         barrier()
         e2e_ms = e_start.elapsed_time(e_stop)
 
+    # ---- supersonic-pocket states (upwind branches and Term 3 active), the
+    # same step timed the same way
+    pocket = None
+    if args.pocket_steps > 0:
+        from up3d_b200.mesh.kuhn import pocket_state
+        fams = ("accelerating", "shockpoint", "mixed")
+        p_phis = [torch.from_numpy(pocket_state(mesh, f)).cuda() for f in fams]
+        for k in range(3):
+            ev.evaluate(p_phis[k], flow, jacobian=True, keep_state=False)
+        p_mon = [None] * 3
+        for k in range(3):
+            ev.evaluate(p_phis[k], flow, jacobian=True, keep_state=False)
+            p_mon[k] = ev.read_monitors()
+        barrier()
+        torch.cuda.synchronize()
+        p_start = torch.cuda.Event(enable_timing=True)
+        p_stop = torch.cuda.Event(enable_timing=True)
+        p_start.record(stream)
+        for k in range(args.pocket_steps):
+            ev.evaluate(p_phis[k % 3], flow, jacobian=True, keep_state=False)
+        p_stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        p_ms = p_start.elapsed_time(p_stop)
+        p_ms = max_over_ranks([p_ms], device="cuda")[0]
+        pocket = {"families": list(fams), "steps": args.pocket_steps,
+                  "value": round(dmesh.n_tets * args.pocket_steps * world / (p_ms * 1e-3) / 1e6, 3),
+                  "unit": "Melem/s", "ms_per_step": round(p_ms / args.pocket_steps, 5),
+                  "n_supersonic": [int(m["n_supersonic"]) for m in p_mon],
+                  "n_term3_active": [int(m["n_term3_active"]) for m in p_mon],
+                  "n_term3_extra": [int(m["n_term3_extra"]) for m in p_mon],
+                  "nu_max": [float(m["nu_max"]) for m in p_mon]}
+
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
     e2e_value = dmesh.n_tets * n_e2e * world / (e2e_ms * 1e-3) / 1e6
@@ -321,7 +361,7 @@ def run_ours(args):
     achieved = bm[dom] / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = read_peaks()
     traffic = read_traffic(dom)
-    step_bytes = bm["elem_sweep"] + bm["row_gather"]
+    step_bytes = bm["fused"]
 
     if rank == 0:
         cpu = None
@@ -342,6 +382,7 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4),
                          "traffic": traffic,
                          "algorithmic_bytes": bm[dom],
+                         "design_bytes": bm["design"][dom],
                          "ms_per_launch": round(per_launch_ms, 5)},
             "step_roofline": {"algorithmic_bytes": step_bytes,
                               "achieved_gbs": round(step_bytes / (ms / args.steps * 1e-3) / 1e9, 1),
@@ -355,6 +396,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
+            "pocket_states": pocket,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
