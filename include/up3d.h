@@ -290,10 +290,20 @@ typedef struct {
     int64_t level_rows[16];
 } up3d_amg_info;
 
-/* Builds the hierarchy of A (setup on the host, cycle on the device). */
+/* Builds the hierarchy of A (solve/linear.py:61-81): aggregation and the
+ * level patterns on the host, every value (D^-1, omega, P, R A P, the
+ * coarsest inverse) on the device; the cycle runs on the device. */
 int up3d_amg_setup(const up3d_csr* A, const up3d_amg_options* options, up3d_precond** out,
                    up3d_stream stream);
 int up3d_amg_get_info(const up3d_precond* M, up3d_amg_info* info);
+/* Recomputes the values of a hierarchy for a new matrix with the same
+ * pattern and Dirichlet mask as its setup matrix: the reference rebuilds
+ * pyamg's hierarchy from scratch every amg_rebuild_every Newton steps
+ * (solve/newton.py:1016-1022); with every connection strong the aggregates
+ * depend on the pattern alone, so the result equals a fresh up3d_amg_setup
+ * bit for bit.  UP3D_ERR_VALUE when the pattern or mask differ.
+ * Synchronises the stream. */
+int up3d_amg_refresh(up3d_precond* M, const up3d_csr* A, up3d_stream stream);
 
 /* Point-Jacobi preconditioner z = D^{-1} r (constrained rows: identity). */
 int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream);

@@ -91,6 +91,41 @@ def test_amg_setup_is_deterministic(c1_system):
     assert torch.equal(z1, z2)
 
 
+@pytest.mark.parametrize("fp32", [False, True])
+def test_amg_refresh_equals_fresh_setup(c1_system, fp32):
+    """A hierarchy set up on one Picard matrix and refreshed with another of
+    the same pattern applies bit-identically to a fresh setup on the second
+    (the aggregates depend on the pattern only)."""
+    import torch
+    from up3d_b200.kernels.jacobian import PicardOperator
+    from up3d_b200.solve.linear import build_amg_preconditioner
+    s = c1_system
+    A2 = _embedded(s["A"], s["mask"])
+    rng = np.random.default_rng(9)
+    A1 = _embedded(s["A"], s["mask"])
+    A1.data = A1.data * torch.from_numpy(1.0 + 0.5 * rng.random(A1.data.numel())).cuda()
+    r = torch.from_numpy(s["b"]).cuda()
+    _, M = build_amg_preconditioner(A1, fp32=fp32)
+    z1 = M.matvec(r)
+    M.refresh(A2)
+    z_ref = build_amg_preconditioner(A2, fp32=fp32)[1].matvec(r)
+    assert torch.equal(M.matvec(r), z_ref)
+    assert not torch.equal(z1, z_ref)
+
+
+def test_amg_refresh_rejects_another_pattern(c1_system):
+    import torch
+    from up3d_b200.solve.linear import build_amg_preconditioner, with_dirichlet
+    s = c1_system
+    _, M = build_amg_preconditioner(_embedded(s["A"], s["mask"]))
+    other = s["mask"].clone()
+    other[int(s["free"][0])] = 1
+    with pytest.raises(ValueError, match="pattern|mask"):
+        M.refresh(with_dirichlet(s["A"], other))
+    with pytest.raises(ValueError, match="pattern|mask"):
+        M.refresh(s["A"])
+
+
 def test_gmres_amg_on_newton_jacobian(c1_system):
     import torch
     from up3d_b200.solve.linear import build_amg_preconditioner, solve_gmres, with_dirichlet

@@ -90,6 +90,7 @@ SIGNATURES = {
     "up3d_spmv_f32": (_int, [_i64, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_amg_setup": (_int, [_p, _p, ctypes.POINTER(_p), _p]),
     "up3d_amg_get_info": (_int, [_p, _p]),
+    "up3d_amg_refresh": (_int, [_p, _p, _p]),
     "up3d_precond_jacobi": (_int, [_p, ctypes.POINTER(_p), _p]),
     "up3d_precond_apply": (_int, [_p, _p, _p, _p]),
     "up3d_precond_destroy": (_int, [_p]),

@@ -2,12 +2,19 @@
 // reference's build_amg_preconditioner, solve/linear.py:61-81, which wraps
 // pyamg.smoothed_aggregation_solver with its defaults).
 //
-// Setup (host, OpenMP): all off-diagonal connections strong (theta = 0),
-// the three-pass standard aggregation, tentative prolongator T for the
-// constant near-null-space vector, smoothed prolongator
-// P = (I - omega D^-1 A) T with omega = (4/3) / rho(D^-1 A), Galerkin
-// coarse operators R A P with R = P^T, down to at most `max_coarse`
-// unknowns, where the operator is inverted densely in FP64.
+// Setup, symbolic (host, once per sparsity pattern): all off-diagonal
+// connections strong (theta = 0), the three-pass standard aggregation, and
+// the patterns of the tentative prolongator T (constant near-null-space
+// vector), the smoothed prolongator P = (I - omega D^-1 A) T, A P and the
+// Galerkin operator R A P with R = P^T, down to at most `max_coarse`
+// unknowns.  With every connection strong the aggregates and all patterns
+// depend on the fine pattern alone.
+//
+// Setup, numeric (device, on every setup and refresh): D^-1, rho(D^-1 A) by
+// power iteration, omega = (4/3) / rho, the values of P, A P and R A P in a
+// fixed per-row order, and the dense FP64 inverse of the coarsest operator
+// (Gauss-Jordan with partial pivoting).  A refresh with a new matrix of the
+// same pattern therefore reproduces a fresh setup bit for bit.
 //
 // Cycle (device): V-cycle with damped-Jacobi pre/post smoothing
 // (omega_s = (4/3) / rho(D^-1 A) per level), in FP64 or FP32 (mixed
@@ -39,7 +46,7 @@ struct HostCSR {
     std::vector<double> x;
 };
 
-// ------------------------------------------------------------ host setup
+// ------------------------------------------------------------ host symbolic setup
 
 // Standard aggregation (three passes, node order).  agg[i] = -1 for nodes
 // without strong connections (isolated / constrained).
@@ -98,98 +105,48 @@ int64_t standard_aggregation(const HostCSR& A, const std::vector<uint8_t>& skip,
     return na;
 }
 
-void host_spmv(const HostCSR& A, const std::vector<double>& x, std::vector<double>& y) {
-#pragma omp parallel for schedule(static)
-    for (int64_t r = 0; r < A.n; ++r) {
-        double s = 0.0;
-        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) s += A.x[k] * x[A.i[k]];
-        y[r] = s;
-    }
+int32_t find_col(const HostCSR& P, int64_t r, int32_t c) {
+    auto b = P.i.begin() + P.p[r], e = P.i.begin() + P.p[r + 1];
+    auto it = std::lower_bound(b, e, c);
+    return (it != e && *it == c) ? (int32_t)(it - P.i.begin()) : -1;
 }
 
-// rho(D^-1 A) by power iteration on the symmetric scaling D^-1/2 A D^-1/2.
-double spectral_radius(const HostCSR& A, const std::vector<double>& dinv, const std::vector<uint8_t>& skip) {
+// Pattern of P = (I - omega D^-1 A) T: row r holds agg[r] and agg[c] of its
+// aggregated neighbours.  amap[k] = slot of A entry k's contribution (-1 when
+// its column is unaggregated), self[r] = slot of agg[r] (-1 when none).
+HostCSR prolongator_pattern(const HostCSR& A, const std::vector<int32_t>& agg, int64_t na,
+                            std::vector<int32_t>& amap, std::vector<int32_t>& self) {
     const int64_t n = A.n;
-    std::vector<double> x(n), y(n), s(n);
-    for (int64_t r = 0; r < n; ++r) s[r] = std::sqrt(std::fabs(dinv[r]));
-    uint64_t h = 0x9E3779B97F4A7C15ull;
-    for (int64_t r = 0; r < n; ++r) {
-        h ^= h << 13;
-        h ^= h >> 7;
-        h ^= h << 17;
-        x[r] = skip[r] ? 0.0 : 0.5 + (double)(h % 1000003) / 1000003.0;
-    }
-    double lam = 0.0;
-    for (int it = 0; it < 20; ++it) {
-        std::vector<double> xs(n);
-        for (int64_t r = 0; r < n; ++r) xs[r] = s[r] * x[r];
-        host_spmv(A, xs, y);
-        double num = 0.0, den = 0.0;
-        for (int64_t r = 0; r < n; ++r) {
-            y[r] = skip[r] ? 0.0 : s[r] * y[r];
-            num += y[r] * x[r];
-            den += x[r] * x[r];
-        }
-        lam = den > 0 ? num / den : 0.0;
-        double nrm = 0.0;
-        for (int64_t r = 0; r < n; ++r) nrm += y[r] * y[r];
-        nrm = std::sqrt(nrm);
-        if (nrm == 0.0) break;
-        for (int64_t r = 0; r < n; ++r) x[r] = y[r] / nrm;
-    }
-    return lam > 0 ? 1.05 * lam : 2.0;  // small safety margin on the Rayleigh quotient
-}
-
-// Smoothed prolongator P = (I - omega D^-1 A) T.
-HostCSR smoothed_prolongator(const HostCSR& A, const std::vector<double>& dinv, const std::vector<int32_t>& agg,
-                             int64_t na, double omega) {
-    const int64_t n = A.n;
-    std::vector<int32_t> size(na, 0);
-    for (int64_t r = 0; r < n; ++r)
-        if (agg[r] >= 0) size[agg[r]]++;
-    std::vector<double> t(n, 0.0);
-    for (int64_t r = 0; r < n; ++r)
-        if (agg[r] >= 0) t[r] = 1.0 / std::sqrt((double)size[agg[r]]);
     HostCSR P;
     P.n = n;
     P.m = na;
     P.p.assign(n + 1, 0);
-    std::vector<std::vector<std::pair<int32_t, double>>> rows(n);
+    std::vector<std::vector<int32_t>> rows(n);
 #pragma omp parallel for schedule(dynamic, 1024)
     for (int64_t r = 0; r < n; ++r) {
         auto& row = rows[r];
-        if (agg[r] >= 0) row.emplace_back(agg[r], t[r]);
-        const double f = omega * dinv[r];
-        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
-            int32_t c = A.i[k];
-            if (agg[c] < 0) continue;
-            row.emplace_back(agg[c], -f * A.x[k] * t[c]);
-        }
-        std::sort(row.begin(), row.end(),
-                  [](const auto& a, const auto& b) { return a.first < b.first; });
-        size_t w = 0;
-        for (size_t q = 0; q < row.size(); ++q) {
-            if (w > 0 && row[w - 1].first == row[q].first) row[w - 1].second += row[q].second;
-            else row[w++] = row[q];
-        }
-        row.resize(w);
+        if (agg[r] >= 0) row.push_back(agg[r]);
+        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
+            if (agg[A.i[k]] >= 0) row.push_back(agg[A.i[k]]);
+        std::sort(row.begin(), row.end());
+        row.erase(std::unique(row.begin(), row.end()), row.end());
     }
     for (int64_t r = 0; r < n; ++r) P.p[r + 1] = P.p[r] + (int32_t)rows[r].size();
     P.i.resize(P.p[n]);
-    P.x.resize(P.p[n]);
+    amap.assign(A.i.size(), -1);
+    self.assign(n, -1);
 #pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < n; ++r) {
-        int32_t o = P.p[r];
-        for (auto& e : rows[r]) {
-            P.i[o] = e.first;
-            P.x[o] = e.second;
-            ++o;
-        }
+        std::copy(rows[r].begin(), rows[r].end(), P.i.begin() + P.p[r]);
+        if (agg[r] >= 0) self[r] = find_col(P, r, agg[r]);
+        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
+            if (agg[A.i[k]] >= 0) amap[k] = find_col(P, r, agg[A.i[k]]);
     }
     return P;
 }
 
-HostCSR transpose(const HostCSR& P) {
+// R = P^T pattern; R entry t takes the value of P entry tperm[t].
+HostCSR transpose_pattern(const HostCSR& P, std::vector<int32_t>& tperm) {
     HostCSR R;
     R.n = P.m;
     R.m = P.n;
@@ -197,64 +154,53 @@ HostCSR transpose(const HostCSR& P) {
     for (int32_t c : P.i) R.p[c + 1]++;
     for (int64_t r = 0; r < R.n; ++r) R.p[r + 1] += R.p[r];
     R.i.resize(P.i.size());
-    R.x.resize(P.x.size());
+    tperm.resize(P.i.size());
     std::vector<int32_t> cur(R.p.begin(), R.p.end() - 1);
     for (int64_t r = 0; r < P.n; ++r)
         for (int32_t k = P.p[r]; k < P.p[r + 1]; ++k) {
-            int32_t c = P.i[k];
+            const int32_t c = P.i[k];
             R.i[cur[c]] = (int32_t)r;
-            R.x[cur[c]] = P.x[k];
+            tperm[cur[c]] = k;
             ++cur[c];
         }
     return R;
 }
 
-// C = A B (Gustavson, sorted columns, OpenMP over rows).
-HostCSR spgemm(const HostCSR& A, const HostCSR& B) {
+// Pattern of C = A B (sorted columns, OpenMP over rows).
+HostCSR spgemm_pattern(const HostCSR& A, const HostCSR& B) {
     HostCSR C;
     C.n = A.n;
     C.m = B.m;
     C.p.assign(A.n + 1, 0);
     std::vector<std::vector<int32_t>> ci(A.n);
-    std::vector<std::vector<double>> cx(A.n);
 #pragma omp parallel
     {
-        std::vector<double> acc(B.m, 0.0);
-        std::vector<int32_t> mark(B.m, -1), cols;
+        std::vector<int32_t> mark(B.m, -1);
 #pragma omp for schedule(dynamic, 512)
         for (int64_t r = 0; r < A.n; ++r) {
-            cols.clear();
+            auto& cols = ci[r];
             for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
                 const int32_t a = A.i[k];
-                const double av = A.x[k];
                 for (int32_t q = B.p[a]; q < B.p[a + 1]; ++q) {
                     const int32_t c = B.i[q];
                     if (mark[c] != (int32_t)r) {
                         mark[c] = (int32_t)r;
-                        acc[c] = 0.0;
                         cols.push_back(c);
                     }
-                    acc[c] += av * B.x[q];
                 }
             }
             std::sort(cols.begin(), cols.end());
-            ci[r] = cols;
-            cx[r].resize(cols.size());
-            for (size_t q = 0; q < cols.size(); ++q) cx[r][q] = acc[cols[q]];
         }
     }
     for (int64_t r = 0; r < A.n; ++r) C.p[r + 1] = C.p[r] + (int32_t)ci[r].size();
     C.i.resize(C.p[A.n]);
-    C.x.resize(C.p[A.n]);
 #pragma omp parallel for schedule(static)
-    for (int64_t r = 0; r < A.n; ++r) {
-        std::copy(ci[r].begin(), ci[r].end(), C.i.begin() + C.p[r]);
-        std::copy(cx[r].begin(), cx[r].end(), C.x.begin() + C.p[r]);
-    }
+    for (int64_t r = 0; r < A.n; ++r) std::copy(ci[r].begin(), ci[r].end(), C.i.begin() + C.p[r]);
     return C;
 }
 
-// Dense inverse by Gauss-Jordan with partial pivoting (coarsest level).
+// Dense inverse by Gauss-Jordan with partial pivoting: the host fallback
+// for a singular coarsest operator, inverted after diagonal regularisation.
 bool dense_inverse(std::vector<double>& a, int64_t n, std::vector<double>& inv) {
     inv.assign(n * n, 0.0);
     for (int64_t r = 0; r < n; ++r) inv[r * n + r] = 1.0;
@@ -285,6 +231,239 @@ bool dense_inverse(std::vector<double>& a, int64_t n, std::vector<double>& inv) 
         }
     }
     return true;
+}
+
+// Power-iteration start vector (deterministic xorshift sequence; 0 on
+// skipped rows).
+std::vector<double> power_start(int64_t n, const std::vector<uint8_t>& skip) {
+    std::vector<double> x(n);
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    for (int64_t r = 0; r < n; ++r) {
+        h ^= h << 13;
+        h ^= h >> 7;
+        h ^= h << 17;
+        x[r] = skip[r] ? 0.0 : 0.5 + (double)(h % 1000003) / 1000003.0;
+    }
+    return x;
+}
+
+// ------------------------------------------------------------ device numeric setup
+
+__device__ __forceinline__ int32_t dev_lower_bound(const int32_t* __restrict__ a, int32_t len, int32_t v) {
+    int32_t lo = 0, hi = len;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// finest operator from the caller's matrix: src[k] = caller entry, or -1
+// for the identity entry of a constrained row
+__global__ void k_embed(int64_t nnz, const int32_t* __restrict__ src, const double* __restrict__ data,
+                        double* __restrict__ out) {
+    GRID_STRIDE(k, nnz) out[k] = src[k] >= 0 ? data[src[k]] : 1.0;
+}
+
+__global__ void k_dinv(int64_t n, const int32_t* __restrict__ diag, const double* __restrict__ Ax,
+                       double* __restrict__ dinv, double* __restrict__ s, const double* __restrict__ x0,
+                       double* __restrict__ x) {
+    GRID_STRIDE(r, n) {
+        const double d = diag[r] >= 0 ? Ax[diag[r]] : 0.0;
+        const double di = d != 0.0 ? __ddiv_rn(1.0, d) : 1.0;
+        dinv[r] = di;
+        s[r] = sqrt(fabs(di));
+        x[r] = x0[r];
+    }
+}
+
+// y = skip ? 0 : s * (A (s * x))   (rows of 8 lanes)
+__global__ void __launch_bounds__(256)
+    k_pw_apply(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
+               const double* __restrict__ Ax, const double* __restrict__ s, const double* __restrict__ x,
+               const uint8_t* __restrict__ skip, double* __restrict__ y, const int* __restrict__ done) {
+    if (*done) return;
+    constexpr int TPR = 8, RPW = 32 / TPR;
+    const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * RPW; base < n; base += n_warps * RPW) {
+        const int64_t r = base + group;
+        double acc = 0.0;
+        if (r < n)
+            for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) {
+                const int32_t c = Ai[k];
+                acc += Ax[k] * (s[c] * x[c]);
+            }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+        if (sub == 0 && r < n) y[r] = (skip && skip[r]) ? 0.0 : s[r] * acc;
+    }
+}
+
+// dots = (x.y, y.y, x.x): lambda = x.y / x.x (Rayleigh quotient), stop when
+// y == 0, else normalise (dots[3] = |y|)
+__global__ void k_pw_update(double* __restrict__ dots, double* __restrict__ lam, int* __restrict__ done) {
+    if (*done) return;
+    *lam = dots[2] > 0.0 ? dots[0] / dots[2] : 0.0;
+    if (dots[1] == 0.0) *done = 1;
+    else dots[3] = sqrt(dots[1]);
+}
+
+__global__ void k_pw_norm(int64_t n, const double* __restrict__ y, double* __restrict__ x,
+                          const double* __restrict__ dots, const int* __restrict__ done) {
+    if (*done) return;
+    const double nrm = dots[3];
+    GRID_STRIDE(r, n) x[r] = y[r] / nrm;
+}
+
+// omega = (4/3) / rho with rho = 1.05 lambda (small safety margin on the
+// Rayleigh quotient), 2 when lambda <= 0
+__global__ void k_pw_finish(const double* __restrict__ lam, double* __restrict__ omega) {
+    const double l = *lam;
+    const double rho = l > 0.0 ? 1.05 * l : 2.0;
+    *omega = (4.0 / 3.0) / rho;
+}
+
+// P = (I - omega D^-1 A) T, one row per thread, contributions in the
+// order (T entry, then A's entries in row order)
+__global__ void k_prolong(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
+                          const double* __restrict__ Ax, const int32_t* __restrict__ amap,
+                          const int32_t* __restrict__ self, const double* __restrict__ t,
+                          const double* __restrict__ dinv, const double* __restrict__ omega,
+                          const int32_t* __restrict__ Pp, double* __restrict__ Px) {
+    GRID_STRIDE(r, n) {
+        for (int32_t q = Pp[r]; q < Pp[r + 1]; ++q) Px[q] = 0.0;
+        if (self[r] >= 0) Px[self[r]] = t[r];
+        const double f = __dmul_rn(*omega, dinv[r]);
+        for (int32_t k = Ap[r]; k < Ap[r + 1]; ++k) {
+            const int32_t q = amap[k];
+            if (q < 0) continue;
+            Px[q] = __dadd_rn(Px[q], __dmul_rn(__dmul_rn(-f, Ax[k]), t[Ai[k]]));
+        }
+    }
+}
+
+__global__ void k_gather_vals(int64_t m, const int32_t* __restrict__ perm, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+    GRID_STRIDE(k, m) dst[k] = src[perm[k]];
+}
+
+// C = A B on C's precomputed pattern, one row per thread, products added in
+// (A entry, B entry) order
+__global__ void k_spgemm_num(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
+                             const double* __restrict__ Ax, const int32_t* __restrict__ Bp,
+                             const int32_t* __restrict__ Bi, const double* __restrict__ Bx,
+                             const int32_t* __restrict__ Cp, const int32_t* __restrict__ Ci,
+                             double* __restrict__ Cx) {
+    GRID_STRIDE(r, n) {
+        const int32_t cb = Cp[r], cl = Cp[r + 1] - cb;
+        for (int32_t q = 0; q < cl; ++q) Cx[cb + q] = 0.0;
+        for (int32_t k = Ap[r]; k < Ap[r + 1]; ++k) {
+            const double a = Ax[k];
+            const int32_t j = Ai[k];
+            for (int32_t q = Bp[j]; q < Bp[j + 1]; ++q) {
+                const int32_t pos = cb + dev_lower_bound(Ci + cb, cl, Bi[q]);
+                Cx[pos] = __dadd_rn(Cx[pos], __dmul_rn(a, Bx[q]));
+            }
+        }
+    }
+}
+
+__global__ void k_densify(int64_t n, const int32_t* __restrict__ Cp, const int32_t* __restrict__ Ci,
+                          const double* __restrict__ Cx, double* __restrict__ a, double* __restrict__ inv) {
+    GRID_STRIDE(r, n) {
+        for (int64_t c = 0; c < n; ++c) {
+            a[r * n + c] = 0.0;
+            inv[r * n + c] = (c == r) ? 1.0 : 0.0;
+        }
+        for (int32_t k = Cp[r]; k < Cp[r + 1]; ++k) a[r * n + Ci[k]] = Cx[k];
+    }
+}
+
+// Gauss-Jordan column step c (one block): pivot = first row of largest
+// |a[r][c]|, r >= c; swap; scale row c; fcol[r] = a[r][c] for r != c.
+__global__ void __launch_bounds__(1024)
+    k_gj_pivot(double* __restrict__ a, double* __restrict__ inv, int64_t n, int64_t c, double* __restrict__ fcol,
+               int* __restrict__ singular) {
+    __shared__ double sv[32];
+    __shared__ int64_t si[32];
+    __shared__ double sd;
+    __shared__ int64_t spiv;
+    if (*singular) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    double best = -1.0;
+    int64_t bi = n;
+    for (int64_t r = c + tid; r < n; r += blockDim.x) {
+        const double v = fabs(a[r * n + c]);
+        if (v > best) {
+            best = v;
+            bi = r;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int64_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) {
+            best = ov;
+            bi = oi;
+        }
+    }
+    if (lane == 0) {
+        sv[w] = best;
+        si[w] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double b = -1.0;
+        int64_t p = n;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k)
+            if (sv[k] > b || (sv[k] == b && si[k] < p)) {
+                b = sv[k];
+                p = si[k];
+            }
+        spiv = p;
+    }
+    __syncthreads();
+    const int64_t piv = spiv;
+    if (piv >= n || a[piv * n + c] == 0.0) {
+        if (tid == 0) *singular = 1;
+        return;
+    }
+    if (piv != c)
+        for (int64_t k = tid; k < n; k += blockDim.x) {
+            double t0 = a[c * n + k];
+            a[c * n + k] = a[piv * n + k];
+            a[piv * n + k] = t0;
+            t0 = inv[c * n + k];
+            inv[c * n + k] = inv[piv * n + k];
+            inv[piv * n + k] = t0;
+        }
+    __syncthreads();
+    if (tid == 0) sd = __ddiv_rn(1.0, a[c * n + c]);
+    __syncthreads();
+    const double d = sd;
+    for (int64_t k = tid; k < n; k += blockDim.x) {
+        a[c * n + k] = __dmul_rn(a[c * n + k], d);
+        inv[c * n + k] = __dmul_rn(inv[c * n + k], d);
+    }
+    __syncthreads();
+    for (int64_t r = tid; r < n; r += blockDim.x) fcol[r] = r == c ? 0.0 : a[r * n + c];
+}
+
+// Gauss-Jordan elimination of column c from every other row.
+__global__ void k_gj_elim(double* __restrict__ a, double* __restrict__ inv, int64_t n, int64_t c,
+                          const double* __restrict__ fcol, const int* __restrict__ singular) {
+    if (*singular) return;
+    GRID_STRIDE(idx, n * 2 * n) {
+        const int64_t r = idx / (2 * n), k = idx % (2 * n);
+        const double f = fcol[r];
+        if (r == c || f == 0.0) continue;
+        if (k < n) a[r * n + k] = __dsub_rn(a[r * n + k], __dmul_rn(f, a[c * n + k]));
+        else inv[r * n + k - n] = __dsub_rn(inv[r * n + k - n], __dmul_rn(f, inv[c * n + k - n]));
+    }
 }
 
 // ------------------------------------------------------------ device kernels
@@ -374,7 +553,7 @@ struct DevCSR {
     int64_t n = 0, m = 0, nnz = 0;
     DBuf<int32_t> p, i;
     DBuf<T> x;
-    void upload(const HostCSR& h, cudaStream_t s) {
+    void upload_pattern(const HostCSR& h, cudaStream_t s) {
         n = h.n;
         m = h.m;
         nnz = (int64_t)h.i.size();
@@ -382,14 +561,40 @@ struct DevCSR {
         i.alloc(std::max<int64_t>(nnz, 1));
         x.alloc(std::max<int64_t>(nnz, 1));
         UP3D_CUDA(cudaMemcpyAsync(p.get(), h.p.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s));
-        if (nnz) {
+        if (nnz)
             UP3D_CUDA(cudaMemcpyAsync(i.get(), h.i.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
-            std::vector<T> v(h.x.begin(), h.x.end());
-            UP3D_CUDA(cudaMemcpyAsync(x.get(), v.data(), sizeof(T) * nnz, cudaMemcpyHostToDevice, s));
-            UP3D_CUDA(cudaStreamSynchronize(s));
-        }
+    }
+    template <class U>
+    void copy_pattern(const DevCSR<U>& o, cudaStream_t s) {
+        n = o.n;
+        m = o.m;
+        nnz = o.nnz;
+        p.alloc(n + 1);
+        i.alloc(std::max<int64_t>(nnz, 1));
+        x.alloc(std::max<int64_t>(nnz, 1));
+        UP3D_CUDA(cudaMemcpyAsync(p.get(), o.p.get(), sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice, s));
+        if (nnz)
+            UP3D_CUDA(cudaMemcpyAsync(i.get(), o.i.get(), sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, s));
     }
 };
+
+template <class T>
+void upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty()) UP3D_CUDA(cudaMemcpyAsync(d.get(), h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+}
+
+// values of type T from FP64 (copy or narrowing)
+template <class T>
+void convert(const double* src, T* dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    if constexpr (std::is_same<T, double>::value) {
+        UP3D_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        k_d2f<<<grid_for(n, 256), 256, 0, s>>>(src, dst, n);
+        UP3D_CHECK_LAUNCH();
+    }
+}
 
 template <class T>
 struct Level {
@@ -399,21 +604,44 @@ struct Level {
     const uint8_t* dir = nullptr;  // finest level only
 };
 
+// Symbolic structure and FP64 values of one level.
+struct SymLevel {
+    DevCSR<double> A;            // level operator
+    DBuf<int32_t> diag;          // (n) slot of the diagonal, -1 when absent
+    DBuf<uint8_t> skip;          // (n) constrained rows (finest level only)
+    DBuf<double> x0, dinv, sq;   // power-iteration start, D^-1, sqrt|D^-1|
+    // to the next level (absent on the coarsest)
+    DBuf<int32_t> amap, self;    // A entry / row -> P slot
+    DBuf<double> t;              // tentative prolongator value of each row
+    DevCSR<double> P, R, AP;     // prolongator, restriction (P^T), A P
+    DBuf<int32_t> tperm;         // R entry -> P entry
+    bool has_skip = false;
+};
+
 }  // namespace
 
 struct Amg {
     bool fp32 = false;
     int pre = 2, post = 2;
     int64_t n_coarse = 0;
+    // the caller's finest pattern (refresh checks) and its embedding
+    int64_t n_in = 0, nnz_in = 0;
+    bool has_dir = false;
+    DBuf<int32_t> in_p, in_i, emb_src;
+    DBuf<uint8_t> in_dir;
+    std::vector<SymLevel*> sym;
+    // numeric scratch
+    DBuf<double> pw_xy, pw_scal, omega_dev, dense_a, fcol;
+    DBuf<int> flags;
+    std::vector<double> omega;
     DBuf<double> cinv;
     std::vector<Level<double>*> Ld;
     std::vector<Level<float>*> Lf;
-    DBuf<float> in_f, out_f;
-    DBuf<double> bc_d, xc_d;
     up3d_amg_info info{};
     ~Amg() {
         for (auto* l : Ld) delete l;
         for (auto* l : Lf) delete l;
+        for (auto* l : sym) delete l;
     }
 };
 
@@ -464,29 +692,154 @@ void vcycle(Amg& a, std::vector<Level<T>*>& L, size_t l, cudaStream_t s) {
     }
 }
 
+// Diagonal slot of each row of a pattern.
+std::vector<int32_t> diag_slots(const HostCSR& A) {
+    std::vector<int32_t> d(A.n, -1);
+    for (int64_t r = 0; r < A.n; ++r)
+        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
+            if (A.i[k] == r) d[r] = k;
+    return d;
+}
+
+// Device numeric phase: every level's D^-1, omega, P, R, A P and coarser
+// operator, then the coarsest inverse; fills the cycle's levels.
+void numeric(Amg& a, cudaStream_t s) {
+    const size_t L = a.sym.size();
+    Blas blas(s);
+    double* dots = a.pw_scal.get();       // x.y, y.y, x.x, |y|
+    double* lam = a.pw_scal.get() + 4;
+    int* done = a.flags.get();
+    int* singular = a.flags.get() + 1;
+    for (size_t l = 0; l + 1 < L; ++l) {
+        SymLevel& F = *a.sym[l];
+        SymLevel& C = *a.sym[l + 1];
+        const int64_t n = F.A.n;
+        double* x = a.pw_xy.get();
+        double* y = a.pw_xy.get() + n;
+        k_dinv<<<grid_for(n, 256), 256, 0, s>>>(n, F.diag.get(), F.A.x.get(), F.dinv.get(), F.sq.get(),
+                                                F.x0.get(), x);
+        UP3D_CHECK_LAUNCH();
+        UP3D_CUDA(cudaMemsetAsync(done, 0, sizeof(int), s));
+        UP3D_CUDA(cudaMemsetAsync(lam, 0, sizeof(double), s));
+        const unsigned g8 = grid_for(8 * n, 256, (int64_t)148 * 64);
+        for (int it = 0; it < 20; ++it) {
+            k_pw_apply<<<g8, 256, 0, s>>>(n, F.A.p.get(), F.A.i.get(), F.A.x.get(), F.sq.get(), x,
+                                          F.has_skip ? F.skip.get() : nullptr, y, done);
+            UP3D_CHECK_LAUNCH();
+            blas.multidot(x, n, 2, y, n, dots);   // (x.y, y.y)
+            blas.multidot(x, 0, 1, x, n, dots + 2);
+            k_pw_update<<<1, 1, 0, s>>>(dots, lam, done);
+            UP3D_CHECK_LAUNCH();
+            k_pw_norm<<<grid_for(n, 256), 256, 0, s>>>(n, y, x, dots, done);
+            UP3D_CHECK_LAUNCH();
+        }
+        k_pw_finish<<<1, 1, 0, s>>>(lam, a.omega_dev.get() + l);
+        UP3D_CHECK_LAUNCH();
+        k_prolong<<<grid_for(n, 128), 128, 0, s>>>(n, F.A.p.get(), F.A.i.get(), F.A.x.get(), F.amap.get(),
+                                                   F.self.get(), F.t.get(), F.dinv.get(), a.omega_dev.get() + l,
+                                                   F.P.p.get(), F.P.x.get());
+        UP3D_CHECK_LAUNCH();
+        k_gather_vals<<<grid_for(F.R.nnz, 256), 256, 0, s>>>(F.R.nnz, F.tperm.get(), F.P.x.get(), F.R.x.get());
+        UP3D_CHECK_LAUNCH();
+        k_spgemm_num<<<grid_for(n, 128), 128, 0, s>>>(n, F.A.p.get(), F.A.i.get(), F.A.x.get(), F.P.p.get(),
+                                                      F.P.i.get(), F.P.x.get(), F.AP.p.get(), F.AP.i.get(),
+                                                      F.AP.x.get());
+        UP3D_CHECK_LAUNCH();
+        k_spgemm_num<<<grid_for(F.R.n, 128), 128, 0, s>>>(F.R.n, F.R.p.get(), F.R.i.get(), F.R.x.get(),
+                                                          F.AP.p.get(), F.AP.i.get(), F.AP.x.get(), C.A.p.get(),
+                                                          C.A.i.get(), C.A.x.get());
+        UP3D_CHECK_LAUNCH();
+    }
+    // coarsest dense inverse
+    const SymLevel& Cl = *a.sym.back();
+    const int64_t nc = Cl.A.n;
+    UP3D_CUDA(cudaMemsetAsync(singular, 0, sizeof(int), s));
+    k_densify<<<grid_for(nc, 128), 128, 0, s>>>(nc, Cl.A.p.get(), Cl.A.i.get(), Cl.A.x.get(), a.dense_a.get(),
+                                                a.cinv.get());
+    UP3D_CHECK_LAUNCH();
+    for (int64_t c = 0; c < nc; ++c) {
+        k_gj_pivot<<<1, 1024, 0, s>>>(a.dense_a.get(), a.cinv.get(), nc, c, a.fcol.get(), singular);
+        UP3D_CHECK_LAUNCH();
+        k_gj_elim<<<grid_for(2 * nc * nc, 256), 256, 0, s>>>(a.dense_a.get(), a.cinv.get(), nc, c, a.fcol.get(),
+                                                             singular);
+        UP3D_CHECK_LAUNCH();
+    }
+    int sing = 0;
+    a.omega.assign(L > 1 ? L - 1 : 0, 0.0);
+    if (L > 1)
+        UP3D_CUDA(cudaMemcpyAsync(a.omega.data(), a.omega_dev.get(), sizeof(double) * (L - 1),
+                                  cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(&sing, singular, sizeof(int), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    if (sing) {
+        // singular coarse operator (e.g. pure-Neumann): regularise the
+        // diagonal and invert on the host
+        HostCSR h;
+        h.n = h.m = nc;
+        h.p.resize(nc + 1);
+        h.i.resize(Cl.A.nnz);
+        h.x.resize(Cl.A.nnz);
+        UP3D_CUDA(cudaMemcpyAsync(h.p.data(), Cl.A.p.get(), sizeof(int32_t) * (nc + 1), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaMemcpyAsync(h.i.data(), Cl.A.i.get(), sizeof(int32_t) * Cl.A.nnz, cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaMemcpyAsync(h.x.data(), Cl.A.x.get(), sizeof(double) * Cl.A.nnz, cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        std::vector<double> dense(nc * nc, 0.0), inv;
+        double dmax = 0.0;
+        for (int64_t r = 0; r < nc; ++r)
+            for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k) {
+                dense[r * nc + h.i[k]] = h.x[k];
+                if (h.i[k] == r) dmax = std::max(dmax, std::fabs(h.x[k]));
+            }
+        for (int64_t r = 0; r < nc; ++r) dense[r * nc + r] += 1e-12 * (dmax > 0 ? dmax : 1.0);
+        UP3D_REQUIRE(dense_inverse(dense, nc, inv), UP3D_ERR_RUNTIME, "AMG coarsest operator is singular");
+        UP3D_CUDA(cudaMemcpyAsync(a.cinv.get(), inv.data(), sizeof(double) * nc * nc, cudaMemcpyHostToDevice, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+// Copies (or narrows) the FP64 level values into the cycle's levels.
 template <class T>
-void upload_levels(Amg& a, std::vector<Level<T>*>& L, const std::vector<HostCSR>& As, const std::vector<HostCSR>& Ps,
-                   const std::vector<std::vector<double>>& dinvs, const std::vector<double>& wsm,
-                   const uint8_t* dir_dev, cudaStream_t s) {
-    for (size_t l = 0; l < As.size(); ++l) {
+void fill_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
+    for (size_t l = 0; l < a.sym.size(); ++l) {
+        SymLevel& F = *a.sym[l];
+        Level<T>& lv = *Lv[l];
+        convert<T>(F.A.x.get(), lv.A.x.get(), F.A.nnz, s);
+        if (l + 1 < a.sym.size()) {
+            convert<T>(F.P.x.get(), lv.P.x.get(), F.P.nnz, s);
+            convert<T>(F.R.x.get(), lv.R.x.get(), F.R.nnz, s);
+            convert<T>(F.dinv.get(), lv.dinv.get(), F.A.n, s);
+            lv.w_smooth = (T)a.omega[l];
+        }
+    }
+}
+
+template <class T>
+void make_levels(Amg& a, std::vector<Level<T>*>& Lv, const uint8_t* dir_dev, cudaStream_t s) {
+    for (size_t l = 0; l < a.sym.size(); ++l) {
+        SymLevel& F = *a.sym[l];
         auto* lv = new Level<T>();
-        lv->A.upload(As[l], s);
-        const int64_t n = As[l].n;
+        Lv.push_back(lv);
+        lv->A.copy_pattern(F.A, s);
+        const int64_t n = F.A.n;
         lv->x.alloc(n);
         lv->b.alloc(n);
         lv->r.alloc(n);
-        if (l < Ps.size()) {
-            lv->P.upload(Ps[l], s);
-            lv->R.upload(transpose(Ps[l]), s);
+        if (l + 1 < a.sym.size()) {
+            lv->P.copy_pattern(F.P, s);
+            lv->R.copy_pattern(F.R, s);
             lv->dinv.alloc(n);
-            std::vector<T> d(dinvs[l].begin(), dinvs[l].end());
-            UP3D_CUDA(cudaMemcpyAsync(lv->dinv.get(), d.data(), sizeof(T) * n, cudaMemcpyHostToDevice, s));
-            UP3D_CUDA(cudaStreamSynchronize(s));
-            lv->w_smooth = (T)wsm[l];
         }
         if (l == 0) lv->dir = dir_dev;
-        L.push_back(lv);
     }
+}
+
+__global__ void k_diff_i32(int64_t n, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                           int* __restrict__ flag) {
+    GRID_STRIDE(i, n) if (a[i] != b[i]) *flag = 1;
+}
+__global__ void k_diff_u8(int64_t n, const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                          int* __restrict__ flag) {
+    GRID_STRIDE(i, n) if ((a[i] != 0) != (b[i] != 0)) *flag = 1;
 }
 
 }  // namespace
@@ -521,6 +874,7 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         a->pre = std::max(1, opt.presmooth);
         a->post = std::max(0, opt.postsmooth);
         const int64_t n = A.n;
+        UP3D_REQUIRE(n > 0, UP3D_ERR_VALUE, "AMG setup: empty matrix");
         HostCSR h;
         h.n = h.m = n;
         h.p.resize(n + 1);
@@ -528,94 +882,116 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         UP3D_CUDA(cudaStreamSynchronize(s));
         const int64_t nnz = h.p[n];
         h.i.resize(nnz);
-        h.x.resize(nnz);
         UP3D_CUDA(cudaMemcpyAsync(h.i.data(), A.indices, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, s));
-        UP3D_CUDA(cudaMemcpyAsync(h.x.data(), A.data, sizeof(double) * nnz, cudaMemcpyDeviceToHost, s));
         std::vector<uint8_t> skip(n, 0);
         if (A.dirichlet)
             UP3D_CUDA(cudaMemcpyAsync(skip.data(), A.dirichlet, n, cudaMemcpyDeviceToHost, s));
         UP3D_CUDA(cudaStreamSynchronize(s));
+        for (auto& v : skip) v = v != 0;
+        // the caller's pattern, kept for refresh checks
+        a->n_in = n;
+        a->nnz_in = nnz;
+        a->has_dir = A.dirichlet != nullptr;
+        upload(a->in_p, h.p, s);
+        upload(a->in_i, h.i, s);
+        if (a->has_dir) upload(a->in_dir, skip, s);
         // finest operator as the embedded free-DOF system: identity rows,
-        // constrained columns dropped
-        if (A.dirichlet) {
-            HostCSR e;
-            e.n = e.m = n;
-            e.p.assign(n + 1, 0);
-            for (int64_t r = 0; r < n; ++r) {
-                int32_t cnt = 0;
-                if (skip[r]) cnt = 1;
-                else
-                    for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k) cnt += !skip[h.i[k]];
-                e.p[r + 1] = e.p[r] + cnt;
-            }
-            e.i.resize(e.p[n]);
-            e.x.resize(e.p[n]);
-            for (int64_t r = 0; r < n; ++r) {
-                int32_t o = e.p[r];
-                if (skip[r]) {
-                    e.i[o] = (int32_t)r;
-                    e.x[o] = 1.0;
-                    continue;
-                }
-                for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k)
-                    if (!skip[h.i[k]]) {
-                        e.i[o] = h.i[k];
-                        e.x[o] = h.x[k];
-                        ++o;
-                    }
-            }
-            h = std::move(e);
+        // constrained columns dropped; src = caller entry (-1: identity)
+        HostCSR e;
+        std::vector<int32_t> src;
+        e.n = e.m = n;
+        e.p.assign(n + 1, 0);
+        for (int64_t r = 0; r < n; ++r) {
+            int32_t cnt = 0;
+            if (skip[r]) cnt = 1;
+            else
+                for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k) cnt += !skip[h.i[k]];
+            e.p[r + 1] = e.p[r] + cnt;
         }
-        std::vector<HostCSR> As, Ps;
-        std::vector<std::vector<double>> dinvs;
-        std::vector<double> wsm;
-        As.push_back(std::move(h));
+        e.i.resize(e.p[n]);
+        src.resize(e.p[n]);
+        for (int64_t r = 0; r < n; ++r) {
+            int32_t o = e.p[r];
+            if (skip[r]) {
+                e.i[o] = (int32_t)r;
+                src[o] = -1;
+                continue;
+            }
+            for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k)
+                if (!skip[h.i[k]]) {
+                    e.i[o] = h.i[k];
+                    src[o] = k;
+                    ++o;
+                }
+        }
+        upload(a->emb_src, src, s);
+        // symbolic levels
+        std::vector<HostCSR> As;
+        As.push_back(std::move(e));
         std::vector<uint8_t> cur_skip = skip;
         const int64_t max_coarse = std::max<int64_t>(opt.max_coarse, 1);
-        while (As.back().n > max_coarse && (int)As.size() < std::max(2, opt.max_levels)) {
+        int64_t nmax = n;
+        while (true) {
             const HostCSR& Al = As.back();
-            std::vector<double> dinv(Al.n, 1.0);
-            for (int64_t r = 0; r < Al.n; ++r)
-                for (int32_t k = Al.p[r]; k < Al.p[r + 1]; ++k)
-                    if (Al.i[k] == r && Al.x[k] != 0.0) dinv[r] = 1.0 / Al.x[k];
-            const double rho = spectral_radius(Al, dinv, cur_skip);
+            auto* F = new SymLevel();
+            a->sym.push_back(F);
+            F->A.upload_pattern(Al, s);
+            upload(F->diag, diag_slots(Al), s);
+            F->has_skip = a->sym.size() == 1 && a->has_dir;
+            if (F->has_skip) upload(F->skip, cur_skip, s);
+            F->dinv.alloc(Al.n);
+            F->sq.alloc(Al.n);
+            if (Al.n <= max_coarse || (int)As.size() >= std::max(2, opt.max_levels)) break;
             std::vector<int32_t> agg;
             const int64_t na = standard_aggregation(Al, cur_skip, agg);
             if (na == 0 || na >= Al.n) break;
-            HostCSR P = smoothed_prolongator(Al, dinv, agg, na, (4.0 / 3.0) / rho);
-            HostCSR AP = spgemm(Al, P);
-            HostCSR Ac = spgemm(transpose(P), AP);
-            dinvs.push_back(std::move(dinv));
-            wsm.push_back((4.0 / 3.0) / rho);
-            Ps.push_back(std::move(P));
+            upload(F->x0, power_start(Al.n, cur_skip), s);
+            std::vector<int32_t> amap, self, tperm;
+            HostCSR P = prolongator_pattern(Al, agg, na, amap, self);
+            std::vector<int32_t> size(na, 0);
+            for (int64_t r = 0; r < Al.n; ++r)
+                if (agg[r] >= 0) size[agg[r]]++;
+            std::vector<double> t(Al.n, 0.0);
+            for (int64_t r = 0; r < Al.n; ++r)
+                if (agg[r] >= 0) t[r] = 1.0 / std::sqrt((double)size[agg[r]]);
+            HostCSR R = transpose_pattern(P, tperm);
+            HostCSR AP = spgemm_pattern(Al, P);
+            HostCSR Ac = spgemm_pattern(R, AP);
+            upload(F->amap, amap, s);
+            upload(F->self, self, s);
+            upload(F->t, t, s);
+            upload(F->tperm, tperm, s);
+            F->P.upload_pattern(P, s);
+            F->R.upload_pattern(R, s);
+            F->AP.upload_pattern(AP, s);
+            UP3D_CUDA(cudaStreamSynchronize(s));  // host vectors above go out of scope
             As.push_back(std::move(Ac));
             cur_skip.assign(As.back().n, 0);
         }
-        // coarsest dense inverse (FP64)
-        const HostCSR& Ac = As.back();
-        const int64_t nc = Ac.n;
+        // a level that stopped early without a start vector is the coarsest
+        const int64_t nc = As.back().n;
         UP3D_REQUIRE(nc <= 8192, UP3D_ERR_RUNTIME, "AMG coarsest level too large for the dense solve");
-        std::vector<double> dense(nc * nc, 0.0), inv;
-        for (int64_t r = 0; r < nc; ++r)
-            for (int32_t k = Ac.p[r]; k < Ac.p[r + 1]; ++k) dense[r * nc + Ac.i[k]] = Ac.x[k];
-        if (!dense_inverse(dense, nc, inv)) {
-            // singular coarse operator (e.g. pure-Neumann): regularise the diagonal
-            dense.assign(nc * nc, 0.0);
-            double dmax = 0.0;
-            for (int64_t r = 0; r < nc; ++r)
-                for (int32_t k = Ac.p[r]; k < Ac.p[r + 1]; ++k) {
-                    dense[r * nc + Ac.i[k]] = Ac.x[k];
-                    if (Ac.i[k] == r) dmax = std::max(dmax, std::fabs(Ac.x[k]));
-                }
-            for (int64_t r = 0; r < nc; ++r) dense[r * nc + r] += 1e-12 * (dmax > 0 ? dmax : 1.0);
-            UP3D_REQUIRE(dense_inverse(dense, nc, inv), UP3D_ERR_RUNTIME, "AMG coarsest operator is singular");
-        }
         a->n_coarse = nc;
+        a->pw_xy.alloc(2 * nmax);
+        a->pw_scal.alloc(8);
+        a->omega_dev.alloc(std::max<size_t>(a->sym.size(), 1));
+        a->flags.alloc(2);
+        a->dense_a.alloc(nc * nc);
         a->cinv.alloc(nc * nc);
-        UP3D_CUDA(cudaMemcpyAsync(a->cinv.get(), inv.data(), sizeof(double) * nc * nc, cudaMemcpyHostToDevice, s));
+        a->fcol.alloc(nc);
+        k_embed<<<grid_for(a->sym[0]->A.nnz, 256), 256, 0, s>>>(a->sym[0]->A.nnz, a->emb_src.get(), A.data,
+                                                                a->sym[0]->A.x.get());
+        UP3D_CHECK_LAUNCH();
+        numeric(*a, s);
+        const uint8_t* dir_dev = A.dirichlet ? a->in_dir.get() : nullptr;
+        if (a->fp32) {
+            make_levels<float>(*a, a->Lf, dir_dev, s);
+            fill_levels<float>(*a, a->Lf, s);
+        } else {
+            make_levels<double>(*a, a->Ld, dir_dev, s);
+            fill_levels<double>(*a, a->Ld, s);
+        }
         UP3D_CUDA(cudaStreamSynchronize(s));
-        if (a->fp32) upload_levels<float>(*a, a->Lf, As, Ps, dinvs, wsm, A.dirichlet, s);
-        else upload_levels<double>(*a, a->Ld, As, Ps, dinvs, wsm, A.dirichlet, s);
         a->info.n_levels = (int32_t)As.size();
         int64_t tot = 0;
         for (auto& M : As) tot += (int64_t)M.i.size();
@@ -627,6 +1003,38 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         throw;
     }
     return a;
+}
+
+// New values for the hierarchy: `A` must have the pattern and Dirichlet
+// mask of the matrix the hierarchy was set up from.
+void amg_refresh(void* p, const up3d_csr& A, cudaStream_t s) {
+    Amg& a = *static_cast<Amg*>(p);
+    UP3D_REQUIRE(A.n == a.n_in, UP3D_ERR_VALUE, "AMG refresh: matrix size differs from the setup matrix");
+    UP3D_REQUIRE((A.dirichlet != nullptr) == a.has_dir, UP3D_ERR_VALUE,
+                 "AMG refresh: Dirichlet mask presence differs from the setup matrix");
+    int* flag = a.flags.get();
+    UP3D_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    k_diff_i32<<<grid_for(a.n_in + 1, 256), 256, 0, s>>>(a.n_in + 1, A.indptr, a.in_p.get(), flag);
+    UP3D_CHECK_LAUNCH();
+    int diff = 0;
+    UP3D_CUDA(cudaMemcpyAsync(&diff, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    UP3D_REQUIRE(!diff, UP3D_ERR_VALUE, "AMG refresh: sparsity pattern differs from the setup matrix");
+    k_diff_i32<<<grid_for(a.nnz_in, 256), 256, 0, s>>>(a.nnz_in, A.indices, a.in_i.get(), flag);
+    UP3D_CHECK_LAUNCH();
+    if (a.has_dir) {
+        k_diff_u8<<<grid_for(a.n_in, 256), 256, 0, s>>>(a.n_in, A.dirichlet, a.in_dir.get(), flag);
+        UP3D_CHECK_LAUNCH();
+    }
+    UP3D_CUDA(cudaMemcpyAsync(&diff, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    UP3D_REQUIRE(!diff, UP3D_ERR_VALUE, "AMG refresh: sparsity pattern or Dirichlet mask differs from the setup matrix");
+    k_embed<<<grid_for(a.sym[0]->A.nnz, 256), 256, 0, s>>>(a.sym[0]->A.nnz, a.emb_src.get(), A.data,
+                                                           a.sym[0]->A.x.get());
+    UP3D_CHECK_LAUNCH();
+    numeric(a, s);
+    if (a.fp32) fill_levels<float>(a, a.Lf, s);
+    else fill_levels<double>(a, a.Ld, s);
 }
 
 const up3d_amg_info* amg_info(void* p) { return &static_cast<Amg*>(p)->info; }
@@ -653,6 +1061,14 @@ int up3d_amg_setup(const up3d_csr* A, const up3d_amg_options* opt, up3d_precond*
             throw;
         }
         *out = M;
+    });
+}
+
+int up3d_amg_refresh(up3d_precond* M, const up3d_csr* A, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(M && A && M->kind == 2 && M->amg && A->indptr && A->indices && A->data, UP3D_ERR_ARGUMENT,
+                     "up3d_amg_refresh: null argument or not an AMG handle");
+        amg_refresh(M->amg, *A, S(stream));
     });
 }
 

@@ -32,6 +32,7 @@ struct Operator {
 void amg_apply(void* amg, const double* r, double* z, cudaStream_t s);
 void amg_destroy(void* amg);
 void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s);
+void amg_refresh(void* amg, const up3d_csr& A, cudaStream_t s);
 const up3d_amg_info* amg_info(void* amg);
 
 }  // namespace up3d

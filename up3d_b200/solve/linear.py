@@ -108,6 +108,17 @@ class DevicePreconditioner:
 
     __call__ = matvec
 
+    def refresh(self, A, dirichlet=None):
+        """New values for an AMG hierarchy from a matrix with the pattern
+        and Dirichlet mask of its setup matrix (up3d_amg_refresh): equal,
+        bit for bit, to a fresh build_amg_preconditioner on A.  ValueError
+        when the pattern or mask differ."""
+        if not self.kind.startswith("amg"):
+            raise TypeError("refresh applies to AMG preconditioners")
+        Ad = as_device_csr(A)
+        L.call("up3d_amg_refresh", self.handle, ctypes.byref(_csr_struct(Ad, dirichlet)), L.stream_ptr())
+        return self
+
 
 class AMGHierarchy:
     """The ``ml`` object of build_amg_preconditioner: level sizes and
@@ -143,6 +154,19 @@ def build_amg_preconditioner(A, fp32: bool = False, max_coarse: int = 500, max_l
            ctypes.byref(h), L.stream_ptr())
     M = DevicePreconditioner(h.value, Ad.shape[0], "amg32" if fp32 else "amg")
     return AMGHierarchy(M), M
+
+
+def amg_for(A, M: Optional[DevicePreconditioner] = None, fp32: bool = False, dirichlet=None):
+    """The AMG preconditioner of A: M refreshed with A's values when M was
+    set up (with the same precision) on A's pattern, else a new setup.
+    Returns the preconditioner."""
+    kind = "amg32" if fp32 else "amg"
+    if M is not None and M.kind == kind:
+        try:
+            return M.refresh(A, dirichlet)
+        except ValueError:
+            pass
+    return build_amg_preconditioner(A, fp32=fp32, dirichlet=dirichlet)[1]
 
 
 def build_jacobi_preconditioner(A, dirichlet=None) -> DevicePreconditioner:

@@ -27,7 +27,7 @@ import numpy as np
 from .. import _lib as L
 from ..mesh.device import DeviceMesh, get_mesh
 from .fused import FlowParams, ResidualJacobian
-from .linear import build_amg_preconditioner, solve_cg, solve_gmres, with_dirichlet
+from .linear import amg_for, solve_cg, solve_gmres, with_dirichlet
 
 
 def _ew_forcing(r_norm, r_norm_prev, eta_prev, eta0=1e-2, gamma_ew=0.9, eta_max=1e-2,
@@ -113,7 +113,7 @@ def picard_seed(ws: ChannelWorkspace, flow: FlowParams, phi, n_iter: int = 5, rt
         rhs = -A.matvec(ws.phi_dir)
         rhs[ws.dn] = 0.0
         Af = with_dirichlet(A, ws.mask)
-        _, M = build_amg_preconditioner(Af, fp32=amg_fp32)
+        ws.amg = M = amg_for(Af, getattr(ws, "amg", None), fp32=amg_fp32)
         x, _, info = solve_cg(Af, rhs, M=M, rtol=rtol, maxiter=2000,
                               x0=t.where(ws.free, phi, t.zeros_like(phi)))
         phi = t.where(ws.free, x, ws.phi_dir)
@@ -239,7 +239,8 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
         timings["assembly"] += clock() - a
         a = clock()
         if M_pre is None or it % amg_rebuild_every == 0:
-            _, M_pre = build_amg_preconditioner(ws.picard_matrix(), fp32=amg_fp32)
+            # a rebuild on the fixed P1 pattern is a refresh of the values
+            ws.amg = M_pre = amg_for(ws.picard_matrix(), getattr(ws, "amg", None), fp32=amg_fp32)
         timings["precond"] += clock() - a
         eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev)
         eta_prev = eta

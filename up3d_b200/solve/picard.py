@@ -15,7 +15,7 @@ import numpy as np
 from .. import _lib as L
 from ..kernels.jacobian import PicardOperator
 from ..physics.isentropic import density_field, mach_squared_field
-from .linear import build_amg_preconditioner, solve_cg, with_dirichlet
+from .linear import amg_for, solve_cg, with_dirichlet
 
 
 def solve_subsonic(nodes, elements, dirichlet_nodes, dirichlet_values, m_inf: float,
@@ -60,6 +60,7 @@ def solve_subsonic(nodes, elements, dirichlet_nodes, dirichlet_values, m_inf: fl
         t.cuda.synchronize()
         return time.perf_counter()
 
+    M = None
     for _ in range(n_picard_max):
         a = tick()
         A = op.assemble_matrix(rho)
@@ -71,7 +72,7 @@ def solve_subsonic(nodes, elements, dirichlet_nodes, dirichlet_values, m_inf: fl
         Af = with_dirichlet(A, mask)
         b2 = tick()
         timings["assembly"] += b2 - a
-        _, M = build_amg_preconditioner(Af, fp32=amg_fp32)
+        M = amg_for(Af, M, fp32=amg_fp32)
         c = tick()
         timings["precond"] += c - b2
         x, n_it, info = solve_cg(Af, rhs, M=M, rtol=rtol, maxiter=maxiter)
