@@ -638,7 +638,24 @@ struct Amg {
     std::vector<Level<double>*> Ld;
     std::vector<Level<float>*> Lf;
     up3d_amg_info info{};
+    // one V-cycle as a CUDA graph per (input, output) pair: captured on a
+    // private stream at first use, replayed on the caller's stream
+    struct Graph {
+        const double* r;
+        double* z;
+        cudaGraphExec_t exec;
+        long long launches;
+    };
+    std::vector<Graph> graphs;
+    cudaStream_t capture_stream = nullptr;
+    int device = 0;
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
     ~Amg() {
+        drop_graphs();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
         for (auto* l : Ld) delete l;
         for (auto* l : Lf) delete l;
         for (auto* l : sym) delete l;
@@ -844,8 +861,8 @@ __global__ void k_diff_u8(int64_t n, const uint8_t* __restrict__ a, const uint8_
 
 }  // namespace
 
-void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
-    Amg& a = *static_cast<Amg*>(p);
+// One V-cycle z = M r as a sequence of launches on stream s.
+void amg_cycle(Amg& a, const double* r, double* z, cudaStream_t s) {
     if (!a.fp32) {
         Level<double>& f = *a.Ld[0];
         const int64_t n = f.A.n;
@@ -861,6 +878,63 @@ void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
         k_f2d<<<grid_for(n, 256), 256, 0, s>>>(f.x.get(), z, n);
         UP3D_CHECK_LAUNCH();
     }
+}
+
+// The cycle's level buffers swap between sweeps; restoring them after each
+// cycle keeps every cycle (and every captured graph) on the same buffers.
+template <class T>
+std::vector<std::pair<T*, T*>> save_buffers(std::vector<Level<T>*>& L) {
+    std::vector<std::pair<T*, T*>> v;
+    for (auto* l : L) v.emplace_back(l->x.p, l->r.p);
+    return v;
+}
+template <class T>
+void restore_buffers(std::vector<Level<T>*>& L, const std::vector<std::pair<T*, T*>>& v) {
+    for (size_t i = 0; i < L.size(); ++i) {
+        L[i]->x.p = v[i].first;
+        L[i]->r.p = v[i].second;
+    }
+}
+
+void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
+    Amg& a = *static_cast<Amg*>(p);
+    for (auto& g : a.graphs)
+        if (g.r == r && g.z == z) {
+            UP3D_CUDA(cudaGraphLaunch(g.exec, s));
+            count_launch((int)g.launches);
+            return;
+        }
+    if (!a.capture_stream) UP3D_CUDA(cudaStreamCreateWithFlags(&a.capture_stream, cudaStreamNonBlocking));
+    auto sd = save_buffers(a.Ld);
+    auto sf = save_buffers(a.Lf);
+    const long long l0 = g_launches.load();
+    cudaGraph_t graph = nullptr;
+    UP3D_CUDA(cudaStreamBeginCapture(a.capture_stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        amg_cycle(a, r, z, a.capture_stream);
+    } catch (...) {
+        cudaStreamEndCapture(a.capture_stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        restore_buffers(a.Ld, sd);
+        restore_buffers(a.Lf, sf);
+        throw;
+    }
+    UP3D_CUDA(cudaStreamEndCapture(a.capture_stream, &graph));
+    restore_buffers(a.Ld, sd);
+    restore_buffers(a.Lf, sf);
+    const long long launches = g_launches.load() - l0;
+    g_launches.fetch_sub(launches);  // counted at each replay instead
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    UP3D_CUDA(e);
+    if (a.graphs.size() >= 16) {
+        cudaGraphExecDestroy(a.graphs.front().exec);
+        a.graphs.erase(a.graphs.begin());
+    }
+    a.graphs.push_back({r, z, exec, launches});
+    UP3D_CUDA(cudaGraphLaunch(exec, s));
+    count_launch((int)launches);
 }
 
 void amg_destroy(void* p) { delete static_cast<Amg*>(p); }
@@ -1035,6 +1109,7 @@ void amg_refresh(void* p, const up3d_csr& A, cudaStream_t s) {
     numeric(a, s);
     if (a.fp32) fill_levels<float>(a, a.Lf, s);
     else fill_levels<double>(a, a.Ld, s);
+    a.drop_graphs();  // the smoothing weights are launch arguments of the graphs
 }
 
 const up3d_amg_info* amg_info(void* p) { return &static_cast<Amg*>(p)->info; }

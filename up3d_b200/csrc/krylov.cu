@@ -93,8 +93,9 @@ __global__ void k_sub(const double* __restrict__ b, const double* __restrict__ a
     GRID_STRIDE(i, n) r[i] = b[i] - ax[i];
 }
 
-__global__ void k_add_to(double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
-    GRID_STRIDE(i, n) out[i] = a[i] + b[i];
+// a += b
+__global__ void k_accumulate(double* __restrict__ a, const double* __restrict__ b, int64_t n) {
+    GRID_STRIDE(i, n) a[i] += b[i];
 }
 
 // CG updates: x += alpha p, r -= alpha q (alpha = num/den from the device)
@@ -195,7 +196,7 @@ void Operator::apply(const double* x, double* y, cudaStream_t s) const {
             k_mask<<<grid_for(A.n, 256), 256, 0, s>>>(tmp.get(), A.dirichlet, A.n);
             UP3D_CHECK_LAUNCH();
         }
-        k_add_to<<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), y, A.n);
+        k_accumulate<<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), A.n);
         UP3D_CHECK_LAUNCH();
     }
 }
@@ -282,6 +283,28 @@ int cg_solve(const Operator& op, const double* b, double* x, double rtol, double
 
 // ------------------------------------------------------------ GMRES
 
+// V_{col+1} *= 1 / |w| unless |w| <= eps |w_before| (Arnoldi breakdown);
+// hn = (|w_before|^2, |w|^2)
+__global__ void k_scale_unless_breakdown(double* __restrict__ v, const double* __restrict__ hn, double eps,
+                                         int64_t n) {
+    const double h0 = sqrt(hn[0]), h1 = sqrt(hn[1]);
+    if (h1 <= eps * h0) return;
+    const double f = 1.0 / h1;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] *= f;
+}
+
+// Page-locked host scratch for small readbacks.
+struct PinnedBuf {
+    double* p = nullptr;
+    explicit PinnedBuf(size_t n) { UP3D_CUDA(cudaMallocHost(&p, sizeof(double) * std::max<size_t>(n, 1))); }
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+};
+
 // Givens rotation as LAPACK xLARTG: c*f + s*g = r, -s*f + c*g = 0.
 static void lartg(double f, double g, double& c, double& sn, double& r) {
     if (g == 0.0) {
@@ -313,7 +336,9 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
     r.alloc(n);
     tmp.alloc(n);
     DBuf<double> hdev;
-    hdev.alloc(2 * (restart + 2));
+    hdev.alloc(2 * (restart + 1) + 2);
+    PinnedBuf hpin(restart + 3);
+    double* hbuf = hpin.p;
     std::vector<double> H((size_t)restart * (restart + 1), 0.0), gc(restart), gs(restart), S(restart + 1);
     const double bnrm = bl.nrm2(b, n);
     double atol_eff = eff_atol(atol, rtol, bnrm);
@@ -351,30 +376,36 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
         bool breakdown = false;
         int col = 0;
         for (col = 0; col < restart; ++col) {
+            // one Arnoldi step on the device, one readback: the column
+            // [h_0 .. h_col] (CGS2: two projections onto V_0..V_col, summed),
+            // |w| before and after the projections
+            double* hsum = hdev.get();
+            double* hpass = hdev.get() + (restart + 1);
+            double* hn = hdev.get() + 2 * (restart + 1);
             op.apply(V.get() + (size_t)col * n, tmp.get(), s);
             precond_apply(M, tmp.get(), w.get(), n, s);
-            const double h0 = bl.nrm2(w.get(), n);
-            // CGS2: two projections onto V_0..V_col
-            std::vector<double> hsum(col + 1, 0.0);
-            for (int pass = 0; pass < 2; ++pass) {
-                bl.multidot(V.get(), n, col + 1, w.get(), n, hdev.get());
-                bl.multiaxpy(V.get(), n, col + 1, hdev.get(), w.get(), n);
-                std::vector<double> hh(col + 1);
-                UP3D_CUDA(cudaMemcpyAsync(hh.data(), hdev.get(), sizeof(double) * (col + 1), cudaMemcpyDeviceToHost,
-                                          s));
-                UP3D_CUDA(cudaStreamSynchronize(s));
-                for (int k = 0; k <= col; ++k) hsum[k] += hh[k];
-            }
-            for (int k = 0; k <= col; ++k) Hat(col, k) = hsum[k];
-            const double h1 = bl.nrm2(w.get(), n);
-            Hat(col, col + 1) = h1;
+            bl.multidot(w.get(), 0, 1, w.get(), n, hn);
+            bl.multidot(V.get(), n, col + 1, w.get(), n, hsum);
+            bl.multiaxpy(V.get(), n, col + 1, hsum, w.get(), n);
+            bl.multidot(V.get(), n, col + 1, w.get(), n, hpass);
+            bl.multiaxpy(V.get(), n, col + 1, hpass, w.get(), n);
+            k_accumulate<<<1, 64, 0, s>>>(hsum, hpass, col + 1);
+            UP3D_CHECK_LAUNCH();
+            bl.multidot(w.get(), 0, 1, w.get(), n, hn + 1);
             UP3D_CUDA(cudaMemcpyAsync(V.get() + (size_t)(col + 1) * n, w.get(), sizeof(double) * n,
                                       cudaMemcpyDeviceToDevice, s));
+            k_scale_unless_breakdown<<<grid_for(n, 256), 256, 0, s>>>(V.get() + (size_t)(col + 1) * n, hn, eps, n);
+            UP3D_CHECK_LAUNCH();
+            UP3D_CUDA(cudaMemcpyAsync(hbuf, hsum, sizeof(double) * (col + 1), cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaMemcpyAsync(hbuf + col + 1, hn, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaStreamSynchronize(s));
+            for (int k = 0; k <= col; ++k) Hat(col, k) = hbuf[k];
+            const double h0 = std::sqrt(hbuf[col + 1]);
+            const double h1 = std::sqrt(hbuf[col + 2]);
+            Hat(col, col + 1) = h1;
             if (h1 <= eps * h0) {
                 Hat(col, col + 1) = 0.0;
                 breakdown = true;
-            } else {
-                bl.scale(V.get() + (size_t)(col + 1) * n, 1.0 / h1, n);
             }
             for (int k = 0; k < col; ++k) {
                 double c = gc[k], sn = gs[k];
