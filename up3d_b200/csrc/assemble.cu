@@ -11,13 +11,13 @@
 // bit-reproducible run to run, as the reference's colour-ordered scatter is
 // (kernels/jacobian.py:1-33, kernels/residual.py:44-76).
 //
-// Term 3 (upstream coupling, off the element pattern) is built per call
-// from the active elements in ascending order as COO triplets, stably
-// sorted and summed per (row, column) -- the reference's fill_term3_coo +
-// COO -> CSR merge (kernels/jacobian.py:184-229, :344-358).
+// Term 3 (upstream coupling, off the element pattern) is built per call,
+// row by row: each row's entries from its incident active elements in
+// ascending element order, stably sorted by column in shared memory and
+// summed per column -- the order of the reference's fill_term3_coo + COO ->
+// CSR merge (kernels/jacobian.py:184-229, :344-358), without a global sort.
 
 #include <cub/cub.cuh>
-#include <thrust/iterator/counting_iterator.h>
 
 #include "elem.cuh"
 #include "internal.cuh"
@@ -393,70 +393,133 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
 
 // ------------------------------------------------------------ Term 3
 
-// fill_term3_coo (kernels/jacobian.py:184-229): 16 entries per active
-// element, rows nodes(e) x cols nodes(u(e)), slot 16a + 4i + k.
-__global__ void k_t3_coo(const int32_t* __restrict__ active, const int64_t* __restrict__ n_active,
-                         const int4* __restrict__ conn, const int32_t* __restrict__ up,
-                         const double* __restrict__ t3v, uint64_t* __restrict__ keys, double* __restrict__ vals,
-                         int32_t* __restrict__ perm) {
-    const int64_t A = *n_active;
-    GRID_STRIDE(a, A) {
-        int64_t e = active[a];
-        int64_t u = up[e];
-        int4 ce = conn[e], cu = conn[u];
-        int re[4] = {ce.x, ce.y, ce.z, ce.w};
-        int cl[4] = {cu.x, cu.y, cu.z, cu.w};
-        const double* t = t3v + 8 * e;
-        for (int i = 0; i < 4; ++i) {
-            const double wi = t[i];
-            for (int k = 0; k < 4; ++k) {
-                int64_t idx = 16 * a + 4 * i + k;
-                keys[idx] = ((uint64_t)(uint32_t)re[i] << 32) | (uint32_t)cl[k];
-                vals[idx] = wi * t[4 + k];
-                perm[idx] = (int32_t)idx;
+// fill_term3_coo (kernels/jacobian.py:184-229) + the merge's duplicate
+// sums (:344-358), one warp per row n.  An active element e (t3flag) with
+// n = nodes(e)_i adds (n, nodes(u(e))_k, a_i b_k) for k = 0..3, where
+// t3v[e] = (a_0..a_3, b_0..b_3).  The row's entries, in (element, k) order
+// -- the COO order restricted to the row -- are stably sorted by column;
+// each column's run is summed left to right and either added to the P1
+// slot (data) or, off the pattern, written to the row's extras scratch at
+// 4 ent_off[n] (at most 4 deg(n) columns), with the count in x_cnt[n].
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_t3_rows(int64_t N, int cap, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
+              const uint8_t* __restrict__ flag, const int32_t* __restrict__ up, const int4* __restrict__ conn,
+              const double* __restrict__ t3v, const int32_t* __restrict__ indptr,
+              const int32_t* __restrict__ indices, double* __restrict__ data, int32_t* __restrict__ xs_col,
+              double* __restrict__ xs_val, int32_t* __restrict__ x_cnt) {
+    extern __shared__ __align__(16) unsigned char t3_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t* col0 = reinterpret_cast<int32_t*>(t3_smem) + (size_t)w * cap;
+    int32_t* col1 = reinterpret_cast<int32_t*>(t3_smem) + (size_t)(WARPS + w) * cap;
+    double* val0 = reinterpret_cast<double*>(t3_smem + (size_t)2 * WARPS * cap * sizeof(int32_t)) + (size_t)w * cap;
+    double* val1 = reinterpret_cast<double*>(t3_smem + (size_t)2 * WARPS * cap * sizeof(int32_t)) +
+                   (size_t)(WARPS + w) * cap;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < N; n += n_warps) {
+        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
+        // 1. the row's entries in (element, k) order
+        int P = 0;
+        for (int base = 0; base < deg; base += 32) {
+            const int j = base + lane;
+            uint32_t x = 0;
+            bool act = false;
+            if (j < deg) {
+                x = ent[eb + j];
+                act = flag[x >> 2] != 0;
             }
+            const unsigned m = __ballot_sync(0xffffffffu, act);
+            if (act) {
+                const int64_t e = x >> 2;
+                const int i = x & 3;
+                const int4 cu = conn[up[e]];
+                const double* t = t3v + 8 * e;
+                const double ai = t[i];
+                const int pos = P + 4 * __popc(m & lt);
+                col0[pos] = cu.x;
+                col0[pos + 1] = cu.y;
+                col0[pos + 2] = cu.z;
+                col0[pos + 3] = cu.w;
+                val0[pos] = ai * t[4];
+                val0[pos + 1] = ai * t[5];
+                val0[pos + 2] = ai * t[6];
+                val0[pos + 3] = ai * t[7];
+            }
+            P += 4 * __popc(m);
+        }
+        if (P == 0) {
+            if (lane == 0) x_cnt[n] = 0;
+            continue;
+        }
+        __syncwarp();
+        // 2. stable sort by column (rank = smaller columns + equal columns before)
+        for (int p = lane; p < P; p += 32) {
+            const int32_t c = col0[p];
+            int r = 0;
+            for (int q = 0; q < P; ++q) {
+                const int32_t cq = col0[q];
+                r += (cq < c) || (cq == c && q < p);
+            }
+            col1[r] = c;
+            val1[r] = val0[p];
+        }
+        __syncwarp();
+        // 3. per-column sums: into the pattern, else to the extras
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb;
+        int X = 0;
+        for (int base = 0; base < P; base += 32) {
+            const int p = base + lane;
+            const bool head = p < P && (p == 0 || col1[p] != col1[p - 1]);
+            bool extra = false;
+            int32_t c = 0;
+            double v = 0.0;
+            if (head) {
+                c = col1[p];
+                for (int q = p; q < P && col1[q] == c; ++q) v += val1[q];
+                int32_t lo = 0, hi = L;
+                while (lo < hi) {
+                    const int32_t mid = (lo + hi) >> 1;
+                    if (indices[rb + mid] < c) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < L && indices[rb + lo] == c) data[rb + lo] += v;
+                else extra = true;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, extra);
+            if (extra) {
+                const int64_t o = 4 * (int64_t)eb + X + __popc(m & lt);
+                xs_col[o] = c;
+                xs_val[o] = v;
+            }
+            X += __popc(m);
+        }
+        if (lane == 0) x_cnt[n] = X;
+        __syncwarp();
+    }
+}
+
+// Extras of every row, compacted in (row, column) order.
+__global__ void k_t3_compact(int64_t N, const int32_t* __restrict__ ent_off, const int32_t* __restrict__ x_ptr,
+                             const int32_t* __restrict__ xs_col, const double* __restrict__ xs_val,
+                             int32_t* __restrict__ x_row, int32_t* __restrict__ x_col, double* __restrict__ x_val) {
+    GRID_STRIDE(n, N) {
+        const int32_t o = x_ptr[n], cnt = x_ptr[n + 1] - o;
+        const int64_t src = 4 * (int64_t)ent_off[n];
+        for (int32_t j = 0; j < cnt; ++j) {
+            x_row[o + j] = (int32_t)n;
+            x_col[o + j] = xs_col[src + j];
+            x_val[o + j] = xs_val[src + j];
         }
     }
 }
 
-__global__ void k_t3_heads(const uint64_t* __restrict__ keys, int64_t n, int32_t* __restrict__ head) {
-    GRID_STRIDE(i, n) head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
-}
-
-// One thread per unique (row, col): the run's values in stable-sorted
-// (= COO) order, then the in-pattern part folded into the P1 data and the
-// rest kept as extras.
-__global__ void k_t3_reduce(const uint64_t* __restrict__ keys, const double* __restrict__ vals,
-                            const int32_t* __restrict__ perm, const int32_t* __restrict__ seg, int64_t n,
-                            const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                            double* __restrict__ data, int32_t* __restrict__ xrow, int32_t* __restrict__ xcol,
-                            double* __restrict__ xval, int32_t* __restrict__ xflag) {
-    GRID_STRIDE(i, n) {
-        if (!(i == 0 || keys[i] != keys[i - 1])) continue;
-        int64_t j = i;
-        double v = 0.0;
-        while (j < n && keys[j] == keys[i]) {
-            v += vals[perm[j]];
-            ++j;
-        }
-        int32_t row = (int32_t)(keys[i] >> 32), col = (int32_t)(keys[i] & 0xffffffffu);
-        int32_t rb = indptr[row], L = indptr[row + 1] - rb;
-        int32_t lo = 0, hi = L;
-        while (lo < hi) {
-            int32_t mid = (lo + hi) >> 1;
-            if (indices[rb + mid] < col) lo = mid + 1; else hi = mid;
-        }
-        int32_t s = seg[i];
-        if (lo < L && indices[rb + lo] == col) {
-            data[rb + lo] += v;
-            xflag[s] = 0;
-        } else {
-            xflag[s] = 1;
-        }
-        xrow[s] = row;
-        xcol[s] = col;
-        xval[s] = v;
-    }
+__global__ void k_count_flags(const uint8_t* __restrict__ f, int64_t n, unsigned long long* out) {
+    unsigned long long c = 0;
+    GRID_STRIDE(i, n) c += (f[i] != 0);
+    c = warp_sum_u64(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
 __global__ void k_count_nonzero(const double* __restrict__ v, int64_t n, unsigned long long* out) {
@@ -500,10 +563,6 @@ __global__ void k_merge_rows(int64_t N, const int32_t* __restrict__ indptr, cons
     }
 }
 
-__global__ void k_rows_from_extras(const int32_t* __restrict__ xrow, int64_t n, int32_t* __restrict__ cnt) {
-    GRID_STRIDE(i, n) atomicAdd(&cnt[xrow[i]], 1);
-}
-
 template <class T>
 void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
     size_t bytes = 0;
@@ -538,96 +597,52 @@ void launch_row_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
 // workspace, and returns (n_active, n_extra).  Synchronises the stream.
 // `known_active` >= 0 is the active count already known to the caller (0
 // skips everything).
+constexpr int T3_WARPS = 4;
 static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
                         int64_t known_active = -1) {
-    const int64_t E = m->E;
+    const int64_t E = m->E, N = m->N;
     n_extra = 0;
     m->last_extra = 0;
-    if (known_active == 0) {
-        n_active = 0;
-        m->last_active = 0;
-        return;
-    }
-    m->t3_active.alloc(E);
     m->i64_ws.alloc(8);
-    size_t bytes = 0;
-    thrust::counting_iterator<int32_t> it(0);
-    UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it, m->t3_flag.get(), m->t3_active.get(), m->i64_ws.get(),
-                                         E, s));
-    m->cub_tmp.alloc(bytes);
-    UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), bytes, it, m->t3_flag.get(), m->t3_active.get(),
-                                         m->i64_ws.get(), E, s));
-    UP3D_CUDA(cudaMemcpyAsync(&n_active, m->i64_ws.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaStreamSynchronize(s));
+    if (known_active < 0) {
+        unsigned long long* c = reinterpret_cast<unsigned long long*>(m->i64_ws.get());
+        UP3D_CUDA(cudaMemsetAsync(c, 0, sizeof(unsigned long long), s));
+        k_count_flags<<<grid_for(E, 256), 256, 0, s>>>(m->t3_flag.get(), E, c);
+        UP3D_CHECK_LAUNCH();
+        UP3D_CUDA(cudaMemcpyAsync(&known_active, c, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+    }
+    n_active = known_active;
     m->last_active = n_active;
     if (n_active == 0) return;
-    const int64_t n = 16 * n_active;
-    m->t3_keys.alloc(n);
-    m->t3_keys_s.alloc(n);
-    m->t3_vals.alloc(n);
-    m->t3_perm.alloc(n);
-    m->t3_perm_s.alloc(n);
-    m->t3_head.alloc(n);
-    m->t3_seg.alloc(n);
-    k_t3_coo<<<grid_for(n_active, 128), 128, 0, s>>>(m->t3_active.get(), m->i64_ws.get(), m->conn.get(),
-                                                     m->up32.get(), m->t3v.get(), m->t3_keys.get(),
-                                                     m->t3_vals.get(), m->t3_perm.get());
+    const int cap = 4 * std::max<int32_t>(m->max_deg, 1);
+    const size_t smem = (size_t)T3_WARPS * cap * 2 * (sizeof(int32_t) + sizeof(double));
+    UP3D_REQUIRE(smem <= 227 * 1024, UP3D_ERR_VALUE, "Term 3: node degree too large for the row kernel");
+    if (smem > 48 * 1024)
+        UP3D_CUDA(cudaFuncSetAttribute(k_t3_rows<T3_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    m->x_col.alloc(16 * E);
+    m->x_val.alloc(16 * E);
+    m->extra_cnt.alloc(N + 1);
+    m->x_ptr.alloc(N + 1);
+    UP3D_CUDA(cudaMemsetAsync(m->extra_cnt.get() + N, 0, sizeof(int32_t), s));
+    k_t3_rows<T3_WARPS><<<grid_for(32 * N, T3_WARPS * 32, (int64_t)148 * 32), T3_WARPS * 32, smem, s>>>(
+        N, cap, m->ent_off.get(), m->ent.get(), m->t3_flag.get(), m->up32.get(), m->conn.get(), m->t3v.get(),
+        m->indptr.get(), m->indices.get(), data, m->x_col.get(), m->x_val.get(), m->extra_cnt.get());
     UP3D_CHECK_LAUNCH();
-    int end_bit = 32;
-    {
-        int b = 1;
-        while ((1ll << b) < m->N) ++b;
-        end_bit = 32 + b;
-    }
-    bytes = 0;
-    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, m->t3_keys.get(), m->t3_keys_s.get(),
-                                              m->t3_perm.get(), m->t3_perm_s.get(), n, 0, end_bit, s));
-    m->cub_tmp.alloc(bytes);
-    UP3D_CUDA(cub::DeviceRadixSort::SortPairs(m->cub_tmp.get(), bytes, m->t3_keys.get(), m->t3_keys_s.get(),
-                                              m->t3_perm.get(), m->t3_perm_s.get(), n, 0, end_bit, s));
-    k_t3_heads<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), n, m->t3_head.get());
-    UP3D_CHECK_LAUNCH();
-    scan(m, m->t3_head.get(), m->t3_seg.get(), n, s);
-    int32_t last_seg = 0, last_head = 0;
-    UP3D_CUDA(cudaMemcpyAsync(&last_seg, m->t3_seg.get() + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(&last_head, m->t3_head.get() + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    scan(m, m->extra_cnt.get(), m->x_ptr.get(), N + 1, s);
+    int32_t total = 0;
+    UP3D_CUDA(cudaMemcpyAsync(&total, m->x_ptr.get() + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaStreamSynchronize(s));
-    const int64_t n_uniq = (int64_t)last_seg + last_head;
-    m->x_row.alloc(n_uniq);
-    m->x_col.alloc(n_uniq);
-    m->x_val.alloc(n_uniq);
-    m->x_flag.alloc(n_uniq + 1);
-    k_t3_reduce<<<grid_for(n, 256), 256, 0, s>>>(m->t3_keys_s.get(), m->t3_vals.get(), m->t3_perm_s.get(),
-                                                 m->t3_seg.get(), n, m->indptr.get(), m->indices.get(), data,
-                                                 m->x_row.get(), m->x_col.get(), m->x_val.get(), m->x_flag.get());
-    UP3D_CHECK_LAUNCH();
-    // compact the extras (keeps the (row, col) order)
-    m->x_row_c.alloc(n_uniq);
-    m->x_col_c.alloc(n_uniq);
-    m->x_val_c.alloc(n_uniq);
-    auto compact = [&](auto* in, auto* out) {
-        size_t b2 = 0;
-        UP3D_CUDA(cub::DeviceSelect::Flagged(nullptr, b2, in, m->x_flag.get(), out, m->i64_ws.get() + 1, n_uniq, s));
-        m->cub_tmp.alloc(b2);
-        UP3D_CUDA(cub::DeviceSelect::Flagged(m->cub_tmp.get(), b2, in, m->x_flag.get(), out, m->i64_ws.get() + 1,
-                                             n_uniq, s));
-    };
-    compact(m->x_row.get(), m->x_row_c.get());
-    compact(m->x_col.get(), m->x_col_c.get());
-    compact(m->x_val.get(), m->x_val_c.get());
-    UP3D_CUDA(cudaMemcpyAsync(&n_extra, m->i64_ws.get() + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaStreamSynchronize(s));
+    n_extra = total;
     m->last_extra = n_extra;
-    // extras row pointer
-    m->x_ptr.alloc(m->N + 1);
-    UP3D_CUDA(cudaMemsetAsync(m->x_ptr.get(), 0, sizeof(int32_t) * (m->N + 1), s));
     if (n_extra > 0) {
-        m->extra_cnt.alloc(m->N + 1);
-        UP3D_CUDA(cudaMemsetAsync(m->extra_cnt.get(), 0, sizeof(int32_t) * (m->N + 1), s));
-        k_rows_from_extras<<<grid_for(n_extra, 256), 256, 0, s>>>(m->x_row_c.get(), n_extra, m->extra_cnt.get());
+        m->x_row_c.alloc(n_extra);
+        m->x_col_c.alloc(n_extra);
+        m->x_val_c.alloc(n_extra);
+        k_t3_compact<<<grid_for(N, 256), 256, 0, s>>>(N, m->ent_off.get(), m->x_ptr.get(), m->x_col.get(),
+                                                      m->x_val.get(), m->x_row_c.get(), m->x_col_c.get(),
+                                                      m->x_val_c.get());
         UP3D_CHECK_LAUNCH();
-        scan(m, m->extra_cnt.get(), m->x_ptr.get(), m->N + 1, s);
-        UP3D_CUDA(cudaStreamSynchronize(s));
     }
 }
 

@@ -136,18 +136,15 @@ struct up3d_mesh {
     up3d::DBuf<int32_t> up32;          // (E) upstream (internal)
     up3d::DBuf<double> grad_ws;        // (E, 3)
     up3d::DBuf<double> q2_ws;          // (E)
-    up3d::DBuf<int32_t> extra_cnt;     // (N+1) Term-3 extras per row, then scanned
-    up3d::DBuf<int32_t> extra_col;     // extras
-    up3d::DBuf<double> extra_val;
+    up3d::DBuf<int32_t> extra_cnt;     // (N+1) Term-3 extras per row
     up3d::DBuf<unsigned char> cub_tmp;
-    // Term-3 scratch (grown on demand)
-    up3d::DBuf<uint8_t> t3_flag;
-    up3d::DBuf<int32_t> t3_active;
-    up3d::DBuf<uint64_t> t3_keys, t3_keys_s;
-    up3d::DBuf<double> t3_vals;
-    up3d::DBuf<int32_t> t3_perm, t3_perm_s, t3_head, t3_seg;
-    up3d::DBuf<int32_t> x_row, x_col, x_flag, x_ptr, x_row_c, x_col_c;
-    up3d::DBuf<double> x_val, x_val_c;
+    // Term 3 (grown on demand)
+    up3d::DBuf<uint8_t> t3_flag;       // (E) active elements
+    up3d::DBuf<int32_t> x_col;         // (16E) per-row extras scratch at 4 ent_off[n]
+    up3d::DBuf<double> x_val;
+    up3d::DBuf<int32_t> x_ptr;         // (N+1) extras row pointer
+    up3d::DBuf<int32_t> x_row_c, x_col_c;  // extras, (row, col) order
+    up3d::DBuf<double> x_val_c;
     up3d::DBuf<up3d_monitors> mon_ws;  // (1)
     up3d::DBuf<int64_t> i64_ws;        // small scalars
     int64_t last_extra = 0;            // extras of the last Jacobian
