@@ -327,6 +327,20 @@ int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double a
 int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double* x,
                double rtol, double atol, int restart, int maxiter, up3d_precond* M,
                int64_t* inner, double* resid, int* info, up3d_stream stream);
+/* Mixed-precision GMRES with FP64 iterative refinement (the mixed form of
+ * the Newton linear solve the reference does with spla.gmres,
+ * solve/newton.py:1029-1040).  The outer loop forms r = b - A x with A's
+ * FP64 values and stops at ||r|| <= max(rtol ||b||, atol) or after
+ * refine_max corrections; each correction solves A d = r by restarted
+ * GMRES in FP32 -- A's FP32 values `data32` (and `extra32` for `extra`),
+ * FP32 vectors, M applied in FP32 (an FP32 AMG hierarchy keeps its
+ * coarsest solve in FP64) -- to max(inner_rtol, tol / ||r||) relative, and
+ * is added to x in FP64.  inner = total Arnoldi steps, outer = corrections.
+ * Synchronous. */
+int up3d_gmres_ir(const up3d_csr* A, const up3d_csr* extra, const float* data32,
+                  const float* extra32, const double* b, double* x, double rtol, double atol,
+                  int restart, int maxiter, int refine_max, double inner_rtol, up3d_precond* M,
+                  int64_t* inner, int64_t* outer, double* resid, int* info, up3d_stream stream);
 
 /* ------------------------------------------------ allocation-free solve */
 

@@ -67,3 +67,19 @@ def test_transonic_newton_converges_on_reference_equations():
     else:
         assert r_live < 2e-10
         assert live["n_supersonic"] == res["n_supersonic"]
+
+
+def test_mixed_precision_newton_matches_fp64():
+    """Newton with FP32 Jacobian SpMV and FP32 AMG inside FP64-refined
+    GMRES reaches the FP64 solve's potential (residual, update and test in
+    FP64) on a 40x12x10 channel at M0.80."""
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    mesh = bump_channel(40, 12, 10, amplitude=0.08, seed=0)
+    ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+    r64 = solve_newton_transonic(ws, 0.80, m_start=0.70, dm=0.05)
+    ws2 = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+    r32 = solve_newton_transonic(ws2, 0.80, m_start=0.70, dm=0.05, precision="mixed")
+    assert r64["converged"] and r32["converged"]
+    assert r32["residual_history"][-1] < 1e-10 and r32["n_refinements"] > 0
+    assert np.abs(r32["phi"].cpu().numpy() - r64["phi"].cpu().numpy()).max() < 1e-8

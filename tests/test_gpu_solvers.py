@@ -162,3 +162,36 @@ def test_cg_amg_drop_in(c1_system):
     x, n_it = solve_cg_amg(As, b, rtol=1e-10)
     assert isinstance(x, np.ndarray)
     assert np.linalg.norm(As @ x - b) <= 1e-10 * np.linalg.norm(b) * 1.01
+
+
+def test_gmres_mixed_refines_to_fp64_accuracy(c1_golden):
+    """FP32 inner GMRES (FP32 Jacobian values, FP32 AMG) with FP64 refinement
+    reaches the FP64 direct solution of the C1 Newton system at the
+    subsonic seeded state; one FP32 solve alone does not."""
+    import torch
+    from up3d_b200.kernels.jacobian import PicardOperator
+    from up3d_b200.solve.linear import build_amg_preconditioner, solve_gmres_mixed, with_dirichlet
+    g = c1_golden
+    op = PicardOperator(g.mesh("nodes"), g.mesh("elements"))
+    label = "seed0_m05"
+    rt = torch.from_numpy(g.state(label, "rho_tilde")).cuda()
+    phi = torch.from_numpy(g.state(label, "phi")).cuda()
+    J = op.assemble_newton_jacobian(phi, rt, torch.from_numpy(g.state(label, "s_e")).cuda(),
+                                    torch.from_numpy(g.state(label, "s_u")).cuda(),
+                                    torch.from_numpy(g.state(label, "upstream").astype(np.int64)).cuda())
+    dn = g.mesh("dirichlet_nodes")
+    n = op.n_nodes
+    free = np.setdiff1d(np.arange(n), dn)
+    mask = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    mask[torch.from_numpy(dn).cuda()] = 1
+    b = np.random.default_rng(5).standard_normal(n)
+    b[dn] = 0.0
+    _, M = build_amg_preconditioner(with_dirichlet(op.assemble_matrix(rt), mask), fp32=True)
+    Jf = with_dirichlet(J, mask)
+    bd = torch.from_numpy(b).cuda()
+    x, n_inner, n_ref, info = solve_gmres_mixed(Jf, bd, M=M, rtol=1e-12, restart=50, maxiter=20)
+    assert info == 0 and n_ref >= 2 and n_inner > 0
+    ref = _direct(J, free, b)
+    assert rel_err(x.cpu().numpy(), ref) < 1e-9
+    x1, _, _, _ = solve_gmres_mixed(Jf, bd, M=M, rtol=1e-12, restart=50, maxiter=20, refine_max=1)
+    assert rel_err(x1.cpu().numpy(), ref) > 1e-9

@@ -98,6 +98,9 @@ SIGNATURES = {
                        ctypes.POINTER(_int), _p]),
     "up3d_gmres": (_int, [_p, _p, _p, _p, _d, _d, _int, _int, _p, ctypes.POINTER(_i64),
                           ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
+    "up3d_gmres_ir": (_int, [_p, _p, _p, _p, _p, _p, _d, _d, _int, _int, _int, _d, _p,
+                             ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_d),
+                             ctypes.POINTER(_int), _p]),
     "up3d_cg_jacobi_noalloc": (_int, [_p, _p, _p, _d, _d, _int, ctypes.POINTER(_i64),
                                       ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
 }

@@ -641,11 +641,13 @@ struct Amg {
     // one V-cycle as a CUDA graph per (input, output) pair: captured on a
     // private stream at first use, replayed on the caller's stream
     struct Graph {
-        const double* r;
-        double* z;
+        const void* r;
+        void* z;
+        bool f32;  // FP32 input and output
         cudaGraphExec_t exec;
         long long launches;
     };
+    DBuf<double> io64_in, io64_out;  // FP32 input/output through an FP64 hierarchy
     std::vector<Graph> graphs;
     cudaStream_t capture_stream = nullptr;
     int device = 0;
@@ -831,7 +833,7 @@ void fill_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
 }
 
 template <class T>
-void make_levels(Amg& a, std::vector<Level<T>*>& Lv, const uint8_t* dir_dev, cudaStream_t s) {
+void make_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
     for (size_t l = 0; l < a.sym.size(); ++l) {
         SymLevel& F = *a.sym[l];
         auto* lv = new Level<T>();
@@ -846,7 +848,8 @@ void make_levels(Amg& a, std::vector<Level<T>*>& Lv, const uint8_t* dir_dev, cud
             lv->R.copy_pattern(F.R, s);
             lv->dinv.alloc(n);
         }
-        if (l == 0) lv->dir = dir_dev;
+        // lv->dir stays null: the embedded finest operator already has
+        // identity rows and no constrained columns
     }
 }
 
@@ -896,14 +899,37 @@ void restore_buffers(std::vector<Level<T>*>& L, const std::vector<std::pair<T*, 
     }
 }
 
-void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
-    Amg& a = *static_cast<Amg*>(p);
+// One V-cycle with FP32 input and output.
+void amg_cycle_f32(Amg& a, const float* r, float* z, cudaStream_t s) {
+    if (a.fp32) {
+        Level<float>& f = *a.Lf[0];
+        const int64_t n = f.A.n;
+        UP3D_CUDA(cudaMemcpyAsync(f.b.get(), r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+        vcycle<float>(a, a.Lf, 0, s);
+        UP3D_CUDA(cudaMemcpyAsync(z, f.x.get(), sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        const int64_t n = a.Ld[0]->A.n;
+        k_f2d<<<grid_for(n, 256), 256, 0, s>>>(r, a.io64_in.get(), n);
+        UP3D_CHECK_LAUNCH();
+        amg_cycle(a, a.io64_in.get(), a.io64_out.get(), s);
+        k_d2f<<<grid_for(n, 256), 256, 0, s>>>(a.io64_out.get(), z, n);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+// Replays the cached graph of one V-cycle for (r, z), capturing it first.
+void apply_graph(Amg& a, const void* r, void* z, bool f32, cudaStream_t s) {
     for (auto& g : a.graphs)
-        if (g.r == r && g.z == z) {
+        if (g.r == r && g.z == z && g.f32 == f32) {
             UP3D_CUDA(cudaGraphLaunch(g.exec, s));
             count_launch((int)g.launches);
             return;
         }
+    if (f32 && !a.fp32) {
+        const int64_t n = a.Ld[0]->A.n;
+        a.io64_in.alloc(n);  // before the capture
+        a.io64_out.alloc(n);
+    }
     if (!a.capture_stream) UP3D_CUDA(cudaStreamCreateWithFlags(&a.capture_stream, cudaStreamNonBlocking));
     auto sd = save_buffers(a.Ld);
     auto sf = save_buffers(a.Lf);
@@ -911,7 +937,8 @@ void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
     cudaGraph_t graph = nullptr;
     UP3D_CUDA(cudaStreamBeginCapture(a.capture_stream, cudaStreamCaptureModeThreadLocal));
     try {
-        amg_cycle(a, r, z, a.capture_stream);
+        if (f32) amg_cycle_f32(a, static_cast<const float*>(r), static_cast<float*>(z), a.capture_stream);
+        else amg_cycle(a, static_cast<const double*>(r), static_cast<double*>(z), a.capture_stream);
     } catch (...) {
         cudaStreamEndCapture(a.capture_stream, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -932,9 +959,17 @@ void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
         cudaGraphExecDestroy(a.graphs.front().exec);
         a.graphs.erase(a.graphs.begin());
     }
-    a.graphs.push_back({r, z, exec, launches});
+    a.graphs.push_back({r, z, f32, exec, launches});
     UP3D_CUDA(cudaGraphLaunch(exec, s));
     count_launch((int)launches);
+}
+
+void amg_apply(void* p, const double* r, double* z, cudaStream_t s) {
+    apply_graph(*static_cast<Amg*>(p), r, z, false, s);
+}
+
+void amg_apply_f32(void* p, const float* r, float* z, cudaStream_t s) {
+    apply_graph(*static_cast<Amg*>(p), r, z, true, s);
 }
 
 void amg_destroy(void* p) { delete static_cast<Amg*>(p); }
@@ -1057,12 +1092,11 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
                                                                 a->sym[0]->A.x.get());
         UP3D_CHECK_LAUNCH();
         numeric(*a, s);
-        const uint8_t* dir_dev = A.dirichlet ? a->in_dir.get() : nullptr;
         if (a->fp32) {
-            make_levels<float>(*a, a->Lf, dir_dev, s);
+            make_levels<float>(*a, a->Lf, s);
             fill_levels<float>(*a, a->Lf, s);
         } else {
-            make_levels<double>(*a, a->Ld, dir_dev, s);
+            make_levels<double>(*a, a->Ld, s);
             fill_levels<double>(*a, a->Ld, s);
         }
         UP3D_CUDA(cudaStreamSynchronize(s));

@@ -12,6 +12,7 @@
 // each Arnoldi step is two batched multi-dot / multi-axpy passes.
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "internal.cuh"
@@ -31,52 +32,63 @@ constexpr int RGRID = 592;   // fixed partial count (4 x 148 SMs): reproducible 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) sh[w] = v;
-    __syncthreads();
-    double t = 0.0;
-    if (w == 0) {
-        t = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
-        t = warp_sum(t);
-    }
-    __syncthreads();
-    return t;
-}
-
-// partial[b*K + k] = sum over this block's slice of x_k . y   (K vectors of V)
+// partial[b*K + k] = sum over this block's slice of x_k . y (K vectors of
+// V), MD_KT dot products per pass: y is read once per MD_KT vectors and one
+// block reduction serves them all.  Products and sums in FP64 whatever the
+// vector type.
+constexpr int MD_KT = 8;
+template <class T>
 __global__ void __launch_bounds__(RB)
-    k_multidot(const double* __restrict__ V, int64_t ldv, int K, const double* __restrict__ y, int64_t n,
+    k_multidot(const T* __restrict__ V, int64_t ldv, int K, const T* __restrict__ y, int64_t n,
                double* __restrict__ partial) {
-    __shared__ double sh[32];
-    for (int k = 0; k < K; ++k) {
-        const double* x = V + k * ldv;
-        double acc = 0.0;
-        GRID_STRIDE(i, n) acc += x[i] * y[i];
-        double t = block_sum(acc, sh);
-        if (threadIdx.x == 0) partial[blockIdx.x * K + k] = t;
+    __shared__ double sh[MD_KT][RB / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k0 = 0; k0 < K; k0 += MD_KT) {
+        const int kt = min(MD_KT, K - k0);
+        double acc[MD_KT];
+#pragma unroll
+        for (int j = 0; j < MD_KT; ++j) acc[j] = 0.0;
+        GRID_STRIDE(i, n) {
+            const double yi = (double)y[i];
+#pragma unroll
+            for (int j = 0; j < MD_KT; ++j)
+                if (j < kt) acc[j] += (double)V[(int64_t)(k0 + j) * ldv + i] * yi;
+        }
+#pragma unroll
+        for (int j = 0; j < MD_KT; ++j) {
+            const double v = warp_sum(acc[j]);
+            if (lane == 0) sh[j][w] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < kt) {
+            double t = 0.0;
+#pragma unroll
+            for (int q = 0; q < RB / 32; ++q) t += sh[threadIdx.x][q];
+            partial[(int64_t)blockIdx.x * K + k0 + threadIdx.x] = t;
+        }
+        __syncthreads();
     }
 }
 
-// out[k] = sum_b partial[b*K + k], fixed order.
+// out[k] = sum_b partial[b*K + k], fixed order: one warp per k.
 __global__ void k_finish(const double* __restrict__ partial, int nb, int K, double* __restrict__ out) {
-    __shared__ double sh[32];
-    for (int k = 0; k < K; ++k) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = w; k < K; k += nw) {
         double acc = 0.0;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[b * K + k];
-        double t = block_sum(acc, sh);
-        if (threadIdx.x == 0) out[k] = t;
+        for (int b = lane; b < nb; b += 32) acc += partial[(int64_t)b * K + k];
+        acc = warp_sum(acc);
+        if (lane == 0) out[k] = acc;
     }
 }
 
 // y -= sum_k h[k] V_k  (h on the device)
-__global__ void k_multiaxpy(const double* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h,
-                            double* __restrict__ y, int64_t n) {
+template <class T>
+__global__ void k_multiaxpy(const T* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h,
+                            T* __restrict__ y, int64_t n) {
     GRID_STRIDE(i, n) {
-        double acc = y[i];
-        for (int k = 0; k < K; ++k) acc -= h[k] * V[k * ldv + i];
-        y[i] = acc;
+        double acc = (double)y[i];
+        for (int k = 0; k < K; ++k) acc -= h[k] * (double)V[k * ldv + i];
+        y[i] = (T)acc;
     }
 }
 
@@ -84,18 +96,29 @@ __global__ void k_axpby(double a, const double* __restrict__ x, double b, double
     GRID_STRIDE(i, n) y[i] = a * x[i] + b * y[i];
 }
 
-__global__ void k_scale(double* __restrict__ x, double a, int64_t n) {
-    GRID_STRIDE(i, n) x[i] *= a;
+template <class T>
+__global__ void k_scale(T* __restrict__ x, double a, int64_t n) {
+    GRID_STRIDE(i, n) x[i] = (T)((double)x[i] * a);
 }
 
-__global__ void k_sub(const double* __restrict__ b, const double* __restrict__ ax, double* __restrict__ r,
-                      int64_t n) {
+template <class T>
+__global__ void k_sub(const T* __restrict__ b, const T* __restrict__ ax, T* __restrict__ r, int64_t n) {
     GRID_STRIDE(i, n) r[i] = b[i] - ax[i];
 }
 
 // a += b
-__global__ void k_accumulate(double* __restrict__ a, const double* __restrict__ b, int64_t n) {
+template <class T>
+__global__ void k_accumulate(T* __restrict__ a, const T* __restrict__ b, int64_t n) {
     GRID_STRIDE(i, n) a[i] += b[i];
+}
+
+// x += (double) d
+__global__ void k_add_f32(double* __restrict__ x, const float* __restrict__ d, int64_t n) {
+    GRID_STRIDE(i, n) x[i] += (double)d[i];
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    GRID_STRIDE(i, n) b[i] = (float)a[i];
 }
 
 // CG updates: x += alpha p, r -= alpha q (alpha = num/den from the device)
@@ -127,12 +150,14 @@ __global__ void k_jacobi_diag(int64_t n, const int32_t* __restrict__ indptr, con
     }
 }
 
-__global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
-    GRID_STRIDE(i, n) out[i] = a[i] * b[i];
+template <class T>
+__global__ void k_mul(const double* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, int64_t n) {
+    GRID_STRIDE(i, n) out[i] = (T)(a[i] * (double)b[i]);
 }
 
-__global__ void k_mask(double* __restrict__ x, const uint8_t* __restrict__ dir, int64_t n) {
-    GRID_STRIDE(i, n) if (dir[i]) x[i] = 0.0;
+template <class T>
+__global__ void k_mask(T* __restrict__ x, const uint8_t* __restrict__ dir, int64_t n) {
+    GRID_STRIDE(i, n) if (dir[i]) x[i] = T(0);
 }
 
 __global__ void k_copy_scalar(const double* __restrict__ src, double* __restrict__ dst) { *dst = *src; }
@@ -150,38 +175,105 @@ Blas::~Blas() {
     if (host) cudaFreeHost(host);
 }
 
-void Blas::multidot(const double* V, int64_t ldv, int K, const double* y, int64_t n, double* out_dev) {
+template <class T>
+void Blas::multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev) {
     for (int k0 = 0; k0 < K; k0 += 64) {
         int kk = std::min(64, K - k0);
-        k_multidot<<<RGRID, RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n, partial.get());
+        k_multidot<T><<<RGRID, RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n, partial.get());
         UP3D_CHECK_LAUNCH();
         k_finish<<<1, 1024, 0, s>>>(partial.get(), RGRID, kk, out_dev + k0);
         UP3D_CHECK_LAUNCH();
     }
 }
 
-double Blas::dot(const double* x, const double* y, int64_t n) {
+template <class T>
+double Blas::dot(const T* x, const T* y, int64_t n) {
     multidot(x, 0, 1, y, n, scal.get());
     UP3D_CUDA(cudaMemcpyAsync(host, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaStreamSynchronize(s));
     return host[0];
 }
 
-double Blas::nrm2(const double* x, int64_t n) { return std::sqrt(dot(x, x, n)); }
+template <class T>
+double Blas::nrm2(const T* x, int64_t n) {
+    return std::sqrt(dot(x, x, n));
+}
 
 void Blas::axpby(double a, const double* x, double b, double* y, int64_t n) {
     k_axpby<<<grid_for(n, 256), 256, 0, s>>>(a, x, b, y, n);
     UP3D_CHECK_LAUNCH();
 }
 
-void Blas::scale(double* x, double a, int64_t n) {
-    k_scale<<<grid_for(n, 256), 256, 0, s>>>(x, a, n);
+template <class T>
+void Blas::scale(T* x, double a, int64_t n) {
+    k_scale<T><<<grid_for(n, 256), 256, 0, s>>>(x, a, n);
     UP3D_CHECK_LAUNCH();
 }
 
-void Blas::multiaxpy(const double* V, int64_t ldv, int K, const double* h_dev, double* y, int64_t n) {
-    k_multiaxpy<<<grid_for(n, 256), 256, 0, s>>>(V, ldv, K, h_dev, y, n);
+template <class T>
+void Blas::multiaxpy(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n) {
+    k_multiaxpy<T><<<grid_for(n, 256), 256, 0, s>>>(V, ldv, K, h_dev, y, n);
     UP3D_CHECK_LAUNCH();
+}
+
+#define UP3D_BLAS_INST(T)                                                                 \
+    template void Blas::multidot<T>(const T*, int64_t, int, const T*, int64_t, double*); \
+    template double Blas::dot<T>(const T*, const T*, int64_t);                           \
+    template double Blas::nrm2<T>(const T*, int64_t);                                    \
+    template void Blas::scale<T>(T*, double, int64_t);                                   \
+    template void Blas::multiaxpy<T>(const T*, int64_t, int, const double*, T*, int64_t);
+UP3D_BLAS_INST(double)
+UP3D_BLAS_INST(float)
+#undef UP3D_BLAS_INST
+
+// ------------------------------------------------------------ solver workspaces
+
+// Per-device Krylov workspaces, kept between solves so that a solve makes
+// no device or pinned allocation once the buffers have grown to its size
+// (cudaMalloc / cudaFree would synchronise the device on every call).  A
+// solve holds its device's lock for its whole duration: concurrent solves
+// on one device run one after the other.
+struct KrylovWs {
+    std::recursive_mutex mu;
+    Blas* bl = nullptr;
+    DBuf<double> d[8];
+    DBuf<float> f[8];
+    double* pin = nullptr;
+    size_t pin_n = 0;
+    double* pinned(size_t n) {
+        if (n > pin_n) {
+            if (pin) cudaFreeHost(pin);
+            pin = nullptr;
+            pin_n = 0;
+            UP3D_CUDA(cudaMallocHost(&pin, sizeof(double) * n));
+            pin_n = n;
+        }
+        return pin;
+    }
+    template <class T>
+    DBuf<T>* bufs();
+};
+template <>
+DBuf<double>* KrylovWs::bufs<double>() {
+    return d;
+}
+template <>
+DBuf<float>* KrylovWs::bufs<float>() {
+    return f;
+}
+
+KrylovWs& krylov_ws() {
+    static KrylovWs ws[64];
+    int dev = 0;
+    UP3D_CUDA(cudaGetDevice(&dev));
+    UP3D_REQUIRE(dev >= 0 && dev < 64, UP3D_ERR_RUNTIME, "device index out of range");
+    return ws[dev];
+}
+
+Blas& ws_blas(KrylovWs& w, cudaStream_t s) {
+    if (!w.bl) w.bl = new Blas(s);
+    w.bl->s = s;
+    return *w.bl;
 }
 
 // ------------------------------------------------------------ operators
@@ -193,10 +285,26 @@ void Operator::apply(const double* x, double* y, cudaStream_t s) const {
         tmp.alloc(A.n);
         launch_spmv<double>(A.n, extra.indptr, extra.indices, extra.data, x, tmp.get(), A.dirichlet, s);
         if (A.dirichlet) {
-            k_mask<<<grid_for(A.n, 256), 256, 0, s>>>(tmp.get(), A.dirichlet, A.n);
+            k_mask<double><<<grid_for(A.n, 256), 256, 0, s>>>(tmp.get(), A.dirichlet, A.n);
             UP3D_CHECK_LAUNCH();
         }
-        k_accumulate<<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), A.n);
+        k_accumulate<double><<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), A.n);
+        UP3D_CHECK_LAUNCH();
+    }
+}
+
+// FP32 operator: the FP32 copies of the values (data32, extra32).
+void Operator::apply(const float* x, float* y, cudaStream_t s) const {
+    UP3D_REQUIRE(data32 && (!extra.indptr || extra32), UP3D_ERR_ARGUMENT, "FP32 operator without FP32 values");
+    launch_spmv<float>(A.n, A.indptr, A.indices, data32, x, y, A.dirichlet, s);
+    if (extra.indptr) {
+        tmp32.alloc(A.n);
+        launch_spmv<float>(A.n, extra.indptr, extra.indices, extra32, x, tmp32.get(), A.dirichlet, s);
+        if (A.dirichlet) {
+            k_mask<float><<<grid_for(A.n, 256), 256, 0, s>>>(tmp32.get(), A.dirichlet, A.n);
+            UP3D_CHECK_LAUNCH();
+        }
+        k_accumulate<float><<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp32.get(), A.n);
         UP3D_CHECK_LAUNCH();
     }
 }
@@ -208,7 +316,7 @@ void Operator::apply(const double* x, double* y, cudaStream_t s) const {
 void up3d_precond::apply(const double* r, double* z, cudaStream_t s) {
     using namespace up3d;
     if (kind == 1) {
-        k_mul<<<grid_for(n, 256), 256, 0, s>>>(dinv.get(), r, z, n);
+        k_mul<double><<<grid_for(n, 256), 256, 0, s>>>(dinv.get(), r, z, n);
         UP3D_CHECK_LAUNCH();
     } else if (kind == 2) {
         amg_apply(amg, r, z, s);
@@ -217,13 +325,26 @@ void up3d_precond::apply(const double* r, double* z, cudaStream_t s) {
     }
 }
 
+void up3d_precond::apply(const float* r, float* z, cudaStream_t s) {
+    using namespace up3d;
+    if (kind == 1) {
+        k_mul<float><<<grid_for(n, 256), 256, 0, s>>>(dinv.get(), r, z, n);
+        UP3D_CHECK_LAUNCH();
+    } else if (kind == 2) {
+        amg_apply_f32(amg, r, z, s);
+    } else {
+        UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    }
+}
+
 namespace up3d {
 
-void precond_apply(up3d_precond* M, const double* r, double* z, int64_t n, cudaStream_t s) {
+template <class T>
+void precond_apply(up3d_precond* M, const T* r, T* z, int64_t n, cudaStream_t s) {
     if (M) {
         M->apply(r, z, s);
     } else {
-        UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
     }
 }
 
@@ -237,18 +358,23 @@ static double eff_atol(double atol, double rtol, double bnrm) { return std::max(
 int cg_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int maxiter, up3d_precond* M,
              int64_t* iters, double* resid, cudaStream_t s) {
     const int64_t n = op.A.n;
-    Blas bl(s);
-    DBuf<double> r, z, p, q;
+    KrylovWs& W = krylov_ws();
+    std::lock_guard<std::recursive_mutex> lock(W.mu);
+    Blas& bl = ws_blas(W, s);
+    DBuf<double>& r = W.d[0];
+    DBuf<double>& z = W.d[1];
+    DBuf<double>& p = W.d[2];
+    DBuf<double>& q = W.d[3];
+    DBuf<double>& sc = W.d[4];
     r.alloc(n);
     z.alloc(n);
     p.alloc(n);
     q.alloc(n);
-    DBuf<double> sc;
     sc.alloc(4);
     const double bnrm = bl.nrm2(b, n);
     const double tol = eff_atol(atol, rtol, bnrm);
     op.apply(x, q.get(), s);
-    k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, q.get(), r.get(), n);
+    k_sub<double><<<grid_for(n, 256), 256, 0, s>>>(b, q.get(), r.get(), n);
     UP3D_CHECK_LAUNCH();
     double rn = bl.nrm2(r.get(), n);
     int64_t it = 0;
@@ -285,25 +411,14 @@ int cg_solve(const Operator& op, const double* b, double* x, double rtol, double
 
 // V_{col+1} *= 1 / |w| unless |w| <= eps |w_before| (Arnoldi breakdown);
 // hn = (|w_before|^2, |w|^2)
-__global__ void k_scale_unless_breakdown(double* __restrict__ v, const double* __restrict__ hn, double eps,
-                                         int64_t n) {
+template <class T>
+__global__ void k_scale_unless_breakdown(T* __restrict__ v, const double* __restrict__ hn, double eps, int64_t n) {
     const double h0 = sqrt(hn[0]), h1 = sqrt(hn[1]);
     if (h1 <= eps * h0) return;
     const double f = 1.0 / h1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[i] *= f;
+        v[i] = (T)((double)v[i] * f);
 }
-
-// Page-locked host scratch for small readbacks.
-struct PinnedBuf {
-    double* p = nullptr;
-    explicit PinnedBuf(size_t n) { UP3D_CUDA(cudaMallocHost(&p, sizeof(double) * std::max<size_t>(n, 1))); }
-    ~PinnedBuf() {
-        if (p) cudaFreeHost(p);
-    }
-    PinnedBuf(const PinnedBuf&) = delete;
-    PinnedBuf& operator=(const PinnedBuf&) = delete;
-};
 
 // Givens rotation as LAPACK xLARTG: c*f + s*g = r, -s*f + c*g = 0.
 static void lartg(double f, double g, double& c, double& sn, double& r) {
@@ -325,25 +440,34 @@ static void lartg(double f, double g, double& c, double& sn, double& r) {
 
 // scipy.sparse.linalg.gmres (solve/linear.py:182-201): restarted,
 // left-preconditioned; `maxiter` counts restart cycles.
-int gmres_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart, int maxiter,
+// T: the vector (and operator value) type -- double, or float for the inner
+// solves of the mixed-precision refinement (dot products accumulate in
+// FP64, the Hessenberg least-squares problem is FP64 on the host).
+template <class T>
+int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, int restart, int maxiter,
                 up3d_precond* M, int64_t* inner, double* resid, cudaStream_t s) {
     const int64_t n = op.A.n;
-    Blas bl(s);
+    KrylovWs& W = krylov_ws();
+    std::lock_guard<std::recursive_mutex> lock(W.mu);
+    Blas& bl = ws_blas(W, s);
     restart = (int)std::min<int64_t>(restart, n);
-    DBuf<double> V, w, r, tmp;
+    DBuf<T>* B = W.bufs<T>();
+    DBuf<T>& V = B[0];
+    DBuf<T>& w = B[1];
+    DBuf<T>& r = B[2];
+    DBuf<T>& tmp = B[3];
+    DBuf<double>& hdev = W.d[5];
     V.alloc((size_t)(restart + 1) * n);
     w.alloc(n);
     r.alloc(n);
     tmp.alloc(n);
-    DBuf<double> hdev;
     hdev.alloc(2 * (restart + 1) + 2);
-    PinnedBuf hpin(restart + 3);
-    double* hbuf = hpin.p;
+    double* hbuf = W.pinned(restart + 3);
     std::vector<double> H((size_t)restart * (restart + 1), 0.0), gc(restart), gs(restart), S(restart + 1);
     const double bnrm = bl.nrm2(b, n);
     double atol_eff = eff_atol(atol, rtol, bnrm);
     if (bnrm == 0.0) {
-        UP3D_CUDA(cudaMemcpyAsync(x, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        UP3D_CUDA(cudaMemcpyAsync(x, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
         if (inner) *inner = 0;
         if (resid) *resid = 0.0;
         return 0;
@@ -360,7 +484,7 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
     for (int cycle = 0; cycle < maxiter && !done; ++cycle) {
         if (cycle == 0) {
             op.apply(x, tmp.get(), s);
-            k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+            k_sub<T><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
             UP3D_CHECK_LAUNCH();
             rnorm = bl.nrm2(r.get(), n);
             if (rnorm < atol_eff) {
@@ -389,12 +513,12 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
             bl.multiaxpy(V.get(), n, col + 1, hsum, w.get(), n);
             bl.multidot(V.get(), n, col + 1, w.get(), n, hpass);
             bl.multiaxpy(V.get(), n, col + 1, hpass, w.get(), n);
-            k_accumulate<<<1, 64, 0, s>>>(hsum, hpass, col + 1);
+            k_accumulate<double><<<1, 64, 0, s>>>(hsum, hpass, col + 1);
             UP3D_CHECK_LAUNCH();
             bl.multidot(w.get(), 0, 1, w.get(), n, hn + 1);
-            UP3D_CUDA(cudaMemcpyAsync(V.get() + (size_t)(col + 1) * n, w.get(), sizeof(double) * n,
+            UP3D_CUDA(cudaMemcpyAsync(V.get() + (size_t)(col + 1) * n, w.get(), sizeof(T) * n,
                                       cudaMemcpyDeviceToDevice, s));
-            k_scale_unless_breakdown<<<grid_for(n, 256), 256, 0, s>>>(V.get() + (size_t)(col + 1) * n, hn, eps, n);
+            k_scale_unless_breakdown<T><<<grid_for(n, 256), 256, 0, s>>>(V.get() + (size_t)(col + 1) * n, hn, eps, n);
             UP3D_CHECK_LAUNCH();
             UP3D_CUDA(cudaMemcpyAsync(hbuf, hsum, sizeof(double) * (col + 1), cudaMemcpyDeviceToHost, s));
             UP3D_CUDA(cudaMemcpyAsync(hbuf + col + 1, hn, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
@@ -442,7 +566,7 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
         UP3D_CUDA(cudaMemcpyAsync(hdev.get(), y.data(), sizeof(double) * (col + 1), cudaMemcpyHostToDevice, s));
         bl.multiaxpy(V.get(), n, col + 1, hdev.get(), x, n);
         op.apply(x, tmp.get(), s);
-        k_sub<<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+        k_sub<T><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
         UP3D_CHECK_LAUNCH();
         rnorm = bl.nrm2(r.get(), n);
         if (rnorm <= atol_eff || breakdown || !std::isfinite(rnorm)) break;
@@ -453,6 +577,59 @@ int gmres_solve(const Operator& op, const double* b, double* x, double rtol, dou
     if (inner) *inner = total;
     if (resid) *resid = rnorm;
     return rnorm <= atol_eff ? 0 : maxiter;
+}
+
+template int gmres_solve<double>(const Operator&, const double*, double*, double, double, int, int, up3d_precond*,
+                                  int64_t*, double*, cudaStream_t);
+template int gmres_solve<float>(const Operator&, const float*, float*, double, double, int, int, up3d_precond*,
+                                 int64_t*, double*, cudaStream_t);
+
+// Mixed-precision GMRES with FP64 iterative refinement: the outer loop forms
+// the true residual r = b - A x with the FP64 values and stops at
+// ||r|| <= max(rtol ||b||, atol); each inner solve is restarted GMRES on the
+// FP32 operator (data32, extra32) and FP32 vectors with the preconditioner
+// applied in FP32, to max(inner_rtol, tol / ||r||) relative, and its
+// correction is added to x in FP64.  Returns 0 when converged.
+int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart,
+                   int maxiter, int refine_max, double inner_rtol, up3d_precond* M, int64_t* inner, int64_t* outer,
+                   double* resid, cudaStream_t s) {
+    const int64_t n = op.A.n;
+    KrylovWs& W = krylov_ws();
+    std::lock_guard<std::recursive_mutex> lock(W.mu);
+    Blas& bl = ws_blas(W, s);
+    DBuf<double>& r = W.d[6];
+    DBuf<double>& tmp = W.d[7];
+    DBuf<float>& r32 = W.f[6];
+    DBuf<float>& d32 = W.f[7];
+    r.alloc(n);
+    tmp.alloc(n);
+    r32.alloc(n);
+    d32.alloc(n);
+    const double bnrm = bl.nrm2(b, n);
+    const double tol = eff_atol(atol, rtol, bnrm);
+    int64_t tot_inner = 0, it = 0;
+    double rn = 0.0;
+    for (;; ++it) {
+        op.apply(x, tmp.get(), s);
+        k_sub<double><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+        UP3D_CHECK_LAUNCH();
+        rn = bl.nrm2(r.get(), n);
+        if (rn <= tol || !std::isfinite(rn) || it >= refine_max) break;
+        k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(r.get(), r32.get(), n);
+        UP3D_CHECK_LAUNCH();
+        UP3D_CUDA(cudaMemsetAsync(d32.get(), 0, sizeof(float) * n, s));
+        int64_t inn = 0;
+        double ires = 0.0;
+        gmres_solve<float>(op, r32.get(), d32.get(), std::max(inner_rtol, tol / rn), 0.0, restart, maxiter, M, &inn,
+                           &ires, s);
+        tot_inner += inn;
+        k_add_f32<<<grid_for(n, 256), 256, 0, s>>>(x, d32.get(), n);
+        UP3D_CHECK_LAUNCH();
+    }
+    if (inner) *inner = tot_inner;
+    if (outer) *outer = it;
+    if (resid) *resid = rn;
+    return rn <= tol ? 0 : maxiter;
 }
 
 }  // namespace up3d
@@ -504,6 +681,25 @@ int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double a
         Operator op;
         make_op(op, A, nullptr);
         int inf = cg_solve(op, b, x, rtol, atol, maxiter, M, iters, resid, S(stream));
+        if (info) *info = inf;
+    });
+}
+
+int up3d_gmres_ir(const up3d_csr* A, const up3d_csr* extra, const float* data32, const float* extra32,
+                  const double* b, double* x, double rtol, double atol, int restart, int maxiter, int refine_max,
+                  double inner_rtol, up3d_precond* M, int64_t* inner, int64_t* outer, double* resid, int* info,
+                  up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(b && x && data32 && restart > 0 && maxiter > 0 && refine_max >= 0, UP3D_ERR_ARGUMENT,
+                     "up3d_gmres_ir: bad argument");
+        Operator op;
+        make_op(op, A, extra);
+        UP3D_REQUIRE(!op.extra.indptr || extra32, UP3D_ERR_ARGUMENT,
+                     "up3d_gmres_ir: extra operand without FP32 values");
+        op.data32 = data32;
+        op.extra32 = extra32;
+        int inf = gmres_ir_solve(op, b, x, rtol, atol, restart, maxiter, refine_max, inner_rtol, M, inner, outer,
+                                 resid, S(stream));
         if (info) *info = inf;
     });
 }

@@ -6,18 +6,24 @@
 namespace up3d {
 
 // Reproducible reductions and vector updates on one stream.
+// Vector arguments are double or float; dot products accumulate in FP64.
 struct Blas {
     cudaStream_t s;
     DBuf<double> partial, scal;
     double* host = nullptr;  // pinned scalar readback
     explicit Blas(cudaStream_t s);
     ~Blas();
-    void multidot(const double* V, int64_t ldv, int K, const double* y, int64_t n, double* out_dev);
-    double dot(const double* x, const double* y, int64_t n);
-    double nrm2(const double* x, int64_t n);
+    template <class T>
+    void multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev);
+    template <class T>
+    double dot(const T* x, const T* y, int64_t n);
+    template <class T>
+    double nrm2(const T* x, int64_t n);
     void axpby(double a, const double* x, double b, double* y, int64_t n);
-    void scale(double* x, double a, int64_t n);
-    void multiaxpy(const double* V, int64_t ldv, int K, const double* h_dev, double* y, int64_t n);
+    template <class T>
+    void scale(T* x, double a, int64_t n);
+    template <class T>
+    void multiaxpy(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n);
 };
 
 // y = A x (+ extra x): the P1-pattern matrix plus, for the Newton Jacobian,
@@ -25,11 +31,16 @@ struct Blas {
 struct Operator {
     up3d_csr A{};
     up3d_csr extra{};
+    const float* data32 = nullptr;   // FP32 copies of the values (mixed precision)
+    const float* extra32 = nullptr;
     mutable DBuf<double> tmp;
+    mutable DBuf<float> tmp32;
     void apply(const double* x, double* y, cudaStream_t s) const;
+    void apply(const float* x, float* y, cudaStream_t s) const;
 };
 
 void amg_apply(void* amg, const double* r, double* z, cudaStream_t s);
+void amg_apply_f32(void* amg, const float* r, float* z, cudaStream_t s);
 void amg_destroy(void* amg);
 void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s);
 void amg_refresh(void* amg, const up3d_csr& A, cudaStream_t s);
@@ -48,4 +59,5 @@ struct up3d_precond {
         if (amg) up3d::amg_destroy(amg);
     }
     void apply(const double* r, double* z, cudaStream_t s);
+    void apply(const float* r, float* z, cudaStream_t s);
 };

@@ -39,35 +39,31 @@ static __device__ __align__(256) double g_scratch[NA_DOUBLES];
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ double na_block_sum(double v, double* sh) {
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) sh[w] = v;
-    __syncthreads();
-    double t = 0.0;
-    if (w == 0) {
-        t = lane < (blockDim.x >> 5) ? sh[lane] : 0.0;
-        t = warp_sum(t);
-    }
-    __syncthreads();
-    return t;
-}
-
+// The two reduction passes of the allocating CG's dot products (krylov.cu
+// k_multidot with one vector, k_finish): per block, warp butterflies then
+// the block's warp sums in order; then one warp over the block partials.
 __global__ void __launch_bounds__(NA_RB) k_na_dot(const double* __restrict__ x, const double* __restrict__ y,
                                                   int64_t n, double* __restrict__ partial) {
-    __shared__ double sh[32];
+    __shared__ double sh[NA_RB / 32];
     double acc = 0.0;
     GRID_STRIDE(i, n) acc += x[i] * y[i];
-    double t = na_block_sum(acc, sh);
-    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    const double v = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < NA_RB / 32; ++q) t += sh[q];
+        partial[blockIdx.x] = t;
+    }
 }
 
 __global__ void k_na_finish(const double* __restrict__ partial, int nb, double* __restrict__ out) {
-    __shared__ double sh[32];
+    if (threadIdx.x >= 32) return;
     double acc = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[b];
-    double t = na_block_sum(acc, sh);
-    if (threadIdx.x == 0) *out = t;
+    for (int b = threadIdx.x; b < nb; b += 32) acc += partial[b];
+    acc = warp_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
 }
 
 __global__ void k_na_diag(int64_t n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,

@@ -225,6 +225,34 @@ def solve_gmres(A, b, M=None, rtol: float = 1e-6, atol: float = 0.0, x0=None, re
     return (x.cpu().numpy() if host else x), n_it, info
 
 
+def solve_gmres_mixed(A, b, M=None, rtol: float = 1e-6, atol: float = 0.0, x0=None, restart: int = 50,
+                      maxiter: int = 20, refine_max: int = 10, inner_rtol: float = 1e-4,
+                      values32=None) -> Tuple[object, int, int, int]:
+    """Mixed-precision GMRES with FP64 iterative refinement (up3d_gmres_ir):
+    inner GMRES(restart) in FP32 on A's FP32 values with M applied in FP32,
+    outer residual, update and convergence test in FP64.  ``values32`` =
+    (data32, extra32) reuses FP32 copies of A's values.  Returns (x,
+    n_inner_iterations, n_refinements, info)."""
+    t = L.require_cuda()
+    Ad = as_device_csr(A)
+    host = not L.is_torch(b)
+    d_b = L.to_device(b, t.float64)
+    x = t.zeros_like(d_b) if x0 is None else L.to_device(x0, t.float64).clone()
+    if M is not None and not isinstance(M, DevicePreconditioner):
+        raise TypeError("M must be a DevicePreconditioner")
+    X = getattr(Ad, "extra", None)
+    if values32 is None:
+        values32 = (Ad.data.to(t.float32), None if X is None else X.data.to(t.float32))
+    d32, x32 = values32
+    inner, outer, resid, info = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_int()
+    L.call("up3d_gmres_ir", ctypes.byref(_csr_struct(Ad)), _extra_struct(Ad), d32.data_ptr(),
+           None if x32 is None else x32.data_ptr(), d_b.data_ptr(), x.data_ptr(), float(rtol),
+           float(atol), int(restart), int(maxiter), int(refine_max), float(inner_rtol),
+           None if M is None else M.handle, ctypes.byref(inner), ctypes.byref(outer),
+           ctypes.byref(resid), ctypes.byref(info), L.stream_ptr())
+    return (x.cpu().numpy() if host else x), int(inner.value), int(outer.value), int(info.value)
+
+
 def solve_cg(A, b, M=None, rtol: float = 1e-10, atol: float = 0.0, maxiter: int = 500, x0=None):
     """Preconditioned CG; returns (x, n_iter, info)."""
     t = L.require_cuda()

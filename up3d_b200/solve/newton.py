@@ -27,7 +27,7 @@ import numpy as np
 from .. import _lib as L
 from ..mesh.device import DeviceMesh, get_mesh
 from .fused import FlowParams, ResidualJacobian
-from .linear import amg_for, solve_cg, solve_gmres, with_dirichlet
+from .linear import amg_for, solve_cg, solve_gmres, solve_gmres_mixed, with_dirichlet
 
 
 def _ew_forcing(r_norm, r_norm_prev, eta_prev, eta0=1e-2, gamma_ew=0.9, eta_max=1e-2,
@@ -129,6 +129,8 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
     """Newton at one Mach level (pyfp3d/solve/newton.py:516-1141 without
     the wake / Kutta blocks)."""
     t = L.require_cuda()
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
     amg_fp32 = precision == "mixed"
     timings = {"seed": 0.0, "assembly": 0.0, "precond": 0.0, "linsolve": 0.0, "residual": 0.0}
 
@@ -147,7 +149,7 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
     timings["seed"] = clock() - t_wall0
 
     residual_history, eta_history, newton_orders = [], [], []
-    n_gmres_total = n_gmres_stalled = 0
+    n_gmres_total = n_gmres_stalled = n_refine_total = 0
     converged = False
     M_pre = None
     eta_prev = None
@@ -247,8 +249,15 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
         eta_history.append(eta)
         a = clock()
         rhs = -Rf
-        dphi, n_it, info = solve_gmres(Jf, rhs, M=M_pre, rtol=eta, restart=gmres_restart,
-                                       maxiter=gmres_maxiter, on_fail="return")
+        if precision == "mixed":
+            # FP32 Jacobian values and FP32 AMG inside FP64-refined GMRES(50)
+            dphi, n_it, n_ref, info = solve_gmres_mixed(Jf, rhs, M=M_pre, rtol=eta, restart=50,
+                                                        maxiter=gmres_maxiter, refine_max=10,
+                                                        inner_rtol=1e-5)
+            n_refine_total += n_ref
+        else:
+            dphi, n_it, info = solve_gmres(Jf, rhs, M=M_pre, rtol=eta, restart=gmres_restart,
+                                           maxiter=gmres_maxiter, on_fail="return")
         timings["linsolve"] += clock() - a
         n_gmres_total += n_it
         n_gmres_stalled += info != 0
@@ -282,7 +291,8 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
             "n_newton": len(residual_history) - (1 if converged else 0),
             "residual_history": residual_history, "eta_history": eta_history,
             "newton_orders": newton_orders, "n_gmres_total": n_gmres_total,
-            "n_gmres_stalled": n_gmres_stalled, "froze": frozen is not None,
+            "n_gmres_stalled": n_gmres_stalled, "n_refinements": n_refine_total,
+            "froze": frozen is not None,
             "frozen_state": frozen,
             "n_freeze_refresh": n_freeze_refresh, "residual_unfrozen": residual_unfrozen,
             "n_freeze_reverts": n_freeze_reverts, "nu_max": mon["nu_max"],
