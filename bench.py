@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--cpu-states", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pocket-steps", type=int, default=300)
+    p.add_argument("--newton", default="200x60x50:0.08:0.70",
+                   help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
 
 
@@ -227,6 +229,45 @@ def read_traffic(kernel: str):
     return None
 
 
+def newton_timing(spec):
+    """Time-to-1e-10 of the device Newton solve (Picard seed, exact
+    Jacobian, GMRES + AMG, line search, frozen finish) from the freestream
+    potential, plain FP64 and mixed precision (FP32 Jacobian SpMV and FP32
+    AMG inside FP64-refined GMRES), each after an untimed solve of the same
+    case; wall clock with the device synchronised."""
+    import torch
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    shape_s, amp_s, mach_s = spec.split(":")
+    shape = tuple(int(v) for v in shape_s.split("x"))
+    amp, mach = float(amp_s), float(mach_s)
+    mesh = bump_channel(*shape, amplitude=amp, seed=0)
+    out = {"case": f"bump channel {shape_s} Kuhn-split ({mesh.n_tets} tets), bump {amp}, "
+                   f"M_inf {mach}, from freestream to |R_free|inf < 1e-10",
+           "n_tets": mesh.n_tets}
+    phis = {}
+    for prec in ("fp64", "mixed"):
+        res = None
+        for rep_ in range(2):
+            ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = solve_newton_transonic(ws, mach, m_start=mach, dm=0.05, precision=prec)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        phis[prec] = res["phi"]
+        out[prec] = {"time_s": round(dt, 4), "converged": bool(res["converged"]),
+                     "final_residual": float(res["residual_history"][-1]),
+                     "n_newton": int(res["level_history"][-1][1]),
+                     "n_gmres": int(res["level_history"][-1][3]),
+                     "n_refinements": int(res.get("n_refinements", 0)),
+                     "n_supersonic": int(res["n_supersonic"]),
+                     "phases_s": {k: round(v, 4) for k, v in res["timings"].items()}}
+    out["mixed_vs_fp64_max_dphi"] = float((phis["mixed"] - phis["fp64"]).abs().max())
+    out["speedup_mixed"] = round(out["fp64"]["time_s"] / out["mixed"]["time_s"], 3)
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -350,6 +391,8 @@ def run_ours(args):
                   "n_term3_extra": [int(m["n_term3_extra"]) for m in p_mon],
                   "nu_max": [float(m["nu_max"]) for m in p_mon]}
 
+    newton = newton_timing(args.newton) if args.newton else None
+
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
     e2e_value = dmesh.n_tets * n_e2e * world / (e2e_ms * 1e-3) / 1e6
@@ -397,6 +440,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
             "pocket_states": pocket,
+            "newton": newton,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

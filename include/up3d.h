@@ -280,7 +280,8 @@ typedef struct {
     int64_t max_coarse; /* dense FP64 solve at or below this size (default 500) */
     int presmooth;      /* Jacobi sweeps (default 2) */
     int postsmooth;     /* Jacobi sweeps (default 2) */
-    int fp32;           /* 0 FP64 cycle, 1 FP32 cycle */
+    int fp32;           /* 0 FP64 cycle, 1 FP32 cycle, 2 both (FP64 vectors take the
+                           FP64 cycle, FP32 vectors the FP32 one) */
 } up3d_amg_options;
 
 typedef struct {

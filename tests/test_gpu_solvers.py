@@ -195,3 +195,16 @@ def test_gmres_mixed_refines_to_fp64_accuracy(c1_golden):
     assert rel_err(x.cpu().numpy(), ref) < 1e-9
     x1, _, _, _ = solve_gmres_mixed(Jf, bd, M=M, rtol=1e-12, restart=50, maxiter=20, refine_max=1)
     assert rel_err(x1.cpu().numpy(), ref) > 1e-9
+
+
+def test_amg_with_both_cycles_matches_fp64_cycle(c1_system):
+    """A hierarchy holding both cycles applies its FP64 cycle to FP64
+    vectors bit-identically to an FP64-only hierarchy."""
+    import torch
+    from up3d_b200.solve.linear import build_amg_preconditioner
+    s = c1_system
+    A = _embedded(s["A"], s["mask"])
+    r = torch.from_numpy(s["b"]).cuda()
+    _, Mb = build_amg_preconditioner(A, fp32="both")
+    _, M64 = build_amg_preconditioner(A)
+    assert torch.equal(Mb.matvec(r), M64.matvec(r))

@@ -621,7 +621,8 @@ struct SymLevel {
 }  // namespace
 
 struct Amg {
-    bool fp32 = false;
+    bool fp32 = false;  // an FP32 cycle exists (Lf)
+    bool fp64 = true;   // an FP64 cycle exists (Ld)
     int pre = 2, post = 2;
     int64_t n_coarse = 0;
     // the caller's finest pattern (refresh checks) and its embedding
@@ -866,7 +867,7 @@ __global__ void k_diff_u8(int64_t n, const uint8_t* __restrict__ a, const uint8_
 
 // One V-cycle z = M r as a sequence of launches on stream s.
 void amg_cycle(Amg& a, const double* r, double* z, cudaStream_t s) {
-    if (!a.fp32) {
+    if (a.fp64) {
         Level<double>& f = *a.Ld[0];
         const int64_t n = f.A.n;
         UP3D_CUDA(cudaMemcpyAsync(f.b.get(), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -979,7 +980,10 @@ void amg_destroy(void* p) { delete static_cast<Amg*>(p); }
 void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) {
     auto* a = new Amg();
     try {
+        // 0: FP64 cycle, 1: FP32 cycle, 2: both (each vector type gets its own)
+        UP3D_REQUIRE(opt.fp32 >= 0 && opt.fp32 <= 2, UP3D_ERR_VALUE, "AMG setup: fp32 must be 0, 1 or 2");
         a->fp32 = opt.fp32 != 0;
+        a->fp64 = opt.fp32 != 1;
         a->pre = std::max(1, opt.presmooth);
         a->post = std::max(0, opt.postsmooth);
         const int64_t n = A.n;
@@ -1095,7 +1099,8 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         if (a->fp32) {
             make_levels<float>(*a, a->Lf, s);
             fill_levels<float>(*a, a->Lf, s);
-        } else {
+        }
+        if (a->fp64) {
             make_levels<double>(*a, a->Ld, s);
             fill_levels<double>(*a, a->Ld, s);
         }
@@ -1142,7 +1147,7 @@ void amg_refresh(void* p, const up3d_csr& A, cudaStream_t s) {
     UP3D_CHECK_LAUNCH();
     numeric(a, s);
     if (a.fp32) fill_levels<float>(a, a.Lf, s);
-    else fill_levels<double>(a, a.Ld, s);
+    if (a.fp64) fill_levels<double>(a, a.Ld, s);
     a.drop_graphs();  // the smoothing weights are launch arguments of the graphs
 }
 

@@ -141,26 +141,31 @@ class AMGHierarchy:
                 f"operator_complexity={self.operator_complexity:.3f})")
 
 
-def build_amg_preconditioner(A, fp32: bool = False, max_coarse: int = 500, max_levels: int = 10,
+_AMG_KINDS = {False: ("amg", 0), True: ("amg32", 1), "both": ("amg64+32", 2)}
+
+
+def build_amg_preconditioner(A, fp32=False, max_coarse: int = 500, max_levels: int = 10,
                              presmooth: int = 2, postsmooth: int = 2, dirichlet=None):
     """Smoothed-aggregation AMG (solve/linear.py:61-81); returns (ml, M).
+    fp32: False (FP64 cycle), True (FP32 cycle, FP64 coarsest solve) or
+    "both" (FP64 vectors take the FP64 cycle, FP32 vectors the FP32 one).
     Setup is deterministic (no random start vector), so repeated setups on
     a bit-identical matrix give bit-identical hierarchies."""
     Ad = as_device_csr(A)
-    opts = L.AmgOptions(int(max_levels), int(max_coarse), int(presmooth), int(postsmooth),
-                        1 if fp32 else 0)
+    kind, code = _AMG_KINDS[fp32]
+    opts = L.AmgOptions(int(max_levels), int(max_coarse), int(presmooth), int(postsmooth), code)
     h = ctypes.c_void_p()
     L.call("up3d_amg_setup", ctypes.byref(_csr_struct(Ad, dirichlet)), ctypes.byref(opts),
            ctypes.byref(h), L.stream_ptr())
-    M = DevicePreconditioner(h.value, Ad.shape[0], "amg32" if fp32 else "amg")
+    M = DevicePreconditioner(h.value, Ad.shape[0], kind)
     return AMGHierarchy(M), M
 
 
-def amg_for(A, M: Optional[DevicePreconditioner] = None, fp32: bool = False, dirichlet=None):
+def amg_for(A, M: Optional[DevicePreconditioner] = None, fp32=False, dirichlet=None):
     """The AMG preconditioner of A: M refreshed with A's values when M was
     set up (with the same precision) on A's pattern, else a new setup.
     Returns the preconditioner."""
-    kind = "amg32" if fp32 else "amg"
+    kind = _AMG_KINDS[fp32][0]
     if M is not None and M.kind == kind:
         try:
             return M.refresh(A, dirichlet)

@@ -103,7 +103,7 @@ class ChannelWorkspace:
 
 
 def picard_seed(ws: ChannelWorkspace, flow: FlowParams, phi, n_iter: int = 5, rtol: float = 1e-7,
-                amg_fp32: bool = False):
+                amg_fp32=False):
     """Upwinded density Picard warm start (the seed of
     pyfp3d/solve/newton.py:708-720): A(rho_tilde(phi)) phi_new = b."""
     t = L.torch()
@@ -131,7 +131,9 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
     t = L.require_cuda()
     if precision not in ("fp64", "mixed"):
         raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
-    amg_fp32 = precision == "mixed"
+    # mixed: one hierarchy with both cycles -- FP64 for the Picard seed's CG
+    # (FP64 vectors), FP32 inside the refined GMRES (FP32 vectors)
+    amg_fp32 = "both" if precision == "mixed" else False
     timings = {"seed": 0.0, "assembly": 0.0, "precond": 0.0, "linsolve": 0.0, "residual": 0.0}
 
     def clock():
