@@ -230,6 +230,28 @@ int up3d_residual_jacobian(up3d_mesh* mesh, const double* phi, const up3d_flow* 
                            int32_t* upstream_out, up3d_monitors* monitors,
                            up3d_stream stream);
 
+/* ------------------------------------------------------ adjoint */
+
+/* Vector-Jacobian product of the residual (the discrete adjoint's
+ * right-hand sides; no reference counterpart -- the reference has no
+ * adjoint): for L = lam^T R(phi, X, M_inf) + sum_e w_q2[e] q2_e(phi, X),
+ * with the upstream elements and, when branch != NULL, the frozen branches
+ * held fixed (the Newton Jacobian's linearisation), writes dL/dX (device,
+ * N x 3, may be NULL), dL/dM_inf (device scalar, may be NULL) and
+ * sum_e w_q2[e] dq2_e/dphi (device, N, may be NULL; needs w_q2).  q2_e =
+ * |grad phi_e|^2 / u_inf^2.  lam (N) and w_q2 (E) are device arrays and
+ * either may be NULL (zero).  The lam^T dR/dphi part is J^T lam: see
+ * up3d_jacobian_transpose.  Deterministic. */
+int up3d_residual_vjp(up3d_mesh* mesh, const double* phi, const up3d_flow* flow,
+                      const int64_t* upstream, const int8_t* branch, const double* lam,
+                      const double* w_q2, double* dphi, double* dX, double* dM,
+                      up3d_stream stream);
+
+/* Values of J^T on the (symmetric) P1 pattern: data_t[z] = data[slot of
+ * the transposed entry of z] (device arrays of nnz). */
+int up3d_jacobian_transpose(up3d_mesh* mesh, const double* data, double* data_t,
+                            up3d_stream stream);
+
 /* ------------------------------------------------------ accounting */
 
 /* Number of library kernel launches since the library was loaded (the

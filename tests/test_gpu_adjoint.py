@@ -1,0 +1,140 @@
+"""Discrete adjoint: the hand-written residual vector-Jacobian product
+against central finite differences of the device residual, and the shape /
+Mach gradient of the lift-like wall integral against finite differences of
+re-converged solves and against a transpose solve with the reference's
+Jacobian (the oracle's)."""
+
+import numpy as np
+import pytest
+
+from conftest import has_cuda
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
+
+
+def _fd_setup(mach=0.8):
+    import torch
+    from up3d_b200.adjoint import AdjointContext
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    from up3d_b200.solve.fused import FlowParams
+    from up3d_b200.solve.newton import ChannelWorkspace
+    mesh = bump_channel(8, 4, 4, amplitude=0.05, seed=3)
+    ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+    phi = torch.from_numpy(pocket_state(mesh, "mixed")).cuda()
+    flow = FlowParams(m_inf=mach)
+    frozen = ws.freeze(phi, flow)
+    actx = AdjointContext(ws, phi, flow, frozen=frozen)
+    rng = np.random.default_rng(0)
+    lam = torch.from_numpy(rng.standard_normal(mesh.n_nodes)).cuda()
+    w = torch.from_numpy(rng.standard_normal(mesh.n_tets)).cuda()
+    return mesh, ws, phi, flow, frozen, actx, lam, w, rng
+
+
+def _L(nodes, mesh, phi, flow, frozen, lam, w):
+    from up3d_b200.solve.newton import ChannelWorkspace
+    ws = ChannelWorkspace(nodes, mesh.elements, mesh.dirichlet_nodes)
+    R = ws.ev.evaluate(phi, flow, jacobian=False, frozen=frozen, keep_state=False)
+    _, q2 = ws.op.velocities(phi)
+    return float(lam @ R) + float(w @ (q2 / flow.u_inf ** 2))
+
+
+def test_vjp_coordinates_and_mach_match_finite_differences():
+    from up3d_b200.solve.fused import FlowParams
+    mesh, ws, phi, flow, frozen, actx, lam, w, rng = _fd_setup()
+    assert int(ws.ev.read_monitors()["n_supersonic"]) > 0
+    _, dX, dM = actx.vjp(lam=lam, w_q2=w)
+    dX = dX.cpu().numpy()
+    h = 1e-6
+    for trial in range(3):
+        d = rng.standard_normal(mesh.nodes.shape)
+        Lp = _L(mesh.nodes + h * d, mesh, phi, flow, frozen, lam, w)
+        Lm = _L(mesh.nodes - h * d, mesh, phi, flow, frozen, lam, w)
+        fd = (Lp - Lm) / (2 * h)
+        ad = float((dX * d).sum())
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-300), (trial, fd, ad)
+    eps = 1e-6
+    Lp = _L(mesh.nodes, mesh, phi, FlowParams(m_inf=flow.m_inf + eps), frozen, lam, w)
+    Lm = _L(mesh.nodes, mesh, phi, FlowParams(m_inf=flow.m_inf - eps), frozen, lam, w)
+    fd = (Lp - Lm) / (2 * eps)
+    assert abs(fd - float(dM)) <= 1e-6 * abs(float(dM)), (fd, float(dM))
+
+
+def test_vjp_phi_part_and_jacobian_transpose():
+    import torch
+    mesh, ws, phi, flow, frozen, actx, lam, w, rng = _fd_setup()
+    dphi, _, _ = actx.vjp(w_q2=w, want_dphi=True)
+    d = torch.from_numpy(rng.standard_normal(mesh.n_nodes)).cuda()
+    h = 1e-6
+
+    def q2w(p):
+        _, q2 = ws.op.velocities(p)
+        return float(w @ (q2 / flow.u_inf ** 2))
+
+    fd = (q2w(phi + h * d) - q2w(phi - h * d)) / (2 * h)
+    ad = float(dphi @ d)
+    assert abs(fd - ad) <= 1e-6 * abs(ad)
+    # <lam, J d> = <J^T lam, d>
+    lhs = float(lam @ actx.J.matvec(d))
+    rhs = float(actx.JT.matvec(lam) @ d)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0)
+
+
+def test_residual_autograd_function_backward():
+    import torch
+    from up3d_b200.adjoint import ResidualFunction
+    mesh, ws, phi, flow, frozen, actx, lam, w, rng = _fd_setup()
+    p = phi.clone().requires_grad_(True)
+    X = torch.from_numpy(mesh.nodes).cuda().requires_grad_(True)
+    M = torch.tensor(flow.m_inf, dtype=torch.float64, device="cuda", requires_grad=True)
+    R = ResidualFunction.apply(actx, p, X, M)
+    (lam @ R).backward()
+    _, dX, dM = actx.vjp(lam=lam)
+    assert torch.equal(X.grad, dX) and float(M.grad) == float(dM)
+    assert torch.allclose(p.grad, actx.JT.matvec(lam), rtol=0, atol=0)
+
+
+@pytest.fixture(scope="module")
+def subsonic_gradient():
+    from up3d_b200.adjoint import BumpShape, adjoint_gradient
+    shape = BumpShape(16, 6, 5, amplitude=0.05, seed=0)
+    kw = {"tol_residual": 1e-13, "n_newton_max": 40}
+    g = adjoint_gradient(shape, 0.5, solve_kw=kw)
+    return shape, g, kw
+
+
+def test_adjoint_shape_and_mach_gradient_match_finite_differences(subsonic_gradient):
+    from up3d_b200.adjoint import objective_value
+    shape, g, kw = subsonic_gradient
+    assert g["gmres_info"] == 0
+    # fourth-order central differences (truncation well below the 1e-6 bar)
+    def fd4(f, h):
+        return (8.0 * (f(h) - f(-h)) - (f(2 * h) - f(-2 * h))) / (12.0 * h)
+
+    for k in (0, 5, 10, 15):
+        def fk(s, k=k):
+            e = np.zeros(shape.n_params)
+            e[k] = s
+            return objective_value(shape, 0.5, p=e, solve_kw=kw)
+        fd = fd4(fk, 1e-4)
+        ad = float(g["dF_dp"][k])
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), abs(fd)), (k, fd, ad)
+    fd = fd4(lambda s: objective_value(shape, 0.5 + s, solve_kw=kw), 1e-4)
+    assert abs(fd - g["dF_dM"]) <= 1e-6 * abs(fd), (fd, g["dF_dM"])
+
+
+def test_adjoint_matches_reference_jacobian_transpose_solve(subsonic_gradient):
+    """lam against scipy's direct solve with the oracle's Jacobian (the
+    reference's assemble_newton_jacobian restated) at the same state."""
+    import scipy.sparse.linalg as spla
+    from oracle import oracle as O
+    shape, g, _ = subsonic_gradient
+    mesh = shape.mesh()
+    phi = g["phi"].cpu().numpy()
+    J = O.chain(O.PicardOperator(mesh.nodes, mesh.elements),
+                O.UpwindOperator(mesh.nodes, mesh.elements), phi, 0.5, jacobian=True)["J"]
+    free = np.setdiff1d(np.arange(mesh.n_nodes), mesh.dirichlet_nodes)
+    rhs = g["dF_dphi"].cpu().numpy()[free]
+    lam_ref = spla.spsolve(J.tocsr()[free][:, free].T.tocsc(), rhs)
+    lam = g["lambda"].cpu().numpy()[free]
+    assert np.abs(lam - lam_ref).max() <= 1e-8 * np.abs(lam_ref).max()

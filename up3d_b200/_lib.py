@@ -83,6 +83,8 @@ SIGNATURES = {
     "up3d_jacobian_export": (_int, [_p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_nnz": (_int, [_p, _p, ctypes.POINTER(_i64), _p]),
     "up3d_residual_jacobian": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_residual_vjp": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_jacobian_transpose": (_int, [_p, _p, _p, _p]),
     "up3d_launch_count": (_int, [ctypes.POINTER(_i64)]),
     "up3d_profile": (_int, [_int]),
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),

@@ -145,6 +145,12 @@ struct up3d_mesh {
     up3d::DBuf<int32_t> x_ptr;         // (N+1) extras row pointer
     up3d::DBuf<int32_t> x_row_c, x_col_c;  // extras, (row, col) order
     up3d::DBuf<double> x_val_c;
+    // adjoint (residual vector-Jacobian products), grown on demand
+    up3d::DBuf<double> adj_t, adj_a, adj_rt, adj_A;   // (E) each
+    up3d::DBuf<double> adj_dx;                        // (E, 12) per-element node gradients
+    up3d::DBuf<double> adj_dphi;                      // (E, 4)
+    up3d::DBuf<double> adj_part;                      // reduction partials
+    up3d::DBuf<int32_t> adj_key, adj_key_s, adj_val, adj_val_s;  // (E) upstream -> element sort
     up3d::DBuf<up3d_monitors> mon_ws;  // (1)
     up3d::DBuf<int64_t> i64_ws;        // small scalars
     int64_t last_extra = 0;            // extras of the last Jacobian
