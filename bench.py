@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--cpu-states", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pocket-steps", type=int, default=300)
+    p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
+                   help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -268,6 +270,31 @@ def newton_timing(spec):
     return out
 
 
+def adjoint_timing(spec):
+    """Shape (16 Gaussian bump modes) and Mach gradient of the lift-like
+    wall integral through the device adjoint: forward continuation solve
+    from M 0.70, then one transpose solve and two vector-Jacobian products;
+    the second of two runs is timed."""
+    import torch
+    from up3d_b200.adjoint import BumpShape, adjoint_gradient
+    shape_s, amp_s, mach_s = spec.split(":")
+    nx, ny, nz = (int(v) for v in shape_s.split("x"))
+    shape = BumpShape(nx, ny, nz, amplitude=float(amp_s), seed=0)
+    mach = float(mach_s)
+    g = None
+    for _ in range(2):
+        g = adjoint_gradient(shape, mach, m_start=min(0.70, mach))
+    torch.cuda.synchronize()
+    return {"case": f"bump channel {shape_s} ({len(shape.elements)} tets), bump {amp_s}, M_inf {mach}, "
+                    f"{shape.n_params} shape modes + Mach",
+            "objective": g["F"], "dF_dM": g["dF_dM"],
+            "dF_dp_norm": float(np.linalg.norm(g["dF_dp"])),
+            "forward_s": round(g["timings"]["forward_s"], 4),
+            "adjoint_s": round(g["timings"]["adjoint_s"], 4),
+            "transpose_gmres_iterations": int(g["gmres_iterations"]),
+            "check": "tests/test_gpu_adjoint.py: finite differences to 1e-6 relative"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -392,6 +419,7 @@ def run_ours(args):
                   "nu_max": [float(m["nu_max"]) for m in p_mon]}
 
     newton = newton_timing(args.newton) if args.newton else None
+    adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -441,6 +469,7 @@ def run_ours(args):
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
             "pocket_states": pocket,
             "newton": newton,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
