@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--pocket-steps", type=int, default=300)
     p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
                    help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
+    p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
+                   help="cases:smallest:largest:mach_lo:mach_hi of the batched comparison ('' to skip); "
+                        "the full batched configuration is 48:20x6x5:200x60x50:0.5:0.85")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -295,6 +298,84 @@ def adjoint_timing(spec):
             "check": "tests/test_gpu_adjoint.py: finite differences to 1e-6 relative"}
 
 
+def batched_timing(spec, seed=0):
+    """Many cases in one launch: meshes of log-uniform size between the
+    smallest and largest box, M_inf ~ U[mach_lo, mach_hi], bump amplitude ~
+    U[0.02, 0.08], one seed.  Reports the residual+Jacobian throughput of
+    one batched evaluation against the same cases evaluated one by one, and
+    the time to converge every case (|R_free|inf < 1e-10) with the lockstep
+    batched Newton against sequential plain solves."""
+    import torch
+    from up3d_b200.mesh.kuhn import bump_channel, seeded_state
+    from up3d_b200.solve.batched import BatchedChannels, solve_newton_batched
+    from up3d_b200.solve.fused import FlowParams
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    k_s, lo_s, hi_s, mlo_s, mhi_s = spec.split(":")
+    K = int(k_s)
+    lo = np.array([int(v) for v in lo_s.split("x")], dtype=float)
+    hi = np.array([int(v) for v in hi_s.split("x")], dtype=float)
+    rng = np.random.default_rng(seed)
+    f = np.exp(rng.uniform(0.0, np.log(hi[0] / lo[0]), size=K))
+    shapes = [tuple(int(round(v)) for v in lo * fi) for fi in f]
+    machs = rng.uniform(float(mlo_s), float(mhi_s), size=K)
+    amps = rng.uniform(0.02, 0.08, size=K)
+    meshes = [bump_channel(*sh, amplitude=float(a), seed=c) for c, (sh, a) in enumerate(zip(shapes, amps))]
+    batch = BatchedChannels(meshes)
+    E = batch.n_tets
+    # assembly throughput: seeded states
+    phi = torch.from_numpy(np.concatenate([seeded_state(m, c) for c, m in enumerate(meshes)])).cuda()
+    wss = [ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes) for m in meshes]
+    phis = [phi[batch.node_off[c]:batch.node_off[c + 1]].contiguous() for c in range(K)]
+    flows = [FlowParams(m_inf=float(M)) for M in machs]
+
+    def t_events(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ms_b = t_events(lambda: batch.evaluate(phi, machs, jacobian=True), 20)
+
+    def seq():
+        for c in range(K):
+            wss[c].ev.evaluate(phis[c], flows[c], jacobian=True, keep_state=False)
+    ms_s = t_events(seq, 10)
+    out = {"cases": K, "shapes": ["x".join(map(str, sh)) for sh in shapes],
+           "machs": [round(float(m), 4) for m in machs], "amplitudes": [round(float(a), 4) for a in amps],
+           "total_tets": int(E),
+           "assembly": {"batched_ms": round(ms_b, 4), "sequential_ms": round(ms_s, 4),
+                        "batched_melem_s": round(E / ms_b / 1e3, 1),
+                        "sequential_melem_s": round(E / ms_s / 1e3, 1)}}
+    # time to 1e-10: batched lockstep vs sequential plain solves (second run timed)
+    res_b = None
+    for _ in range(2):
+        batch2 = BatchedChannels(meshes)
+        res_b = solve_newton_batched(batch2, machs)
+    seq_s, seq_ok = [], []
+    for c, m in enumerate(meshes):
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = solve_newton_transonic(ws, float(machs[c]), m_start=min(0.70, float(machs[c])))
+        torch.cuda.synchronize()
+        seq_s.append(time.perf_counter() - t0)
+        seq_ok.append(bool(r["converged"]))
+    out["newton"] = {"batched_s": round(res_b["time_s"], 4), "sequential_s": round(float(sum(seq_s)), 4),
+                     "speedup": round(float(sum(seq_s)) / res_b["time_s"], 3),
+                     "batched_converged": [bool(v) for v in res_b["converged"]],
+                     "sequential_converged": seq_ok,
+                     "batched_case_s": [None if np.isnan(v) else round(float(v), 4)
+                                        for v in res_b["converged_s"]],
+                     "sequential_case_s": [round(v, 4) for v in seq_s]}
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -420,6 +501,7 @@ def run_ours(args):
 
     newton = newton_timing(args.newton) if args.newton else None
     adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
+    batched = batched_timing(args.batched) if args.batched else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -470,6 +552,7 @@ def run_ours(args):
             "pocket_states": pocket,
             "newton": newton,
             "adjoint": adjoint,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -252,6 +252,21 @@ int up3d_residual_vjp(up3d_mesh* mesh, const double* phi, const up3d_flow* flow,
 int up3d_jacobian_transpose(up3d_mesh* mesh, const double* data, double* data_t,
                             up3d_stream stream);
 
+/* ------------------------------------------------------ batched cases */
+
+/* up3d_residual_jacobian for several cases in one mesh (their meshes
+ * concatenated as disconnected components, no reference counterpart: the
+ * reference solves one case at a time): element e takes the flow of its
+ * case, flows[case_of[e]] (host array of n_cases; one u_inf for all),
+ * case_of a device int32 array of n_tets.  One launch of each pass covers
+ * every case.  UP3D_ERR_VALUE for a case index outside [0, n_cases). */
+int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cases,
+                                   const up3d_flow* flows, const int32_t* case_of,
+                                   const int64_t* upstream_frozen, const int8_t* branch_frozen,
+                                   double* R, double* data, double* rho_tilde_out,
+                                   int32_t* upstream_out, up3d_monitors* monitors,
+                                   up3d_stream stream);
+
 /* ------------------------------------------------------ accounting */
 
 /* Number of library kernel launches since the library was loaded (the

@@ -1,0 +1,69 @@
+"""Several channel cases in one mesh: the batched residual/Jacobian equals
+the per-case evaluations bit for bit, and the lockstep Newton reaches the
+per-case plain solves' potentials."""
+
+import numpy as np
+import pytest
+
+from conftest import has_cuda
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
+
+
+def _cases():
+    from up3d_b200.mesh.kuhn import bump_channel
+    return [bump_channel(10, 4, 3, amplitude=0.08, seed=1), bump_channel(14, 5, 4, amplitude=0.03, seed=2),
+            bump_channel(8, 3, 3, amplitude=0.05, seed=3)]
+
+
+def test_batched_evaluation_equals_per_case_bitwise():
+    import torch
+    from up3d_b200.mesh.kuhn import pocket_state
+    from up3d_b200.solve.batched import BatchedChannels
+    from up3d_b200.solve.fused import FlowParams
+    from up3d_b200.solve.newton import ChannelWorkspace
+    meshes = _cases()
+    machs = [0.8, 0.6, 0.85]
+    fams = ["mixed", "accelerating", "shockpoint"]
+    batch = BatchedChannels(meshes)
+    phis = [pocket_state(m, f) for m, f in zip(meshes, fams)]
+    phi = torch.from_numpy(np.concatenate(phis)).cuda()
+    R = batch.evaluate(phi, machs, jacobian=True).clone()
+    Jb = batch.ws.ev.jacobian().to_scipy()
+    for c, (m, p, M) in enumerate(zip(meshes, phis, machs)):
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        Rc = ws.ev.evaluate(torch.from_numpy(p).cuda(), FlowParams(m_inf=M), jacobian=True).clone()
+        a, b = batch.node_off[c], batch.node_off[c + 1]
+        assert torch.equal(R[a:b], Rc)
+        Jc = ws.ev.jacobian().to_scipy()
+        blk = Jb[a:b][:, a:b].tocsr()
+        assert (blk != Jc).nnz == 0
+    assert (Jb[batch.node_off[0]:batch.node_off[1]][:, batch.node_off[1]:]).nnz == 0
+
+
+def test_case_index_out_of_range_raises():
+    import torch
+    from up3d_b200.solve.batched import BatchedChannels
+    batch = BatchedChannels(_cases()[:2])
+    batch.case_of_elem[0] = 5
+    with pytest.raises(ValueError, match="case index"):
+        batch.evaluate(batch.ws.freestream.clone(), [0.5, 0.5])
+
+
+def test_batched_newton_matches_plain_solves():
+    from up3d_b200.solve.batched import BatchedChannels, solve_newton_batched
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    meshes = _cases()
+    machs = [0.6, 0.5, 0.7]
+    batch = BatchedChannels(meshes)
+    res = solve_newton_batched(batch, machs)
+    assert res["converged"].all(), res
+    phi = res["phi"].cpu().numpy()
+    for c, (m, M) in enumerate(zip(meshes, machs)):
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        r = solve_newton_transonic(ws, M, m_start=min(0.70, M))
+        assert r["converged"]
+        ref = r["phi"].cpu().numpy()
+        a, b = batch.node_off[c], batch.node_off[c + 1]
+        assert np.abs(phi[a:b] - ref).max() < 1e-8

@@ -299,16 +299,20 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // frozen selection), the upstream element's state recomputed in place, the
 // flux, its sensitivities, and the element's residual contributions and
 // local matrix (JAC) or residual contributions only.
-template <bool FROZEN, bool JAC>
+// BATCH: several cases in one mesh (disconnected components), element e
+// taking the flow of its case, flows[case_of[e]].
+template <bool FROZEN, bool JAC, bool BATCH = false>
 __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
                  const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
-                 const double* __restrict__ phi, Flow F, double u2, const int64_t* __restrict__ up_fz,
+                 const double* __restrict__ phi, Flow F0, double u2, const int64_t* __restrict__ up_fz,
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
-                 double* __restrict__ rt_out, up3d_monitors* mon) {
+                 double* __restrict__ rt_out, up3d_monitors* mon, const Flow* __restrict__ flows,
+                 const int32_t* __restrict__ case_of) {
     MonAcc acc;
     GRID_STRIDE(e, E) {
+        const Flow& F = BATCH ? flows[case_of[e]] : F0;
         // own state; B_e is reduced to gB_j = grad . B_j at once so that
         // only 7 values stay live through the walk
         double g[3], gB[4];
@@ -759,24 +763,39 @@ int up3d_jacobian_nnz(up3d_mesh* m, const double* data, int64_t* newton_nnz, up3
     });
 }
 
-int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flow, const int64_t* up_fz,
-                           const int8_t* br_fz, double* R, double* data, double* rt_out, int32_t* up_out,
-                           up3d_monitors* mon, up3d_stream stream) {
-    return guarded([&] {
-        UP3D_REQUIRE(m && phi && flow && R, UP3D_ERR_ARGUMENT, "up3d_residual_jacobian: null argument");
-        UP3D_REQUIRE((up_fz == nullptr) == (br_fz == nullptr), UP3D_ERR_ARGUMENT,
-                     "up3d_residual_jacobian: frozen upstream and branch go together");
-        cudaStream_t s = S(stream);
-        Flow F = make_flow(*flow);
-        const double u2 = flow->u_inf * flow->u_inf;
-        up3d_monitors* mo = mon ? mon : m->mon_ws.get();
-        UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
-        const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
+}  // extern "C"
+
+namespace up3d {
+namespace {
+
+__global__ void k_check_cases(const int32_t* __restrict__ case_of, int64_t E, int n_cases, int* __restrict__ bad) {
+    GRID_STRIDE(e, E) if (case_of[e] < 0 || case_of[e] >= n_cases) *bad = 1;
+}
+
+}  // namespace
+
+// The fused evaluation: element sweep, row gather, Term 3.  flows_d /
+// case_of select per-element flows (several cases in one mesh) when set.
+static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
+                           const int32_t* case_of, const int64_t* up_fz, const int8_t* br_fz, double* R,
+                           double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon, cudaStream_t s) {
+    up3d_monitors* mo = mon ? mon : m->mon_ws.get();
+    UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
+    const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
 #define FUSED_ARGS                                                                                                \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
-        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo
-        const bool jac = data != nullptr;
-        prof_begin(PROF_ELEM, s);
+        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of
+    const bool jac = data != nullptr;
+    prof_begin(PROF_ELEM, s);
+    if (flows_d) {
+        if (up_fz) {
+            if (jac) k_fused_elem<true, true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            else k_fused_elem<true, false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+        } else {
+            if (jac) k_fused_elem<false, true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            else k_fused_elem<false, false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+        }
+    } else {
         if (up_fz) {
             if (jac) k_fused_elem<true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
             else k_fused_elem<true, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
@@ -784,31 +803,80 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
             if (jac) k_fused_elem<false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
             else k_fused_elem<false, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
         }
+    }
 #undef FUSED_ARGS
-        UP3D_CHECK_LAUNCH();
-        prof_end(PROF_ELEM, s, 1);
-        if (up_out)
-            UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
-        prof_begin(PROF_ROW, s);
-        if (jac) launch_row_gather(m, R, data, s);
-        else launch_row_residual(m, R, s);
-        prof_end(PROF_ROW, s, 1);
-        if (jac) {
-            // the element sweep counted the active elements: Term 3 is
-            // built only when there are any (flags already written)
-            int64_t known = 0;
-            UP3D_CUDA(cudaMemcpyAsync(&known, &mo->n_term3_active, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UP3D_CHECK_LAUNCH();
+    prof_end(PROF_ELEM, s, 1);
+    if (up_out)
+        UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
+    prof_begin(PROF_ROW, s);
+    if (jac) launch_row_gather(m, R, data, s);
+    else launch_row_residual(m, R, s);
+    prof_end(PROF_ROW, s, 1);
+    if (jac) {
+        // the element sweep counted the active elements: Term 3 is
+        // built only when there are any (flags already written)
+        int64_t known = 0;
+        UP3D_CUDA(cudaMemcpyAsync(&known, &mo->n_term3_active, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        int64_t na = 0, nx = 0;
+        prof_begin(PROF_TERM3, s);
+        build_term3(m, data, s, na, nx, known);
+        prof_end(PROF_TERM3, s, 0);
+        m->last_drop_zeros = na > 0;
+        if (nx) {
+            UP3D_CUDA(cudaMemcpyAsync(&mo->n_term3_extra, &nx, sizeof(int64_t), cudaMemcpyHostToDevice, s));
             UP3D_CUDA(cudaStreamSynchronize(s));
-            int64_t na = 0, nx = 0;
-            prof_begin(PROF_TERM3, s);
-            build_term3(m, data, s, na, nx, known);
-            prof_end(PROF_TERM3, s, 0);
-            m->last_drop_zeros = na > 0;
-            if (nx) {
-                UP3D_CUDA(cudaMemcpyAsync(&mo->n_term3_extra, &nx, sizeof(int64_t), cudaMemcpyHostToDevice, s));
-                UP3D_CUDA(cudaStreamSynchronize(s));
-            }
         }
+    }
+}
+
+}  // namespace up3d
+
+extern "C" {
+
+int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flow, const int64_t* up_fz,
+                           const int8_t* br_fz, double* R, double* data, double* rt_out, int32_t* up_out,
+                           up3d_monitors* mon, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && flow && R, UP3D_ERR_ARGUMENT, "up3d_residual_jacobian: null argument");
+        UP3D_REQUIRE((up_fz == nullptr) == (br_fz == nullptr), UP3D_ERR_ARGUMENT,
+                     "up3d_residual_jacobian: frozen upstream and branch go together");
+        const Flow F = make_flow(*flow);
+        fused_evaluate(m, phi, F, flow->u_inf * flow->u_inf, nullptr, nullptr, up_fz, br_fz, R, data, rt_out,
+                       up_out, mon, S(stream));
+    });
+}
+
+int up3d_residual_jacobian_batched(up3d_mesh* m, const double* phi, int n_cases, const up3d_flow* flows,
+                                   const int32_t* case_of, const int64_t* up_fz, const int8_t* br_fz, double* R,
+                                   double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon,
+                                   up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && flows && case_of && R && n_cases > 0, UP3D_ERR_ARGUMENT,
+                     "up3d_residual_jacobian_batched: null argument");
+        UP3D_REQUIRE((up_fz == nullptr) == (br_fz == nullptr), UP3D_ERR_ARGUMENT,
+                     "up3d_residual_jacobian_batched: frozen upstream and branch go together");
+        cudaStream_t s = S(stream);
+        std::vector<Flow> host(n_cases);
+        for (int c = 0; c < n_cases; ++c) {
+            UP3D_REQUIRE(flows[c].u_inf == flows[0].u_inf, UP3D_ERR_VALUE,
+                         "up3d_residual_jacobian_batched: the cases must share u_inf");
+            host[c] = make_flow(flows[c]);
+        }
+        m->flows_ws.alloc(n_cases);
+        m->i64_ws.alloc(8);
+        int* bad = reinterpret_cast<int*>(m->i64_ws.get() + 7);
+        UP3D_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+        k_check_cases<<<grid_for(m->E, 256), 256, 0, s>>>(case_of, m->E, n_cases, bad);
+        UP3D_CHECK_LAUNCH();
+        int hbad = 0;
+        UP3D_CUDA(cudaMemcpyAsync(m->flows_ws.get(), host.data(), sizeof(Flow) * n_cases, cudaMemcpyHostToDevice, s));
+        UP3D_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        UP3D_REQUIRE(!hbad, UP3D_ERR_VALUE, "up3d_residual_jacobian_batched: case index out of range");
+        fused_evaluate(m, phi, host[0], flows[0].u_inf * flows[0].u_inf, m->flows_ws.get(), case_of, up_fz, br_fz,
+                       R, data, rt_out, up_out, mon, s);
     });
 }
 

@@ -102,6 +102,8 @@ struct DBuf {
 //   T3V (E, 8): a_i = w3 gB_i, b_k = grad_u . B_u,k (Term-3 active elements)
 constexpr int LOC_STRIDE = 14;
 
+struct Flow;  // physics constants of one flow (below)
+
 }  // namespace up3d
 
 struct up3d_mesh {
@@ -151,6 +153,7 @@ struct up3d_mesh {
     up3d::DBuf<double> adj_dphi;                      // (E, 4)
     up3d::DBuf<double> adj_part;                      // reduction partials
     up3d::DBuf<int32_t> adj_key, adj_key_s, adj_val, adj_val_s;  // (E) upstream -> element sort
+    up3d::DBuf<up3d::Flow> flows_ws;   // per-case flows of batched evaluations
     up3d::DBuf<up3d_monitors> mon_ws;  // (1)
     up3d::DBuf<int64_t> i64_ws;        // small scalars
     int64_t last_extra = 0;            // extras of the last Jacobian

@@ -1,0 +1,190 @@
+"""Many channel cases solved together on one device.
+
+The reference solves one case at a time.  Here the cases' meshes are
+concatenated into one mesh of disconnected components, so that every pass
+(element sweep, row gather, Term 3, SpMV, AMG V-cycle, Krylov vectors) is
+one launch over all cases: small cases no longer leave the GPU idle between
+launches.  Each element carries its case index and takes that case's flow
+(up3d_residual_jacobian_batched); the Jacobian, the Picard block and the AMG
+hierarchy are block diagonal, so the Krylov solution of the joint system is
+the per-case solutions.
+
+``solve_newton_batched`` steps all cases in lockstep with the plain driver's
+ingredients per case -- Picard seed, exact Jacobian, GMRES(60) + AMG rebuilt
+(refreshed) every two steps, Eisenstat-Walker forcing (the smallest over the
+active cases), a merit line search with up to five halvings decided per case,
+and the Mach continuation as a shared ramp that each case follows up to its
+own target.  A case stops moving once its |R_free|_inf is below the
+tolerance at its target Mach.  Unlike the plain driver there is no frozen
+(upstream, branch) finish: a case that needs it is reported unconverged.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from .. import _lib as L
+from ..mesh.kuhn import BumpMesh
+from .fused import FlowParams
+from .linear import amg_for, solve_cg, solve_gmres, with_dirichlet
+from .newton import ChannelWorkspace, _ew_forcing, mach_schedule
+
+
+class BatchedChannels:
+    """The union of several channel meshes on one device."""
+
+    def __init__(self, meshes: Sequence[BumpMesh], u_inf: float = 1.0):
+        t = L.require_cuda()
+        self.meshes = list(meshes)
+        self.n_cases = len(self.meshes)
+        node_off = np.cumsum([0] + [m.n_nodes for m in self.meshes])
+        elem_off = np.cumsum([0] + [m.n_tets for m in self.meshes])
+        nodes = np.concatenate([m.nodes for m in self.meshes])
+        elements = np.concatenate([m.elements.astype(np.int64) + node_off[c]
+                                   for c, m in enumerate(self.meshes)]).astype(np.int32)
+        dirichlet = np.concatenate([m.dirichlet_nodes + node_off[c] for c, m in enumerate(self.meshes)])
+        self.node_off, self.elem_off = node_off, elem_off
+        self.ws = ChannelWorkspace(nodes, elements, dirichlet, u_inf=u_inf)
+        case_e = np.repeat(np.arange(self.n_cases, dtype=np.int32), np.diff(elem_off))
+        case_n = np.repeat(np.arange(self.n_cases, dtype=np.int64), np.diff(node_off))
+        self.case_of_elem = t.from_numpy(case_e).cuda()
+        self.case_of_node = t.from_numpy(case_n).cuda()
+        self.n_tets = int(elem_off[-1])
+        self.u_inf = float(u_inf)
+
+    def _flows(self, machs):
+        arr = (L.Flow * self.n_cases)()
+        for c, m in enumerate(machs):
+            arr[c] = FlowParams(m_inf=float(m), u_inf=self.u_inf).c()
+        return arr
+
+    def evaluate(self, phi, machs, jacobian: bool = True):
+        """R (and the Jacobian data, rho~, upstream) of every case at once,
+        into the union workspace."""
+        ev = self.ws.ev
+        L.call("up3d_residual_jacobian_batched", ev.mesh.handle, phi.data_ptr(), self.n_cases,
+               self._flows(machs), self.case_of_elem.data_ptr(), None, None, ev.R.data_ptr(),
+               ev.data.data_ptr() if jacobian else None, ev.rho_tilde.data_ptr(),
+               ev.upstream.data_ptr(), ev.monitors.data_ptr(), L.stream_ptr())
+        return ev.R
+
+    def per_case(self, v, op: str):
+        """Per-case max |v| ("amax") or sum v^2 ("sumsq") over the nodes."""
+        t = L.torch()
+        out = t.zeros(self.n_cases, dtype=t.float64, device=v.device)
+        if op == "amax":
+            return out.scatter_reduce(0, self.case_of_node, v.abs(), reduce="amax", include_self=True)
+        return out.index_add(0, self.case_of_node, v * v)
+
+
+def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start: float = 0.70,
+                         dm: float = 0.05, tol_residual: float = 1e-10, n_newton_max: int = 30,
+                         n_picard_seed: int = 5, amg_rebuild_every: int = 2, gmres_restart: int = 60,
+                         gmres_maxiter: int = 10, verbose: bool = False) -> Dict[str, object]:
+    """Lockstep Newton of every case (module docstring); returns the union
+    potential, per-case convergence, iteration counts and timings."""
+    t = L.require_cuda()
+    ws = batch.ws
+    machs = np.asarray(machs, dtype=np.float64)
+    C = batch.n_cases
+    mask_b = ws.mask.bool()
+
+    def clock():
+        t.cuda.synchronize()
+        return time.perf_counter()
+
+    t0 = clock()
+    levels = sorted(set(mach_schedule(float(machs.max()), min(m_start, float(machs.max())), dm)))
+    converged_at = np.full(C, -1.0)
+    converged_s = np.full(C, np.nan)
+    failed = np.zeros(C, dtype=bool)
+    n_newton = np.zeros(C, dtype=np.int64)
+    n_gmres_total = 0
+    phi = ws.freestream.clone()
+    M_pre = None
+    case_node = batch.case_of_node
+
+    # Picard seed at the first level's Mach (A(rho~(phi)) phi = b, all cases)
+    m_level = np.minimum(machs, levels[0])
+    for _ in range(n_picard_seed):
+        batch.evaluate(phi, m_level, jacobian=False)
+        A = ws.op.assemble_matrix(ws.ev.rho_tilde)
+        rhs = -A.matvec(ws.phi_dir)
+        rhs[ws.dn] = 0.0
+        Af = with_dirichlet(A, ws.mask)
+        ws.amg = M_pre = amg_for(Af, getattr(ws, "amg", None))
+        x, _, _ = solve_cg(Af, rhs, M=M_pre, rtol=1e-7, maxiter=2000,
+                           x0=t.where(ws.free, phi, t.zeros_like(phi)))
+        phi = t.where(ws.free, x, ws.phi_dir)
+    t_seed = clock() - t0
+
+    for lvl, m_lev in enumerate(levels):
+        m_level = np.minimum(machs, m_lev)
+        # cases already converged at their target stay put
+        active = ~failed & ~((converged_at >= 0) & (m_level == machs))
+        history = []
+        eta_prev = None
+        for it in range(n_newton_max):
+            R = batch.evaluate(phi, m_level, jacobian=False)
+            Rf = R.masked_fill(mask_b, 0.0)
+            r_case = batch.per_case(Rf, "amax").cpu().numpy()
+            merit = batch.per_case(Rf, "sumsq")
+            history.append(r_case.copy())
+            done = r_case < tol_residual
+            for c in np.nonzero(active & done)[0]:
+                if m_level[c] == machs[c]:
+                    converged_at[c] = m_level[c]
+                    converged_s[c] = time.perf_counter() - t0
+            active = active & ~done
+            if not active.any():
+                break
+            batch.evaluate(phi, m_level, jacobian=True)
+            J = with_dirichlet(ws.ev.jacobian(), ws.mask)
+            if M_pre is None or it % amg_rebuild_every == 0:
+                ws.amg = M_pre = amg_for(ws.picard_matrix(), getattr(ws, "amg", None))
+            r_act = r_case[active]
+            r_prev = history[-2][active] if len(history) > 1 else None
+            etas = [_ew_forcing(float(a), None if r_prev is None else float(b), eta_prev)
+                    for a, b in zip(r_act, r_prev if r_prev is not None else [None] * len(r_act))]
+            eta = min(etas)
+            eta_prev = eta
+            act_node = t.from_numpy(active).cuda()[case_node]
+            rhs = (-Rf).masked_fill(~act_node, 0.0)
+            dphi, n_it, _ = solve_gmres(J, rhs, M=M_pre, rtol=eta, restart=gmres_restart,
+                                        maxiter=gmres_maxiter, on_fail="return")
+            n_gmres_total += n_it
+            n_newton[active] += 1
+            dphi = dphi.masked_fill(mask_b | ~act_node, 0.0)
+            # per-case backtracking: lam halves for the cases whose merit rose
+            lam = np.where(active, 1.0, 0.0)
+            accepted = ~active
+            best_lam = np.zeros(C)
+            best_merit = np.full(C, np.inf)
+            merit_h = merit.cpu().numpy()
+            for _ in range(5):
+                lam_node = t.from_numpy(lam).cuda()[case_node]
+                phi_try = phi + lam_node * dphi
+                R_try = batch.evaluate(phi_try, m_level, jacobian=False)
+                m_try = batch.per_case(R_try.masked_fill(mask_b, 0.0), "sumsq").cpu().numpy()
+                ok = np.isfinite(m_try) & (m_try <= merit_h) & ~accepted
+                better = np.isfinite(m_try) & (m_try < best_merit) & ~accepted
+                best_lam[better] = lam[better]
+                best_merit[better] = m_try[better]
+                accepted |= ok
+                if accepted.all():
+                    break
+                lam = np.where(accepted, lam, 0.5 * lam)
+            lam = np.where(accepted, lam, best_lam)
+            phi = phi + t.from_numpy(lam).cuda()[case_node] * dphi
+            if verbose:
+                print(f"  level M<={m_lev:.3f} it {it}: max|R| active = {r_act.max():.3e}")
+        # a case still active at the end of a level failed it
+        failed |= active
+    t_total = clock() - t0
+    return {"phi": phi, "converged": converged_at >= 0, "failed": failed, "n_newton": n_newton,
+            "n_gmres_total": n_gmres_total, "levels": levels, "time_s": t_total, "seed_s": t_seed,
+            "converged_s": converged_s}
