@@ -76,6 +76,26 @@ __device__ __forceinline__ void store_local(double* __restrict__ loc, int64_t e,
     p[6] = make_double2(jij(b, gB, w1, w2, 1, 3), jij(b, gB, w1, w2, 2, 3));
 }
 
+// store_local with B_e read from memory pair by pair (an L1/L2 hit: the
+// sweep read B_e at its start) instead of twelve values held in registers;
+// the same fma order, so identical bits.
+__device__ __forceinline__ double jij_mem(const double* __restrict__ b, const double gB[4], double w1, double w2,
+                                          int i, int j) {
+    double v = w1 * fma(b[3 * i + 2], b[3 * j + 2], fma(b[3 * i + 1], b[3 * j + 1], b[3 * i] * b[3 * j]));
+    if (w2 != 0.0) v = fma(w2 * gB[i], gB[j], v);
+    return v;
+}
+__device__ __forceinline__ void store_local_mem(double* __restrict__ loc, int64_t e, const double* __restrict__ B,
+                                                const double gB[4], double w1, double w2) {
+    const double* b = B + 12 * e;
+    double2* p = reinterpret_cast<double2*>(loc + (size_t)LOC_STRIDE * e);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) p[i] = make_double2(w1 * gB[i], jij_mem(b, gB, w1, w2, i, i));
+    p[4] = make_double2(jij_mem(b, gB, w1, w2, 0, 1), jij_mem(b, gB, w1, w2, 0, 2));
+    p[5] = make_double2(jij_mem(b, gB, w1, w2, 0, 3), jij_mem(b, gB, w1, w2, 1, 2));
+    p[6] = make_double2(jij_mem(b, gB, w1, w2, 1, 3), jij_mem(b, gB, w1, w2, 2, 3));
+}
+
 __device__ __forceinline__ void store_res(double* __restrict__ res, int64_t e, const double gB[4], double w1) {
     double2* p = reinterpret_cast<double2*>(res + 4 * e);
     p[0] = make_double2(w1 * gB[0], w1 * gB[1]);
@@ -313,31 +333,23 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
     MonAcc acc;
     GRID_STRIDE(e, E) {
         const Flow& F = BATCH ? flows[case_of[e]] : F0;
-        // own state; B_e is reduced to gB_j = grad . B_j at once so that
-        // only 7 values stay live through the walk
-        double g[3], gB[4];
-        {
-            double b[12];
-            int4 c;
-            elem_grad_B(conn, B, phi, e, g, b, c);
-            gB_of(g, b, gB);
-        }
+        // only grad phi_e stays live through the walk; the element's own
+        // state and gB_j = grad . B_j are formed after it (B_e again: an
+        // L1/L2 hit)
+        double g[3];
+        elem_grad(conn, B, phi, e, g);
+        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, disp, X, conn, e, E, g);
         double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), u2);
         double q2l = q2n < F.q2cap ? q2n : F.q2cap;
         bool lim_e = q2l == q2n;
         double rho_e, drho_e;
         rho_drho(q2l, F, rho_e, drho_e);
-
-        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, disp, X, conn, e, E, g);
         // upstream state, and its Term-3 factors grad_u . B_u,k
         double q2lu = q2l, rho_u = rho_e;
         bool lim_u = lim_e;
-        double f[4] = {gB[0], gB[1], gB[2], gB[3]};
         if (u != e) {
-            double gu[3], bu[12];
-            int4 cu;
-            elem_grad_B(conn, B, phi, u, gu, bu, cu);
-            if (JAC) gB_of(gu, bu, f);
+            double gu[3];
+            elem_grad(conn, B, phi, u, gu);
             double q2nu = __ddiv_rn(dot3r(gu[0], gu[1], gu[2], gu[0], gu[1], gu[2]), u2);
             q2lu = q2nu < F.q2cap ? q2nu : F.q2cap;
             lim_u = q2lu == q2nu;
@@ -372,6 +384,12 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
 
         const double Ve = V[e];
         const double w1 = rt * Ve;
+        double gB[4];
+        {
+            const double* be = B + 12 * e;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) gB[j] = g[0] * be[3 * j] + g[1] * be[3 * j + 1] + g[2] * be[3 * j + 2];
+        }
         if (JAC) {
             s_e = s_e * (lim_e ? 1.0 : 0.0);
             s_u = s_u * (lim_u ? 1.0 : 0.0);
@@ -379,13 +397,20 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
             const double w3 = 2.0 * F.inv_u2 * s_u * Ve;
             const bool active = s_u != 0.0;
             if (active) {
+                // Term-3 factors grad_u . B_u,k, recomputed for the (few)
+                // active elements only
+                double f[4] = {gB[0], gB[1], gB[2], gB[3]};
+                if (u != e) {
+                    double gu[3], bu[12];
+                    int4 cu;
+                    elem_grad_B(conn, B, phi, u, gu, bu, cu);
+                    gB_of(gu, bu, f);
+                }
                 store_t3(t3v, e, w3, gB, f);
                 acc.act += 1;
             }
             t3flag[e] = active ? 1 : 0;
-            double b[12];
-            load_B(B, e, b);  // second touch of B_e: an L2 hit
-            store_local(loc, e, b, gB, w1, w2, true);
+            store_local_mem(loc, e, B, gB, w1, w2);  // second touch of B_e: an L1/L2 hit
         } else {
             store_res(res, e, gB, w1);
         }
