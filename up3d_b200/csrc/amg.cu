@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -45,6 +47,49 @@ struct HostCSR {
     std::vector<int32_t> p, i;
     std::vector<double> x;
 };
+
+// Host <-> device copies of the setup through one process-wide page-locked
+// staging buffer (grown once, kept): pageable copies of the level patterns
+// were a large part of the setup time.
+struct Stage {
+    std::mutex mu;
+    unsigned char* p = nullptr;
+    size_t n = 0;
+};
+Stage& stage() {
+    static Stage st;
+    return st;
+}
+constexpr size_t STAGE_CHUNK = size_t(32) << 20;
+unsigned char* stage_buffer(Stage& st) {
+    if (!st.p) {
+        UP3D_CUDA(cudaMallocHost(&st.p, STAGE_CHUNK));
+        st.n = STAGE_CHUNK;
+    }
+    return st.p;
+}
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    Stage& st = stage();
+    std::lock_guard<std::mutex> g(st.mu);
+    unsigned char* buf = stage_buffer(st);
+    for (size_t o = 0; o < bytes; o += STAGE_CHUNK) {
+        const size_t b = std::min(STAGE_CHUNK, bytes - o);
+        std::memcpy(buf, static_cast<const unsigned char*>(src) + o, b);
+        UP3D_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + o, buf, b, cudaMemcpyHostToDevice, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+    }
+}
+void d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    Stage& st = stage();
+    std::lock_guard<std::mutex> g(st.mu);
+    unsigned char* buf = stage_buffer(st);
+    for (size_t o = 0; o < bytes; o += STAGE_CHUNK) {
+        const size_t b = std::min(STAGE_CHUNK, bytes - o);
+        UP3D_CUDA(cudaMemcpyAsync(buf, static_cast<const unsigned char*>(src) + o, b, cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(static_cast<unsigned char*>(dst) + o, buf, b);
+    }
+}
 
 // ------------------------------------------------------------ host symbolic setup
 
@@ -114,6 +159,8 @@ int32_t find_col(const HostCSR& P, int64_t r, int32_t c) {
 // Pattern of P = (I - omega D^-1 A) T: row r holds agg[r] and agg[c] of its
 // aggregated neighbours.  amap[k] = slot of A entry k's contribution (-1 when
 // its column is unaggregated), self[r] = slot of agg[r] (-1 when none).
+// Two passes (count, fill) with a per-thread marker array: no per-row
+// allocation.
 HostCSR prolongator_pattern(const HostCSR& A, const std::vector<int32_t>& agg, int64_t na,
                             std::vector<int32_t>& amap, std::vector<int32_t>& self) {
     const int64_t n = A.n;
@@ -121,26 +168,52 @@ HostCSR prolongator_pattern(const HostCSR& A, const std::vector<int32_t>& agg, i
     P.n = n;
     P.m = na;
     P.p.assign(n + 1, 0);
-    std::vector<std::vector<int32_t>> rows(n);
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int64_t r = 0; r < n; ++r) {
-        auto& row = rows[r];
-        if (agg[r] >= 0) row.push_back(agg[r]);
-        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
-            if (agg[A.i[k]] >= 0) row.push_back(agg[A.i[k]]);
-        std::sort(row.begin(), row.end());
-        row.erase(std::unique(row.begin(), row.end()), row.end());
+#pragma omp parallel
+    {
+        std::vector<int32_t> mark(na, -1);
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < n; ++r) {
+            int32_t cnt = 0;
+            if (agg[r] >= 0) {
+                mark[agg[r]] = (int32_t)r;
+                ++cnt;
+            }
+            for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
+                const int32_t a = agg[A.i[k]];
+                if (a >= 0 && mark[a] != (int32_t)r) {
+                    mark[a] = (int32_t)r;
+                    ++cnt;
+                }
+            }
+            P.p[r + 1] = cnt;
+        }
     }
-    for (int64_t r = 0; r < n; ++r) P.p[r + 1] = P.p[r] + (int32_t)rows[r].size();
+    for (int64_t r = 0; r < n; ++r) P.p[r + 1] += P.p[r];
     P.i.resize(P.p[n]);
     amap.assign(A.i.size(), -1);
     self.assign(n, -1);
-#pragma omp parallel for schedule(static)
-    for (int64_t r = 0; r < n; ++r) {
-        std::copy(rows[r].begin(), rows[r].end(), P.i.begin() + P.p[r]);
-        if (agg[r] >= 0) self[r] = find_col(P, r, agg[r]);
-        for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
-            if (agg[A.i[k]] >= 0) amap[k] = find_col(P, r, agg[A.i[k]]);
+#pragma omp parallel
+    {
+        std::vector<int32_t> mark(na, -1);
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < n; ++r) {
+            int32_t o = P.p[r];
+            if (agg[r] >= 0) {
+                mark[agg[r]] = (int32_t)r;
+                P.i[o++] = agg[r];
+            }
+            for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
+                const int32_t a = agg[A.i[k]];
+                if (a >= 0 && mark[a] != (int32_t)r) {
+                    mark[a] = (int32_t)r;
+                    P.i[o++] = a;
+                }
+            }
+            std::sort(P.i.begin() + P.p[r], P.i.begin() + P.p[r + 1]);
+            if (agg[r] >= 0) self[r] = find_col(P, r, agg[r]);
+            for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
+                if (agg[A.i[k]] >= 0) amap[k] = find_col(P, r, agg[A.i[k]]);
+        }
     }
     return P;
 }
@@ -166,36 +239,53 @@ HostCSR transpose_pattern(const HostCSR& P, std::vector<int32_t>& tperm) {
     return R;
 }
 
-// Pattern of C = A B (sorted columns, OpenMP over rows).
+// Pattern of C = A B (sorted columns, OpenMP over rows; count and fill
+// passes with a per-thread marker array, no per-row allocation).
 HostCSR spgemm_pattern(const HostCSR& A, const HostCSR& B) {
     HostCSR C;
     C.n = A.n;
     C.m = B.m;
     C.p.assign(A.n + 1, 0);
-    std::vector<std::vector<int32_t>> ci(A.n);
 #pragma omp parallel
     {
         std::vector<int32_t> mark(B.m, -1);
-#pragma omp for schedule(dynamic, 512)
+#pragma omp for schedule(dynamic, 1024)
         for (int64_t r = 0; r < A.n; ++r) {
-            auto& cols = ci[r];
+            int32_t cnt = 0;
             for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
                 const int32_t a = A.i[k];
                 for (int32_t q = B.p[a]; q < B.p[a + 1]; ++q) {
                     const int32_t c = B.i[q];
                     if (mark[c] != (int32_t)r) {
                         mark[c] = (int32_t)r;
-                        cols.push_back(c);
+                        ++cnt;
                     }
                 }
             }
-            std::sort(cols.begin(), cols.end());
+            C.p[r + 1] = cnt;
         }
     }
-    for (int64_t r = 0; r < A.n; ++r) C.p[r + 1] = C.p[r] + (int32_t)ci[r].size();
+    for (int64_t r = 0; r < A.n; ++r) C.p[r + 1] += C.p[r];
     C.i.resize(C.p[A.n]);
-#pragma omp parallel for schedule(static)
-    for (int64_t r = 0; r < A.n; ++r) std::copy(ci[r].begin(), ci[r].end(), C.i.begin() + C.p[r]);
+#pragma omp parallel
+    {
+        std::vector<int32_t> mark(B.m, -1);
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t r = 0; r < A.n; ++r) {
+            int32_t o = C.p[r];
+            for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k) {
+                const int32_t a = A.i[k];
+                for (int32_t q = B.p[a]; q < B.p[a + 1]; ++q) {
+                    const int32_t c = B.i[q];
+                    if (mark[c] != (int32_t)r) {
+                        mark[c] = (int32_t)r;
+                        C.i[o++] = c;
+                    }
+                }
+            }
+            std::sort(C.i.begin() + C.p[r], C.i.begin() + C.p[r + 1]);
+        }
+    }
     return C;
 }
 
@@ -560,9 +650,8 @@ struct DevCSR {
         p.alloc(n + 1);
         i.alloc(std::max<int64_t>(nnz, 1));
         x.alloc(std::max<int64_t>(nnz, 1));
-        UP3D_CUDA(cudaMemcpyAsync(p.get(), h.p.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s));
-        if (nnz)
-            UP3D_CUDA(cudaMemcpyAsync(i.get(), h.i.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
+        h2d(p.get(), h.p.data(), sizeof(int32_t) * (n + 1), s);
+        if (nnz) h2d(i.get(), h.i.data(), sizeof(int32_t) * nnz, s);
     }
     template <class U>
     void copy_pattern(const DevCSR<U>& o, cudaStream_t s) {
@@ -581,7 +670,7 @@ struct DevCSR {
 template <class T>
 void upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
     d.alloc(std::max<size_t>(h.size(), 1));
-    if (!h.empty()) UP3D_CUDA(cudaMemcpyAsync(d.get(), h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    if (!h.empty()) h2d(d.get(), h.data(), sizeof(T) * h.size(), s);
 }
 
 // values of type T from FP64 (copy or narrowing)
@@ -597,9 +686,25 @@ void convert(const double* src, T* dst, int64_t n, cudaStream_t s) {
 }
 
 template <class T>
+struct Ref {  // non-owning device pointer with the DBuf accessor
+    T* v = nullptr;
+    T* get() const { return v; }
+};
+template <class T>
+struct CsrRef {
+    int64_t n = 0, m = 0, nnz = 0;
+    Ref<const int32_t> p, i;
+    Ref<T> x;
+};
+
+// One level of the cycle: views of the symbolic level's patterns and, for
+// the FP64 cycle, of its FP64 values; the FP32 cycle owns FP32 copies.
+template <class T>
 struct Level {
-    DevCSR<T> A, P, R;
-    DBuf<T> dinv, x, b, r;
+    CsrRef<T> A, P, R;
+    Ref<T> dinv;
+    DBuf<T> own_A, own_P, own_R, own_dinv;  // FP32 values (unused for FP64)
+    DBuf<T> x, b, r;
     T w_smooth = T(0);
     const uint8_t* dir = nullptr;  // finest level only
 };
@@ -715,6 +820,7 @@ void vcycle(Amg& a, std::vector<Level<T>*>& L, size_t l, cudaStream_t s) {
 // Diagonal slot of each row of a pattern.
 std::vector<int32_t> diag_slots(const HostCSR& A) {
     std::vector<int32_t> d(A.n, -1);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < A.n; ++r)
         for (int32_t k = A.p[r]; k < A.p[r + 1]; ++k)
             if (A.i[k] == r) d[r] = k;
@@ -817,19 +923,37 @@ void numeric(Amg& a, cudaStream_t s) {
     }
 }
 
-// Copies (or narrows) the FP64 level values into the cycle's levels.
+// Narrows the FP64 level values into the FP32 cycle (the FP64 cycle views
+// them in place) and sets the smoothing weights.
 template <class T>
 void fill_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
     for (size_t l = 0; l < a.sym.size(); ++l) {
         SymLevel& F = *a.sym[l];
         Level<T>& lv = *Lv[l];
-        convert<T>(F.A.x.get(), lv.A.x.get(), F.A.nnz, s);
+        if constexpr (!std::is_same<T, double>::value) convert<T>(F.A.x.get(), lv.A.x.get(), F.A.nnz, s);
         if (l + 1 < a.sym.size()) {
-            convert<T>(F.P.x.get(), lv.P.x.get(), F.P.nnz, s);
-            convert<T>(F.R.x.get(), lv.R.x.get(), F.R.nnz, s);
-            convert<T>(F.dinv.get(), lv.dinv.get(), F.A.n, s);
+            if constexpr (!std::is_same<T, double>::value) {
+                convert<T>(F.P.x.get(), lv.P.x.get(), F.P.nnz, s);
+                convert<T>(F.R.x.get(), lv.R.x.get(), F.R.nnz, s);
+                convert<T>(F.dinv.get(), lv.dinv.get(), F.A.n, s);
+            }
             lv.w_smooth = (T)a.omega[l];
         }
+    }
+}
+
+template <class T>
+void view(CsrRef<T>& r, const DevCSR<double>& F, DBuf<T>& own) {
+    r.n = F.n;
+    r.m = F.m;
+    r.nnz = F.nnz;
+    r.p.v = F.p.get();
+    r.i.v = F.i.get();
+    if constexpr (std::is_same<T, double>::value) {
+        r.x.v = F.x.get();
+    } else {
+        own.alloc(std::max<int64_t>(F.nnz, 1));
+        r.x.v = own.get();
     }
 }
 
@@ -839,15 +963,20 @@ void make_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
         SymLevel& F = *a.sym[l];
         auto* lv = new Level<T>();
         Lv.push_back(lv);
-        lv->A.copy_pattern(F.A, s);
+        view(lv->A, F.A, lv->own_A);
         const int64_t n = F.A.n;
         lv->x.alloc(n);
         lv->b.alloc(n);
         lv->r.alloc(n);
         if (l + 1 < a.sym.size()) {
-            lv->P.copy_pattern(F.P, s);
-            lv->R.copy_pattern(F.R, s);
-            lv->dinv.alloc(n);
+            view(lv->P, F.P, lv->own_P);
+            view(lv->R, F.R, lv->own_R);
+            if constexpr (std::is_same<T, double>::value) {
+                lv->dinv.v = F.dinv.get();
+            } else {
+                lv->own_dinv.alloc(n);
+                lv->dinv.v = lv->own_dinv.get();
+            }
         }
         // lv->dir stays null: the embedded finest operator already has
         // identity rows and no constrained columns
@@ -995,7 +1124,7 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         UP3D_CUDA(cudaStreamSynchronize(s));
         const int64_t nnz = h.p[n];
         h.i.resize(nnz);
-        UP3D_CUDA(cudaMemcpyAsync(h.i.data(), A.indices, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, s));
+        d2h(h.i.data(), A.indices, sizeof(int32_t) * nnz, s);
         std::vector<uint8_t> skip(n, 0);
         if (A.dirichlet)
             UP3D_CUDA(cudaMemcpyAsync(skip.data(), A.dirichlet, n, cudaMemcpyDeviceToHost, s));
@@ -1014,15 +1143,18 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         std::vector<int32_t> src;
         e.n = e.m = n;
         e.p.assign(n + 1, 0);
+#pragma omp parallel for schedule(static)
         for (int64_t r = 0; r < n; ++r) {
             int32_t cnt = 0;
             if (skip[r]) cnt = 1;
             else
                 for (int32_t k = h.p[r]; k < h.p[r + 1]; ++k) cnt += !skip[h.i[k]];
-            e.p[r + 1] = e.p[r] + cnt;
+            e.p[r + 1] = cnt;
         }
+        for (int64_t r = 0; r < n; ++r) e.p[r + 1] += e.p[r];
         e.i.resize(e.p[n]);
         src.resize(e.p[n]);
+#pragma omp parallel for schedule(static)
         for (int64_t r = 0; r < n; ++r) {
             int32_t o = e.p[r];
             if (skip[r]) {
