@@ -564,44 +564,38 @@ __global__ void k_jacobi_first(const T* __restrict__ dinv, const T* __restrict__
     GRID_STRIDE(i, n) x[i] = w * dinv[i] * b[i];
 }
 
-// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x)
-template <class T, bool RESID>
+// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x); TPR lanes
+// per row, chosen per level from its mean row length.  The finest operator
+// is the embedded one (identity rows, no constrained columns): no mask.
+template <class T, bool RESID, int TPR>
 __global__ void __launch_bounds__(256)
     k_jacobi_sweep(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
                    const T* __restrict__ Ax, const T* __restrict__ dinv, const T* __restrict__ b,
-                   const T* __restrict__ x, T* __restrict__ out, T w, const uint8_t* __restrict__ dir) {
-    constexpr int TPR = 8, RPW = 32 / TPR;
+                   const T* __restrict__ x, T* __restrict__ out, T w) {
+    constexpr int RPW = 32 / TPR;
     const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t base = warp * RPW; base < n; base += n_warps * RPW) {
         const int64_t r = base + group;
         T acc = T(0);
-        bool fixed = false;
-        if (r < n) {
-            fixed = dir && dir[r];
-            if (!fixed)
-                for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) {
-                    int32_t c = Ai[k];
-                    if (!dir || !dir[c]) acc += Ax[k] * x[c];
-                }
-        }
+        if (r < n)
+            for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) acc += Ax[k] * x[Ai[k]];
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
         if (sub == 0 && r < n) {
-            T ax = fixed ? x[r] : acc;
-            T res = b[r] - ax;
+            const T res = b[r] - acc;
             out[r] = RESID ? res : x[r] + w * dinv[r] * res;
         }
     }
 }
 
-// y (+)= A x, rectangular (restriction / prolongation)
-template <class T, bool ADD>
+// y (+)= A x, rectangular (restriction / prolongation), TPR lanes per row
+template <class T, bool ADD, int TPR>
 __global__ void __launch_bounds__(256)
     k_spmv_rect(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai, const T* __restrict__ Ax,
                 const T* __restrict__ x, T* __restrict__ y) {
-    constexpr int TPR = 8, RPW = 32 / TPR;
+    constexpr int RPW = 32 / TPR;
     const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -614,6 +608,49 @@ __global__ void __launch_bounds__(256)
         for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
         if (sub == 0 && r < n) y[r] = ADD ? y[r] + acc : acc;
     }
+}
+
+// Lanes per row from the mean row length (thresholds tuned on B200).
+#ifndef UP3D_AMG_T4
+#define UP3D_AMG_T4 16
+#endif
+#ifndef UP3D_AMG_T8
+#define UP3D_AMG_T8 24
+#endif
+#ifndef UP3D_AMG_T16
+#define UP3D_AMG_T16 96
+#endif
+inline int lanes_per_row(int64_t nnz, int64_t n) {
+    const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
+    return avg <= UP3D_AMG_T4 ? 4 : avg <= UP3D_AMG_T8 ? 8 : avg <= UP3D_AMG_T16 ? 16 : 32;
+}
+inline unsigned rows_grid(int64_t n, int tpr) { return grid_for(n, 256 / tpr, (int64_t)148 * 64); }
+
+template <class T, bool RESID>
+void launch_sweep(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* dinv,
+                  const T* b, const T* x, T* out, T w, cudaStream_t s) {
+    switch (lanes_per_row(nnz, n)) {
+        case 4: k_jacobi_sweep<T, RESID, 4><<<rows_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
+        case 8: k_jacobi_sweep<T, RESID, 8><<<rows_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
+        case 16:
+            k_jacobi_sweep<T, RESID, 16><<<rows_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+            break;
+        default:
+            k_jacobi_sweep<T, RESID, 32><<<rows_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+    }
+    UP3D_CHECK_LAUNCH();
+}
+
+template <class T, bool ADD>
+void launch_rect(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* x, T* y,
+                 cudaStream_t s) {
+    switch (lanes_per_row(nnz, n)) {
+        case 4: k_spmv_rect<T, ADD, 4><<<rows_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+        case 8: k_spmv_rect<T, ADD, 8><<<rows_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+        case 16: k_spmv_rect<T, ADD, 16><<<rows_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+        default: k_spmv_rect<T, ADD, 32><<<rows_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, x, y);
+    }
+    UP3D_CHECK_LAUNCH();
 }
 
 // x = Cinv b (dense, one warp per row), FP64, inputs/outputs of type T
@@ -706,7 +743,6 @@ struct Level {
     DBuf<T> own_A, own_P, own_R, own_dinv;  // FP32 values (unused for FP64)
     DBuf<T> x, b, r;
     T w_smooth = T(0);
-    const uint8_t* dir = nullptr;  // finest level only
 };
 
 // Symbolic structure and FP64 values of one level.
@@ -786,33 +822,27 @@ void vcycle(Amg& a, std::vector<Level<T>*>& L, size_t l, cudaStream_t s) {
         UP3D_CHECK_LAUNCH();
         return;
     }
-    const unsigned g1 = grid_for(n, 256), g8 = grid_for(8 * n, 256, (int64_t)148 * 64);
+    const unsigned g1 = grid_for(n, 256);
+    const int64_t nnz = lv.A.nnz;
     // pre-smoothing from x = 0
     k_jacobi_first<T><<<g1, 256, 0, s>>>(lv.dinv.get(), lv.b.get(), lv.x.get(), lv.w_smooth, n);
     UP3D_CHECK_LAUNCH();
     for (int k = 1; k < a.pre; ++k) {
-        k_jacobi_sweep<T, false><<<g8, 256, 0, s>>>(n, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(),
-                                                    lv.b.get(), lv.x.get(), lv.r.get(), lv.w_smooth, lv.dir);
-        UP3D_CHECK_LAUNCH();
+        launch_sweep<T, false>(n, nnz, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(), lv.b.get(),
+                               lv.x.get(), lv.r.get(), lv.w_smooth, s);
         std::swap(lv.x.p, lv.r.p);
     }
     // residual, restriction
-    k_jacobi_sweep<T, true><<<g8, 256, 0, s>>>(n, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(),
-                                               lv.b.get(), lv.x.get(), lv.r.get(), lv.w_smooth, lv.dir);
-    UP3D_CHECK_LAUNCH();
+    launch_sweep<T, true>(n, nnz, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(), lv.b.get(), lv.x.get(),
+                          lv.r.get(), lv.w_smooth, s);
     Level<T>& cv = *L[l + 1];
-    k_spmv_rect<T, false><<<grid_for(8 * cv.A.n, 256, (int64_t)148 * 64), 256, 0, s>>>(
-        lv.R.n, lv.R.p.get(), lv.R.i.get(), lv.R.x.get(), lv.r.get(), cv.b.get());
-    UP3D_CHECK_LAUNCH();
+    launch_rect<T, false>(lv.R.n, lv.R.nnz, lv.R.p.get(), lv.R.i.get(), lv.R.x.get(), lv.r.get(), cv.b.get(), s);
     vcycle<T>(a, L, l + 1, s);
     // prolongation
-    k_spmv_rect<T, true><<<g8, 256, 0, s>>>(lv.P.n, lv.P.p.get(), lv.P.i.get(), lv.P.x.get(), cv.x.get(),
-                                            lv.x.get());
-    UP3D_CHECK_LAUNCH();
+    launch_rect<T, true>(lv.P.n, lv.P.nnz, lv.P.p.get(), lv.P.i.get(), lv.P.x.get(), cv.x.get(), lv.x.get(), s);
     for (int k = 0; k < a.post; ++k) {
-        k_jacobi_sweep<T, false><<<g8, 256, 0, s>>>(n, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(),
-                                                    lv.b.get(), lv.x.get(), lv.r.get(), lv.w_smooth, lv.dir);
-        UP3D_CHECK_LAUNCH();
+        launch_sweep<T, false>(n, nnz, lv.A.p.get(), lv.A.i.get(), lv.A.x.get(), lv.dinv.get(), lv.b.get(),
+                               lv.x.get(), lv.r.get(), lv.w_smooth, s);
         std::swap(lv.x.p, lv.r.p);
     }
 }
@@ -978,8 +1008,6 @@ void make_levels(Amg& a, std::vector<Level<T>*>& Lv, cudaStream_t s) {
                 lv->dinv.v = lv->own_dinv.get();
             }
         }
-        // lv->dir stays null: the embedded finest operator already has
-        // identity rows and no constrained columns
     }
 }
 
