@@ -23,6 +23,9 @@ namespace up3d {
 template <class T>
 void launch_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const T* x, T* y,
                  const uint8_t* dir, cudaStream_t s);
+template <class T>
+void launch_spmv2(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const int32_t* xptr,
+                  const int32_t* xidx, const T* xdata, const T* x, T* y, const uint8_t* dir, cudaStream_t s);
 
 namespace {
 
@@ -279,34 +282,16 @@ Blas& ws_blas(KrylovWs& w, cudaStream_t s) {
 // ------------------------------------------------------------ operators
 
 void Operator::apply(const double* x, double* y, cudaStream_t s) const {
-    launch_spmv<double>(A.n, A.indptr, A.indices, A.data, x, y, A.dirichlet, s);
-    if (extra.indptr) {
-        // y += extra x (Term-3 entries outside the P1 pattern)
-        tmp.alloc(A.n);
-        launch_spmv<double>(A.n, extra.indptr, extra.indices, extra.data, x, tmp.get(), A.dirichlet, s);
-        if (A.dirichlet) {
-            k_mask<double><<<grid_for(A.n, 256), 256, 0, s>>>(tmp.get(), A.dirichlet, A.n);
-            UP3D_CHECK_LAUNCH();
-        }
-        k_accumulate<double><<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp.get(), A.n);
-        UP3D_CHECK_LAUNCH();
-    }
+    // y = A x (+ extra x: the Term-3 entries outside the P1 pattern), one pass
+    launch_spmv2<double>(A.n, A.indptr, A.indices, A.data, extra.indptr, extra.indices, extra.data, x, y,
+                         A.dirichlet, s);
 }
 
 // FP32 operator: the FP32 copies of the values (data32, extra32).
 void Operator::apply(const float* x, float* y, cudaStream_t s) const {
     UP3D_REQUIRE(data32 && (!extra.indptr || extra32), UP3D_ERR_ARGUMENT, "FP32 operator without FP32 values");
-    launch_spmv<float>(A.n, A.indptr, A.indices, data32, x, y, A.dirichlet, s);
-    if (extra.indptr) {
-        tmp32.alloc(A.n);
-        launch_spmv<float>(A.n, extra.indptr, extra.indices, extra32, x, tmp32.get(), A.dirichlet, s);
-        if (A.dirichlet) {
-            k_mask<float><<<grid_for(A.n, 256), 256, 0, s>>>(tmp32.get(), A.dirichlet, A.n);
-            UP3D_CHECK_LAUNCH();
-        }
-        k_accumulate<float><<<grid_for(A.n, 256), 256, 0, s>>>(y, tmp32.get(), A.n);
-        UP3D_CHECK_LAUNCH();
-    }
+    launch_spmv2<float>(A.n, A.indptr, A.indices, data32, extra.indptr, extra.indices, extra32, x, y, A.dirichlet,
+                        s);
 }
 
 }  // namespace up3d

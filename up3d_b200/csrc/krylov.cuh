@@ -33,8 +33,6 @@ struct Operator {
     up3d_csr extra{};
     const float* data32 = nullptr;   // FP32 copies of the values (mixed precision)
     const float* extra32 = nullptr;
-    mutable DBuf<double> tmp;
-    mutable DBuf<float> tmp32;
     void apply(const double* x, double* y, cudaStream_t s) const;
     void apply(const float* x, float* y, cudaStream_t s) const;
 };
