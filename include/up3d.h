@@ -259,13 +259,17 @@ int up3d_jacobian_transpose(up3d_mesh* mesh, const double* data, double* data_t,
  * reference solves one case at a time): element e takes the flow of its
  * case, flows[case_of[e]] (host array of n_cases; one u_inf for all),
  * case_of a device int32 array of n_tets.  One launch of each pass covers
- * every case.  UP3D_ERR_VALUE for a case index outside [0, n_cases). */
+ * every case.  With frozen arrays, an element whose branch is negative
+ * stays live (cases freeze one by one).  branch_out (device int8, may be
+ * NULL) receives each element's branch: the frozen one, or the one a live
+ * element took (classify_upwind_branches, kernels/upwind.py:504-541).
+ * UP3D_ERR_VALUE for a case index outside [0, n_cases). */
 int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cases,
                                    const up3d_flow* flows, const int32_t* case_of,
                                    const int64_t* upstream_frozen, const int8_t* branch_frozen,
                                    double* R, double* data, double* rho_tilde_out,
-                                   int32_t* upstream_out, up3d_monitors* monitors,
-                                   up3d_stream stream);
+                                   int32_t* upstream_out, int8_t* branch_out,
+                                   up3d_monitors* monitors, up3d_stream stream);
 
 /* ------------------------------------------------------ accounting */
 

@@ -85,7 +85,7 @@ SIGNATURES = {
     "up3d_residual_jacobian": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_residual_vjp": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_transpose": (_int, [_p, _p, _p, _p]),
-    "up3d_residual_jacobian_batched": (_int, [_p, _p, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_residual_jacobian_batched": (_int, [_p, _p, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_launch_count": (_int, [ctypes.POINTER(_i64)]),
     "up3d_profile": (_int, [_int]),
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),

@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
                  double* __restrict__ rt_out, up3d_monitors* mon, const Flow* __restrict__ flows,
-                 const int32_t* __restrict__ case_of) {
+                 const int32_t* __restrict__ case_of, int8_t* __restrict__ br_out) {
     MonAcc acc;
     GRID_STRIDE(e, E) {
         const Flow& F = BATCH ? flows[case_of[e]] : F0;
@@ -338,7 +338,11 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
         // L1/L2 hit)
         double g[3];
         elem_grad(conn, B, phi, e, g);
-        int64_t u = FROZEN ? safe_up(up_fz[e], e, E) : upstream_walk(fn, disp, X, conn, e, E, g);
+        // frozen (upstream, branch) per element; a negative branch keeps the
+        // element live (several cases in one mesh, frozen one by one)
+        const int brf = FROZEN ? (int)br_fz[e] : -1;
+        const bool frz = FROZEN && brf >= 0;
+        int64_t u = frz ? safe_up(up_fz[e], e, E) : upstream_walk(fn, disp, X, conn, e, E, g);
         double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), u2);
         double q2l = q2n < F.q2cap ? q2n : F.q2cap;
         bool lim_e = q2l == q2n;
@@ -358,8 +362,9 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
         acc.lim += !lim_e;
 
         double nu, rt, s_e = 0.0, s_u = 0.0;
-        if (FROZEN) {
-            int br = br_fz[e];
+        if (frz) {
+            const int br = brf;
+            if (br_out) br_out[e] = (int8_t)br;
             if (br == 3) {
                 nu = 0.0;
                 rt = F.floor_;
@@ -373,8 +378,14 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
             }
             if (JAC) frozen_sensitivities(br, q2l, rho_e, q2lu, rho_u, F, s_e, s_u);
         } else {
-            nu = fmax(switch_of(mach2_of(q2l, F), F), switch_of(mach2_of(q2lu, F), F));
+            const double nu_e = switch_of(mach2_of(q2l, F), F), nu_u = switch_of(mach2_of(q2lu, F), F);
+            nu = fmax(nu_e, nu_u);
             rt = rho_e - nu * (rho_e - rho_u);
+            // the branch this live evaluation took (classify_upwind_branches,
+            // kernels/upwind.py:504-541)
+            if (br_out)
+                br_out[e] = (int8_t)(u == e ? (rho_e <= F.floor_ ? 3 : 0)
+                                            : (rt <= F.floor_ ? 3 : (nu == 0.0 ? 0 : (nu_e >= nu_u ? 1 : 2))));
             rt = rt > F.floor_ ? rt : F.floor_;
             acc.flo += (rt == F.floor_);
             if (JAC) live_sensitivities(q2l, rho_e, q2lu, rho_u, u == e, F, s_e, s_u);
@@ -803,13 +814,15 @@ __global__ void k_check_cases(const int32_t* __restrict__ case_of, int64_t E, in
 // case_of select per-element flows (several cases in one mesh) when set.
 static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
                            const int32_t* case_of, const int64_t* up_fz, const int8_t* br_fz, double* R,
-                           double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon, cudaStream_t s) {
+                           double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon, cudaStream_t s,
+                           int8_t* br_out = nullptr) {
     up3d_monitors* mo = mon ? mon : m->mon_ws.get();
     UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
     const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
 #define FUSED_ARGS                                                                                                \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
-        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of
+        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of, \
+        br_out
     const bool jac = data != nullptr;
     prof_begin(PROF_ELEM, s);
     if (flows_d) {
@@ -875,8 +888,8 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
 
 int up3d_residual_jacobian_batched(up3d_mesh* m, const double* phi, int n_cases, const up3d_flow* flows,
                                    const int32_t* case_of, const int64_t* up_fz, const int8_t* br_fz, double* R,
-                                   double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon,
-                                   up3d_stream stream) {
+                                   double* data, double* rt_out, int32_t* up_out, int8_t* branch_out,
+                                   up3d_monitors* mon, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(m && phi && flows && case_of && R && n_cases > 0, UP3D_ERR_ARGUMENT,
                      "up3d_residual_jacobian_batched: null argument");
@@ -901,7 +914,7 @@ int up3d_residual_jacobian_batched(up3d_mesh* m, const double* phi, int n_cases,
         UP3D_CUDA(cudaStreamSynchronize(s));
         UP3D_REQUIRE(!hbad, UP3D_ERR_VALUE, "up3d_residual_jacobian_batched: case index out of range");
         fused_evaluate(m, phi, host[0], flows[0].u_inf * flows[0].u_inf, m->flows_ws.get(), case_of, up_fz, br_fz,
-                       R, data, rt_out, up_out, mon, s);
+                       R, data, rt_out, up_out, mon, s, branch_out);
     });
 }
 

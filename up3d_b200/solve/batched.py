@@ -15,8 +15,11 @@ ingredients per case -- Picard seed, exact Jacobian, GMRES(60) + AMG rebuilt
 active cases), a merit line search with up to five halvings decided per case,
 and the Mach continuation as a shared ramp that each case follows up to its
 own target.  A case stops moving once its |R_free|_inf is below the
-tolerance at its target Mach.  Unlike the plain driver there is no frozen
-(upstream, branch) finish: a case that needs it is reported unconverged.
+tolerance at its target Mach.  Each case freezes its (upstream, branch)
+state once its residual is below ``freeze_tol`` (the plain driver's frozen
+finish; the other cases stay live in the same launches) and is accepted on
+frozen convergence -- the plain driver's refresh / revert of the frozen state
+is not repeated here.
 """
 
 from __future__ import annotations
@@ -55,6 +58,27 @@ class BatchedChannels:
         self.case_of_node = t.from_numpy(case_n).cuda()
         self.n_tets = int(elem_off[-1])
         self.u_inf = float(u_inf)
+        self.branch = t.empty(self.n_tets, dtype=t.int8, device="cuda")
+        self.up_fz = None   # (E) int64 frozen upstream, once a case freezes
+        self.br_fz = None   # (E) int8 frozen branch, -1 = live
+
+    def unfreeze(self, cases):
+        """Return the listed cases to the live flux."""
+        if self.br_fz is None:
+            return
+        for c in cases:
+            self.br_fz[int(self.elem_off[c]):int(self.elem_off[c + 1])] = -1
+
+    def freeze(self, cases):
+        """Freeze the listed cases at the state of the last evaluation."""
+        t = L.torch()
+        if self.up_fz is None:
+            self.up_fz = t.zeros(self.n_tets, dtype=t.int64, device="cuda")
+            self.br_fz = t.full((self.n_tets,), -1, dtype=t.int8, device="cuda")
+        for c in cases:
+            a, b = int(self.elem_off[c]), int(self.elem_off[c + 1])
+            self.up_fz[a:b] = self.ws.ev.upstream[a:b].to(t.int64)
+            self.br_fz[a:b] = self.branch[a:b]
 
     def _flows(self, machs):
         arr = (L.Flow * self.n_cases)()
@@ -67,9 +91,9 @@ class BatchedChannels:
         into the union workspace."""
         ev = self.ws.ev
         L.call("up3d_residual_jacobian_batched", ev.mesh.handle, phi.data_ptr(), self.n_cases,
-               self._flows(machs), self.case_of_elem.data_ptr(), None, None, ev.R.data_ptr(),
-               ev.data.data_ptr() if jacobian else None, ev.rho_tilde.data_ptr(),
-               ev.upstream.data_ptr(), ev.monitors.data_ptr(), L.stream_ptr())
+               self._flows(machs), self.case_of_elem.data_ptr(), L.ptr(self.up_fz), L.ptr(self.br_fz),
+               ev.R.data_ptr(), ev.data.data_ptr() if jacobian else None, ev.rho_tilde.data_ptr(),
+               ev.upstream.data_ptr(), self.branch.data_ptr(), ev.monitors.data_ptr(), L.stream_ptr())
         return ev.R
 
     def per_case(self, v, op: str):
@@ -84,7 +108,8 @@ class BatchedChannels:
 def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start: float = 0.70,
                          dm: float = 0.05, tol_residual: float = 1e-10, n_newton_max: int = 30,
                          n_picard_seed: int = 5, amg_rebuild_every: int = 2, gmres_restart: int = 60,
-                         gmres_maxiter: int = 10, verbose: bool = False) -> Dict[str, object]:
+                         gmres_maxiter: int = 10, freeze_tol: float = 1e-6, freeze_refresh_max: int = 2,
+                         verbose: bool = False) -> Dict[str, object]:
     """Lockstep Newton of every case (module docstring); returns the union
     potential, per-case convergence, iteration counts and timings."""
     t = L.require_cuda()
@@ -102,6 +127,9 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
     converged_at = np.full(C, -1.0)
     converged_s = np.full(C, np.nan)
     failed = np.zeros(C, dtype=bool)
+    frozen = np.zeros(C, dtype=bool)
+    n_refresh = np.zeros(C, dtype=np.int64)
+    prev_live = np.full(C, np.nan)
     n_newton = np.zeros(C, dtype=np.int64)
     n_gmres_total = 0
     phi = ws.freestream.clone()
@@ -124,8 +152,13 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
 
     for lvl, m_lev in enumerate(levels):
         m_level = np.minimum(machs, m_lev)
-        # cases already converged at their target stay put
+        # cases already converged at their target stay put; the others start
+        # the level live (each level is a fresh Newton solve)
         active = ~failed & ~((converged_at >= 0) & (m_level == machs))
+        batch.unfreeze(np.nonzero(active)[0])
+        frozen &= ~active
+        n_refresh[active] = 0
+        prev_live[active] = np.nan
         history = []
         eta_prev = None
         for it in range(n_newton_max):
@@ -135,6 +168,28 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
             merit = batch.per_case(Rf, "sumsq")
             history.append(r_case.copy())
             done = r_case < tol_residual
+            # frozen convergence: check the live residual; refreeze there (at
+            # most freeze_refresh_max times) while it has not converged and
+            # still improves, as the plain driver does
+            fdone = np.nonzero(active & done & frozen)[0]
+            if len(fdone):
+                batch.unfreeze(fdone)
+                R_live = batch.evaluate(phi, m_level, jacobian=False)
+                r_live = batch.per_case(R_live.masked_fill(mask_b, 0.0), "amax").cpu().numpy()
+                refreeze = [c for c in fdone if r_live[c] >= tol_residual and n_refresh[c] < freeze_refresh_max
+                            and (np.isnan(prev_live[c]) or r_live[c] <= 0.5 * prev_live[c])]
+                for c in refreeze:
+                    n_refresh[c] += 1
+                    prev_live[c] = r_live[c]
+                    done[c] = False
+                accepted_frozen = [c for c in fdone if c not in refreeze]
+                batch.freeze(refreeze)  # the state of the live evaluation just made
+                batch.freeze(accepted_frozen)
+                if refreeze:
+                    R = batch.evaluate(phi, m_level, jacobian=False)
+                    Rf = R.masked_fill(mask_b, 0.0)
+                    r_case = batch.per_case(Rf, "amax").cpu().numpy()
+                    merit = batch.per_case(Rf, "sumsq")
             for c in np.nonzero(active & done)[0]:
                 if m_level[c] == machs[c]:
                     converged_at[c] = m_level[c]
@@ -142,6 +197,19 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
             active = active & ~done
             if not active.any():
                 break
+            # frozen finish, case by case
+            stalled = np.zeros(C, dtype=bool)
+            if len(history) >= 7:
+                # the plain driver's stall test: no progress over six steps
+                prev_min = np.min(np.array(history[-7:-1]), axis=0)
+                stalled = (r_case < 1e-3) & (r_case > 0.25 * prev_min) & (r_case < 2.0 * prev_min)
+            to_freeze = active & ~frozen & ((r_case < freeze_tol) | stalled)
+            if to_freeze.any():
+                batch.freeze(np.nonzero(to_freeze)[0])
+                frozen |= to_freeze
+                R = batch.evaluate(phi, m_level, jacobian=False)
+                Rf = R.masked_fill(mask_b, 0.0)
+                merit = batch.per_case(Rf, "sumsq")
             batch.evaluate(phi, m_level, jacobian=True)
             J = with_dirichlet(ws.ev.jacobian(), ws.mask)
             if M_pre is None or it % amg_rebuild_every == 0:
@@ -153,9 +221,14 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
             eta = min(etas)
             eta_prev = eta
             act_node = t.from_numpy(active).cuda()[case_node]
-            rhs = (-Rf).masked_fill(~act_node, 0.0)
-            dphi, n_it, _ = solve_gmres(J, rhs, M=M_pre, rtol=eta, restart=gmres_restart,
-                                        maxiter=gmres_maxiter, on_fail="return")
+            # each case's block of the right-hand side scaled to unit norm, so
+            # that the joint Krylov residual weighs the cases equally (the
+            # Jacobian is block diagonal: the scaling comes back out exactly)
+            scale = t.sqrt(merit).clamp_min(1e-300)
+            rhs = (-Rf / scale[case_node]).masked_fill(~act_node, 0.0)
+            y, n_it, _ = solve_gmres(J, rhs, M=M_pre, rtol=eta / np.sqrt(active.sum()),
+                                     restart=gmres_restart, maxiter=gmres_maxiter, on_fail="return")
+            dphi = y * scale[case_node]
             n_gmres_total += n_it
             n_newton[active] += 1
             dphi = dphi.masked_fill(mask_b | ~act_node, 0.0)
@@ -187,4 +260,4 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
     t_total = clock() - t0
     return {"phi": phi, "converged": converged_at >= 0, "failed": failed, "n_newton": n_newton,
             "n_gmres_total": n_gmres_total, "levels": levels, "time_s": t_total, "seed_s": t_seed,
-            "converged_s": converged_s}
+            "converged_s": converged_s, "froze": frozen}
