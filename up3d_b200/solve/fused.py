@@ -109,8 +109,9 @@ class ResidualJacobian:
 
 class HostPipeline:
     """Residual + Jacobian evaluations on host buffers, double-buffered:
-    step k's phi upload and result download run on a copy stream while the
-    evaluation of the neighbouring step runs on the compute stream.  Every
+    uploads and downloads run on two copy streams (PCIe is full duplex), so
+    step k's results come back while step k+1's phi goes up and step k+1 is
+    evaluated on the compute stream.  Every
     step still copies its phi host -> device and its R and Jacobian data
     device -> host; ``finish()`` returns when all requested results are in
     their host buffers."""
@@ -120,7 +121,8 @@ class HostPipeline:
         self.ev = ev
         m = ev.mesh
         self.compute = t.cuda.current_stream()
-        self.copy = t.cuda.Stream()
+        self.up = t.cuda.Stream()
+        self.down = t.cuda.Stream()
         self.slots = []
         for _ in range(2):
             self.slots.append({
@@ -129,28 +131,29 @@ class HostPipeline:
                 "J": t.empty(m.nnz, dtype=t.float64, device="cuda"),
                 "free": t.cuda.Event(), "loaded": t.cuda.Event(), "done": t.cuda.Event(),
             })
-            self.slots[-1]["free"].record(self.copy)
+            self.slots[-1]["free"].record(self.down)
         self.k = 0
 
     def submit(self, phi_host, flow: FlowParams, R_host, J_host) -> None:
         t = L.torch()
         s = self.slots[self.k % 2]
         self.k += 1
-        with t.cuda.stream(self.copy):
-            self.copy.wait_event(s["free"])
+        with t.cuda.stream(self.up):
+            self.up.wait_event(s["free"])
             s["phi"].copy_(phi_host, non_blocking=True)
-            s["loaded"].record(self.copy)
+            s["loaded"].record(self.up)
         self.compute.wait_event(s["loaded"])
         with t.cuda.stream(self.compute):
             self.ev.evaluate(s["phi"], flow, jacobian=True, keep_state=False, R_out=s["R"],
                              data_out=s["J"])
             s["done"].record(self.compute)
-        with t.cuda.stream(self.copy):
-            self.copy.wait_event(s["done"])
+        with t.cuda.stream(self.down):
+            self.down.wait_event(s["done"])
             R_host.copy_(s["R"], non_blocking=True)
             J_host.copy_(s["J"], non_blocking=True)
-            s["free"].record(self.copy)
+            s["free"].record(self.down)
 
     def finish(self) -> None:
-        self.copy.synchronize()
+        self.up.synchronize()
+        self.down.synchronize()
         self.compute.synchronize()
