@@ -494,46 +494,71 @@ __global__ void __launch_bounds__(WARPS * 32)
             continue;
         }
         __syncwarp();
-        // 2. stable sort by column (rank = smaller columns + equal columns before)
-        for (int p = lane; p < P; p += 32) {
-            const int32_t c = col0[p];
-            int r = 0;
-            for (int q = 0; q < P; ++q) {
-                const int32_t cq = col0[q];
-                r += (cq < c) || (cq == c && q < p);
-            }
-            col1[r] = c;
-            val1[r] = val0[p];
-        }
-        __syncwarp();
-        // 3. per-column sums: into the pattern, else to the extras
-        const int32_t rb = indptr[n], L = indptr[n + 1] - rb;
-        int X = 0;
+        // 2. the distinct columns in order of first appearance, each with the
+        //    sequential sum of its entries in (element, k) order: chunks of 32
+        //    entries, equal columns grouped by match_any, the group's lowest
+        //    lane adding the group's values in lane (= entry) order to the
+        //    column's running sum -- the reference's duplicate summation order
+        int D = 0;
         for (int base = 0; base < P; base += 32) {
             const int p = base + lane;
-            const bool head = p < P && (p == 0 || col1[p] != col1[p - 1]);
-            bool extra = false;
-            int32_t c = 0;
-            double v = 0.0;
-            if (head) {
-                c = col1[p];
-                for (int q = p; q < P && col1[q] == c; ++q) v += val1[q];
-                int32_t lo = 0, hi = L;
-                while (lo < hi) {
-                    const int32_t mid = (lo + hi) >> 1;
-                    if (indices[rb + mid] < c) lo = mid + 1;
-                    else hi = mid;
+            const bool valid = p < P;
+            const int32_t c = valid ? col0[p] : -1 - lane;  // idle lanes: distinct dummies
+            const unsigned grp = __match_any_sync(0xffffffffu, c);
+            const bool leader = valid && (__ffs(grp) - 1) == lane;
+            int idx = -1;
+            if (leader)
+                for (int d = 0; d < D; ++d)
+                    if (col1[d] == c) {
+                        idx = d;
+                        break;
+                    }
+            const unsigned newm = __ballot_sync(0xffffffffu, leader && idx < 0);
+            if (leader) {
+                double acc_c = 0.0;
+                if (idx < 0) idx = D + __popc(newm & lt);
+                else acc_c = val1[idx];
+                unsigned gm = grp;
+                while (gm) {
+                    const int j = __ffs(gm) - 1;
+                    gm &= gm - 1;
+                    acc_c += val0[base + j];
                 }
-                if (lo < L && indices[rb + lo] == c) data[rb + lo] += v;
-                else extra = true;
+                col1[idx] = c;
+                val1[idx] = acc_c;
             }
-            const unsigned m = __ballot_sync(0xffffffffu, extra);
+            D += __popc(newm);
+            __syncwarp();
+        }
+        // 3. per distinct column: into the P1 slot, else an extra; extras are
+        //    written in column order (rank among the row's extra columns)
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb;
+        for (int d = lane; d < D; d += 32) {
+            const int32_t c = col1[d];
+            int32_t lo = 0, hi = L;
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (indices[rb + mid] < c) lo = mid + 1;
+                else hi = mid;
+            }
+            const bool in_pattern = lo < L && indices[rb + lo] == c;
+            if (in_pattern) data[rb + lo] += val1[d];
+            col0[d] = in_pattern ? INT32_MAX : c;  // extra columns, for the ranks
+        }
+        __syncwarp();
+        int X = 0;
+        for (int base = 0; base < D; base += 32) {
+            const int d = base + lane;
+            const bool extra = d < D && col0[d] != INT32_MAX;
             if (extra) {
-                const int64_t o = 4 * (int64_t)eb + X + __popc(m & lt);
+                const int32_t c = col0[d];
+                int r = 0;
+                for (int q = 0; q < D; ++q) r += col0[q] < c;
+                const int64_t o = 4 * (int64_t)eb + r;
                 xs_col[o] = c;
-                xs_val[o] = v;
+                xs_val[o] = val1[d];
             }
-            X += __popc(m);
+            X += __popc(__ballot_sync(0xffffffffu, extra));
         }
         if (lane == 0) x_cnt[n] = X;
         __syncwarp();
