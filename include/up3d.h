@@ -377,8 +377,9 @@ int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double
  * GMRES in FP32 -- A's FP32 values `data32` (and `extra32` for `extra`),
  * FP32 vectors, M applied in FP32 (an FP32 AMG hierarchy keeps its
  * coarsest solve in FP64) -- to max(inner_rtol, tol / ||r||) relative, and
- * is added to x in FP64.  inner = total Arnoldi steps, outer = corrections.
- * Synchronous. */
+ * is added to x in FP64; once a correction fails to halve the true
+ * residual, FP64 GMRES finishes the solve from the current iterate.
+ * inner = total Arnoldi steps, outer = corrections.  Synchronous. */
 int up3d_gmres_ir(const up3d_csr* A, const up3d_csr* extra, const float* data32,
                   const float* extra32, const double* b, double* x, double rtol, double atol,
                   int restart, int maxiter, int refine_max, double inner_rtol, up3d_precond* M,

@@ -574,7 +574,9 @@ template int gmres_solve<float>(const Operator&, const float*, float*, double, d
 // ||r|| <= max(rtol ||b||, atol); each inner solve is restarted GMRES on the
 // FP32 operator (data32, extra32) and FP32 vectors with the preconditioner
 // applied in FP32, to max(inner_rtol, tol / ||r||) relative, and its
-// correction is added to x in FP64.  Returns 0 when converged.
+// correction is added to x in FP64.  A correction that fails to halve the
+// true residual hands the rest of the solve to FP64 GMRES.  Returns 0 when
+// converged.
 int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart,
                    int maxiter, int refine_max, double inner_rtol, up3d_precond* M, int64_t* inner, int64_t* outer,
                    double* resid, cudaStream_t s) {
@@ -593,13 +595,23 @@ int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, 
     const double bnrm = bl.nrm2(b, n);
     const double tol = eff_atol(atol, rtol, bnrm);
     int64_t tot_inner = 0, it = 0;
-    double rn = 0.0;
+    double rn = 0.0, rn_prev = 0.0;
     for (;; ++it) {
         op.apply(x, tmp.get(), s);
         k_sub<double><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
         UP3D_CHECK_LAUNCH();
         rn = bl.nrm2(r.get(), n);
         if (rn <= tol || !std::isfinite(rn) || it >= refine_max) break;
+        if (it > 0 && rn > 0.5 * rn_prev) {
+            // the FP32 corrections stopped paying (a system too ill-conditioned
+            // for FP32): finish with FP64 GMRES from the current iterate
+            int64_t inn = 0;
+            gmres_solve<double>(op, b, x, rtol, atol, restart, maxiter, M, &inn, &rn, s);
+            tot_inner += inn;
+            ++it;
+            break;
+        }
+        rn_prev = rn;
         k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(r.get(), r32.get(), n);
         UP3D_CHECK_LAUNCH();
         UP3D_CUDA(cudaMemsetAsync(d32.get(), 0, sizeof(float) * n, s));
