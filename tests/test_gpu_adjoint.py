@@ -138,3 +138,24 @@ def test_adjoint_matches_reference_jacobian_transpose_solve(subsonic_gradient):
     lam_ref = spla.spsolve(J.tocsr()[free][:, free].T.tocsc(), rhs)
     lam = g["lambda"].cpu().numpy()[free]
     assert np.abs(lam - lam_ref).max() <= 1e-8 * np.abs(lam_ref).max()
+
+
+def test_drag_gradient_matches_finite_differences():
+    """The drag-like (x) wall force: the x components of the wall faces'
+    area vectors follow the wall slope, so the shape modes act on it both
+    through Cp (the adjoint part) and through the geometry (explicit part)."""
+    from up3d_b200.adjoint import BumpShape, adjoint_gradient, objective_value
+    shape = BumpShape(16, 6, 5, amplitude=0.05, seed=0)
+    kw = {"tol_residual": 1e-13, "n_newton_max": 40}
+    g = adjoint_gradient(shape, 0.5, solve_kw=kw, axis=0)
+
+    def fk(s, k):
+        e = np.zeros(shape.n_params)
+        e[k] = s
+        return objective_value(shape, 0.5, p=e, solve_kw=kw, axis=0)
+
+    for k in (3, 9):
+        h = 1e-4
+        fd = (8.0 * (fk(h, k) - fk(-h, k)) - (fk(2 * h, k) - fk(-2 * h, k))) / (12.0 * h)
+        ad = float(g["dF_dp"][k])
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), abs(fd)), (k, fd, ad)

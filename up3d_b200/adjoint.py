@@ -1,5 +1,5 @@
 """Discrete adjoint of the full-potential channel solve: shape and Mach
-gradients of a lift-like wall-pressure integral.
+gradients of the lift-like and drag-like wall-pressure integrals.
 
 The reference has no adjoint; this module adds one on top of its discrete
 equations (the residual of kernels/jacobian.py and kernels/upwind.py):
@@ -8,7 +8,8 @@ equations (the residual of kernels/jacobian.py and kernels/upwind.py):
   by the base Gaussian plus ``n_side x n_side`` Gaussian shape modes whose
   amplitudes are the design parameters (centres on a grid over the bump,
   jittered from a seed);
-* ``lift_objective`` -- F = -sum over lower-wall faces of Cp_e (S_f . z),
+* ``lift_objective`` -- F = -sum over lower-wall faces of Cp_e (S_f . e),
+  e = z (lift-like) or x (drag-like),
   Cp_e the pressure coefficient of the face's element (physics/isentropic.py
   pressure_coefficient at the element's limited speed) and S_f the outward
   area vector, with its explicit partial derivatives (torch autograd);
@@ -114,10 +115,12 @@ def _cp_torch(q2n, mach, gamma=GAMMA, m_cap=3.0):
     return 2.0 / (gamma * m2) * (rho ** gamma - 1.0)
 
 
-def lift_objective(X, q2n_elem, faces_dev, mach, interior_nodes_dev, gamma=GAMMA):
-    """F = -sum_f Cp_e(f) (S_f . z), S_f the outward area vector of the
-    face (away from the element's fourth node).  All arguments are torch
-    tensors; X (N, 3), q2n_elem (E) and mach may require grad."""
+def lift_objective(X, q2n_elem, faces_dev, mach, interior_nodes_dev, gamma=GAMMA, axis: int = 2):
+    """F = -sum_f Cp_e(f) (S_f . e_axis), S_f the outward area vector of the
+    face (away from the element's fourth node): the lift-like force on the
+    lower wall for axis 2 (z), the drag-like one for axis 0 (x).  All
+    arguments are torch tensors; X (N, 3), q2n_elem (E) and mach may require
+    grad."""
     t = L.torch()
     e = faces_dev[:, 0]
     a, b, c = X[faces_dev[:, 1]], X[faces_dev[:, 2]], X[faces_dev[:, 3]]
@@ -125,9 +128,9 @@ def lift_objective(X, q2n_elem, faces_dev, mach, interior_nodes_dev, gamma=GAMMA
     # orientation: outward, away from the element's off-face node
     d = X[interior_nodes_dev] - a
     sign = t.where((S * d).sum(dim=1) > 0, -1.0, 1.0).to(X.dtype)
-    Sz = sign.detach() * S[:, 2]
+    Sa = sign.detach() * S[:, axis]
     cp = _cp_torch(q2n_elem[e], mach, gamma)
-    return -(cp * Sz).sum()
+    return -(cp * Sa).sum()
 
 
 def transpose_csr(A):
@@ -228,9 +231,10 @@ class ResidualFunction:
 
 def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[float] = None,
                      dm: float = 0.05, tol_lambda: float = 1e-12, ws=None,
-                     solve_kw: Optional[dict] = None) -> Dict[str, object]:
+                     solve_kw: Optional[dict] = None, axis: int = 2) -> Dict[str, object]:
     """Converges the channel at (p, M_inf) on the device, then returns the
-    objective F, dF/dp (n_params), dF/dM_inf, the adjoint lam and timings."""
+    objective F (lift-like for axis 2, drag-like for axis 0), dF/dp
+    (n_params), dF/dM_inf, the adjoint lam and timings."""
     t = L.require_cuda()
     from .solve.fused import FlowParams
     from .solve.linear import amg_for, solve_gmres, with_dirichlet
@@ -260,7 +264,7 @@ def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[fl
         opp[r] = [v for v in mesh.elements[e] if v not in (a, b, c)][0]
     faces_d = t.from_numpy(faces).cuda()
     M = t.tensor(float(mach), dtype=t.float64, device="cuda", requires_grad=True)
-    F = lift_objective(X, q2n, faces_d, M, t.from_numpy(opp).cuda())
+    F = lift_objective(X, q2n, faces_d, M, t.from_numpy(opp).cuda(), axis=axis)
     gX_exp, gq2, gM_exp = t.autograd.grad(F, (X, q2n, M))
     w = gq2.contiguous()
     # dF/dphi, then J^T lam = dF/dphi on the free DOFs
@@ -275,7 +279,7 @@ def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[fl
     _, dX, dMr = actx.vjp(lam=(-lam).contiguous(), w_q2=w)
     dX_total = gX_exp.detach() + dX
     dz = t.from_numpy(shape.dz_dp()).cuda()
-    dFdp = (dX_total[:, 2:3] * dz).sum(dim=0)
+    dFdp = (dX_total[:, 2:3] * dz).sum(dim=0)  # the modes move z only
     dFdM = float(gM_exp) + float(dMr)
     t.cuda.synchronize()
     timings["adjoint_s"] = time.perf_counter() - c1
@@ -285,7 +289,7 @@ def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[fl
 
 
 def objective_value(shape: BumpShape, mach: float, p=None, m_start: Optional[float] = None,
-                    dm: float = 0.05, solve_kw: Optional[dict] = None) -> float:
+                    dm: float = 0.05, solve_kw: Optional[dict] = None, axis: int = 2) -> float:
     """F at (p, M_inf) after a converged solve (for finite differences)."""
     t = L.require_cuda()
     from .solve.newton import ChannelWorkspace, solve_newton_transonic
@@ -302,4 +306,4 @@ def objective_value(shape: BumpShape, mach: float, p=None, m_start: Optional[flo
     X = t.from_numpy(mesh.nodes).cuda()
     M = t.tensor(float(mach), dtype=t.float64, device="cuda")
     return float(lift_objective(X, q2 / ws.u_inf ** 2, t.from_numpy(faces).cuda(), M,
-                                t.from_numpy(opp).cuda()))
+                                t.from_numpy(opp).cuda(), axis=axis))
