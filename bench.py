@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--cpu-states", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pocket-steps", type=int, default=300)
+    p.add_argument("--tune", default="auto",
+                   help="launch shapes: 'auto' (autotuner), 'default', or "
+                        "'persistent,prefetch,row_lanes'")
     p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
                    help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
     p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
@@ -402,6 +405,12 @@ def run_ours(args):
     d_phis = [torch.from_numpy(p).cuda() for p in phis]
     stream = torch.cuda.current_stream()
 
+    if args.tune == "auto":
+        dmesh.autotune(d_phis[0], flow, reps=5)
+    elif args.tune != "default":
+        dmesh.set_tuning(*(int(v) for v in args.tune.split(",")))
+    tuning = dmesh.tuning()
+
     def step(k):
         ev.evaluate(d_phis[k % N_STATES], flow, jacobian=True, keep_state=False)
 
@@ -547,6 +556,7 @@ def run_ours(args):
                     "h2d_bytes_per_step": 8 * dmesh.n_nodes,
                     "d2h_bytes_per_step": 8 * dmesh.n_nodes + 8 * dmesh.nnz},
             "gpu_launches": int(launches),
+            "tuning": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in tuning.items()},
             "clocks": clocks.summary(),
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
             "pocket_states": pocket,

@@ -271,6 +271,43 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
                                    int32_t* upstream_out, int8_t* branch_out,
                                    up3d_monitors* monitors, up3d_stream stream);
 
+/* ------------------------------------------------------ launch shapes */
+
+/* Launch shapes of the fused evaluation's two passes (no reference
+ * counterpart: numba picks its own).  Every shape computes the same bits:
+ * the element sweep's per-element arithmetic does not depend on the grid,
+ * and the row gather sums every row in a fixed 32-slot order whatever its
+ * lanes per row.
+ *   elem_persistent  0: one thread per element (grid capped at 64 blocks
+ *                    per SM); 1: one resident wave of blocks looping over
+ *                    256-element tiles
+ *   elem_prefetch    persistent sweep: the tile this many iterations ahead
+ *                    is prefetched into L2 (bulk prefetch) before each
+ *                    tile; 0 = none (ignored when not persistent)
+ *   row_lanes        lanes per row of the row gather: 4, 8, 16 or 32
+ *   elem_us, row_us  autotune output: median time per launch of the
+ *                    chosen shapes (0 when set by hand) */
+typedef struct {
+    int32_t elem_persistent;
+    int32_t elem_prefetch;
+    int32_t row_lanes;
+    int32_t reserved;
+    double elem_us;
+    double row_us;
+} up3d_tuning;
+
+/* Default: {0, 0, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
+int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
+int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
+
+/* Times every candidate shape of the two passes on this mesh (the Newton
+ * Jacobian sweep at phi and the flow, live upwind selection; `reps` timed
+ * launches each after one warm-up, median kept), installs the fastest and
+ * returns it in `tuning` (may be NULL).  Overwrites the mesh's internal
+ * workspaces only; synchronises the stream. */
+int up3d_autotune(up3d_mesh* mesh, const double* phi, const up3d_flow* flow, int reps,
+                  up3d_tuning* tuning, up3d_stream stream);
+
 /* ------------------------------------------------------ accounting */
 
 /* Number of library kernel launches since the library was loaded (the

@@ -1,0 +1,85 @@
+"""Launch shapes of the fused evaluation: every shape (one thread per
+element or a persistent wave with L2 prefetch; 4-32 lanes per row) gives the
+same bits, the autotuner installs one of them, and bad shapes are refused."""
+
+import numpy as np
+import pytest
+
+from conftest import has_cuda, rel_err
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
+
+SHAPES = [(0, 0, 4), (0, 0, 8), (1, 0, 8), (1, 1, 16), (1, 2, 32), (1, 4, 4), (0, 3, 16)]
+
+
+def _setup():
+    import torch
+    from up3d_b200.mesh.device import DeviceMesh
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    from up3d_b200.solve.fused import ResidualJacobian
+    # 30x10x9 hexes: 16,200 tets, not a multiple of the 256-element tile
+    mesh = bump_channel(30, 10, 9, amplitude=0.08, seed=2)
+    phi_h = pocket_state(mesh, "mixed")
+    dm = DeviceMesh(mesh.nodes, mesh.elements)
+    return mesh, phi_h, dm, ResidualJacobian(dm), torch.from_numpy(phi_h).cuda()
+
+
+def _outputs(ev, phi, flow, frozen=None):
+    R = ev.evaluate(phi, flow, jacobian=True, frozen=frozen).clone()
+    J = ev.jacobian().to_scipy()
+    return R, J, ev.upstream.clone(), ev.rho_tilde.clone(), ev.read_monitors()
+
+
+def test_every_shape_gives_the_same_bits():
+    import torch
+    from up3d_b200.solve.fused import FlowParams
+    mesh, phi_h, dm, ev, phi = _setup()
+    assert dm.n_tets % 256 != 0
+    flow = FlowParams(m_inf=0.8)
+    assert dm.tuning()["row_lanes"] == 8 and dm.tuning()["elem_persistent"] == 0
+    R0, J0, up0, rt0, mon0 = _outputs(ev, phi, flow)
+    assert mon0["n_term3_active"] > 0
+    frozen = (up0.to(torch.int64), torch.zeros(dm.n_tets, dtype=torch.int8, device="cuda"))
+    Rf0 = ev.evaluate(phi, flow, jacobian=True, frozen=frozen).clone()
+    Rr0 = ev.evaluate(phi, flow, jacobian=False).clone()
+    # the residual-only gather sums in the row gather's order
+    assert torch.equal(Rr0, R0)
+    for p, pf, lanes in SHAPES:
+        dm.set_tuning(p, pf, lanes)
+        R, J, up, rt, mon = _outputs(ev, phi, flow)
+        assert torch.equal(R, R0), (p, pf, lanes)
+        assert (J != J0).nnz == 0 and J.nnz == J0.nnz, (p, pf, lanes)
+        assert torch.equal(up, up0) and torch.equal(rt, rt0)
+        assert mon == mon0
+        assert torch.equal(ev.evaluate(phi, flow, jacobian=True, frozen=frozen), Rf0)
+        assert torch.equal(ev.evaluate(phi, flow, jacobian=False), Rr0)
+
+
+def test_autotune_installs_a_listed_shape_and_keeps_parity():
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.solve.fused import FlowParams
+    mesh, phi_h, dm, ev, phi = _setup()
+    flow = FlowParams(m_inf=0.8)
+    R0 = ev.evaluate(phi, flow, jacobian=True).clone()
+    J0 = ev.jacobian().to_scipy()
+    t = dm.autotune(phi, flow, reps=3)
+    assert t == dm.tuning()
+    assert (t["elem_persistent"], t["elem_prefetch"]) in {(0, 0), (1, 0), (1, 1), (1, 2), (1, 4)}
+    assert t["row_lanes"] in (4, 8, 16, 32)
+    assert t["elem_us"] > 0 and t["row_us"] > 0
+    R = ev.evaluate(phi, flow, jacobian=True).clone()
+    assert torch.equal(R, R0)
+    assert (ev.jacobian().to_scipy() != J0).nnz == 0
+    ref = O.chain(O.PicardOperator(mesh.nodes, mesh.elements),
+                  O.UpwindOperator(mesh.nodes, mesh.elements), phi_h, 0.8)
+    assert rel_err(R.cpu().numpy(), ref["R"]) < 1e-12
+
+
+def test_bad_shapes_are_refused():
+    _, _, dm, _, _ = _setup()
+    for bad in [(2, 0, 8), (1, -1, 8), (1, 9, 8), (0, 0, 2), (0, 0, 12), (0, 0, 64)]:
+        with pytest.raises(ValueError):
+            dm.set_tuning(*bad)
+    assert dm.tuning()["row_lanes"] == 8

@@ -46,6 +46,15 @@ class MeshInfo(ctypes.Structure):
                 ("max_node_degree", _i32), ("n_colors", _i32), ("device", _i32)]
 
 
+class Tuning(ctypes.Structure):
+    """up3d_tuning: launch shapes of the fused evaluation's two passes."""
+    _fields_ = [("elem_persistent", _i32), ("elem_prefetch", _i32), ("row_lanes", _i32),
+                ("reserved", _i32), ("elem_us", _d), ("row_us", _d)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 MONITOR_BYTES = ctypes.sizeof(Monitors)
 
 # name -> (restype, argtypes); every entry returns int status
@@ -86,6 +95,9 @@ SIGNATURES = {
     "up3d_residual_vjp": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_transpose": (_int, [_p, _p, _p, _p]),
     "up3d_residual_jacobian_batched": (_int, [_p, _p, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_mesh_set_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
+    "up3d_mesh_get_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
+    "up3d_autotune": (_int, [_p, _p, ctypes.POINTER(Flow), _int, ctypes.POINTER(Tuning), _p]),
     "up3d_launch_count": (_int, [ctypes.POINTER(_i64)]),
     "up3d_profile": (_int, [_int]),
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),

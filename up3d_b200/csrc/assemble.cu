@@ -19,6 +19,9 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <vector>
+
 #include "elem.cuh"
 #include "internal.cuh"
 
@@ -125,17 +128,47 @@ __device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, 
 
 // ------------------------------------------------------------ row gather
 
+// Sums over a row's incident entries k < deg in a fixed order that does
+// not depend on the lanes per row: entry k goes to slot k mod 4, each slot
+// sums its entries in ascending k, and the row sum is (s0 + s2) + (s1 + s3).
+// LPR lanes per row (LPR >= 4; lane `sub` of the row's group loads entry
+// k0 + sub of each chunk of LPR entries through load(k) -> (x, y)); the
+// sums of x and y land in lane sub == 0.  Every lane of the warp must call
+// it (warp-uniform trip count over the warp's longest row).
+template <int LPR, class Load>
+__device__ __forceinline__ void slot_sum(int deg, int sub, Load&& load, double& sx, double& sy) {
+    static_assert(LPR >= 4 && LPR <= 32 && (LPR & (LPR - 1)) == 0, "LPR: power of two in [4, 32]");
+    const int maxdeg = __reduce_max_sync(0xffffffffu, deg);
+    double x = 0.0, y = 0.0;  // slot sub & 3 in lanes sub < 4
+    for (int k0 = 0; k0 < maxdeg; k0 += LPR) {
+        double2 v = make_double2(0.0, 0.0);
+        if (k0 + sub < deg) v = load(k0 + sub);
+#pragma unroll
+        for (int j = 0; j < LPR / 4; ++j) {
+            const double vx = j == 0 ? v.x : __shfl_down_sync(0xffffffffu, v.x, 4 * j, LPR);
+            const double vy = j == 0 ? v.y : __shfl_down_sync(0xffffffffu, v.y, 4 * j, LPR);
+            if (k0 + (sub & 3) + 4 * j < deg) {
+                x += vx;
+                y += vy;
+            }
+        }
+    }
+    x += __shfl_down_sync(0xffffffffu, x, 2, LPR);
+    y += __shfl_down_sync(0xffffffffu, y, 2, LPR);
+    x += __shfl_down_sync(0xffffffffu, x, 1, LPR);
+    y += __shfl_down_sync(0xffffffffu, y, 1, LPR);
+    sx = x;
+    sy = y;
+}
+
 // Jacobian rows (and, when R != null, the residual) from the local
 // matrices, LPR lanes per row (32 / LPR rows per warp in flight):
-//   R_n  = sum_e R_e,i        J_nn = sum_e J_e,ii      (lanes stride the
-//   incident entries, then a butterfly over the row's lanes)
+//   R_n  = sum_e R_e,i        J_nn = sum_e J_e,ii      (in the order of
+//   slot_sum: the same bits for every LPR and for the residual-only gather)
 //   J_nm = sum_e J_e,ij  for the upper slots m > n (lanes stride the slots;
 //   each slot sums its plan's contributors in ascending element order) and
 //   is written to (n, m) and, the element matrices being symmetric and row m
 //   listing the same elements in the same order, to its transposed slot.
-#ifndef UP3D_ROW_LPR
-#define UP3D_ROW_LPR 8
-#endif
 template <int WARPS, int LPR>
 __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
@@ -160,13 +193,11 @@ __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
             L = indptr[n + 1] - rb;
             ds = diag[n];
         }
-        double r = 0.0, d = 0.0;
-        for (int k = sub; k < deg; k += LPR) {
+        double r, d;
+        slot_sum<LPR>(deg, sub, [&](int k) {
             const uint32_t x = ent[eb + k];
-            const double2 v = reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
-            r += v.x;
-            d += v.y;
-        }
+            return reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
+        }, r, d);
         for (int s = ds + 1 + sub; s < L; s += LPR) {
             int32_t p = plan_off[rb + s];
             const int32_t p1 = plan_off[rb + s + 1];
@@ -189,12 +220,6 @@ __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
             J[rb + s] = v;
             J[zt[rb + s]] = v;
         }
-#pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-        if (R) {
-#pragma unroll
-            for (int o = LPR / 2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-        }
         if (valid && sub == 0) {
             if (deg > 0) J[rb + ds] = d;  // a node of no element has an empty row
             if (R) R[n] = r;
@@ -202,22 +227,28 @@ __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     }
 }
 
-// Residual rows only: R_n = sum_e R_e,i from the compact residual array.
+// Residual rows only: R_n = sum_e R_e,i from the compact residual array,
+// 8 lanes per row, in the row gather's order (slot_sum).
 __global__ void __launch_bounds__(256)
     k_row_residual(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
                    const double* __restrict__ res, double* __restrict__ R) {
-    const int lane = threadIdx.x & 31;
+    constexpr int LPR = 8, RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t n = warp; n < N; n += n_warps) {
-        const int32_t eb = ent_off[n], deg = ent_off[n + 1] - eb;
-        double r = 0.0;
-        for (int k = lane; k < deg; k += 32) {
-            const uint32_t x = ent[eb + k];
-            r += res[4 * (size_t)(x >> 2) + (x & 3)];
+    for (int64_t base = warp * RPW; base < N; base += n_warps * RPW) {
+        const int64_t n = base + lane / LPR;
+        int32_t eb = 0, deg = 0;
+        if (n < N) {
+            eb = ent_off[n];
+            deg = ent_off[n + 1] - eb;
         }
-        r = warp_sum(r);
-        if (lane == 0) R[n] = r;
+        double r, unused;
+        slot_sum<LPR>(deg, sub, [&](int k) {
+            const uint32_t x = ent[eb + k];
+            return make_double2(res[4 * (size_t)(x >> 2) + (x & 3)], 0.0);
+        }, r, unused);
+        if (n < N && sub == 0) R[n] = r;
     }
 }
 
@@ -314,6 +345,29 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
     }
 }
 
+// Bulk prefetch into L2 of the per-element inputs of elements [t, t + n)
+// (cp.async.bulk.prefetch: 16-byte aligned start and size -- every array
+// here is a cudaMalloc base and t a multiple of the 256-thread block, so
+// each start is aligned; sizes are rounded down to 16 bytes).  Lane k of
+// warp 0 issues array k; the prefetch is a hint and never faults within
+// the arrays' bounds, which n keeps it to.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    if (bytes >= 16) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes & ~15u) : "memory");
+}
+__device__ __forceinline__ void prefetch_tile(int lane, int64_t t, int tile, int64_t E, const int4* conn,
+                                              const double* B, const double* V, const int4* fn,
+                                              const double* disp) {
+    if (t >= E || lane >= 5) return;
+    const uint32_t n = (uint32_t)(E - t < tile ? E - t : tile);
+    switch (lane) {
+        case 0: prefetch_l2(conn + t, 16u * n); break;
+        case 1: prefetch_l2(B + 12 * t, 96u * n); break;
+        case 2: prefetch_l2(V + t, 8u * n); break;
+        case 3: prefetch_l2(fn + t, 16u * n); break;
+        default: prefetch_l2(disp + 12 * t, 96u * n); break;
+    }
+}
+
 // eval_residual + assemble_coupled, per element (pyfp3d/solve/newton.py:
 // 345-372, :435-452): gradient, limiter, density, upstream walk (or the
 // frozen selection), the upstream element's state recomputed in place, the
@@ -329,9 +383,15 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
                  double* __restrict__ rt_out, up3d_monitors* mon, const Flow* __restrict__ flows,
-                 const int32_t* __restrict__ case_of, int8_t* __restrict__ br_out) {
+                 const int32_t* __restrict__ case_of, int8_t* __restrict__ br_out, int pf) {
     MonAcc acc;
-    GRID_STRIDE(e, E) {
+    // tiles of blockDim elements, block-strided over the grid; with pf > 0
+    // warp 0 first prefetches the tile pf iterations ahead into L2
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < E; base += stride) {
+        if (pf > 0 && threadIdx.x < 32) prefetch_tile(threadIdx.x, base + pf * stride, blockDim.x, E, conn, B, V, fn, disp);
+        const int64_t e = base + threadIdx.x;
+        if (e >= E) continue;
         const Flow& F = BATCH ? flows[case_of[e]] : F0;
         // only grad phi_e stays live through the walk; the element's own
         // state and gB_j = grad . B_j are formed after it (B_e again: an
@@ -640,19 +700,28 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 
 // ------------------------------------------------------------ launchers
 
-// Jacobian (+ residual) rows from m->loc.
-void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
-    constexpr int rows_per_block = RG_WARPS * 32 / UP3D_ROW_LPR;
-    const unsigned grid = grid_for(m->N, rows_per_block, (int64_t)148 * 64);
-    k_row_gather<RG_WARPS, UP3D_ROW_LPR><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(),
-                                                          m->plan_off.get(), m->plan.get(), m->diag.get(),
-                                                          m->zt.get(), m->loc.get(), R, J);
+// Jacobian (+ residual) rows from m->loc, m->tune.row_lanes lanes per row.
+template <int LPR>
+static void launch_row_gather_lpr(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
+    constexpr int rows_per_block = RG_WARPS * 32 / LPR;
+    const unsigned grid = grid_for(m->N, rows_per_block, (int64_t)m->n_sms * 64);
+    k_row_gather<RG_WARPS, LPR><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(),
+                                                                m->indptr.get(), m->plan_off.get(), m->plan.get(),
+                                                                m->diag.get(), m->zt.get(), m->loc.get(), R, J);
     UP3D_CHECK_LAUNCH();
+}
+void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
+    switch (m->tune.row_lanes) {
+        case 4: launch_row_gather_lpr<4>(m, R, J, s); break;
+        case 16: launch_row_gather_lpr<16>(m, R, J, s); break;
+        case 32: launch_row_gather_lpr<32>(m, R, J, s); break;
+        default: launch_row_gather_lpr<8>(m, R, J, s); break;
+    }
 }
 
 // Residual rows from m->res.
 void launch_row_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
-    k_row_residual<<<grid_for(32 * m->N, 256, (int64_t)148 * 64), 256, 0, s>>>(m->N, m->ent_off.get(),
+    k_row_residual<<<grid_for(8 * m->N, 256, (int64_t)m->n_sms * 64), 256, 0, s>>>(m->N, m->ent_off.get(),
                                                                              m->ent.get(), m->res.get(), R);
     UP3D_CHECK_LAUNCH();
 }
@@ -835,6 +904,32 @@ __global__ void k_check_cases(const int32_t* __restrict__ case_of, int64_t E, in
 
 }  // namespace
 
+// One launch of the fused element sweep in the mesh's tuned shape: one
+// thread per element (grid capped at 64 blocks per SM), or one resident
+// wave (SMs x the kernel's occupancy) looping over tiles with the L2
+// prefetch distance m->tune.elem_prefetch.
+template <bool FR, bool JA, bool BA, class... A>
+static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
+    constexpr int block = 256;
+    auto kern = k_fused_elem<FR, JA, BA>;
+    unsigned grid;
+    int pf = 0;
+    if (m->tune.elem_persistent) {
+        static int occ = 0;  // same for every device of the process (one architecture)
+        if (occ == 0) {
+            int nb = 0;
+            UP3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, block, 0));
+            occ = nb > 0 ? nb : 1;
+        }
+        grid = grid_for(m->E, block, (int64_t)m->n_sms * occ);
+        pf = m->tune.elem_prefetch;
+    } else {
+        grid = grid_for(m->E, block, (int64_t)m->n_sms * 64);
+    }
+    kern<<<grid, block, 0, s>>>(args..., pf);
+    UP3D_CHECK_LAUNCH();
+}
+
 // The fused evaluation: element sweep, row gather, Term 3.  flows_d /
 // case_of select per-element flows (several cases in one mesh) when set.
 static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
@@ -843,7 +938,6 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
                            int8_t* br_out = nullptr) {
     up3d_monitors* mo = mon ? mon : m->mon_ws.get();
     UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
-    const unsigned grid = grid_for(m->E, 256, (int64_t)148 * 64);
 #define FUSED_ARGS                                                                                                \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
         m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of, \
@@ -852,23 +946,22 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     prof_begin(PROF_ELEM, s);
     if (flows_d) {
         if (up_fz) {
-            if (jac) k_fused_elem<true, true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
-            else k_fused_elem<true, false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            if (jac) launch_sweep<true, true, true>(m, s, FUSED_ARGS);
+            else launch_sweep<true, false, true>(m, s, FUSED_ARGS);
         } else {
-            if (jac) k_fused_elem<false, true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
-            else k_fused_elem<false, false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            if (jac) launch_sweep<false, true, true>(m, s, FUSED_ARGS);
+            else launch_sweep<false, false, true>(m, s, FUSED_ARGS);
         }
     } else {
         if (up_fz) {
-            if (jac) k_fused_elem<true, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
-            else k_fused_elem<true, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            if (jac) launch_sweep<true, true, false>(m, s, FUSED_ARGS);
+            else launch_sweep<true, false, false>(m, s, FUSED_ARGS);
         } else {
-            if (jac) k_fused_elem<false, true><<<grid, 256, 0, s>>>(FUSED_ARGS);
-            else k_fused_elem<false, false><<<grid, 256, 0, s>>>(FUSED_ARGS);
+            if (jac) launch_sweep<false, true, false>(m, s, FUSED_ARGS);
+            else launch_sweep<false, false, false>(m, s, FUSED_ARGS);
         }
     }
 #undef FUSED_ARGS
-    UP3D_CHECK_LAUNCH();
     prof_end(PROF_ELEM, s, 1);
     if (up_out)
         UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
@@ -908,6 +1001,113 @@ int up3d_residual_jacobian(up3d_mesh* m, const double* phi, const up3d_flow* flo
         const Flow F = make_flow(*flow);
         fused_evaluate(m, phi, F, flow->u_inf * flow->u_inf, nullptr, nullptr, up_fz, br_fz, R, data, rt_out,
                        up_out, mon, S(stream));
+    });
+}
+
+int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && t, UP3D_ERR_ARGUMENT, "up3d_mesh_set_tuning: null argument");
+        UP3D_REQUIRE(t->elem_persistent == 0 || t->elem_persistent == 1, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: elem_persistent must be 0 or 1");
+        UP3D_REQUIRE(t->elem_prefetch >= 0 && t->elem_prefetch <= 8, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: elem_prefetch must be in [0, 8]");
+        UP3D_REQUIRE(t->row_lanes == 4 || t->row_lanes == 8 || t->row_lanes == 16 || t->row_lanes == 32,
+                     UP3D_ERR_VALUE, "up3d_mesh_set_tuning: row_lanes must be 4, 8, 16 or 32");
+        m->tune = *t;
+        m->tune.reserved = 0;
+    });
+}
+
+int up3d_mesh_get_tuning(const up3d_mesh* m, up3d_tuning* t) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && t, UP3D_ERR_ARGUMENT, "up3d_mesh_get_tuning: null argument");
+        *t = m->tune;
+    });
+}
+
+int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int reps, up3d_tuning* out,
+                  up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && phi && flow, UP3D_ERR_ARGUMENT, "up3d_autotune: null argument");
+        UP3D_REQUIRE(reps >= 1 && reps <= 1000, UP3D_ERR_VALUE, "up3d_autotune: reps must be in [1, 1000]");
+        cudaStream_t s = S(stream);
+        const Flow F = make_flow(*flow);
+        const double u2 = flow->u_inf * flow->u_inf;
+        DBuf<double> R, J;
+        R.alloc(m->N);
+        J.alloc(m->nnz);
+        struct Events {
+            cudaEvent_t a = nullptr, b = nullptr;
+            ~Events() {
+                if (a) cudaEventDestroy(a);
+                if (b) cudaEventDestroy(b);
+            }
+        } ev;
+        UP3D_CUDA(cudaEventCreate(&ev.a));
+        UP3D_CUDA(cudaEventCreate(&ev.b));
+        // median device time (us) of `reps` launches after one warm-up
+        auto time_it = [&](auto&& launch) {
+            launch();
+            std::vector<float> t(reps);
+            for (int r = 0; r < reps; ++r) {
+                UP3D_CUDA(cudaEventRecord(ev.a, s));
+                launch();
+                UP3D_CUDA(cudaEventRecord(ev.b, s));
+                UP3D_CUDA(cudaEventSynchronize(ev.b));
+                UP3D_CUDA(cudaEventElapsedTime(&t[r], ev.a, ev.b));
+            }
+            std::sort(t.begin(), t.end());
+            return 1e3 * (double)t[reps / 2];
+        };
+        const up3d_tuning saved = m->tune;
+        try {
+            const int64_t* no_up = nullptr;
+            const int8_t* no_br = nullptr;
+            double* no_rt = nullptr;
+            const Flow* no_flows = nullptr;
+            const int32_t* no_case = nullptr;
+            int8_t* no_brout = nullptr;
+            up3d_monitors* mo = m->mon_ws.get();
+            // the element sweep: Newton Jacobian, live upwind selection
+            static const int shapes[][2] = {{0, 0}, {1, 0}, {1, 1}, {1, 2}, {1, 4}};
+            double best_e = 0.0;
+            int best_k = -1;
+            for (int k = 0; k < (int)(sizeof(shapes) / sizeof(shapes[0])); ++k) {
+                m->tune.elem_persistent = shapes[k][0];
+                m->tune.elem_prefetch = shapes[k][1];
+                const double t = time_it([&] {
+                    launch_sweep<false, true, false>(m, s, m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(),
+                                                     m->disp.get(), m->nodes4.get(), phi, F, u2, no_up, no_br, m->E,
+                                                     m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(),
+                                                     m->up32.get(), no_rt, mo, no_flows, no_case, no_brout);
+                });
+                if (best_k < 0 || t < best_e) {
+                    best_e = t;
+                    best_k = k;
+                }
+            }
+            m->tune.elem_persistent = shapes[best_k][0];
+            m->tune.elem_prefetch = shapes[best_k][1];
+            // the row gather, on the local matrices the sweep left
+            static const int lanes[] = {4, 8, 16, 32};
+            double best_r = 0.0;
+            int best_l = -1;
+            for (int l : lanes) {
+                m->tune.row_lanes = l;
+                const double t = time_it([&] { launch_row_gather(m, R.get(), J.get(), s); });
+                if (best_l < 0 || t < best_r) {
+                    best_r = t;
+                    best_l = l;
+                }
+            }
+            m->tune.row_lanes = best_l;
+            m->tune.elem_us = best_e;
+            m->tune.row_us = best_r;
+        } catch (...) {
+            m->tune = saved;
+            throw;
+        }
+        if (out) *out = m->tune;
     });
 }
 

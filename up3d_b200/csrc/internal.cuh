@@ -111,6 +111,8 @@ struct up3d_mesh {
     int64_t N = 0, E = 0, nnz = 0;
     int32_t max_row_len = 0, max_deg = 0;
     int32_t n_colors = -1;
+    int32_t n_sms = 148;                       // multiprocessors of the mesh's device
+    up3d_tuning tune = {0, 0, 8, 0, 0.0, 0.0};  // launch shapes of the fused passes
 
     // geometry (device)
     up3d::DBuf<double4> nodes4;  // (N) x, y, z, 0

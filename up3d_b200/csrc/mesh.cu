@@ -499,6 +499,7 @@ int up3d_mesh_create(const double* nodes, const int32_t* elements, int64_t n_nod
         m->N = n_nodes;
         m->E = n_tets;
         try {
+            UP3D_CUDA(cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, device));
             build_mesh(m, nodes, elements, S(stream));
             ensure_workspaces(m);
             auto* x = extra_of(m, true);

@@ -124,6 +124,27 @@ class DeviceMesh:
             self._colors = (off, el, int(nc.value))
         return self._colors
 
+    # ---------------------------------------------------------- launch shapes
+
+    def tuning(self) -> dict:
+        """The launch shapes of the fused evaluation (up3d_tuning)."""
+        t = L.Tuning()
+        L.call("up3d_mesh_get_tuning", self.handle, ctypes.byref(t))
+        return t.as_dict()
+
+    def set_tuning(self, elem_persistent: int = 0, elem_prefetch: int = 0, row_lanes: int = 8) -> None:
+        """Installs launch shapes by hand; every shape computes the same bits."""
+        t = L.Tuning(elem_persistent, elem_prefetch, row_lanes, 0, 0.0, 0.0)
+        L.call("up3d_mesh_set_tuning", self.handle, ctypes.byref(t))
+
+    def autotune(self, phi, flow, reps: int = 5) -> dict:
+        """Times every candidate shape of the element sweep and the row
+        gather on this mesh at (phi, flow) and installs the fastest."""
+        t = L.Tuning()
+        L.call("up3d_autotune", self.handle, phi.data_ptr(), flow.c(), int(reps), ctypes.byref(t),
+               L.stream_ptr())
+        return t.as_dict()
+
     def elem_to_csr(self):
         t = L.torch()
         out = t.empty((self.n_tets, 4, 4), dtype=t.int64, device="cuda")
