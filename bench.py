@@ -51,9 +51,11 @@ def parse():
     p.add_argument("--cpu-states", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pocket-steps", type=int, default=300)
+    p.add_argument("--order", default="given", choices=["given", "morton", "hilbert"],
+                   help="node/element numbering of the device mesh")
     p.add_argument("--tune", default="auto",
                    help="launch shapes: 'auto' (autotuner), 'default', or "
-                        "'persistent,prefetch,row_lanes'")
+                        "'persistent,blocks_per_sm,row_lanes'")
     p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
                    help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
     p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
@@ -323,12 +325,17 @@ def batched_timing(spec, seed=0):
     machs = rng.uniform(float(mlo_s), float(mhi_s), size=K)
     amps = rng.uniform(0.02, 0.08, size=K)
     meshes = [bump_channel(*sh, amplitude=float(a), seed=c) for c, (sh, a) in enumerate(zip(shapes, amps))]
-    batch = BatchedChannels(meshes)
+    # the ordering and launch shapes picked by the tuner (timed candidates)
+    t_tune = time.perf_counter()
+    batch = BatchedChannels.tuned(meshes, machs)
+    t_tune = time.perf_counter() - t_tune
+    shapes_tuned = batch.ws.ev.mesh.tuning()
     E = batch.n_tets
     # assembly throughput: seeded states
-    phi = torch.from_numpy(np.concatenate([seeded_state(m, c) for c, m in enumerate(meshes)])).cuda()
+    states = [seeded_state(m, c) for c, m in enumerate(meshes)]
+    phi = batch.union_phi(states)
     wss = [ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes) for m in meshes]
-    phis = [phi[batch.node_off[c]:batch.node_off[c + 1]].contiguous() for c in range(K)]
+    phis = [torch.from_numpy(p).cuda() for p in states]
     flows = [FlowParams(m_inf=float(M)) for M in machs]
 
     def t_events(fn, reps):
@@ -352,14 +359,22 @@ def batched_timing(spec, seed=0):
     out = {"cases": K, "shapes": ["x".join(map(str, sh)) for sh in shapes],
            "machs": [round(float(m), 4) for m in machs], "amplitudes": [round(float(a), 4) for a in amps],
            "total_tets": int(E),
+           "tuning": {"ordering": batch.ordering, "tuner_s": round(t_tune, 3),
+                      "candidates_ms": {k: round(v["ms"], 4) for k, v in batch.tuning_report["candidates"].items()},
+                      "shapes": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in shapes_tuned.items()}},
            "assembly": {"batched_ms": round(ms_b, 4), "sequential_ms": round(ms_s, 4),
                         "batched_melem_s": round(E / ms_b / 1e3, 1),
                         "sequential_melem_s": round(E / ms_s / 1e3, 1)}}
     # time to 1e-10: batched lockstep vs sequential plain solves (second run timed)
+    def fresh():
+        b = BatchedChannels(meshes, ordering=batch.ordering)
+        b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_blocks_per_sm"],
+                                shapes_tuned["row_lanes"])
+        return b
     res_b = None
     for _ in range(2):
-        batch2 = BatchedChannels(meshes)
-        res_b = solve_newton_batched(batch2, machs)
+        res_b = solve_newton_batched(fresh(), machs)
+    res_ng = solve_newton_batched(fresh(), machs, use_graphs=False)
     seq_s, seq_ok = [], []
     for c, m in enumerate(meshes):
         ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
@@ -370,6 +385,7 @@ def batched_timing(spec, seed=0):
         seq_s.append(time.perf_counter() - t0)
         seq_ok.append(bool(r["converged"]))
     out["newton"] = {"batched_s": round(res_b["time_s"], 4), "sequential_s": round(float(sum(seq_s)), 4),
+                     "batched_without_graphs_s": round(res_ng["time_s"], 4),
                      "speedup": round(float(sum(seq_s)) / res_b["time_s"], 3),
                      "batched_converged": [bool(v) for v in res_b["converged"]],
                      "sequential_converged": seq_ok,
@@ -398,11 +414,14 @@ def run_ours(args):
 
     shape = tuple(int(v) for v in args.mesh.split("x"))
     mesh, phis = workload(shape)
-    dmesh = DeviceMesh(mesh.nodes, mesh.elements)
+    from up3d_b200.mesh.order import renumber
+    order = renumber(mesh.nodes, mesh.elements, args.order)
+    dmesh = DeviceMesh(order.nodes, order.elements)
+    phis_dev = [order.nodal(p) for p in phis]
     info = {"n_tets": dmesh.n_tets, "n_nodes": dmesh.n_nodes, "nnz": dmesh.nnz}
     ev = ResidualJacobian(dmesh)
     flow = FlowParams(m_inf=M_INF)
-    d_phis = [torch.from_numpy(p).cuda() for p in phis]
+    d_phis = [torch.from_numpy(p).cuda() for p in phis_dev]
     stream = torch.cuda.current_stream()
 
     if args.tune == "auto":
@@ -454,7 +473,7 @@ def run_ours(args):
         # double-buffered pipeline overlaps one step's copies with the
         # neighbouring step's evaluation
         from up3d_b200.solve.fused import HostPipeline
-        h_phis = [torch.from_numpy(p).pin_memory() for p in phis]
+        h_phis = [torch.from_numpy(p).pin_memory() for p in phis_dev]
         h_R = torch.empty(dmesh.n_nodes, dtype=torch.float64).pin_memory()
         h_J = torch.empty(dmesh.nnz, dtype=torch.float64).pin_memory()
         pipe = HostPipeline(ev)
@@ -481,7 +500,7 @@ def run_ours(args):
     if args.pocket_steps > 0:
         from up3d_b200.mesh.kuhn import pocket_state
         fams = ("accelerating", "shockpoint", "mixed")
-        p_phis = [torch.from_numpy(pocket_state(mesh, f)).cuda() for f in fams]
+        p_phis = [torch.from_numpy(order.nodal(pocket_state(mesh, f))).cuda() for f in fams]
         for k in range(3):
             ev.evaluate(p_phis[k], flow, jacobian=True, keep_state=False)
         p_mon = [None] * 3
@@ -557,6 +576,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": 8 * dmesh.n_nodes + 8 * dmesh.nnz},
             "gpu_launches": int(launches),
             "tuning": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in tuning.items()},
+            "mesh_order": args.order,
             "clocks": clocks.summary(),
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
             "pocket_states": pocket,

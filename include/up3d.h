@@ -263,7 +263,12 @@ int up3d_jacobian_transpose(up3d_mesh* mesh, const double* data, double* data_t,
  * stays live (cases freeze one by one).  branch_out (device int8, may be
  * NULL) receives each element's branch: the frozen one, or the one a live
  * element took (classify_upwind_branches, kernels/upwind.py:504-541).
- * UP3D_ERR_VALUE for a case index outside [0, n_cases). */
+ * UP3D_ERR_VALUE for a case index outside [0, n_cases).
+ * flows == NULL reuses the flow table of the last call with flows on this
+ * mesh (same n_cases, else UP3D_ERR_VALUE) without validating case_of
+ * again: no host synchronisation, so a residual-only call (data == NULL)
+ * can be captured in a CUDA graph.  An index outside [0, n_cases) then
+ * reads case 0. */
 int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cases,
                                    const up3d_flow* flows, const int32_t* case_of,
                                    const int64_t* upstream_frozen, const int8_t* branch_frozen,
@@ -276,27 +281,27 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
 /* Launch shapes of the fused evaluation's two passes (no reference
  * counterpart: numba picks its own).  Every shape computes the same bits:
  * the element sweep's per-element arithmetic does not depend on the grid,
- * and the row gather sums every row in a fixed 32-slot order whatever its
- * lanes per row.
+ * and the row gather sums every row in a fixed order whatever its lanes
+ * per row.
  *   elem_persistent  0: one thread per element (grid capped at 64 blocks
  *                    per SM); 1: one resident wave of blocks looping over
  *                    256-element tiles
- *   elem_prefetch    persistent sweep: the tile this many iterations ahead
- *                    is prefetched into L2 (bulk prefetch) before each
- *                    tile; 0 = none (ignored when not persistent)
+ *   elem_blocks_per_sm  register budget of the Newton-Jacobian sweep:
+ *                    2 (up to 128 registers per thread, no spills) or 3
+ *                    (up to 80, spilling to L1) resident 256-thread blocks
  *   row_lanes        lanes per row of the row gather: 4, 8, 16 or 32
  *   elem_us, row_us  autotune output: median time per launch of the
  *                    chosen shapes (0 when set by hand) */
 typedef struct {
     int32_t elem_persistent;
-    int32_t elem_prefetch;
+    int32_t elem_blocks_per_sm;
     int32_t row_lanes;
-    int32_t reserved;
+    int32_t reserved; /* 0 */
     double elem_us;
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 0, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
+/* Default: {0, 2, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 

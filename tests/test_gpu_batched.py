@@ -67,3 +67,63 @@ def test_batched_newton_matches_plain_solves():
         ref = r["phi"].cpu().numpy()
         a, b = batch.node_off[c], batch.node_off[c + 1]
         assert np.abs(phi[a:b] - ref).max() < 1e-8
+
+
+def test_graph_replayed_trial_merits_match_direct_evaluation():
+    import torch
+    from up3d_b200.mesh.kuhn import pocket_state
+    from up3d_b200.solve.batched import BatchedChannels
+    meshes = _cases()
+    machs = [0.8, 0.6, 0.85]
+    batch = BatchedChannels(meshes)
+    mask_b = batch.ws.mask.bool()
+    phi = torch.from_numpy(np.concatenate([pocket_state(m, f) for m, f in
+                                           zip(meshes, ["mixed", "accelerating", "shockpoint"])])).cuda()
+    dphi = torch.from_numpy(np.random.default_rng(5).standard_normal(len(phi)) * 1e-3).cuda()
+    dphi = dphi.masked_fill(mask_b, 0.0)
+    batch.evaluate(phi, machs, jacobian=True)   # uploads the flows, as the Newton loop does
+    for lam in ([1.0, 0.5, 0.25], [0.0, 1.0, 0.125], [0.5, 0.5, 0.5]):
+        m_graph = batch.trial_merits(phi, dphi, np.array(lam), mask_b)
+        lam_node = torch.tensor(lam, dtype=torch.float64, device="cuda")[batch.case_of_node]
+        R = batch.evaluate(phi + lam_node * dphi, machs, jacobian=False)
+        m_direct = batch.per_case(R.masked_fill(mask_b, 0.0), "sumsq").cpu().numpy()
+        assert np.allclose(m_graph, m_direct, rtol=1e-12, atol=0)
+    # machs=None without a table of this many cases on the mesh is refused
+    other = BatchedChannels(meshes[:2])
+    with pytest.raises(ValueError, match="flow table"):
+        other.evaluate(other.ws.freestream.clone(), None)
+
+
+@pytest.mark.parametrize("ordering", ["morton", "hilbert"])
+def test_renumbered_batch_matches_per_case_evaluations(ordering):
+    import torch
+    from up3d_b200.mesh.kuhn import pocket_state
+    from up3d_b200.solve.batched import BatchedChannels
+    from up3d_b200.solve.fused import FlowParams
+    from up3d_b200.solve.newton import ChannelWorkspace
+    meshes = _cases()
+    machs = [0.8, 0.6, 0.85]
+    phis = [pocket_state(m, f) for m, f in zip(meshes, ["mixed", "accelerating", "shockpoint"])]
+    batch = BatchedChannels(meshes, ordering=ordering)
+    phi = batch.union_phi(phis)
+    R = batch.evaluate(phi, machs, jacobian=True).clone()
+    for c, (m, p, M) in enumerate(zip(meshes, phis, machs)):
+        assert torch.equal(batch.case_phi(phi, c).cpu(), torch.from_numpy(p))
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        Rc = ws.ev.evaluate(torch.from_numpy(p).cuda(), FlowParams(m_inf=M), jacobian=True)
+        Rb = batch.case_phi(R, c)
+        scale = Rc.abs().max()
+        assert float((Rb - Rc).abs().max() / scale) < 1e-12
+
+
+def test_tuned_batch_picks_an_ordering_and_converges():
+    from up3d_b200.solve.batched import BatchedChannels, solve_newton_batched
+    meshes = _cases()[:2]
+    machs = [0.6, 0.5]
+    batch = BatchedChannels.tuned(meshes, machs, reps=3)
+    rep = batch.tuning_report
+    assert rep["ordering"] == batch.ordering
+    assert set(rep["candidates"]) == {"given", "morton", "hilbert"}
+    assert all(v["ms"] > 0 for v in rep["candidates"].values())
+    res = solve_newton_batched(batch, machs)
+    assert res["converged"].all()

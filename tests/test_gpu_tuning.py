@@ -10,7 +10,8 @@ from conftest import has_cuda, rel_err
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
 
-SHAPES = [(0, 0, 4), (0, 0, 8), (1, 0, 8), (1, 1, 16), (1, 2, 32), (1, 4, 4), (0, 3, 16)]
+# (persistent, blocks per SM, lanes per row)
+SHAPES = [(0, 2, 4), (0, 3, 8), (1, 2, 8), (1, 3, 16), (1, 2, 32), (1, 3, 4), (0, 2, 16)]
 
 
 def _setup():
@@ -38,6 +39,7 @@ def test_every_shape_gives_the_same_bits():
     assert dm.n_tets % 256 != 0
     flow = FlowParams(m_inf=0.8)
     assert dm.tuning()["row_lanes"] == 8 and dm.tuning()["elem_persistent"] == 0
+    assert dm.tuning()["elem_blocks_per_sm"] == 2
     R0, J0, up0, rt0, mon0 = _outputs(ev, phi, flow)
     assert mon0["n_term3_active"] > 0
     frozen = (up0.to(torch.int64), torch.zeros(dm.n_tets, dtype=torch.int8, device="cuda"))
@@ -45,11 +47,11 @@ def test_every_shape_gives_the_same_bits():
     Rr0 = ev.evaluate(phi, flow, jacobian=False).clone()
     # the residual-only gather sums in the row gather's order
     assert torch.equal(Rr0, R0)
-    for p, pf, lanes in SHAPES:
-        dm.set_tuning(p, pf, lanes)
+    for shape in SHAPES:
+        dm.set_tuning(*shape)
         R, J, up, rt, mon = _outputs(ev, phi, flow)
-        assert torch.equal(R, R0), (p, pf, lanes)
-        assert (J != J0).nnz == 0 and J.nnz == J0.nnz, (p, pf, lanes)
+        assert torch.equal(R, R0), shape
+        assert (J != J0).nnz == 0 and J.nnz == J0.nnz, shape
         assert torch.equal(up, up0) and torch.equal(rt, rt0)
         assert mon == mon0
         assert torch.equal(ev.evaluate(phi, flow, jacobian=True, frozen=frozen), Rf0)
@@ -66,7 +68,7 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
     J0 = ev.jacobian().to_scipy()
     t = dm.autotune(phi, flow, reps=3)
     assert t == dm.tuning()
-    assert (t["elem_persistent"], t["elem_prefetch"]) in {(0, 0), (1, 0), (1, 1), (1, 2), (1, 4)}
+    assert (t["elem_persistent"], t["elem_blocks_per_sm"]) in {(0, 2), (1, 2), (0, 3), (1, 3)}
     assert t["row_lanes"] in (4, 8, 16, 32)
     assert t["elem_us"] > 0 and t["row_us"] > 0
     R = ev.evaluate(phi, flow, jacobian=True).clone()
@@ -79,7 +81,36 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
 
 def test_bad_shapes_are_refused():
     _, _, dm, _, _ = _setup()
-    for bad in [(2, 0, 8), (1, -1, 8), (1, 9, 8), (0, 0, 2), (0, 0, 12), (0, 0, 64)]:
+    for bad in [(2, 2, 8), (-1, 2, 8), (0, 1, 8), (0, 4, 8), (0, 2, 2), (0, 2, 12), (0, 2, 64)]:
         with pytest.raises(ValueError):
             dm.set_tuning(*bad)
     assert dm.tuning()["row_lanes"] == 8
+
+
+@pytest.mark.parametrize("ordering", ["morton", "hilbert"])
+def test_renumbered_mesh_matches_the_oracle(ordering):
+    """A renumbered mesh gives the oracle's results on the original
+    numbering, permuted: upstream elements exactly, R and J within the
+    parity tolerance (only the per-node summation order changes)."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.mesh.device import DeviceMesh
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    from up3d_b200.mesh.order import renumber
+    from up3d_b200.solve.fused import FlowParams, ResidualJacobian
+    mesh = bump_channel(16, 6, 5, amplitude=0.08, seed=4)
+    phi = pocket_state(mesh, "shockpoint")
+    r = renumber(mesh.nodes, mesh.elements, ordering)
+    dm = DeviceMesh(r.nodes, r.elements)
+    ev = ResidualJacobian(dm)
+    R = ev.evaluate(torch.from_numpy(r.nodal(phi)).cuda(), FlowParams(m_inf=0.8), jacobian=True)
+    R = r.nodal_back(R.cpu().numpy())
+    J = ev.jacobian().to_scipy()[r.node_inv][:, r.node_inv]
+    up = r.element_ids_back(r.elemental_back(ev.upstream.cpu().numpy()))
+    ref = O.chain(O.PicardOperator(mesh.nodes, mesh.elements),
+                  O.UpwindOperator(mesh.nodes, mesh.elements), phi, 0.8)
+    assert ref["n_term3_active"] > 0
+    assert np.array_equal(up, ref["upstream"])
+    assert rel_err(R, ref["R"]) < 1e-12
+    D = (J - ref["J"]).tocoo()
+    assert (np.abs(D.data).max() if D.nnz else 0.0) / np.abs(ref["J"].data).max() < 1e-12

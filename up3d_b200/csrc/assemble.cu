@@ -79,26 +79,6 @@ __device__ __forceinline__ void store_local(double* __restrict__ loc, int64_t e,
     p[6] = make_double2(jij(b, gB, w1, w2, 1, 3), jij(b, gB, w1, w2, 2, 3));
 }
 
-// store_local with B_e read from memory pair by pair (an L1/L2 hit: the
-// sweep read B_e at its start) instead of twelve values held in registers;
-// the same fma order, so identical bits.
-__device__ __forceinline__ double jij_mem(const double* __restrict__ b, const double gB[4], double w1, double w2,
-                                          int i, int j) {
-    double v = w1 * fma(b[3 * i + 2], b[3 * j + 2], fma(b[3 * i + 1], b[3 * j + 1], b[3 * i] * b[3 * j]));
-    if (w2 != 0.0) v = fma(w2 * gB[i], gB[j], v);
-    return v;
-}
-__device__ __forceinline__ void store_local_mem(double* __restrict__ loc, int64_t e, const double* __restrict__ B,
-                                                const double gB[4], double w1, double w2) {
-    const double* b = B + 12 * e;
-    double2* p = reinterpret_cast<double2*>(loc + (size_t)LOC_STRIDE * e);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) p[i] = make_double2(w1 * gB[i], jij_mem(b, gB, w1, w2, i, i));
-    p[4] = make_double2(jij_mem(b, gB, w1, w2, 0, 1), jij_mem(b, gB, w1, w2, 0, 2));
-    p[5] = make_double2(jij_mem(b, gB, w1, w2, 0, 3), jij_mem(b, gB, w1, w2, 1, 2));
-    p[6] = make_double2(jij_mem(b, gB, w1, w2, 1, 3), jij_mem(b, gB, w1, w2, 2, 3));
-}
-
 __device__ __forceinline__ void store_res(double* __restrict__ res, int64_t e, const double gB[4], double w1) {
     double2* p = reinterpret_cast<double2*>(res + 4 * e);
     p[0] = make_double2(w1 * gB[0], w1 * gB[1]);
@@ -116,15 +96,7 @@ __device__ __forceinline__ void store_t3(double* __restrict__ t3v, int64_t e, do
     p[3] = make_double2(f[2], f[3]);
 }
 
-__device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, double b[12]) {
-    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        double2 v = b2[k];
-        b[2 * k] = v.x;
-        b[2 * k + 1] = v.y;
-    }
-}
+__device__ __forceinline__ void load_B(const double* __restrict__ B, int64_t e, double b[12]) { ld_B(B + 12 * e, b); }
 
 // ------------------------------------------------------------ row gather
 
@@ -345,59 +317,43 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
     }
 }
 
-// Bulk prefetch into L2 of the per-element inputs of elements [t, t + n)
-// (cp.async.bulk.prefetch: 16-byte aligned start and size -- every array
-// here is a cudaMalloc base and t a multiple of the 256-thread block, so
-// each start is aligned; sizes are rounded down to 16 bytes).  Lane k of
-// warp 0 issues array k; the prefetch is a hint and never faults within
-// the arrays' bounds, which n keeps it to.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-    if (bytes >= 16) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes & ~15u) : "memory");
-}
-__device__ __forceinline__ void prefetch_tile(int lane, int64_t t, int tile, int64_t E, const int4* conn,
-                                              const double* B, const double* V, const int4* fn,
-                                              const double* disp) {
-    if (t >= E || lane >= 5) return;
-    const uint32_t n = (uint32_t)(E - t < tile ? E - t : tile);
-    switch (lane) {
-        case 0: prefetch_l2(conn + t, 16u * n); break;
-        case 1: prefetch_l2(B + 12 * t, 96u * n); break;
-        case 2: prefetch_l2(V + t, 8u * n); break;
-        case 3: prefetch_l2(fn + t, 16u * n); break;
-        default: prefetch_l2(disp + 12 * t, 96u * n); break;
-    }
-}
-
 // eval_residual + assemble_coupled, per element (pyfp3d/solve/newton.py:
 // 345-372, :435-452): gradient, limiter, density, upstream walk (or the
 // frozen selection), the upstream element's state recomputed in place, the
 // flux, its sensitivities, and the element's residual contributions and
 // local matrix (JAC) or residual contributions only.
 // BATCH: several cases in one mesh (disconnected components), element e
-// taking the flow of its case, flows[case_of[e]].
-template <bool FROZEN, bool JAC, bool BATCH = false>
-__global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB)
+// taking the flow of its case, flows[case_of[e]] (an index outside
+// [0, n_cases) reads case 0: the host validates the indices, and a table
+// reused without validation can never be read out of bounds).
+// MB: resident blocks per SM the register allocation must allow.
+template <bool FROZEN, bool JAC, bool BATCH, int MB>
+__global__ void __launch_bounds__(256, MB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
                  const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F0, double u2, const int64_t* __restrict__ up_fz,
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
                  double* __restrict__ rt_out, up3d_monitors* mon, const Flow* __restrict__ flows,
-                 const int32_t* __restrict__ case_of, int8_t* __restrict__ br_out, int pf) {
+                 const int32_t* __restrict__ case_of, int n_cases, int8_t* __restrict__ br_out) {
     MonAcc acc;
-    // tiles of blockDim elements, block-strided over the grid; with pf > 0
-    // warp 0 first prefetches the tile pf iterations ahead into L2
+    // tiles of blockDim elements, block-strided over the grid
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < E; base += stride) {
-        if (pf > 0 && threadIdx.x < 32) prefetch_tile(threadIdx.x, base + pf * stride, blockDim.x, E, conn, B, V, fn, disp);
         const int64_t e = base + threadIdx.x;
         if (e >= E) continue;
-        const Flow& F = BATCH ? flows[case_of[e]] : F0;
+        int ci = 0;
+        if (BATCH) {
+            ci = case_of[e];
+            ci = (unsigned)ci < (unsigned)n_cases ? ci : 0;
+        }
+        const Flow& F = BATCH ? flows[ci] : F0;
         // only grad phi_e stays live through the walk; the element's own
         // state and gB_j = grad . B_j are formed after it (B_e again: an
         // L1/L2 hit)
+        const double* be = B + 12 * e;
         double g[3];
-        elem_grad(conn, B, phi, e, g);
+        elem_grad_rec(conn[e], be, phi, g);
         // frozen (upstream, branch) per element; a negative branch keeps the
         // element live (several cases in one mesh, frozen one by one)
         const int brf = FROZEN ? (int)br_fz[e] : -1;
@@ -455,12 +411,11 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
 
         const double Ve = V[e];
         const double w1 = rt * Ve;
+        // second touch of B_e (an L1/L2 hit), held in registers from here
+        double b[12];
+        ld_B(be, b);
         double gB[4];
-        {
-            const double* be = B + 12 * e;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) gB[j] = g[0] * be[3 * j] + g[1] * be[3 * j + 1] + g[2] * be[3 * j + 2];
-        }
+        gB_of(g, b, gB);
         if (JAC) {
             s_e = s_e * (lim_e ? 1.0 : 0.0);
             s_u = s_u * (lim_u ? 1.0 : 0.0);
@@ -481,7 +436,7 @@ __global__ void __launch_bounds__(256, JAC ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB
                 acc.act += 1;
             }
             t3flag[e] = active ? 1 : 0;
-            store_local_mem(loc, e, B, gB, w1, w2);  // second touch of B_e: an L1/L2 hit
+            store_local(loc, e, b, gB, w1, w2, true);
         } else {
             store_res(res, e, gB, w1);
         }
@@ -905,15 +860,14 @@ __global__ void k_check_cases(const int32_t* __restrict__ case_of, int64_t E, in
 }  // namespace
 
 // One launch of the fused element sweep in the mesh's tuned shape: one
-// thread per element (grid capped at 64 blocks per SM), or one resident
-// wave (SMs x the kernel's occupancy) looping over tiles with the L2
-// prefetch distance m->tune.elem_prefetch.
-template <bool FR, bool JA, bool BA, class... A>
-static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
+// thread per element (grid capped at 64 blocks per SM) or one resident
+// wave (SMs x the kernel's occupancy) looping over 256-element tiles; the
+// Jacobian sweep compiled for 2 or 3 resident blocks per SM.
+template <bool FR, bool JA, bool BA, int MB, class... A>
+static void launch_sweep_mb(const up3d_mesh* m, cudaStream_t s, A... args) {
     constexpr int block = 256;
-    auto kern = k_fused_elem<FR, JA, BA>;
+    auto kern = k_fused_elem<FR, JA, BA, MB>;
     unsigned grid;
-    int pf = 0;
     if (m->tune.elem_persistent) {
         static int occ = 0;  // same for every device of the process (one architecture)
         if (occ == 0) {
@@ -922,12 +876,17 @@ static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
             occ = nb > 0 ? nb : 1;
         }
         grid = grid_for(m->E, block, (int64_t)m->n_sms * occ);
-        pf = m->tune.elem_prefetch;
     } else {
         grid = grid_for(m->E, block, (int64_t)m->n_sms * 64);
     }
-    kern<<<grid, block, 0, s>>>(args..., pf);
+    kern<<<grid, block, 0, s>>>(args...);
     UP3D_CHECK_LAUNCH();
+}
+
+template <bool FR, bool JA, bool BA, class... A>
+static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
+    if (JA && m->tune.elem_blocks_per_sm == 3) launch_sweep_mb<FR, JA, BA, 3>(m, s, args...);
+    else launch_sweep_mb<FR, JA, BA, JA ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB>(m, s, args...);
 }
 
 // The fused evaluation: element sweep, row gather, Term 3.  flows_d /
@@ -935,13 +894,13 @@ static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
 static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
                            const int32_t* case_of, const int64_t* up_fz, const int8_t* br_fz, double* R,
                            double* data, double* rt_out, int32_t* up_out, up3d_monitors* mon, cudaStream_t s,
-                           int8_t* br_out = nullptr) {
+                           int8_t* br_out = nullptr, int n_cases = 0) {
     up3d_monitors* mo = mon ? mon : m->mon_ws.get();
     UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
 #define FUSED_ARGS                                                                                                \
     m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
         m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of, \
-        br_out
+        n_cases, br_out
     const bool jac = data != nullptr;
     prof_begin(PROF_ELEM, s);
     if (flows_d) {
@@ -1009,10 +968,11 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
         UP3D_REQUIRE(m && t, UP3D_ERR_ARGUMENT, "up3d_mesh_set_tuning: null argument");
         UP3D_REQUIRE(t->elem_persistent == 0 || t->elem_persistent == 1, UP3D_ERR_VALUE,
                      "up3d_mesh_set_tuning: elem_persistent must be 0 or 1");
-        UP3D_REQUIRE(t->elem_prefetch >= 0 && t->elem_prefetch <= 8, UP3D_ERR_VALUE,
-                     "up3d_mesh_set_tuning: elem_prefetch must be in [0, 8]");
         UP3D_REQUIRE(t->row_lanes == 4 || t->row_lanes == 8 || t->row_lanes == 16 || t->row_lanes == 32,
                      UP3D_ERR_VALUE, "up3d_mesh_set_tuning: row_lanes must be 4, 8, 16 or 32");
+        UP3D_REQUIRE(t->elem_blocks_per_sm == 2 || t->elem_blocks_per_sm == 3, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: elem_blocks_per_sm must be 2 or 3");
+
         m->tune = *t;
         m->tune.reserved = 0;
     });
@@ -1069,17 +1029,18 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
             int8_t* no_brout = nullptr;
             up3d_monitors* mo = m->mon_ws.get();
             // the element sweep: Newton Jacobian, live upwind selection
-            static const int shapes[][2] = {{0, 0}, {1, 0}, {1, 1}, {1, 2}, {1, 4}};
+            // (persistent, blocks per SM)
+            static const int shapes[][2] = {{0, 2}, {1, 2}, {0, 3}, {1, 3}};
             double best_e = 0.0;
             int best_k = -1;
             for (int k = 0; k < (int)(sizeof(shapes) / sizeof(shapes[0])); ++k) {
                 m->tune.elem_persistent = shapes[k][0];
-                m->tune.elem_prefetch = shapes[k][1];
+                m->tune.elem_blocks_per_sm = shapes[k][1];
                 const double t = time_it([&] {
                     launch_sweep<false, true, false>(m, s, m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(),
                                                      m->disp.get(), m->nodes4.get(), phi, F, u2, no_up, no_br, m->E,
                                                      m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(),
-                                                     m->up32.get(), no_rt, mo, no_flows, no_case, no_brout);
+                                                     m->up32.get(), no_rt, mo, no_flows, no_case, 0, no_brout);
                 });
                 if (best_k < 0 || t < best_e) {
                     best_e = t;
@@ -1087,7 +1048,7 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
                 }
             }
             m->tune.elem_persistent = shapes[best_k][0];
-            m->tune.elem_prefetch = shapes[best_k][1];
+            m->tune.elem_blocks_per_sm = shapes[best_k][1];
             // the row gather, on the local matrices the sweep left
             static const int lanes[] = {4, 8, 16, 32};
             double best_r = 0.0;
@@ -1116,30 +1077,41 @@ int up3d_residual_jacobian_batched(up3d_mesh* m, const double* phi, int n_cases,
                                    double* data, double* rt_out, int32_t* up_out, int8_t* branch_out,
                                    up3d_monitors* mon, up3d_stream stream) {
     return guarded([&] {
-        UP3D_REQUIRE(m && phi && flows && case_of && R && n_cases > 0, UP3D_ERR_ARGUMENT,
+        UP3D_REQUIRE(m && phi && case_of && R && n_cases > 0, UP3D_ERR_ARGUMENT,
                      "up3d_residual_jacobian_batched: null argument");
         UP3D_REQUIRE((up_fz == nullptr) == (br_fz == nullptr), UP3D_ERR_ARGUMENT,
                      "up3d_residual_jacobian_batched: frozen upstream and branch go together");
         cudaStream_t s = S(stream);
-        std::vector<Flow> host(n_cases);
-        for (int c = 0; c < n_cases; ++c) {
-            UP3D_REQUIRE(flows[c].u_inf == flows[0].u_inf, UP3D_ERR_VALUE,
-                         "up3d_residual_jacobian_batched: the cases must share u_inf");
-            host[c] = make_flow(flows[c]);
+        if (flows) {
+            std::vector<Flow> host(n_cases);
+            for (int c = 0; c < n_cases; ++c) {
+                UP3D_REQUIRE(flows[c].u_inf == flows[0].u_inf, UP3D_ERR_VALUE,
+                             "up3d_residual_jacobian_batched: the cases must share u_inf");
+                host[c] = make_flow(flows[c]);
+            }
+            m->flows_ws.alloc(n_cases);
+            m->i64_ws.alloc(8);
+            int* bad = reinterpret_cast<int*>(m->i64_ws.get() + 7);
+            UP3D_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+            k_check_cases<<<grid_for(m->E, 256), 256, 0, s>>>(case_of, m->E, n_cases, bad);
+            UP3D_CHECK_LAUNCH();
+            int hbad = 0;
+            UP3D_CUDA(cudaMemcpyAsync(m->flows_ws.get(), host.data(), sizeof(Flow) * n_cases,
+                                      cudaMemcpyHostToDevice, s));
+            UP3D_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaStreamSynchronize(s));
+            m->batch_cases = 0;
+            UP3D_REQUIRE(!hbad, UP3D_ERR_VALUE, "up3d_residual_jacobian_batched: case index out of range");
+            m->batch_cases = n_cases;
+            m->batch_flow0 = flows[0];
+        } else {
+            UP3D_REQUIRE(m->batch_cases == n_cases, UP3D_ERR_VALUE,
+                         "up3d_residual_jacobian_batched: no flow table of this many cases on the mesh "
+                         "(pass the flows once)");
         }
-        m->flows_ws.alloc(n_cases);
-        m->i64_ws.alloc(8);
-        int* bad = reinterpret_cast<int*>(m->i64_ws.get() + 7);
-        UP3D_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
-        k_check_cases<<<grid_for(m->E, 256), 256, 0, s>>>(case_of, m->E, n_cases, bad);
-        UP3D_CHECK_LAUNCH();
-        int hbad = 0;
-        UP3D_CUDA(cudaMemcpyAsync(m->flows_ws.get(), host.data(), sizeof(Flow) * n_cases, cudaMemcpyHostToDevice, s));
-        UP3D_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
-        UP3D_CUDA(cudaStreamSynchronize(s));
-        UP3D_REQUIRE(!hbad, UP3D_ERR_VALUE, "up3d_residual_jacobian_batched: case index out of range");
-        fused_evaluate(m, phi, host[0], flows[0].u_inf * flows[0].u_inf, m->flows_ws.get(), case_of, up_fz, br_fz,
-                       R, data, rt_out, up_out, mon, s, branch_out);
+        const up3d_flow& f0 = m->batch_flow0;
+        fused_evaluate(m, phi, make_flow(f0), f0.u_inf * f0.u_inf, m->flows_ws.get(), case_of, up_fz, br_fz, R,
+                       data, rt_out, up_out, mon, s, branch_out, n_cases);
     });
 }
 

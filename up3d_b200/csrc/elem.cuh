@@ -8,15 +8,33 @@ namespace up3d {
 
 // grad(phi)_e = sum_i phi_i B_e[i,:] in the reference's order
 // (kernels/gradient.py:52-60), IEEE-rounded.
+// 32-byte read-only global load (one 256-bit request on sm_100 instead of
+// two 128-bit ones: every per-element record here -- B (96 bytes), the face
+// displacements (96 bytes), a node's (x, y, z, 0) (32 bytes) -- starts on a
+// 32-byte boundary, and the L1 request count is what bounds the sweep).
+__device__ __forceinline__ void ld4(const double* p, double& a, double& b, double& c, double& d) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+// The 12 B values of an element (global memory, 32-byte aligned).
+__device__ __forceinline__ void ld_B(const double* __restrict__ be, double b[12]) {
+    ld4(be, b[0], b[1], b[2], b[3]);
+    ld4(be + 4, b[4], b[5], b[6], b[7]);
+    ld4(be + 8, b[8], b[9], b[10], b[11]);
+}
+
+// From the element's nodes c and its 12 B values at `be` (global memory).
+__device__ __forceinline__ void elem_grad_rec(int4 c, const double* __restrict__ be, const double* __restrict__ phi,
+                                              double g[3]) {
+    double b[12];
+    ld_B(be, b);
+    double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
+    g[0] = radd(radd(radd(rmul(p0, b[0]), rmul(p1, b[3])), rmul(p2, b[6])), rmul(p3, b[9]));
+    g[1] = radd(radd(radd(rmul(p0, b[1]), rmul(p1, b[4])), rmul(p2, b[7])), rmul(p3, b[10]));
+    g[2] = radd(radd(radd(rmul(p0, b[2]), rmul(p1, b[5])), rmul(p2, b[8])), rmul(p3, b[11]));
+}
 __device__ __forceinline__ void elem_grad(const int4* __restrict__ conn, const double* __restrict__ B,
                                           const double* __restrict__ phi, int64_t e, double g[3]) {
-    int4 c = conn[e];
-    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
-    double2 b01 = b2[0], b23 = b2[1], b45 = b2[2], b67 = b2[3], b89 = b2[4], bab = b2[5];
-    double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
-    g[0] = radd(radd(radd(rmul(p0, b01.x), rmul(p1, b23.y)), rmul(p2, b67.x)), rmul(p3, b89.y));
-    g[1] = radd(radd(radd(rmul(p0, b01.y), rmul(p1, b45.x)), rmul(p2, b67.y)), rmul(p3, bab.x));
-    g[2] = radd(radd(radd(rmul(p0, b23.x), rmul(p1, b45.y)), rmul(p2, b89.x)), rmul(p3, bab.y));
+    elem_grad_rec(conn[e], B + 12 * e, phi, g);
 }
 
 // Same, also returning B_e (12 values) for reuse.
@@ -24,13 +42,7 @@ __device__ __forceinline__ void elem_grad_B(const int4* __restrict__ conn, const
                                             const double* __restrict__ phi, int64_t e, double g[3],
                                             double b[12], int4& c) {
     c = conn[e];
-    const double2* b2 = reinterpret_cast<const double2*>(B + 12 * e);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        double2 v = b2[k];
-        b[2 * k] = v.x;
-        b[2 * k + 1] = v.y;
-    }
+    ld_B(B + 12 * e, b);
     double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
 #pragma unroll
     for (int d = 0; d < 3; ++d)
@@ -54,8 +66,9 @@ __device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, co
     double pmin = 1e300, pmax = -1e300;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        double4 x = X[nd[k]];
-        double p = dot3r(x.x, x.y, x.z, gx, gy, gz);
+        double x, y, z, w;
+        ld4(reinterpret_cast<const double*>(X + nd[k]), x, y, z, w);
+        double p = dot3r(x, y, z, gx, gy, gz);
         if (p < pmin) pmin = p;
         if (p > pmax) pmax = p;
     }
@@ -64,11 +77,11 @@ __device__ __forceinline__ int64_t upstream_walk(const int4* __restrict__ fn, co
     double reach = 0.0;
     for (int hops = 0; hops < 4 && reach < target; ++hops) {
         const int4 f = fn[cur];
-        const double2* dp = reinterpret_cast<const double2*>(disp + 12 * cur);
-        const double2 a0 = dp[0], a1 = dp[1], a2 = dp[2], a3 = dp[3], a4 = dp[4], a5 = dp[5];
+        double a[12];
+        ld_B(disp + 12 * cur, a);  // the face displacements: the same 96-byte record shape
         const int nb[4] = {f.x, f.y, f.z, f.w};
-        const double d[4] = {dot3r(a0.x, a0.y, a1.x, gx, gy, gz), dot3r(a1.y, a2.x, a2.y, gx, gy, gz),
-                             dot3r(a3.x, a3.y, a4.x, gx, gy, gz), dot3r(a4.y, a5.x, a5.y, gx, gy, gz)};
+        const double d[4] = {dot3r(a[0], a[1], a[2], gx, gy, gz), dot3r(a[3], a[4], a[5], gx, gy, gz),
+                             dot3r(a[6], a[7], a[8], gx, gy, gz), dot3r(a[9], a[10], a[11], gx, gy, gz)};
         int64_t best = -1;
         double best_disp = 0.0;
 #pragma unroll

@@ -38,20 +38,33 @@ from .newton import ChannelWorkspace, _ew_forcing, mach_schedule
 
 
 class BatchedChannels:
-    """The union of several channel meshes on one device."""
+    """The union of several channel meshes on one device.
 
-    def __init__(self, meshes: Sequence[BumpMesh], u_inf: float = 1.0):
+    ``ordering`` renumbers each case's nodes and elements within its own
+    block (``up3d_b200.mesh.order``: "given", "morton", "hilbert"); potentials
+    of the union are in that numbering, ``case_phi`` maps a case's block back
+    to the case mesh's own numbering.  ``BatchedChannels.tuned`` picks the
+    ordering and the launch shapes by timing them."""
+
+    def __init__(self, meshes: Sequence[BumpMesh], u_inf: float = 1.0, ordering: str = "given",
+                 tune: bool = True):
         t = L.require_cuda()
+        from ..mesh.order import renumber
         self.meshes = list(meshes)
         self.n_cases = len(self.meshes)
+        self.ordering = ordering
+        self.renum = [renumber(m.nodes, m.elements, ordering) for m in self.meshes]
         node_off = np.cumsum([0] + [m.n_nodes for m in self.meshes])
         elem_off = np.cumsum([0] + [m.n_tets for m in self.meshes])
-        nodes = np.concatenate([m.nodes for m in self.meshes])
-        elements = np.concatenate([m.elements.astype(np.int64) + node_off[c]
-                                   for c, m in enumerate(self.meshes)]).astype(np.int32)
-        dirichlet = np.concatenate([m.dirichlet_nodes + node_off[c] for c, m in enumerate(self.meshes)])
+        nodes = np.concatenate([r.nodes for r in self.renum])
+        elements = np.concatenate([r.elements.astype(np.int64) + node_off[c]
+                                   for c, r in enumerate(self.renum)]).astype(np.int32)
+        dirichlet = np.concatenate([r.node_set(m.dirichlet_nodes) + node_off[c]
+                                    for c, (m, r) in enumerate(zip(self.meshes, self.renum))])
         self.node_off, self.elem_off = node_off, elem_off
-        self.ws = ChannelWorkspace(nodes, elements, dirichlet, u_inf=u_inf)
+        self.ws = ChannelWorkspace(nodes, elements, dirichlet, u_inf=u_inf, tune=tune)
+        self._node_inv = [t.from_numpy(r.node_inv).cuda() for r in self.renum]
+        self._trial = None
         case_e = np.repeat(np.arange(self.n_cases, dtype=np.int32), np.diff(elem_off))
         case_n = np.repeat(np.arange(self.n_cases, dtype=np.int64), np.diff(node_off))
         self.case_of_elem = t.from_numpy(case_e).cuda()
@@ -88,13 +101,104 @@ class BatchedChannels:
 
     def evaluate(self, phi, machs, jacobian: bool = True):
         """R (and the Jacobian data, rho~, upstream) of every case at once,
-        into the union workspace."""
+        into the union workspace.  machs=None reuses the Mach numbers of the
+        last call (no host synchronisation: capturable for jacobian=False)."""
         ev = self.ws.ev
         L.call("up3d_residual_jacobian_batched", ev.mesh.handle, phi.data_ptr(), self.n_cases,
-               self._flows(machs), self.case_of_elem.data_ptr(), L.ptr(self.up_fz), L.ptr(self.br_fz),
+               None if machs is None else self._flows(machs), self.case_of_elem.data_ptr(),
+               L.ptr(self.up_fz), L.ptr(self.br_fz),
                ev.R.data_ptr(), ev.data.data_ptr() if jacobian else None, ev.rho_tilde.data_ptr(),
                ev.upstream.data_ptr(), self.branch.data_ptr(), ev.monitors.data_ptr(), L.stream_ptr())
         return ev.R
+
+    def case_phi(self, phi, c: int):
+        """Case c's block of a union nodal vector, in the case mesh's own
+        numbering."""
+        a, b = int(self.node_off[c]), int(self.node_off[c + 1])
+        return phi[a:b][self._node_inv[c]]
+
+    def union_phi(self, per_case):
+        """The union nodal vector of per-case vectors (case numbering)."""
+        t = L.torch()
+        parts = [t.as_tensor(v, dtype=t.float64, device="cuda")[t.from_numpy(r.node_perm).cuda()]
+                 for v, r in zip(per_case, self.renum)]
+        return t.cat(parts)
+
+    def trial_merits(self, phi, dphi, lam, mask_b):
+        """sum_free R(phi + lam_c dphi)^2 per case for the per-case step
+        lengths lam (host array), at the Mach numbers of the last evaluate:
+        one CUDA-graph replay (the step, the batched residual and the
+        per-case reduction) and one read-back."""
+        t = L.torch()
+        g = self._trial
+        if g is None or g["frozen"] != (self.up_fz is not None) or g["mask"] is not mask_b:
+            g = self._trial = self._capture_trial(mask_b)
+        g["phi_base"].copy_(phi)
+        g["dphi"].copy_(dphi)
+        g["lam"].copy_(t.from_numpy(np.ascontiguousarray(lam, dtype=np.float64)))
+        g["graph"].replay()
+        return g["merit"].cpu().numpy()
+
+    def _capture_trial(self, mask_b):
+        t = L.torch()
+        n = int(self.node_off[-1])
+        g = {"frozen": self.up_fz is not None, "mask": mask_b,
+             "phi_base": t.zeros(n, dtype=t.float64, device="cuda"),
+             "dphi": t.zeros(n, dtype=t.float64, device="cuda"),
+             "lam": t.zeros(self.n_cases, dtype=t.float64, device="cuda")}
+
+        def body():
+            phi_try = g["phi_base"] + g["lam"][self.case_of_node] * g["dphi"]
+            R = self.evaluate(phi_try, None, jacobian=False)
+            g["merit"] = self.per_case(R.masked_fill(mask_b, 0.0), "sumsq")
+            g["phi_try"] = phi_try
+
+        # captured on a side stream with capture_begin/end directly (the
+        # torch.cuda.graph context would also empty the allocator cache)
+        side = t.cuda.Stream()
+        side.wait_stream(t.cuda.current_stream())
+        graph = t.cuda.CUDAGraph()
+        with t.cuda.stream(side):
+            body()  # warm-up outside the graph (allocations, lazy init)
+            graph.capture_begin()
+            try:
+                body()
+            finally:
+                graph.capture_end()
+        t.cuda.current_stream().wait_stream(side)
+        g["graph"] = graph
+        return g
+
+    @classmethod
+    def tuned(cls, meshes: Sequence[BumpMesh], machs: Sequence[float], u_inf: float = 1.0,
+              orderings: Sequence[str] = ("given", "morton", "hilbert"), reps: int = 5):
+        """The union in the fastest of `orderings`, each with its launch
+        shapes autotuned: one residual + Jacobian evaluation at the
+        freestream is timed per candidate (CUDA events, median of reps).
+        The report lands in ``.tuning_report``."""
+        t = L.require_cuda()
+        best, best_ms, report = None, None, {}
+        for o in orderings:
+            b = cls(meshes, u_inf=u_inf, ordering=o, tune=False)
+            phi = b.ws.freestream.clone()
+            b.evaluate(phi, machs, jacobian=True)
+            shapes = b.ws.ev.mesh.autotune(phi, FlowParams(m_inf=float(np.min(machs)), u_inf=u_inf), reps=reps)
+            ms = []
+            for _ in range(reps):
+                e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+                e0.record()
+                b.evaluate(phi, machs, jacobian=True)
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            med = float(np.median(ms))
+            report[o] = {"ms": med, "shapes": shapes}
+            if best is None or med < best_ms:
+                best, best_ms = b, med
+            else:
+                del b
+        best.tuning_report = {"ordering": best.ordering, "candidates": report}
+        return best
 
     def per_case(self, v, op: str):
         """Per-case max |v| ("amax") or sum v^2 ("sumsq") over the nodes."""
@@ -109,9 +213,11 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                          dm: float = 0.05, tol_residual: float = 1e-10, n_newton_max: int = 30,
                          n_picard_seed: int = 5, amg_rebuild_every: int = 2, gmres_restart: int = 60,
                          gmres_maxiter: int = 10, freeze_tol: float = 1e-6, freeze_refresh_max: int = 2,
-                         verbose: bool = False) -> Dict[str, object]:
+                         use_graphs: bool = True, verbose: bool = False) -> Dict[str, object]:
     """Lockstep Newton of every case (module docstring); returns the union
-    potential, per-case convergence, iteration counts and timings."""
+    potential, per-case convergence, iteration counts and timings.  With
+    use_graphs the line search's trial evaluations replay one captured CUDA
+    graph (step, batched residual, per-case merit)."""
     t = L.require_cuda()
     ws = batch.ws
     machs = np.asarray(machs, dtype=np.float64)
@@ -239,10 +345,13 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
             best_merit = np.full(C, np.inf)
             merit_h = merit.cpu().numpy()
             for _ in range(5):
-                lam_node = t.from_numpy(lam).cuda()[case_node]
-                phi_try = phi + lam_node * dphi
-                R_try = batch.evaluate(phi_try, m_level, jacobian=False)
-                m_try = batch.per_case(R_try.masked_fill(mask_b, 0.0), "sumsq").cpu().numpy()
+                if use_graphs:
+                    m_try = batch.trial_merits(phi, dphi, lam, mask_b)
+                else:
+                    lam_node = t.from_numpy(lam).cuda()[case_node]
+                    phi_try = phi + lam_node * dphi
+                    R_try = batch.evaluate(phi_try, m_level, jacobian=False)
+                    m_try = batch.per_case(R_try.masked_fill(mask_b, 0.0), "sumsq").cpu().numpy()
                 ok = np.isfinite(m_try) & (m_try <= merit_h) & ~accepted
                 better = np.isfinite(m_try) & (m_try < best_merit) & ~accepted
                 best_lam[better] = lam[better]

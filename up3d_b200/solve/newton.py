@@ -56,8 +56,11 @@ class ChannelWorkspace:
     """Per-mesh device state of the channel solves: the mesh, the fused
     evaluator, the Dirichlet split and the Picard operator."""
 
+    # meshes from this size on get their launch shapes autotuned once
+    TUNE_MIN_TETS = 100_000
+
     def __init__(self, nodes, elements, dirichlet_nodes, u_inf: float = 1.0,
-                 mesh: Optional[DeviceMesh] = None):
+                 mesh: Optional[DeviceMesh] = None, tune: bool = True):
         t = L.require_cuda()
         self.mesh = mesh if mesh is not None else get_mesh(nodes, elements)
         from ..kernels.jacobian import PicardOperator
@@ -74,6 +77,10 @@ class ChannelWorkspace:
         self.phi_dir = t.zeros(n, dtype=t.float64, device="cuda")
         self.phi_dir[self.dn] = self.u_inf * x[self.dn]
         self.freestream = self.u_inf * x
+        if tune and self.mesh.n_tets >= self.TUNE_MIN_TETS and self.mesh.tuning()["elem_us"] == 0.0:
+            # launch shapes timed at the freestream (every element walks);
+            # every shape computes the same bits
+            self.mesh.autotune(self.freestream, FlowParams(m_inf=0.7, u_inf=self.u_inf))
 
     def residual(self, phi, flow: FlowParams, frozen=None, jacobian=False):
         """R (device view), monitors; R on constrained rows is ignored."""
