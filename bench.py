@@ -55,7 +55,7 @@ def parse():
                    help="node/element numbering of the device mesh")
     p.add_argument("--tune", default="auto",
                    help="launch shapes: 'auto' (autotuner), 'default', or "
-                        "'persistent,blocks_per_sm,row_lanes'")
+                        "'persistent,threads_per_sm,row_lanes'")
     p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
                    help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
     p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
@@ -368,7 +368,7 @@ def batched_timing(spec, seed=0):
     # time to 1e-10: batched lockstep vs sequential plain solves (second run timed)
     def fresh():
         b = BatchedChannels(meshes, ordering=batch.ordering)
-        b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_blocks_per_sm"],
+        b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_threads_per_sm"],
                                 shapes_tuned["row_lanes"])
         return b
     res_b = None

@@ -286,22 +286,24 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
  *   elem_persistent  0: one thread per element (grid capped at 64 blocks
  *                    per SM); 1: one resident wave of blocks looping over
  *                    256-element tiles
- *   elem_blocks_per_sm  register budget of the Newton-Jacobian sweep:
- *                    2 (up to 128 registers per thread, no spills) or 3
- *                    (up to 80, spilling to L1) resident 256-thread blocks
+ *   elem_threads_per_sm  register budget of the Newton-Jacobian sweep as
+ *                    the resident threads per SM it allows: 512 (256-thread
+ *                    blocks, up to 128 registers, no spills), 640 (128-thread
+ *                    blocks, up to 102) or 768 (256-thread blocks, up to 80,
+ *                    spilling to L1)
  *   row_lanes        lanes per row of the row gather: 4, 8, 16 or 32
  *   elem_us, row_us  autotune output: median time per launch of the
  *                    chosen shapes (0 when set by hand) */
 typedef struct {
     int32_t elem_persistent;
-    int32_t elem_blocks_per_sm;
+    int32_t elem_threads_per_sm;
     int32_t row_lanes;
     int32_t reserved; /* 0 */
     double elem_us;
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 2, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
+/* Default: {0, 512, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 

@@ -10,8 +10,8 @@ from conftest import has_cuda, rel_err
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
 
-# (persistent, blocks per SM, lanes per row)
-SHAPES = [(0, 2, 4), (0, 3, 8), (1, 2, 8), (1, 3, 16), (1, 2, 32), (1, 3, 4), (0, 2, 16)]
+# (persistent, resident threads per SM, lanes per row)
+SHAPES = [(0, 512, 4), (0, 768, 8), (1, 512, 8), (1, 768, 16), (1, 640, 32), (0, 640, 4), (1, 640, 16)]
 
 
 def _setup():
@@ -39,7 +39,7 @@ def test_every_shape_gives_the_same_bits():
     assert dm.n_tets % 256 != 0
     flow = FlowParams(m_inf=0.8)
     assert dm.tuning()["row_lanes"] == 8 and dm.tuning()["elem_persistent"] == 0
-    assert dm.tuning()["elem_blocks_per_sm"] == 2
+    assert dm.tuning()["elem_threads_per_sm"] == 512
     R0, J0, up0, rt0, mon0 = _outputs(ev, phi, flow)
     assert mon0["n_term3_active"] > 0
     frozen = (up0.to(torch.int64), torch.zeros(dm.n_tets, dtype=torch.int8, device="cuda"))
@@ -68,7 +68,7 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
     J0 = ev.jacobian().to_scipy()
     t = dm.autotune(phi, flow, reps=3)
     assert t == dm.tuning()
-    assert (t["elem_persistent"], t["elem_blocks_per_sm"]) in {(0, 2), (1, 2), (0, 3), (1, 3)}
+    assert (t["elem_persistent"], t["elem_threads_per_sm"]) in {(0, 512), (1, 512), (1, 640), (0, 768), (1, 768)}
     assert t["row_lanes"] in (4, 8, 16, 32)
     assert t["elem_us"] > 0 and t["row_us"] > 0
     R = ev.evaluate(phi, flow, jacobian=True).clone()
@@ -81,7 +81,7 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
 
 def test_bad_shapes_are_refused():
     _, _, dm, _, _ = _setup()
-    for bad in [(2, 2, 8), (-1, 2, 8), (0, 1, 8), (0, 4, 8), (0, 2, 2), (0, 2, 12), (0, 2, 64)]:
+    for bad in [(2, 512, 8), (-1, 512, 8), (0, 256, 8), (0, 1024, 8), (0, 512, 2), (0, 512, 12), (0, 512, 64)]:
         with pytest.raises(ValueError):
             dm.set_tuning(*bad)
     assert dm.tuning()["row_lanes"] == 8

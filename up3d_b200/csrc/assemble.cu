@@ -326,9 +326,10 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // taking the flow of its case, flows[case_of[e]] (an index outside
 // [0, n_cases) reads case 0: the host validates the indices, and a table
 // reused without validation can never be read out of bounds).
-// MB: resident blocks per SM the register allocation must allow.
-template <bool FROZEN, bool JAC, bool BATCH, int MB>
-__global__ void __launch_bounds__(256, MB)
+// NT threads per block, MB resident blocks per SM that the register
+// allocation must allow.
+template <bool FROZEN, bool JAC, bool BATCH, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB)
     k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
                  const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F0, double u2, const int64_t* __restrict__ up_fz,
@@ -861,32 +862,36 @@ __global__ void k_check_cases(const int32_t* __restrict__ case_of, int64_t E, in
 
 // One launch of the fused element sweep in the mesh's tuned shape: one
 // thread per element (grid capped at 64 blocks per SM) or one resident
-// wave (SMs x the kernel's occupancy) looping over 256-element tiles; the
-// Jacobian sweep compiled for 2 or 3 resident blocks per SM.
-template <bool FR, bool JA, bool BA, int MB, class... A>
+// wave (SMs x the kernel's occupancy) looping over block-sized tiles; the
+// Jacobian sweep compiled for 512 (256 x 2), 640 (128 x 5) or 768 (256 x 3)
+// resident threads per SM.
+template <bool FR, bool JA, bool BA, int NT, int MB, class... A>
 static void launch_sweep_mb(const up3d_mesh* m, cudaStream_t s, A... args) {
-    constexpr int block = 256;
-    auto kern = k_fused_elem<FR, JA, BA, MB>;
+    auto kern = k_fused_elem<FR, JA, BA, NT, MB>;
     unsigned grid;
     if (m->tune.elem_persistent) {
         static int occ = 0;  // same for every device of the process (one architecture)
         if (occ == 0) {
             int nb = 0;
-            UP3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, block, 0));
+            UP3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, NT, 0));
             occ = nb > 0 ? nb : 1;
         }
-        grid = grid_for(m->E, block, (int64_t)m->n_sms * occ);
+        grid = grid_for(m->E, NT, (int64_t)m->n_sms * occ);
     } else {
-        grid = grid_for(m->E, block, (int64_t)m->n_sms * 64);
+        grid = grid_for(m->E, NT, (int64_t)m->n_sms * 64 * (256 / NT));
     }
-    kern<<<grid, block, 0, s>>>(args...);
+    kern<<<grid, NT, 0, s>>>(args...);
     UP3D_CHECK_LAUNCH();
 }
 
 template <bool FR, bool JA, bool BA, class... A>
 static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
-    if (JA && m->tune.elem_blocks_per_sm == 3) launch_sweep_mb<FR, JA, BA, 3>(m, s, args...);
-    else launch_sweep_mb<FR, JA, BA, JA ? UP3D_ELEM_MINB_JAC : UP3D_ELEM_MINB>(m, s, args...);
+    if (!JA) return launch_sweep_mb<FR, JA, BA, 256, UP3D_ELEM_MINB>(m, s, args...);
+    switch (m->tune.elem_threads_per_sm) {
+        case 640: launch_sweep_mb<FR, JA, BA, 128, 5>(m, s, args...); break;
+        case 768: launch_sweep_mb<FR, JA, BA, 256, 3>(m, s, args...); break;
+        default: launch_sweep_mb<FR, JA, BA, 256, UP3D_ELEM_MINB_JAC>(m, s, args...); break;
+    }
 }
 
 // The fused evaluation: element sweep, row gather, Term 3.  flows_d /
@@ -970,8 +975,9 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
                      "up3d_mesh_set_tuning: elem_persistent must be 0 or 1");
         UP3D_REQUIRE(t->row_lanes == 4 || t->row_lanes == 8 || t->row_lanes == 16 || t->row_lanes == 32,
                      UP3D_ERR_VALUE, "up3d_mesh_set_tuning: row_lanes must be 4, 8, 16 or 32");
-        UP3D_REQUIRE(t->elem_blocks_per_sm == 2 || t->elem_blocks_per_sm == 3, UP3D_ERR_VALUE,
-                     "up3d_mesh_set_tuning: elem_blocks_per_sm must be 2 or 3");
+        UP3D_REQUIRE(t->elem_threads_per_sm == 512 || t->elem_threads_per_sm == 640 ||
+                         t->elem_threads_per_sm == 768,
+                     UP3D_ERR_VALUE, "up3d_mesh_set_tuning: elem_threads_per_sm must be 512, 640 or 768");
 
         m->tune = *t;
         m->tune.reserved = 0;
@@ -1029,13 +1035,13 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
             int8_t* no_brout = nullptr;
             up3d_monitors* mo = m->mon_ws.get();
             // the element sweep: Newton Jacobian, live upwind selection
-            // (persistent, blocks per SM)
-            static const int shapes[][2] = {{0, 2}, {1, 2}, {0, 3}, {1, 3}};
+            // (persistent, resident threads per SM)
+            static const int shapes[][2] = {{0, 512}, {1, 512}, {1, 640}, {0, 768}, {1, 768}};
             double best_e = 0.0;
             int best_k = -1;
             for (int k = 0; k < (int)(sizeof(shapes) / sizeof(shapes[0])); ++k) {
                 m->tune.elem_persistent = shapes[k][0];
-                m->tune.elem_blocks_per_sm = shapes[k][1];
+                m->tune.elem_threads_per_sm = shapes[k][1];
                 const double t = time_it([&] {
                     launch_sweep<false, true, false>(m, s, m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(),
                                                      m->disp.get(), m->nodes4.get(), phi, F, u2, no_up, no_br, m->E,
@@ -1048,7 +1054,7 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
                 }
             }
             m->tune.elem_persistent = shapes[best_k][0];
-            m->tune.elem_blocks_per_sm = shapes[best_k][1];
+            m->tune.elem_threads_per_sm = shapes[best_k][1];
             // the row gather, on the local matrices the sweep left
             static const int lanes[] = {4, 8, 16, 32};
             double best_r = 0.0;

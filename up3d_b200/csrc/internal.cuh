@@ -112,7 +112,7 @@ struct up3d_mesh {
     int32_t max_row_len = 0, max_deg = 0;
     int32_t n_colors = -1;
     int32_t n_sms = 148;                       // multiprocessors of the mesh's device
-    up3d_tuning tune = {0, 2, 8, 0, 0.0, 0.0};  // launch shapes of the fused passes
+    up3d_tuning tune = {0, 512, 8, 0, 0.0, 0.0};  // launch shapes of the fused passes
     int32_t batch_cases = 0;                   // cases of the flow table in flows_ws (0 = none)
     up3d_flow batch_flow0 = {};                // its case 0
 
