@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
                    help="cases:smallest:largest:mach_lo:mach_hi of the batched comparison ('' to skip); "
                         "the full batched configuration is 48:20x6x5:200x60x50:0.5:0.85")
+    p.add_argument("--weighted", default="200x60x50:0.8",
+                   help="mesh:mach of the weighted upwind timing ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -303,6 +305,61 @@ def adjoint_timing(spec):
             "check": "tests/test_gpu_adjoint.py: finite differences to 1e-6 relative"}
 
 
+def weighted_timing(spec):
+    """The weighted upwind densities (UpwindOperator(weighted=True), modes
+    "kernel" and "blend", kernels/upwind.py:176-454) on a channel mesh at
+    the three supersonic-pocket states: device time per sweep (CUDA events,
+    inputs resident), the neighbourhood build, and the oracle's time on the
+    box's host cores for the same sweep (a bounded sample: one state)."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.kernels.upwind import UpwindOperator
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    mesh_s, mach_s = spec.split(":")
+    shape = tuple(int(v) for v in mesh_s.split("x"))
+    M = float(mach_s)
+    m = bump_channel(*shape, amplitude=AMPLITUDE, seed=0)
+    op = O.PicardOperator(m.nodes, m.elements)
+    states = []
+    for fam in ("accelerating", "shockpoint", "mixed"):
+        grad, q2 = op.velocities(pocket_state(m, fam))
+        q2l = O.limit_q2_field(q2, M, 3.0)
+        rho = O.density_field(q2l, M)
+        states.append((grad.copy(), q2l, rho))
+    dev = [tuple(torch.from_numpy(a).cuda() for a in st) for st in states]
+    out = {"mesh": mesh_s, "n_tets": int(m.n_tets), "m_inf": M}
+    for mode in ("kernel", "blend"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        upw = UpwindOperator(m.nodes, m.elements, weighted=True, mode=mode)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        for k in range(3):
+            upw.rho_tilde(*dev[k], M, 1.5, 0.95)
+        reps = 30
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for k in range(reps):
+            upw.rho_tilde(*dev[k % 3], M, 1.5, 0.95)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        ref = O.UpwindOperator(m.nodes, m.elements, weighted=True, mode=mode)
+        t0 = time.perf_counter()
+        r = ref.rho_tilde(*states[0], M, 1.5, 0.95).copy()
+        cpu_s = time.perf_counter() - t0
+        d = upw.rho_tilde(*dev[0], M, 1.5, 0.95).cpu().numpy()
+        out[mode] = {"ms_per_sweep": round(ms, 4), "melem_s": round(m.n_tets / ms / 1e3, 1),
+                     "setup_s": round(setup_s, 4),
+                     "n_supersonic": int(upw.n_supersonic),
+                     "cpu_oracle_s": round(cpu_s, 4), "cpu_cores": O.num_threads(),
+                     "max_rel_err_vs_oracle": float(np.abs(d - r).max() / np.abs(r).max())}
+        if mode == "kernel":
+            out[mode]["neighbors_per_element"] = round(float(len(upw._nb_idx)) / m.n_tets, 2)
+    return out
+
+
 def batched_timing(spec, seed=0):
     """Many cases in one launch: meshes of log-uniform size between the
     smallest and largest box, M_inf ~ U[mach_lo, mach_hi], bump amplitude ~
@@ -530,6 +587,7 @@ def run_ours(args):
     newton = newton_timing(args.newton) if args.newton else None
     adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
     batched = batched_timing(args.batched) if args.batched else None
+    weighted = weighted_timing(args.weighted) if args.weighted else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -583,6 +641,7 @@ def run_ours(args):
             "newton": newton,
             "adjoint": adjoint,
             "batched": batched,
+            "weighted_upwind": weighted,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -252,6 +252,48 @@ int up3d_residual_vjp(up3d_mesh* mesh, const double* phi, const up3d_flow* flow,
 int up3d_jacobian_transpose(up3d_mesh* mesh, const double* data, double* data_t,
                             up3d_stream stream);
 
+/* ------------------------------------------------------ weighted upwind */
+
+/* compute_face_normals (kernels/upwind.py:128-172): outward unit normal of
+ * face f (opposite local node f) into out (n_tets, 4, 3), device. */
+int up3d_face_normals(const up3d_mesh* mesh, double* out, up3d_stream stream);
+
+/* build_upstream_neighborhoods (kernels/upwind.py:313-341): the elements
+ * within `depth` face hops of each element, itself excluded, ascending;
+ * built once per depth and kept on the mesh (rebuilt after
+ * up3d_mesh_set_face_neighbors).  Device views of the CSR (offsets int64
+ * n_tets + 1, indices int32) and the total; any output may be NULL.
+ * UP3D_ERR_VALUE for depth outside [1, 4] (the reference takes any depth;
+ * 4 hops reach up to 160 elements).  Synchronises the stream when it
+ * builds. */
+int up3d_mesh_neighborhoods(up3d_mesh* mesh, int depth, const int64_t** offsets,
+                            const int32_t** indices, int64_t* total, up3d_stream stream);
+
+/* The same from a face-neighbour table alone (device int32 (n, 4), -1 =
+ * boundary), into caller buffers: with indices == NULL fills offsets
+ * (n + 1, device int64) and *total (host; synchronises the stream); then,
+ * with indices (device int32, *total), fills them. */
+int up3d_face_neighborhoods(const int32_t* face_neighbors, int64_t n, int depth, int64_t* offsets,
+                            int32_t* indices, int64_t* total, up3d_stream stream);
+
+/* rho_tilde_kernel_sweep (kernels/upwind.py:345-454), the "kernel" mode of
+ * UpwindOperator(weighted=True) (:744-819): rho_up and M^2_up as Gaussian
+ * averages over the depth-hop neighbourhood centred one streamwise reach
+ * upstream.  grad (n_tets, 3), q2, rho, nu, rho_tilde (n_tets) device;
+ * monitors (device, may be NULL) get nu_max / n_supersonic / n_floored. */
+int up3d_rho_tilde_kernel(up3d_mesh* mesh, const double* grad, const double* q2, const double* rho,
+                          const up3d_flow* flow, int depth, double reach_frac,
+                          double sigma_s_frac, double sigma_p_frac, double* nu,
+                          double* rho_tilde, up3d_monitors* monitors, up3d_stream stream);
+
+/* rho_tilde_weighted_sweep (kernels/upwind.py:176-309), the "blend" mode:
+ * an upstream-weighted blend over the face neighbours with reach
+ * compensation.  Arrays as up3d_rho_tilde_kernel. */
+int up3d_rho_tilde_blend(const up3d_mesh* mesh, const double* grad, const double* q2,
+                         const double* rho, const up3d_flow* flow, double p_weight,
+                         double reach_frac, double reach_gain_max, double* nu,
+                         double* rho_tilde, up3d_monitors* monitors, up3d_stream stream);
+
 /* ------------------------------------------------------ batched cases */
 
 /* up3d_residual_jacobian for several cases in one mesh (their meshes

@@ -80,6 +80,12 @@ def _declare(L):
         "orc_term3_coo": (None, [_p, _i64, _p, _p, _p, _p, _p, _p, _d, _p, _p, _p]),
         "orc_spmv": (None, [_p, _p, _p, _p, _i64, _p]),
         "orc_num_threads": (ctypes.c_int, []),
+        "orc_face_normals": (None, [_p, _p, _i64, _p]),
+        "orc_neighborhoods": (_i64, [_p, _i64, ctypes.c_int, _p, _p]),
+        "orc_rho_tilde_kernel": (None, [_p, _p, _p, _p, _p, _p, _p, _p, _i64, _d, _d, _d, _d, _d,
+                                        _d, _d, _d, _p, _p]),
+        "orc_rho_tilde_blend": (None, [_p, _p, _p, _p, _p, _p, _p, _i64, _d, _d, _d, _d, _d,
+                                       _d, _d, _d, _p, _p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -284,14 +290,44 @@ class PicardOperator:
         return J
 
 
-class UpwindOperator:
-    """Oracle restatement of ``kernels/upwind.py:733-920`` (walk flux)."""
+def face_normals(nodes, elements):
+    """compute_face_normals (kernels/upwind.py:128-172): (n, 4, 3)."""
+    X, el = _c(nodes, np.float64), _c(elements, np.int32)
+    out = np.empty((len(el), 4, 3))
+    lib().orc_face_normals(_ptr(X), _ptr(el), len(el), _ptr(out))
+    return out
 
-    def __init__(self, nodes, elements):
+
+def build_upstream_neighborhoods(face_neighbors, depth=3):
+    """build_upstream_neighborhoods (kernels/upwind.py:313-341): CSR
+    (offsets int64, indices int64) of the elements within `depth` face
+    hops, e excluded, ascending."""
+    fn = _c(face_neighbors, np.int32)
+    n = len(fn)
+    off = np.zeros(n + 1, dtype=np.int64)
+    total = lib().orc_neighborhoods(_ptr(fn), n, int(depth), _ptr(off), None)
+    idx = np.empty(max(total, 1), dtype=np.int32)
+    lib().orc_neighborhoods(_ptr(fn), n, int(depth), _ptr(off), _ptr(idx))
+    return off, idx[:total].astype(np.int64)
+
+
+class UpwindOperator:
+    """Oracle restatement of ``kernels/upwind.py:733-920``: the walk flux,
+    and the weighted "kernel" / "blend" modes of ``rho_tilde``."""
+
+    def __init__(self, nodes, elements, weighted=False, mode="kernel", p_weight=3.0,
+                 reach_frac=1.0, reach_gain_max=4.0, nbr_depth=3, sigma_s_frac=0.35,
+                 sigma_p_frac=0.35):
         self.nodes = _c(nodes, np.float64)
         self.elements = _c(elements, np.int32)
         self.face_neighbors = face_adjacency(self.elements)
         self.centroids = centroids(self.nodes, self.elements)
+        self.weighted, self.mode = weighted, mode
+        self.p_weight, self.reach_frac, self.reach_gain_max = p_weight, reach_frac, reach_gain_max
+        self.sigma_s_frac, self.sigma_p_frac = sigma_s_frac, sigma_p_frac
+        self._nb_off = self._nb_idx = None
+        if weighted and mode == "kernel":
+            self._nb_off, self._nb_idx = build_upstream_neighborhoods(self.face_neighbors, nbr_depth)
         n = len(self.elements)
         self._upstream = np.empty(n, dtype=np.int64)
         self.nu = np.empty(n)
@@ -320,10 +356,34 @@ class UpwindOperator:
             self.n_floored = int(np.count_nonzero(branch == 3))
 
     def rho_tilde(self, grad, q2, rho, m_inf, C, m_crit, gamma=GAMMA, rho_floor=0.05):
+        if self.weighted:
+            return self._rho_tilde_weighted(grad, q2, rho, m_inf, C, m_crit, gamma, rho_floor)
         up = self.upstream(grad)
         q2, rho = _c(q2, np.float64), _c(rho, np.float64)
         lib().orc_rho_tilde(_ptr(q2), _ptr(rho), _ptr(up), len(q2), m_inf, m_crit, C,
                             gamma, rho_floor, _ptr(self.nu), _ptr(self._rho_tilde))
+        self._monitors(rho_floor)
+        return self._rho_tilde
+
+    def _rho_tilde_weighted(self, grad, q2, rho, m_inf, C, m_crit, gamma, rho_floor):
+        grad = _c(grad, np.float64)
+        q2, rho = _c(q2, np.float64), _c(rho, np.float64)
+        cen = _c(self.centroids, np.float64)
+        n = len(q2)
+        if self.mode == "kernel":
+            off = _c(self._nb_off, np.int64)
+            idx = _c(self._nb_idx, np.int32)
+            lib().orc_rho_tilde_kernel(_ptr(q2), _ptr(rho), _ptr(grad), _ptr(self.nodes),
+                                       _ptr(self.elements), _ptr(cen), _ptr(off), _ptr(idx), n,
+                                       m_inf, m_crit, C, gamma, rho_floor, self.reach_frac,
+                                       self.sigma_s_frac, self.sigma_p_frac, _ptr(self.nu),
+                                       _ptr(self._rho_tilde))
+        else:
+            fn = _c(self.face_neighbors, np.int32)
+            lib().orc_rho_tilde_blend(_ptr(q2), _ptr(rho), _ptr(grad), _ptr(self.nodes),
+                                      _ptr(self.elements), _ptr(cen), _ptr(fn), n, m_inf, m_crit, C,
+                                      gamma, rho_floor, self.p_weight, self.reach_frac,
+                                      self.reach_gain_max, _ptr(self.nu), _ptr(self._rho_tilde))
         self._monitors(rho_floor)
         return self._rho_tilde
 

@@ -667,3 +667,192 @@ ORC_API int orc_num_threads(void) {
     }
     return n;
 }
+
+/* ------------------------------------------------------------------ */
+/* Weighted upwind modes, kernels/upwind.py:128-454                     */
+/* ------------------------------------------------------------------ */
+
+/* compute_face_normals, kernels/upwind.py:128-172: outward unit normal of
+ * face f (opposite local node f), out (n, 4, 3). */
+ORC_API void orc_face_normals(const double* X, const int32_t* el, int64_t n, double* out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < n; ++e)
+        for (int f = 0; f < 4; ++f) {
+            const double* a = X + 3 * (int64_t)el[4 * e + orc_face_nodes[f][0]];
+            const double* b = X + 3 * (int64_t)el[4 * e + orc_face_nodes[f][1]];
+            const double* c = X + 3 * (int64_t)el[4 * e + orc_face_nodes[f][2]];
+            const double* p = X + 3 * (int64_t)el[4 * e + f];
+            double e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+            double e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+            double nx = e1y * e2z - e1z * e2y;
+            double ny = e1z * e2x - e1x * e2z;
+            double nz = e1x * e2y - e1y * e2x;
+            double nn = sqrt(nx * nx + ny * ny + nz * nz);
+            if (nn > 0.0) { nx /= nn; ny /= nn; nz /= nn; }
+            double ox = (a[0] + b[0] + c[0]) / 3.0 - p[0];
+            double oy = (a[1] + b[1] + c[1]) / 3.0 - p[1];
+            double oz = (a[2] + b[2] + c[2]) / 3.0 - p[2];
+            if (nx * ox + ny * oy + nz * oz < 0.0) { nx = -nx; ny = -ny; nz = -nz; }
+            out[12 * e + 3 * f] = nx;
+            out[12 * e + 3 * f + 1] = ny;
+            out[12 * e + 3 * f + 2] = nz;
+        }
+}
+
+/* build_upstream_neighborhoods, kernels/upwind.py:313-341: the elements
+ * within `depth` face hops of e, e excluded, ascending.  With idx == NULL
+ * fills off (n + 1) and returns the total; else fills idx from off. */
+ORC_API int64_t orc_neighborhoods(const int32_t* fn, int64_t n, int depth, int64_t* off, int32_t* idx) {
+    int64_t total = 0;
+    if (!idx) off[0] = 0;
+    int64_t cap = 16;
+    int64_t* seen = (int64_t*)malloc(sizeof(int64_t) * cap);
+    int64_t* frontier = (int64_t*)malloc(sizeof(int64_t) * cap);
+    int64_t* next = (int64_t*)malloc(sizeof(int64_t) * cap);
+    for (int64_t e = 0; e < n; ++e) {
+        int64_t ns = 0, nf = 0;
+        seen[ns++] = e;
+        frontier[nf++] = e;
+        for (int d = 0; d < depth; ++d) {
+            int64_t nn = 0;
+            for (int64_t i = 0; i < nf; ++i)
+                for (int f = 0; f < 4; ++f) {
+                    int64_t nb = fn[4 * frontier[i] + f];
+                    if (nb < 0) continue;
+                    int found = 0;
+                    for (int64_t j = 0; j < ns && !found; ++j) found = seen[j] == nb;
+                    if (found) continue;
+                    if (ns + 1 > cap || nn + 1 > cap) {
+                        cap *= 2;
+                        seen = (int64_t*)realloc(seen, sizeof(int64_t) * cap);
+                        frontier = (int64_t*)realloc(frontier, sizeof(int64_t) * cap);
+                        next = (int64_t*)realloc(next, sizeof(int64_t) * cap);
+                    }
+                    seen[ns++] = nb;
+                    next[nn++] = nb;
+                }
+            int64_t* t = frontier;
+            frontier = next;
+            next = t;
+            nf = nn;
+        }
+        qsort(seen, (size_t)ns, sizeof(int64_t), cmp_i64);
+        if (idx) {
+            int64_t w = off[e];
+            for (int64_t j = 0; j < ns; ++j)
+                if (seen[j] != e) idx[w++] = (int32_t)seen[j];
+        } else {
+            total += ns - 1;
+            off[e + 1] = total;
+        }
+    }
+    free(seen);
+    free(frontier);
+    free(next);
+    return idx ? off[n] : total;
+}
+
+/* rho_tilde_kernel_sweep, kernels/upwind.py:345-454 */
+ORC_API void orc_rho_tilde_kernel(const double* q2, const double* rho, const double* grad, const double* X,
+                                  const int32_t* el, const double* cen, const int64_t* nb_off,
+                                  const int32_t* nb_idx, int64_t n, double m_inf, double m_crit, double C,
+                                  double gamma, double rho_floor, double reach_frac, double sig_s,
+                                  double sig_p, double* nu_out, double* rt_out) {
+    double mc2 = m_crit * m_crit;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < n; ++e) {
+        double gx = grad[3 * e], gy = grad[3 * e + 1], gz = grad[3 * e + 2];
+        double gmag = sqrt(gx * gx + gy * gy + gz * gz);
+        double nu_e = orc_switch(orc_mach2(q2[e], m_inf, gamma), mc2, C);
+        if (gmag <= 0.0) { nu_out[e] = nu_e; rt_out[e] = rho[e]; continue; }
+        double vx = gx / gmag, vy = gy / gmag, vz = gz / gmag;
+        double pmin = 1e300, pmax = -1e300;
+        for (int k = 0; k < 4; ++k) {
+            const double* x = X + 3 * (int64_t)el[4 * e + k];
+            double pr = x[0] * vx + x[1] * vy + x[2] * vz;
+            if (pr < pmin) pmin = pr;
+            if (pr > pmax) pmax = pr;
+        }
+        double extent = pmax - pmin;
+        double target = reach_frac * extent;
+        double ss = sig_s * extent, sp = sig_p * extent;
+        double inv2ss = 1.0 / (2.0 * (ss * ss) + 1e-300);
+        double inv2sp = 1.0 / (2.0 * (sp * sp) + 1e-300);
+        double w_sum = 0.0, rho_acc = 0.0, m2_acc = 0.0;
+        for (int64_t j = nb_off[e]; j < nb_off[e + 1]; ++j) {
+            int64_t c = nb_idx[j];
+            double dx = cen[3 * c] - cen[3 * e], dy = cen[3 * c + 1] - cen[3 * e + 1],
+                   dz = cen[3 * c + 2] - cen[3 * e + 2];
+            double up = -(vx * dx + vy * dy + vz * dz);
+            if (up <= 0.0) continue;
+            double d2 = dx * dx + dy * dy + dz * dz;
+            double perp2 = d2 - up * up;
+            if (perp2 < 0.0) perp2 = 0.0;
+            double w = exp(-((up - target) * (up - target) * inv2ss + perp2 * inv2sp));
+            w_sum += w;
+            rho_acc += w * rho[c];
+            m2_acc += w * orc_mach2(q2[c], m_inf, gamma);
+        }
+        if (w_sum <= 0.0) { nu_out[e] = nu_e; rt_out[e] = rho[e]; continue; }
+        double rho_up = rho_acc / w_sum, m2_up = m2_acc / w_sum;
+        double nu_u = orc_switch(m2_up, mc2, C);
+        double nu = nu_e > nu_u ? nu_e : nu_u;
+        nu_out[e] = nu;
+        if (nu <= 0.0) { rt_out[e] = rho[e]; continue; }
+        double rt = rho[e] - nu * (rho[e] - rho_up);
+        rt_out[e] = rt > rho_floor ? rt : rho_floor;
+    }
+}
+
+/* rho_tilde_weighted_sweep ("blend"), kernels/upwind.py:176-309 */
+ORC_API void orc_rho_tilde_blend(const double* q2, const double* rho, const double* grad, const double* X,
+                                 const int32_t* el, const double* cen, const int32_t* fn, int64_t n,
+                                 double m_inf, double m_crit, double C, double gamma, double rho_floor,
+                                 double p_weight, double reach_frac, double gain_max, double* nu_out,
+                                 double* rt_out) {
+    double mc2 = m_crit * m_crit;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < n; ++e) {
+        double gx = grad[3 * e], gy = grad[3 * e + 1], gz = grad[3 * e + 2];
+        double gmag = sqrt(gx * gx + gy * gy + gz * gz);
+        double nu_e = orc_switch(orc_mach2(q2[e], m_inf, gamma), mc2, C);
+        if (gmag <= 0.0) { nu_out[e] = nu_e; rt_out[e] = rho[e]; continue; }
+        double vx = gx / gmag, vy = gy / gmag, vz = gz / gmag;
+        double w_sum = 0.0, rho_acc = 0.0, m2_acc = 0.0, reach_acc = 0.0;
+        for (int f = 0; f < 4; ++f) {
+            int64_t nb = fn[4 * e + f];
+            if (nb < 0) continue;
+            double dx = cen[3 * nb] - cen[3 * e], dy = cen[3 * nb + 1] - cen[3 * e + 1],
+                   dz = cen[3 * nb + 2] - cen[3 * e + 2];
+            double dlen = sqrt(dx * dx + dy * dy + dz * dz);
+            if (dlen <= 0.0) continue;
+            double up = -(vx * dx + vy * dy + vz * dz);
+            double a = up / dlen;
+            if (a <= 0.0) continue;
+            double w = pow(a, p_weight);
+            w_sum += w;
+            rho_acc += w * rho[nb];
+            m2_acc += w * orc_mach2(q2[nb], m_inf, gamma);
+            reach_acc += w * up;
+        }
+        if (w_sum <= 0.0) { nu_out[e] = nu_e; rt_out[e] = rho[e]; continue; }
+        double rho_up = rho_acc / w_sum, m2_up = m2_acc / w_sum, reach = reach_acc / w_sum;
+        double nu_u = orc_switch(m2_up, mc2, C);
+        double nu = nu_e > nu_u ? nu_e : nu_u;
+        nu_out[e] = nu;
+        if (nu <= 0.0) { rt_out[e] = rho[e]; continue; }
+        double pmin = 1e300, pmax = -1e300;
+        for (int k = 0; k < 4; ++k) {
+            const double* x = X + 3 * (int64_t)el[4 * e + k];
+            double pr = x[0] * vx + x[1] * vy + x[2] * vz;
+            if (pr < pmin) pmin = pr;
+            if (pr > pmax) pmax = pr;
+        }
+        double reach_target = reach_frac * (pmax - pmin);
+        double g = reach_target / (reach > 1e-30 ? reach : 1e-30);
+        if (g < 1.0) g = 1.0;
+        else if (g > gain_max) g = gain_max;
+        double rt = rho[e] - nu * g * (rho[e] - rho_up);
+        rt_out[e] = rt > rho_floor ? rt : rho_floor;
+    }
+}

@@ -4,7 +4,7 @@ reference (pyfp3d, pure Python + Numba) on synthetic Kuhn bump meshes.
 Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
-    python tests/golden/make_golden.py /path/to/UP3D
+    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -21,6 +21,8 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   op.assemble_residual / assemble_matrix / assemble_newton_jacobian
                                                       kernels/jacobian.py:272-375
   solve_subsonic (pyamg swapped for scipy spilu)      solve/picard.py:271-417
+  UpwindOperator(weighted=True, mode="kernel"|"blend"), compute_face_normals
+                                                      kernels/upwind.py:128-454, :744-819
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -187,9 +189,58 @@ def make_picard(name, mesh, m_inf):
           f"|R|={res['residual_history'][-1]:.2e}")
 
 
+# The weighted upwind modes (kernels/upwind.py:128-454): outward face
+# normals, the BFS neighbourhoods, and rho_tilde / nu / monitors of the
+# "kernel" (streamline-Gaussian) and "blend" (face-ring) operators, with the
+# default parameters and one other set.
+WEIGHTED_PARAMS = {
+    "default": dict(p_weight=3.0, reach_frac=1.0, reach_gain_max=4.0, nbr_depth=3,
+                    sigma_s_frac=0.35, sigma_p_frac=0.35),
+    "alt": dict(p_weight=2.0, reach_frac=0.8, reach_gain_max=3.0, nbr_depth=2,
+                sigma_s_frac=0.5, sigma_p_frac=0.25),
+}
+
+
+def make_weighted(jac, upw_mod, isen, name, mesh, states):
+    op = jac.PicardOperator(mesh.nodes, mesh.elements)
+    arrays = {"mesh/nodes": mesh.nodes, "mesh/elements": mesh.elements}
+    fnorm = np.empty((len(mesh.elements), 4, 3), dtype=np.float64)
+    upw_mod.compute_face_normals(np.ascontiguousarray(mesh.nodes, dtype=np.float64),
+                                 np.ascontiguousarray(mesh.elements), fnorm)
+    arrays["mesh/face_normals"] = fnorm
+    for pname, prm in WEIGHTED_PARAMS.items():
+        for mode in ("kernel", "blend"):
+            upw = upw_mod.UpwindOperator(mesh.nodes, mesh.elements, weighted=True, mode=mode,
+                                         **prm)
+            if mode == "kernel":
+                arrays[f"{pname}/nb_off"] = upw._nb_off.astype(np.int64)
+                arrays[f"{pname}/nb_idx"] = upw._nb_idx.astype(np.int32)
+            for label, (phi, m_inf) in states.items():
+                grad, q2 = op.velocities(phi)
+                grad, q2 = grad.copy(), q2.copy()
+                q2l = isen.limit_q2_field(q2, m_inf, M_CAP, GAMMA)
+                rho = isen.density_field(q2l, m_inf, GAMMA)
+                rt = upw.rho_tilde(grad, q2l, rho, m_inf, UPWIND_C, M_CRIT, GAMMA, RHO_FLOOR).copy()
+                key = f"{pname}/{mode}/{label}"
+                arrays[f"{key}/rho_tilde"] = rt
+                arrays[f"{key}/nu"] = upw.nu.copy()
+                arrays[f"{key}/nu_max"] = np.float64(upw.nu_max)
+                arrays[f"{key}/n_supersonic"] = np.int64(upw.n_supersonic)
+                arrays[f"{key}/n_floored"] = np.int64(upw.n_floored)
+                if pname == "default" and mode == "kernel":
+                    arrays[f"state/{label}/phi"] = phi
+                    arrays[f"state/{label}/m_inf"] = np.float64(m_inf)
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
+    if "--weighted-only" in sys.argv:
+        _weighted(jac, upw_mod, isen)
+        return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
     s_states = {
@@ -209,6 +260,20 @@ def main():
     }
     make_case(jac, upw_mod, isen, "c1_bump", c1, c1_states, full=False)
     make_picard("c1_picard", c1, 0.5)
+    _weighted(jac, upw_mod, isen)
+
+
+def _weighted(jac, upw_mod, isen):
+    small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
+    w_states = {
+        "freestream_m05": (small.freestream(), 0.5),
+        "seed0_m085": (seeded_state(small, 0), 0.85),
+        "accelerating_m08": (pocket_state(small, "accelerating"), 0.8),
+        "shockpoint_m08": (pocket_state(small, "shockpoint"), 0.8),
+        "mixed_m08": (pocket_state(small, "mixed"), 0.8),
+        "supersonic_m08": (1.3 * small.freestream(), 0.8),
+    }
+    make_weighted(jac, upw_mod, isen, "weighted_upwind", small, w_states)
 
 
 if __name__ == "__main__":

@@ -95,6 +95,13 @@ SIGNATURES = {
     "up3d_residual_vjp": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_transpose": (_int, [_p, _p, _p, _p]),
     "up3d_residual_jacobian_batched": (_int, [_p, _p, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_face_normals": (_int, [_p, _p, _p]),
+    "up3d_mesh_neighborhoods": (_int, [_p, _int, ctypes.POINTER(_p), ctypes.POINTER(_p),
+                                       ctypes.POINTER(_i64), _p]),
+    "up3d_face_neighborhoods": (_int, [_p, _i64, _int, _p, _p, ctypes.POINTER(_i64), _p]),
+    "up3d_rho_tilde_kernel": (_int, [_p, _p, _p, _p, ctypes.POINTER(Flow), _int, _d, _d, _d, _p, _p,
+                                     _p, _p]),
+    "up3d_rho_tilde_blend": (_int, [_p, _p, _p, _p, ctypes.POINTER(Flow), _d, _d, _d, _p, _p, _p, _p]),
     "up3d_mesh_set_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
     "up3d_mesh_get_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
     "up3d_autotune": (_int, [_p, _p, ctypes.POINTER(Flow), _int, ctypes.POINTER(Tuning), _p]),

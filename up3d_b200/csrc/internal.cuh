@@ -114,6 +114,12 @@ struct up3d_mesh {
     int32_t n_sms = 148;                       // multiprocessors of the mesh's device
     up3d_tuning tune = {0, 512, 8, 0, 0.0, 0.0};  // launch shapes of the fused passes
     int32_t batch_cases = 0;                   // cases of the flow table in flows_ws (0 = none)
+    // face-hop neighbourhoods of the weighted "kernel" upwind mode (built on
+    // request; nb_depth 0 = none)
+    up3d::DBuf<int64_t> nb_off;  // (E+1)
+    up3d::DBuf<int32_t> nb_idx;  // (nb_total) ascending per element
+    int32_t nb_depth = 0;
+    int64_t nb_total = 0;
     up3d_flow batch_flow0 = {};                // its case 0
 
     // geometry (device)

@@ -576,6 +576,7 @@ int up3d_mesh_set_face_neighbors(up3d_mesh* m, const int32_t* in, up3d_stream st
         DeviceGuard g(m->device);
         UP3D_CUDA(cudaMemcpyAsync(m->fnbr.get(), in, sizeof(int4) * m->E, cudaMemcpyDeviceToDevice, S(stream)));
         refresh_disp(m, S(stream));
+        m->nb_depth = 0;  // the neighbourhoods follow the face neighbours
     });
 }
 
