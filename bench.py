@@ -63,6 +63,8 @@ def parse():
                         "the full batched configuration is 48:20x6x5:200x60x50:0.5:0.85")
     p.add_argument("--weighted", default="200x60x50:0.8",
                    help="mesh:mach of the weighted upwind timing ('' to skip)")
+    p.add_argument("--wake", default="200x60x50",
+                   help="channel mesh of the wake-elimination timing ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -360,6 +362,62 @@ def weighted_timing(spec):
     return out
 
 
+def wake_timing(spec):
+    """The wake master-slave elimination (constraints/wake.py:59-97) on a
+    plane sheet cut into the channel (the sheet at mid-height over the
+    downstream half, one station per spanwise line): A_red = T^T A T and
+    the Gamma columns H for a matrix on the cut mesh's P1 pattern.  Device
+    time per reduction (CUDA events, A resident), the host symbolic phase
+    once per pattern, and the oracle's scipy reduction on the host."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200 import _lib as L
+    from up3d_b200.constraints.wake import WakeConstraint
+    from up3d_b200.mesh.device import DeviceCSR, DeviceMesh
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.mesh.wake_cut import cut_channel_sheet
+    shape = tuple(int(v) for v in spec.split("x"))
+    cut = cut_channel_sheet(bump_channel(*shape, amplitude=AMPLITUDE, seed=0))
+    dm = DeviceMesh(cut.nodes, cut.elements)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = DeviceCSR(dm.indptr, dm.indices, torch.rand(dm.nnz, dtype=torch.float64, device="cuda", generator=g),
+                  (dm.n_nodes, dm.n_nodes))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    con = WakeConstraint(A, cut.wc)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    plan = con._plan
+    red = torch.empty(plan.nnz_red, dtype=torch.float64, device="cuda")
+    h = torch.empty(max(plan.nnz_h, 1), dtype=torch.float64, device="cuda")
+
+    def once():
+        L.call("up3d_wake_reduce", plan.handle, A.data.data_ptr(), red.data_ptr(), h.data_ptr(), L.stream_ptr())
+    for _ in range(3):
+        once()
+    reps = 50
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        once()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    A_h = A.to_scipy()
+    t0 = time.perf_counter()
+    ref = O.WakeConstraint(A_h, cut.wc)
+    cpu_s = time.perf_counter() - t0
+    err = float(np.abs(red.cpu().numpy() - ref.A_reduced.data).max() / np.abs(ref.A_reduced.data).max())
+    bytes_moved = 8 * plan.nnz_a + 8 * plan.nnz_red + 16 * plan.nnz_red + 8 * plan.nnz_h
+    return {"mesh": spec, "n_cut": int(dm.n_nodes), "n_red": int(plan.n_red),
+            "n_slaves": int(len(cut.wc.slave_nodes)), "n_stations": int(cut.wc.n_stations),
+            "nnz_a": int(plan.nnz_a), "nnz_red": int(plan.nnz_red), "nnz_h": int(plan.nnz_h),
+            "ms_per_reduce": round(ms, 4), "gbs": round(bytes_moved / (ms * 1e-3) / 1e9, 1),
+            "symbolic_s": round(setup_s, 3), "cpu_oracle_s": round(cpu_s, 3),
+            "max_rel_err_vs_oracle": err}
+
+
 def batched_timing(spec, seed=0):
     """Many cases in one launch: meshes of log-uniform size between the
     smallest and largest box, M_inf ~ U[mach_lo, mach_hi], bump amplitude ~
@@ -588,6 +646,7 @@ def run_ours(args):
     adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
     batched = batched_timing(args.batched) if args.batched else None
     weighted = weighted_timing(args.weighted) if args.weighted else None
+    wake = wake_timing(args.wake) if args.wake else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -642,6 +701,7 @@ def run_ours(args):
             "adjoint": adjoint,
             "batched": batched,
             "weighted_upwind": weighted,
+            "wake_elimination": wake,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -294,6 +294,48 @@ int up3d_rho_tilde_blend(const up3d_mesh* mesh, const double* grad, const double
                          double reach_frac, double reach_gain_max, double* nu,
                          double* rho_tilde, up3d_monitors* monitors, up3d_stream stream);
 
+/* ------------------------------------------------------ wake constraint */
+
+typedef struct up3d_wake up3d_wake; /* opaque: fold map, reduction plans */
+
+/* WakeConstraint.__init__ / reduce_operator (constraints/wake.py:32-97):
+ * the "+"-side copies of the wake-sheet nodes (slaves, ids in [n_red,
+ * n_cut)) fold onto their originals (masters, ids in [0, n_red)); for a
+ * cut-mesh operator A with the CSR pattern (a_indptr int64 n_cut + 1,
+ * a_indices int32) the plans of A_red = T^T A T and of the Gamma columns
+ * H = T^T A G (G[slave_k, station_k] = 1, n_red x n_stations) are built on
+ * the host and kept on `device`.  All inputs are HOST arrays.
+ * UP3D_ERR_VALUE when n_cut != n_red + n_dup (the reference's ValueError)
+ * or an index is out of range.  One handle serves every A of this pattern. */
+int up3d_wake_create(int64_t n_cut, int64_t n_red, int64_t n_dup, const int64_t* masters,
+                     const int64_t* slaves, const int64_t* node_station, int32_t n_stations,
+                     const int64_t* a_indptr, const int32_t* a_indices, int device,
+                     up3d_wake** out);
+int up3d_wake_destroy(up3d_wake* wake);
+int up3d_wake_info(const up3d_wake* wake, int64_t* n_red, int64_t* nnz_red, int64_t* nnz_h,
+                   int32_t* n_stations);
+/* Device views of the A_red pattern (n_red + 1, nnz_red; columns ascending)
+ * and of H's (n_red + 1, nnz_h; columns = stations ascending). */
+int up3d_wake_patterns(const up3d_wake* wake, const int32_t** red_indptr,
+                       const int32_t** red_indices, const int32_t** h_indptr,
+                       const int32_t** h_indices);
+/* Values of A_red and H (h_data may be NULL) from A's values (device, the
+ * pattern given at creation).  Each reduced entry sums, for every cut row
+ * folding onto its row (the row itself, then its slaves ascending), that
+ * row's entries folding onto its column, in stored order: the grouping of
+ * the reference's T^T (A T). */
+int up3d_wake_reduce(const up3d_wake* wake, const double* a_data, double* red_data,
+                     double* h_data, up3d_stream stream);
+/* reduced_rhs (constraints/wake.py:99-102): out = T^T b - sum_j gamma_j h_j
+ * with h_j H's station-j column (h_data from up3d_wake_reduce); b (n_cut),
+ * gamma (n_stations), out (n_red), all device. */
+int up3d_wake_reduced_rhs(const up3d_wake* wake, const double* b, const double* gamma,
+                          const double* h_data, double* out, up3d_stream stream);
+/* expand (constraints/wake.py:104-112): phi_cut (n_cut) = phi_red on the
+ * original nodes, phi_red[master] + gamma[station] on each slave. */
+int up3d_wake_expand(const up3d_wake* wake, const double* phi_red, const double* gamma,
+                     double* phi_cut, up3d_stream stream);
+
 /* ------------------------------------------------------ batched cases */
 
 /* up3d_residual_jacobian for several cases in one mesh (their meshes

@@ -465,3 +465,55 @@ def chain(op: PicardOperator, upw: UpwindOperator, phi, m_inf, u_inf=1.0,
         out.update(s_e=s_e, s_u=s_u, J=J, n_term3_active=op.n_term3_active,
                    newton_nnz=op.newton_nnz)
     return out
+
+
+class WakeConstraint:
+    """Oracle restatement of the wake master-slave elimination
+    (``constraints/wake.py:32-127``): T maps every cut-mesh node to its
+    reduced node (a slave to its master), A_red = T^T A T, H = T^T A G with
+    G the per-station slave indicators, h = H^T as a dense array."""
+
+    def __init__(self, A, wc):
+        n_cut, n_red, n_dup = A.shape[0], wc.n_nodes_orig, len(wc.slave_nodes)
+        if n_cut != n_red + n_dup:
+            raise ValueError(f"A is {n_cut}x{n_cut} but WakeCut implies {n_red} + {n_dup} nodes")
+        red = np.arange(n_cut, dtype=np.int64)
+        red[np.asarray(wc.slave_nodes, dtype=np.int64)] = np.asarray(wc.master_nodes, dtype=np.int64)
+        self.T = sp.csr_matrix((np.ones(n_cut), (np.arange(n_cut), red)), shape=(n_cut, n_red))
+        self.wc, self.n_reduced = wc, n_red
+        self.update_matrix(A)
+
+    def reduce_operator(self, A):
+        A = sp.csr_matrix(A)
+        wc = self.wc
+        G = sp.csr_matrix((np.ones(len(wc.slave_nodes)), (np.asarray(wc.slave_nodes), np.asarray(wc.node_station))),
+                          shape=(self.T.shape[0], wc.n_stations))
+        A_red = (self.T.T @ (A @ self.T)).tocsr()
+        H = (self.T.T @ (A @ G)).tocsr()
+        for M in (A_red, H):
+            M.sum_duplicates()
+            M.sort_indices()
+        return A_red, H
+
+    def update_matrix(self, A):
+        self.A_reduced, H = self.reduce_operator(A)
+        self._h = H.T.toarray()
+
+    def reduced_rhs(self, b, gamma):
+        gamma = np.atleast_1d(np.asarray(gamma, dtype=np.float64))
+        return self.T.T @ np.asarray(b, dtype=np.float64) - gamma @ self._h
+
+    def expand(self, phi_red, gamma):
+        wc = self.wc
+        phi = np.empty(self.n_reduced + len(wc.slave_nodes))
+        phi[:self.n_reduced] = phi_red
+        phi[wc.slave_nodes] = np.asarray(phi_red)[wc.master_nodes] + wc.gamma_at_nodes(gamma)
+        return phi
+
+
+def kutta_targets(phi, wc):
+    """Per-station mean of phi[upper probe] - phi[lower probe]
+    (``constraints/wake.py:196-212``)."""
+    jumps = np.asarray(phi)[wc.kutta_upper] - np.asarray(phi)[wc.kutta_lower]
+    sums = np.bincount(wc.te_station, weights=jumps, minlength=wc.n_stations)
+    return sums / np.bincount(wc.te_station, minlength=wc.n_stations)

@@ -4,7 +4,7 @@ reference (pyfp3d, pure Python + Numba) on synthetic Kuhn bump meshes.
 Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
-    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only]
+    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -23,6 +23,7 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   solve_subsonic (pyamg swapped for scipy spilu)      solve/picard.py:271-417
   UpwindOperator(weighted=True, mode="kernel"|"blend"), compute_face_normals
                                                       kernels/upwind.py:128-454, :744-819
+  WakeConstraint, kutta_targets                       constraints/wake.py:32-127, :196-212
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -235,11 +236,73 @@ def make_weighted(jac, upw_mod, isen, name, mesh, states):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+def make_wake(jac, upw_mod, isen, name):
+    """WakeConstraint (constraints/wake.py:32-127) and kutta_targets
+    (:196-212) of the reference on synthetic plane-sheet cuts of the
+    channel (up3d_b200.mesh.wake_cut.cut_channel_sheet): a Picard matrix
+    (symmetric) and a Newton Jacobian at a pocket state (Term-3 entries
+    off the P1 pattern), with one station per spanwise line and with a
+    single station."""
+    import scipy.sparse as sp
+    from pyfp3d.constraints.wake import WakeConstraint, kutta_targets
+    from up3d_b200.mesh.wake_cut import cut_channel_sheet
+    rng = np.random.default_rng(7)
+    mesh = bump_channel(10, 4, 4, amplitude=0.08, seed=1)
+    arrays = {}
+    for tag, single in (("multi", False), ("single", True)):
+        cut = cut_channel_sheet(mesh, single_station=single)
+        wc = cut.wc
+        pre = f"{tag}/"
+        arrays.update({pre + "nodes": cut.nodes, pre + "elements": cut.elements,
+                       pre + "dirichlet_nodes": cut.dirichlet_nodes})
+        op = jac.PicardOperator(cut.nodes, cut.elements)
+        rho = rng.uniform(0.5, 1.5, len(cut.elements))
+        mats = {"picard": op.assemble_matrix(rho)}
+        upw = upw_mod.UpwindOperator(cut.nodes, cut.elements, weighted=False)
+        phi0 = pocket_state(mesh, "mixed")
+        phi_cut = np.concatenate([phi0, phi0[wc.master_nodes] + 0.01 * (1 + wc.node_station)])
+        res = chain(jac, upw_mod, isen, op, upw, phi_cut, 0.8)
+        mats["newton"] = sp.csr_matrix((res["J_data"], res["J_indices"], res["J_indptr"]),
+                                       shape=(len(cut.nodes),) * 2)
+        for mname, A in mats.items():
+            A = A.tocsr()
+            con = WakeConstraint(A, wc)
+            A_red, H = con.reduce_operator(A)
+            A_red = A_red.tocsr().copy()
+            A_red.sum_duplicates()
+            A_red.sort_indices()
+            H = H.tocsr().copy()
+            H.sum_duplicates()
+            H.sort_indices()
+            b = rng.standard_normal(A.shape[0])
+            gamma = rng.standard_normal(wc.n_stations)
+            phi_red = rng.standard_normal(con.n_reduced)
+            q = f"{pre}{mname}/"
+            arrays.update({q + "A_indptr": A.indptr.astype(np.int64), q + "A_indices": A.indices.astype(np.int32),
+                           q + "A_data": A.data.copy(),
+                           q + "red_indptr": A_red.indptr.astype(np.int64),
+                           q + "red_indices": A_red.indices.astype(np.int32), q + "red_data": A_red.data,
+                           q + "H_indptr": H.indptr.astype(np.int64), q + "H_indices": H.indices.astype(np.int32),
+                           q + "H_data": H.data, q + "h_dense": con._h.copy(),
+                           q + "b": b, q + "gamma": gamma, q + "rhs": con.reduced_rhs(b, gamma),
+                           q + "phi_red": phi_red, q + "expand": con.expand(phi_red, gamma)})
+        vals = cut.nodes[cut.dirichlet_nodes, 0] * 1.1
+        dn, dv = WakeConstraint(mats["picard"].tocsr(), wc).to_reduced_dirichlet(cut.dirichlet_nodes, vals)
+        arrays.update({pre + "dir_values": vals, pre + "red_dir_nodes": dn, pre + "red_dir_values": dv,
+                       pre + "phi_cut": phi_cut, pre + "kutta": kutta_targets(phi_cut, wc)})
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
     if "--weighted-only" in sys.argv:
         _weighted(jac, upw_mod, isen)
+        return
+    if "--wake-only" in sys.argv:
+        make_wake(jac, upw_mod, isen, "wake_constraint")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -261,6 +324,7 @@ def main():
     make_case(jac, upw_mod, isen, "c1_bump", c1, c1_states, full=False)
     make_picard("c1_picard", c1, 0.5)
     _weighted(jac, upw_mod, isen)
+    make_wake(jac, upw_mod, isen, "wake_constraint")
 
 
 def _weighted(jac, upw_mod, isen):

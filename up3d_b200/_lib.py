@@ -95,6 +95,15 @@ SIGNATURES = {
     "up3d_residual_vjp": (_int, [_p, _p, ctypes.POINTER(Flow), _p, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_transpose": (_int, [_p, _p, _p, _p]),
     "up3d_residual_jacobian_batched": (_int, [_p, _p, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_wake_create": (_int, [_i64, _i64, _i64, _p, _p, _p, _i32, _p, _p, _int, ctypes.POINTER(_p)]),
+    "up3d_wake_destroy": (_int, [_p]),
+    "up3d_wake_info": (_int, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                              ctypes.POINTER(_i32)]),
+    "up3d_wake_patterns": (_int, [_p, ctypes.POINTER(_p), ctypes.POINTER(_p), ctypes.POINTER(_p),
+                                  ctypes.POINTER(_p)]),
+    "up3d_wake_reduce": (_int, [_p, _p, _p, _p, _p]),
+    "up3d_wake_reduced_rhs": (_int, [_p, _p, _p, _p, _p, _p]),
+    "up3d_wake_expand": (_int, [_p, _p, _p, _p, _p]),
     "up3d_face_normals": (_int, [_p, _p, _p]),
     "up3d_mesh_neighborhoods": (_int, [_p, _int, ctypes.POINTER(_p), ctypes.POINTER(_p),
                                        ctypes.POINTER(_i64), _p]),
