@@ -634,11 +634,20 @@ def run_ours(args):
         barrier()
         p_ms = p_start.elapsed_time(p_stop)
         p_ms = max_over_ranks([p_ms], device="cuda")[0]
+        # per-phase split of the pocket step (a separate, profiled pass)
+        n_prof = min(args.pocket_steps, 30)
+        L.profile(True)
+        for k in range(n_prof):
+            ev.evaluate(p_phis[k % 3], flow, jacobian=True, keep_state=False)
+        torch.cuda.synchronize()
+        p_prof = L.profile_read()
+        L.profile(False)
         pocket = {"families": list(fams), "steps": args.pocket_steps,
                   "value": round(dmesh.n_tets * args.pocket_steps * world / (p_ms * 1e-3) / 1e6, 3),
                   "unit": "Melem/s", "ms_per_step": round(p_ms / args.pocket_steps, 5),
                   "n_supersonic": [int(m["n_supersonic"]) for m in p_mon],
                   "n_term3_active": [int(m["n_term3_active"]) for m in p_mon],
+                  "phases_ms_per_step": {k: round(v["ms"] / n_prof, 5) for k, v in p_prof.items() if v["calls"]},
                   "n_term3_extra": [int(m["n_term3_extra"]) for m in p_mon],
                   "nu_max": [float(m["nu_max"]) for m in p_mon]}
 
