@@ -65,6 +65,8 @@ def parse():
                    help="mesh:mach of the weighted upwind timing ('' to skip)")
     p.add_argument("--wake", default="200x60x50",
                    help="channel mesh of the wake-elimination timing ('' to skip)")
+    p.add_argument("--wall", default="200x60x50",
+                   help="channel mesh of the wall-force timing ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -418,6 +420,49 @@ def wake_timing(spec):
             "max_rel_err_vs_oracle": err}
 
 
+def wall_timing(spec):
+    """Wall Cp and pressure forces (post/surface.py:309-363) on the
+    channel's lower wall at a pocket state, M0.8, two smoothing passes:
+    time per evaluation on a wall handle (CUDA events; each evaluation ends
+    with the 3-value read-back), one call through the public function, the
+    one-time owner/adjacency set-up, and the oracle's numpy evaluation on
+    the host."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.adjoint import lower_wall_faces
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    from up3d_b200.post.surface import wall_force_coefficients
+    shape = tuple(int(v) for v in spec.split("x"))
+    m = bump_channel(*shape, amplitude=AMPLITUDE, seed=0)
+    wf = lower_wall_faces(m.elements, m.shape)[:, 1:]
+    phi = torch.from_numpy(pocket_state(m, "mixed")).cuda()
+    t0 = time.perf_counter()
+    r = wall_force_coefficients(m.nodes, m.elements, wf, phi, m_inf=0.8, smooth_passes=2)
+    setup_s = time.perf_counter() - t0
+    from up3d_b200.post.surface import _wall
+    w = _wall(m.nodes, m.elements, wf)
+    reps = 50
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        w.run(phi, 1.0, 0.8, 1.4, 1.0, 2, want=("cp",))
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    t0 = time.perf_counter()
+    wall_force_coefficients(m.nodes, m.elements, wf, phi, m_inf=0.8, smooth_passes=2)
+    api_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    ref = O.wall_force_coefficients(m.nodes, m.elements, wf, phi.cpu().numpy(), m_inf=0.8, smooth_passes=2)
+    cpu_s = time.perf_counter() - t0
+    return {"mesh": spec, "n_wall_triangles": int(len(wf)), "ms_per_evaluation": round(ms, 4),
+            "ms_per_api_call": round(api_ms, 2),
+            "api_note": "the API call also looks the mesh handle up by a digest of nodes and elements",
+            "first_call_s": round(setup_s, 3), "cpu_oracle_s": round(cpu_s, 3),
+            "cl": r["cl"], "max_abs_cf_diff_vs_oracle": float(np.abs(r["cf"] - ref["cf"]).max())}
+
+
 def batched_timing(spec, seed=0):
     """Many cases in one launch: meshes of log-uniform size between the
     smallest and largest box, M_inf ~ U[mach_lo, mach_hi], bump amplitude ~
@@ -656,6 +701,7 @@ def run_ours(args):
     batched = batched_timing(args.batched) if args.batched else None
     weighted = weighted_timing(args.weighted) if args.weighted else None
     wake = wake_timing(args.wake) if args.wake else None
+    wall = wall_timing(args.wall) if args.wall else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -711,6 +757,7 @@ def run_ours(args):
             "batched": batched,
             "weighted_upwind": weighted,
             "wake_elimination": wake,
+            "wall_forces": wall,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

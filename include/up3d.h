@@ -336,6 +336,34 @@ int up3d_wake_reduced_rhs(const up3d_wake* wake, const double* b, const double* 
 int up3d_wake_expand(const up3d_wake* wake, const double* phi_red, const double* gamma,
                      double* phi_cut, up3d_stream stream);
 
+/* ------------------------------------------------------ wall post-processing */
+
+typedef struct up3d_wall up3d_wall; /* opaque: wall triangles, owners, adjacency */
+
+/* The wall triangles of `mesh` (wall_faces HOST int64 (n_w, 3), stored
+ * winding; elements HOST int32 (n_tets, 4), the mesh's connectivity): each
+ * triangle's owning tet (wall_outward_normals, post/surface.py:192-231;
+ * UP3D_ERR_VALUE unless exactly one tet owns it) and its edge neighbours
+ * (wall_triangle_adjacency, :121-144) are found here, on the host. */
+int up3d_wall_create(const up3d_mesh* mesh, const int32_t* elements, const int64_t* wall_faces,
+                     int64_t n_w, up3d_wall** out);
+int up3d_wall_destroy(up3d_wall* wall);
+
+/* wall_force_coefficients (post/surface.py:309-363): per triangle the
+ * in-plane P1 gradient of phi (triangle_tangential_gradients, :80-118),
+ * smooth_passes of the normal-gated edge-neighbour smoothing (:147-189,
+ * cos threshold 0.2), Cp by the exact isentropic law at m_inf > 0 or
+ * Bernoulli at m_inf = 0 (physics/isentropic.py:122-160), and
+ * cf = -sum Cp A n_out / s_ref into the HOST array cf (3).  phi is the
+ * device potential of the mesh; grad_out (n_w, 3, after smoothing),
+ * area_out (n_w), normal_out (n_w, 3, the stored winding's unit normal),
+ * outward_out (n_w, 3) and cp_out (n_w) are device arrays, each may be
+ * NULL.  Synchronises the stream. */
+int up3d_wall_forces(up3d_wall* wall, const up3d_mesh* mesh, const double* phi, double u_inf,
+                     double m_inf, double gamma, double s_ref, int smooth_passes, double* grad_out,
+                     double* area_out, double* normal_out, double* outward_out, double* cp_out,
+                     double* cf, up3d_stream stream);
+
 /* ------------------------------------------------------ batched cases */
 
 /* up3d_residual_jacobian for several cases in one mesh (their meshes

@@ -517,3 +517,116 @@ def kutta_targets(phi, wc):
     jumps = np.asarray(phi)[wc.kutta_upper] - np.asarray(phi)[wc.kutta_lower]
     sums = np.bincount(wc.te_station, weights=jumps, minlength=wc.n_stations)
     return sums / np.bincount(wc.te_station, minlength=wc.n_stations)
+
+
+# ---------------------------------------------------------------- wall post
+# post/surface.py:80-363, restated with numpy (the per-triangle arithmetic
+# in the reference's order).
+
+def _cross(a, b):
+    return np.stack([a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1],
+                     a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2],
+                     a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]], axis=1)
+
+
+def _dot(a, b):
+    return (a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1]) + a[:, 2] * b[:, 2]
+
+
+def wall_tri_gradients(nodes, wall_faces, phi):
+    """In-plane P1 gradient, area and stored-winding unit normal of each wall
+    triangle (post/surface.py:80-118)."""
+    wf = np.asarray(wall_faces, dtype=np.int64)
+    p0, p1, p2 = nodes[wf[:, 0]], nodes[wf[:, 1]], nodes[wf[:, 2]]
+    ed1, ed2 = p1 - p0, p2 - p0
+    av = _cross(ed1, ed2)
+    ta = np.sqrt(_dot(av, av))
+    tn = av / ta[:, None]
+    e1 = ed1 / np.sqrt(_dot(ed1, ed1))[:, None]
+    e2 = _cross(tn, e1)
+    u1, v1, u2, v2 = _dot(ed1, e1), _dot(ed1, e2), _dot(ed2, e1), _dot(ed2, e2)
+    phi = np.asarray(phi)
+    df1, df2 = phi[wf[:, 1]] - phi[wf[:, 0]], phi[wf[:, 2]] - phi[wf[:, 0]]
+    det = u1 * v2 - v1 * u2
+    du = (v2 * df1 - v1 * df2) / det
+    dv = (-u2 * df1 + u1 * df2) / det
+    return du[:, None] * e1 + dv[:, None] * e2, 0.5 * ta, tn
+
+
+def wall_owners(elements, wall_faces):
+    """The one tet owning each wall triangle (ValueError otherwise)."""
+    el = np.asarray(elements, dtype=np.int64)
+    faces = np.concatenate([el[:, [1, 2, 3]], el[:, [0, 2, 3]], el[:, [0, 1, 3]], el[:, [0, 1, 2]]])
+    faces.sort(axis=1)
+    owner_of = {}
+    for i, f in enumerate(map(tuple, faces)):
+        owner_of.setdefault(f, []).append(i % len(el))
+    out = []
+    for f in map(tuple, np.sort(np.asarray(wall_faces, dtype=np.int64), axis=1)):
+        own = owner_of.get(f, [])
+        if len(own) != 1:
+            raise ValueError("wall face not owned by exactly one tet")
+        out.append(own[0])
+    return np.array(out, dtype=np.int64)
+
+
+def wall_outward_normals(nodes, elements, wall_faces):
+    """Unit normals pointing toward the owning tet (post/surface.py:192-231)."""
+    wf = np.asarray(wall_faces, dtype=np.int64)
+    owner = wall_owners(elements, wf)
+    _, _, n = wall_tri_gradients(nodes, wf, np.zeros(len(nodes)))
+    fc = ((nodes[wf[:, 0]] + nodes[wf[:, 1]]) + nodes[wf[:, 2]]) / 3.0
+    el = np.asarray(elements, dtype=np.int64)[owner]
+    oc = (((nodes[el[:, 0]] + nodes[el[:, 1]]) + nodes[el[:, 2]]) + nodes[el[:, 3]]) / 4.0
+    n = n.copy()
+    n[_dot(n, oc - fc) < 0] *= -1.0
+    return n
+
+
+def wall_adjacency(wall_faces):
+    """Edge neighbour of each triangle across edges (0,1), (1,2), (2,0), -1
+    on a boundary edge or an edge of more than two triangles
+    (post/surface.py:121-144)."""
+    wf = np.asarray(wall_faces, dtype=np.int64)
+    adj = np.full((len(wf), 3), -1, dtype=np.int64)
+    occ = {}
+    for t in range(len(wf)):
+        for k, (a, b) in enumerate(((0, 1), (1, 2), (2, 0))):
+            va, vb = wf[t, a], wf[t, b]
+            occ.setdefault((min(va, vb), max(va, vb)), []).append((t, k))
+    for v in occ.values():
+        if len(v) == 2:
+            (t0, k0), (t1, k1) = v
+            adj[t0, k0], adj[t1, k1] = t1, t0
+    return adj
+
+
+def wall_force_coefficients(nodes, elements, wall_faces, phi, alpha_deg=0.0, u_inf=1.0, s_ref=1.0,
+                            m_inf=0.0, smooth_passes=0, gamma=GAMMA):
+    """Pressure-integrated force coefficients on the wall
+    (post/surface.py:309-363, smoothing :147-189)."""
+    g, area, _ = wall_tri_gradients(nodes, wall_faces, phi)
+    n_out = wall_outward_normals(nodes, elements, wall_faces)
+    if smooth_passes > 0:
+        adj = wall_adjacency(wall_faces)
+        for _ in range(smooth_passes):
+            acc = g * area[:, None]
+            wsum = area.copy()
+            for k in range(3):
+                nb = adj[:, k]
+                m = nb >= 0
+                m[m] = _dot(n_out[m], n_out[nb[m]]) > 0.2
+                acc[m] += g[nb[m]] * area[nb[m], None]
+                wsum[m] += area[nb[m]]
+            g = acc / wsum[:, None]
+    q2 = _dot(g, g) / u_inf ** 2
+    if m_inf > 0.0:
+        base = np.maximum(1.0 + 0.5 * (gamma - 1.0) * (m_inf * m_inf) * (1.0 - q2), 1e-10)
+        rho = base ** (1.0 / (gamma - 1.0))
+        cp = 2.0 / (gamma * m_inf ** 2) * (rho ** gamma - 1.0)
+    else:
+        cp = 1.0 - q2
+    cf = -((cp * area)[:, None] * n_out).sum(axis=0) / s_ref
+    a = np.deg2rad(alpha_deg)
+    lift, drag = np.array([-np.sin(a), np.cos(a), 0.0]), np.array([np.cos(a), np.sin(a), 0.0])
+    return {"cl": float(cf @ lift), "cd_pressure": float(cf @ drag), "cf": cf, "cp_tri": cp}

@@ -4,7 +4,7 @@ reference (pyfp3d, pure Python + Numba) on synthetic Kuhn bump meshes.
 Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
-    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only]
+    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only | --wall-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -24,6 +24,7 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   UpwindOperator(weighted=True, mode="kernel"|"blend"), compute_face_normals
                                                       kernels/upwind.py:128-454, :744-819
   WakeConstraint, kutta_targets                       constraints/wake.py:32-127, :196-212
+  wall_force_coefficients and its pieces              post/surface.py:80-363
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -295,6 +296,42 @@ def make_wake(jac, upw_mod, isen, name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+def make_wall(name):
+    """wall_force_coefficients and its pieces (post/surface.py:80-363) of the
+    reference on the channel's lower wall: per-triangle tangential gradient,
+    area and outward normal, edge adjacency, per-triangle Cp and the force
+    coefficients, at incompressible and compressible Mach numbers, two
+    incidences and with / without gradient smoothing."""
+    import pyfp3d.post.surface as surf
+    from up3d_b200.adjoint import lower_wall_faces
+    mesh = bump_channel(12, 5, 4, amplitude=0.08, seed=2)
+    wf = lower_wall_faces(mesh.elements, mesh.shape)[:, 1:]
+    arrays = {"nodes": mesh.nodes, "elements": mesh.elements, "wall_faces": wf}
+    g, area, tn = surf.triangle_tangential_gradients(mesh.nodes, wf, mesh.freestream())
+    arrays.update(tri_normal=tn, area=area,
+                  out_normal=surf.wall_outward_normals(mesh.nodes, mesh.elements, wf),
+                  adjacency=surf.wall_triangle_adjacency(wf))
+    cases = {"seed_m05": (seeded_state(mesh, 1), 0.5), "mixed_m08": (pocket_state(mesh, "mixed"), 0.8),
+             "seed_m0": (seeded_state(mesh, 2), 0.0)}
+    for label, (phi, m) in cases.items():
+        g, _, _ = surf.triangle_tangential_gradients(mesh.nodes, wf, phi)
+        arrays[f"{label}/phi"] = phi
+        arrays[f"{label}/m_inf"] = np.float64(m)
+        arrays[f"{label}/grad"] = g
+        for alpha in (0.0, 4.0):
+            for sp_ in (0, 2):
+                r = surf.wall_force_coefficients(mesh.nodes, mesh.elements, wf, phi, alpha_deg=alpha,
+                                                 u_inf=1.0, s_ref=2.5, m_inf=m, smooth_passes=sp_)
+                q = f"{label}/a{int(alpha)}_s{sp_}/"
+                arrays[q + "cl"] = np.float64(r["cl"])
+                arrays[q + "cd"] = np.float64(r["cd_pressure"])
+                arrays[q + "cf"] = np.asarray(r["cf"])
+                arrays[q + "cp_tri"] = np.asarray(r["cp_tri"])
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -303,6 +340,9 @@ def main():
         return
     if "--wake-only" in sys.argv:
         make_wake(jac, upw_mod, isen, "wake_constraint")
+        return
+    if "--wall-only" in sys.argv:
+        make_wall("wall_forces")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -325,6 +365,7 @@ def main():
     make_picard("c1_picard", c1, 0.5)
     _weighted(jac, upw_mod, isen)
     make_wake(jac, upw_mod, isen, "wake_constraint")
+    make_wall("wall_forces")
 
 
 def _weighted(jac, upw_mod, isen):

@@ -104,6 +104,9 @@ SIGNATURES = {
     "up3d_wake_reduce": (_int, [_p, _p, _p, _p, _p]),
     "up3d_wake_reduced_rhs": (_int, [_p, _p, _p, _p, _p, _p]),
     "up3d_wake_expand": (_int, [_p, _p, _p, _p, _p]),
+    "up3d_wall_create": (_int, [_p, _p, _p, _i64, ctypes.POINTER(_p)]),
+    "up3d_wall_destroy": (_int, [_p]),
+    "up3d_wall_forces": (_int, [_p, _p, _p, _d, _d, _d, _d, _int, _p, _p, _p, _p, _p, _p, _p]),
     "up3d_face_normals": (_int, [_p, _p, _p]),
     "up3d_mesh_neighborhoods": (_int, [_p, _int, ctypes.POINTER(_p), ctypes.POINTER(_p),
                                        ctypes.POINTER(_i64), _p]),
