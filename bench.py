@@ -65,7 +65,7 @@ def parse():
                    help="mesh:mach of the weighted upwind timing ('' to skip)")
     p.add_argument("--wake", default="200x60x50",
                    help="channel mesh of the wake-elimination timing ('' to skip)")
-    p.add_argument("--wall", default="200x60x50",
+    p.add_argument("--wall", default="100x30x25",
                    help="channel mesh of the wall-force timing ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
