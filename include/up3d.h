@@ -364,6 +364,26 @@ int up3d_wall_forces(up3d_wall* wall, const up3d_mesh* mesh, const double* phi, 
                      double* area_out, double* normal_out, double* outward_out, double* cp_out,
                      double* cf, up3d_stream stream);
 
+/* ------------------------------------------------------ level-set sides */
+
+/* newton_terms23_side_coo (kernels/cut_assembly.py:401-488): one side's
+ * Newton Terms 2 and 3 as COO triplets on extended DOFs.  keep (uint8 E),
+ * dofvec / readvec (int64 E x 4: where the element's residual lands / which
+ * DOFs its side field reads; readvec NULL = dofvec), grad / grad_row
+ * (E x 3: the read and the scatter field's gradients; grad_row NULL =
+ * grad), lim_mask (f64 E, 1 or 0), s_e, s_u (f64 E), upstream (int64 E),
+ * all device.  Term-2 blocks of the kept elements with s_e lim != 0, in
+ * ascending element order, then Term-3 blocks of those with
+ * s_u lim[upstream] != 0, 16 triplets per block (a-major).  With rows ==
+ * NULL only *count (host) is set; then rows, cols (int64) and data (f64)
+ * of `capacity` >= *count entries are filled.  UP3D_ERR_VALUE for an
+ * upstream index outside [0, E).  Synchronises the stream. */
+int up3d_terms23_side_coo(const up3d_mesh* mesh, const uint8_t* keep, const int64_t* dofvec,
+                          const int64_t* readvec, const double* grad, const double* grad_row,
+                          const double* lim_mask, const double* s_e, const double* s_u,
+                          const int64_t* upstream, double u_inf, int64_t* rows, int64_t* cols,
+                          double* data, int64_t capacity, int64_t* count, up3d_stream stream);
+
 /* ------------------------------------------------------ batched cases */
 
 /* up3d_residual_jacobian for several cases in one mesh (their meshes

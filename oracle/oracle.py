@@ -630,3 +630,36 @@ def wall_force_coefficients(nodes, elements, wall_faces, phi, alpha_deg=0.0, u_i
     a = np.deg2rad(alpha_deg)
     lift, drag = np.array([-np.sin(a), np.cos(a), 0.0]), np.array([np.cos(a), np.sin(a), 0.0])
     return {"cl": float(cf @ lift), "cd_pressure": float(cf @ drag), "cf": cf, "cp_tri": cp}
+
+
+def newton_terms23_side_coo(B, V, side, u_inf=1.0):
+    """Per-side Newton Terms 2 and 3 as COO triplets on extended DOFs
+    (kernels/cut_assembly.py:401-488): rows from the residual DOF map,
+    columns from the read map; Term-2 blocks of the kept elements with
+    s_e != 0 (ascending), then Term-3 blocks of those with s_u != 0."""
+    B = np.asarray(B).reshape(-1, 4, 3)
+    keep, dof = np.asarray(side["keep"]), np.asarray(side["dofvec"], dtype=np.int64)
+    read = np.asarray(side.get("readvec", dof), dtype=np.int64)
+    grad = np.asarray(side["grad"])
+    grad_row = np.asarray(side.get("grad_row", grad))
+    lim = np.asarray(side["lim_mask"])
+    inv_u2 = 1.0 / (u_inf * u_inf)
+    gbr = ((grad_row[:, None, 0] * B[:, :, 0] + grad_row[:, None, 1] * B[:, :, 1])
+           + grad_row[:, None, 2] * B[:, :, 2])
+    gb = (grad[:, None, 0] * B[:, :, 0] + grad[:, None, 1] * B[:, :, 1]) + grad[:, None, 2] * B[:, :, 2]
+    up = np.asarray(side["upstream"], dtype=np.int64)
+    s_e = np.asarray(side["s_e"]) * lim
+    s_u = np.asarray(side["s_u"]) * lim[up]
+    rows, cols, data = [], [], []
+    e2 = np.flatnonzero(keep & (s_e != 0.0))
+    w2 = (2.0 * inv_u2) * s_e[e2] * V[e2]
+    rows.append(np.repeat(dof[e2], 4, axis=1).reshape(-1))
+    cols.append(np.tile(read[e2], (1, 4)).reshape(-1))
+    data.append((w2[:, None, None] * (gbr[e2][:, :, None] * gb[e2][:, None, :])).reshape(-1))
+    e3 = np.flatnonzero(keep & (s_u != 0.0))
+    u3 = up[e3]
+    w3 = (2.0 * inv_u2) * s_u[e3] * V[e3]
+    rows.append(np.repeat(dof[e3], 4, axis=1).reshape(-1))
+    cols.append(np.tile(read[u3], (1, 4)).reshape(-1))
+    data.append((w3[:, None, None] * (gbr[e3][:, :, None] * gb[u3][:, None, :])).reshape(-1))
+    return np.concatenate(rows), np.concatenate(cols), np.concatenate(data)

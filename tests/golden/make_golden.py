@@ -4,7 +4,8 @@ reference (pyfp3d, pure Python + Numba) on synthetic Kuhn bump meshes.
 Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
-    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only | --wall-only]
+    python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only | --wall-only |
+                                                      --sides-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -25,6 +26,8 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
                                                       kernels/upwind.py:128-454, :744-819
   WakeConstraint, kutta_targets                       constraints/wake.py:32-127, :196-212
   wall_force_coefficients and its pieces              post/surface.py:80-363
+  per-side walks, newton_terms23_side_coo             wake/multivalued.py:456-466,
+                                                      kernels/cut_assembly.py:401-488
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -332,6 +335,55 @@ def make_wall(name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+def make_sides(jac, upw_mod, isen, name):
+    """The level-set path's per-side pieces: the upwind walk and rho~ on a
+    face graph restricted to one side's elements (the masking of
+    wake/multivalued.py:456-466) and newton_terms23_side_coo
+    (kernels/cut_assembly.py:401-488) on a synthetic side record
+    (keep mask, residual and read DOF maps with auxiliary DOFs past the
+    nodes, row and column gradients, limiter mask, sensitivities, upstream
+    elements)."""
+    from pyfp3d.kernels.cut_assembly import newton_terms23_side_coo
+    rng = np.random.default_rng(11)
+    mesh = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
+    op = jac.PicardOperator(mesh.nodes, mesh.elements)
+    phi = pocket_state(mesh, "mixed")
+    grad, q2 = op.velocities(phi)
+    grad, q2 = grad.copy(), q2.copy()
+    q2l = isen.limit_q2_field(q2, 0.8, M_CAP, GAMMA)
+    rho = isen.density_field(q2l, 0.8, GAMMA)
+    cz = mesh.nodes[mesh.elements].mean(axis=1)[:, 2]
+    arrays = {"nodes": mesh.nodes, "elements": mesh.elements, "phi": phi}
+    for label, keep in (("upper", cz > 0.5), ("lower", cz <= 0.5)):
+        upw = upw_mod.UpwindOperator(mesh.nodes, mesh.elements)
+        fn = upw.face_neighbors.copy()
+        nb_ok = np.where(fn >= 0, keep[np.clip(fn, 0, None)], False)
+        fn[~(nb_ok & keep[:, None])] = -1
+        upw.face_neighbors = np.ascontiguousarray(fn)
+        rt = upw.rho_tilde(grad, q2l, rho, 0.8, UPWIND_C, M_CRIT, GAMMA, RHO_FLOOR).copy()
+        arrays.update({f"{label}/keep": keep, f"{label}/fn": fn, f"{label}/upstream": upw._upstream.copy(),
+                       f"{label}/rho_tilde": rt, f"{label}/nu": upw.nu.copy()})
+        if label == "upper":
+            up_walk = upw._upstream.copy()
+    E, N = len(mesh.elements), len(mesh.nodes)
+    el = mesh.elements.astype(np.int64)
+    aux = rng.random(E) < 0.3
+    dofvec = np.where(aux[:, None] & (rng.random((E, 4)) < 0.5), N + (el % 37), el)
+    readvec = np.where(rng.random((E, 4)) < 0.15, N + (el % 23), dofvec)
+    grad_row = grad + np.where(rng.random(E)[:, None] < 0.2, 1e-3 * rng.standard_normal((E, 3)), 0.0)
+    s_e = np.where(rng.random(E) < 0.6, rng.standard_normal(E), 0.0)
+    s_u = np.where(rng.random(E) < 0.5, rng.standard_normal(E), 0.0)
+    side = {"keep": rng.random(E) < 0.7, "dofvec": dofvec, "readvec": readvec, "grad": grad,
+            "grad_row": grad_row, "lim_mask": (rng.random(E) < 0.9).astype(np.float64), "s_e": s_e,
+            "s_u": s_u, "upstream": up_walk}
+    rows, cols, data = newton_terms23_side_coo(op, side, u_inf=1.3)
+    arrays.update({f"t23/{k}": np.asarray(v) for k, v in side.items()})
+    arrays.update({"t23/rows": rows, "t23/cols": cols, "t23/data": data})
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB), {len(data)} triplets")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -343,6 +395,9 @@ def main():
         return
     if "--wall-only" in sys.argv:
         make_wall("wall_forces")
+        return
+    if "--sides-only" in sys.argv:
+        make_sides(jac, upw_mod, isen, "side_terms")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -366,6 +421,7 @@ def main():
     _weighted(jac, upw_mod, isen)
     make_wake(jac, upw_mod, isen, "wake_constraint")
     make_wall("wall_forces")
+    make_sides(jac, upw_mod, isen, "side_terms")
 
 
 def _weighted(jac, upw_mod, isen):

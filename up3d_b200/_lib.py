@@ -104,6 +104,8 @@ SIGNATURES = {
     "up3d_wake_reduce": (_int, [_p, _p, _p, _p, _p]),
     "up3d_wake_reduced_rhs": (_int, [_p, _p, _p, _p, _p, _p]),
     "up3d_wake_expand": (_int, [_p, _p, _p, _p, _p]),
+    "up3d_terms23_side_coo": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _d, _p, _p, _p, _i64,
+                                     ctypes.POINTER(_i64), _p]),
     "up3d_wall_create": (_int, [_p, _p, _p, _i64, ctypes.POINTER(_p)]),
     "up3d_wall_destroy": (_int, [_p]),
     "up3d_wall_forces": (_int, [_p, _p, _p, _d, _d, _d, _d, _int, _p, _p, _p, _p, _p, _p, _p]),
