@@ -55,7 +55,7 @@ def parse():
                    help="node/element numbering of the device mesh")
     p.add_argument("--tune", default="auto",
                    help="launch shapes: 'auto' (autotuner), 'default', or "
-                        "'persistent,threads_per_sm,row_lanes'")
+                        "'persistent,threads_per_sm,row_lanes[,row_plan8]'")
     p.add_argument("--adjoint", default="100x30x25:0.05:0.80",
                    help="mesh:bump:Mach of the adjoint shape-gradient case ('' to skip)")
     p.add_argument("--batched", default="12:20x6x5:100x30x25:0.5:0.75",
@@ -529,7 +529,7 @@ def batched_timing(spec, seed=0):
     def fresh():
         b = BatchedChannels(meshes, ordering=batch.ordering)
         b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_threads_per_sm"],
-                                shapes_tuned["row_lanes"])
+                                shapes_tuned["row_lanes"], shapes_tuned["row_plan8"])
         return b
     res_b = None
     for _ in range(2):

@@ -424,18 +424,22 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
  *                    blocks, up to 102) or 768 (256-thread blocks, up to 80,
  *                    spilling to L1)
  *   row_lanes        lanes per row of the row gather: 4, 8, 16 or 32
+ *   row_plan8        1: the row gather reads each upper slot's
+ *                    contributors from a fixed-width record (built at mesh
+ *                    set-up when no slot has more than 8); 0: from the
+ *                    offset list.  Ignored when the mesh has no records.
  *   elem_us, row_us  autotune output: median time per launch of the
  *                    chosen shapes (0 when set by hand) */
 typedef struct {
     int32_t elem_persistent;
     int32_t elem_threads_per_sm;
     int32_t row_lanes;
-    int32_t reserved; /* 0 */
+    int32_t row_plan8;
     double elem_us;
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 512, 8}.  UP3D_ERR_VALUE for a shape outside the lists. */
+/* Default: {0, 512, 8, 0}.  UP3D_ERR_VALUE for a shape outside the lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 

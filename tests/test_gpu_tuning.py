@@ -10,8 +10,9 @@ from conftest import has_cuda, rel_err
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not has_cuda(), reason="needs a CUDA device")]
 
-# (persistent, resident threads per SM, lanes per row)
-SHAPES = [(0, 512, 4), (0, 768, 8), (1, 512, 8), (1, 768, 16), (1, 640, 32), (0, 640, 4), (1, 640, 16)]
+# (persistent, resident threads per SM, lanes per row, fixed-width gather records)
+SHAPES = [(0, 512, 4, 0), (0, 768, 8, 1), (1, 512, 8, 0), (1, 768, 16, 1), (1, 640, 32, 0), (0, 640, 4, 1),
+          (1, 640, 16, 1), (1, 640, 8, 1)]
 
 
 def _setup():
@@ -69,7 +70,7 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
     t = dm.autotune(phi, flow, reps=3)
     assert t == dm.tuning()
     assert (t["elem_persistent"], t["elem_threads_per_sm"]) in {(0, 512), (1, 512), (1, 640), (0, 768), (1, 768)}
-    assert t["row_lanes"] in (4, 8, 16, 32)
+    assert t["row_lanes"] in (4, 8, 16, 32) and t["row_plan8"] in (0, 1)
     assert t["elem_us"] > 0 and t["row_us"] > 0
     R = ev.evaluate(phi, flow, jacobian=True).clone()
     assert torch.equal(R, R0)
@@ -81,7 +82,8 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
 
 def test_bad_shapes_are_refused():
     _, _, dm, _, _ = _setup()
-    for bad in [(2, 512, 8), (-1, 512, 8), (0, 256, 8), (0, 1024, 8), (0, 512, 2), (0, 512, 12), (0, 512, 64)]:
+    for bad in [(2, 512, 8), (-1, 512, 8), (0, 256, 8), (0, 1024, 8), (0, 512, 2), (0, 512, 12), (0, 512, 64),
+                (0, 512, 8, 2), (0, 512, 8, -1)]:
         with pytest.raises(ValueError):
             dm.set_tuning(*bad)
     assert dm.tuning()["row_lanes"] == 8

@@ -49,10 +49,10 @@ class MeshInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """up3d_tuning: launch shapes of the fused evaluation's two passes."""
     _fields_ = [("elem_persistent", _i32), ("elem_threads_per_sm", _i32), ("row_lanes", _i32),
-                ("reserved", _i32), ("elem_us", _d), ("row_us", _d)]
+                ("row_plan8", _i32), ("elem_us", _d), ("row_us", _d)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 MONITOR_BYTES = ctypes.sizeof(Monitors)

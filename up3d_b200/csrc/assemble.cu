@@ -141,12 +141,16 @@ __device__ __forceinline__ void slot_sum(int deg, int sub, Load&& load, double& 
 //   each slot sums its plan's contributors in ascending element order) and
 //   is written to (n, m) and, the element matrices being symmetric and row m
 //   listing the same elements in the same order, to its transposed slot.
-template <int WARPS, int LPR>
+// P8: the upper slots read their contributors from the fixed-width records
+// (plan8, one 32-byte record per slot found from up_off) instead of
+// plan_off -> plan: one dependent load less, the same order and bits.
+template <int WARPS, int LPR, bool P8>
 __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     k_row_gather(int64_t N, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
                  const int32_t* __restrict__ indptr, const int32_t* __restrict__ plan_off,
                  const uint32_t* __restrict__ plan, const int32_t* __restrict__ diag,
-                 const int32_t* __restrict__ zt, const double* __restrict__ loc, double* __restrict__ R,
+                 const int32_t* __restrict__ zt, const int32_t* __restrict__ up_off,
+                 const uint32_t* __restrict__ plan8, const double* __restrict__ loc, double* __restrict__ R,
                  double* __restrict__ J) {
     static_assert(LPR >= 1 && LPR <= 32 && (LPR & (LPR - 1)) == 0, "LPR: power of two <= 32");
     constexpr int RPW = 32 / LPR;
@@ -157,13 +161,14 @@ __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
     for (int64_t base = warp * RPW; base < N; base += n_warps * RPW) {
         const int64_t n = base + lane / LPR;
         const bool valid = n < N;
-        int32_t eb = 0, deg = 0, rb = 0, L = 0, ds = -1;
+        int32_t eb = 0, deg = 0, rb = 0, L = 0, ds = -1, uo = 0;
         if (valid) {
             eb = ent_off[n];
             deg = ent_off[n + 1] - eb;
             rb = indptr[n];
             L = indptr[n + 1] - rb;
             ds = diag[n];
+            if (P8) uo = up_off[n];
         }
         double r, d;
         slot_sum<LPR>(deg, sub, [&](int k) {
@@ -171,9 +176,24 @@ __global__ void __launch_bounds__(WARPS * 32, UP3D_ROW_MINB)
             return reinterpret_cast<const double2*>(loc + (size_t)LOC_STRIDE * (x >> 2))[x & 3];
         }, r, d);
         for (int s = ds + 1 + sub; s < L; s += LPR) {
+            double v = 0.0;
+            if constexpr (P8) {
+                const uint4* rec = reinterpret_cast<const uint4*>(plan8 + (size_t)PLAN8 * (uo + (s - ds - 1)));
+                const uint4 h0 = __ldg(rec), h1 = __ldg(rec + 1);
+                const uint32_t c[PLAN8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+                double a[PLAN8];
+#pragma unroll
+                for (int k = 0; k < PLAN8; ++k)
+                    a[k] = c[k] != PLAN8_END ? loc[(size_t)LOC_STRIDE * (c[k] >> 3) + 8 + (c[k] & 7)] : 0.0;
+#pragma unroll
+                for (int k = 0; k < PLAN8; ++k)
+                    if (c[k] != PLAN8_END) v += a[k];
+                J[rb + s] = v;
+                J[zt[rb + s]] = v;
+                continue;
+            }
             int32_t p = plan_off[rb + s];
             const int32_t p1 = plan_off[rb + s + 1];
-            double v = 0.0;
             for (; p + 3 < p1; p += 4) {
                 const uint32_t c0 = plan[p], c1 = plan[p + 1], c2 = plan[p + 2], c3 = plan[p + 3];
                 const double a0 = loc[(size_t)LOC_STRIDE * (c0 >> 3) + 8 + (c0 & 7)];
@@ -656,23 +676,30 @@ void scan(up3d_mesh* m, const T* in, T* out, int64_t n, cudaStream_t s) {
 
 // ------------------------------------------------------------ launchers
 
-// Jacobian (+ residual) rows from m->loc, m->tune.row_lanes lanes per row.
-template <int LPR>
+// Jacobian (+ residual) rows from m->loc, m->tune.row_lanes lanes per row,
+// from the fixed-width contributor records when the mesh has them and the
+// tuning asks for them (row_plan8).
+template <int LPR, bool P8>
 static void launch_row_gather_lpr(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
     constexpr int rows_per_block = RG_WARPS * 32 / LPR;
     const unsigned grid = grid_for(m->N, rows_per_block, (int64_t)m->n_sms * 64);
-    k_row_gather<RG_WARPS, LPR><<<grid, RG_WARPS * 32, 0, s>>>(m->N, m->ent_off.get(), m->ent.get(),
-                                                                m->indptr.get(), m->plan_off.get(), m->plan.get(),
-                                                                m->diag.get(), m->zt.get(), m->loc.get(), R, J);
+    k_row_gather<RG_WARPS, LPR, P8><<<grid, RG_WARPS * 32, 0, s>>>(
+        m->N, m->ent_off.get(), m->ent.get(), m->indptr.get(), m->plan_off.get(), m->plan.get(), m->diag.get(),
+        m->zt.get(), m->up_off.get(), m->plan8.get(), m->loc.get(), R, J);
     UP3D_CHECK_LAUNCH();
 }
-void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
+template <bool P8>
+static void launch_row_gather_p(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
     switch (m->tune.row_lanes) {
-        case 4: launch_row_gather_lpr<4>(m, R, J, s); break;
-        case 16: launch_row_gather_lpr<16>(m, R, J, s); break;
-        case 32: launch_row_gather_lpr<32>(m, R, J, s); break;
-        default: launch_row_gather_lpr<8>(m, R, J, s); break;
+        case 4: launch_row_gather_lpr<4, P8>(m, R, J, s); break;
+        case 16: launch_row_gather_lpr<16, P8>(m, R, J, s); break;
+        case 32: launch_row_gather_lpr<32, P8>(m, R, J, s); break;
+        default: launch_row_gather_lpr<8, P8>(m, R, J, s); break;
     }
+}
+void launch_row_gather(const up3d_mesh* m, double* R, double* J, cudaStream_t s) {
+    if (m->has_plan8 && m->tune.row_plan8) launch_row_gather_p<true>(m, R, J, s);
+    else launch_row_gather_p<false>(m, R, J, s);
 }
 
 // Residual rows from m->res.
@@ -979,8 +1006,9 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
                          t->elem_threads_per_sm == 768,
                      UP3D_ERR_VALUE, "up3d_mesh_set_tuning: elem_threads_per_sm must be 512, 640 or 768");
 
+        UP3D_REQUIRE(t->row_plan8 == 0 || t->row_plan8 == 1, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: row_plan8 must be 0 or 1");
         m->tune = *t;
-        m->tune.reserved = 0;
     });
 }
 
@@ -1058,16 +1086,20 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
             // the row gather, on the local matrices the sweep left
             static const int lanes[] = {4, 8, 16, 32};
             double best_r = 0.0;
-            int best_l = -1;
-            for (int l : lanes) {
-                m->tune.row_lanes = l;
-                const double t = time_it([&] { launch_row_gather(m, R.get(), J.get(), s); });
-                if (best_l < 0 || t < best_r) {
-                    best_r = t;
-                    best_l = l;
+            int best_l = -1, best_p = 0;
+            for (int p8 = 0; p8 <= (m->has_plan8 ? 1 : 0); ++p8)
+                for (int l : lanes) {
+                    m->tune.row_lanes = l;
+                    m->tune.row_plan8 = p8;
+                    const double t = time_it([&] { launch_row_gather(m, R.get(), J.get(), s); });
+                    if (best_l < 0 || t < best_r) {
+                        best_r = t;
+                        best_l = l;
+                        best_p = p8;
+                    }
                 }
-            }
             m->tune.row_lanes = best_l;
+            m->tune.row_plan8 = best_p;
             m->tune.elem_us = best_e;
             m->tune.row_us = best_r;
         } catch (...) {

@@ -101,6 +101,8 @@ struct DBuf {
 //   RES (E, 4): R_i only (residual-only evaluations)
 //   T3V (E, 8): a_i = w3 gB_i, b_k = grad_u . B_u,k (Term-3 active elements)
 constexpr int LOC_STRIDE = 14;
+constexpr int PLAN8 = 8;
+constexpr uint32_t PLAN8_END = 0xFFFFFFFFu;
 
 struct Flow;  // physics constants of one flow (below)
 
@@ -140,6 +142,12 @@ struct up3d_mesh {
     up3d::DBuf<uint32_t> plan;    // (6E) upper-slot contributors (e << 3) | pair index
     up3d::DBuf<int32_t> diag;     // (N) slot of the diagonal within its row
     up3d::DBuf<int32_t> zt;       // (nnz) slot of the transposed entry
+    // the same upper-slot contributors in fixed-width records (PLAN8 per
+    // slot, padded with PLAN8_END), indexed by upper-slot ordinal
+    // up_off[n] + (s - diag[n] - 1); built when no slot has more
+    up3d::DBuf<int32_t> up_off;   // (N+1)
+    up3d::DBuf<uint32_t> plan8;   // (n_upper, PLAN8)
+    bool has_plan8 = false;
 
     // workspaces (device)
     up3d::DBuf<double> loc;            // (E, LOC_STRIDE) local matrices + residual

@@ -174,6 +174,37 @@ __global__ void k_plan(int64_t N, const int4* __restrict__ conn, const int32_t* 
     }
 }
 
+// Upper-slot counts per row (slots right of the diagonal) and the largest
+// contributor count of any upper slot.
+__global__ void k_upper_counts(int64_t N, const int32_t* __restrict__ indptr, const int32_t* __restrict__ diag,
+                               const int32_t* __restrict__ plan_off, int32_t* __restrict__ cnt,
+                               int32_t* __restrict__ most) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
+        const int32_t u = L - ds - 1;
+        cnt[n] = u > 0 ? u : 0;
+        int32_t mx = 0;
+        for (int32_t s = ds + 1; s < L; ++s) mx = max(mx, plan_off[rb + s + 1] - plan_off[rb + s]);
+        most[n] = mx;
+    }
+}
+
+// The fixed-width contributor records of every upper slot, in plan order.
+__global__ void k_plan8(int64_t N, const int32_t* __restrict__ indptr, const int32_t* __restrict__ diag,
+                        const int32_t* __restrict__ up_off, const int32_t* __restrict__ plan_off,
+                        const uint32_t* __restrict__ plan, uint32_t* __restrict__ plan8) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t rb = indptr[n], L = indptr[n + 1] - rb, ds = diag[n];
+        for (int32_t s = ds + 1; s < L; ++s) {
+            uint32_t* out = plan8 + (size_t)PLAN8 * (up_off[n] + (s - ds - 1));
+            const int32_t p0 = plan_off[rb + s], p1 = plan_off[rb + s + 1];
+            for (int k = 0; k < PLAN8; ++k) out[k] = p0 + k < p1 ? plan[p0 + k] : PLAN8_END;
+        }
+    }
+}
+
 // Transposed slot of every non-zero: for (n, m) at z, the position of (m, n).
 __global__ void k_transpose_slots(int64_t N, const int32_t* __restrict__ indptr,
                                   const int32_t* __restrict__ indices, int32_t* __restrict__ zt) {
@@ -453,6 +484,28 @@ static void build_mesh(up3d_mesh* m, const double* nodes, const int32_t* element
                                                      m->indptr.get(), m->indices.get(), cursor.get(),
                                                      m->plan_off.get(), m->plan.get(), m->diag.get());
         UP3D_CHECK_LAUNCH();
+        // fixed-width records when every upper slot has at most PLAN8
+        // contributors
+        DBuf<int32_t> most, ucnt;
+        most.alloc(N);
+        ucnt.alloc(N + 1);
+        m->up_off.alloc(N + 1);
+        UP3D_CUDA(cudaMemsetAsync(ucnt.get() + N, 0, sizeof(int32_t), s));
+        k_upper_counts<<<grid_for(N, 128), 128, 0, s>>>(N, m->indptr.get(), m->diag.get(), m->plan_off.get(),
+                                                       ucnt.get(), most.get());
+        UP3D_CHECK_LAUNCH();
+        cub_exclusive_scan(m, ucnt.get(), m->up_off.get(), N + 1, s);
+        int32_t n_upper = 0;
+        UP3D_CUDA(cudaMemcpyAsync(&n_upper, m->up_off.get() + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        const int32_t widest = device_max(m, most.get(), N, s);
+        m->has_plan8 = false;
+        if (widest <= PLAN8 && n_upper > 0) {
+            m->plan8.alloc((size_t)PLAN8 * n_upper);
+            k_plan8<<<grid_for(N, 128), 128, 0, s>>>(N, m->indptr.get(), m->diag.get(), m->up_off.get(),
+                                                    m->plan_off.get(), m->plan.get(), m->plan8.get());
+            UP3D_CHECK_LAUNCH();
+            m->has_plan8 = true;
+        }
     }
     // face adjacency
     m->fnbr.alloc(E);

@@ -132,9 +132,10 @@ class DeviceMesh:
         L.call("up3d_mesh_get_tuning", self.handle, ctypes.byref(t))
         return t.as_dict()
 
-    def set_tuning(self, elem_persistent: int = 0, elem_threads_per_sm: int = 512, row_lanes: int = 8) -> None:
+    def set_tuning(self, elem_persistent: int = 0, elem_threads_per_sm: int = 512, row_lanes: int = 8,
+                   row_plan8: int = 0) -> None:
         """Installs launch shapes by hand; every shape computes the same bits."""
-        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, 0, 0.0, 0.0)
+        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, 0.0, 0.0)
         L.call("up3d_mesh_set_tuning", self.handle, ctypes.byref(t))
 
     def autotune(self, phi, flow, reps: int = 5) -> dict:
