@@ -601,14 +601,18 @@ __global__ void __launch_bounds__(WARPS * 32)
     }
 }
 
-// Extras of every row, compacted in (row, column) order.
+// Extras of every row, compacted in (row, column) order: one warp per row,
+// coalesced copies.
 __global__ void k_t3_compact(int64_t N, const int32_t* __restrict__ ent_off, const int32_t* __restrict__ x_ptr,
                              const int32_t* __restrict__ xs_col, const double* __restrict__ xs_val,
                              int32_t* __restrict__ x_row, int32_t* __restrict__ x_col, double* __restrict__ x_val) {
-    GRID_STRIDE(n, N) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < N; n += n_warps) {
         const int32_t o = x_ptr[n], cnt = x_ptr[n + 1] - o;
         const int64_t src = 4 * (int64_t)ent_off[n];
-        for (int32_t j = 0; j < cnt; ++j) {
+        for (int32_t j = lane; j < cnt; j += 32) {
             x_row[o + j] = (int32_t)n;
             x_col[o + j] = xs_col[src + j];
             x_val[o + j] = xs_val[src + j];
@@ -756,7 +760,7 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
         m->x_row_c.alloc(n_extra);
         m->x_col_c.alloc(n_extra);
         m->x_val_c.alloc(n_extra);
-        k_t3_compact<<<grid_for(N, 256), 256, 0, s>>>(N, m->ent_off.get(), m->x_ptr.get(), m->x_col.get(),
+        k_t3_compact<<<grid_for(32 * N, 256, (int64_t)m->n_sms * 32), 256, 0, s>>>(N, m->ent_off.get(), m->x_ptr.get(), m->x_col.get(),
                                                       m->x_val.get(), m->x_row_c.get(), m->x_col_c.get(),
                                                       m->x_val_c.get());
         UP3D_CHECK_LAUNCH();
