@@ -2,7 +2,7 @@
 
 C1 (subsonic channel 40x10x10, M_inf 0.5): the reference ``solve_subsonic``
 converged potential (golden fixture, pyamg swapped for spilu there); the
-north-star bar is converged Cp within 1e-8.
+parity bar is converged Cp within 1e-8.
 """
 
 import numpy as np
