@@ -341,7 +341,10 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // 345-372, :435-452): gradient, limiter, density, upstream walk (or the
 // frozen selection), the upstream element's state recomputed in place, the
 // flux, its sensitivities, and the element's residual contributions and
-// local matrix (JAC) or residual contributions only.
+// local matrix (JAC) or residual contributions only.  B_e and V_e are
+// recomputed from the node coordinates (geom_B, the mesh set-up's
+// arithmetic, so the same bits) instead of streamed: the coordinates are
+// gathered for the walk anyway, and 104 bytes per element stay in HBM.
 // BATCH: several cases in one mesh (disconnected components), element e
 // taking the flow of its case, flows[case_of[e]] (an index outside
 // [0, n_cases) reads case 0: the host validates the indices, and a table
@@ -350,8 +353,7 @@ __device__ __forceinline__ void flush(MonAcc a, up3d_monitors* mon) {
 // allocation must allow.
 template <bool FROZEN, bool JAC, bool BATCH, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB)
-    k_fused_elem(const int4* __restrict__ conn, const double* __restrict__ B, const double* __restrict__ V,
-                 const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
+    k_fused_elem(const int4* __restrict__ conn, const int4* __restrict__ fn, const double* __restrict__ disp, const double4* __restrict__ X,
                  const double* __restrict__ phi, Flow F0, double u2, const int64_t* __restrict__ up_fz,
                  const int8_t* __restrict__ br_fz, int64_t E, double* __restrict__ loc, double* __restrict__ res,
                  double* __restrict__ t3v, uint8_t* __restrict__ t3flag, int32_t* __restrict__ up_out,
@@ -370,11 +372,15 @@ __global__ void __launch_bounds__(NT, MB)
         }
         const Flow& F = BATCH ? flows[ci] : F0;
         // only grad phi_e stays live through the walk; the element's own
-        // state and gB_j = grad . B_j are formed after it (B_e again: an
-        // L1/L2 hit)
-        const double* be = B + 12 * e;
-        double g[3];
-        elem_grad_rec(conn[e], be, phi, g);
+        // state and gB_j = grad . B_j are formed after it (B_e recomputed
+        // from the coordinates, L1/L2 hits)
+        const int4 ce = conn[e];
+        double g[3], Ve;
+        {
+            double bb[12];
+            geom_B(X, ce, bb, Ve);
+            grad_from_B(ce, bb, phi, g);
+        }
         // frozen (upstream, branch) per element; a negative branch keeps the
         // element live (several cases in one mesh, frozen one by one)
         const int brf = FROZEN ? (int)br_fz[e] : -1;
@@ -390,7 +396,12 @@ __global__ void __launch_bounds__(NT, MB)
         bool lim_u = lim_e;
         if (u != e) {
             double gu[3];
-            elem_grad(conn, B, phi, u, gu);
+            {
+                const int4 cu = conn[u];
+                double bu[12], vu;
+                geom_B(X, cu, bu, vu);
+                grad_from_B(cu, bu, phi, gu);
+            }
             double q2nu = __ddiv_rn(dot3r(gu[0], gu[1], gu[2], gu[0], gu[1], gu[2]), u2);
             q2lu = q2nu < F.q2cap ? q2nu : F.q2cap;
             lim_u = q2lu == q2nu;
@@ -430,11 +441,13 @@ __global__ void __launch_bounds__(NT, MB)
         acc.nu_max = fmax(acc.nu_max, nu);
         acc.sup += (nu > 0.0);
 
-        const double Ve = V[e];
         const double w1 = rt * Ve;
-        // second touch of B_e (an L1/L2 hit), held in registers from here
+        // B_e again (recomputed), held in registers from here
         double b[12];
-        ld_B(be, b);
+        {
+            double vtmp;
+            geom_B(X, ce, b, vtmp);
+        }
         double gB[4];
         gB_of(g, b, gB);
         if (JAC) {
@@ -450,7 +463,10 @@ __global__ void __launch_bounds__(NT, MB)
                 if (u != e) {
                     double gu[3], bu[12];
                     int4 cu;
-                    elem_grad_B(conn, B, phi, u, gu, bu, cu);
+                    cu = conn[u];
+                    double vu;
+                    geom_B(X, cu, bu, vu);
+                    grad_from_B(cu, bu, phi, gu);
                     gB_of(gu, bu, f);
                 }
                 store_t3(t3v, e, w3, gB, f);
@@ -934,7 +950,7 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     up3d_monitors* mo = mon ? mon : m->mon_ws.get();
     UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
 #define FUSED_ARGS                                                                                                \
-    m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz, \
+    m->conn.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz,                       \
         m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of, \
         n_cases, br_out
     const bool jac = data != nullptr;
@@ -1075,7 +1091,7 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
                 m->tune.elem_persistent = shapes[k][0];
                 m->tune.elem_threads_per_sm = shapes[k][1];
                 const double t = time_it([&] {
-                    launch_sweep<false, true, false>(m, s, m->conn.get(), m->B.get(), m->V.get(), m->fnbr.get(),
+                    launch_sweep<false, true, false>(m, s, m->conn.get(), m->fnbr.get(),
                                                      m->disp.get(), m->nodes4.get(), phi, F, u2, no_up, no_br, m->E,
                                                      m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(),
                                                      m->up32.get(), no_rt, mo, no_flows, no_case, 0, no_brout);

@@ -22,6 +22,43 @@ __device__ __forceinline__ void ld_B(const double* __restrict__ be, double b[12]
     ld4(be + 8, b[8], b[9], b[10], b[11]);
 }
 
+// B_e (12 values) and V_e from the node coordinates, with the operations of
+// the mesh set-up's geometry kernel, k_geometry (identical bits for every
+// element that passed its degeneracy check).
+__device__ __forceinline__ void geom_B(const double4* __restrict__ X, int4 c, double b[12], double& V) {
+    double x0x, x0y, x0z, w, x1x, x1y, x1z, x2x, x2y, x2z, x3x, x3y, x3z;
+    ld4(reinterpret_cast<const double*>(X + c.x), x0x, x0y, x0z, w);
+    ld4(reinterpret_cast<const double*>(X + c.y), x1x, x1y, x1z, w);
+    ld4(reinterpret_cast<const double*>(X + c.z), x2x, x2y, x2z, w);
+    ld4(reinterpret_cast<const double*>(X + c.w), x3x, x3y, x3z, w);
+    const double v1x = rsub(x1x, x0x), v1y = rsub(x1y, x0y), v1z = rsub(x1z, x0z);
+    const double v2x = rsub(x2x, x0x), v2y = rsub(x2y, x0y), v2z = rsub(x2z, x0z);
+    const double v3x = rsub(x3x, x0x), v3y = rsub(x3y, x0y), v3z = rsub(x3z, x0z);
+    const double c23x = rsub(rmul(v2y, v3z), rmul(v2z, v3y));
+    const double c23y = rsub(rmul(v2z, v3x), rmul(v2x, v3z));
+    const double c23z = rsub(rmul(v2x, v3y), rmul(v2y, v3x));
+    const double c31x = rsub(rmul(v3y, v1z), rmul(v3z, v1y));
+    const double c31y = rsub(rmul(v3z, v1x), rmul(v3x, v1z));
+    const double c31z = rsub(rmul(v3x, v1y), rmul(v3y, v1x));
+    const double c12x = rsub(rmul(v1y, v2z), rmul(v1z, v2y));
+    const double c12y = rsub(rmul(v1z, v2x), rmul(v1x, v2z));
+    const double c12z = rsub(rmul(v1x, v2y), rmul(v1y, v2x));
+    const double det = dot3r(v1x, v1y, v1z, c23x, c23y, c23z);
+    V = __ddiv_rn(fabs(det), 6.0);
+    const double inv = __ddiv_rn(1.0, det);
+    b[3] = rmul(c23x, inv); b[4] = rmul(c23y, inv); b[5] = rmul(c23z, inv);
+    b[6] = rmul(c31x, inv); b[7] = rmul(c31y, inv); b[8] = rmul(c31z, inv);
+    b[9] = rmul(c12x, inv); b[10] = rmul(c12y, inv); b[11] = rmul(c12z, inv);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) b[d] = -radd(radd(b[3 + d], b[6 + d]), b[9 + d]);
+}
+__device__ __forceinline__ void grad_from_B(int4 c, const double b[12], const double* __restrict__ phi, double g[3]) {
+    const double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        g[d] = radd(radd(radd(rmul(p0, b[d]), rmul(p1, b[3 + d])), rmul(p2, b[6 + d])), rmul(p3, b[9 + d]));
+}
+
 // From the element's nodes c and its 12 B values at `be` (global memory).
 __device__ __forceinline__ void elem_grad_rec(int4 c, const double* __restrict__ be, const double* __restrict__ phi,
                                               double g[3]) {

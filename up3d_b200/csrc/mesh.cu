@@ -44,7 +44,9 @@ __global__ void k_pad_nodes(const double* __restrict__ nodes, int64_t N, double4
 // B_e, V_e and centroids (mesh/metrics.py:27-70, :130-204;
 // kernels/upwind.py:750).  Rows of J^{-1} are the cross products of J's
 // columns over det J; B_0 = -(B_1 + B_2 + B_3).  `bad` receives the smallest
-// degenerate element index (|det J| < 1e-12 * |v1||v2||v3|).
+// degenerate element index (|det J| < 1e-12 * |v1||v2||v3|).  The fused
+// element sweep recomputes B_e and V_e with the same operations (geom_B,
+// elem.cuh); the two must stay in step.
 __global__ void k_geometry(const double4* __restrict__ X, const int4* __restrict__ conn, int64_t E,
                            double* __restrict__ B, double* __restrict__ V, double4* __restrict__ cen,
                            unsigned long long* bad) {
