@@ -213,13 +213,15 @@ def bytes_model(info, n_active=0):
     the scatter map (elem_to_csr as int32) and the outputs R and J.  Term 3
     adds 16 COO triplets (8 + 4 + 4 bytes) per active element.
 
-    `design` counts what this library's layout moves on top: the walk's face
-    displacements and the local-matrix round trip between the two kernels."""
+    `design` counts what this library's layout moves instead: the sweep
+    recomputes B and V from the node coordinates (no 104 bytes per element)
+    but reads the walk's face displacements and round-trips the local
+    matrices between the two kernels."""
     E, N, Z = info["n_tets"], info["n_nodes"], info["nnz"]
     elem = E * (16 + 96 + 8 + 16 + 24 + 4) + N * (24 + 8)
     row = E * 64 + N * 8 + Z * 8
     t3 = n_active * 16 * 16
-    design_elem = (E * (16 + 96 + 8 + 16 + 96 + 4 + 14 * 8 + 1) + N * (24 + 8))
+    design_elem = (E * (16 + 16 + 96 + 4 + 14 * 8 + 1) + N * (24 + 8))
     design_row = (E * (16 + 24 + 14 * 8) + Z * (4 + 4 + 8) + N * (4 * 3 + 8))
     return {"elem_sweep": elem, "row_gather": row, "term3": t3, "fused": elem + row + t3,
             "design": {"elem_sweep": design_elem, "row_gather": design_row}}
