@@ -67,6 +67,8 @@ def parse():
                    help="channel mesh of the wake-elimination timing ('' to skip)")
     p.add_argument("--wall", default="100x30x25",
                    help="channel mesh of the wall-force timing ('' to skip)")
+    p.add_argument("--lifting", default="100x30x25:0.7:2:40x12x10",
+                   help="mesh:Mach:alpha:oracle_mesh of the wake-coupled (lifting) Newton solve ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -422,6 +424,80 @@ def wake_timing(spec):
             "max_rel_err_vs_oracle": err}
 
 
+def lifting_timing(spec):
+    """Wake-coupled Newton (solve_newton_lifting, solve/newton.py:516-1141,
+    probe Kutta estimator) on a bump channel cut by a plane sheet normal to
+    y with the far-field vortex on the trailing-edge line: time from the
+    freestream to |R_f|inf < 1e-10 and |F|inf < 1e-8 on the device
+    (GMRES(60) on the coupled operator, AMG on the reduced Picard block,
+    the frozen-selection finish from |R| < 1e-6 or a stall), the upward
+    Mach continuation to M + 0.05 from M - 0.1 (solve_newton_transonic,
+    :1144-1307), and, on a smaller mesh, the device solve beside the
+    oracle's exact-step (sparse LU + Woodbury) solve on the host, both with
+    the live selection, with the distance between their solutions."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.constraints.dirichlet import FarfieldBasis, freestream_phi
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.mesh.wake_cut import channel_vortex_center, cut_channel_sheet
+    from up3d_b200.solve.lifting import NewtonWorkspace, solve_newton_lifting, solve_newton_transonic
+    parts = spec.split(":")
+    shape = tuple(int(v) for v in parts[0].split("x"))
+    m_inf, alpha = float(parts[1]), float(parts[2])
+
+    def case(sh):
+        cut = cut_channel_sheet(bump_channel(*sh, amplitude=AMPLITUDE, seed=0), normal="y")
+        return cut, channel_vortex_center(cut)
+
+    def device_solve(cut, vc, freeze_tol):
+        t0 = time.perf_counter()
+        ws = NewtonWorkspace(cut, cut.wc, alpha, vortex_center=vc)
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        res = solve_newton_lifting(cut, cut.wc, m_inf, alpha_deg=alpha, vortex_center=vc, workspace=ws,
+                                   n_picard_seed=0, freeze_tol=freeze_tol)
+        return ws, res, setup
+
+    cut, vc = case(shape)
+    device_solve(cut, vc, 1e-6)                # warm-up (library, mesh caches)
+    ws, res, setup = device_solve(cut, vc, 1e-6)
+    out = {"case": f"bump channel {parts[0]} Kuhn-split, y-normal wake sheet from x = {vc[0]:.2f}, "
+                   f"M_inf {m_inf}, alpha {alpha} deg, from the freestream",
+           "n_tets": int(len(cut.elements)), "n_red": int(ws.n_red), "n_stations": int(ws.n_st),
+           "time_s": round(res["timings"]["wall"], 4), "setup_s": round(setup, 3),
+           "converged": bool(res["converged"]), "n_newton": int(res["n_newton"]),
+           "n_gmres": int(res["n_gmres_total"]), "n_freeze_refresh": int(res["n_freeze_refresh"]),
+           "final_residual": res["residual_history"][-1], "final_F": res["F_history"][-1],
+           "n_supersonic": int(res["n_nu_active"]), "n_term3_active": int(res["n_term3_active"]),
+           "phases_s": {k: round(v, 4) for k, v in res["timings"].items()}}
+    t0 = time.perf_counter()
+    cont = solve_newton_transonic(cut, cut.wc, m_inf + 0.05, alpha, m_start=m_inf - 0.1,
+                                  newton_kw={"vortex_center": vc})
+    out["continuation"] = {"mach": [round(m_inf - 0.1, 3), round(m_inf + 0.05, 3)],
+                           "time_s": round(time.perf_counter() - t0, 3), "converged": bool(cont["converged"]),
+                           "levels": [[round(m, 4), n, r] for m, n, r in cont["level_history"]],
+                           "n_supersonic": int(cont["n_nu_active"])}
+    if len(parts) > 3 and parts[3]:
+        sh = tuple(int(v) for v in parts[3].split("x"))
+        cut, vc = case(sh)
+        ws, res, _ = device_solve(cut, vc, None)
+        basis = FarfieldBasis(cut, cut.wc, alpha, 1.0, vc)
+        vals0, V = basis.at_mach(float(np.sqrt(1.0 - m_inf ** 2)))
+        sysm = O.LiftingSystem(cut.nodes, cut.elements, cut.wc, basis.dir_red, vals0, V)
+        phi0 = freestream_phi(cut.nodes[:sysm.n_red], alpha, 1.0)
+        t0 = time.perf_counter()
+        phi_o, gam_o, hist, ok = sysm.solve(phi0[sysm.free], np.zeros(sysm.n_st), m_inf)
+        cpu_s = time.perf_counter() - t0
+        out["oracle_comparison"] = {
+            "mesh": parts[3], "n_tets": int(len(cut.elements)), "device_s": round(res["timings"]["wall"], 4),
+            "device_converged": bool(res["converged"]), "device_n_newton": int(res["n_newton"]),
+            "cpu_oracle_s": round(cpu_s, 3), "cpu_oracle_n_newton": len(hist) - 1,
+            "cpu_oracle_converged": bool(ok), "cpu_cores": O.num_threads(),
+            "max_abs_phi_diff": float(np.abs(res["phi"].cpu().numpy() - phi_o).max()),
+            "max_abs_gamma_diff": float(np.abs(res["gamma"].cpu().numpy() - gam_o).max())}
+    return out
+
+
 def wall_timing(spec):
     """Wall Cp and pressure forces (post/surface.py:309-363) on the
     channel's lower wall at a pocket state, M0.8, two smoothing passes:
@@ -704,6 +780,7 @@ def run_ours(args):
     weighted = weighted_timing(args.weighted) if args.weighted else None
     wake = wake_timing(args.wake) if args.wake else None
     wall = wall_timing(args.wall) if args.wall else None
+    lifting = lifting_timing(args.lifting) if args.lifting else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -760,6 +837,7 @@ def run_ours(args):
             "weighted_upwind": weighted,
             "wake_elimination": wake,
             "wall_forces": wall,
+            "lifting_newton": lifting,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

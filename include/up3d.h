@@ -549,6 +549,64 @@ int up3d_cg(const up3d_csr* A, const double* b, double* x, double rtol, double a
 int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double* x,
                double rtol, double atol, int restart, int maxiter, up3d_precond* M,
                int64_t* inner, double* resid, int* info, up3d_stream stream);
+/* ------------------------------------------- coupled (phi, Gamma) Newton system */
+
+typedef struct up3d_coupled up3d_coupled; /* opaque: far-field rows, Kutta rows, basis */
+
+/* NewtonWorkspace's coupled system (solve/newton.py:97-502, the "probe"
+ * Kutta estimator) on the unknowns of a wake handle: dir_nodes (HOST, n_dir
+ * distinct reduced ids) are the far-field rows (`dir_red`, :243-256); K
+ * (HOST CSR, n_stations rows, int64 k_indptr / k_cols = reduced ids of free
+ * rows, k_vals) is dF/dphi_free (:276-292, the tip taper already applied);
+ * the Kutta targets average phi[kutta_upper] - phi[kutta_lower] over each
+ * station's TE entries (te_station, n_te entries, TE order: kutta_targets,
+ * constraints/wake.py:196-212) and are scaled by taper (n_stations, HOST).
+ * The handle refers to `wake`, which must outlive it.  UP3D_ERR_VALUE for
+ * ids out of range, a K column on a far-field row or a station without
+ * TE entries.  Calls on one handle must not overlap. */
+int up3d_coupled_create(const up3d_wake* wake, int64_t n_dir, const int64_t* dir_nodes,
+                        const int64_t* k_indptr, const int64_t* k_cols, const double* k_vals,
+                        int64_t n_te, const int64_t* te_station, const int64_t* kutta_upper,
+                        const int64_t* kutta_lower, const double* taper, up3d_coupled** out);
+int up3d_coupled_destroy(up3d_coupled* coupled);
+/* set_mach's affine far-field basis (solve/newton.py:295-324): far-field
+ * values vals0 + V Gamma (HOST vals0 n_dir, V n_dir x n_stations row-major,
+ * rows in dir_nodes order). */
+int up3d_coupled_set_farfield(up3d_coupled* coupled, const double* vals0, const double* V);
+/* Device view of the far-field row mask (n_red, 1 on far-field rows): the
+ * `dirichlet` of the reduced Picard block's up3d_csr. */
+int up3d_coupled_dirichlet(const up3d_coupled* coupled, const uint8_t** mask);
+/* eval_residual's state (solve/newton.py:340-344): phi_red = phi_f on free
+ * rows and vals0 + V gamma on far-field rows (phi_red may alias phi_f),
+ * phi_cut = T phi_red + G gamma.  Device vectors (n_red, n_stations,
+ * n_red, n_cut). */
+int up3d_coupled_state(const up3d_coupled* coupled, const double* phi_f, const double* gamma,
+                       double* phi_red, double* phi_cut, up3d_stream stream);
+/* eval_residual's outputs (:399-419): R_red = T^T R_cut on free rows, 0 on
+ * far-field rows; F = taper * kutta_targets(phi_cut) - gamma. */
+int up3d_coupled_residual(const up3d_coupled* coupled, const double* R_cut, const double* phi_cut,
+                          const double* gamma, double* R_red, double* F, up3d_stream stream);
+/* The eliminated coupled step's operator (:1029-1032, :1079):
+ * t = K x + g (g may be NULL), y = J_ff x + B t on free rows with
+ * B = J_red[free, dir] V + H_J[free] (assemble_coupled, :430-457), y = x on
+ * far-field rows.  J (+ extra, may be NULL) is the Jacobian of the CUT mesh
+ * (n_cut rows, no Dirichlet mask); J_red, H_J and B are never formed: the
+ * operator is T^T J (T u + G t) with u = x on free rows and V t on
+ * far-field rows.  x = 0, g = F gives B F; t (n_stations, may be NULL)
+ * returns K x + g, the step's dGamma. */
+int up3d_coupled_apply(const up3d_coupled* coupled, const up3d_csr* J, const up3d_csr* extra,
+                       const double* x, const double* g, double* y, double* t, up3d_stream stream);
+
+
+/* up3d_gmres on the coupled operator (up3d_coupled_apply with g = NULL):
+ * the inexact Newton solve of solve_newton_lifting (solve/newton.py:
+ * 1029-1046).  b and x are reduced-size vectors, b zero on far-field rows;
+ * M (may be NULL) must be of reduced size -- the AMG of the reduced Picard
+ * block with the far-field mask (:1013-1022).  Synchronous. */
+int up3d_gmres_coupled(const up3d_coupled* coupled, const up3d_csr* J, const up3d_csr* extra,
+                       const double* b, double* x, double rtol, double atol, int restart,
+                       int maxiter, up3d_precond* M, int64_t* inner, double* resid, int* info,
+                       up3d_stream stream);
 /* Mixed-precision GMRES with FP64 iterative refinement (the mixed form of
  * the Newton linear solve the reference does with spla.gmres,
  * solve/newton.py:1029-1040).  The outer loop forms r = b - A x with A's

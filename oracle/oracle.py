@@ -519,6 +519,101 @@ def kutta_targets(phi, wc):
     return sums / np.bincount(wc.te_station, minlength=wc.n_stations)
 
 
+# -------------------------------------------------- coupled (phi, Gamma) Newton
+# solve/newton.py:97-1141 restated for the probe Kutta estimator, with the
+# far-field split and basis given (dir_red, vals0_red, V_red: set_mach's
+# output) and exact (sparse LU + Woodbury) Newton steps -- the reference's
+# precond="direct" path (:966-1011).
+
+
+class LiftingSystem:
+    """NewtonWorkspace.eval_residual / assemble_coupled / the probe
+    kutta_blocks (solve/newton.py:326-502) over the oracle kernels."""
+
+    def __init__(self, nodes, elements, wc, dir_red, vals0_red, V_red, tip_taper=None, u_inf=1.0):
+        self.op = PicardOperator(nodes, elements)
+        self.upw = UpwindOperator(nodes, elements)
+        self.wc, self.u_inf = wc, float(u_inf)
+        self.con = WakeConstraint(self.op.assemble_matrix(np.ones(len(elements))), wc)
+        self.n_red, self.n_st = self.con.n_reduced, wc.n_stations
+        self.dir_red = np.asarray(dir_red, dtype=np.int64)
+        is_dir = np.zeros(self.n_red, dtype=bool)
+        is_dir[self.dir_red] = True
+        self.free = np.where(~is_dir)[0]
+        self.vals0_red, self.V_red = np.asarray(vals0_red), np.asarray(V_red)
+        self.taper = np.ones(self.n_st) if tip_taper is None else np.asarray(tip_taper, dtype=np.float64)
+        counts = np.bincount(wc.te_station, minlength=self.n_st).astype(np.float64)
+        probes = np.concatenate([wc.kutta_upper, wc.kutta_lower])
+        cols = np.searchsorted(self.free, probes)
+        w = 1.0 / counts[wc.te_station]
+        self.K = sp.coo_matrix((np.concatenate([w, -w]), (np.concatenate([wc.te_station, wc.te_station]), cols)),
+                               shape=(self.n_st, len(self.free))).tocsr()
+        if not np.all(self.taper == 1.0):
+            self.K = sp.diags(self.taper) @ self.K
+
+    def eval_residual(self, phi_free, gamma, m_inf, frozen=None, **kw):
+        """(R_free, F, state) (newton.py:340-419)."""
+        gamma = np.asarray(gamma, dtype=np.float64)
+        phi_red = np.empty(self.n_red)
+        phi_red[self.free] = phi_free
+        phi_red[self.dir_red] = self.vals0_red + self.V_red @ gamma
+        phi_cut = self.con.expand(phi_red, gamma)
+        st = chain(self.op, self.upw, phi_cut, m_inf, self.u_inf, jacobian=True, **kw)
+        R_red = self.con.T.T @ st["R"]
+        F = self.taper * kutta_targets(phi_cut, self.wc) - gamma
+        st.update(phi_red=phi_red, phi_cut=phi_cut)
+        return R_red[self.free], F, st
+
+    def blocks(self, st):
+        """(J_ff, B), B = J_red[free, dir] V + H_J[free] (newton.py:430-457)."""
+        J_red, H = self.con.reduce_operator(st["J"])
+        J_ff = J_red[self.free][:, self.free].tocsr()
+        J_fd = J_red[self.free][:, self.dir_red].tocsr()
+        B = J_fd @ sp.csr_matrix(self.V_red) + H.tocsr()[self.free, :]
+        return J_ff, B.tocsc()
+
+    def solve(self, phi_free, gamma, m_inf, n_newton_max=30, tol_residual=1e-10, tol_gamma=1e-8, **kw):
+        """Exact Newton with the merit line search (newton.py:779-1111 on
+        the precond="direct" branch, live upwind selection):
+        (phi_cut, gamma, residual history)."""
+        import scipy.sparse.linalg as spla
+        phi_free = np.asarray(phi_free, dtype=np.float64).copy()
+        gamma = np.asarray(gamma, dtype=np.float64).copy()
+        R, F, st = self.eval_residual(phi_free, gamma, m_inf, **kw)
+        merit = float(R @ R + F @ F)
+        hist = []
+        for _ in range(n_newton_max):
+            r_norm = float(np.max(np.abs(R)))
+            hist.append(r_norm)
+            if (np.max(np.abs(F)) < tol_gamma and st["n_limited"] == 0 and st["n_floored"] == 0
+                    and r_norm < tol_residual):
+                return st["phi_cut"], gamma, hist, True
+            J_ff, B = self.blocks(st)
+            rhs = -R - B @ F
+            lu = spla.splu(J_ff.tocsc())
+            z = lu.solve(rhs)
+            JB = lu.solve(B.toarray())
+            S = np.eye(self.n_st) + self.K @ JB
+            dphi = z - JB @ np.linalg.solve(S, self.K @ z)
+            dgamma = self.K @ dphi + F
+            lam, best = 1.0, None
+            for _ in range(5):
+                R_t, F_t, st_t = self.eval_residual(phi_free + lam * dphi, gamma + lam * dgamma, m_inf, **kw)
+                m_t = float(R_t @ R_t + F_t @ F_t)
+                if np.isfinite(m_t) and m_t <= merit:
+                    best = None
+                    break
+                if np.isfinite(m_t) and (best is None or m_t < best[0]):
+                    best = (m_t, lam, R_t, F_t, st_t)
+                lam *= 0.5
+            if best is not None:
+                m_t, lam, R_t, F_t, st_t = best
+            phi_free = phi_free + lam * dphi
+            gamma = gamma + lam * dgamma
+            R, F, st, merit = R_t, F_t, st_t, m_t
+        return st["phi_cut"], gamma, hist, False
+
+
 # ---------------------------------------------------------------- wall post
 # post/surface.py:80-363, restated with numpy (the per-triangle arithmetic
 # in the reference's order).

@@ -5,7 +5,7 @@ Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
     python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only | --wall-only |
-                                                      --sides-only]
+                                                      --sides-only | --lifting-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -28,6 +28,7 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   wall_force_coefficients and its pieces              post/surface.py:80-363
   per-side walks, newton_terms23_side_coo             wake/multivalued.py:456-466,
                                                       kernels/cut_assembly.py:401-488
+  NewtonWorkspace, solve_newton_lifting (direct)      solve/newton.py:97-1141
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -384,6 +385,93 @@ def make_sides(jac, upw_mod, isen, name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB), {len(data)} triplets")
 
 
+
+LIFTING_CASES = {
+    # name: (channel shape, M_inf, alpha_deg, farfield_spanwise_gamma)
+    "sub": ((12, 6, 4), 0.5, 3.0, False),
+    "trans": ((16, 6, 4), 0.8, 2.0, True),
+}
+
+
+def make_lifting(name):
+    """The coupled (phi, Gamma) Newton system of the reference
+    (NewtonWorkspace, solve_newton_lifting: solve/newton.py:97-1141, the
+    probe Kutta estimator) on a bump channel cut by a plane sheet normal to
+    y (up3d_b200.mesh.wake_cut.cut_channel_sheet(normal="y")) with the
+    far-field vortex centred on the trailing-edge line: the workspace's
+    far-field split, basis and Kutta row; eval_residual and the
+    assemble_coupled blocks at a seeded state with the coupled product
+    J_ff x + B (K x) and B F; and the converged solve from the freestream
+    (precond="direct": exact Newton steps, no pyamg)."""
+    from types import SimpleNamespace
+    from pyfp3d.mesh.wake_cut import WakeCut as RefWakeCut
+    from pyfp3d.solve.newton import NewtonWorkspace, solve_newton_lifting
+    from pyfp3d.constraints.dirichlet import freestream_phi
+    from up3d_b200.mesh.wake_cut import channel_vortex_center, cut_channel_sheet
+    rng = np.random.default_rng(11)
+    arrays = {}
+    for case, (shape, m_inf, alpha, spanwise) in LIFTING_CASES.items():
+        mesh = bump_channel(*shape, amplitude=0.08, seed=3)
+        cut = cut_channel_sheet(mesh, normal="y")
+        wc = RefWakeCut()
+        for k in ("n_nodes_orig", "master_nodes", "slave_nodes", "te_nodes", "station_z",
+                  "node_station", "te_station", "kutta_upper", "kutta_lower"):
+            setattr(wc, k, getattr(cut.wc, k))
+        mc = SimpleNamespace(nodes=cut.nodes, elements=cut.elements, boundary_faces=cut.boundary_faces)
+        vc = channel_vortex_center(cut)
+        ws = NewtonWorkspace(mc, wc, alpha, vortex_center=vc, farfield_spanwise_gamma=spanwise)
+        ws.set_mach(m_inf)
+        pre = f"{case}/"
+        # the converged solve first (the transonic seed perturbs it)
+        res = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, vortex_center=vc,
+                                   farfield_spanwise_gamma=spanwise, n_picard_seed=0, precond="direct")
+        assert res["converged"], case
+        arrays.update({pre + "sol_phi": res["phi"], pre + "sol_gamma": res["gamma"],
+                       pre + "sol_residual_history": np.array(res["residual_history"]),
+                       pre + "sol_F_history": np.array(res["F_history"]),
+                       pre + "sol_n_newton": np.int64(res["n_newton"]),
+                       pre + "sol_n_nu_active": np.int64(res["n_nu_active"]),
+                       pre + "sol_n_term3_active": np.int64(res["n_term3_active"] or 0)})
+        K = ws.K.tocsr()
+        arrays.update({pre + "shape": np.array(shape), pre + "m_inf": np.float64(m_inf),
+                       pre + "alpha_deg": np.float64(alpha), pre + "spanwise": np.bool_(spanwise),
+                       pre + "vortex_center": np.array(vc, dtype=np.float64),
+                       pre + "nodes": cut.nodes, pre + "elements": cut.elements,
+                       pre + "farfield_faces": cut.boundary_faces["farfield"],
+                       pre + "dir_red": ws.dir_red.astype(np.int64), pre + "free": ws.free.astype(np.int64),
+                       pre + "vals0_red": ws.vals0_red, pre + "V_red": ws.V_red,
+                       pre + "K_indptr": K.indptr.astype(np.int64), pre + "K_indices": K.indices.astype(np.int64),
+                       pre + "K_data": K.data})
+        # a seeded state: a smooth perturbation of the freestream (subsonic
+        # case) or of the converged solution (transonic case: supersonic
+        # elements and Term 3 active), small Gamma perturbations
+        x = cut.nodes[:ws.n_red, 0]
+        wiggle = np.sin(1.3 * x) * (1.0 + 0.1 * rng.standard_normal(ws.n_red))
+        if m_inf < 0.7:
+            phi_red = freestream_phi(cut.nodes[:ws.n_red], alpha, 1.0) + 0.01 * wiggle
+            gamma = 0.01 * rng.standard_normal(ws.n_st)
+        else:
+            phi_red = res["phi"][:ws.n_red] + 0.002 * wiggle
+            gamma = res["gamma"] + 0.001 * rng.standard_normal(ws.n_st)
+        phi_free = phi_red[ws.free].copy()
+        R_free, F, state = ws.eval_residual(phi_free, gamma, UPWIND_C, M_CRIT, M_CAP, RHO_FLOOR)
+        J_ff, B = ws.assemble_coupled(state, UPWIND_C, M_CRIT, RHO_FLOOR)
+        J_ff = J_ff.tocsr()
+        Bd = B.toarray()
+        xv = rng.standard_normal(ws.n_free)
+        arrays.update({pre + "seed_phi_free": phi_free, pre + "seed_gamma": gamma,
+                       pre + "seed_R_free": R_free, pre + "seed_F": F,
+                       pre + "seed_phi_cut": state["phi_cut"],
+                       pre + "seed_n_supersonic": np.int64(state["n_nu_active"]),
+                       pre + "Jff_indptr": J_ff.indptr.astype(np.int64),
+                       pre + "Jff_indices": J_ff.indices.astype(np.int64), pre + "Jff_data": J_ff.data,
+                       pre + "B": Bd, pre + "x": xv, pre + "y": J_ff @ xv + B @ (ws.K @ xv),
+                       pre + "BF": B @ F, pre + "n_term3_active": np.int64(ws.op.n_term3_active or 0)})
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -398,6 +486,9 @@ def main():
         return
     if "--sides-only" in sys.argv:
         make_sides(jac, upw_mod, isen, "side_terms")
+        return
+    if "--lifting-only" in sys.argv:
+        make_lifting("lifting_newton")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -422,6 +513,7 @@ def main():
     make_wake(jac, upw_mod, isen, "wake_constraint")
     make_wall("wall_forces")
     make_sides(jac, upw_mod, isen, "side_terms")
+    make_lifting("lifting_newton")
 
 
 def _weighted(jac, upw_mod, isen):

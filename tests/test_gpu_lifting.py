@@ -1,0 +1,177 @@
+"""Device coupled (phi, Gamma) lifting Newton against the reference's
+NewtonWorkspace / solve_newton_lifting (tests/golden/lifting_newton.npz,
+solve/newton.py:97-1141, probe Kutta estimator): eval_residual, the coupled
+operator J_ff + B K and B F, the coupled GMRES, and the converged solve
+from the freestream, through the up3d_coupled_* C ABI."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["sub", "trans"]
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLDEN / "lifting_newton.npz")
+
+
+def _case(gold, name):
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.mesh.wake_cut import cut_channel_sheet
+    g = {k.split("/", 1)[1]: gold[k] for k in gold.files if k.startswith(name + "/")}
+    cut = cut_channel_sheet(bump_channel(*tuple(int(v) for v in g["shape"]), amplitude=0.08, seed=3),
+                            normal="y")
+    return g, cut
+
+
+def _ws(g, cut):
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import NewtonWorkspace
+    ws = NewtonWorkspace(cut, cut.wc, float(g["alpha_deg"]), vortex_center=channel_vortex_center(cut),
+                         farfield_spanwise_gamma=bool(g["spanwise"]))
+    ws.set_mach(float(g["m_inf"]))
+    return ws
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _full(ws, free_vals):
+    import torch
+    x = np.zeros(ws.n_red)
+    x[ws.free] = free_vals
+    return torch.from_numpy(x).cuda()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_eval_residual(gold, name):
+    g, cut = _case(gold, name)
+    ws = _ws(g, cut)
+    R, F, st = ws.eval_residual(_full(ws, g["seed_phi_free"]), g["seed_gamma"], 1.5, 0.95, 3.0, 0.05)
+    # far-field rows: vals0 + V Gamma, a dot product the reference leaves to
+    # BLAS (summation order unspecified): equal to within rounding
+    assert _rel(st["phi_cut"].cpu().numpy(), g["seed_phi_cut"]) <= 1e-14
+    R = R.cpu().numpy()
+    assert np.all(R[ws.dir_red] == 0.0)
+    assert _rel(R[ws.free], g["seed_R_free"]) <= 1e-12
+    assert _rel(F.cpu().numpy(), g["seed_F"]) <= 1e-12
+    assert st["n_nu_active"] == int(g["seed_n_supersonic"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_coupled_operator(gold, name):
+    import torch
+    g, cut = _case(gold, name)
+    ws = _ws(g, cut)
+    R, F, st = ws.eval_residual(_full(ws, g["seed_phi_free"]), g["seed_gamma"], 1.5, 0.95, 3.0, 0.05)
+    A = ws.assemble_coupled(st)
+    assert st["n_term3_active"] == int(g["n_term3_active"])
+    x = _full(ws, g["x"])
+    x[torch.from_numpy(ws.dir_red).cuda()] = 7.0      # far-field rows pass through
+    y, t = A.apply(x)
+    y = y.cpu().numpy()
+    assert _rel(y[ws.free], g["y"]) <= 1e-12
+    assert np.all(y[ws.dir_red] == 7.0)
+    Kx = ws.K[:, ws.free] @ g["x"]
+    assert _rel(t.cpu().numpy(), Kx) <= 1e-14
+    BF, tF = A.apply(torch.zeros(ws.n_red, dtype=torch.float64, device="cuda"), F)
+    BF = BF.cpu().numpy()
+    assert _rel(BF[ws.free], g["BF"]) <= 1e-12
+    assert np.all(BF[ws.dir_red] == 0.0)
+    assert np.array_equal(tF.cpu().numpy(), F.cpu().numpy())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_coupled_gmres(gold, name):
+    import torch
+    from up3d_b200.solve.linear import amg_for
+    g, cut = _case(gold, name)
+    ws = _ws(g, cut)
+    R, F, st = ws.eval_residual(_full(ws, g["seed_phi_free"]), g["seed_gamma"], 1.5, 0.95, 3.0, 0.05)
+    A = ws.assemble_coupled(st)
+    M = amg_for(ws.picard_block())
+    b = -R - A.apply(torch.zeros_like(R), F)[0]
+    x, n_it, info = A.solve(b, M=M, rtol=1e-10, restart=60, maxiter=10)
+    assert info == 0 and n_it > 0
+    r = (A.matvec(x) - b).cpu().numpy()
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b.cpu().numpy()) * 1.01
+    assert np.all(x.cpu().numpy()[ws.dir_red] == 0.0)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_newton_matches_reference(gold, name):
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    g, cut = _case(gold, name)
+    res = solve_newton_lifting(cut, cut.wc, float(g["m_inf"]), alpha_deg=float(g["alpha_deg"]),
+                               vortex_center=channel_vortex_center(cut),
+                               farfield_spanwise_gamma=bool(g["spanwise"]), n_picard_seed=0)
+    assert res["converged"]
+    assert res["residual_history"][-1] < 1e-10 and res["F_history"][-1] < 1e-8
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-9
+    assert res["n_nu_active"] == int(g["sol_n_nu_active"])
+
+
+def test_gpu_lifting_rejects_unbuilt_options(gold):
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import NewtonWorkspace, solve_newton_lifting
+    g, cut = _case(gold, "sub")
+    vc = channel_vortex_center(cut)
+    with pytest.raises(NotImplementedError):
+        NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="pressure")
+    with pytest.raises(NotImplementedError):
+        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct")
+    with pytest.raises(NotImplementedError):
+        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, n_picard_seed=5)
+
+
+def test_gpu_coupled_create_rejects_bad_ids(gold):
+    from up3d_b200 import _lib as L
+    g, cut = _case(gold, "sub")
+    ws = _ws(g, cut)
+    h = ctypes.c_void_p()
+    dr = np.array([ws.n_red], dtype=np.int64)             # out of range
+    kp = np.zeros(ws.n_st + 1, dtype=np.int64)
+    ts = np.ascontiguousarray(cut.wc.te_station, dtype=np.int64)
+    ku = np.ascontiguousarray(cut.wc.kutta_upper, dtype=np.int64)
+    kl = np.ascontiguousarray(cut.wc.kutta_lower, dtype=np.int64)
+    tp = np.ones(ws.n_st)
+    with pytest.raises(ValueError):
+        L.call("up3d_coupled_create", ws._plan.handle, 1, dr.ctypes.data, kp.ctypes.data, None, None,
+               len(ts), ts.ctypes.data, ku.ctypes.data, kl.ctypes.data, tp.ctypes.data, ctypes.byref(h))
+    dr = np.array([cut.wc.kutta_upper[0]], dtype=np.int64)  # a K column on a far-field row
+    kp = np.ascontiguousarray(ws.K.indptr, dtype=np.int64)
+    kc = np.ascontiguousarray(ws.K.indices, dtype=np.int64)
+    kv = np.ascontiguousarray(ws.K.data, dtype=np.float64)
+    with pytest.raises(ValueError):
+        L.call("up3d_coupled_create", ws._plan.handle, 1, dr.ctypes.data, kp.ctypes.data, kc.ctypes.data,
+               kv.ctypes.data, len(ts), ts.ctypes.data, ku.ctypes.data, kl.ctypes.data, tp.ctypes.data,
+               ctypes.byref(h))
+
+
+@pytest.mark.parametrize("intermediate_tol", [None, 1e-6])
+def test_gpu_lifting_continuation_reaches_reference_solution(gold, intermediate_tol):
+    """Upward Mach continuation (solve/newton.py:1144-1307) to the transonic
+    golden case from M0.7, with and without loose intermediate levels: the
+    final level's solution is the reference's."""
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_newton_transonic
+    g, cut = _case(gold, "trans")
+    res = solve_newton_transonic(cut, cut.wc, float(g["m_inf"]), float(g["alpha_deg"]), m_start=0.7,
+                                 intermediate_tol=intermediate_tol,
+                                 newton_kw={"vortex_center": channel_vortex_center(cut),
+                                            "farfield_spanwise_gamma": bool(g["spanwise"])})
+    assert res["converged"]
+    assert [round(m, 6) for m, _, _ in res["level_history"]][-1] == round(float(g["m_inf"]), 6)
+    if intermediate_tol is not None:
+        assert res["level_results"][0]["accept_reason"] in ("loose_tol", "rel_drop", "stall", "tol")
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-9

@@ -104,6 +104,15 @@ SIGNATURES = {
     "up3d_wake_reduce": (_int, [_p, _p, _p, _p, _p]),
     "up3d_wake_reduced_rhs": (_int, [_p, _p, _p, _p, _p, _p]),
     "up3d_wake_expand": (_int, [_p, _p, _p, _p, _p]),
+    "up3d_coupled_create": (_int, [_p, _i64, _p, _p, _p, _p, _i64, _p, _p, _p, _p, ctypes.POINTER(_p)]),
+    "up3d_coupled_destroy": (_int, [_p]),
+    "up3d_coupled_set_farfield": (_int, [_p, _p, _p]),
+    "up3d_coupled_dirichlet": (_int, [_p, ctypes.POINTER(_p)]),
+    "up3d_coupled_state": (_int, [_p, _p, _p, _p, _p, _p]),
+    "up3d_coupled_residual": (_int, [_p, _p, _p, _p, _p, _p, _p]),
+    "up3d_coupled_apply": (_int, [_p, _p, _p, _p, _p, _p, _p, _p]),
+    "up3d_gmres_coupled": (_int, [_p, _p, _p, _p, _p, _d, _d, _int, _int, _p, ctypes.POINTER(_i64),
+                                  ctypes.POINTER(_d), ctypes.POINTER(_int), _p]),
     "up3d_terms23_side_coo": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _d, _p, _p, _p, _i64,
                                      ctypes.POINTER(_i64), _p]),
     "up3d_wall_create": (_int, [_p, _p, _p, _i64, ctypes.POINTER(_p)]),

@@ -20,13 +20,6 @@
 
 namespace up3d {
 
-template <class T>
-void launch_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const T* x, T* y,
-                 const uint8_t* dir, cudaStream_t s);
-template <class T>
-void launch_spmv2(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const int32_t* xptr,
-                  const int32_t* xidx, const T* xdata, const T* x, T* y, const uint8_t* dir, cudaStream_t s);
-
 namespace {
 
 constexpr int RB = 256;      // reduction block
@@ -282,6 +275,10 @@ Blas& ws_blas(KrylovWs& w, cudaStream_t s) {
 // ------------------------------------------------------------ operators
 
 void Operator::apply(const double* x, double* y, cudaStream_t s) const {
+    if (coupled) {
+        coupled_apply(coupled, A, extra, x, nullptr, y, nullptr, s);
+        return;
+    }
     // y = A x (+ extra x: the Term-3 entries outside the P1 pattern), one pass
     launch_spmv2<double>(A.n, A.indptr, A.indices, A.data, extra.indptr, extra.indices, extra.data, x, y,
                          A.dirichlet, s);
@@ -289,6 +286,7 @@ void Operator::apply(const double* x, double* y, cudaStream_t s) const {
 
 // FP32 operator: the FP32 copies of the values (data32, extra32).
 void Operator::apply(const float* x, float* y, cudaStream_t s) const {
+    UP3D_REQUIRE(!coupled, UP3D_ERR_ARGUMENT, "the coupled wake operator is FP64 only");
     UP3D_REQUIRE(data32 && (!extra.indptr || extra32), UP3D_ERR_ARGUMENT, "FP32 operator without FP32 values");
     launch_spmv2<float>(A.n, A.indptr, A.indices, data32, extra.indptr, extra.indices, extra32, x, y, A.dirichlet,
                         s);
@@ -342,7 +340,7 @@ static double eff_atol(double atol, double rtol, double bnrm) { return std::max(
 // preconditioned CG, converged when ||r|| <= max(rtol ||b||, atol).
 int cg_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int maxiter, up3d_precond* M,
              int64_t* iters, double* resid, cudaStream_t s) {
-    const int64_t n = op.A.n;
+    const int64_t n = op.rows();
     KrylovWs& W = krylov_ws();
     std::lock_guard<std::recursive_mutex> lock(W.mu);
     Blas& bl = ws_blas(W, s);
@@ -431,7 +429,7 @@ static void lartg(double f, double g, double& c, double& sn, double& r) {
 template <class T>
 int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, int restart, int maxiter,
                 up3d_precond* M, int64_t* inner, double* resid, cudaStream_t s) {
-    const int64_t n = op.A.n;
+    const int64_t n = op.rows();
     KrylovWs& W = krylov_ws();
     std::lock_guard<std::recursive_mutex> lock(W.mu);
     Blas& bl = ws_blas(W, s);
@@ -580,7 +578,7 @@ template int gmres_solve<float>(const Operator&, const float*, float*, double, d
 int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart,
                    int maxiter, int refine_max, double inner_rtol, up3d_precond* M, int64_t* inner, int64_t* outer,
                    double* resid, cudaStream_t s) {
-    const int64_t n = op.A.n;
+    const int64_t n = op.rows();
     KrylovWs& W = krylov_ws();
     std::lock_guard<std::recursive_mutex> lock(W.mu);
     Blas& bl = ws_blas(W, s);
@@ -708,6 +706,21 @@ int up3d_gmres(const up3d_csr* A, const up3d_csr* extra, const double* b, double
         UP3D_REQUIRE(b && x && restart > 0 && maxiter > 0, UP3D_ERR_ARGUMENT, "up3d_gmres: bad argument");
         Operator op;
         make_op(op, A, extra);
+        int inf = gmres_solve(op, b, x, rtol, atol, restart, maxiter, M, inner, resid, S(stream));
+        if (info) *info = inf;
+    });
+}
+
+int up3d_gmres_coupled(const up3d_coupled* c, const up3d_csr* J, const up3d_csr* extra, const double* b,
+                       double* x, double rtol, double atol, int restart, int maxiter, up3d_precond* M,
+                       int64_t* inner, double* resid, int* info, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && b && x && restart > 0 && maxiter > 0, UP3D_ERR_ARGUMENT, "up3d_gmres_coupled: bad argument");
+        Operator op;
+        make_op(op, J, extra);
+        op.coupled = c;
+        UP3D_REQUIRE(!M || M->n == coupled_rows(c), UP3D_ERR_ARGUMENT,
+                     "up3d_gmres_coupled: preconditioner size differs from the reduced system");
         int inf = gmres_solve(op, b, x, rtol, atol, restart, maxiter, M, inner, resid, S(stream));
         if (info) *info = inf;
     });

@@ -3,7 +3,23 @@
 
 #include "internal.cuh"
 
+struct up3d_coupled;
+
 namespace up3d {
+
+// y = A x (+ xA x) on the device (linear.cu); dir = identity rows or NULL
+template <class T>
+void launch_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const T* x, T* y,
+                 const uint8_t* dir, cudaStream_t s);
+template <class T>
+void launch_spmv2(int64_t n, const int32_t* indptr, const int32_t* indices, const T* data, const int32_t* xptr,
+                  const int32_t* xidx, const T* xdata, const T* x, T* y, const uint8_t* dir, cudaStream_t s);
+
+// The coupled (phi, Gamma) operator of a wake-cut mesh (wake.cu): y =
+// J_ff x + B (K x + g) in full reduced size, t = K x + g when t != NULL.
+int64_t coupled_rows(const up3d_coupled* c);
+void coupled_apply(const up3d_coupled* c, const up3d_csr& J, const up3d_csr& extra, const double* x,
+                   const double* g, double* y, double* t, cudaStream_t s);
 
 // Reproducible reductions and vector updates on one stream.
 // Vector arguments are double or float; dot products accumulate in FP64.
@@ -27,12 +43,16 @@ struct Blas {
 };
 
 // y = A x (+ extra x): the P1-pattern matrix plus, for the Newton Jacobian,
-// the Term-3 entries outside the pattern.
+// the Term-3 entries outside the pattern.  With `coupled` set, A (+ extra)
+// is a wake-cut mesh's Jacobian and the operator is the coupled system's
+// J_ff + B K on the reduced unknowns (FP64 only).
 struct Operator {
     up3d_csr A{};
     up3d_csr extra{};
     const float* data32 = nullptr;   // FP32 copies of the values (mixed precision)
     const float* extra32 = nullptr;
+    const up3d_coupled* coupled = nullptr;
+    int64_t rows() const { return coupled ? coupled_rows(coupled) : A.n; }
     void apply(const double* x, double* y, cudaStream_t s) const;
     void apply(const float* x, float* y, cudaStream_t s) const;
 };

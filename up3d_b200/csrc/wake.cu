@@ -16,10 +16,12 @@
 // within a group before adding the group to the total.
 
 #include <algorithm>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "internal.cuh"
+#include "krylov.cuh"
 
 struct up3d_wake {
     int device = 0;
@@ -292,6 +294,279 @@ int up3d_wake_expand(const up3d_wake* w, const double* phi_red, const double* ga
         k_wake_expand<<<grid_for(w->n_red + w->n_dup, 256, (int64_t)148 * 32), 256, 0, S(stream)>>>(
             w->n_red, w->n_dup, w->slave.get(), w->master.get(), w->station.get(), phi_red, gamma, phi_cut);
         UP3D_CHECK_LAUNCH();
+    });
+}
+
+}  // extern "C"
+
+// ===================================================== the coupled (phi, Gamma) system
+//
+// NewtonWorkspace (solve/newton.py:97-502) solves for the free reduced
+// potentials phi_f and the station circulations Gamma together:
+//   phi_red = phi_f on free rows, vals0 + V Gamma on the far-field rows,
+//   phi_cut = T phi_red + G Gamma,
+//   R_f = (T^T R(phi_cut))[free],  F = taper * kutta(phi_cut) - Gamma.
+// Its eliminated Newton step (kutta_blocks, :459-502, probe estimator)
+// solves (J_ff + B K) dphi = -R_f - B F with B = J_red[free, dir] V +
+// H_J[free] and dGamma = K dphi + F.  The operator here applies that
+// linearisation without forming J_red, J_ff or B:
+//   t = K x + g,  u_red = x on free rows, V t on far-field rows,
+//   y = (T^T J (T u_red + G t))[free],  y = x on far-field rows,
+// i.e. J_ff x + B (K x + g): one expand, one SpMV of the cut-mesh Jacobian
+// (Term-3 entries included), one fold.  Vectors are full reduced size with
+// the far-field rows carried as identity rows (the up3d_csr Dirichlet
+// convention), so the solvers and the AMG of the reduced Picard block take
+// them unchanged.
+
+struct up3d_coupled {
+    const up3d_wake* wake = nullptr;
+    int64_t n_red = 0, n_cut = 0, n_dir = 0;
+    int32_t n_st = 0;
+    up3d::DBuf<int32_t> dir;                  // far-field reduced rows (n_dir)
+    up3d::DBuf<uint8_t> mask;                 // n_red, 1 on far-field rows
+    up3d::DBuf<int32_t> k_ptr, k_idx;         // K = dF/dphi_f (n_st rows, reduced columns)
+    up3d::DBuf<double> k_val;
+    up3d::DBuf<int32_t> te_ptr, te_up, te_lo; // Kutta probes per station, TE order
+    up3d::DBuf<double> taper;                 // n_st
+    up3d::DBuf<double> vals0, V;              // far-field basis (n_dir, n_dir x n_st row-major)
+    bool has_farfield = false;
+    mutable up3d::DBuf<double> u_red, u_cut, y_cut, t;
+};
+
+namespace up3d {
+namespace {
+
+// t[s] = sum_q K[s, q] x[col q] (+ g[s]), one thread per station
+__global__ void k_kutta_rows(int32_t n_st, const int32_t* __restrict__ kp, const int32_t* __restrict__ ki,
+                             const double* __restrict__ kv, const double* __restrict__ x,
+                             const double* __restrict__ g, double* __restrict__ t) {
+    for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_st; s += gridDim.x * blockDim.x) {
+        double a = 0.0;
+        for (int32_t q = kp[s]; q < kp[s + 1]; ++q) a = radd(a, rmul(kv[q], x[ki[q]]));
+        t[s] = g ? radd(a, g[s]) : a;
+    }
+}
+
+// u[i] = x[i] on free rows; on far-field row dir[k]: (vals0[k] +) V[k, :] t
+__global__ void k_farfield_fill(int64_t n_red, int64_t n_dir, int32_t n_st, const int32_t* __restrict__ dir,
+                                const uint8_t* __restrict__ mask, const double* __restrict__ vals0,
+                                const double* __restrict__ V, const double* __restrict__ t,
+                                const double* __restrict__ x, double* __restrict__ u) {
+    GRID_STRIDE(i, n_red + n_dir) {
+        if (i < n_red) {
+            if (!mask[i]) u[i] = x[i];
+        } else {
+            const int64_t k = i - n_red;
+            double a = 0.0;
+            for (int32_t j = 0; j < n_st; ++j) a = radd(a, rmul(V[k * n_st + j], t[j]));
+            u[dir[k]] = vals0 ? radd(vals0[k], a) : a;
+        }
+    }
+}
+
+// y = T^T b on free rows (the row itself, then its slaves ascending: the
+// order of the reference's T.T @ b); far-field rows take xdir (0 if NULL)
+__global__ void k_wake_fold(int64_t n_red, const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ t_idx,
+                            const uint8_t* __restrict__ mask, const double* __restrict__ b,
+                            const double* __restrict__ xdir, double* __restrict__ y) {
+    GRID_STRIDE(r, n_red) {
+        if (mask[r]) {
+            y[r] = xdir ? xdir[r] : 0.0;
+        } else {
+            double a = radd(0.0, b[r]);
+            for (int32_t q = t_ptr[r]; q < t_ptr[r + 1]; ++q) a = radd(a, b[t_idx[q]]);
+            y[r] = a;
+        }
+    }
+}
+
+// F[s] = taper[s] * (sum over the station's TE probes of phi[up] - phi[lo])
+//        / count - Gamma[s]   (kutta_targets, constraints/wake.py:196-212,
+// as used by eval_residual, solve/newton.py:417-419)
+__global__ void k_kutta_residual(int32_t n_st, const int32_t* __restrict__ te_ptr, const int32_t* __restrict__ up,
+                                 const int32_t* __restrict__ lo, const double* __restrict__ taper,
+                                 const double* __restrict__ phi, const double* __restrict__ gamma,
+                                 double* __restrict__ F) {
+    for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_st; s += gridDim.x * blockDim.x) {
+        double a = 0.0;
+        for (int32_t q = te_ptr[s]; q < te_ptr[s + 1]; ++q) a = radd(a, rsub(phi[up[q]], phi[lo[q]]));
+        const double mean = __ddiv_rn(a, (double)(te_ptr[s + 1] - te_ptr[s]));
+        F[s] = rsub(rmul(taper[s], mean), gamma[s]);
+    }
+}
+
+}  // namespace
+
+int64_t coupled_rows(const up3d_coupled* c) { return c->n_red; }
+
+void coupled_apply(const up3d_coupled* c, const up3d_csr& J, const up3d_csr& extra, const double* x,
+                   const double* g, double* y, double* t_out, cudaStream_t s) {
+    UP3D_REQUIRE(c->has_farfield, UP3D_ERR_VALUE, "coupled operator: far-field basis not set");
+    UP3D_REQUIRE(J.n == c->n_cut && J.indptr && J.indices && J.data, UP3D_ERR_ARGUMENT,
+                 "coupled operator: J must be the cut-mesh operator (n_cut rows)");
+    const up3d_wake* w = c->wake;
+    double* t = t_out ? t_out : c->t.get();
+    if (c->n_st > 0) {
+        k_kutta_rows<<<1, 128, 0, s>>>(c->n_st, c->k_ptr.get(), c->k_idx.get(), c->k_val.get(), x, g, t);
+        UP3D_CHECK_LAUNCH();
+    }
+    k_farfield_fill<<<grid_for(c->n_red + c->n_dir, 256), 256, 0, s>>>(
+        c->n_red, c->n_dir, c->n_st, c->dir.get(), c->mask.get(), nullptr, c->V.get(), t, x, c->u_red.get());
+    UP3D_CHECK_LAUNCH();
+    k_wake_expand<<<grid_for(w->n_red + w->n_dup, 256), 256, 0, s>>>(w->n_red, w->n_dup, w->slave.get(),
+                                                                     w->master.get(), w->station.get(),
+                                                                     c->u_red.get(), t, c->u_cut.get());
+    UP3D_CHECK_LAUNCH();
+    launch_spmv2<double>(J.n, J.indptr, J.indices, J.data, extra.indptr, extra.indices, extra.data, c->u_cut.get(),
+                         c->y_cut.get(), nullptr, s);
+    k_wake_fold<<<grid_for(c->n_red, 256), 256, 0, s>>>(c->n_red, w->t_ptr.get(), w->t_idx.get(), c->mask.get(),
+                                                        c->y_cut.get(), x, y);
+    UP3D_CHECK_LAUNCH();
+}
+
+}  // namespace up3d
+
+extern "C" {
+
+int up3d_coupled_create(const up3d_wake* w, int64_t n_dir, const int64_t* dir_nodes, const int64_t* k_indptr,
+                        const int64_t* k_cols, const double* k_vals, int64_t n_te, const int64_t* te_station,
+                        const int64_t* kutta_upper, const int64_t* kutta_lower, const double* taper,
+                        up3d_coupled** out) {
+    return guarded([&] {
+        UP3D_REQUIRE(w && out && (n_dir == 0 || dir_nodes) && k_indptr && (n_te == 0 || (te_station && kutta_upper
+                     && kutta_lower)) && (w->n_st == 0 || taper), UP3D_ERR_ARGUMENT,
+                     "up3d_coupled_create: null argument");
+        UP3D_REQUIRE(n_dir >= 0 && n_dir <= w->n_red && n_te >= 0, UP3D_ERR_VALUE, "up3d_coupled_create: bad sizes");
+        UP3D_CUDA(cudaSetDevice(w->device));
+        auto c = std::make_unique<up3d_coupled>();
+        c->wake = w;
+        c->n_red = w->n_red;
+        c->n_cut = w->n_cut;
+        c->n_dir = n_dir;
+        c->n_st = w->n_st;
+        const int32_t n_st = w->n_st;
+        std::vector<uint8_t> mask(w->n_red, 0);
+        std::vector<int32_t> dir(n_dir);
+        for (int64_t k = 0; k < n_dir; ++k) {
+            UP3D_REQUIRE(dir_nodes[k] >= 0 && dir_nodes[k] < w->n_red && !mask[dir_nodes[k]], UP3D_ERR_VALUE,
+                         "up3d_coupled_create: far-field rows must be distinct reduced ids");
+            mask[dir_nodes[k]] = 1;
+            dir[k] = (int32_t)dir_nodes[k];
+        }
+        UP3D_REQUIRE(k_indptr[0] == 0, UP3D_ERR_VALUE, "up3d_coupled_create: K indptr[0] must be 0");
+        for (int32_t s = 0; s < n_st; ++s)
+            UP3D_REQUIRE(k_indptr[s + 1] >= k_indptr[s], UP3D_ERR_VALUE, "up3d_coupled_create: K indptr not monotone");
+        const int64_t k_nnz = k_indptr[n_st];
+        UP3D_REQUIRE(k_nnz == 0 || (k_cols && k_vals), UP3D_ERR_ARGUMENT, "up3d_coupled_create: null K");
+        std::vector<int32_t> kp(n_st + 1), ki(k_nnz);
+        for (int32_t s = 0; s <= n_st; ++s) kp[s] = (int32_t)k_indptr[s];
+        for (int64_t q = 0; q < k_nnz; ++q) {
+            UP3D_REQUIRE(k_cols[q] >= 0 && k_cols[q] < w->n_red && !mask[k_cols[q]], UP3D_ERR_VALUE,
+                         "up3d_coupled_create: K columns must be free reduced ids");
+            ki[q] = (int32_t)k_cols[q];
+        }
+        // TE probes grouped by station, each group in TE order
+        std::vector<int32_t> tp(n_st + 1, 0), tu(n_te), tl(n_te);
+        for (int64_t q = 0; q < n_te; ++q) {
+            UP3D_REQUIRE(te_station[q] >= 0 && te_station[q] < n_st, UP3D_ERR_VALUE,
+                         "up3d_coupled_create: TE station out of range");
+            UP3D_REQUIRE(kutta_upper[q] >= 0 && kutta_upper[q] < w->n_red && kutta_lower[q] >= 0 &&
+                             kutta_lower[q] < w->n_red,
+                         UP3D_ERR_VALUE, "up3d_coupled_create: Kutta probes must be original nodes");
+            ++tp[te_station[q] + 1];
+        }
+        for (int32_t s = 0; s < n_st; ++s) {
+            UP3D_REQUIRE(tp[s + 1] > 0, UP3D_ERR_VALUE, "up3d_coupled_create: a station without TE probes");
+            tp[s + 1] += tp[s];
+        }
+        std::vector<int32_t> fill(tp.begin(), tp.end() - 1);
+        for (int64_t q = 0; q < n_te; ++q) {
+            const int32_t at = fill[te_station[q]]++;
+            tu[at] = (int32_t)kutta_upper[q];
+            tl[at] = (int32_t)kutta_lower[q];
+        }
+        upload(c->dir, dir);
+        upload(c->mask, mask);
+        upload(c->k_ptr, kp);
+        upload(c->k_idx, ki);
+        upload(c->k_val, std::vector<double>(k_vals, k_vals + k_nnz));
+        upload(c->te_ptr, tp);
+        upload(c->te_up, tu);
+        upload(c->te_lo, tl);
+        upload(c->taper, std::vector<double>(taper, taper + n_st));
+        c->u_red.alloc(c->n_red);
+        c->u_cut.alloc(c->n_cut);
+        c->y_cut.alloc(c->n_cut);
+        c->t.alloc(std::max<int64_t>(n_st, 1));
+        *out = c.release();
+    });
+}
+
+int up3d_coupled_destroy(up3d_coupled* c) {
+    return guarded([&] { delete c; });
+}
+
+int up3d_coupled_set_farfield(up3d_coupled* c, const double* vals0, const double* V) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && (c->n_dir == 0 || vals0) && (c->n_dir * c->n_st == 0 || V), UP3D_ERR_ARGUMENT,
+                     "up3d_coupled_set_farfield: null argument");
+        UP3D_CUDA(cudaSetDevice(c->wake->device));
+        upload(c->vals0, std::vector<double>(vals0, vals0 + c->n_dir));
+        upload(c->V, std::vector<double>(V, V + c->n_dir * c->n_st));
+        c->has_farfield = true;
+    });
+}
+
+int up3d_coupled_dirichlet(const up3d_coupled* c, const uint8_t** mask) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && mask, UP3D_ERR_ARGUMENT, "up3d_coupled_dirichlet: null argument");
+        *mask = c->mask.get();
+    });
+}
+
+int up3d_coupled_state(const up3d_coupled* c, const double* phi_f, const double* gamma, double* phi_red,
+                       double* phi_cut, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && phi_f && phi_red && phi_cut && (c->n_st == 0 || gamma), UP3D_ERR_ARGUMENT,
+                     "up3d_coupled_state: null argument");
+        UP3D_REQUIRE(c->has_farfield, UP3D_ERR_VALUE, "up3d_coupled_state: far-field basis not set");
+        cudaStream_t s = S(stream);
+        const up3d_wake* w = c->wake;
+        k_farfield_fill<<<grid_for(c->n_red + c->n_dir, 256), 256, 0, s>>>(c->n_red, c->n_dir, c->n_st,
+                                                                           c->dir.get(), c->mask.get(),
+                                                                           c->vals0.get(), c->V.get(), gamma,
+                                                                           phi_f, phi_red);
+        UP3D_CHECK_LAUNCH();
+        k_wake_expand<<<grid_for(w->n_red + w->n_dup, 256), 256, 0, s>>>(
+            w->n_red, w->n_dup, w->slave.get(), w->master.get(), w->station.get(), phi_red, gamma, phi_cut);
+        UP3D_CHECK_LAUNCH();
+    });
+}
+
+int up3d_coupled_residual(const up3d_coupled* c, const double* R_cut, const double* phi_cut, const double* gamma,
+                          double* R_red, double* F, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && R_cut && R_red && (c->n_st == 0 || (phi_cut && gamma && F)), UP3D_ERR_ARGUMENT,
+                     "up3d_coupled_residual: null argument");
+        cudaStream_t s = S(stream);
+        const up3d_wake* w = c->wake;
+        k_wake_fold<<<grid_for(c->n_red, 256), 256, 0, s>>>(c->n_red, w->t_ptr.get(), w->t_idx.get(),
+                                                            c->mask.get(), R_cut, nullptr, R_red);
+        UP3D_CHECK_LAUNCH();
+        if (c->n_st > 0) {
+            k_kutta_residual<<<1, 128, 0, s>>>(c->n_st, c->te_ptr.get(), c->te_up.get(), c->te_lo.get(),
+                                               c->taper.get(), phi_cut, gamma, F);
+            UP3D_CHECK_LAUNCH();
+        }
+    });
+}
+
+int up3d_coupled_apply(const up3d_coupled* c, const up3d_csr* J, const up3d_csr* extra, const double* x,
+                       const double* g, double* y, double* t, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && J && x && y, UP3D_ERR_ARGUMENT, "up3d_coupled_apply: null argument");
+        up3d_csr none{};
+        coupled_apply(c, *J, extra && extra->indptr ? *extra : none, x, g, y, t, S(stream));
     });
 }
 

@@ -1,0 +1,552 @@
+"""Wake-coupled (lifting) Newton solve on the B200.
+
+``NewtonWorkspace`` and ``solve_newton_lifting`` keep the signatures of
+pyfp3d/solve/newton.py:97-1141 for the "probe" Kutta estimator: the
+unknowns are the free reduced potentials phi_f and the station
+circulations Gamma; far-field values are affine in Gamma (set_mach's basis
+vals0 + V Gamma); the wake sheet's "+"-side copies follow
+phi_cut = T phi_red + G Gamma.  Each Newton step eliminates the Kutta rows
+(F = taper * kutta_targets(phi_cut) - Gamma, dF/dphi_f = K,
+dF/dGamma = -I) and solves
+
+    (J_ff + B K) dphi = -R_f - B F,   dGamma = K dphi + F,
+
+with B = J_red[free, dir] V + H_J[free], by GMRES(60) preconditioned with
+smoothed-aggregation AMG on the reduced Picard block.  On the device none of
+J_red, J_ff or B is formed: the coupled operator is one expand, one SpMV of
+the cut-mesh Jacobian (Term 3 included) and one fold (up3d_coupled_apply),
+so the same cut-mesh Jacobian the fused evaluation writes serves the
+solve.  Vectors are reduced-size CUDA tensors with the far-field rows
+carried as identity rows; only norms and monitors return to the host.
+
+Not built: the "pressure" Kutta estimator (constraints/te_pressure.py),
+precond="direct" / "ilu" (host sparse LU), and the Picard warm start
+(solve_subsonic_lifting) -- pass n_picard_seed=0 or phi_init.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Dict, Optional
+
+import numpy as np
+
+from .. import _lib as L
+from ..constraints.dirichlet import FarfieldBasis, freestream_phi, kutta_row
+from ..constraints.wake import WakeConstraint
+from ..mesh.device import DeviceCSR, device_view, get_mesh
+from .fused import FlowParams, ResidualJacobian
+from .linear import _csr_struct, amg_for
+from .newton import _ew_forcing
+
+
+class CoupledOperator:
+    """J_ff + B K of one Newton step (the cut-mesh Jacobian J bound to a
+    workspace's coupled handle)."""
+
+    def __init__(self, ws: "NewtonWorkspace", J: DeviceCSR):
+        self.ws = ws
+        self.J = J
+        self.shape = (ws.n_red, ws.n_red)
+        self._c = _csr_struct(J, None)
+
+    def apply(self, x, g=None):
+        """(J_ff x + B (K x + g), K x + g), reduced-size x (far-field rows
+        pass through)."""
+        t = L.torch()
+        y = t.empty(self.ws.n_red, dtype=t.float64, device="cuda")
+        tv = t.empty(max(self.ws.n_st, 1), dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_apply", self.ws._coupled, ctypes.byref(self._c), None, x.data_ptr(),
+               L.ptr(g), y.data_ptr(), tv.data_ptr(), L.stream_ptr())
+        return y, tv[:self.ws.n_st]
+
+    def matvec(self, x):
+        return self.apply(x)[0]
+
+    __matmul__ = matvec
+
+    def solve(self, b, M=None, rtol=1e-5, atol=0.0, restart=60, maxiter=10, x0=None):
+        """GMRES on this operator (up3d_gmres_coupled): (x, inner steps,
+        info) with info 0 when converged."""
+        t = L.torch()
+        x = t.zeros_like(b) if x0 is None else x0.clone()
+        inner, resid, info = ctypes.c_int64(), ctypes.c_double(), ctypes.c_int()
+        L.call("up3d_gmres_coupled", self.ws._coupled, ctypes.byref(self._c), None, b.data_ptr(),
+               x.data_ptr(), float(rtol), float(atol), int(restart), int(maxiter),
+               None if M is None else M.handle, ctypes.byref(inner), ctypes.byref(resid),
+               ctypes.byref(info), L.stream_ptr())
+        return x, int(inner.value), int(info.value)
+
+
+class NewtonWorkspace:
+    """Per-case device state of the coupled Newton solve
+    (pyfp3d/solve/newton.py:97-324): the cut mesh and its fused evaluator,
+    the wake fold, the far-field split, the Kutta row K and, per Mach level,
+    the far-field basis."""
+
+    TUNE_MIN_TETS = 100_000
+
+    def __init__(self, mesh_cut, wc, alpha_deg: float = 0.0, u_inf: float = 1.0,
+                 gamma_air: float = 1.4, vortex_center=(0.25, 0.0),
+                 farfield_spanwise_gamma: bool = False, tip_taper=None,
+                 kutta_estimator: str = "probe", external_rhs=None, tune: bool = True):
+        t = L.require_cuda()
+        if kutta_estimator != "probe":
+            raise NotImplementedError("the device workspace implements the 'probe' Kutta estimator; "
+                                      "the 'pressure' estimator (constraints/te_pressure.py) is not built")
+        self.mesh_cut, self.wc = mesh_cut, wc
+        self.alpha_deg, self.u_inf, self.gamma_air = float(alpha_deg), float(u_inf), float(gamma_air)
+        self.vortex_center = tuple(vortex_center)
+        self.spanwise = bool(farfield_spanwise_gamma)
+        self.kutta_estimator = kutta_estimator
+        n_st = wc.n_stations
+        self.tip_taper = (np.ones(n_st) if tip_taper is None
+                          else np.asarray(tip_taper, dtype=np.float64).copy())
+        if self.tip_taper.shape != (n_st,):
+            raise ValueError(f"tip_taper must be ({n_st},), got {self.tip_taper.shape}")
+        nodes = np.asarray(mesh_cut.nodes, dtype=np.float64)
+        self.mesh = get_mesh(nodes, mesh_cut.elements)
+        self.ev = ResidualJacobian(self.mesh)
+        from ..kernels.jacobian import PicardOperator
+        self.op = PicardOperator(t.as_tensor(nodes), t.as_tensor(np.asarray(self.mesh.elements)))
+        self.external_rhs = None
+        if external_rhs is not None:
+            b = np.asarray(external_rhs, dtype=np.float64)
+            if b.shape != (len(nodes),):
+                raise ValueError(f"external_rhs must be ({len(nodes)},) on the cut mesh, got {b.shape}")
+            self.external_rhs = L.to_device(b, t.float64)
+        # the wake fold on the cut mesh's P1 pattern (the Picard block's)
+        A0 = self.op.assemble_matrix(t.ones(self.mesh.n_tets, dtype=t.float64, device="cuda"))
+        self.con = WakeConstraint(A0, wc)
+        self._plan = self.con._plan            # keeps the wake handle alive
+        self.n_red, self.n_st = self.con.n_reduced, n_st
+        # far-field split (Gamma-, rho- and beta-independent) and the Kutta row
+        self.basis = FarfieldBasis(mesh_cut, wc, self.alpha_deg, self.u_inf, self.vortex_center,
+                                   self.spanwise)
+        self.dir_red, self.free = self.basis.dir_red, self.basis.free
+        self.n_free = len(self.free)
+        K = self.K = kutta_row(wc, self.basis.is_dir, self.tip_taper)
+        h = ctypes.c_void_p()
+        dr = np.ascontiguousarray(self.dir_red, dtype=np.int64)
+        kp = np.ascontiguousarray(K.indptr, dtype=np.int64)
+        kc = np.ascontiguousarray(K.indices, dtype=np.int64)
+        kv = np.ascontiguousarray(K.data, dtype=np.float64)
+        ts = np.ascontiguousarray(wc.te_station, dtype=np.int64)
+        ku = np.ascontiguousarray(wc.kutta_upper, dtype=np.int64)
+        kl = np.ascontiguousarray(wc.kutta_lower, dtype=np.int64)
+        tp = np.ascontiguousarray(self.tip_taper, dtype=np.float64)
+        L.call("up3d_coupled_create", self._plan.handle, len(dr), dr.ctypes.data, kp.ctypes.data,
+               kc.ctypes.data, kv.ctypes.data, len(ts), ts.ctypes.data, ku.ctypes.data, kl.ctypes.data,
+               tp.ctypes.data, ctypes.byref(h))
+        self._coupled = h.value
+        mp = ctypes.c_void_p()
+        L.call("up3d_coupled_dirichlet", self._coupled, ctypes.byref(mp))
+        self.mask = device_view(mp.value, (self.n_red,), np.uint8)
+        self.m_inf = self.beta = self.vals0_red = self.V_red = None
+        self.amg = None
+        if tune and self.mesh.n_tets >= self.TUNE_MIN_TETS and self.mesh.tuning()["elem_us"] == 0.0:
+            fs = L.to_device(freestream_phi(nodes, self.alpha_deg, self.u_inf), t.float64)
+            self.mesh.autotune(fs, FlowParams(m_inf=0.7, u_inf=self.u_inf))
+
+    def __del__(self):
+        h = getattr(self, "_coupled", None)
+        if h:
+            try:
+                L.lib().up3d_coupled_destroy(h)
+            except Exception:
+                pass
+            self._coupled = None
+
+    def set_mach(self, m_inf: float) -> None:
+        """Prandtl-Glauert beta and the far-field basis vals0 + V Gamma
+        (newton.py:295-324)."""
+        if not 0.0 <= m_inf < 1.0:
+            raise ValueError(f"Newton driver needs 0 <= M_inf < 1, got {m_inf}")
+        self.m_inf = float(m_inf)
+        self.beta = float(np.sqrt(1.0 - m_inf ** 2))
+        self.vals0_red, self.V_red = self.basis.at_mach(self.beta)
+        v0c = np.ascontiguousarray(self.vals0_red)
+        Vc = np.ascontiguousarray(self.V_red)
+        L.call("up3d_coupled_set_farfield", self._coupled, v0c.ctypes.data, Vc.ctypes.data)
+
+    def flow(self, upwind_c=1.5, m_crit=0.95, m_cap=3.0, rho_floor=0.05) -> FlowParams:
+        return FlowParams(m_inf=self.m_inf, gamma=self.gamma_air, u_inf=self.u_inf, m_cap=m_cap,
+                          m_crit=m_crit, upwind_c=upwind_c, rho_floor=rho_floor)
+
+    def eval_residual(self, phi_f, gamma, upwind_c: float, m_crit: float, m_cap: float,
+                      rho_floor: float, frozen=None, jacobian: bool = False):
+        """(R_f, F, state) at (phi_f, Gamma) (newton.py:326-428): phi_f a
+        reduced-size CUDA tensor (far-field rows ignored), R_f reduced-size
+        with zeros on the far-field rows.  jacobian=True also leaves the
+        cut-mesh Jacobian in the evaluator (assemble_coupled reads it)."""
+        t = L.torch()
+        phi_f = L.to_device(phi_f, t.float64)
+        g = L.to_device(np.atleast_1d(gamma) if not L.is_torch(gamma) else gamma, t.float64)
+        phi_red = t.empty(self.n_red, dtype=t.float64, device="cuda")
+        phi_cut = t.empty(self.mesh.n_nodes, dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_state", self._coupled, phi_f.data_ptr(), g.data_ptr(), phi_red.data_ptr(),
+               phi_cut.data_ptr(), L.stream_ptr())
+        flow = self.flow(upwind_c, m_crit, m_cap, rho_floor)
+        self.ev.evaluate(phi_cut, flow, jacobian=jacobian, frozen=frozen, keep_state=True)
+        R_cut = self.ev.R if self.external_rhs is None else self.ev.R - self.external_rhs
+        R_red = t.empty(self.n_red, dtype=t.float64, device="cuda")
+        F = t.empty(max(self.n_st, 1), dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_residual", self._coupled, R_cut.data_ptr(), phi_cut.data_ptr(), g.data_ptr(),
+               R_red.data_ptr(), F.data_ptr(), L.stream_ptr())
+        mon = self.ev.read_monitors()
+        state = {"phi_red": phi_red, "phi_cut": phi_cut, "gamma": g, "flow": flow, "frozen": frozen,
+                 "n_limited": mon["n_limited"], "n_floored": mon["n_floored"], "nu_max": mon["nu_max"],
+                 "n_nu_active": mon["n_supersonic"], "n_term3_active": mon["n_term3_active"],
+                 "jacobian": jacobian}
+        return R_red, F[:self.n_st], state
+
+    def assemble_coupled(self, state, upwind_c: float = 1.5, m_crit: float = 0.95,
+                         rho_floor: float = 0.05, frozen=None) -> CoupledOperator:
+        """The coupled operator J_ff + B K at the state of eval_residual
+        (newton.py:430-457): the evaluation is redone with the Jacobian
+        unless it already produced it."""
+        if not state.get("jacobian"):
+            self.ev.evaluate(state["phi_cut"], state["flow"], jacobian=True, frozen=frozen, keep_state=True)
+            state["jacobian"] = True
+            state["n_term3_active"] = self.ev.read_monitors()["n_term3_active"]
+        return CoupledOperator(self, self.ev.jacobian())
+
+    def kutta_blocks(self, state, F):
+        """(K, F) of the probe estimator (newton.py:459-502): dF/dGamma = -I."""
+        return self.K, F
+
+    def picard_block(self) -> DeviceCSR:
+        """T^T A(rho_tilde) T with the far-field mask: the AMG source
+        (newton.py:1013-1022), rho_tilde of the last evaluation."""
+        A = self.op.assemble_matrix(self.ev.rho_tilde)
+        A_red, _ = self.con.reduce_operator(A)
+        A_red.dirichlet = self.mask
+        A_red.extra = None
+        return A_red
+
+    def freeze(self, state):
+        """(upstream, branch) at the state (kernels/upwind.py:821-843)."""
+        from ..kernels.upwind import UpwindOperator
+        from ..physics.isentropic import density_field, limit_q2_field
+        t = L.torch()
+        fl = state["flow"]
+        grad, q2 = self.op.velocities(state["phi_cut"])
+        q2l = limit_q2_field(q2 / fl.u_inf ** 2, fl.m_inf, fl.m_cap, fl.gamma)
+        rho = density_field(q2l, fl.m_inf, fl.gamma)
+        if not hasattr(self, "_upw"):
+            self._upw = UpwindOperator(t.as_tensor(np.asarray(self.mesh.nodes)),
+                                       t.as_tensor(np.asarray(self.mesh.elements)))
+        up, br = self._upw.freeze_upwind_state(grad, q2l, rho, fl.m_inf, fl.upwind_c, fl.m_crit,
+                                               fl.gamma, fl.rho_floor)
+        return up.clone(), br.clone()
+
+
+def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_inf: float = 1.0,
+                         gamma_air: float = 1.4, vortex_center=(0.25, 0.0),
+                         farfield_spanwise_gamma: bool = False, upwind_c: float = 1.5,
+                         m_crit: float = 0.95, m_cap: float = 3.0, rho_floor: float = 0.05,
+                         phi_init=None, gamma_init=None, n_picard_seed: int = 0,
+                         n_newton_max: int = 30, tol_residual: float = 1e-10,
+                         tol_gamma: float = 1e-8, ew_eta0: float = 1e-2, ew_gamma: float = 0.9,
+                         ew_eta_max: float = 1e-2, amg_rebuild_every: int = 2,
+                         precond: str = "amg", gmres_restart: int = 60, gmres_maxiter: int = 10,
+                         line_search: bool = True, tol_residual_loose: Optional[float] = None,
+                         tol_residual_rel: Optional[float] = None, accept_on_stall: bool = False,
+                         freeze_tol: Optional[float] = None,
+                         freeze_refresh_max: int = 2, freeze_max_reverts: int = 3,
+                         workspace: Optional[NewtonWorkspace] = None, tip_taper=None,
+                         kutta_estimator: str = "probe", external_rhs=None,
+                         verbose: bool = False) -> Dict[str, object]:
+    """Fully coupled (phi_red, Gamma) Newton at one Mach level
+    (pyfp3d/solve/newton.py:516-1141): Eisenstat-Walker forcing, GMRES(60)
+    with AMG on the reduced Picard block (rebuilt every amg_rebuild_every
+    steps), merit |R|^2 + |F|^2 line search with at most five halvings,
+    the level fail-fast and the optional frozen-selection finish.
+    Converged when |R_f|_inf < tol_residual and |F|_inf < tol_gamma with no
+    limited or floored element; tol_residual_loose / tol_residual_rel /
+    accept_on_stall accept an intermediate continuation level earlier
+    (after at least one step, never while frozen) as the reference does.  The Picard warm start is not built:
+    n_picard_seed must be 0 (start from phi_init, or the freestream)."""
+    t = L.require_cuda()
+    if m_inf > 0.0 and upwind_c <= 0.0:
+        raise ValueError("the Newton driver runs with the walk upwind machinery active for m_inf > 0; "
+                         "pass upwind_c > 0")
+    if precond != "amg":
+        raise NotImplementedError(f"precond={precond!r}: the device driver preconditions with AMG")
+    if n_picard_seed > 0 and phi_init is None:
+        raise NotImplementedError("the Picard warm start (solve_subsonic_lifting) is not built on the "
+                                  "device: pass n_picard_seed=0 or phi_init")
+    ws = workspace
+    if ws is None:
+        ws = NewtonWorkspace(mesh_cut, wc, alpha_deg, u_inf, gamma_air, vortex_center,
+                             farfield_spanwise_gamma, tip_taper=tip_taper,
+                             kutta_estimator=kutta_estimator, external_rhs=external_rhs)
+    elif ws.kutta_estimator != kutta_estimator:
+        raise ValueError(f"workspace was built with kutta_estimator={ws.kutta_estimator!r} but "
+                         f"{kutta_estimator!r} was requested")
+    ws.set_mach(m_inf)
+    timings = {"seed": 0.0, "assembly": 0.0, "precond": 0.0, "linsolve": 0.0, "residual": 0.0}
+
+    def clock():
+        t.cuda.synchronize()
+        return time.perf_counter()
+
+    t_wall0 = clock()
+    if phi_init is not None:
+        phi_f = (phi_init[:ws.n_red].to(device="cuda", dtype=t.float64).clone() if L.is_torch(phi_init)
+                 else L.to_device(np.asarray(phi_init, dtype=np.float64)[:ws.n_red], t.float64).clone())
+        gamma = (t.zeros(ws.n_st, dtype=t.float64, device="cuda") if gamma_init is None
+                 else L.to_device(np.atleast_1d(np.asarray(gamma_init, dtype=np.float64)), t.float64).clone())
+    else:
+        phi_f = L.to_device(freestream_phi(np.asarray(mesh_cut.nodes)[:ws.n_red], alpha_deg, u_inf),
+                            t.float64)
+        gamma = (t.zeros(ws.n_st, dtype=t.float64, device="cuda") if gamma_init is None
+                 else L.to_device(np.atleast_1d(np.asarray(gamma_init, dtype=np.float64)), t.float64).clone())
+    timings["seed"] = clock() - t_wall0
+
+    def merit_of(R, F):
+        return float(R @ R) + (float(F @ F) if ws.n_st else 0.0)
+
+    res_kw = dict(upwind_c=upwind_c, m_crit=m_crit, m_cap=m_cap, rho_floor=rho_floor)
+    residual_history, F_history, gamma_history, eta_history, newton_orders = [], [], [], [], []
+    n_gmres_total = n_gmres_stalled = 0
+    converged = False
+    accept_reason = None
+    M_pre = None
+    eta_prev = None
+    frozen = None
+    freeze_point = None
+    freeze_cooldown = 0
+    n_freeze_reverts = n_freeze_refresh = 0
+    freeze_armed = freeze_tol is not None
+    prev_live_residual = None
+    residual_unfrozen = None
+    r_level_best = np.inf
+    n_term3_last = 0
+
+    a = clock()
+    R, F, state = ws.eval_residual(phi_f, gamma, **res_kw)
+    merit = merit_of(R, F)
+    timings["residual"] += clock() - a
+
+    for it in range(n_newton_max):
+        r_norm = float(R.abs().max())
+        f_norm = float(F.abs().max()) if ws.n_st else 0.0
+        residual_history.append(r_norm)
+        F_history.append(f_norm)
+        gamma_history.append(gamma.cpu().numpy().copy())
+        if len(residual_history) >= 3:
+            r2, r1, r0 = residual_history[-1], residual_history[-2], residual_history[-3]
+            if r2 > 0 and r1 > 0 and r0 > 0 and r1 != r0:
+                newton_orders.append(float(np.log(r2 / r1) / np.log(r1 / r0)))
+        if verbose:
+            print(f"  newton {it:2d}: |R|={r_norm:.3e} |F|={f_norm:.3e} lim={state['n_limited']} "
+                  f"flr={state['n_floored']}" + (" [frozen]" if frozen is not None else ""))
+        r_level_best = min(r_level_best, r_norm)
+        clean = state["n_limited"] == 0 and state["n_floored"] == 0
+
+        if frozen is not None and freeze_point is not None:
+            if r_norm > 10.0 * freeze_point[2] or not clean:
+                phi_f, gamma = freeze_point[0].clone(), freeze_point[1].clone()
+                frozen = freeze_point = None
+                freeze_cooldown = 5
+                n_freeze_reverts += 1
+                r_level_best = np.inf
+                if n_freeze_reverts >= freeze_max_reverts:
+                    freeze_armed = False
+                R, F, state = ws.eval_residual(phi_f, gamma, **res_kw)
+                merit = merit_of(R, F)
+                continue
+        if freeze_cooldown > 0:
+            freeze_cooldown -= 1
+        if r_norm > 100.0 * r_level_best and r_norm > 1e-3:
+            break
+        live_stalled = (len(residual_history) >= 7 and r_norm < 1e-3
+                        and r_norm > 0.25 * min(residual_history[-7:-1])
+                        and r_norm < 2.0 * min(residual_history[-7:-1]))
+        if (frozen is None and freeze_armed and freeze_cooldown == 0 and m_inf > 0.0
+                and (r_norm < freeze_tol or live_stalled) and clean):
+            frozen = ws.freeze(state)
+            freeze_point = (phi_f.clone(), gamma.clone(), r_norm)
+            r_level_best = np.inf
+        accept = None
+        if f_norm < tol_gamma and clean:
+            if r_norm < tol_residual:
+                accept = "tol"
+            elif frozen is None and it > 0:
+                if tol_residual_loose is not None and r_norm < tol_residual_loose:
+                    accept = "loose_tol"
+                elif tol_residual_rel is not None and r_norm <= tol_residual_rel * residual_history[0]:
+                    accept = "rel_drop"
+                elif accept_on_stall and live_stalled:
+                    accept = "stall"
+        if accept is not None:
+            if frozen is None:
+                converged = True
+                accept_reason = accept
+                break
+            R_live, F_live, st_live = ws.eval_residual(phi_f, gamma, **res_kw)
+            residual_unfrozen = float(R_live.abs().max())
+            if residual_unfrozen < tol_residual:
+                converged = True
+                R, F, state = R_live, F_live, st_live
+                break
+            if prev_live_residual is not None and residual_unfrozen > 0.5 * prev_live_residual:
+                converged = True
+                break
+            if n_freeze_refresh >= freeze_refresh_max:
+                converged = True
+                break
+            prev_live_residual = residual_unfrozen
+            n_freeze_refresh += 1
+            frozen = ws.freeze(st_live)
+            freeze_point = (phi_f.clone(), gamma.clone(), residual_unfrozen)
+            r_level_best = np.inf
+            R, F, state = ws.eval_residual(phi_f, gamma, frozen=frozen, **res_kw)
+            merit = merit_of(R, F)
+            continue
+
+        a = clock()
+        Aop = ws.assemble_coupled(state, frozen=frozen)
+        n_term3_last = state["n_term3_active"]
+        timings["assembly"] += clock() - a
+        a = clock()
+        if M_pre is None or it % amg_rebuild_every == 0:
+            ws.amg = M_pre = amg_for(ws.picard_block(), ws.amg)
+        timings["precond"] += clock() - a
+        # rhs = -R_f - B F  (B F = the coupled operator at x = 0, g = F)
+        a = clock()
+        zero = t.zeros(ws.n_red, dtype=t.float64, device="cuda")
+        BF, _ = Aop.apply(zero, F)
+        rhs = -R - BF
+        eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev, ew_eta0, ew_gamma,
+                          ew_eta_max)
+        eta_prev = eta
+        eta_history.append(eta)
+        dphi, n_it, info = Aop.solve(rhs, M=M_pre, rtol=eta, restart=gmres_restart, maxiter=gmres_maxiter)
+        n_gmres_total += n_it
+        n_gmres_stalled += info != 0
+        dphi = dphi.masked_fill(ws.mask.bool(), 0.0)
+        _, dgamma = Aop.apply(dphi, F)             # dGamma = K dphi + F
+        timings["linsolve"] += clock() - a
+
+        lam, best, accepted = 1.0, None, False
+        a = clock()
+        for _ in range(5):
+            phi_try = phi_f + lam * dphi
+            g_try = gamma + lam * dgamma
+            R_try, F_try, st_try = ws.eval_residual(phi_try, g_try, frozen=frozen, **res_kw)
+            merit_try = merit_of(R_try, F_try)
+            if np.isfinite(merit_try) and (not line_search or merit_try <= merit):
+                accepted = True
+                break
+            if np.isfinite(merit_try) and (best is None or merit_try < best[0]):
+                best = (merit_try, lam)
+            lam *= 0.5
+        if not accepted:
+            if best is None:
+                raise RuntimeError(f"Newton line search failed at iteration {it} "
+                                   f"(merit {merit:.3e} -> {merit_try:.3e})")
+            merit_try, lam = best
+            phi_try = phi_f + lam * dphi
+            g_try = gamma + lam * dgamma
+            R_try, F_try, st_try = ws.eval_residual(phi_try, g_try, frozen=frozen, **res_kw)
+        timings["residual"] += clock() - a
+        phi_f, gamma = phi_try, g_try
+        R, F, state, merit = R_try, F_try, st_try, merit_try
+
+    timings["wall"] = clock() - t_wall0
+    if converged and accept_reason is None:
+        accept_reason = "tol"
+    return {"phi": state["phi_cut"], "gamma": gamma, "converged": converged, "accept_reason": accept_reason,
+            "n_newton": len(residual_history) - (1 if converged else 0),
+            "residual_history": residual_history, "F_history": F_history,
+            "gamma_history": gamma_history, "newton_orders": newton_orders, "eta_history": eta_history,
+            "n_gmres_total": n_gmres_total, "n_gmres_stalled": n_gmres_stalled,
+            "froze": frozen is not None, "n_freeze_refresh": n_freeze_refresh,
+            "residual_unfrozen": residual_unfrozen, "n_freeze_reverts": n_freeze_reverts,
+            "nu_max": state["nu_max"], "n_nu_active": state["n_nu_active"],
+            "n_limited": state["n_limited"], "n_floored": state["n_floored"],
+            "n_term3_active": n_term3_last, "timings": timings, "workspace": ws,
+            "kutta_estimator": ws.kutta_estimator}
+
+
+def solve_newton_transonic(mesh_cut, wc, m_inf: float, alpha_deg: float, m_start: float = 0.70,
+                           dm: float = 0.05, dm_min: float = 0.01, upwind_c: float = 1.5,
+                           m_crit: float = 0.95, upwind_c_post=None, freeze_tol: Optional[float] = 1e-6,
+                           intermediate_tol: Optional[float] = None, newton_kw: Optional[dict] = None,
+                           verbose: bool = False) -> Dict[str, object]:
+    """Upward Mach continuation of the coupled solve
+    (pyfp3d/solve/newton.py:1144-1307): every level warm-starts (phi, Gamma)
+    from the last converged one and reuses its workspace; a level that
+    fails is retried with the Mach step halved down to dm_min; with
+    intermediate_tol the original-schedule levels before the last accept
+    loosely; upwind_c_post re-solves the final level at each listed
+    upwind_c.  Level 0 starts from newton_kw's phi_init or the freestream
+    (the device driver has no Picard warm start)."""
+    from .newton import mach_schedule
+    if m_inf < m_start:
+        raise ValueError(f"upward ramp only: m_inf {m_inf} < m_start {m_start}")
+    kw = dict(newton_kw or {})
+    kw.setdefault("upwind_c", upwind_c)
+    kw.setdefault("m_crit", m_crit)
+    kw.setdefault("freeze_tol", freeze_tol)
+    kw.setdefault("n_picard_seed", 0)
+    ws = kw.pop("workspace", None)
+    t0 = time.perf_counter()
+    result, last_good = None, None
+    level_history, level_results = [], []
+    levels = mach_schedule(m_inf, m_start, dm)
+    loose = [True] * (len(levels) - 1) + [False]
+
+    def run(m, lvl_kw):
+        nonlocal ws
+        a = time.perf_counter()
+        res = solve_newton_lifting(mesh_cut, wc, m_inf=m, alpha_deg=alpha_deg, workspace=ws,
+                                   verbose=verbose, **lvl_kw)
+        ws = res["workspace"]
+        level_history.append((m, res["n_newton"], res["residual_history"][-1]))
+        level_results.append({"m": m, "upwind_c": lvl_kw["upwind_c"], "converged": res["converged"],
+                              "accept_reason": res["accept_reason"], "n_newton": res["n_newton"],
+                              "residual_history": res["residual_history"], "F_history": res["F_history"],
+                              "gamma_history": res["gamma_history"], "n_lin_iters": res["n_gmres_total"],
+                              "wall_s": time.perf_counter() - a, "timings": res["timings"]})
+        return res
+
+    i = 0
+    while i < len(levels):
+        m = levels[i]
+        lvl_kw = dict(kw)
+        if intermediate_tol is not None and loose[i]:
+            lvl_kw.update(tol_residual_loose=intermediate_tol, tol_residual_rel=1e-3, accept_on_stall=True,
+                          freeze_tol=None)
+        if last_good is not None:
+            lvl_kw.update(phi_init=last_good["phi"], gamma_init=last_good["gamma"].cpu().numpy(),
+                          n_picard_seed=0)
+        if verbose:
+            print(f"newton continuation level M = {m:.4f}")
+        result = run(m, lvl_kw)
+        if not result["converged"]:
+            m_prev = m_start if i == 0 else levels[i - 1]
+            dm_new = 0.5 * (m - m_prev)
+            if i == 0 or dm_new < dm_min:
+                break
+            levels.insert(i, m_prev + dm_new)
+            loose.insert(i, False)
+            continue
+        last_good = result
+        i += 1
+    if result["converged"] and upwind_c_post:
+        for c_post in upwind_c_post:
+            lvl_kw = dict(kw)
+            lvl_kw.update(upwind_c=c_post, phi_init=result["phi"], gamma_init=result["gamma"].cpu().numpy(),
+                          n_picard_seed=0)
+            result = run(m_inf, lvl_kw)
+            if not result["converged"]:
+                break
+    result = dict(result)
+    result["level_history"] = level_history
+    result["level_results"] = level_results
+    result["wall_total"] = time.perf_counter() - t0
+    return result
