@@ -69,6 +69,7 @@ def parse():
                    help="channel mesh of the wall-force timing ('' to skip)")
     p.add_argument("--lifting", default="100x30x25:0.7:2:40x12x10",
                    help="mesh:Mach:alpha:oracle_mesh of the wake-coupled (lifting) Newton solve ('' to skip)")
+    p.add_argument("--naca", default="1", help="NACA0012 2.5D timings ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
     return p.parse_args()
@@ -498,6 +499,82 @@ def lifting_timing(spec):
     return out
 
 
+def naca_timing():
+    """The reference's own NACA0012 2.5D meshes (read from MSH 2.2 by
+    up3d_b200.mesh.reader; arrays in tests/golden): (1) the Picard matrix
+    assembly on the medium mesh (61,788 tets), the one hot-path timing the
+    reference publishes (2.1 ms per call, colour-ordered Numba, 16 threads:
+    cases/demo/p3_subsonic/results/assembly_debt.csv), timed on the device
+    (CUDA events, median of 50) and by the oracle on the host; (2) the
+    lifting Newton on the coarse mesh cut by the reference's cut_wake at
+    the reference's own subsonic case (M0.5, alpha 1.25 deg; published
+    conforming Newton 2.716 s wall including a 1.92 s Picard seed,
+    cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:3), from the
+    freestream on the device, beside the oracle's exact-step solve."""
+    import torch
+    from oracle import oracle as O
+    from up3d_b200.constraints.dirichlet import FarfieldBasis, freestream_phi
+    from up3d_b200.kernels.jacobian import PicardOperator
+    from up3d_b200.mesh.wake_cut import load_cut
+    from up3d_b200.solve.lifting import NewtonWorkspace, solve_newton_lifting
+    golden = REPO / "tests" / "golden"
+    med = np.load(golden / "naca_medium_mesh.npz")
+    nodes, elements = med["nodes"], med["elements"]
+    op = PicardOperator(torch.as_tensor(nodes).cuda(), torch.as_tensor(elements).cuda())
+    rho = torch.rand(len(elements), dtype=torch.float64, device="cuda") + 0.5
+    for _ in range(5):
+        op.assemble_matrix(rho)
+    times = []
+    for _ in range(50):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        op.assemble_matrix(rho)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    dev_ms = float(np.median(times))
+    oop = O.PicardOperator(nodes, elements)
+    rho_h = rho.cpu().numpy()
+    oop.assemble_matrix(rho_h)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        A_h = oop.assemble_matrix(rho_h)
+    cpu_ms = (time.perf_counter() - t0) / 10 * 1e3
+    A_d = op.assemble_matrix(rho).to_scipy()
+    err = float(np.abs(A_d.data - A_h.data).max() / np.abs(A_h.data).max())
+    out = {"picard_assembly_medium": {
+        "n_tets": int(len(elements)), "n_nodes": int(len(nodes)), "device_ms": round(dev_ms, 4),
+        "device_melem_s": round(len(elements) / (dev_ms * 1e-3) / 1e6, 1),
+        "reference_published_ms": 2.1, "cpu_oracle_ms": round(cpu_ms, 3), "cpu_cores": O.num_threads(),
+        "max_rel_diff_vs_oracle": err}}
+    g = np.load(golden / "naca_coarse.npz")
+    mc, wc = load_cut(g)
+    m_inf, alpha = 0.5, 1.25
+    solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, n_picard_seed=0)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ws = NewtonWorkspace(mc, wc, alpha)
+    res = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, n_picard_seed=0, workspace=ws)
+    torch.cuda.synchronize()
+    dev_s = time.perf_counter() - t0
+    basis = FarfieldBasis(mc, wc, alpha, 1.0)
+    vals0, V = basis.at_mach(float(np.sqrt(1.0 - m_inf ** 2)))
+    t0 = time.perf_counter()
+    sysm = O.LiftingSystem(mc.nodes, mc.elements, wc, basis.dir_red, vals0, V)
+    phi0 = freestream_phi(mc.nodes[:sysm.n_red], alpha, 1.0)
+    phi_o, gam_o, hist, ok = sysm.solve(phi0[sysm.free], np.zeros(sysm.n_st), m_inf)
+    cpu_s = time.perf_counter() - t0
+    out["lifting_coarse_m05"] = {
+        "n_tets": int(len(mc.elements)), "n_stations": int(wc.n_stations), "m_inf": m_inf, "alpha_deg": alpha,
+        "device_s": round(dev_s, 4), "device_converged": bool(res["converged"]),
+        "device_n_newton": int(res["n_newton"]), "device_n_gmres": int(res["n_gmres_total"]),
+        "gamma_mean": float(res["gamma"].mean()), "reference_published_wall_s": 2.716,
+        "reference_published_note": "conforming Newton with a 5-step Picard seed (1.919 s), 16 threads",
+        "cpu_oracle_s": round(cpu_s, 3), "cpu_oracle_n_newton": len(hist) - 1, "cpu_oracle_converged": bool(ok),
+        "max_abs_phi_diff_vs_oracle": float(np.abs(res["phi"].cpu().numpy() - phi_o).max())}
+    return out
+
+
 def wall_timing(spec):
     """Wall Cp and pressure forces (post/surface.py:309-363) on the
     channel's lower wall at a pocket state, M0.8, two smoothing passes:
@@ -781,6 +858,7 @@ def run_ours(args):
     wake = wake_timing(args.wake) if args.wake else None
     wall = wall_timing(args.wall) if args.wall else None
     lifting = lifting_timing(args.lifting) if args.lifting else None
+    naca = naca_timing() if args.naca else None
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
@@ -838,6 +916,7 @@ def run_ours(args):
             "wake_elimination": wake,
             "wall_forces": wall,
             "lifting_newton": lifting,
+            "naca0012": naca,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -5,7 +5,8 @@ Usage (needs the reference source tree; it cannot run where that tree is
 absent, which is why its outputs are committed):
 
     python tests/golden/make_golden.py /path/to/UP3D [--weighted-only | --wake-only | --wall-only |
-                                                      --sides-only | --lifting-only]
+                                                      --sides-only | --lifting-only |
+                                                      --naca-only]
 
 Every array is produced by the reference's own public entry points, composed
 exactly as ``NewtonWorkspace.eval_residual`` / ``assemble_coupled`` compose
@@ -29,6 +30,7 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   per-side walks, newton_terms23_side_coo             wake/multivalued.py:456-466,
                                                       kernels/cut_assembly.py:401-488
   NewtonWorkspace, solve_newton_lifting (direct)      solve/newton.py:97-1141
+  cut_wake on the NACA0012 2.5D coarse mesh           mesh/wake_cut.py:225-441
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
@@ -472,6 +474,78 @@ def make_lifting(name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+
+NACA_CASES = {
+    # name: (M_inf, alpha_deg)
+    "m05": (0.5, 2.0),
+    "m07": (0.7, 1.0),
+}
+
+
+def make_naca(ref_root, name):
+    """The reference's NACA0012 2.5D coarse mesh (cases/meshes/
+    naca0012_2.5d/coarse.msh, MSH 2.2 binary) read with
+    up3d_b200.mesh.reader.read_mesh -- its mesh_stats checked against the
+    reference's committed coarse_stats.csv -- then cut by the reference's
+    own cut_wake (mesh/wake_cut.py:225-441) and solved by its
+    solve_newton_lifting (precond="direct", from the freestream) at two
+    flow conditions; the wall Cp and force coefficients of each solution
+    (post/surface.py:309-363).  The mesh arrays, the cut, the stats and the
+    solutions are stored: the mesh file itself is not needed afterwards."""
+    import csv
+    from types import SimpleNamespace
+    import pyfp3d.post.surface as surf
+    from pyfp3d.mesh.reader import Mesh as RefMesh
+    from pyfp3d.mesh.wake_cut import cut_wake
+    from pyfp3d.solve.newton import solve_newton_lifting
+    from up3d_b200.mesh.reader import mesh_stats, read_mesh
+    from up3d_b200.mesh.wake_cut import cut_arrays
+    base = Path(ref_root) / "cases" / "meshes" / "naca0012_2.5d"
+    mesh = read_mesh(base / "coarse.msh")
+    ref_stats = {r["metric"]: float(r["value"]) for r in csv.DictReader(open(base / "coarse_stats.csv"))}
+    st = mesh_stats(mesh)
+    for k, v in st.items():
+        assert abs(v - ref_stats[k]) <= 1e-12 * abs(ref_stats[k]), (k, v, ref_stats[k])
+    assert len(mesh.boundary_faces["wake"]) == ref_stats["n_wake_faces"]
+    rm = RefMesh()
+    rm.nodes, rm.elements = mesh.nodes, mesh.elements
+    rm.boundary_faces = dict(mesh.boundary_faces)
+    rm.element_tags, rm.tag_names, rm.name = mesh.element_tags, list(mesh.tag_names), mesh.name
+    mc, wc = cut_wake(rm)
+    arrays = {"nodes": mesh.nodes, "elements": mesh.elements,
+              "stats_keys": np.array(list(ref_stats.keys())), "stats_values": np.array(list(ref_stats.values()))}
+    for tag, faces in mesh.boundary_faces.items():
+        arrays["faces/" + tag] = np.asarray(faces, dtype=np.int64)
+    arrays.update(cut_arrays(mc, wc))
+    for case, (m_inf, alpha) in NACA_CASES.items():
+        res = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, n_picard_seed=0, precond="direct")
+        assert res["converged"], case
+        wall = np.asarray(mc.boundary_faces["wall"])
+        f = surf.wall_force_coefficients(mc.nodes, mc.elements, wall, res["phi"], alpha_deg=alpha, m_inf=m_inf)
+        pre = f"{case}/"
+        arrays.update({pre + "m_inf": np.float64(m_inf), pre + "alpha_deg": np.float64(alpha),
+                       pre + "phi": res["phi"], pre + "gamma": res["gamma"],
+                       pre + "residual_history": np.array(res["residual_history"]),
+                       pre + "n_newton": np.int64(res["n_newton"]),
+                       pre + "n_nu_active": np.int64(res["n_nu_active"]),
+                       pre + "cp_tri": np.asarray(f["cp_tri"]), pre + "cl": np.float64(f["cl"]),
+                       pre + "cd_pressure": np.float64(f["cd_pressure"])})
+        print(case, res["n_newton"], res["gamma"].mean(), f["cl"], res["n_nu_active"])
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+    # the medium mesh (61,788 tets): the mesh of the reference's one
+    # published hot-path timing (Picard matrix assembly, 2.1 ms)
+    med = read_mesh(base / "medium.msh")
+    ref_stats = {r["metric"]: float(r["value"]) for r in csv.DictReader(open(base / "medium_stats.csv"))}
+    for k, v in mesh_stats(med).items():
+        assert abs(v - ref_stats[k]) <= 1e-12 * abs(ref_stats[k]), (k, v, ref_stats[k])
+    path = HERE / "naca_medium_mesh.npz"
+    np.savez_compressed(path, nodes=med.nodes, elements=med.elements,
+                        stats_keys=np.array(list(ref_stats.keys())), stats_values=np.array(list(ref_stats.values())))
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -489,6 +563,9 @@ def main():
         return
     if "--lifting-only" in sys.argv:
         make_lifting("lifting_newton")
+        return
+    if "--naca-only" in sys.argv:
+        make_naca(ref_root, "naca_coarse")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -514,6 +591,7 @@ def main():
     make_wall("wall_forces")
     make_sides(jac, upw_mod, isen, "side_terms")
     make_lifting("lifting_newton")
+    make_naca(ref_root, "naca_coarse")
 
 
 def _weighted(jac, upw_mod, isen):

@@ -1,0 +1,37 @@
+"""Device lifting Newton on the reference's NACA0012 2.5D coarse mesh, cut
+by the reference's own cut_wake (tests/golden/naca_coarse.npz): the
+converged potential, circulation, wall Cp and lift against the reference's
+solve_newton_lifting and wall_force_coefficients (solve/newton.py:516-1141,
+post/surface.py:309-363) -- converged Cp within 1e-8."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from test_mesh_reader import naca_cut
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def naca():
+    return np.load(GOLDEN / "naca_coarse.npz")
+
+
+@pytest.mark.parametrize("case", ["m05", "m07"])
+def test_gpu_naca_lifting_matches_reference(naca, case):
+    from up3d_b200.post.surface import wall_force_coefficients
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    mc, wc = naca_cut(naca)
+    m_inf, alpha = float(naca[case + "/m_inf"]), float(naca[case + "/alpha_deg"])
+    res = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, n_picard_seed=0)
+    assert res["converged"]
+    phi = res["phi"].cpu().numpy()
+    assert np.max(np.abs(phi - naca[case + "/phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - naca[case + "/gamma"])) <= 1e-9
+    assert res["n_nu_active"] == int(naca[case + "/n_nu_active"])
+    f = wall_force_coefficients(mc.nodes, mc.elements, np.asarray(mc.boundary_faces["wall"]), res["phi"],
+                                alpha_deg=alpha, m_inf=m_inf)
+    cp = f["cp_tri"].cpu().numpy() if hasattr(f["cp_tri"], "cpu") else np.asarray(f["cp_tri"])
+    assert np.max(np.abs(cp - naca[case + "/cp_tri"])) <= 1e-8
+    assert abs(float(f["cl"]) - float(naca[case + "/cl"])) <= 1e-10

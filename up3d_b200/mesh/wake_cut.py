@@ -42,6 +42,8 @@ class WakeCut:
     te_station: np.ndarray = field(default_factory=lambda: np.empty(0, dtype=np.int64))
     kutta_upper: np.ndarray = field(default_factory=lambda: np.empty(0, dtype=np.int64))
     kutta_lower: np.ndarray = field(default_factory=lambda: np.empty(0, dtype=np.int64))
+    wake_faces_minus: np.ndarray = field(default_factory=lambda: np.empty((0, 3), dtype=np.int32))
+    wake_faces_plus: np.ndarray = field(default_factory=lambda: np.empty((0, 3), dtype=np.int32))
 
     @property
     def n_stations(self) -> int:
@@ -163,3 +165,32 @@ def channel_vortex_center(cut: CutMesh):
     exactly on the sheet's nodes (dy = 0 there)."""
     wc = cut.wc
     return (float(cut.nodes[wc.te_nodes[0], 0]), float(cut.nodes[wc.master_nodes[-1], 1]))
+
+
+_WC_ARRAYS = ("master_nodes", "slave_nodes", "free_nodes", "te_nodes", "station_z", "node_station",
+              "te_station", "kutta_upper", "kutta_lower", "wake_faces_minus", "wake_faces_plus")
+
+
+def cut_arrays(mesh_cut, wc) -> dict:
+    """A cut mesh and its WakeCut as flat arrays ("cut/nodes",
+    "cut/elements", "cut/faces/<group>", "wc/<attribute>"), for np.savez."""
+    out = {"cut/nodes": np.asarray(mesh_cut.nodes), "cut/elements": np.asarray(mesh_cut.elements),
+           "wc/n_nodes_orig": np.int64(wc.n_nodes_orig)}
+    for tag, faces in mesh_cut.boundary_faces.items():
+        out["cut/faces/" + tag] = np.asarray(faces, dtype=np.int64)
+    for k in _WC_ARRAYS:
+        out["wc/" + k] = np.asarray(getattr(wc, k))
+    return out
+
+
+def load_cut(arrays):
+    """(mesh_cut, WakeCut) from the arrays of cut_arrays (a dict or an
+    NpzFile); mesh_cut carries nodes, elements and boundary_faces."""
+    from types import SimpleNamespace
+    keys = arrays.files if hasattr(arrays, "files") else list(arrays)
+    faces = {k[len("cut/faces/"):]: np.asarray(arrays[k]) for k in keys if k.startswith("cut/faces/")}
+    mc = SimpleNamespace(nodes=np.asarray(arrays["cut/nodes"]), elements=np.asarray(arrays["cut/elements"]),
+                         boundary_faces=faces)
+    wc = WakeCut(n_nodes_orig=int(arrays["wc/n_nodes_orig"]),
+                 **{k: np.asarray(arrays["wc/" + k]) for k in _WC_ARRAYS if "wc/" + k in keys})
+    return mc, wc
