@@ -546,6 +546,68 @@ def make_naca(ref_root, name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+
+def swept_sheet_mesh():
+    """A tagged mesh with a swept, part-span wake sheet, built from the
+    bump channel 12x6x5 (seed 4): x sheared by 0.3 z, the inflow plane is
+    the "wall" (the sheet's trailing edge lies on it, one station per TE
+    node because the shear sweeps it), the outflow plane "farfield", the
+    other sides "symmetry" / "top" / "side"; the sheet is the interior
+    plane j = 3 for k <= 3 (its edge at k = 3 is an interior free edge)."""
+    from up3d_b200.mesh.reader import Mesh
+    mesh = bump_channel(12, 6, 5, amplitude=0.08, seed=4)
+    nx, ny, nz = mesh.shape
+    nodes = mesh.nodes.copy()
+    nodes[:, 0] += 0.3 * nodes[:, 2]
+    el = mesh.elements.astype(np.int64)
+    ijk = np.stack(np.unravel_index(np.arange(len(nodes)), (nx + 1, ny + 1, nz + 1)), axis=1)
+    faces = el[:, [[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]]].reshape(-1, 3)
+    key = np.sort(faces, axis=1)
+    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    bnd = faces[cnt[inv.ravel()] == 1]
+    fi = ijk[bnd]
+    groups = {}
+    for name, (axis, val) in (("wall", (0, 0)), ("farfield", (0, nx)), ("symmetry", (2, 0)), ("top", (2, nz)),
+                              ("side", (1, 0)), ("side2", (1, ny))):
+        sel = np.all(fi[:, :, axis] == val, axis=1)
+        groups[name] = bnd[sel]
+        bnd, fi = bnd[~sel], fi[~sel]
+    assert len(bnd) == 0
+    interior = faces[cnt[inv.ravel()] == 2]
+    _, first = np.unique(np.sort(interior, axis=1), axis=0, return_index=True)
+    interior = interior[np.sort(first)]
+    ii = ijk[interior]
+    groups["wake"] = interior[np.all(ii[:, :, 1] == 3, axis=1) & np.all(ii[:, :, 2] <= 3, axis=1)]
+    m = Mesh()
+    m.nodes, m.elements = nodes, mesh.elements
+    m.boundary_faces = {k: v.astype(np.int32) for k, v in groups.items()}
+    m.element_tags = np.zeros(len(m.elements), dtype=np.int32)
+    m.tag_names = ["fluid"]
+    m.name = "swept_sheet"
+    return m
+
+
+def make_swept_cut(name):
+    """The reference's cut_wake (mesh/wake_cut.py:225-594) on
+    swept_sheet_mesh(): several stations, interior free-edge nodes."""
+    from pyfp3d.mesh.reader import Mesh as RefMesh
+    from pyfp3d.mesh.wake_cut import cut_wake
+    from up3d_b200.mesh.wake_cut import cut_arrays
+    m = swept_sheet_mesh()
+    rm = RefMesh()
+    rm.nodes, rm.elements, rm.boundary_faces = m.nodes, m.elements, dict(m.boundary_faces)
+    rm.element_tags, rm.tag_names, rm.name = m.element_tags, list(m.tag_names), m.name
+    mc, wc = cut_wake(rm)
+    print("swept cut:", wc.n_stations, "stations,", len(wc.free_nodes), "free nodes,", len(wc.slave_nodes), "copies")
+    arrays = {"nodes": m.nodes, "elements": m.elements}
+    for tag, faces in m.boundary_faces.items():
+        arrays["faces/" + tag] = np.asarray(faces, dtype=np.int64)
+    arrays.update(cut_arrays(mc, wc))
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -566,6 +628,7 @@ def main():
         return
     if "--naca-only" in sys.argv:
         make_naca(ref_root, "naca_coarse")
+        make_swept_cut("swept_cut")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -592,6 +655,7 @@ def main():
     make_sides(jac, upw_mod, isen, "side_terms")
     make_lifting("lifting_newton")
     make_naca(ref_root, "naca_coarse")
+    make_swept_cut("swept_cut")
 
 
 def _weighted(jac, upw_mod, isen):

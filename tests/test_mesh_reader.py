@@ -114,3 +114,50 @@ def test_naca_medium_mesh_stats_match_reference():
     ref = dict(zip(g["stats_keys"].tolist(), g["stats_values"].tolist()))
     for k, v in mesh_stats(m).items():
         assert abs(v - ref[k]) <= 1e-12 * abs(ref[k]), k
+
+
+def test_cut_wake_matches_reference_on_naca(naca):
+    """cut_wake on the NACA mesh reproduces the reference's own cut
+    (mesh/wake_cut.py:225-441) array for array."""
+    from up3d_b200.mesh.wake_cut import cut_arrays, cut_wake
+    mc, wc = cut_wake(_mesh(naca))
+    got = cut_arrays(mc, wc)
+    ref_keys = [k for k in naca.files if k.startswith(("cut/", "wc/"))]
+    assert sorted(got) == sorted(ref_keys)
+    for k in ref_keys:
+        assert np.array_equal(np.asarray(got[k]), naca[k]), k
+
+
+def test_cut_wake_rejects_bad_sheets(naca):
+    from up3d_b200.mesh.wake_cut import cut_wake
+    m = _mesh(naca)
+    with pytest.raises(ValueError):
+        cut_wake(m, wake_tag="nope")
+    bad = _mesh(naca)
+    bad.boundary_faces["wake"] = bad.boundary_faces["wall"][:4]     # boundary faces: one owner each
+    with pytest.raises(AssertionError):
+        cut_wake(bad)
+    with pytest.raises(AssertionError):
+        cut_wake(m, upper_hint=(0.0, 0.0, 1.0))                     # sides not separable along z
+
+
+def test_cut_wake_matches_reference_on_swept_part_span_sheet():
+    """A swept, part-span sheet (several stations, interior free-edge nodes
+    kept single-valued): cut_wake reproduces the reference's cut
+    (tests/golden/swept_cut.npz)."""
+    from up3d_b200.mesh.reader import Mesh
+    from up3d_b200.mesh.wake_cut import cut_arrays, cut_wake
+    g = np.load(GOLDEN / "swept_cut.npz")
+    m = Mesh()
+    m.nodes, m.elements = g["nodes"], g["elements"]
+    m.boundary_faces = {k.split("/", 1)[1]: g[k].astype(np.int32) for k in g.files if k.startswith("faces/")}
+    m.element_tags = np.zeros(len(m.elements), dtype=np.int32)
+    m.tag_names = ["fluid"]
+    m.name = "swept_sheet"
+    mc, wc = cut_wake(m)
+    assert wc.n_stations == 3 and len(wc.free_nodes) == 13
+    got = cut_arrays(mc, wc)
+    ref_keys = [k for k in g.files if k.startswith(("cut/", "wc/"))]
+    assert sorted(got) == sorted(ref_keys)
+    for k in ref_keys:
+        assert np.array_equal(np.asarray(got[k]), g[k]), k
