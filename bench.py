@@ -510,7 +510,10 @@ def naca_timing():
     the reference's own subsonic case (M0.5, alpha 1.25 deg; published
     conforming Newton 2.716 s wall including a 1.92 s Picard seed,
     cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:3), from the
-    freestream on the device, beside the oracle's exact-step solve."""
+    freestream on the device, beside the oracle's exact-step solve; (3)
+    the nested lifting Picard on the coarse mesh at the same case
+    (published 6.247 s, 15 outer iterations, 35 linear solves:
+    a1_runs.csv:2)."""
     import torch
     from oracle import oracle as O
     from up3d_b200.constraints.dirichlet import FarfieldBasis, freestream_phi
@@ -564,6 +567,18 @@ def naca_timing():
     phi0 = freestream_phi(mc.nodes[:sysm.n_red], alpha, 1.0)
     phi_o, gam_o, hist, ok = sysm.solve(phi0[sysm.free], np.zeros(sysm.n_st), m_inf)
     cpu_s = time.perf_counter() - t0
+    from up3d_b200.solve.lifting import solve_subsonic_lifting
+    solve_subsonic_lifting(mc, wc, m_inf, alpha_deg=alpha, workspace=ws)        # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pic = solve_subsonic_lifting(mc, wc, m_inf, alpha_deg=alpha, workspace=NewtonWorkspace(mc, wc, alpha))
+    torch.cuda.synchronize()
+    out["picard_coarse_m05"] = {
+        "device_s": round(time.perf_counter() - t0, 4), "converged": bool(pic["converged"]),
+        "n_picard": int(pic["n_picard"]), "n_lin_solves": int(pic["n_solves_total"]),
+        "n_cg": int(pic["n_cg_total"]), "gamma": float(pic["gamma"].mean()),
+        "reference_published": {"wall_s": 6.247, "n_outer": 15, "n_lin_solves": 35, "n_lin_iters": 5381,
+                                "source": "cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:2"}}
     out["lifting_coarse_m05"] = {
         "n_tets": int(len(mc.elements)), "n_stations": int(wc.n_stations), "m_inf": m_inf, "alpha_deg": alpha,
         "device_s": round(dev_s, 4), "device_converged": bool(res["converged"]),

@@ -583,7 +583,8 @@ int up3d_coupled_dirichlet(const up3d_coupled* coupled, const uint8_t** mask);
 int up3d_coupled_state(const up3d_coupled* coupled, const double* phi_f, const double* gamma,
                        double* phi_red, double* phi_cut, up3d_stream stream);
 /* eval_residual's outputs (:399-419): R_red = T^T R_cut on free rows, 0 on
- * far-field rows; F = taper * kutta_targets(phi_cut) - gamma. */
+ * far-field rows; F = taper * kutta_targets(phi_cut) - gamma (F NULL: the
+ * fold alone, phi_cut and gamma unused). */
 int up3d_coupled_residual(const up3d_coupled* coupled, const double* R_cut, const double* phi_cut,
                           const double* gamma, double* R_red, double* F, up3d_stream stream);
 /* The eliminated coupled step's operator (:1029-1032, :1079):

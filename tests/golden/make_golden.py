@@ -608,6 +608,71 @@ def make_swept_cut(name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+
+def make_lifting_picard(name):
+    """The reference's nested lifting Picard (solve_subsonic_lifting,
+    solve/picard.py:420-883; pyamg swapped for scipy spilu, as in
+    make_picard) to convergence on the lifting channel's subsonic case and
+    on the NACA0012 coarse mesh at the reference's own subsonic case (M0.5,
+    alpha 1.25 deg), and its solve_newton_lifting with the default 5-step
+    Picard warm start (precond="direct") on the lifting channel."""
+    from types import SimpleNamespace
+    import scipy.sparse.linalg as spla
+    import pyfp3d.solve.linear as lin
+    from pyfp3d.mesh.wake_cut import WakeCut as RefWakeCut
+    from pyfp3d.solve.newton import solve_newton_lifting
+    from pyfp3d.solve.picard import solve_subsonic_lifting
+    from up3d_b200.mesh.wake_cut import channel_vortex_center, cut_channel_sheet, load_cut
+
+    def _ilu_preconditioner(A):
+        ilu = spla.spilu(A.tocsc(), drop_tol=1e-5, fill_factor=20.0)
+        return None, spla.LinearOperator(A.shape, matvec=ilu.solve)
+
+    def ref_wc(wc):
+        r = RefWakeCut()
+        for k in ("n_nodes_orig", "master_nodes", "slave_nodes", "free_nodes", "te_nodes", "station_z",
+                  "node_station", "te_station", "kutta_upper", "kutta_lower"):
+            setattr(r, k, getattr(wc, k))
+        return r
+
+    saved = lin.build_amg_preconditioner
+    lin.build_amg_preconditioner = _ilu_preconditioner
+    arrays = {}
+    try:
+        shape, m_inf, alpha, spanwise = LIFTING_CASES["sub"]
+        cut = cut_channel_sheet(bump_channel(*shape, amplitude=0.08, seed=3), normal="y")
+        mc = SimpleNamespace(nodes=cut.nodes, elements=cut.elements, boundary_faces=cut.boundary_faces)
+        vc = channel_vortex_center(cut)
+        runs = {"channel": (mc, ref_wc(cut.wc), m_inf, alpha, vc)}
+        g = np.load(HERE / "naca_coarse.npz")
+        nmc, nwc = load_cut(g)
+        runs["naca"] = (nmc, ref_wc(nwc), 0.5, 1.25, (0.25, 0.0))
+        for tag, (m, wc, mi, al, vcen) in runs.items():
+            res = solve_subsonic_lifting(m, wc, mi, alpha_deg=al, vortex_center=vcen)
+            assert res["converged"], tag
+            pre = f"{tag}/"
+            arrays.update({pre + "m_inf": np.float64(mi), pre + "alpha_deg": np.float64(al),
+                           pre + "vortex_center": np.array(vcen, dtype=np.float64),
+                           pre + "phi": res["phi"], pre + "gamma": res["gamma"],
+                           pre + "n_picard": np.int64(res["n_picard"]),
+                           pre + "n_solves_total": np.int64(res["n_solves_total"]),
+                           pre + "residual_history": np.array(res["residual_history"]),
+                           pre + "drho_history": np.array(res["drho_history"])})
+            print(tag, "picard", res["n_picard"], res["n_solves_total"], res["gamma"][:3])
+        res = solve_newton_lifting(mc, ref_wc(cut.wc), m_inf, alpha_deg=alpha, vortex_center=vc,
+                                   precond="direct")
+        assert res["converged"]
+        arrays.update({"channel_newton_seeded/phi": res["phi"], "channel_newton_seeded/gamma": res["gamma"],
+                       "channel_newton_seeded/n_newton": np.int64(res["n_newton"]),
+                       "channel_newton_seeded/residual_history": np.array(res["residual_history"])})
+        print("seeded newton", res["n_newton"], res["residual_history"])
+    finally:
+        lin.build_amg_preconditioner = saved
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -625,6 +690,7 @@ def main():
         return
     if "--lifting-only" in sys.argv:
         make_lifting("lifting_newton")
+        make_lifting_picard("lifting_picard")
         return
     if "--naca-only" in sys.argv:
         make_naca(ref_root, "naca_coarse")
@@ -656,6 +722,7 @@ def main():
     make_lifting("lifting_newton")
     make_naca(ref_root, "naca_coarse")
     make_swept_cut("swept_cut")
+    make_lifting_picard("lifting_picard")
 
 
 def _weighted(jac, upw_mod, isen):

@@ -546,14 +546,14 @@ int up3d_coupled_state(const up3d_coupled* c, const double* phi_f, const double*
 int up3d_coupled_residual(const up3d_coupled* c, const double* R_cut, const double* phi_cut, const double* gamma,
                           double* R_red, double* F, up3d_stream stream) {
     return guarded([&] {
-        UP3D_REQUIRE(c && R_cut && R_red && (c->n_st == 0 || (phi_cut && gamma && F)), UP3D_ERR_ARGUMENT,
+        UP3D_REQUIRE(c && R_cut && R_red && (!F || c->n_st == 0 || (phi_cut && gamma)), UP3D_ERR_ARGUMENT,
                      "up3d_coupled_residual: null argument");
         cudaStream_t s = S(stream);
         const up3d_wake* w = c->wake;
         k_wake_fold<<<grid_for(c->n_red, 256), 256, 0, s>>>(c->n_red, w->t_ptr.get(), w->t_idx.get(),
                                                             c->mask.get(), R_cut, nullptr, R_red);
         UP3D_CHECK_LAUNCH();
-        if (c->n_st > 0) {
+        if (F && c->n_st > 0) {
             k_kutta_residual<<<1, 128, 0, s>>>(c->n_st, c->te_ptr.get(), c->te_up.get(), c->te_lo.get(),
                                                c->taper.get(), phi_cut, gamma, F);
             UP3D_CHECK_LAUNCH();

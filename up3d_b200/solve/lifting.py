@@ -19,9 +19,11 @@ so the same cut-mesh Jacobian the fused evaluation writes serves the
 solve.  Vectors are reduced-size CUDA tensors with the far-field rows
 carried as identity rows; only norms and monitors return to the host.
 
-Not built: the "pressure" Kutta estimator (constraints/te_pressure.py),
-precond="direct" / "ilu" (host sparse LU), and the Picard warm start
-(solve_subsonic_lifting) -- pass n_picard_seed=0 or phi_init.
+``solve_subsonic_lifting`` is the nested lifting Picard
+(pyfp3d/solve/picard.py:420-883), also the Newton driver's warm start.
+
+Not built: the "pressure" Kutta estimator (constraints/te_pressure.py) and
+precond="direct" / "ilu" (host sparse LU).
 """
 
 from __future__ import annotations
@@ -246,12 +248,13 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
                          gamma_air: float = 1.4, vortex_center=(0.25, 0.0),
                          farfield_spanwise_gamma: bool = False, upwind_c: float = 1.5,
                          m_crit: float = 0.95, m_cap: float = 3.0, rho_floor: float = 0.05,
-                         phi_init=None, gamma_init=None, n_picard_seed: int = 0,
+                         phi_init=None, gamma_init=None, n_picard_seed: int = 5,
                          n_newton_max: int = 30, tol_residual: float = 1e-10,
                          tol_gamma: float = 1e-8, ew_eta0: float = 1e-2, ew_gamma: float = 0.9,
                          ew_eta_max: float = 1e-2, amg_rebuild_every: int = 2,
                          precond: str = "amg", gmres_restart: int = 60, gmres_maxiter: int = 10,
-                         line_search: bool = True, tol_residual_loose: Optional[float] = None,
+                         line_search: bool = True, rtol_seed: float = 1e-7,
+                         tol_residual_loose: Optional[float] = None,
                          tol_residual_rel: Optional[float] = None, accept_on_stall: bool = False,
                          freeze_tol: Optional[float] = None,
                          freeze_refresh_max: int = 2, freeze_max_reverts: int = 3,
@@ -266,17 +269,15 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     Converged when |R_f|_inf < tol_residual and |F|_inf < tol_gamma with no
     limited or floored element; tol_residual_loose / tol_residual_rel /
     accept_on_stall accept an intermediate continuation level earlier
-    (after at least one step, never while frozen) as the reference does.  The Picard warm start is not built:
-    n_picard_seed must be 0 (start from phi_init, or the freestream)."""
+    (after at least one step, never while frozen) as the reference does.
+    Start: phi_init / gamma_init, else n_picard_seed outer iterations of
+    solve_subsonic_lifting (tol_rho 1e-3, rtol_seed), else the freestream."""
     t = L.require_cuda()
     if m_inf > 0.0 and upwind_c <= 0.0:
         raise ValueError("the Newton driver runs with the walk upwind machinery active for m_inf > 0; "
                          "pass upwind_c > 0")
     if precond != "amg":
         raise NotImplementedError(f"precond={precond!r}: the device driver preconditions with AMG")
-    if n_picard_seed > 0 and phi_init is None:
-        raise NotImplementedError("the Picard warm start (solve_subsonic_lifting) is not built on the "
-                                  "device: pass n_picard_seed=0 or phi_init")
     ws = workspace
     if ws is None:
         ws = NewtonWorkspace(mesh_cut, wc, alpha_deg, u_inf, gamma_air, vortex_center,
@@ -298,6 +299,14 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
                  else L.to_device(np.asarray(phi_init, dtype=np.float64)[:ws.n_red], t.float64).clone())
         gamma = (t.zeros(ws.n_st, dtype=t.float64, device="cuda") if gamma_init is None
                  else L.to_device(np.atleast_1d(np.asarray(gamma_init, dtype=np.float64)), t.float64).clone())
+    elif n_picard_seed > 0:
+        seed = solve_subsonic_lifting(mesh_cut, wc, m_inf=m_inf, alpha_deg=alpha_deg, u_inf=u_inf,
+                                      gamma_air=gamma_air, vortex_center=vortex_center, upwind_c=upwind_c,
+                                      m_crit=m_crit, m_cap=m_cap, n_picard_max=n_picard_seed, tol_rho=1e-3,
+                                      rtol=rtol_seed, farfield_spanwise_gamma=farfield_spanwise_gamma,
+                                      workspace=ws)
+        phi_f = seed["phi"][:ws.n_red].clone()
+        gamma = L.to_device(np.atleast_1d(seed["gamma"]), t.float64).clone()
     else:
         phi_f = L.to_device(freestream_phi(np.asarray(mesh_cut.nodes)[:ws.n_red], alpha_deg, u_inf),
                             t.float64)
@@ -483,8 +492,8 @@ def solve_newton_transonic(mesh_cut, wc, m_inf: float, alpha_deg: float, m_start
     fails is retried with the Mach step halved down to dm_min; with
     intermediate_tol the original-schedule levels before the last accept
     loosely; upwind_c_post re-solves the final level at each listed
-    upwind_c.  Level 0 starts from newton_kw's phi_init or the freestream
-    (the device driver has no Picard warm start)."""
+    upwind_c.  Level 0 starts from the Picard warm start (or newton_kw's
+    phi_init)."""
     from .newton import mach_schedule
     if m_inf < m_start:
         raise ValueError(f"upward ramp only: m_inf {m_inf} < m_start {m_start}")
@@ -492,7 +501,6 @@ def solve_newton_transonic(mesh_cut, wc, m_inf: float, alpha_deg: float, m_start
     kw.setdefault("upwind_c", upwind_c)
     kw.setdefault("m_crit", m_crit)
     kw.setdefault("freeze_tol", freeze_tol)
-    kw.setdefault("n_picard_seed", 0)
     ws = kw.pop("workspace", None)
     t0 = time.perf_counter()
     result, last_good = None, None
@@ -550,3 +558,201 @@ def solve_newton_transonic(mesh_cut, wc, m_inf: float, alpha_deg: float, m_start
     result["level_results"] = level_results
     result["wall_total"] = time.perf_counter() - t0
     return result
+
+
+def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_inf: float = 1.0,
+                           gamma_air: float = 1.4, vortex_center=(0.25, 0.0), gamma_fixed=None,
+                           omega: float = 1.0, omega_gamma: float = 0.9, tol_gamma: float = 1e-8,
+                           tol_rho: float = 1e-10, n_picard_max: int = 40, rtol: float = 1e-10,
+                           maxiter: int = 3000, amg_rebuild_every: int = 4, forcing: float = 0.0,
+                           upwind_c: float = 1.5, m_crit: float = 0.95, upwind_weighted: bool = False,
+                           phi_init=None, gamma_init=None, kutta_per_outer: Optional[int] = None,
+                           m_cap: float = 3.0, omega_rho: float = 1.0, pseudo_dt: Optional[float] = None,
+                           damping_theta: Optional[float] = None, tol_residual: Optional[float] = None,
+                           farfield_spanwise_gamma: bool = False, body_source_rhs=None,
+                           workspace: Optional[NewtonWorkspace] = None,
+                           rho_floor: float = 0.05) -> Dict[str, object]:
+    """Nested lifting Picard (pyfp3d/solve/picard.py:420-883): per outer
+    iteration the upwinded density of the current potential weights the
+    stiffness matrix, reduced by the wake fold, with an AMG hierarchy
+    rebuilt every amg_rebuild_every outers; the inner loop solves the
+    free-node system by CG (warm-started when m_inf > 0, forcing gives the
+    inexact atol) for the current Gamma and updates Gamma from the Kutta
+    targets -- secant steps until |target - Gamma| < tol_gamma (at most 30),
+    or kutta_per_outer plain under-relaxed steps.  Converged when the Kutta
+    loop met tol_gamma, the density lag max|rho_new - rho| < tol_rho and
+    (with tol_residual) |T^T R|inf < tol_residual.  Matrix, right-hand
+    side, CG, density and residual run on the device; Gamma (n_stations
+    numbers) and the convergence scalars on the host.  Not built:
+    upwind_weighted, pseudo_dt, damping_theta (NotImplementedError)."""
+    t = L.require_cuda()
+    from ..physics.isentropic import mach_squared_field
+    from .linear import solve_cg
+    if not 0.0 <= m_inf < 1.0:
+        raise ValueError(f"solve_subsonic_lifting needs 0 <= M_inf < 1, got {m_inf}")
+    if pseudo_dt is not None and damping_theta is not None:
+        raise ValueError("pseudo_dt and damping_theta are mutually exclusive stabilizers -- pick one")
+    if upwind_weighted or pseudo_dt is not None or damping_theta is not None:
+        raise NotImplementedError("upwind_weighted, pseudo_dt and damping_theta are not built in the device "
+                                  "lifting Picard")
+    t_wall0 = time.perf_counter()
+    ws = workspace
+    if ws is None:
+        ws = NewtonWorkspace(mesh_cut, wc, alpha_deg, u_inf, gamma_air, vortex_center, farfield_spanwise_gamma)
+    ws.set_mach(m_inf)
+    n_red, n_st = ws.n_red, ws.n_st
+    flow = ws.flow(upwind_c if m_inf > 0.0 else 0.0, m_crit, m_cap, rho_floor)
+    mask_b = ws.mask.bool()
+    timings = {"assembly": 0.0, "precond": 0.0, "linsolve": 0.0, "residual": 0.0, "kutta": 0.0}
+
+    def clock():
+        t.cuda.synchronize()
+        return time.perf_counter()
+
+    b_fold = None
+    if body_source_rhs is not None:
+        b = np.asarray(body_source_rhs, dtype=np.float64)
+        if b.shape != (ws.mesh.n_nodes,):
+            raise ValueError(f"body_source_rhs must be ({ws.mesh.n_nodes},) on the cut mesh, got {b.shape}")
+        b_cut = L.to_device(b, t.float64)
+        b_fold = t.empty(n_red, dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_residual", ws._coupled, b_cut.data_ptr(), None, None, b_fold.data_ptr(), None,
+               L.stream_ptr())
+
+    def state_of(phi_f, g):
+        """(phi_red, phi_cut): far-field rows vals(Gamma), copies expanded."""
+        g_d = L.to_device(np.ascontiguousarray(g, dtype=np.float64), t.float64)
+        phi_red = t.empty(n_red, dtype=t.float64, device="cuda")
+        phi_cut = t.empty(ws.mesh.n_nodes, dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_state", ws._coupled, phi_f.data_ptr(), g_d.data_ptr(), phi_red.data_ptr(),
+               phi_cut.data_ptr(), L.stream_ptr())
+        return phi_red, phi_cut
+
+    def fold(v_cut):
+        out = t.empty(n_red, dtype=t.float64, device="cuda")
+        L.call("up3d_coupled_residual", ws._coupled, v_cut.data_ptr(), None, None, out.data_ptr(), None,
+               L.stream_ptr())
+        return out
+
+    probes = L.to_device(np.concatenate([wc.kutta_upper, wc.kutta_lower]).astype(np.int64), t.int64)
+    n_te = len(wc.kutta_upper)
+    counts = np.bincount(wc.te_station, minlength=n_st)
+
+    def kutta_host(phi_cut):
+        """kutta_targets (constraints/wake.py:196-212) in the reference's
+        bincount order, on the host (2 n_TE values cross)."""
+        v = phi_cut[probes].cpu().numpy()
+        return np.bincount(wc.te_station, weights=v[:n_te] - v[n_te:], minlength=n_st) / counts
+
+    def evaluate(phi_cut):
+        ws.ev.evaluate(phi_cut, flow, jacobian=False, keep_state=True)
+        return ws.ev.rho_tilde.clone(), ws.ev.read_monitors()
+
+    if gamma_fixed is not None:
+        gamma = np.broadcast_to(np.atleast_1d(np.asarray(gamma_fixed, dtype=np.float64)), (n_st,)).copy()
+    elif gamma_init is not None:
+        gamma = np.atleast_1d(np.asarray(gamma_init, dtype=np.float64)).copy()
+    else:
+        gamma = np.zeros(n_st, dtype=np.float64)
+    if phi_init is not None:
+        phi_cut = (phi_init.to(device="cuda", dtype=t.float64).clone() if L.is_torch(phi_init)
+                   else L.to_device(np.asarray(phi_init, dtype=np.float64), t.float64).clone())
+        phi_red = phi_cut[:n_red].clone()
+    else:
+        phi_cut = L.to_device(freestream_phi(np.asarray(mesh_cut.nodes), alpha_deg, u_inf), t.float64)
+        phi_red = None
+    rho_t, mon = evaluate(phi_cut)
+
+    residual_history, drho_history, gamma_history = [], [], [gamma.copy()]
+    n_cg_total = n_solves_total = 0
+    M = None
+    converged = False
+    kutta_converged = gamma_fixed is not None
+    zeros = t.zeros(n_red, dtype=t.float64, device="cuda")
+    for outer in range(n_picard_max):
+        a = clock()
+        A_cut = ws.op.assemble_matrix(rho_t)
+        A_red = ws.con.reduce_operator(A_cut)[0]
+        A_red.dirichlet = ws.mask
+        A_red.extra = None
+        timings["assembly"] += clock() - a
+        if M is None or outer % amg_rebuild_every == 0:
+            a = clock()
+            ws.amg = M = amg_for(A_red, ws.amg)
+            timings["precond"] += clock() - a
+        x0 = phi_red.masked_fill(mask_b, 0.0) if (m_inf > 0.0 and phi_red is not None) else None
+
+        def solve_for(g, x0):
+            a = clock()
+            _, u_cut = state_of(zeros, g)
+            rhs = -fold(A_cut.matvec(u_cut))
+            if b_fold is not None:
+                rhs = rhs + b_fold
+            if m_inf > 0.0 and forcing > 0.0:
+                r0 = rhs - A_red.matvec(x0, dirichlet=ws.mask) if x0 is not None else rhs
+                atol_k = forcing * float(t.linalg.vector_norm(r0))
+            else:
+                atol_k = 0.0
+            b2 = clock()
+            timings["assembly"] += b2 - a
+            x, n_it, info = solve_cg(A_red, rhs, M=M, rtol=rtol, atol=atol_k, maxiter=maxiter, x0=x0)
+            timings["linsolve"] += clock() - b2
+            if info != 0:
+                raise RuntimeError(f"CG did not converge (info={info})")
+            return state_of(x, g), n_it
+
+        n_inner = 30 if kutta_per_outer is None else kutta_per_outer
+        prev_gamma = prev_target = None
+        if gamma_fixed is not None:
+            (phi_red_new, cut_new), n_it = solve_for(gamma, x0)
+            n_cg_total += n_it
+            n_solves_total += 1
+        else:
+            for _ in range(n_inner):
+                (phi_red_new, cut_new), n_it = solve_for(gamma, x0)
+                n_cg_total += n_it
+                n_solves_total += 1
+                a = clock()
+                if m_inf > 0.0:
+                    x0 = phi_red_new.masked_fill(mask_b, 0.0)
+                target = kutta_host(cut_new)
+                kutta_converged = float(np.max(np.abs(target - gamma))) < tol_gamma
+                if not kutta_converged:
+                    if prev_gamma is None or kutta_per_outer is not None:
+                        new_gamma = gamma + omega_gamma * (target - gamma)
+                    else:
+                        dg = gamma - prev_gamma
+                        slope = np.where(np.abs(dg) > 1e-14, (target - prev_target) / np.where(dg == 0, 1, dg), 0.0)
+                        denom = 1.0 - slope
+                        relaxed = gamma + omega_gamma * (target - gamma)
+                        new_gamma = np.where(np.abs(denom) > 1e-3,
+                                             (target - slope * gamma) / np.where(denom == 0, 1, denom), relaxed)
+                    prev_gamma, prev_target = gamma, target
+                    gamma = new_gamma
+                    gamma_history.append(gamma.copy())
+                timings["kutta"] += clock() - a
+                if kutta_converged:
+                    break
+        phi_red = phi_red_new if (omega == 1.0 or phi_red is None) else phi_red + omega * (phi_red_new - phi_red)
+        phi_cut = ws.con.expand(phi_red, gamma)
+        a = clock()
+        rho_t_new, mon = evaluate(phi_cut)
+        R = ws.ev.R if b_fold is None else ws.ev.R - b_cut
+        residual_history.append(float(fold(R).abs().max()))
+        drho = float((rho_t_new - rho_t).abs().max())
+        drho_history.append(drho)
+        rho_t = rho_t_new if omega_rho == 1.0 else rho_t + omega_rho * (rho_t_new - rho_t)
+        timings["residual"] += clock() - a
+        if kutta_converged and drho < tol_rho and (tol_residual is None or residual_history[-1] < tol_residual):
+            converged = True
+            break
+
+    _, q2 = ws.op.velocities(phi_cut)
+    mach2_max = float(mach_squared_field(q2 / u_inf ** 2, m_inf, gamma_air).max())
+    timings["wall"] = time.perf_counter() - t_wall0
+    return {"phi": phi_cut, "gamma": gamma, "n_picard": len(residual_history), "converged": converged,
+            "kutta_converged": kutta_converged, "residual_history": residual_history,
+            "drho_history": drho_history, "gamma_history": gamma_history, "timings": timings, "rho": rho_t,
+            "mach2_max": mach2_max, "nu_max": mon["nu_max"], "n_nu_active": mon["n_supersonic"],
+            "n_limited": mon["n_limited"], "n_floored": mon["n_floored"], "n_cg_total": n_cg_total,
+            "n_solves_total": n_solves_total, "workspace": ws}
