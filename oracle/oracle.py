@@ -530,7 +530,8 @@ class LiftingSystem:
     """NewtonWorkspace.eval_residual / assemble_coupled / the probe
     kutta_blocks (solve/newton.py:326-502) over the oracle kernels."""
 
-    def __init__(self, nodes, elements, wc, dir_red, vals0_red, V_red, tip_taper=None, u_inf=1.0):
+    def __init__(self, nodes, elements, wc, dir_red, vals0_red, V_red, tip_taper=None, u_inf=1.0,
+                 external_rhs=None):
         self.op = PicardOperator(nodes, elements)
         self.upw = UpwindOperator(nodes, elements)
         self.wc, self.u_inf = wc, float(u_inf)
@@ -542,6 +543,7 @@ class LiftingSystem:
         self.free = np.where(~is_dir)[0]
         self.vals0_red, self.V_red = np.asarray(vals0_red), np.asarray(V_red)
         self.taper = np.ones(self.n_st) if tip_taper is None else np.asarray(tip_taper, dtype=np.float64)
+        self.b_ext = None if external_rhs is None else np.asarray(external_rhs, dtype=np.float64)
         counts = np.bincount(wc.te_station, minlength=self.n_st).astype(np.float64)
         probes = np.concatenate([wc.kutta_upper, wc.kutta_lower])
         cols = np.searchsorted(self.free, probes)
@@ -559,7 +561,7 @@ class LiftingSystem:
         phi_red[self.dir_red] = self.vals0_red + self.V_red @ gamma
         phi_cut = self.con.expand(phi_red, gamma)
         st = chain(self.op, self.upw, phi_cut, m_inf, self.u_inf, jacobian=True, **kw)
-        R_red = self.con.T.T @ st["R"]
+        R_red = self.con.T.T @ (st["R"] if self.b_ext is None else st["R"] - self.b_ext)
         F = self.taper * kutta_targets(phi_cut, self.wc) - gamma
         st.update(phi_red=phi_red, phi_cut=phi_cut)
         return R_red[self.free], F, st

@@ -461,6 +461,17 @@ def make_lifting(name):
         J_ff = J_ff.tocsr()
         Bd = B.toarray()
         xv = rng.standard_normal(ws.n_free)
+        if case == "sub":
+            # a tapered Kutta row (tip_taper) and a lagged external
+            # right-hand side (external_rhs) on the same case
+            taper = np.linspace(1.0, 0.4, ws.n_st)
+            b_ext = 1e-4 * np.sin(3.0 * cut.nodes[:, 0]) * np.cos(2.0 * cut.nodes[:, 2])
+            rt = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, vortex_center=vc,
+                                      farfield_spanwise_gamma=spanwise, n_picard_seed=0, precond="direct",
+                                      tip_taper=taper, external_rhs=b_ext)
+            assert rt["converged"]
+            arrays.update({pre + "taper": taper, pre + "external_rhs": b_ext, pre + "taper_phi": rt["phi"],
+                           pre + "taper_gamma": rt["gamma"], pre + "taper_n_newton": np.int64(rt["n_newton"])})
         arrays.update({pre + "seed_phi_free": phi_free, pre + "seed_gamma": gamma,
                        pre + "seed_R_free": R_free, pre + "seed_F": F,
                        pre + "seed_phi_cut": state["phi_cut"],

@@ -229,3 +229,17 @@ def test_gpu_lifting_newton_with_picard_seed(gold, picard_gold):
     assert res["n_newton"] <= int(picard_gold["channel_newton_seeded/n_newton"]) + 1
     assert np.max(np.abs(res["phi"].cpu().numpy() - picard_gold["channel_newton_seeded/phi"])) <= 1e-9
     assert np.max(np.abs(res["gamma"].cpu().numpy() - picard_gold["channel_newton_seeded/gamma"])) <= 1e-9
+
+
+def test_gpu_lifting_taper_and_external_rhs(gold):
+    """tip_taper scales K and F, external_rhs is subtracted before the fold:
+    the reference's converged solution with both."""
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    g, cut = _case(gold, "sub")
+    res = solve_newton_lifting(cut, cut.wc, float(g["m_inf"]), alpha_deg=float(g["alpha_deg"]),
+                               vortex_center=channel_vortex_center(cut), n_picard_seed=0,
+                               tip_taper=g["taper"], external_rhs=g["external_rhs"])
+    assert res["converged"]
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g["taper_phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g["taper_gamma"])) <= 1e-9

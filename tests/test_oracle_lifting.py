@@ -99,3 +99,18 @@ def test_oracle_lifting_solve_matches_reference(gold, name):
     assert len(hist) - 1 == int(g["sol_n_newton"])
     assert np.max(np.abs(phi - g["sol_phi"])) <= 1e-10
     assert np.max(np.abs(gamma - g["sol_gamma"])) <= 1e-10
+
+
+def test_oracle_lifting_taper_and_external_rhs_match_reference(gold):
+    """A tapered Kutta row and a lagged external right-hand side
+    (solve/newton.py:165-214, :399-419): the reference's converged solution."""
+    from up3d_b200.constraints.dirichlet import freestream_phi
+    from oracle import oracle as O
+    g, cut = _case(gold, "sub")
+    sysm = O.LiftingSystem(g["nodes"], g["elements"], cut.wc, g["dir_red"], g["vals0_red"], g["V_red"],
+                           tip_taper=g["taper"], external_rhs=g["external_rhs"])
+    phi0 = freestream_phi(g["nodes"][:sysm.n_red], float(g["alpha_deg"]), 1.0)
+    phi, gamma, hist, ok = sysm.solve(phi0[sysm.free], np.zeros(sysm.n_st), float(g["m_inf"]))
+    assert ok and len(hist) - 1 == int(g["taper_n_newton"])
+    assert np.max(np.abs(phi - g["taper_phi"])) <= 1e-10
+    assert np.max(np.abs(gamma - g["taper_gamma"])) <= 1e-10
