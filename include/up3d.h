@@ -569,6 +569,11 @@ int up3d_coupled_create(const up3d_wake* wake, int64_t n_dir, const int64_t* dir
                         int64_t n_te, const int64_t* te_station, const int64_t* kutta_upper,
                         const int64_t* kutta_lower, const double* taper, up3d_coupled** out);
 int up3d_coupled_destroy(up3d_coupled* coupled);
+/* Replaces K (HOST CSR as at creation): the pressure Kutta estimator's
+ * eliminated row -D^-1 K_p, rebuilt every Newton step (kutta_blocks,
+ * solve/newton.py:459-502).  Synchronous. */
+int up3d_coupled_set_kutta_row(up3d_coupled* coupled, const int64_t* k_indptr, const int64_t* k_cols,
+                               const double* k_vals);
 /* set_mach's affine far-field basis (solve/newton.py:295-324): far-field
  * values vals0 + V Gamma (HOST vals0 n_dir, V n_dir x n_stations row-major,
  * rows in dir_nodes order). */

@@ -684,6 +684,51 @@ def make_lifting_picard(name):
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 
+
+def make_te_pressure(name):
+    """The pressure-equality Kutta estimator (constraints/te_pressure.py,
+    TEControlVolumes) on the NACA0012 coarse cut: its control-volume
+    velocities, station residual and exact rows (Kp_cut, D) at the probe
+    solution of case m05, and solve_newton_lifting with
+    kutta_estimator="pressure" (precond="direct", from the freestream) at
+    M0.5, alpha 1.25 deg, untapered and with a tip taper."""
+    from types import SimpleNamespace
+    from pyfp3d.constraints.dirichlet import farfield_dirichlet
+    from pyfp3d.constraints.te_pressure import TEControlVolumes
+    from pyfp3d.mesh.wake_cut import WakeCut as RefWakeCut
+    from pyfp3d.solve.newton import solve_newton_lifting
+    from up3d_b200.mesh.wake_cut import load_cut
+    g = np.load(HERE / "naca_coarse.npz")
+    mc, wc0 = load_cut(g)
+    wc = RefWakeCut()
+    for k in ("n_nodes_orig", "master_nodes", "slave_nodes", "free_nodes", "te_nodes", "station_z",
+              "node_station", "te_station", "kutta_upper", "kutta_lower", "wake_faces_minus", "wake_faces_plus"):
+        setattr(wc, k, getattr(wc0, k))
+    dn, _ = farfield_dirichlet(mc, wc, 1.25, np.zeros(wc.n_stations))
+    cvs = TEControlVolumes(mc, wc, dirichlet_nodes=dn)
+    phi = g["m05/phi"]
+    qu, ql = cvs.te_velocities(phi)
+    Kp, D = cvs.newton_rows(phi)
+    Kp = Kp.tocsr()
+    arrays = {"phi": phi, "qu": qu, "ql": ql, "F_raw": cvs.residual_stations(phi),
+              "Kp_indptr": Kp.indptr.astype(np.int64), "Kp_indices": Kp.indices.astype(np.int64),
+              "Kp_data": Kp.data, "D": D, "D_frozen": cvs.gamma_jacobian(phi, mode="frozen"),
+              "implied": cvs.implied_targets(phi, g["m05/gamma"] * 0.9)}
+    for tag, taper in (("plain", None), ("taper", np.array([0.7]))):
+        res = solve_newton_lifting(mc, wc, 0.5, alpha_deg=1.25, n_picard_seed=0, precond="direct",
+                                   kutta_estimator="pressure", tip_taper=taper)
+        assert res["converged"], tag
+        arrays.update({tag + "/phi": res["phi"], tag + "/gamma": res["gamma"],
+                       tag + "/kutta_sigma": np.asarray(res["kutta_sigma"]),
+                       tag + "/n_newton": np.int64(res["n_newton"])})
+        if res["kutta_weld_sign"] is not None:
+            arrays[tag + "/kutta_weld_sign"] = np.asarray(res["kutta_weld_sign"])
+        print(tag, res["n_newton"], res["gamma"], res["kutta_sigma"])
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     jac, upw_mod, isen = import_reference(ref_root)
@@ -706,6 +751,7 @@ def main():
     if "--naca-only" in sys.argv:
         make_naca(ref_root, "naca_coarse")
         make_swept_cut("swept_cut")
+        make_te_pressure("te_pressure")
         return
 
     small = bump_channel(10, 4, 3, amplitude=0.08, seed=1)
@@ -734,6 +780,7 @@ def main():
     make_naca(ref_root, "naca_coarse")
     make_swept_cut("swept_cut")
     make_lifting_picard("lifting_picard")
+    make_te_pressure("te_pressure")
 
 
 def _weighted(jac, upw_mod, isen):

@@ -125,7 +125,9 @@ def test_gpu_lifting_rejects_unbuilt_options(gold):
     from up3d_b200.solve.lifting import NewtonWorkspace, solve_newton_lifting
     g, cut = _case(gold, "sub")
     vc = channel_vortex_center(cut)
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):
+        NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="nope")
+    with pytest.raises(ValueError):                 # the channel cut has no wall group
         NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="pressure")
     with pytest.raises(NotImplementedError):
         solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct")

@@ -41,3 +41,21 @@ def test_gpu_naca_lifting_matches_reference(naca, case):
     cp = f["cp_tri"].cpu().numpy() if hasattr(f["cp_tri"], "cpu") else np.asarray(f["cp_tri"])
     assert np.max(np.abs(cp - naca[case + "/cp_tri"])) <= 1e-8
     assert abs(float(f["cl"]) - float(naca[case + "/cl"])) <= 1e-10
+
+
+@pytest.mark.parametrize("tag", ["plain", "taper"])
+def test_gpu_naca_pressure_kutta_matches_reference(naca, tag):
+    """kutta_estimator="pressure" (constraints/te_pressure.py, the
+    eliminated step of solve/newton.py:459-502), untapered and with the
+    tip-taper blend: the reference's converged solution and frozen
+    scaling (tests/golden/te_pressure.npz)."""
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    g = np.load(GOLDEN / "te_pressure.npz")
+    mc, wc = naca_cut(naca)
+    taper = None if tag == "plain" else np.array([0.7])
+    res = solve_newton_lifting(mc, wc, 0.5, alpha_deg=1.25, n_picard_seed=0, kutta_estimator="pressure",
+                               tip_taper=taper)
+    assert res["converged"]
+    assert np.max(np.abs(res["kutta_sigma"] - g[tag + "/kutta_sigma"])) <= 1e-12 * np.max(g[tag + "/kutta_sigma"])
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g[tag + "/phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g[tag + "/gamma"])) <= 1e-9

@@ -106,6 +106,7 @@ SIGNATURES = {
     "up3d_wake_expand": (_int, [_p, _p, _p, _p, _p]),
     "up3d_coupled_create": (_int, [_p, _i64, _p, _p, _p, _p, _i64, _p, _p, _p, _p, ctypes.POINTER(_p)]),
     "up3d_coupled_destroy": (_int, [_p]),
+    "up3d_coupled_set_kutta_row": (_int, [_p, _p, _p, _p]),
     "up3d_coupled_set_farfield": (_int, [_p, _p, _p]),
     "up3d_coupled_dirichlet": (_int, [_p, ctypes.POINTER(_p)]),
     "up3d_coupled_state": (_int, [_p, _p, _p, _p, _p, _p]),

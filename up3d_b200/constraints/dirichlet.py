@@ -78,6 +78,7 @@ class FarfieldBasis:
         n_red, n_st = int(wc.n_nodes_orig), wc.n_stations
         nodes, _ = farfield_dirichlet(mesh_cut, wc, self.alpha_deg, np.zeros(n_st), self.u_inf,
                                       self.vortex_center, beta=1.0, spanwise_gamma=self.spanwise)
+        self.dir_cut = nodes                     # far-field nodes in cut-mesh ids
         self._keep = nodes < n_red
         self.dir_red, self._idx = np.unique(nodes[self._keep], return_index=True)
         is_dir = np.zeros(n_red, dtype=bool)

@@ -502,6 +502,33 @@ int up3d_coupled_create(const up3d_wake* w, int64_t n_dir, const int64_t* dir_no
     });
 }
 
+int up3d_coupled_set_kutta_row(up3d_coupled* c, const int64_t* k_indptr, const int64_t* k_cols,
+                               const double* k_vals) {
+    return guarded([&] {
+        UP3D_REQUIRE(c && k_indptr, UP3D_ERR_ARGUMENT, "up3d_coupled_set_kutta_row: null argument");
+        UP3D_CUDA(cudaSetDevice(c->wake->device));
+        const int32_t n_st = c->n_st;
+        UP3D_REQUIRE(k_indptr[0] == 0, UP3D_ERR_VALUE, "up3d_coupled_set_kutta_row: indptr[0] must be 0");
+        for (int32_t s = 0; s < n_st; ++s)
+            UP3D_REQUIRE(k_indptr[s + 1] >= k_indptr[s], UP3D_ERR_VALUE,
+                         "up3d_coupled_set_kutta_row: indptr not monotone");
+        const int64_t nnz = k_indptr[n_st];
+        UP3D_REQUIRE(nnz == 0 || (k_cols && k_vals), UP3D_ERR_ARGUMENT, "up3d_coupled_set_kutta_row: null K");
+        std::vector<uint8_t> mask(c->n_red);
+        UP3D_CUDA(cudaMemcpy(mask.data(), c->mask.get(), c->n_red, cudaMemcpyDeviceToHost));
+        std::vector<int32_t> kp(n_st + 1), ki(nnz);
+        for (int32_t s = 0; s <= n_st; ++s) kp[s] = (int32_t)k_indptr[s];
+        for (int64_t q = 0; q < nnz; ++q) {
+            UP3D_REQUIRE(k_cols[q] >= 0 && k_cols[q] < c->n_red && !mask[k_cols[q]], UP3D_ERR_VALUE,
+                         "up3d_coupled_set_kutta_row: K columns must be free reduced ids");
+            ki[q] = (int32_t)k_cols[q];
+        }
+        upload(c->k_ptr, kp);
+        upload(c->k_idx, ki);
+        upload(c->k_val, std::vector<double>(k_vals, k_vals + nnz));
+    });
+}
+
 int up3d_coupled_destroy(up3d_coupled* c) {
     return guarded([&] { delete c; });
 }

@@ -22,8 +22,11 @@ carried as identity rows; only norms and monitors return to the host.
 ``solve_subsonic_lifting`` is the nested lifting Picard
 (pyfp3d/solve/picard.py:420-883), also the Newton driver's warm start.
 
-Not built: the "pressure" Kutta estimator (constraints/te_pressure.py) and
-precond="direct" / "ilu" (host sparse LU).
+kutta_estimator="pressure" replaces the probe row by the pressure
+equality on wall-adjacent TE control volumes (constraints/te_pressure.py):
+its state-dependent eliminated row -D^-1 K_p is rebuilt on the host per
+Newton step (n_stations rows over the TE fans' nodes) and uploaded to the
+coupled handle.  Not built: precond="direct" / "ilu" (host sparse LU).
 """
 
 from __future__ import annotations
@@ -94,9 +97,8 @@ class NewtonWorkspace:
                  farfield_spanwise_gamma: bool = False, tip_taper=None,
                  kutta_estimator: str = "probe", external_rhs=None, tune: bool = True):
         t = L.require_cuda()
-        if kutta_estimator != "probe":
-            raise NotImplementedError("the device workspace implements the 'probe' Kutta estimator; "
-                                      "the 'pressure' estimator (constraints/te_pressure.py) is not built")
+        if kutta_estimator not in ("probe", "pressure"):
+            raise ValueError(f"unknown kutta_estimator {kutta_estimator!r}")
         self.mesh_cut, self.wc = mesh_cut, wc
         self.alpha_deg, self.u_inf, self.gamma_air = float(alpha_deg), float(u_inf), float(gamma_air)
         self.vortex_center = tuple(vortex_center)
@@ -129,6 +131,20 @@ class NewtonWorkspace:
         self.dir_red, self.free = self.basis.dir_red, self.basis.free
         self.n_free = len(self.free)
         K = self.K = kutta_row(wc, self.basis.is_dir, self.tip_taper)
+        self._taper_active = not np.all(self.tip_taper == 1.0)
+        # pressure estimator: TE control volumes and the frozen scaling
+        self.cvs = None
+        self.kutta_sigma = self.kutta_weld_sign = None
+        self.kutta_sigma_sign_flips = 0
+        if kutta_estimator == "pressure":
+            from ..constraints.te_pressure import TEControlVolumes
+            self.cvs = TEControlVolumes(mesh_cut, wc, dirichlet_nodes=self.basis.dir_cut,
+                                        geometry=self.mesh.geometry())
+            red_of = np.arange(len(nodes), dtype=np.int64)
+            red_of[np.asarray(wc.slave_nodes, dtype=np.int64)] = np.asarray(wc.master_nodes, dtype=np.int64)
+            import scipy.sparse as sp
+            self._T = sp.csr_matrix((np.ones(len(nodes)), (np.arange(len(nodes)), red_of)),
+                                    shape=(len(nodes), self.n_red))
         h = ctypes.c_void_p()
         dr = np.ascontiguousarray(self.dir_red, dtype=np.int64)
         kp = np.ascontiguousarray(K.indptr, dtype=np.int64)
@@ -196,6 +212,8 @@ class NewtonWorkspace:
         F = t.empty(max(self.n_st, 1), dtype=t.float64, device="cuda")
         L.call("up3d_coupled_residual", self._coupled, R_cut.data_ptr(), phi_cut.data_ptr(), g.data_ptr(),
                R_red.data_ptr(), F.data_ptr(), L.stream_ptr())
+        if self.cvs is not None:
+            F = L.to_device(self._pressure_F(phi_cut, g.cpu().numpy()), t.float64)
         mon = self.ev.read_monitors()
         state = {"phi_red": phi_red, "phi_cut": phi_cut, "gamma": g, "flow": flow, "frozen": frozen,
                  "n_limited": mon["n_limited"], "n_floored": mon["n_floored"], "nu_max": mon["nu_max"],
@@ -214,9 +232,55 @@ class NewtonWorkspace:
             state["n_term3_active"] = self.ev.read_monitors()["n_term3_active"]
         return CoupledOperator(self, self.ev.jacobian())
 
+    def _pressure_F(self, phi_cut, gamma):
+        """sigma F_raw, or with a tip taper the blend taper sigma F_raw +
+        (1 - taper) s Gamma; sigma and s frozen at the first evaluation
+        (newton.py:376-416)."""
+        F_raw = self.cvs.residual_stations(phi_cut)
+        if self.kutta_sigma is None:
+            dj = np.diag(self.cvs.gamma_jacobian(phi_cut, mode="exact"))
+            ref = np.sign(np.median(dj))
+            self.kutta_sigma_sign_flips = int(np.count_nonzero(np.sign(dj) != ref))
+            a = np.abs(dj)
+            self.kutta_sigma = 1.0 / np.maximum(a, 0.1 * np.median(a))
+            sg = np.sign(dj)
+            self.kutta_weld_sign = np.where(sg == 0.0, ref, sg)
+        if not self._taper_active:
+            return self.kutta_sigma * F_raw
+        return (self.kutta_sigma * (self.tip_taper * F_raw)
+                + (1.0 - self.tip_taper) * (self.kutta_weld_sign * gamma))
+
     def kutta_blocks(self, state, F):
-        """(K, F) of the probe estimator (newton.py:459-502): dF/dGamma = -I."""
-        return self.K, F
+        """(K, F_elim) of the eliminated step (newton.py:459-502): the probe
+        estimator's constant K and F; the pressure estimator's
+        K = -D^-1 K_p and F_elim = -D^-1 F / sigma from the exact rows at
+        this state (tip taper: D = taper D + (1 - taper) s / sigma, K_p
+        scaled by taper), uploaded to the coupled handle."""
+        if self.cvs is None:
+            return self.K, F
+        import scipy.linalg as sla
+        import scipy.sparse as sp
+        t = L.torch()
+        Kp_cut, D = self.cvs.newton_rows(state["phi_cut"])
+        Kp = (Kp_cut @ self._T).tocsr()
+        Kp.sum_duplicates()
+        Fh = F.cpu().numpy() / self.kutta_sigma
+        if self._taper_active:
+            tp = self.tip_taper
+            Kp = (sp.diags(tp) @ Kp).tocsr()
+            D = tp[:, None] * D
+            D[np.diag_indices_from(D)] += (1.0 - tp) * self.kutta_weld_sign / self.kutta_sigma
+        lu = sla.lu_factor(D)
+        F_elim = -sla.lu_solve(lu, Fh)
+        cols = np.unique(Kp.indices)
+        Kd = -sla.lu_solve(lu, Kp[:, cols].toarray())
+        n_st = self.n_st
+        kp = np.ascontiguousarray(np.arange(n_st + 1, dtype=np.int64) * len(cols))
+        kc = np.ascontiguousarray(np.tile(cols.astype(np.int64), n_st))
+        kv = np.ascontiguousarray(Kd.ravel())
+        L.call("up3d_coupled_set_kutta_row", self._coupled, kp.ctypes.data, kc.ctypes.data, kv.ctypes.data)
+        K = sp.csr_matrix((kv, kc, kp), shape=(n_st, self.n_red))
+        return K, L.to_device(F_elim, t.float64)
 
     def picard_block(self) -> DeviceCSR:
         """T^T A(rho_tilde) T with the far-field mask: the AMG source
@@ -424,10 +488,11 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
         if M_pre is None or it % amg_rebuild_every == 0:
             ws.amg = M_pre = amg_for(ws.picard_block(), ws.amg)
         timings["precond"] += clock() - a
-        # rhs = -R_f - B F  (B F = the coupled operator at x = 0, g = F)
+        # rhs = -R_f - B F_elim  (B F_elim = the coupled operator at x = 0)
         a = clock()
+        _, F_elim = ws.kutta_blocks(state, F)
         zero = t.zeros(ws.n_red, dtype=t.float64, device="cuda")
-        BF, _ = Aop.apply(zero, F)
+        BF, _ = Aop.apply(zero, F_elim)
         rhs = -R - BF
         eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev, ew_eta0, ew_gamma,
                           ew_eta_max)
@@ -437,7 +502,7 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
         n_gmres_total += n_it
         n_gmres_stalled += info != 0
         dphi = dphi.masked_fill(ws.mask.bool(), 0.0)
-        _, dgamma = Aop.apply(dphi, F)             # dGamma = K dphi + F
+        _, dgamma = Aop.apply(dphi, F_elim)        # dGamma = K dphi + F_elim
         timings["linsolve"] += clock() - a
 
         lam, best, accepted = 1.0, None, False
@@ -478,7 +543,8 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
             "nu_max": state["nu_max"], "n_nu_active": state["n_nu_active"],
             "n_limited": state["n_limited"], "n_floored": state["n_floored"],
             "n_term3_active": n_term3_last, "timings": timings, "workspace": ws,
-            "kutta_estimator": ws.kutta_estimator}
+            "kutta_estimator": ws.kutta_estimator, "kutta_sigma": ws.kutta_sigma,
+            "kutta_sigma_sign_flips": ws.kutta_sigma_sign_flips, "kutta_weld_sign": ws.kutta_weld_sign}
 
 
 def solve_newton_transonic(mesh_cut, wc, m_inf: float, alpha_deg: float, m_start: float = 0.70,
