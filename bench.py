@@ -579,6 +579,22 @@ def naca_timing():
         "n_cg": int(pic["n_cg_total"]), "gamma": float(pic["gamma"].mean()),
         "reference_published": {"wall_s": 6.247, "n_outer": 15, "n_lin_solves": 35, "n_lin_iters": 5381,
                                 "source": "cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:2"}}
+    from up3d_b200.solve.lifting import solve_newton_transonic
+    recipe = dict(m_start=0.70, dm=0.025, dm_min=0.003, freeze_tol=1e-6,
+                  newton_kw=dict(freeze_refresh_max=8, precond="direct", n_newton_max=60, n_picard_seed=0))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tr = solve_newton_transonic(mc, wc, 0.8, alpha, **recipe)
+    torch.cuda.synchronize()
+    out["transonic_coarse_m08"] = {
+        "device_s": round(time.perf_counter() - t0, 3), "converged": bool(tr["converged"]),
+        "levels": [[round(m, 4), n] for m, n, _ in tr["level_history"]],
+        "n_newton_total": int(sum(n for _, n, _ in tr["level_history"])), "gamma": float(tr["gamma"][0]),
+        "n_supersonic": int(tr["n_nu_active"]),
+        "recipe": "Mach ramp 0.70 -> 0.80 by 0.025, freeze 1e-6, exact (dense LU) steps, from the freestream",
+        "reference_published": {"wall_s": 4.712, "n_levels": 5, "n_newton": 57, "gamma": 0.233826,
+                                "note": "with a Picard warm start (2.689 s of it) and sparse LU, 16 threads",
+                                "source": "cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:7"}}
     out["lifting_coarse_m05"] = {
         "n_tets": int(len(mc.elements)), "n_stations": int(wc.n_stations), "m_inf": m_inf, "alpha_deg": alpha,
         "device_s": round(dev_s, 4), "device_converged": bool(res["converged"]),

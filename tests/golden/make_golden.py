@@ -542,6 +542,29 @@ def make_naca(ref_root, name):
                        pre + "cp_tri": np.asarray(f["cp_tri"]), pre + "cl": np.float64(f["cl"]),
                        pre + "cd_pressure": np.float64(f["cd_pressure"])})
         print(case, res["n_newton"], res["gamma"].mean(), f["cl"], res["n_nu_active"])
+    # the reference's own transonic case (cases/analysis/a1_solver_bottleneck:
+    # M0.80, alpha 1.25 deg, Mach ramp from 0.70 with its committed recipe)
+    # (its level-0 Picard warm start with scipy spilu standing in for pyamg)
+    import scipy.sparse.linalg as spla
+    import pyfp3d.solve.linear as lin
+    from pyfp3d.solve.newton import solve_newton_transonic
+
+    def _ilu_preconditioner(A):
+        ilu = spla.spilu(A.tocsc(), drop_tol=1e-5, fill_factor=20.0)
+        return None, spla.LinearOperator(A.shape, matvec=ilu.solve)
+
+    saved = lin.build_amg_preconditioner
+    lin.build_amg_preconditioner = _ilu_preconditioner
+    try:
+        rt = solve_newton_transonic(mc, wc, m_inf=0.8, alpha_deg=1.25, m_start=0.70, dm=0.025, dm_min=0.003,
+                                    freeze_tol=1e-6,
+                                    newton_kw=dict(freeze_refresh_max=8, precond="direct", n_newton_max=60))
+    finally:
+        lin.build_amg_preconditioner = saved
+    assert rt["converged"]
+    arrays.update({"m08/phi": rt["phi"], "m08/gamma": rt["gamma"], "m08/n_nu_active": np.int64(rt["n_nu_active"]),
+                   "m08/levels": np.array([[m, n, r] for m, n, r in rt["level_history"]])})
+    print("m08", rt["gamma"], len(rt["level_history"]), sum(n for _, n, _ in rt["level_history"]))
     path = HERE / f"{name}.npz"
     np.savez_compressed(path, **arrays)
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")

@@ -130,7 +130,9 @@ def test_gpu_lifting_rejects_unbuilt_options(gold):
     with pytest.raises(ValueError):                 # the channel cut has no wall group
         NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="pressure")
     with pytest.raises(NotImplementedError):
-        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct")
+        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="ilu")
+    with pytest.raises(NotImplementedError):
+        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct", direct_refactor_every=2)
     from up3d_b200.solve.lifting import solve_subsonic_lifting
     with pytest.raises(NotImplementedError):
         solve_subsonic_lifting(cut, cut.wc, 0.5, vortex_center=vc, damping_theta=0.2)
@@ -245,3 +247,25 @@ def test_gpu_lifting_taper_and_external_rhs(gold):
     assert res["converged"]
     assert np.max(np.abs(res["phi"].cpu().numpy() - g["taper_phi"])) <= 1e-9
     assert np.max(np.abs(res["gamma"].cpu().numpy() - g["taper_gamma"])) <= 1e-9
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_direct_steps_match_reference(gold, name):
+    """precond="direct": exact Newton steps (dense LU of J_ff + Woodbury,
+    solve/newton.py:966-1011) take the reference's iterates: its step count
+    and converged solution (the fixtures were made with precond="direct")."""
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    g, cut = _case(gold, name)
+    res = solve_newton_lifting(cut, cut.wc, float(g["m_inf"]), alpha_deg=float(g["alpha_deg"]),
+                               vortex_center=channel_vortex_center(cut),
+                               farfield_spanwise_gamma=bool(g["spanwise"]), n_picard_seed=0, precond="direct")
+    assert res["converged"]
+    assert res["n_newton"] == int(g["sol_n_newton"]) and res["n_refactor"] == res["n_newton"]
+    hist = np.array(res["residual_history"])
+    ref = g["sol_residual_history"]
+    # the iterates agree until the residual reaches rounding level
+    big = ref > 1e-8
+    assert np.allclose(hist[big], ref[big], rtol=1e-6)
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-10
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-10

@@ -59,3 +59,23 @@ def test_gpu_naca_pressure_kutta_matches_reference(naca, tag):
     assert np.max(np.abs(res["kutta_sigma"] - g[tag + "/kutta_sigma"])) <= 1e-12 * np.max(g[tag + "/kutta_sigma"])
     assert np.max(np.abs(res["phi"].cpu().numpy() - g[tag + "/phi"])) <= 1e-9
     assert np.max(np.abs(res["gamma"].cpu().numpy() - g[tag + "/gamma"])) <= 1e-9
+
+
+def test_gpu_naca_transonic_recipe_matches_reference(naca):
+    """The reference's own transonic case (M0.80, alpha 1.25 deg, Mach ramp
+    from 0.70 with its committed recipe: dm 0.025, freeze 1e-6, direct
+    steps; cases/analysis/a1_solver_bottleneck, published 5 levels, 57
+    Newton steps, Gamma 0.233826): the same level sequence and the
+    reference's converged solution."""
+    from up3d_b200.solve.lifting import solve_newton_transonic
+    mc, wc = naca_cut(naca)
+    res = solve_newton_transonic(mc, wc, 0.8, 1.25, m_start=0.70, dm=0.025, dm_min=0.003, freeze_tol=1e-6,
+                                 newton_kw=dict(freeze_refresh_max=8, precond="direct", n_newton_max=60,
+                                                n_picard_seed=0))
+    assert res["converged"]
+    ref = naca["m08/levels"]
+    got = np.array([[m, n, r] for m, n, r in res["level_history"]])
+    assert np.allclose(got[:, 0], ref[:, 0])
+    assert np.all(np.abs(got[:, 1] - ref[:, 1]) <= 2)
+    assert abs(float(res["gamma"][0]) - float(naca["m08/gamma"][0])) <= 1e-8
+    assert np.max(np.abs(res["phi"].cpu().numpy() - naca["m08/phi"])) <= 1e-8

@@ -282,6 +282,58 @@ class NewtonWorkspace:
         K = sp.csr_matrix((kv, kc, kp), shape=(n_st, self.n_red))
         return K, L.to_device(F_elim, t.float64)
 
+    # dense direct steps are for small cases (the reference's sparse LU
+    # path: "seconds at 6e4 dofs"); 20,000 free unknowns are 3.2 GB dense
+    DIRECT_MAX_FREE = 20_000
+
+    def dense_lu(self, Aop: CoupledOperator):
+        """(LU, pivots) of the dense J_ff = (T^T J T)[free, free] of this
+        step (J the cut-mesh Jacobian, reduced by the wake plan of its
+        pattern: the fixed grouping of the reference's T^T (J T)), and the
+        dense B (n_free, n_stations) from the coupled operator at x = 0,
+        g = e_j.  The factorisation is cuSOLVER's dense LU (torch.linalg)."""
+        t = L.torch()
+        if self.n_free > self.DIRECT_MAX_FREE:
+            raise ValueError(f"precond='direct' is for small cases: {self.n_free} free unknowns "
+                             f"(limit {self.DIRECT_MAX_FREE}); use precond='amg'")
+        if not hasattr(self, "_con_direct"):
+            self._con_direct = WakeConstraint(Aop.J, self.wc)   # plans of the merged Jacobian patterns
+            self._free_pos = t.full((self.n_red,), -1, dtype=t.int64, device="cuda")
+            self._free_pos[L.to_device(self.free, t.int64)] = t.arange(self.n_free, device="cuda")
+            self._free_d = L.to_device(self.free, t.int64)
+        J_red, _ = self._con_direct.reduce_operator(Aop.J)
+        ip = J_red.indptr.to(t.int64)
+        rows = t.repeat_interleave(t.arange(self.n_red, device="cuda"), ip[1:] - ip[:-1])
+        cols = J_red.indices.to(t.int64)
+        fr, fc = self._free_pos[rows], self._free_pos[cols]
+        keep = (fr >= 0) & (fc >= 0)
+        D = t.zeros((self.n_free, self.n_free), dtype=t.float64, device="cuda")
+        D[fr[keep], fc[keep]] = J_red.data[keep]
+        zero = t.zeros(self.n_red, dtype=t.float64, device="cuda")
+        cols_b = []
+        for j in range(self.n_st):
+            e = t.zeros(self.n_st, dtype=t.float64, device="cuda")
+            e[j] = 1.0
+            cols_b.append(Aop.apply(zero, e)[0][self._free_d])
+        B = t.stack(cols_b, dim=1) if cols_b else t.zeros((self.n_free, 0), dtype=t.float64, device="cuda")
+        LU, piv = t.linalg.lu_factor(D)
+        return LU, piv, B
+
+    def direct_step(self, lu, K, rhs):
+        """dphi = z - JB S^-1 K z with z = J_ff^-1 rhs, JB = J_ff^-1 B,
+        S = I + K JB (newton.py:1003-1008); reduced-size, far-field rows 0."""
+        t = L.torch()
+        LU, piv, B = lu
+        Kd = L.to_device(np.ascontiguousarray(K[:, self.free].toarray()), t.float64)
+        z = t.linalg.lu_solve(LU, piv, rhs[self._free_d].unsqueeze(1)).squeeze(1)
+        if self.n_st:
+            JB = t.linalg.lu_solve(LU, piv, B)
+            S = t.eye(self.n_st, dtype=t.float64, device="cuda") + Kd @ JB
+            z = z - JB @ t.linalg.solve(S, Kd @ z)
+        out = t.zeros(self.n_red, dtype=t.float64, device="cuda")
+        out[self._free_d] = z
+        return out
+
     def picard_block(self) -> DeviceCSR:
         """T^T A(rho_tilde) T with the far-field mask: the AMG source
         (newton.py:1013-1022), rho_tilde of the last evaluation."""
@@ -316,7 +368,8 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
                          n_newton_max: int = 30, tol_residual: float = 1e-10,
                          tol_gamma: float = 1e-8, ew_eta0: float = 1e-2, ew_gamma: float = 0.9,
                          ew_eta_max: float = 1e-2, amg_rebuild_every: int = 2,
-                         precond: str = "amg", gmres_restart: int = 60, gmres_maxiter: int = 10,
+                         precond: str = "amg", direct_refactor_every: int = 1,
+                         gmres_restart: int = 60, gmres_maxiter: int = 10,
                          line_search: bool = True, rtol_seed: float = 1e-7,
                          tol_residual_loose: Optional[float] = None,
                          tol_residual_rel: Optional[float] = None, accept_on_stall: bool = False,
@@ -340,8 +393,11 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     if m_inf > 0.0 and upwind_c <= 0.0:
         raise ValueError("the Newton driver runs with the walk upwind machinery active for m_inf > 0; "
                          "pass upwind_c > 0")
-    if precond != "amg":
-        raise NotImplementedError(f"precond={precond!r}: the device driver preconditions with AMG")
+    if precond not in ("amg", "direct"):
+        raise NotImplementedError(f"precond={precond!r}: the device driver solves with AMG-GMRES or a "
+                                  "dense direct factorisation")
+    if precond == "direct" and direct_refactor_every != 1:
+        raise NotImplementedError("direct_refactor_every != 1 (lagged-LU GMRES) is not built")
     ws = workspace
     if ws is None:
         ws = NewtonWorkspace(mesh_cut, wc, alpha_deg, u_inf, gamma_air, vortex_center,
@@ -397,6 +453,7 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     residual_unfrozen = None
     r_level_best = np.inf
     n_term3_last = 0
+    n_refactor = 0
 
     a = clock()
     R, F, state = ws.eval_residual(phi_f, gamma, **res_kw)
@@ -485,22 +542,32 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
         n_term3_last = state["n_term3_active"]
         timings["assembly"] += clock() - a
         a = clock()
-        if M_pre is None or it % amg_rebuild_every == 0:
+        if precond == "amg" and (M_pre is None or it % amg_rebuild_every == 0):
             ws.amg = M_pre = amg_for(ws.picard_block(), ws.amg)
         timings["precond"] += clock() - a
         # rhs = -R_f - B F_elim  (B F_elim = the coupled operator at x = 0)
         a = clock()
-        _, F_elim = ws.kutta_blocks(state, F)
+        K_elim, F_elim = ws.kutta_blocks(state, F)
         zero = t.zeros(ws.n_red, dtype=t.float64, device="cuda")
         BF, _ = Aop.apply(zero, F_elim)
         rhs = -R - BF
-        eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev, ew_eta0, ew_gamma,
-                          ew_eta_max)
-        eta_prev = eta
-        eta_history.append(eta)
-        dphi, n_it, info = Aop.solve(rhs, M=M_pre, rtol=eta, restart=gmres_restart, maxiter=gmres_maxiter)
-        n_gmres_total += n_it
-        n_gmres_stalled += info != 0
+        if precond == "direct":
+            # exact step: dense LU of J_ff and the Woodbury update for the
+            # rank-n_stations coupling B K (newton.py:966-1011)
+            b2 = clock()
+            lu = ws.dense_lu(Aop)
+            timings["precond"] += clock() - b2
+            n_refactor += 1
+            dphi = ws.direct_step(lu, K_elim, rhs)
+            eta_history.append(0.0)
+        else:
+            eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev, ew_eta0, ew_gamma,
+                              ew_eta_max)
+            eta_prev = eta
+            eta_history.append(eta)
+            dphi, n_it, info = Aop.solve(rhs, M=M_pre, rtol=eta, restart=gmres_restart, maxiter=gmres_maxiter)
+            n_gmres_total += n_it
+            n_gmres_stalled += info != 0
         dphi = dphi.masked_fill(ws.mask.bool(), 0.0)
         _, dgamma = Aop.apply(dphi, F_elim)        # dGamma = K dphi + F_elim
         timings["linsolve"] += clock() - a
@@ -543,6 +610,7 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
             "nu_max": state["nu_max"], "n_nu_active": state["n_nu_active"],
             "n_limited": state["n_limited"], "n_floored": state["n_floored"],
             "n_term3_active": n_term3_last, "timings": timings, "workspace": ws,
+            "n_refactor": n_refactor,
             "kutta_estimator": ws.kutta_estimator, "kutta_sigma": ws.kutta_sigma,
             "kutta_sigma_sign_flips": ws.kutta_sigma_sign_flips, "kutta_weld_sign": ws.kutta_weld_sign}
 
