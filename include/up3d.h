@@ -206,6 +206,16 @@ int up3d_jacobian(up3d_mesh* mesh, const double* phi, const double* rho_tilde,
                   const uint8_t* lim_mask, double* data, int64_t* n_term3_active,
                   int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream);
 
+/* The same two calls under data-only names: up3d_picard_matrix_data is
+ * up3d_picard_matrix, up3d_jacobian_data is up3d_jacobian (the data array
+ * on the P1 pattern, the new nnz / pattern through up3d_jacobian_export). */
+int up3d_picard_matrix_data(up3d_mesh* mesh, const double* rho_tilde, double* data,
+                            up3d_stream stream);
+int up3d_jacobian_data(up3d_mesh* mesh, const double* phi, const double* rho_tilde,
+                       const double* s_e, const double* s_u, const int64_t* upstream, double u_inf,
+                       const uint8_t* lim_mask, double* data, int64_t* n_term3_active,
+                       int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream);
+
 /* The merged CSR (P1 pattern data + Term-3 extras) of the last up3d_jacobian
  * or up3d_residual_jacobian call into caller device buffers of sizes
  * n_nodes+1 and newton_nnz. */
@@ -531,6 +541,10 @@ int up3d_amg_refresh(up3d_precond* M, const up3d_csr* A, up3d_stream stream);
 int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream);
 /* z = M r */
 int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream stream);
+/* One V-cycle of an AMG hierarchy from up3d_amg_setup (pyamg's
+ * ml.aspreconditioner() applied once): z = M r.  UP3D_ERR_VALUE when M is
+ * not an AMG hierarchy. */
+int up3d_amg_vcycle(up3d_precond* M, const double* r, double* z, up3d_stream stream);
 int up3d_precond_destroy(up3d_precond* M);
 
 /* Preconditioned CG (scipy.sparse.linalg.cg as called by solve_cg_amg,

@@ -208,3 +208,42 @@ def test_amg_with_both_cycles_matches_fp64_cycle(c1_system):
     _, Mb = build_amg_preconditioner(A, fp32="both")
     _, M64 = build_amg_preconditioner(A)
     assert torch.equal(Mb.matvec(r), M64.matvec(r))
+
+
+def test_data_only_names_and_vcycle(c1_system, c1_golden):
+    """up3d_picard_matrix_data / up3d_jacobian_data give the bits of
+    up3d_picard_matrix / up3d_jacobian; up3d_amg_vcycle is one V-cycle
+    (the AMG preconditioner's apply) and refuses a Jacobi preconditioner."""
+    import ctypes
+    import torch
+    from up3d_b200 import _lib as L
+    from up3d_b200.kernels.jacobian import PicardOperator
+    from up3d_b200.solve.linear import build_amg_preconditioner, build_jacobi_preconditioner
+    s = c1_system
+    g = c1_golden
+    op = PicardOperator(g.mesh("nodes"), g.mesh("elements"))
+    rt = torch.from_numpy(g.state("mixed_m08", "rho_tilde")).cuda()
+    d0 = op.assemble_matrix(rt).data
+    d1 = torch.empty_like(d0)
+    L.call("up3d_picard_matrix_data", op._mesh.handle, rt.data_ptr(), d1.data_ptr(), L.stream_ptr())
+    assert torch.equal(d0, d1)
+    args = [torch.from_numpy(g.state("mixed_m08", k)).cuda() for k in ("phi", "s_e", "s_u")]
+    up = torch.from_numpy(g.state("mixed_m08", "upstream").astype(np.int64)).cuda()
+    outs = []
+    for name in ("up3d_jacobian", "up3d_jacobian_data"):
+        d = torch.empty_like(d0)
+        na, nx, nn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        L.call(name, op._mesh.handle, args[0].data_ptr(), rt.data_ptr(), args[1].data_ptr(), args[2].data_ptr(),
+               up.data_ptr(), 1.0, None, d.data_ptr(), ctypes.byref(na), ctypes.byref(nx), ctypes.byref(nn),
+               L.stream_ptr())
+        outs.append((d, na.value, nx.value, nn.value))
+    assert torch.equal(outs[0][0], outs[1][0]) and outs[0][1:] == outs[1][1:]
+    A = _embedded(s["A"], s["mask"])
+    M = build_amg_preconditioner(A)[1]
+    r = torch.from_numpy(s["b"]).cuda()
+    z = torch.empty_like(r)
+    L.call("up3d_amg_vcycle", M.handle, r.data_ptr(), z.data_ptr(), L.stream_ptr())
+    assert torch.equal(z, M.matvec(r))
+    Mj = build_jacobi_preconditioner(A)
+    with pytest.raises(ValueError):
+        L.call("up3d_amg_vcycle", Mj.handle, r.data_ptr(), z.data_ptr(), L.stream_ptr())

@@ -87,7 +87,10 @@ SIGNATURES = {
     "up3d_rho_tilde_frozen_sens": (_int, [_p, _p, _p, _p, _i64, ctypes.POINTER(Flow), _p, _p, _p]),
     "up3d_residual": (_int, [_p, _p, _p, _p, _p, _p, _p]),
     "up3d_picard_matrix": (_int, [_p, _p, _p, _p]),
+    "up3d_picard_matrix_data": (_int, [_p, _p, _p, _p]),
     "up3d_jacobian": (_int, [_p, _p, _p, _p, _p, _p, _d, _p, _p, ctypes.POINTER(_i64),
+                             ctypes.POINTER(_i64), ctypes.POINTER(_i64), _p]),
+    "up3d_jacobian_data": (_int, [_p, _p, _p, _p, _p, _p, _d, _p, _p, ctypes.POINTER(_i64),
                              ctypes.POINTER(_i64), ctypes.POINTER(_i64), _p]),
     "up3d_jacobian_export": (_int, [_p, _p, _p, _p, _p, _p]),
     "up3d_jacobian_nnz": (_int, [_p, _p, ctypes.POINTER(_i64), _p]),
@@ -139,6 +142,7 @@ SIGNATURES = {
     "up3d_amg_refresh": (_int, [_p, _p, _p]),
     "up3d_precond_jacobi": (_int, [_p, ctypes.POINTER(_p), _p]),
     "up3d_precond_apply": (_int, [_p, _p, _p, _p]),
+    "up3d_amg_vcycle": (_int, [_p, _p, _p, _p]),
     "up3d_precond_destroy": (_int, [_p]),
     "up3d_cg": (_int, [_p, _p, _p, _d, _d, _int, _p, ctypes.POINTER(_i64), ctypes.POINTER(_d),
                        ctypes.POINTER(_int), _p]),

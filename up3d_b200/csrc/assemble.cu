@@ -836,6 +836,10 @@ int up3d_picard_matrix(up3d_mesh* m, const double* rt, double* data, up3d_stream
     });
 }
 
+int up3d_picard_matrix_data(up3d_mesh* m, const double* rt, double* data, up3d_stream stream) {
+    return up3d_picard_matrix(m, rt, data, stream);
+}
+
 int up3d_jacobian(up3d_mesh* m, const double* phi, const double* rt, const double* se, const double* su,
                   const int64_t* upstream, double u_inf, const uint8_t* lim, double* data, int64_t* n_active,
                   int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream) {
@@ -864,6 +868,12 @@ int up3d_jacobian(up3d_mesh* m, const double* phi, const double* rt, const doubl
         if (n_extra) *n_extra = nx;
         if (newton_nnz) *newton_nnz = merged_nnz(m, data, s);
     });
+}
+
+int up3d_jacobian_data(up3d_mesh* m, const double* phi, const double* rt, const double* se, const double* su,
+                       const int64_t* upstream, double u_inf, const uint8_t* lim, double* data, int64_t* n_active,
+                       int64_t* n_extra, int64_t* newton_nnz, up3d_stream stream) {
+    return up3d_jacobian(m, phi, rt, se, su, upstream, u_inf, lim, data, n_active, n_extra, newton_nnz, stream);
 }
 
 int up3d_jacobian_export(up3d_mesh* m, const double* data, int32_t* indptr, int32_t* indices, double* merged,

@@ -665,6 +665,14 @@ int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream 
     });
 }
 
+int up3d_amg_vcycle(up3d_precond* M, const double* r, double* z, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(M && r && z, UP3D_ERR_ARGUMENT, "up3d_amg_vcycle: null argument");
+        UP3D_REQUIRE(M->kind == 2, UP3D_ERR_VALUE, "up3d_amg_vcycle: not an AMG hierarchy");
+        M->apply(r, z, S(stream));
+    });
+}
+
 int up3d_precond_destroy(up3d_precond* M) {
     return guarded([&] { delete M; });
 }
