@@ -114,3 +114,16 @@ def test_oracle_lifting_taper_and_external_rhs_match_reference(gold):
     assert ok and len(hist) - 1 == int(g["taper_n_newton"])
     assert np.max(np.abs(phi - g["taper_phi"])) <= 1e-10
     assert np.max(np.abs(gamma - g["taper_gamma"])) <= 1e-10
+
+
+def test_lifting_drivers_at_the_reference_module_paths():
+    """The reference keeps the coupled workspace and drivers in
+    solve/newton.py and the lifting Picard in solve/picard.py: the same
+    imports work here."""
+    from up3d_b200.solve import lifting
+    from up3d_b200.solve.newton import NewtonWorkspace, solve_newton_lifting, solve_newton_transonic
+    from up3d_b200.solve.picard import solve_subsonic_lifting
+    assert NewtonWorkspace is lifting.NewtonWorkspace
+    assert solve_newton_lifting is lifting.solve_newton_lifting
+    assert solve_subsonic_lifting is lifting.solve_subsonic_lifting
+    assert callable(solve_newton_transonic)

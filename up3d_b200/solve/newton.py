@@ -310,12 +310,34 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
             "timings": timings}
 
 
-def solve_newton_transonic(ws: ChannelWorkspace, m_inf: float, m_start: float = 0.70,
-                           dm: float = 0.05, dm_min: float = 0.01, freeze_tol: Optional[float] = 1e-6,
-                           precision: str = "fp64", verbose: bool = False,
-                           **newton_kw) -> Dict[str, object]:
-    """Upward Mach continuation (pyfp3d/solve/newton.py:1144-1307): each
-    level warm-starts from the previous converged level; a failed level is
+def solve_newton_transonic(first, *args, **kw) -> Dict[str, object]:
+    """Upward Mach continuation (pyfp3d/solve/newton.py:1144-1307).  With a
+    cut mesh and its WakeCut first -- the reference's signature
+    (mesh_cut, wc, m_inf, alpha_deg, ...) -- the coupled lifting solve
+    (solve.lifting.solve_newton_transonic); with a ChannelWorkspace first,
+    the wake-free channel solve (solve_channel_transonic)."""
+    if isinstance(first, ChannelWorkspace):
+        return solve_channel_transonic(first, *args, **kw)
+    from .lifting import solve_newton_transonic as lifting
+    return lifting(first, *args, **kw)
+
+
+def __getattr__(name):
+    # the reference's module also holds the coupled lifting workspace and
+    # driver (solve/newton.py:97-1141); they live in solve.lifting
+    if name in ("NewtonWorkspace", "solve_newton_lifting"):
+        from . import lifting
+        return getattr(lifting, name)
+    raise AttributeError(name)
+
+
+def solve_channel_transonic(ws: ChannelWorkspace, m_inf: float, m_start: float = 0.70,
+                            dm: float = 0.05, dm_min: float = 0.01, freeze_tol: Optional[float] = 1e-6,
+                            precision: str = "fp64", verbose: bool = False,
+                            **newton_kw) -> Dict[str, object]:
+    """Upward Mach continuation of the channel solve (the ramp of
+    pyfp3d/solve/newton.py:1144-1307 without the wake): each level
+    warm-starts from the previous converged level; a failed level is
     retried with the Mach step halved down to dm_min."""
     t = L.require_cuda()
     t0 = time.perf_counter()

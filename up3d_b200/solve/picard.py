@@ -105,3 +105,12 @@ def solve_subsonic(nodes, elements, dirichlet_nodes, dirichlet_values, m_inf: fl
             "residual_history": residual_history, "drho_history": drho_history,
             "rho": rho.cpu().numpy(), "mach2_max": mach2_max, "n_cg_total": n_cg_total,
             "timings": timings}
+
+
+def __getattr__(name):
+    # the reference's module also holds the nested lifting Picard
+    # (solve/picard.py:420-883); it lives in solve.lifting
+    if name == "solve_subsonic_lifting":
+        from .lifting import solve_subsonic_lifting
+        return solve_subsonic_lifting
+    raise AttributeError(name)
