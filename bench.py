@@ -595,6 +595,27 @@ def naca_timing():
         "reference_published": {"wall_s": 4.712, "n_levels": 5, "n_newton": 57, "gamma": 0.233826,
                                 "note": "with a Picard warm start (2.689 s of it) and sparse LU, 16 threads",
                                 "source": "cases/analysis/a1_solver_bottleneck/results/a1_runs.csv:7"}}
+    # the medium mesh end to end: cut, then the lifting Newton at M0.5
+    from up3d_b200.mesh.reader import Mesh
+    from up3d_b200.mesh.wake_cut import cut_wake
+    mm = Mesh()
+    mm.nodes, mm.elements = nodes, elements
+    mm.boundary_faces = {k.split("/", 1)[1]: med[k] for k in med.files if k.startswith("faces/")}
+    mm.element_tags = np.zeros(len(elements), dtype=np.int32)
+    mm.tag_names = ["fluid"]
+    t0 = time.perf_counter()
+    mcm, wcm = cut_wake(mm)
+    cut_s = time.perf_counter() - t0
+    solve_newton_lifting(mcm, wcm, 0.5, alpha_deg=1.25, n_picard_seed=0)             # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rm = solve_newton_lifting(mcm, wcm, 0.5, alpha_deg=1.25, n_picard_seed=0,
+                              workspace=NewtonWorkspace(mcm, wcm, 1.25))
+    torch.cuda.synchronize()
+    out["lifting_medium_m05"] = {
+        "n_tets": int(len(elements)), "n_copies": int(len(wcm.slave_nodes)), "cut_wake_s": round(cut_s, 3),
+        "device_s": round(time.perf_counter() - t0, 4), "converged": bool(rm["converged"]),
+        "n_newton": int(rm["n_newton"]), "n_gmres": int(rm["n_gmres_total"]), "gamma": float(rm["gamma"][0])}
     out["lifting_coarse_m05"] = {
         "n_tets": int(len(mc.elements)), "n_stations": int(wc.n_stations), "m_inf": m_inf, "alpha_deg": alpha,
         "device_s": round(dev_s, 4), "device_converged": bool(res["converged"]),

@@ -576,7 +576,8 @@ def make_naca(ref_root, name):
         assert abs(v - ref_stats[k]) <= 1e-12 * abs(ref_stats[k]), (k, v, ref_stats[k])
     path = HERE / "naca_medium_mesh.npz"
     np.savez_compressed(path, nodes=med.nodes, elements=med.elements,
-                        stats_keys=np.array(list(ref_stats.keys())), stats_values=np.array(list(ref_stats.values())))
+                        stats_keys=np.array(list(ref_stats.keys())), stats_values=np.array(list(ref_stats.values())),
+                        **{"faces/" + k: np.asarray(v, dtype=np.int32) for k, v in med.boundary_faces.items()})
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
 
 

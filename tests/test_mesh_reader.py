@@ -161,3 +161,19 @@ def test_cut_wake_matches_reference_on_swept_part_span_sheet():
     assert sorted(got) == sorted(ref_keys)
     for k in ref_keys:
         assert np.array_equal(np.asarray(got[k]), g[k]), k
+
+
+def test_cut_wake_on_naca_medium():
+    """cut_wake on the NACA medium mesh (61,788 tets, 984 wake faces): the
+    topology asserts hold and every sheet node is duplicated."""
+    from up3d_b200.mesh.reader import Mesh
+    from up3d_b200.mesh.wake_cut import cut_wake
+    g = np.load(GOLDEN / "naca_medium_mesh.npz")
+    m = Mesh()
+    m.nodes, m.elements = g["nodes"], g["elements"]
+    m.boundary_faces = {k.split("/", 1)[1]: g[k] for k in g.files if k.startswith("faces/")}
+    m.element_tags = np.zeros(len(m.elements), dtype=np.int32)
+    m.tag_names = ["fluid"]
+    mc, wc = cut_wake(m)
+    assert len(wc.slave_nodes) == len(np.unique(m.boundary_faces["wake"])) and wc.n_stations == 1
+    assert len(mc.nodes) == len(m.nodes) + len(wc.slave_nodes)
