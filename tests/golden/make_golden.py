@@ -694,6 +694,18 @@ def make_lifting_picard(name):
                            pre + "residual_history": np.array(res["residual_history"]),
                            pre + "drho_history": np.array(res["drho_history"])})
             print(tag, "picard", res["n_picard"], res["n_solves_total"], res["gamma"][:3])
+        # the pseudo-transient forms on the channel case
+        # (warm-started near the solution: the damped iterations converge
+        # slowly from the freestream)
+        gl = np.load(HERE / "lifting_newton.npz")
+        warm = dict(phi_init=gl["sub/sol_phi"], gamma_init=0.98 * gl["sub/sol_gamma"], n_picard_max=400)
+        for tag, kw in (("channel_theta", dict(damping_theta=0.05, **warm)),
+                        ("channel_dt", dict(pseudo_dt=1.0, **warm))):
+            res = solve_subsonic_lifting(mc, ref_wc(cut.wc), m_inf, alpha_deg=alpha, vortex_center=vc, **kw)
+            assert res["converged"], tag
+            arrays.update({tag + "/phi": res["phi"], tag + "/gamma": res["gamma"],
+                           tag + "/n_picard": np.int64(res["n_picard"])})
+            print(tag, res["n_picard"], res["n_solves_total"])
         res = solve_newton_lifting(mc, ref_wc(cut.wc), m_inf, alpha_deg=alpha, vortex_center=vc,
                                    precond="direct")
         assert res["converged"]

@@ -135,7 +135,7 @@ def test_gpu_lifting_rejects_unbuilt_options(gold):
         solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct", direct_refactor_every=2)
     from up3d_b200.solve.lifting import solve_subsonic_lifting
     with pytest.raises(NotImplementedError):
-        solve_subsonic_lifting(cut, cut.wc, 0.5, vortex_center=vc, damping_theta=0.2)
+        solve_subsonic_lifting(cut, cut.wc, 0.5, vortex_center=vc, upwind_weighted=True)
     with pytest.raises(ValueError):
         solve_subsonic_lifting(cut, cut.wc, 0.5, vortex_center=vc, damping_theta=0.2, pseudo_dt=1.0)
 
@@ -269,3 +269,21 @@ def test_gpu_lifting_direct_steps_match_reference(gold, name):
     assert np.allclose(hist[big], ref[big], rtol=1e-6)
     assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-10
     assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-10
+
+
+@pytest.mark.parametrize("tag,kw", [("channel_theta", {"damping_theta": 0.05}), ("channel_dt", {"pseudo_dt": 1.0})])
+def test_gpu_lifting_picard_pseudo_transient(gold, picard_gold, tag, kw):
+    """The lifting Picard's pseudo-transient forms (solve/picard.py:586-596,
+    :736-745, :841-848), warm-started near the solution: the reference's
+    converged state and outer count (within the preconditioner's
+    influence)."""
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_subsonic_lifting
+    g, cut = _case(gold, "sub")
+    res = solve_subsonic_lifting(cut, cut.wc, float(g["m_inf"]), alpha_deg=float(g["alpha_deg"]),
+                                 vortex_center=channel_vortex_center(cut), phi_init=g["sol_phi"],
+                                 gamma_init=0.98 * g["sol_gamma"], n_picard_max=400, **kw)
+    assert res["converged"]
+    assert abs(res["n_picard"] - int(picard_gold[tag + "/n_picard"])) <= max(3, int(picard_gold[tag + "/n_picard"]) // 10)
+    assert np.max(np.abs(res["phi"].cpu().numpy() - picard_gold[tag + "/phi"])) <= 1e-7
+    assert np.max(np.abs(res["gamma"] - picard_gold[tag + "/gamma"])) <= 1e-7

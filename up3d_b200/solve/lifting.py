@@ -702,6 +702,7 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
                            upwind_c: float = 1.5, m_crit: float = 0.95, upwind_weighted: bool = False,
                            phi_init=None, gamma_init=None, kutta_per_outer: Optional[int] = None,
                            m_cap: float = 3.0, omega_rho: float = 1.0, pseudo_dt: Optional[float] = None,
+                           pseudo_dt_growth: float = 1.1, pseudo_dt_max_ratio: float = 100.0,
                            damping_theta: Optional[float] = None, tol_residual: Optional[float] = None,
                            farfield_spanwise_gamma: bool = False, body_source_rhs=None,
                            workspace: Optional[NewtonWorkspace] = None,
@@ -717,8 +718,11 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
     loop met tol_gamma, the density lag max|rho_new - rho| < tol_rho and
     (with tol_residual) |T^T R|inf < tol_residual.  Matrix, right-hand
     side, CG, density and residual run on the device; Gamma (n_stations
-    numbers) and the convergence scalars on the host.  Not built:
-    upwind_weighted, pseudo_dt, damping_theta (NotImplementedError)."""
+    numbers) and the convergence scalars on the host.  damping_theta adds
+    theta diag(A_free) of each outer, pseudo_dt the lumped volumes over an
+    adaptive dtau, to the matrix and D phi_k to the right-hand side (the
+    reference's pseudo-transient forms).  Not built: upwind_weighted
+    (NotImplementedError)."""
     t = L.require_cuda()
     from ..physics.isentropic import mach_squared_field
     from .linear import solve_cg
@@ -726,9 +730,8 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         raise ValueError(f"solve_subsonic_lifting needs 0 <= M_inf < 1, got {m_inf}")
     if pseudo_dt is not None and damping_theta is not None:
         raise ValueError("pseudo_dt and damping_theta are mutually exclusive stabilizers -- pick one")
-    if upwind_weighted or pseudo_dt is not None or damping_theta is not None:
-        raise NotImplementedError("upwind_weighted, pseudo_dt and damping_theta are not built in the device "
-                                  "lifting Picard")
+    if upwind_weighted:
+        raise NotImplementedError("upwind_weighted is not built in the device lifting Picard")
     t_wall0 = time.perf_counter()
     ws = workspace
     if ws is None:
@@ -796,6 +799,18 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         phi_cut = L.to_device(freestream_phi(np.asarray(mesh_cut.nodes), alpha_deg, u_inf), t.float64)
         phi_red = None
     rho_t, mon = evaluate(phi_cut)
+    # pseudo-transient term D (picard.py:586-596, :736-745): the local
+    # theta diag(A_free) of each outer, or the lumped volumes over dtau
+    diag_pos = None
+    d_tau = None
+    dt_cur = pseudo_dt
+    if pseudo_dt is not None:
+        _, V = ws.mesh.geometry()
+        m_h = np.zeros(ws.mesh.n_nodes)
+        np.add.at(m_h, np.asarray(ws.mesh.elements).reshape(-1), np.repeat(V.cpu().numpy() / 4.0, 4))
+        m_cut = L.to_device(m_h, t.float64)
+        m_red = fold(m_cut)                         # T^T m, zero on far-field rows
+        d_tau = m_red / dt_cur
 
     residual_history, drho_history, gamma_history = [], [], [gamma.copy()]
     n_cg_total = n_solves_total = 0
@@ -807,6 +822,16 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         a = clock()
         A_cut = ws.op.assemble_matrix(rho_t)
         A_red = ws.con.reduce_operator(A_cut)[0]
+        if damping_theta is not None or d_tau is not None:
+            if diag_pos is None:
+                ip = A_red.indptr.to(t.int64)
+                rows = t.repeat_interleave(t.arange(n_red, device="cuda"), ip[1:] - ip[:-1])
+                diag_pos = t.nonzero(A_red.indices.to(t.int64) == rows).flatten()
+            if damping_theta is not None:
+                d_tau = (damping_theta * A_red.data[diag_pos]).masked_fill(mask_b, 0.0)
+            data = A_red.data.clone()
+            data[diag_pos] += d_tau
+            A_red = DeviceCSR(A_red.indptr, A_red.indices, data, A_red.shape)
         A_red.dirichlet = ws.mask
         A_red.extra = None
         timings["assembly"] += clock() - a
@@ -822,6 +847,8 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
             rhs = -fold(A_cut.matvec(u_cut))
             if b_fold is not None:
                 rhs = rhs + b_fold
+            if d_tau is not None and x0 is not None:
+                rhs = rhs + d_tau * x0
             if m_inf > 0.0 and forcing > 0.0:
                 r0 = rhs - A_red.matvec(x0, dirichlet=ws.mask) if x0 is not None else rhs
                 atol_k = forcing * float(t.linalg.vector_norm(r0))
@@ -876,6 +903,12 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         drho = float((rho_t_new - rho_t).abs().max())
         drho_history.append(drho)
         rho_t = rho_t_new if omega_rho == 1.0 else rho_t + omega_rho * (rho_t_new - rho_t)
+        if pseudo_dt is not None and len(drho_history) >= 2:
+            if drho < drho_history[-2]:
+                dt_cur = min(dt_cur * pseudo_dt_growth, pseudo_dt * pseudo_dt_max_ratio)
+            elif drho > 2.0 * drho_history[-2]:
+                dt_cur = max(dt_cur / 2.0, pseudo_dt)
+            d_tau = m_red / dt_cur
         timings["residual"] += clock() - a
         if kutta_converged and drho < tol_rho and (tol_residual is None or residual_history[-1] < tol_residual):
             converged = True
