@@ -638,6 +638,15 @@ def make_swept_cut(name):
     for tag, faces in m.boundary_faces.items():
         arrays["faces/" + tag] = np.asarray(faces, dtype=np.int64)
     arrays.update(cut_arrays(mc, wc))
+    # the spanwise far field on this cut (several stations, the sheet's tip
+    # inside the span: the Gamma(z) interpolation anchored to 0 at the tip)
+    from pyfp3d.constraints.dirichlet import farfield_dirichlet
+    g_st = np.array([0.10, 0.20, 0.15])
+    vc = (0.0, float(m.nodes[wc.master_nodes[0], 1]))
+    for beta in (1.0, 0.8):
+        dn, dv = farfield_dirichlet(mc, wc, 2.0, g_st, 1.0, vc, beta=beta, spanwise_gamma=True)
+        arrays.update({f"ff_beta{beta}/nodes": dn, f"ff_beta{beta}/values": dv})
+    arrays.update({"ff_gamma": g_st, "ff_vortex_center": np.array(vc)})
     path = HERE / f"{name}.npz"
     np.savez_compressed(path, **arrays)
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")

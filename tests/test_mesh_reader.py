@@ -177,3 +177,18 @@ def test_cut_wake_on_naca_medium():
     mc, wc = cut_wake(m)
     assert len(wc.slave_nodes) == len(np.unique(m.boundary_faces["wake"])) and wc.n_stations == 1
     assert len(mc.nodes) == len(m.nodes) + len(wc.slave_nodes)
+
+
+@pytest.mark.parametrize("beta", [1.0, 0.8])
+def test_spanwise_farfield_matches_reference(beta):
+    """farfield_dirichlet with the spanwise vortex strength on the swept
+    part-span cut (Gamma(z) interpolated over three stations, anchored to 0
+    at the sheet tip inside the span; constraints/dirichlet.py:98-182)."""
+    from up3d_b200.constraints.dirichlet import farfield_dirichlet
+    from up3d_b200.mesh.wake_cut import load_cut
+    g = np.load(GOLDEN / "swept_cut.npz")
+    mc, wc = load_cut(g)
+    dn, dv = farfield_dirichlet(mc, wc, 2.0, g["ff_gamma"], 1.0, tuple(g["ff_vortex_center"]), beta=beta,
+                                spanwise_gamma=True)
+    assert np.array_equal(dn, g[f"ff_beta{beta}/nodes"])
+    assert np.array_equal(dv, g[f"ff_beta{beta}/values"])
