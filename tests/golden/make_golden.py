@@ -647,6 +647,14 @@ def make_swept_cut(name):
         dn, dv = farfield_dirichlet(mc, wc, 2.0, g_st, 1.0, vc, beta=beta, spanwise_gamma=True)
         arrays.update({f"ff_beta{beta}/nodes": dn, f"ff_beta{beta}/values": dv})
     arrays.update({"ff_gamma": g_st, "ff_vortex_center": np.array(vc)})
+    # the coupled Newton on this cut (three stations, tip nodes single-valued)
+    from pyfp3d.solve.newton import solve_newton_lifting
+    res = solve_newton_lifting(mc, wc, 0.3, alpha_deg=2.0, vortex_center=vc, farfield_spanwise_gamma=True,
+                               n_picard_seed=0, precond="direct")
+    assert res["converged"]
+    arrays.update({"newton/phi": res["phi"], "newton/gamma": res["gamma"],
+                   "newton/n_newton": np.int64(res["n_newton"])})
+    print("swept newton", res["n_newton"], res["gamma"])
     path = HERE / f"{name}.npz"
     np.savez_compressed(path, **arrays)
     print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
