@@ -30,7 +30,12 @@ them (``pyfp3d/solve/newton.py:345-372``, ``:430-452``) with no wake
   per-side walks, newton_terms23_side_coo             wake/multivalued.py:456-466,
                                                       kernels/cut_assembly.py:401-488
   NewtonWorkspace, solve_newton_lifting (direct)      solve/newton.py:97-1141
-  cut_wake on the NACA0012 2.5D coarse mesh           mesh/wake_cut.py:225-441
+  solve_newton_transonic (the committed NACA recipe)  solve/newton.py:1144-1307
+  solve_subsonic_lifting (pyamg swapped for spilu)    solve/picard.py:420-883
+  cut_wake on the NACA0012 2.5D coarse mesh and on a
+  swept part-span sheet; farfield_dirichlet           mesh/wake_cut.py:225-594,
+                                                      constraints/dirichlet.py:98-182
+  TEControlVolumes (pressure Kutta estimator)         constraints/te_pressure.py:73-323
 
 The optional reference dependencies that are absent here (meshio, pyamg) are
 replaced by empty modules before import; neither is on the hot path.
