@@ -35,8 +35,7 @@ enum up3d_status {
     UP3D_ERR_VALUE = -1,           /* ValueError: degenerate tet, > 256 colours, bad shapes */
     UP3D_ERR_RUNTIME = -2,         /* RuntimeError: CUDA failure, Krylov non-convergence */
     UP3D_ERR_NOT_IMPLEMENTED = -3, /* NotImplementedError */
-    UP3D_ERR_ARGUMENT = -4,        /* null pointer, wrong size, misuse */
-    UP3D_ERR_TIMEOUT = -5          /* a bounded device-side wait gave up */
+    UP3D_ERR_ARGUMENT = -4         /* null pointer, wrong size, misuse */
 };
 
 /* Flow / upwind parameters shared by the per-step calls.  Defaults of the
@@ -650,14 +649,20 @@ int up3d_gmres_ir(const up3d_csr* A, const up3d_csr* extra, const float* data32,
  * cudaFree (a process whose device memory belongs to another allocator or a
  * fixed pre-reserved pool, or a time-critical loop that cannot take the
  * implicit synchronisation of those calls).  Working vectors live in one
- * static device array of UP3D_NOALLOC_MAX_ROWS rows (about 10.5 MB, resident
- * on every GPU that loads the library until exit).  Same arguments and
- * result as up3d_cg with an up3d_precond_jacobi preconditioner.
- * UP3D_ERR_VALUE for more rows than the limit.  The first call on a device
- * resolves the array's device address (cudaGetSymbolAddress) with that
- * device current; make it before capturing any stream.  All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the
- * caller.  Synchronous.  This entry point has no counterpart in the
+ * static device array of UP3D_NOALLOC_MAX_ROWS rows (about 10.5 MB).  Same
+ * arguments and result as up3d_cg with an up3d_precond_jacobi
+ * preconditioner.  UP3D_ERR_VALUE for more rows than the limit.  With
+ * CUDA's default lazy module loading the driver commits the array on a
+ * device at the first call there (one driver-side allocation, which fails
+ * with out-of-memory if another allocator has already reserved the whole
+ * device): make the first call on each device -- or run with
+ * CUDA_MODULE_LOADING=EAGER -- before a pool reserves the device, and
+ * before capturing any stream; later calls allocate nothing and the array
+ * stays resident until the process exits.  Every call looks the array's
+ * device address up (cudaGetSymbolAddress) with the caller's device
+ * current.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Synchronous (x is complete on
+ * return, b = 0 included).  This entry point has no counterpart in the
  * reference. */
 #define UP3D_NOALLOC_MAX_ROWS (1 << 18)
 int up3d_cg_jacobi_noalloc(const up3d_csr* A, const double* b, double* x, double rtol,

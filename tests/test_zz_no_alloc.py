@@ -81,6 +81,30 @@ def test_noalloc_cg_matches_allocating_cg_twice(system):
         assert rel_err(x.cpu().numpy(), x_ref.cpu().numpy()) <= TOL
 
 
+def test_noalloc_call_allocates_nothing(system):
+    """After a first call on the device (which lets the driver commit the
+    static array under lazy module loading), a call changes neither the
+    device's free memory nor the caching allocator's total."""
+    import torch
+    from up3d_b200 import _lib as L
+    x = torch.zeros_like(system["b"])
+    it, res, info = ctypes.c_int64(), ctypes.c_double(), ctypes.c_int()
+
+    def call():
+        L.call("up3d_cg_jacobi_noalloc", ctypes.byref(system["csr"]), system["b"].data_ptr(), x.data_ptr(),
+               1e-12, 0.0, 5000, ctypes.byref(it), ctypes.byref(res), ctypes.byref(info), L.stream_ptr())
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    used0 = torch.cuda.memory_allocated()
+    call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert info.value == 0
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == used0
+
+
 def test_noalloc_rejects_oversized_systems(system):
     import torch
     from up3d_b200 import _lib as L

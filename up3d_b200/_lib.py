@@ -7,7 +7,7 @@ CUDA device is visible, every device entry point raises.
 Status codes map to the reference's exception classes:
 UP3D_ERR_VALUE -> ValueError, UP3D_ERR_RUNTIME -> RuntimeError,
 UP3D_ERR_NOT_IMPLEMENTED -> NotImplementedError, UP3D_ERR_ARGUMENT ->
-TypeError, UP3D_ERR_TIMEOUT -> TimeoutError.
+TypeError.
 """
 
 from __future__ import annotations
@@ -174,8 +174,7 @@ class AmgInfo(ctypes.Structure):
     _fields_ = [("n_levels", _i32), ("n_coarse", _i64), ("operator_complexity", _d),
                 ("level_rows", _i64 * 16)]
 
-STATUS_EXC = {-1: ValueError, -2: RuntimeError, -3: NotImplementedError, -4: TypeError,
-              -5: TimeoutError}
+STATUS_EXC = {-1: ValueError, -2: RuntimeError, -3: NotImplementedError, -4: TypeError}
 
 _lib = None
 

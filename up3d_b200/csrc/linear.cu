@@ -2,8 +2,8 @@
 // reference's spla.cg / spla.gmres calls, solve/picard.py:375-380,
 // solve/linear.py:182, solve/newton.py:1029-1032).
 //
-// One 8-lane group per row (P1 rows hold ~15 entries), fixed reduction tree
-// (bit-reproducible).  The optional Dirichlet mask embeds the free-DOF
+// UP3D_SPMV_TPR lanes per row (4: P1 rows hold ~15 entries), fixed reduction
+// tree (bit-reproducible).  The optional Dirichlet mask embeds the free-DOF
 // operator A[free][:, free] (solve/linear.py:20-58) in full size:
 // constrained rows act as identity, constrained columns are dropped.
 

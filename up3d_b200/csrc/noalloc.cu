@@ -10,13 +10,19 @@
 // only its inputs and outputs.  The result equals up3d_cg with an
 // up3d_precond_jacobi preconditioner (same kernels, same reduction order).
 //
-// The array holds UP3D_NOALLOC_MAX_ROWS rows (see up3d.h) and stays
-// resident on every GPU that loads the library until the process exits.
-// All calls share it: calls that overlap on the GPU (other streams or
-// threads) race on it and must be serialised by the caller.
+// The array holds UP3D_NOALLOC_MAX_ROWS rows (see up3d.h).  CUDA loads a
+// library's device code lazily by default (CUDA_MODULE_LOADING=LAZY, CUDA
+// 12.2 and later), so the driver commits the array's device memory on each
+// device at the first use of this file's device code there -- the first
+// call of this entry point on that device, which therefore makes one
+// driver-side allocation (and can fail with out-of-memory once another
+// allocator has reserved the device).  Callers make that first call, or run
+// with CUDA_MODULE_LOADING=EAGER, before their pool reserves the device; from
+// then on the array stays resident until the process exits and no call
+// allocates.  All calls share it: calls that overlap on the GPU (other
+// streams or threads) race on it and must be serialised by the caller.
 
 #include <cmath>
-#include <mutex>
 
 #include "internal.cuh"
 
@@ -105,22 +111,14 @@ __global__ void k_na_dir(const double* __restrict__ sc, const double* __restrict
 
 __global__ void k_na_copy_scalar(const double* __restrict__ src, double* __restrict__ dst) { *dst = *src; }
 
-// Device address of g_scratch per device, resolved once per device with
-// that device current (the host-side name is only a stand-in).
-std::mutex g_na_mu;
-double* g_na_ptr[64] = {nullptr};
-
+// Device address of g_scratch on the current device.  The host-side name is
+// only a stand-in, so the address is asked for on every call (cheap once the
+// module is loaded): a pointer cached across a device reset could point at
+// memory of a dead context.
 double* scratch_for_current_device() {
-    int dev = 0;
-    UP3D_CUDA(cudaGetDevice(&dev));
-    UP3D_REQUIRE(dev >= 0 && dev < 64, UP3D_ERR_RUNTIME, "up3d_cg_jacobi_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_ptr[dev]) {
-        void* p = nullptr;
-        UP3D_CUDA(cudaGetSymbolAddress(&p, g_scratch));
-        g_na_ptr[dev] = static_cast<double*>(p);
-    }
-    return g_na_ptr[dev];
+    void* p = nullptr;
+    UP3D_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+    return static_cast<double*>(p);
 }
 
 }  // namespace
@@ -199,6 +197,8 @@ extern "C" int up3d_cg_jacobi_noalloc(const up3d_csr* A, const double* b, double
                 }
                 if (it > maxiter) it = maxiter;
             }
+            // every path (b = 0 included) leaves x complete on return
+            UP3D_CUDA(cudaStreamSynchronize(s));
             if (iters) *iters = it;
             if (resid) *resid = rn;
             if (info) *info = rn <= tol ? 0 : maxiter;

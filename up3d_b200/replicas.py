@@ -1,7 +1,8 @@
 """Multi-GPU plumbing for the replica runs: one process per GPU, no data-path
-collective (every configuration fits one B200; batched cases are independent
-solves).  Only timing is reduced across ranks (max), and the batched cases are
-partitioned deterministically over ranks.
+collective (every configuration fits one B200).  Only timing is reduced
+across ranks (max).  ``shard`` gives the deterministic contiguous partition
+of independent items (batched cases) over ranks for a caller that splits
+them; the benchmark runs identical replicas and does not split.
 """
 
 from __future__ import annotations

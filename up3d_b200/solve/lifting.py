@@ -26,7 +26,9 @@ kutta_estimator="pressure" replaces the probe row by the pressure
 equality on wall-adjacent TE control volumes (constraints/te_pressure.py):
 its state-dependent eliminated row -D^-1 K_p is rebuilt on the host per
 Newton step (n_stations rows over the TE fans' nodes) and uploaded to the
-coupled handle.  Not built: precond="direct" / "ilu" (host sparse LU).
+coupled handle.  precond="direct" takes exact steps (dense LU of the
+reduced J_ff on the device with the Woodbury update for the Kutta
+coupling); precond="ilu" (the reference's host incomplete LU) is not built.
 """
 
 from __future__ import annotations
