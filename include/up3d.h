@@ -437,6 +437,20 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
  *                    contributors from a fixed-width record (built at mesh
  *                    set-up when no slot has more than 8); 0: from the
  *                    offset list.  Ignored when the mesh has no records.
+ *   assembly         1: single-pass tiled assembly -- one CTA per tile of
+ *                    spatially compact elements evaluates the tile's
+ *                    elements with their state in shared memory and sums
+ *                    the residual and Jacobian outputs there (outputs that
+ *                    straddle tiles through a partial-sum buffer and a
+ *                    short combine pass); 0: the two-pass form above (an
+ *                    element sweep writing per-element local matrices to
+ *                    HBM and a row gather reading them back).  The two
+ *                    forms sum each output in a different fixed order, so
+ *                    they agree to rounding, not bit for bit; each is
+ *                    bit-reproducible.
+ *   tile_elems       elements per tile of the tiled form: 128 or 256 (the
+ *                    plan is rebuilt when it changes; the summation order
+ *                    depends on it)
  *   elem_us, row_us  autotune output: median time per launch of the
  *                    chosen shapes (0 when set by hand) */
 typedef struct {
@@ -444,19 +458,43 @@ typedef struct {
     int32_t elem_threads_per_sm;
     int32_t row_lanes;
     int32_t row_plan8;
+    int32_t assembly;
+    int32_t tile_elems;
     double elem_us;
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 512, 8, 0}.  UP3D_ERR_VALUE for a shape outside the lists. */
+/* Default: {0, 512, 8, 0, 1, 256}.  UP3D_ERR_VALUE for a shape outside the
+ * lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 
+/* The tile plan of the tiled assembly (built on first use, or here, for
+ * `tile_elems` elements per tile; no reference counterpart -- the
+ * reference scatters element contributions colour by colour,
+ * kernels/jacobian.py:106-181).  Builds the plan when it is missing or of
+ * another tile size; synchronises the stream. */
+typedef struct {
+    int32_t tile_elems;
+    int32_t max_nodes;          /* most distinct nodes of one tile */
+    int64_t n_tiles;
+    int64_t n_tile_nodes;       /* sum over tiles of their distinct nodes */
+    int64_t n_tile_edges;       /* sum over tiles of their distinct element edges */
+    int64_t n_partials;         /* partial sums per evaluation */
+    int64_t n_combined_nodes;   /* residual/diagonal outputs summed from partials */
+    int64_t n_combined_slots;   /* upper Jacobian slots summed from partials */
+    double build_s;             /* host time of the plan build */
+} up3d_tile_info;
+int up3d_mesh_tile_info(up3d_mesh* mesh, int32_t tile_elems, up3d_tile_info* info, up3d_stream stream);
+
 /* Times every candidate shape of the two passes on this mesh (the Newton
  * Jacobian sweep at phi and the flow, live upwind selection; `reps` timed
- * launches each after one warm-up, median kept), installs the fastest and
- * returns it in `tuning` (may be NULL).  Overwrites the mesh's internal
- * workspaces only; synchronises the stream. */
+ * launches each after one warm-up, median kept), then the tiled form at
+ * each tile size (the whole evaluation), installs the fastest form and
+ * shapes and returns them in `tuning` (may be NULL); for the tiled form
+ * elem_us is the whole evaluation and row_us 0.  Builds the tile plans
+ * (host work) and overwrites the mesh's internal workspaces only;
+ * synchronises the stream. */
 int up3d_autotune(up3d_mesh* mesh, const double* phi, const up3d_flow* flow, int reps,
                   up3d_tuning* tuning, up3d_stream stream);
 
@@ -544,6 +582,10 @@ int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream 
  * ml.aspreconditioner() applied once): z = M r.  UP3D_ERR_VALUE when M is
  * not an AMG hierarchy. */
 int up3d_amg_vcycle(up3d_precond* M, const double* r, double* z, up3d_stream stream);
+/* The same cycle on FP32 vectors, as the mixed-precision GMRES applies it
+ * (the FP32 cycle of a hierarchy built with fp32 = 1 or 2, else the FP64
+ * cycle between conversions). */
+int up3d_amg_vcycle_f32(up3d_precond* M, const float* r, float* z, up3d_stream stream);
 int up3d_precond_destroy(up3d_precond* M);
 
 /* Preconditioned CG (scipy.sparse.linalg.cg as called by solve_cg_amg,

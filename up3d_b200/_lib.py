@@ -49,7 +49,18 @@ class MeshInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """up3d_tuning: launch shapes of the fused evaluation's two passes."""
     _fields_ = [("elem_persistent", _i32), ("elem_threads_per_sm", _i32), ("row_lanes", _i32),
-                ("row_plan8", _i32), ("elem_us", _d), ("row_us", _d)]
+                ("row_plan8", _i32), ("assembly", _i32), ("tile_elems", _i32), ("elem_us", _d),
+                ("row_us", _d)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TileInfo(ctypes.Structure):
+    """up3d_tile_info: size of the tiled assembly's plan."""
+    _fields_ = [("tile_elems", _i32), ("max_nodes", _i32), ("n_tiles", _i64), ("n_tile_nodes", _i64),
+                ("n_tile_edges", _i64), ("n_partials", _i64), ("n_combined_nodes", _i64),
+                ("n_combined_slots", _i64), ("build_s", _d)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -132,6 +143,7 @@ SIGNATURES = {
     "up3d_mesh_set_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
     "up3d_mesh_get_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
     "up3d_autotune": (_int, [_p, _p, ctypes.POINTER(Flow), _int, ctypes.POINTER(Tuning), _p]),
+    "up3d_mesh_tile_info": (_int, [_p, _i32, ctypes.POINTER(TileInfo), _p]),
     "up3d_launch_count": (_int, [ctypes.POINTER(_i64)]),
     "up3d_profile": (_int, [_int]),
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),
@@ -143,6 +155,7 @@ SIGNATURES = {
     "up3d_precond_jacobi": (_int, [_p, ctypes.POINTER(_p), _p]),
     "up3d_precond_apply": (_int, [_p, _p, _p, _p]),
     "up3d_amg_vcycle": (_int, [_p, _p, _p, _p]),
+    "up3d_amg_vcycle_f32": (_int, [_p, _p, _p, _p]),
     "up3d_precond_destroy": (_int, [_p]),
     "up3d_cg": (_int, [_p, _p, _p, _d, _d, _int, _p, ctypes.POINTER(_i64), ctypes.POINTER(_d),
                        ctypes.POINTER(_int), _p]),

@@ -24,6 +24,7 @@
 
 #include "elem.cuh"
 #include "internal.cuh"
+#include "tiles.cuh"
 
 namespace up3d {
 
@@ -483,6 +484,414 @@ __global__ void __launch_bounds__(NT, MB)
     flush(acc, mon);
 }
 
+// ------------------------------------------------------------ tiled sweep
+
+// Arguments of the tiled evaluation (tiles.cuh): the plan's arrays, the
+// inputs and the outputs.  Element arrays of the plan are in internal
+// (tile) order; per-element outputs are written in user order.
+struct TileArgs {
+    const int4* conn;        // (E) global node ids, internal order
+    const int4* fnbr;        // (E) internal ids
+    const double4* cen;      // (E) internal order
+    const double4* X;        // (N) node positions
+    const double* phi;       // (N)
+    const int32_t* perm;     // internal -> user
+    const int32_t* iperm;    // user -> internal
+    const int32_t* eoff;
+    const int32_t* noff;
+    const int32_t* uoff;
+    const int32_t* tnode;
+    const ushort4* lconn;
+    const int32_t* nent_off;
+    const uint16_t* nent;
+    const int2* ndst;
+    const int32_t* uent_off;
+    const uint16_t* uent;
+    const int2* udst;
+    double* part;
+    double* R;
+    double* J;
+    double* t3v;
+    uint8_t* t3flag;
+    int32_t* up_out;
+    double* rt_out;
+    int8_t* br_out;
+    up3d_monitors* mon;
+    const int64_t* up_fz;
+    const int8_t* br_fz;
+    const Flow* flows;
+    const int32_t* case_of;
+    int n_cases;
+    int max_nodes;
+    int64_t E;
+    int64_t n_tiles;
+    Flow F0;
+    double u2;
+};
+
+// Shared memory of one tile of NT elements: the tile's nodes (x, y, z,
+// phi), then per element its centroid, gradient, unlimited q^2 and density,
+// 14 local values (LOC layout), face neighbours, local connectivity and
+// limiter flag -- all structure-of-arrays.
+constexpr int TS_DOUBLES = 8 + LOC_STRIDE;  // cx cy cz gx gy gz q2 rho + loc
+__host__ __device__ constexpr size_t tile_smem_bytes(int max_nodes, int nt) {
+    return (size_t)max_nodes * sizeof(double4) +
+           (size_t)nt * (TS_DOUBLES * sizeof(double) + sizeof(int4) + sizeof(ushort4) + 1);
+}
+
+// Local values of one element into the tile's shared memory (the
+// arithmetic of store_local: R_i, J_ii pairs, then the six J_ij).
+__device__ __forceinline__ void store_local_s(double* __restrict__ sloc, int nt, int l, const double* b,
+                                              const double gB[4], double w1, double w2) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        sloc[(2 * i) * nt + l] = w1 * gB[i];
+        sloc[(2 * i + 1) * nt + l] = jij(b, gB, w1, w2, i, i);
+    }
+    sloc[8 * nt + l] = jij(b, gB, w1, w2, 0, 1);
+    sloc[9 * nt + l] = jij(b, gB, w1, w2, 0, 2);
+    sloc[10 * nt + l] = jij(b, gB, w1, w2, 0, 3);
+    sloc[11 * nt + l] = jij(b, gB, w1, w2, 1, 2);
+    sloc[12 * nt + l] = jij(b, gB, w1, w2, 1, 3);
+    sloc[13 * nt + l] = jij(b, gB, w1, w2, 2, 3);
+}
+
+// The fused evaluation of k_fused_elem with the row gather folded in, one
+// CTA per tile of at most NT elements (one thread per element), a
+// persistent grid looping over the tiles:
+//   P0  the tile's node positions and potentials, the elements' local
+//       connectivity and face neighbours into shared memory;
+//   P1  per element: B_e and V_e from the staged positions (the mesh
+//       set-up's arithmetic), the gradient, q^2, the limiter, the density
+//       and the centroid (k_geometry's arithmetic) into shared memory;
+//   P2  the upstream walk (or the frozen selection): displacements
+//       cen(nbr) - cen(cur) formed from shared memory while the walk stays
+//       in the tile, from the internal-order centroid table outside it --
+//       the same IEEE operations as the precomputed displacements, so the
+//       same selections;
+//   P3  the upstream element's state from shared memory (or recomputed
+//       from global memory when the walk left the tile);
+//   P4  flux, sensitivities, residual vector and local matrix into shared
+//       memory, Term-3 vectors of active elements to global memory;
+//   P5  every output of the tile summed over its contributors in the
+//       plan's order (ascending local element), written to R / J when the
+//       tile holds all its contributors, else to the partial buffer.
+// Per-element outputs (upstream, rho~, branch, Term-3 vectors and flags)
+// go to user order through perm.
+template <bool FROZEN, bool JAC, bool BATCH, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ TileArgs a) {
+    extern __shared__ __align__(16) unsigned char tsm[];
+    double4* xs = reinterpret_cast<double4*>(tsm);
+    double* sd = reinterpret_cast<double*>(xs + a.max_nodes);
+    double* scx = sd;
+    double* scy = sd + NT;
+    double* scz = sd + 2 * NT;
+    double* sgx = sd + 3 * NT;
+    double* sgy = sd + 4 * NT;
+    double* sgz = sd + 5 * NT;
+    double* sq2 = sd + 6 * NT;
+    double* srho = sd + 7 * NT;
+    double* sloc = sd + 8 * NT;
+    int4* sfn = reinterpret_cast<int4*>(sd + TS_DOUBLES * NT);
+    ushort4* slc = reinterpret_cast<ushort4*>(sfn + NT);
+    uint8_t* slim = reinterpret_cast<uint8_t*>(slc + NT);
+    const int tid = threadIdx.x;
+    const int64_t E = a.E;
+    MonAcc acc;
+    for (int64_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const int32_t e0 = a.eoff[t], ne = a.eoff[t + 1] - e0;
+        const int32_t n0 = a.noff[t], nn = a.noff[t + 1] - n0;
+        // ---- P0
+        for (int r = tid; r < nn; r += NT) {
+            const int32_t n = a.tnode[n0 + r];
+            double x, y, z, w;
+            ld4(reinterpret_cast<const double*>(a.X + n), x, y, z, w);
+            xs[r] = make_double4(x, y, z, a.phi[n]);
+        }
+        const bool act = tid < ne;
+        const int64_t xe = (int64_t)e0 + tid;
+        int32_t user = 0;
+        ushort4 lc = make_ushort4(0, 0, 0, 0);
+        if (act) {
+            lc = a.lconn[xe];
+            slc[tid] = lc;
+            sfn[tid] = a.fnbr[xe];
+            user = a.perm[xe];
+        }
+        __syncthreads();
+        // ---- P1
+        int ci = 0;
+        if (BATCH && act) {
+            ci = a.case_of[user];
+            ci = (unsigned)ci < (unsigned)a.n_cases ? ci : 0;
+        }
+        const Flow& F = BATCH ? a.flows[ci] : a.F0;
+        double g[3] = {0.0, 0.0, 0.0}, Ve = 0.0, q2l = 0.0, rho_e = 0.0, ccx = 0.0, ccy = 0.0, ccz = 0.0;
+        bool lim_e = true;
+        if (act) {
+            const double4 p0 = xs[lc.x], p1 = xs[lc.y], p2 = xs[lc.z], p3 = xs[lc.w];
+            {
+                double bb[12];
+                geom_B_pts(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z, bb, Ve);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    g[d] = radd(radd(radd(rmul(p0.w, bb[d]), rmul(p1.w, bb[3 + d])), rmul(p2.w, bb[6 + d])),
+                                rmul(p3.w, bb[9 + d]));
+            }
+            const double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), a.u2);
+            q2l = q2n < F.q2cap ? q2n : F.q2cap;
+            lim_e = q2l == q2n;
+            rho_e = rho_of(q2l, F);
+            ccx = radd(radd(radd(p0.x, p1.x), p2.x), p3.x) * 0.25;
+            ccy = radd(radd(radd(p0.y, p1.y), p2.y), p3.y) * 0.25;
+            ccz = radd(radd(radd(p0.z, p1.z), p2.z), p3.z) * 0.25;
+            scx[tid] = ccx;
+            scy[tid] = ccy;
+            scz[tid] = ccz;
+            sgx[tid] = g[0];
+            sgy[tid] = g[1];
+            sgz[tid] = g[2];
+            sq2[tid] = q2n;
+            srho[tid] = rho_e;
+            slim[tid] = lim_e ? 1 : 0;
+        }
+        __syncthreads();
+        if (act) {
+            // ---- P2: upstream element (internal id)
+            const int brf = FROZEN ? (int)a.br_fz[user] : -1;
+            const bool frz = FROZEN && brf >= 0;
+            int64_t u = xe;
+            if (frz) {
+                u = a.iperm[safe_up(a.up_fz[user], user, E)];
+            } else {
+                const double gx = g[0], gy = g[1], gz = g[2];
+                double pmin = 1e300, pmax = -1e300;
+                {
+                    const unsigned short li[4] = {lc.x, lc.y, lc.z, lc.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const double4 p = xs[li[k]];
+                        const double pr = dot3r(p.x, p.y, p.z, gx, gy, gz);
+                        if (pr < pmin) pmin = pr;
+                        if (pr > pmax) pmax = pr;
+                    }
+                }
+                const double target = rmul(0.8, rsub(pmax, pmin));
+                double reach = 0.0, cx = ccx, cy = ccy, cz = ccz;
+                int64_t cur = xe;
+                for (int hops = 0; hops < 4 && reach < target; ++hops) {
+                    const uint32_t lcur = (uint32_t)(cur - e0);
+                    const int4 f = lcur < (uint32_t)ne ? sfn[lcur] : a.fnbr[cur];
+                    const int nb[4] = {f.x, f.y, f.z, f.w};
+                    int64_t best = -1;
+                    double best_disp = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (nb[k] >= 0 && nb[k] < E) {
+                            const uint32_t ln = (uint32_t)(nb[k] - e0);
+                            double nx, ny, nz;
+                            if (ln < (uint32_t)ne) {
+                                nx = scx[ln];
+                                ny = scy[ln];
+                                nz = scz[ln];
+                            } else {
+                                double w;
+                                ld4(reinterpret_cast<const double*>(a.cen + nb[k]), nx, ny, nz, w);
+                            }
+                            const double d = dot3r(rsub(nx, cx), rsub(ny, cy), rsub(nz, cz), gx, gy, gz);
+                            if (d < best_disp) {
+                                best_disp = d;
+                                best = nb[k];
+                                bx = nx;
+                                by = ny;
+                                bz = nz;
+                            }
+                        }
+                    }
+                    if (best < 0) break;
+                    cur = best;
+                    cx = bx;
+                    cy = by;
+                    cz = bz;
+                    reach = radd(reach, -best_disp);
+                }
+                u = cur;
+            }
+            // ---- P3: the upstream element's state
+            const uint32_t lu = (uint32_t)(u - e0);
+            const bool u_in = lu < (uint32_t)ne;
+            double q2lu = q2l, rho_u = rho_e;
+            bool lim_u = lim_e;
+            if (u != xe) {
+                double q2nu;
+                if (u_in) {
+                    q2nu = sq2[lu];
+                } else {
+                    const int4 cu = a.conn[u];
+                    double bu[12], vu, gu[3];
+                    geom_B(a.X, cu, bu, vu);
+                    grad_from_B(cu, bu, a.phi, gu);
+                    q2nu = __ddiv_rn(dot3r(gu[0], gu[1], gu[2], gu[0], gu[1], gu[2]), a.u2);
+                }
+                q2lu = q2nu < F.q2cap ? q2nu : F.q2cap;
+                lim_u = q2lu == q2nu;
+                rho_u = (u_in && !BATCH) ? srho[lu] : rho_of(q2lu, F);
+            }
+            acc.lim += !lim_e;
+            // ---- P4: flux, sensitivities, local values
+            double nu, rt, s_e = 0.0, s_u = 0.0;
+            if (frz) {
+                const int br = brf;
+                if (a.br_out) a.br_out[user] = (int8_t)br;
+                if (br == 3) {
+                    nu = 0.0;
+                    rt = F.floor_;
+                    acc.flo += 1;
+                } else if (br == 0) {
+                    nu = 0.0;
+                    rt = rho_e;
+                } else {
+                    nu = switch_of(mach2_of(br == 1 ? q2l : q2lu, F), F);
+                    rt = rho_e - nu * (rho_e - rho_u);
+                }
+                if (JAC) frozen_sensitivities(br, q2l, rho_e, q2lu, rho_u, F, s_e, s_u);
+            } else {
+                const double nu_e = switch_of(mach2_of(q2l, F), F), nu_u = switch_of(mach2_of(q2lu, F), F);
+                nu = fmax(nu_e, nu_u);
+                rt = rho_e - nu * (rho_e - rho_u);
+                if (a.br_out)
+                    a.br_out[user] = (int8_t)(u == xe ? (rho_e <= F.floor_ ? 3 : 0)
+                                                      : (rt <= F.floor_ ? 3 : (nu == 0.0 ? 0 : (nu_e >= nu_u ? 1 : 2))));
+                rt = rt > F.floor_ ? rt : F.floor_;
+                acc.flo += (rt == F.floor_);
+                if (JAC) live_sensitivities(q2l, rho_e, q2lu, rho_u, u == xe, F, s_e, s_u);
+            }
+            acc.nu_max = fmax(acc.nu_max, nu);
+            acc.sup += (nu > 0.0);
+            const double w1 = rt * Ve;
+            double b[12];
+            {
+                const double4 p0 = xs[lc.x], p1 = xs[lc.y], p2 = xs[lc.z], p3 = xs[lc.w];
+                double vtmp;
+                geom_B_pts(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z, b, vtmp);
+            }
+            double gB[4];
+            gB_of(g, b, gB);
+            if (JAC) {
+                s_e = s_e * (lim_e ? 1.0 : 0.0);
+                s_u = s_u * (lim_u ? 1.0 : 0.0);
+                const double w2 = 2.0 * F.inv_u2 * s_e * Ve;
+                const double w3 = 2.0 * F.inv_u2 * s_u * Ve;
+                const bool active = s_u != 0.0;
+                if (active) {
+                    double f[4] = {gB[0], gB[1], gB[2], gB[3]};
+                    if (u != xe) {
+                        double gu[3], bu[12], vu;
+                        if (u_in) {
+                            const ushort4 lcu = slc[lu];
+                            const double4 q0 = xs[lcu.x], q1 = xs[lcu.y], q2 = xs[lcu.z], q3 = xs[lcu.w];
+                            geom_B_pts(q0.x, q0.y, q0.z, q1.x, q1.y, q1.z, q2.x, q2.y, q2.z, q3.x, q3.y, q3.z, bu, vu);
+                            gu[0] = sgx[lu];
+                            gu[1] = sgy[lu];
+                            gu[2] = sgz[lu];
+                        } else {
+                            const int4 cu = a.conn[u];
+                            geom_B(a.X, cu, bu, vu);
+                            grad_from_B(cu, bu, a.phi, gu);
+                        }
+                        gB_of(gu, bu, f);
+                    }
+                    store_t3(a.t3v, user, w3, gB, f);
+                    acc.act += 1;
+                }
+                a.t3flag[user] = active ? 1 : 0;
+                store_local_s(sloc, NT, tid, b, gB, w1, w2);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) sloc[(2 * i) * NT + tid] = w1 * gB[i];
+            }
+            a.up_out[user] = a.perm[u];
+            if (a.rt_out) a.rt_out[user] = rt;
+        }
+        __syncthreads();
+        // ---- P5: the tile's outputs
+        for (int r = tid; r < nn; r += NT) {
+            const int32_t p = n0 + r;
+            const int32_t k1 = a.nent_off[p + 1];
+            double rs = 0.0, ds = 0.0;
+            for (int32_t k = a.nent_off[p]; k < k1; ++k) {
+                const uint32_t c = a.nent[k];
+                const int l = c >> 2, i = c & 3;
+                rs += sloc[(2 * i) * NT + l];
+                if (JAC) ds += sloc[(2 * i + 1) * NT + l];
+            }
+            const int2 d = a.ndst[p];
+            if (d.x >= 0) {
+                a.R[d.x] = rs;
+                if (JAC) a.J[d.y] = ds;
+            } else {
+                const int64_t q = -1 - (int64_t)d.x;
+                a.part[q] = rs;
+                if (JAC) a.part[q + 1] = ds;
+            }
+        }
+        if (JAC) {
+            const int32_t u1 = a.uoff[t + 1];
+            for (int32_t p = a.uoff[t] + tid; p < u1; p += NT) {
+                const int32_t k1 = a.uent_off[p + 1];
+                double v = 0.0;
+                for (int32_t k = a.uent_off[p]; k < k1; ++k) {
+                    const uint32_t c = a.uent[k];
+                    v += sloc[(8 + (c & 7)) * NT + (c >> 3)];
+                }
+                const int2 d = a.udst[p];
+                if (d.x >= 0) {
+                    a.J[d.x] = v;
+                    a.J[d.y] = v;
+                } else {
+                    a.part[-1 - (int64_t)d.x] = v;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    flush(acc, a.mon);
+}
+
+// Outputs summed from the tiles' partials, in tile order: residual and
+// diagonal of the nodes shared by several tiles (and R = 0 at nodes of no
+// element), then the shared upper slots and their transposes.
+template <bool JAC>
+__global__ void __launch_bounds__(256)
+    k_tile_combine(int64_t n_cnode, const int32_t* __restrict__ cn_off, const int32_t* __restrict__ cn_idx,
+                   const int2* __restrict__ cn_dst, int64_t n_cedge, const int32_t* __restrict__ ce_off,
+                   const int32_t* __restrict__ ce_idx, const int2* __restrict__ ce_dst,
+                   const double* __restrict__ part, double* __restrict__ R, double* __restrict__ J) {
+    const int64_t n = n_cnode + (JAC ? n_cedge : 0);
+    GRID_STRIDE(k, n) {
+        if (k < n_cnode) {
+            double rs = 0.0, ds = 0.0;
+            const int32_t j1 = cn_off[k + 1];
+            for (int32_t j = cn_off[k]; j < j1; ++j) {
+                const int32_t q = cn_idx[j];
+                rs += part[q];
+                if (JAC) ds += part[q + 1];
+            }
+            const int2 d = cn_dst[k];
+            R[d.x] = rs;
+            if (JAC && d.y >= 0) J[d.y] = ds;
+        } else {
+            const int64_t kk = k - n_cnode;
+            double v = 0.0;
+            const int32_t j1 = ce_off[kk + 1];
+            for (int32_t j = ce_off[kk]; j < j1; ++j) v += part[ce_idx[j]];
+            const int2 d = ce_dst[kk];
+            J[d.x] = v;
+            J[d.y] = v;
+        }
+    }
+}
+
 // ------------------------------------------------------------ Term 3
 
 // fill_term3_coo (kernels/jacobian.py:184-229) + the merge's duplicate
@@ -736,7 +1145,8 @@ void launch_row_residual(const up3d_mesh* m, double* R, cudaStream_t s) {
 // skips everything).
 constexpr int T3_WARPS = 4;
 static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
-                        int64_t known_active = -1) {
+                        int64_t known_active = -1, const int32_t* upstream = nullptr) {
+    if (!upstream) upstream = m->up32.get();
     const int64_t E = m->E, N = m->N;
     n_extra = 0;
     m->last_extra = 0;
@@ -763,7 +1173,7 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
     m->x_ptr.alloc(N + 1);
     UP3D_CUDA(cudaMemsetAsync(m->extra_cnt.get() + N, 0, sizeof(int32_t), s));
     k_t3_rows<T3_WARPS><<<grid_for(32 * N, T3_WARPS * 32, (int64_t)148 * 32), T3_WARPS * 32, smem, s>>>(
-        N, cap, m->ent_off.get(), m->ent.get(), m->t3_flag.get(), m->up32.get(), m->conn.get(), m->t3v.get(),
+        N, cap, m->ent_off.get(), m->ent.get(), m->t3_flag.get(), upstream, m->conn.get(), m->t3v.get(),
         m->indptr.get(), m->indices.get(), data, m->x_col.get(), m->x_val.get(), m->extra_cnt.get());
     UP3D_CHECK_LAUNCH();
     scan(m, m->extra_cnt.get(), m->x_ptr.get(), N + 1, s);
@@ -951,6 +1361,112 @@ static void launch_sweep(const up3d_mesh* m, cudaStream_t s, A... args) {
     }
 }
 
+// One launch of the tiled evaluation over every tile (a persistent grid of
+// SMs x occupancy CTAs).
+template <bool FR, bool JA, bool BA, int NT, int MB>
+static void launch_tiles_nt(const up3d_mesh* m, const TileArgs& ta, cudaStream_t s) {
+    auto kern = k_tile_eval<FR, JA, BA, NT, MB>;
+    const TilePlan& P = *m->tiles;
+    const size_t smem = tile_smem_bytes(P.max_nodes, NT);
+    UP3D_REQUIRE(smem <= 227 * 1024, UP3D_ERR_VALUE, "tiled assembly: a tile's shared memory exceeds 227 KB");
+    if (smem > 48 * 1024)  // per device: set on every launch that needs it
+        UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    UP3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem));
+    UP3D_REQUIRE(occ > 0, UP3D_ERR_RUNTIME, "tiled assembly: the tile kernel cannot be resident");
+    const int64_t grid = std::min<int64_t>(P.n_tiles, (int64_t)m->n_sms * occ);
+    kern<<<(unsigned)std::max<int64_t>(grid, 1), NT, smem, s>>>(ta);
+    UP3D_CHECK_LAUNCH();
+}
+
+template <bool FR, bool JA, bool BA>
+static void launch_tiles(const up3d_mesh* m, const TileArgs& ta, cudaStream_t s) {
+    if (m->tiles->T == 128) launch_tiles_nt<FR, JA, BA, 128, 4>(m, ta, s);
+    else launch_tiles_nt<FR, JA, BA, 256, 2>(m, ta, s);
+}
+
+// The tiled evaluation: the tile kernel, then the combine pass.
+static void tiled_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
+                           const int32_t* case_of, int n_cases, const int64_t* up_fz, const int8_t* br_fz,
+                           double* R, double* data, double* rt_out, int32_t* up_dst, up3d_monitors* mo,
+                           int8_t* br_out, cudaStream_t s) {
+    ensure_tiles(m, m->tune.tile_elems, s);
+    const TilePlan& P = *m->tiles;
+    TileArgs ta;
+    ta.conn = P.conn.get();
+    ta.fnbr = P.fnbr.get();
+    ta.cen = P.cen.get();
+    ta.X = m->nodes4.get();
+    ta.phi = phi;
+    ta.perm = P.perm.get();
+    ta.iperm = P.iperm.get();
+    ta.eoff = P.eoff.get();
+    ta.noff = P.noff.get();
+    ta.uoff = P.uoff.get();
+    ta.tnode = P.tnode.get();
+    ta.lconn = P.lconn.get();
+    ta.nent_off = P.nent_off.get();
+    ta.nent = P.nent.get();
+    ta.ndst = P.ndst.get();
+    ta.uent_off = P.uent_off.get();
+    ta.uent = P.uent.get();
+    ta.udst = P.udst.get();
+    ta.part = P.part.get();
+    ta.R = R;
+    ta.J = data;
+    ta.t3v = m->t3v.get();
+    ta.t3flag = m->t3_flag.get();
+    ta.up_out = up_dst;
+    ta.rt_out = rt_out;
+    ta.br_out = br_out;
+    ta.mon = mo;
+    ta.up_fz = up_fz;
+    ta.br_fz = br_fz;
+    ta.flows = flows_d;
+    ta.case_of = case_of;
+    ta.n_cases = n_cases;
+    ta.max_nodes = P.max_nodes;
+    ta.E = m->E;
+    ta.n_tiles = P.n_tiles;
+    ta.F0 = F;
+    ta.u2 = u2;
+    const bool jac = data != nullptr;
+    prof_begin(PROF_ELEM, s);
+    if (flows_d) {
+        if (up_fz) {
+            if (jac) launch_tiles<true, true, true>(m, ta, s);
+            else launch_tiles<true, false, true>(m, ta, s);
+        } else {
+            if (jac) launch_tiles<false, true, true>(m, ta, s);
+            else launch_tiles<false, false, true>(m, ta, s);
+        }
+    } else {
+        if (up_fz) {
+            if (jac) launch_tiles<true, true, false>(m, ta, s);
+            else launch_tiles<true, false, false>(m, ta, s);
+        } else {
+            if (jac) launch_tiles<false, true, false>(m, ta, s);
+            else launch_tiles<false, false, false>(m, ta, s);
+        }
+    }
+    prof_end(PROF_ELEM, s, 1);
+    prof_begin(PROF_ROW, s);
+    const int64_t n_out = P.n_cnode + (jac ? P.n_cedge : 0);
+    if (n_out > 0) {
+        const unsigned grid = grid_for(n_out, 256, (int64_t)m->n_sms * 16);
+        if (jac)
+            k_tile_combine<true><<<grid, 256, 0, s>>>(P.n_cnode, P.cn_off.get(), P.cn_idx.get(), P.cn_dst.get(),
+                                                      P.n_cedge, P.ce_off.get(), P.ce_idx.get(), P.ce_dst.get(),
+                                                      P.part.get(), R, data);
+        else
+            k_tile_combine<false><<<grid, 256, 0, s>>>(P.n_cnode, P.cn_off.get(), P.cn_idx.get(), P.cn_dst.get(),
+                                                       P.n_cedge, P.ce_off.get(), P.ce_idx.get(), P.ce_dst.get(),
+                                                       P.part.get(), R, data);
+        UP3D_CHECK_LAUNCH();
+    }
+    prof_end(PROF_ROW, s, 1);
+}
+
 // The fused evaluation: element sweep, row gather, Term 3.  flows_d /
 // case_of select per-element flows (several cases in one mesh) when set.
 static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, double u2, const Flow* flows_d,
@@ -959,11 +1475,18 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
                            int8_t* br_out = nullptr, int n_cases = 0) {
     up3d_monitors* mo = mon ? mon : m->mon_ws.get();
     UP3D_CUDA(cudaMemsetAsync(mo, 0, sizeof(up3d_monitors), s));
+    const bool jac = data != nullptr;
+    // the walk's result goes straight to the caller's buffer when there is
+    // one (Term 3 reads it from there), else to the mesh workspace
+    int32_t* up_dst = up_out ? up_out : m->up32.get();
+    if (m->tune.assembly == 1) {
+        tiled_evaluate(m, phi, F, u2, flows_d, case_of, n_cases, up_fz, br_fz, R, data, rt_out, up_dst, mo, br_out,
+                       s);
+    } else {
 #define FUSED_ARGS                                                                                                \
     m->conn.get(), m->fnbr.get(), m->disp.get(), m->nodes4.get(), phi, F, u2, up_fz, br_fz,                       \
-        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), m->up32.get(), rt_out, mo, flows_d, case_of, \
+        m->E, m->loc.get(), m->res.get(), m->t3v.get(), m->t3_flag.get(), up_dst, rt_out, mo, flows_d, case_of, \
         n_cases, br_out
-    const bool jac = data != nullptr;
     prof_begin(PROF_ELEM, s);
     if (flows_d) {
         if (up_fz) {
@@ -984,12 +1507,11 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     }
 #undef FUSED_ARGS
     prof_end(PROF_ELEM, s, 1);
-    if (up_out)
-        UP3D_CUDA(cudaMemcpyAsync(up_out, m->up32.get(), sizeof(int32_t) * m->E, cudaMemcpyDeviceToDevice, s));
     prof_begin(PROF_ROW, s);
     if (jac) launch_row_gather(m, R, data, s);
     else launch_row_residual(m, R, s);
     prof_end(PROF_ROW, s, 1);
+    }
     if (jac) {
         // the element sweep counted the active elements: Term 3 is
         // built only when there are any (flags already written)
@@ -998,7 +1520,7 @@ static void fused_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
         UP3D_CUDA(cudaStreamSynchronize(s));
         int64_t na = 0, nx = 0;
         prof_begin(PROF_TERM3, s);
-        build_term3(m, data, s, na, nx, known);
+        build_term3(m, data, s, na, nx, known, up_dst);
         prof_end(PROF_TERM3, s, 0);
         m->last_drop_zeros = na > 0;
         if (nx) {
@@ -1038,6 +1560,10 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
 
         UP3D_REQUIRE(t->row_plan8 == 0 || t->row_plan8 == 1, UP3D_ERR_VALUE,
                      "up3d_mesh_set_tuning: row_plan8 must be 0 or 1");
+        UP3D_REQUIRE(t->assembly == 0 || t->assembly == 1, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: assembly must be 0 (two-pass) or 1 (tiled)");
+        UP3D_REQUIRE(t->tile_elems == 128 || t->tile_elems == 256, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: tile_elems must be 128 or 256");
         m->tune = *t;
     });
 }
@@ -1132,6 +1658,31 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
             m->tune.row_plan8 = best_p;
             m->tune.elem_us = best_e;
             m->tune.row_us = best_r;
+            // the tiled form, one plan per tile size: the whole evaluation
+            // (tile kernel + combine) against the two passes
+            static const int tile_sizes[] = {128, 256};
+            double best_t = 0.0;
+            int best_T = 0;
+            for (int T : tile_sizes) {
+                m->tune.tile_elems = T;
+                const double t = time_it([&] {
+                    tiled_evaluate(m, phi, F, u2, no_flows, no_case, 0, no_up, no_br, R.get(), J.get(), no_rt,
+                                   m->up32.get(), mo, no_brout, s);
+                });
+                if (best_T == 0 || t < best_t) {
+                    best_t = t;
+                    best_T = T;
+                }
+            }
+            m->tune.tile_elems = best_T;
+            if (best_t < best_e + best_r) {
+                m->tune.assembly = 1;
+                m->tune.elem_us = best_t;
+                m->tune.row_us = 0.0;
+                ensure_tiles(m, best_T, s);
+            } else {
+                m->tune.assembly = 0;
+            }
         } catch (...) {
             m->tune = saved;
             throw;

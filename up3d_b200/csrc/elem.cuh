@@ -22,15 +22,12 @@ __device__ __forceinline__ void ld_B(const double* __restrict__ be, double b[12]
     ld4(be + 8, b[8], b[9], b[10], b[11]);
 }
 
-// B_e (12 values) and V_e from the node coordinates, with the operations of
-// the mesh set-up's geometry kernel, k_geometry (identical bits for every
+// B_e (12 values) and V_e from the four node positions, with the operations
+// of the mesh set-up's geometry kernel, k_geometry (identical bits for every
 // element that passed its degeneracy check).
-__device__ __forceinline__ void geom_B(const double4* __restrict__ X, int4 c, double b[12], double& V) {
-    double x0x, x0y, x0z, w, x1x, x1y, x1z, x2x, x2y, x2z, x3x, x3y, x3z;
-    ld4(reinterpret_cast<const double*>(X + c.x), x0x, x0y, x0z, w);
-    ld4(reinterpret_cast<const double*>(X + c.y), x1x, x1y, x1z, w);
-    ld4(reinterpret_cast<const double*>(X + c.z), x2x, x2y, x2z, w);
-    ld4(reinterpret_cast<const double*>(X + c.w), x3x, x3y, x3z, w);
+__device__ __forceinline__ void geom_B_pts(double x0x, double x0y, double x0z, double x1x, double x1y, double x1z,
+                                           double x2x, double x2y, double x2z, double x3x, double x3y, double x3z,
+                                           double b[12], double& V) {
     const double v1x = rsub(x1x, x0x), v1y = rsub(x1y, x0y), v1z = rsub(x1z, x0z);
     const double v2x = rsub(x2x, x0x), v2y = rsub(x2y, x0y), v2z = rsub(x2z, x0z);
     const double v3x = rsub(x3x, x0x), v3y = rsub(x3y, x0y), v3z = rsub(x3z, x0z);
@@ -51,6 +48,15 @@ __device__ __forceinline__ void geom_B(const double4* __restrict__ X, int4 c, do
     b[9] = rmul(c12x, inv); b[10] = rmul(c12y, inv); b[11] = rmul(c12z, inv);
 #pragma unroll
     for (int d = 0; d < 3; ++d) b[d] = -radd(radd(b[3 + d], b[6 + d]), b[9 + d]);
+}
+// The same from the node table (global memory).
+__device__ __forceinline__ void geom_B(const double4* __restrict__ X, int4 c, double b[12], double& V) {
+    double x0x, x0y, x0z, w, x1x, x1y, x1z, x2x, x2y, x2z, x3x, x3y, x3z;
+    ld4(reinterpret_cast<const double*>(X + c.x), x0x, x0y, x0z, w);
+    ld4(reinterpret_cast<const double*>(X + c.y), x1x, x1y, x1z, w);
+    ld4(reinterpret_cast<const double*>(X + c.z), x2x, x2y, x2z, w);
+    ld4(reinterpret_cast<const double*>(X + c.w), x3x, x3y, x3z, w);
+    geom_B_pts(x0x, x0y, x0z, x1x, x1y, x1z, x2x, x2y, x2z, x3x, x3y, x3z, b, V);
 }
 __device__ __forceinline__ void grad_from_B(int4 c, const double b[12], const double* __restrict__ phi, double g[3]) {
     const double p0 = phi[c.x], p1 = phi[c.y], p2 = phi[c.z], p3 = phi[c.w];

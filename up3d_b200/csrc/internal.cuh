@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -104,7 +105,8 @@ constexpr int LOC_STRIDE = 14;
 constexpr int PLAN8 = 8;
 constexpr uint32_t PLAN8_END = 0xFFFFFFFFu;
 
-struct Flow;  // physics constants of one flow (below)
+struct Flow;      // physics constants of one flow (below)
+struct TilePlan;  // tiled assembly plan (tiles.cuh)
 
 }  // namespace up3d
 
@@ -114,7 +116,8 @@ struct up3d_mesh {
     int32_t max_row_len = 0, max_deg = 0;
     int32_t n_colors = -1;
     int32_t n_sms = 148;                       // multiprocessors of the mesh's device
-    up3d_tuning tune = {0, 512, 8, 0, 0.0, 0.0};  // launch shapes of the fused passes
+    up3d_tuning tune = {0, 512, 8, 0, 1, 256, 0.0, 0.0};  // launch shapes of the fused evaluation
+    std::shared_ptr<up3d::TilePlan> tiles;     // tiled assembly plan (built on first use)
     int32_t batch_cases = 0;                   // cases of the flow table in flows_ws (0 = none)
     // face-hop neighbourhoods of the weighted "kernel" upwind mode (built on
     // request; nb_depth 0 = none)
@@ -153,7 +156,7 @@ struct up3d_mesh {
     up3d::DBuf<double> loc;            // (E, LOC_STRIDE) local matrices + residual
     up3d::DBuf<double> res;            // (E, 4) residual contributions
     up3d::DBuf<double> t3v;            // (E, 8) Term-3 vectors of active elements
-    up3d::DBuf<int32_t> up32;          // (E) upstream (internal)
+    up3d::DBuf<int32_t> up32;          // (E) upstream elements (workspace of the fused evaluation)
     up3d::DBuf<double> grad_ws;        // (E, 3)
     up3d::DBuf<double> q2_ws;          // (E)
     up3d::DBuf<int32_t> extra_cnt;     // (N+1) Term-3 extras per row

@@ -673,6 +673,14 @@ int up3d_amg_vcycle(up3d_precond* M, const double* r, double* z, up3d_stream str
     });
 }
 
+int up3d_amg_vcycle_f32(up3d_precond* M, const float* r, float* z, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(M && r && z, UP3D_ERR_ARGUMENT, "up3d_amg_vcycle_f32: null argument");
+        UP3D_REQUIRE(M->kind == 2, UP3D_ERR_VALUE, "up3d_amg_vcycle_f32: not an AMG hierarchy");
+        M->apply(r, z, S(stream));
+    });
+}
+
 int up3d_precond_destroy(up3d_precond* M) {
     return guarded([&] { delete M; });
 }

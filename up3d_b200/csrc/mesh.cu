@@ -13,6 +13,7 @@
 #include <mutex>
 
 #include "internal.cuh"
+#include "tiles.cuh"
 
 namespace up3d {
 
@@ -632,6 +633,7 @@ int up3d_mesh_set_face_neighbors(up3d_mesh* m, const int32_t* in, up3d_stream st
         UP3D_CUDA(cudaMemcpyAsync(m->fnbr.get(), in, sizeof(int4) * m->E, cudaMemcpyDeviceToDevice, S(stream)));
         refresh_disp(m, S(stream));
         m->nb_depth = 0;  // the neighbourhoods follow the face neighbours
+        m->tiles.reset();  // so does the tile plan (its neighbour table and components)
     });
 }
 

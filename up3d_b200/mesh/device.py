@@ -133,10 +133,20 @@ class DeviceMesh:
         return t.as_dict()
 
     def set_tuning(self, elem_persistent: int = 0, elem_threads_per_sm: int = 512, row_lanes: int = 8,
-                   row_plan8: int = 0) -> None:
-        """Installs launch shapes by hand; every shape computes the same bits."""
-        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, 0.0, 0.0)
+                   row_plan8: int = 0, assembly: int = 1, tile_elems: int = 256) -> None:
+        """Installs launch shapes by hand.  Within one assembly form (and,
+        for the tiled form, one tile size) every shape computes the same
+        bits; the forms agree to rounding."""
+        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, assembly, tile_elems, 0.0, 0.0)
         L.call("up3d_mesh_set_tuning", self.handle, ctypes.byref(t))
+
+    def tile_info(self, tile_elems: int | None = None) -> dict:
+        """Sizes of the tiled assembly's plan (built here when missing)."""
+        if tile_elems is None:
+            tile_elems = self.tuning()["tile_elems"]
+        t = L.TileInfo()
+        L.call("up3d_mesh_tile_info", self.handle, int(tile_elems), ctypes.byref(t), L.stream_ptr())
+        return t.as_dict()
 
     def autotune(self, phi, flow, reps: int = 5) -> dict:
         """Times every candidate shape of the element sweep and the row

@@ -104,6 +104,11 @@ class Renumbered:
     elem_inv: np.ndarray
     ordering: str
 
+    @property
+    def identity(self) -> bool:
+        """True for the given numbering (no permutation)."""
+        return self.ordering == "given"
+
     def nodal(self, a):
         """An old-numbering nodal array in the new numbering."""
         return np.asarray(a)[self.node_perm]

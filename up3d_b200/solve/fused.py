@@ -4,9 +4,10 @@ One call does what ``NewtonWorkspace.eval_residual`` followed by
 ``assemble_coupled`` do without a wake (pyfp3d/solve/newton.py:345-372,
 :430-457 with T = I): velocities, speed limiter, density, upstream walk (or
 the frozen selection), upwinded density, its sensitivities, the residual R
-and the Newton Jacobian (Terms 1-3) -- two passes over the mesh (an element
-sweep and a row gather) plus the Term-3 sort/merge when supersonic elements
-exist.
+and the Newton Jacobian (Terms 1-3) -- one tiled pass over the mesh and a
+short combine of the outputs shared by tiles (or, by tuning, two passes: an
+element sweep and a row gather), plus the Term-3 merge when supersonic
+elements exist.
 """
 
 from __future__ import annotations
@@ -45,12 +46,16 @@ class ResidualJacobian:
         self.upstream = t.empty(mesh.n_tets, dtype=t.int32, device="cuda")
         self.monitors = L.monitors_buffer()
         self._n_extra = 0
+        if mesh.tuning()["assembly"] == 1:
+            mesh.tile_info()  # the tile plan now, not inside a timed solve
 
     def evaluate(self, phi, flow: FlowParams, jacobian: bool = True, frozen=None,
-                 keep_state: bool = True, R_out=None, data_out=None):
+                 keep_state=True, R_out=None, data_out=None):
         """R(phi) (and the Jacobian data on the P1 pattern) into this
         workspace, or into R_out / data_out when given.  `frozen` =
-        (upstream int64, branch int8) selects the frozen flux."""
+        (upstream int64, branch int8) selects the frozen flux.  keep_state:
+        True writes rho~ and the upstream map to ``rho_tilde`` /
+        ``upstream``, "upstream" the upstream map only, False neither."""
         up_fz = br_fz = None
         if frozen is not None:
             t = L.torch()
@@ -61,7 +66,7 @@ class ResidualJacobian:
         L.call("up3d_residual_jacobian", self.mesh.handle, phi.data_ptr(), flow.c(),
                L.ptr(up_fz), L.ptr(br_fz), R.data_ptr(),
                data.data_ptr() if jacobian else None,
-               self.rho_tilde.data_ptr() if keep_state else None,
+               self.rho_tilde.data_ptr() if keep_state is True else None,
                self.upstream.data_ptr() if keep_state else None,
                self.monitors.data_ptr(), L.stream_ptr())
         return R
