@@ -72,6 +72,11 @@ def parse():
     p.add_argument("--naca", default="1", help="NACA0012 2.5D timings ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
+    p.add_argument("--parity", type=int, default=1,
+                   help="1: compare the timed states with the oracle after timing; 2: also the pocket states; "
+                        "0: skip")
+    p.add_argument("--linear", type=int, default=1,
+                   help="1: SpMV / V-cycle / GMRES timings on the bench mesh's Jacobian")
     return p.parse_args()
 
 
@@ -82,7 +87,7 @@ def workload(shape):
     return mesh, phis
 
 
-def config_dict(shape, mesh, nnz=None):
+def config_dict(shape, mesh):
     nx, ny, nz = shape
     d = {"workload": f"transonic bump channel {nx}x{ny}x{nz} Kuhn-split "
                      f"({mesh.n_tets} tets), M_inf {M_INF}, fused residual + Newton Jacobian "
@@ -91,8 +96,6 @@ def config_dict(shape, mesh, nnz=None):
          "m_inf": M_INF, "bump_amplitude": AMPLITUDE, "states": N_STATES,
          "l2": "inputs larger than L2 (mesh data ~1.3 GB >> 126 MB); no flush",
          "parallelism": "replicas"}
-    if nnz is not None:
-        d["nnz"] = nnz
     return d
 
 
@@ -103,8 +106,7 @@ def cpu_chain_timing(mesh, phis, n_states, threads):
     reference kernels), timed on the host cores."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import oracle as O
-    op = O.PicardOperator(mesh.nodes, mesh.elements)
-    upw = O.UpwindOperator(mesh.nodes, mesh.elements)
+    op, upw = oracle_ops(mesh)
     O.chain(op, upw, phis[0], M_INF)          # warm (page-in, thread pool)
     t0 = time.perf_counter()
     for k in range(n_states):
@@ -226,8 +228,22 @@ def bytes_model(info, n_active=0):
     t3 = n_active * 16 * 16
     design_elem = (E * (16 + 16 + 96 + 4 + 14 * 8 + 1) + N * (24 + 8))
     design_row = (E * (16 + 24 + 14 * 8) + Z * (4 + 4 + 8) + N * (4 * 3 + 8))
-    return {"elem_sweep": elem, "row_gather": row, "term3": t3, "fused": elem + row + t3,
-            "design": {"elem_sweep": design_elem, "row_gather": design_row}}
+    out = {"elem_sweep": elem, "row_gather": row, "term3": t3, "fused": elem + row + t3,
+           "design": {"elem_sweep": design_elem, "row_gather": design_row}}
+    ti = info.get("tiles")
+    if ti:
+        # the tiled form: per element its local connectivity (8), internal
+        # face neighbours (16), id map (4), upstream out (4), Term-3 flag
+        # (1), node entries (2 x 4) and edge contributors (2 x 6); per
+        # tile-node its global id (4), offset (4), destination (8) and the
+        # staged position + potential (32 + 8, L2 hits where tiles share
+        # nodes); per tile-edge its offset (4) and destination (8); every
+        # partial written and read (8 + 8) with its combine index (4); the
+        # outputs R and J
+        out["design"]["tile_eval"] = (E * (8 + 16 + 4 + 4 + 1 + 8 + 12) + ti["n_tile_nodes"] * (4 + 4 + 8 + 40)
+                                      + ti["n_tile_edges"] * (4 + 8) + ti["n_partials"] * (8 + 8 + 4)
+                                      + N * 8 + Z * 8)
+    return out
 
 
 def read_peaks():
@@ -736,7 +752,9 @@ def batched_timing(spec, seed=0):
     def fresh():
         b = BatchedChannels(meshes, ordering=batch.ordering)
         b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_threads_per_sm"],
-                                shapes_tuned["row_lanes"], shapes_tuned["row_plan8"])
+                                shapes_tuned["row_lanes"], shapes_tuned["row_plan8"], shapes_tuned["assembly"],
+                                shapes_tuned["tile_elems"])
+        b.ws.ev.mesh.tile_info()
         return b
     res_b = None
     for _ in range(2):
@@ -760,6 +778,137 @@ def batched_timing(spec, seed=0):
                                         for v in res_b["converged_s"]],
                      "sequential_case_s": [round(v, 4) for v in seq_s]}
     return out
+
+
+_ORACLE_OPS = {}
+
+
+def oracle_ops(mesh):
+    """The oracle's operators on the bench mesh (built once per process)."""
+    from oracle import oracle as O
+    key = id(mesh)
+    if key not in _ORACLE_OPS:
+        _ORACLE_OPS[key] = (O.PicardOperator(mesh.nodes, mesh.elements), O.UpwindOperator(mesh.nodes, mesh.elements))
+    return _ORACLE_OPS[key]
+
+
+def bench_parity(mesh, order, ev, flow, d_phis, phis, pocket: bool):
+    """The timed states (and, when asked, the three supersonic-pocket
+    families) evaluated once more outside the timed region and compared
+    with the oracle's chain of the reference kernels: largest relative
+    error of R, rho~ and the merged Newton Jacobian (over the union
+    pattern), upstream mismatches, Term-3 counts."""
+    from oracle import oracle as O
+    from up3d_b200.mesh.kuhn import pocket_state
+    op, upw = oracle_ops(mesh)
+    states = [(f"seed{k}", phis[k], d_phis[k]) for k in range(len(phis))]
+    if pocket:
+        import torch
+        for fam in ("accelerating", "shockpoint", "mixed"):
+            ph = pocket_state(mesh, fam)
+            states.append((fam, ph, torch.from_numpy(order.nodal(ph)).cuda()))
+    t0 = time.perf_counter()
+    worst = {"R": 0.0, "rho_tilde": 0.0, "J": 0.0}
+    per = {}
+    mism = 0
+    for label, ph, pd in states:
+        ev.evaluate(pd, flow, jacobian=True, keep_state=True)
+        R = order.nodal_back(ev.R.cpu().numpy())
+        rt = order.elemental_back(ev.rho_tilde.cpu().numpy())
+        up = order.element_ids_back(order.elemental_back(ev.upstream.cpu().numpy()))
+        n3 = int(ev.read_monitors()["n_term3_active"])
+        J = ev.jacobian().to_scipy()
+        if not order.identity:
+            J = J[order.node_inv][:, order.node_inv]
+        ref = O.chain(op, upw, ph, M_INF)
+        eR = float(np.abs(R - ref["R"]).max() / np.abs(ref["R"]).max())
+        ert = float(np.abs(rt - ref["rho_tilde"]).max() / np.abs(ref["rho_tilde"]).max())
+        D = (J - ref["J"]).tocoo()
+        eJ = float((np.abs(D.data).max() if D.nnz else 0.0) / np.abs(ref["J"].data).max())
+        nm = int(np.count_nonzero(up != ref["upstream"]))
+        mism += nm
+        worst["R"] = max(worst["R"], eR)
+        worst["rho_tilde"] = max(worst["rho_tilde"], ert)
+        worst["J"] = max(worst["J"], eJ)
+        per[label] = {"R": eR, "rho_tilde": ert, "J": eJ, "upstream_mismatch": nm,
+                      "n_term3_active": n3, "oracle_n_term3_active": int(ref["n_term3_active"])}
+    return {"max_rel_err": worst, "upstream_mismatch": mism, "tolerance": 1e-12,
+            "ok": bool(max(worst.values()) < 1e-12 and mism == 0), "states": per,
+            "reference": "oracle chain (C/OpenMP restatement of the reference kernels, pinned to "
+                         "reference-generated fixtures)",
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
+def linear_timing(ev, dmesh, mesh, order, phi_d, flow):
+    """The Krylov solve's kernels on the bench mesh's Newton Jacobian at the
+    first timed state (Dirichlet inflow/outflow rows masked): FP64 and FP32
+    SpMV against their compulsory bytes (12 Z + 4 (N+1) + 16 N and
+    8 Z + 4 (N+1) + 8 N, plus the N-byte mask), the AMG V-cycle in FP64 and
+    FP32, and one GMRES(60) restart cycle with the FP64 V-cycle as
+    preconditioner (per Arnoldi step).  CUDA events, inputs resident."""
+    import torch
+    from up3d_b200 import _lib as L
+    from up3d_b200.solve.linear import build_amg_preconditioner, solve_gmres, with_dirichlet
+    ev.evaluate(phi_d, flow, jacobian=True, keep_state=False)
+    J = ev.jacobian()
+    N, Z = dmesh.n_nodes, int(J.data.numel())
+    mask_h = np.zeros(N, dtype=np.uint8)
+    mask_h[mesh.dirichlet_nodes] = 1
+    mask = torch.from_numpy(order.nodal(mask_h)).cuda()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    x32, y32, d32 = x.float(), torch.empty(N, dtype=torch.float32, device="cuda"), J.data.float()
+    st = L.stream_ptr()
+
+    def t_events(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    peak, _ = read_peaks()
+    ms64 = t_events(lambda: L.call("up3d_spmv", N, J.indptr.data_ptr(), J.indices.data_ptr(), J.data.data_ptr(),
+                                   x.data_ptr(), y.data_ptr(), mask.data_ptr(), st), 100)
+    ms32 = t_events(lambda: L.call("up3d_spmv_f32", N, J.indptr.data_ptr(), J.indices.data_ptr(), d32.data_ptr(),
+                                   x32.data_ptr(), y32.data_ptr(), mask.data_ptr(), st), 100)
+    b64 = 12 * Z + 4 * (N + 1) + 16 * N + N
+    b32 = 8 * Z + 4 * (N + 1) + 8 * N + N
+    A = with_dirichlet(J, mask)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ml, M = build_amg_preconditioner(A, fp32="both")
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    z = torch.empty_like(x)
+    z32 = torch.empty_like(x32)
+    v64 = t_events(lambda: L.call("up3d_amg_vcycle", M.handle, x.data_ptr(), z.data_ptr(), st), 20)
+    v32 = t_events(lambda: L.call("up3d_amg_vcycle_f32", M.handle, x32.data_ptr(), z32.data_ptr(), st), 20)
+    b = x.clone()
+    b[mask.bool()] = 0.0
+    solve_gmres(A, b, M=M, rtol=1e-30, restart=60, maxiter=1, on_fail="return")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, n_inner, _ = solve_gmres(A, b, M=M, rtol=1e-30, restart=60, maxiter=1, on_fail="return")
+    torch.cuda.synchronize()
+    gm_s = time.perf_counter() - t0
+    return {"matrix": f"Newton Jacobian of the bench mesh at the first timed state ({N} rows, {Z} entries)",
+            "spmv_fp64": {"ms": round(ms64, 5), "bytes": b64, "gbs": round(b64 / (ms64 * 1e-3) / 1e9, 1),
+                          "frac": round(b64 / (ms64 * 1e-3) / 1e9 / peak, 4)},
+            "spmv_fp32": {"ms": round(ms32, 5), "bytes": b32, "gbs": round(b32 / (ms32 * 1e-3) / 1e9, 1),
+                          "frac": round(b32 / (ms32 * 1e-3) / 1e9 / peak, 4)},
+            "amg": {"setup_s": round(setup_s, 3), "levels": ml.level_rows,
+                    "operator_complexity": round(ml.operator_complexity, 3),
+                    "vcycle_fp64_ms": round(v64, 4), "vcycle_fp32_ms": round(v32, 4)},
+            "gmres_fp64": {"restart": 60, "arnoldi_steps": int(n_inner),
+                           "ms_per_arnoldi_step": round(1e3 * gm_s / max(n_inner, 1), 4),
+                           "note": "one restart cycle, wall clock with the device synchronised"}}
 
 
 def run_ours(args):
@@ -796,9 +945,12 @@ def run_ours(args):
     elif args.tune != "default":
         dmesh.set_tuning(*(int(v) for v in args.tune.split(",")))
     tuning = dmesh.tuning()
+    tiled = tuning["assembly"] == 1
+    if tiled:
+        info["tiles"] = dmesh.tile_info()
 
     def step(k):
-        ev.evaluate(d_phis[k % N_STATES], flow, jacobian=True, keep_state=False)
+        ev.evaluate(d_phis[k % N_STATES], flow, jacobian=True, keep_state="upstream")
 
     for w in range(max(args.warmup, 3)):
         step(w)
@@ -834,6 +986,21 @@ def run_ours(args):
         prof = L.profile_read()
         L.profile(False)
         ms = t_start.elapsed_time(t_stop)
+
+        # ---- sustained: the same step for about two seconds (at least 200
+        # steps), so that the clock record covers a long stretch of work
+        n_sus = max(200, int(2000.0 / max(ms / max(args.steps, 1), 1e-3)))
+        barrier()
+        torch.cuda.synchronize()
+        s_start = torch.cuda.Event(enable_timing=True)
+        s_stop = torch.cuda.Event(enable_timing=True)
+        s_start.record(stream)
+        for k in range(n_sus):
+            step(k)
+        s_stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        sus_ms = s_start.elapsed_time(s_stop)
 
         # ---- end-to-end through the public API with host buffers: every
         # step uploads its phi and downloads R and the Jacobian data; the
@@ -912,18 +1079,35 @@ def run_ours(args):
     lifting = lifting_timing(args.lifting) if args.lifting else None
     naca = naca_timing() if args.naca else None
 
-    ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
+    parity = bench_parity(mesh, order, ev, flow, d_phis, phis, args.parity >= 2) if args.parity else None
+    linear = linear_timing(ev, dmesh, mesh, order, d_phis[0], flow) if args.linear else None
+
+    ms, e2e_ms, sus_ms = max_over_ranks([ms, e2e_ms, sus_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
     e2e_value = dmesh.n_tets * n_e2e * world / (e2e_ms * 1e-3) / 1e6
 
     # roofline of the dominant kernel, timed live over the timed region
     bm = bytes_model(info, n_active=int(mon["n_term3_active"]))
-    dom = max(("elem_sweep", "row_gather"), key=lambda s: prof[s]["ms"])
-    per_launch_ms = prof[dom]["ms"] / max(prof[dom]["calls"], 1)
-    achieved = bm[dom] / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = read_peaks()
-    traffic = read_traffic(dom)
+    if tiled:
+        # the tile kernel does both passes' work (every element, every
+        # output of the tile); the combine adds the partials of outputs
+        # shared by tiles: the pair is timed and credited together
+        dom = "tile_eval+combine"
+        calls = max(prof["elem_sweep"]["calls"], 1)
+        per_launch_ms = (prof["elem_sweep"]["ms"] + prof["row_gather"]["ms"]) / calls
+        dom_bytes = bm["elem_sweep"] + bm["row_gather"]
+        design_bytes = bm["design"]["tile_eval"]
+        traffic = read_traffic("tile_eval")
+    else:
+        dom = max(("elem_sweep", "row_gather"), key=lambda s: prof[s]["ms"])
+        per_launch_ms = prof[dom]["ms"] / max(prof[dom]["calls"], 1)
+        dom_bytes = bm[dom]
+        design_bytes = bm["design"][dom]
+        traffic = read_traffic(dom)
+    achieved = dom_bytes / (per_launch_ms * 1e-3) / 1e9
     step_bytes = bm["fused"]
+    phase_names = {"elem_sweep": "tile_eval", "row_gather": "combine"} if tiled else {}
 
     if rank == 0:
         cpu = None
@@ -938,19 +1122,28 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(shape, mesh, dmesh.nnz),
+            "config": config_dict(shape, mesh),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "traffic": traffic,
-                         "algorithmic_bytes": bm[dom],
-                         "design_bytes": bm["design"][dom],
+                         "algorithmic_bytes": dom_bytes,
+                         "design_bytes": design_bytes,
                          "ms_per_launch": round(per_launch_ms, 5)},
             "step_roofline": {"algorithmic_bytes": step_bytes,
                               "achieved_gbs": round(step_bytes / (ms / args.steps * 1e-3) / 1e9, 1),
                               "frac": round(step_bytes / (ms / args.steps * 1e-3) / 1e9 / peak, 4),
-                              "phases_ms_per_step": {k: round(v["ms"] / max(args.steps, 1), 5)
+                              "phases_ms_per_step": {phase_names.get(k, k): round(v["ms"] / max(args.steps, 1), 5)
                                                      for k, v in prof.items() if v["calls"]}},
+            "sustained": {"steps": n_sus, "ms_per_step": round(sus_ms / n_sus, 5),
+                          "value": round(dmesh.n_tets * n_sus * world / (sus_ms * 1e-3) / 1e6, 3),
+                          "unit": "Melem/s",
+                          "note": "the timed step repeated for ~2 s right after the timed region, "
+                                  "inside the clock record"},
+            "assembly": "tiled" if tiled else "two-pass",
+            "tiles": info.get("tiles"),
+            "parity": parity,
+            "linear": linear,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 3), "unit": "Melem/s",
                     "h2d_bytes_per_step": 8 * dmesh.n_nodes,
