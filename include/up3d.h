@@ -487,6 +487,22 @@ typedef struct {
 } up3d_tile_info;
 int up3d_mesh_tile_info(up3d_mesh* mesh, int32_t tile_elems, up3d_tile_info* info, up3d_stream stream);
 
+/* The same plan built on the host from host arrays, for tests and
+ * inspection (no device is touched): elements and face_neighbors (n_tets,
+ * 4) int32, centroids (n_tets, 3), the P1 pattern (indptr, indices).
+ * up3d_tile_plan_host_array copies one named array of the plan ("perm",
+ * "iperm", "eoff", "noff", "uoff", "tnode", "lconn", "nent_off", "nent",
+ * "ndst", "uent_off", "uent", "udst", "cn_off", "cn_idx", "cn_dst",
+ * "ce_off", "ce_idx", "ce_dst", "fnbr") into dst (NULL: size only) and
+ * returns its byte size. */
+typedef struct up3d_tile_plan up3d_tile_plan; /* opaque host-side plan */
+int up3d_tile_plan_host_create(const int32_t* elements, const int32_t* face_neighbors, const double* centroids,
+                               int64_t n_nodes, int64_t n_tets, const int32_t* indptr, const int32_t* indices,
+                               int32_t tile_elems, up3d_tile_plan** out);
+int up3d_tile_plan_host_info(const up3d_tile_plan* plan, up3d_tile_info* info);
+int up3d_tile_plan_host_array(const up3d_tile_plan* plan, const char* name, void* dst, int64_t* nbytes);
+int up3d_tile_plan_host_destroy(up3d_tile_plan* plan);
+
 /* Times every candidate shape of the two passes on this mesh (the Newton
  * Jacobian sweep at phi and the flow, live upwind selection; `reps` timed
  * launches each after one warm-up, median kept), then the tiled form at

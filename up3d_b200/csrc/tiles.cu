@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cstring>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "tiles.cuh"
@@ -102,23 +103,45 @@ constexpr int PAIR_J[6] = {1, 2, 3, 2, 3, 3};
 
 }  // namespace
 
-void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
-    if (m->tiles && m->tiles->T == T) return;
+// The plan as host arrays (uploaded as they are into a TilePlan).
+struct PlanHost {
+    int32_t T = 0, max_nodes = 0;
+    int64_t n_tiles = 0, n_tile_nodes = 0, n_tile_edges = 0, n_part = 0;
+    std::vector<int32_t> perm, iperm, eoff, noff, uoff, tnode, nent_off, uent_off;
+    std::vector<ushort4> lconn;
+    std::vector<uint16_t> nent, uent;
+    std::vector<int2> ndst, udst, cn_dst, ce_dst;
+    std::vector<int32_t> cn_off, cn_idx, ce_off, ce_idx;
+    std::vector<int4> conn_t, fn_t;
+    std::vector<double4> cen_t;
+};
+
+// Builds the plan from host copies of the mesh data: connectivity, face
+// neighbours, centroids and the P1 pattern (sorted rows).
+PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>& fn, const std::vector<double4>& cen,
+                         int64_t N, const std::vector<int32_t>& indptr, const std::vector<int32_t>& indices,
+                         int T) {
     UP3D_REQUIRE(T == 128 || T == 256, UP3D_ERR_VALUE, "tile plan: tile_elems must be 128 or 256");
-    const auto t_start = std::chrono::steady_clock::now();
-    const int64_t E = m->E, N = m->N, Z = m->nnz;
-    // ---- host copies of the mesh data the plan needs
-    std::vector<int4> conn(E), fn(E);
-    std::vector<double4> cen(E);
-    std::vector<int32_t> indptr(N + 1), indices(Z), diag(N), zt(Z);
-    UP3D_CUDA(cudaMemcpyAsync(conn.data(), m->conn.get(), sizeof(int4) * E, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(fn.data(), m->fnbr.get(), sizeof(int4) * E, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(cen.data(), m->cen.get(), sizeof(double4) * E, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(indptr.data(), m->indptr.get(), sizeof(int32_t) * (N + 1), cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(indices.data(), m->indices.get(), sizeof(int32_t) * Z, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(diag.data(), m->diag.get(), sizeof(int32_t) * N, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaMemcpyAsync(zt.data(), m->zt.get(), sizeof(int32_t) * Z, cudaMemcpyDeviceToHost, s));
-    UP3D_CUDA(cudaStreamSynchronize(s));
+    const int64_t E = (int64_t)conn.size(), Z = (int64_t)indices.size();
+    // absolute diagonal slot of each row (-1 for an empty row) and the
+    // transposed slot of every entry
+    auto find = [&](int32_t r, int32_t c) -> int32_t {
+        const int32_t* b = indices.data() + indptr[r];
+        const int32_t* e = indices.data() + indptr[r + 1];
+        const int32_t* f = std::lower_bound(b, e, c);
+        return (f == e || *f != c) ? -1 : (int32_t)(f - indices.data());
+    };
+    std::vector<int32_t> diag(N), zt(Z);
+    int bad_pattern = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_pattern)
+    for (int64_t r = 0; r < N; ++r) {
+        diag[r] = find((int32_t)r, (int32_t)r);
+        for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k) {
+            zt[k] = find(indices[k], (int32_t)r);
+            if (zt[k] < 0) bad_pattern = 1;
+        }
+    }
+    UP3D_REQUIRE(!bad_pattern, UP3D_ERR_VALUE, "tile plan: the pattern is not structurally symmetric");
 
     // ---- 1. components of the face graph, in order of their smallest element
     Dsu dsu(E);
@@ -377,44 +400,91 @@ void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
         fn_t[x] = make_int4(nb[0], nb[1], nb[2], nb[3]);
     }
 
-    // ---- upload
+    PlanHost H;
+    H.T = T;
+    H.max_nodes = max_nodes;
+    H.n_tiles = n_tiles;
+    H.n_tile_nodes = n_tn;
+    H.n_tile_edges = n_te;
+    H.n_part = q;
+    H.perm = std::move(order);
+    H.iperm = std::move(iperm);
+    H.eoff = std::move(eoff);
+    H.noff = std::move(noff);
+    H.uoff = std::move(uoff);
+    H.tnode = std::move(tnode);
+    H.lconn = std::move(lconn);
+    H.nent_off = std::move(nent_off);
+    H.nent = std::move(nent);
+    H.ndst = std::move(ndst);
+    H.uent_off = std::move(uent_off);
+    H.uent = std::move(uent);
+    H.udst = std::move(udst);
+    H.cn_off = std::move(cn_off);
+    H.cn_idx = std::move(cn_idx);
+    H.cn_dst = std::move(cn_dst);
+    H.ce_off = std::move(ce_off);
+    H.ce_idx = std::move(ce_idx);
+    H.ce_dst = std::move(ce_dst);
+    H.conn_t = std::move(conn_t);
+    H.fn_t = std::move(fn_t);
+    H.cen_t = std::move(cen_t);
+    return H;
+}
+
+void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
+    if (m->tiles && m->tiles->T == T) return;
+    UP3D_REQUIRE(T == 128 || T == 256, UP3D_ERR_VALUE, "tile plan: tile_elems must be 128 or 256");
+    const auto t_start = std::chrono::steady_clock::now();
+    const int64_t E = m->E, N = m->N, Z = m->nnz;
+    // host copies of the mesh data the plan needs
+    std::vector<int4> conn(E), fn(E);
+    std::vector<double4> cen(E);
+    std::vector<int32_t> indptr(N + 1), indices(Z);
+    UP3D_CUDA(cudaMemcpyAsync(conn.data(), m->conn.get(), sizeof(int4) * E, cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(fn.data(), m->fnbr.get(), sizeof(int4) * E, cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(cen.data(), m->cen.get(), sizeof(double4) * E, cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(indptr.data(), m->indptr.get(), sizeof(int32_t) * (N + 1), cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaMemcpyAsync(indices.data(), m->indices.get(), sizeof(int32_t) * Z, cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    PlanHost H = build_plan_host(conn, fn, cen, N, indptr, indices, T);
     auto P = std::make_shared<TilePlan>();
     P->T = T;
-    P->n_tiles = n_tiles;
-    P->max_nodes = max_nodes;
-    P->n_tile_nodes = n_tn;
-    P->n_tile_edges = n_te;
-    P->n_part = q;
-    P->n_cnode = (int64_t)cn_dst.size();
-    P->n_cedge = (int64_t)ce_dst.size();
+    P->n_tiles = H.n_tiles;
+    P->max_nodes = H.max_nodes;
+    P->n_tile_nodes = H.n_tile_nodes;
+    P->n_tile_edges = H.n_tile_edges;
+    P->n_part = H.n_part;
+    P->n_cnode = (int64_t)H.cn_dst.size();
+    P->n_cedge = (int64_t)H.ce_dst.size();
     auto up = [&](auto& buf, const auto& vec) {
         buf.alloc(vec.size());
         if (!vec.empty())
             UP3D_CUDA(cudaMemcpyAsync(buf.get(), vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice, s));
     };
-    up(P->perm, order);
-    up(P->iperm, iperm);
-    up(P->conn, conn_t);
-    up(P->fnbr, fn_t);
-    up(P->cen, cen_t);
-    up(P->eoff, eoff);
-    up(P->noff, noff);
-    up(P->uoff, uoff);
-    up(P->tnode, tnode);
-    up(P->lconn, lconn);
-    up(P->nent_off, nent_off);
-    up(P->nent, nent);
-    up(P->ndst, ndst);
-    up(P->uent_off, uent_off);
-    up(P->uent, uent);
-    up(P->udst, udst);
-    P->part.alloc(std::max<int64_t>(q, 1));
-    up(P->cn_off, cn_off);
-    up(P->cn_idx, cn_idx);
-    up(P->cn_dst, cn_dst);
-    up(P->ce_off, ce_off);
-    up(P->ce_idx, ce_idx);
-    up(P->ce_dst, ce_dst);
+    up(P->perm, H.perm);
+    up(P->iperm, H.iperm);
+    up(P->conn, H.conn_t);
+    up(P->fnbr, H.fn_t);
+    up(P->cen, H.cen_t);
+    up(P->eoff, H.eoff);
+    up(P->noff, H.noff);
+    up(P->uoff, H.uoff);
+    up(P->tnode, H.tnode);
+    up(P->lconn, H.lconn);
+    up(P->nent_off, H.nent_off);
+    up(P->nent, H.nent);
+    up(P->ndst, H.ndst);
+    up(P->uent_off, H.uent_off);
+    up(P->uent, H.uent);
+    up(P->udst, H.udst);
+    P->part.alloc(std::max<int64_t>(H.n_part, 1));
+    up(P->cn_off, H.cn_off);
+    up(P->cn_idx, H.cn_idx);
+    up(P->cn_dst, H.cn_dst);
+    up(P->ce_off, H.ce_off);
+    up(P->ce_idx, H.ce_idx);
+    up(P->ce_dst, H.ce_dst);
     UP3D_CUDA(cudaStreamSynchronize(s));
     P->build_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     m->tiles = P;
@@ -441,6 +511,101 @@ int up3d_mesh_tile_info(up3d_mesh* m, int32_t tile_elems, up3d_tile_info* info, 
         info->n_combined_slots = P.n_cedge;
         info->build_s = P.build_s;
     });
+}
+
+// Host-side plan for tests and inspection (no device involved).
+struct up3d_tile_plan {
+    up3d::PlanHost H;
+};
+
+int up3d_tile_plan_host_create(const int32_t* elements, const int32_t* face_neighbors, const double* centroids,
+                               int64_t n_nodes, int64_t n_tets, const int32_t* indptr, const int32_t* indices,
+                               int32_t tile_elems, up3d_tile_plan** out) {
+    return guarded([&] {
+        UP3D_REQUIRE(elements && face_neighbors && centroids && indptr && indices && out, UP3D_ERR_ARGUMENT,
+                     "up3d_tile_plan_host_create: null argument");
+        UP3D_REQUIRE(n_nodes > 0 && n_tets > 0 && n_tets < (1ll << 29), UP3D_ERR_VALUE,
+                     "up3d_tile_plan_host_create: bad sizes");
+        std::vector<int4> conn(n_tets), fn(n_tets);
+        std::vector<double4> cen(n_tets);
+        for (int64_t e = 0; e < n_tets; ++e) {
+            const int32_t* c = elements + 4 * e;
+            const int32_t* f = face_neighbors + 4 * e;
+            for (int k = 0; k < 4; ++k)
+                UP3D_REQUIRE(c[k] >= 0 && c[k] < n_nodes, UP3D_ERR_VALUE,
+                             "up3d_tile_plan_host_create: node index out of range");
+            conn[e] = make_int4(c[0], c[1], c[2], c[3]);
+            fn[e] = make_int4(f[0], f[1], f[2], f[3]);
+            cen[e] = make_double4(centroids[3 * e], centroids[3 * e + 1], centroids[3 * e + 2], 0.0);
+        }
+        const int64_t Z = indptr[n_nodes];
+        std::vector<int32_t> ip(indptr, indptr + n_nodes + 1), ix(indices, indices + Z);
+        auto* h = new up3d_tile_plan();
+        try {
+            h->H = build_plan_host(conn, fn, cen, n_nodes, ip, ix, tile_elems);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int up3d_tile_plan_host_array(const up3d_tile_plan* h, const char* name, void* dst, int64_t* nbytes) {
+    return guarded([&] {
+        UP3D_REQUIRE(h && name && nbytes, UP3D_ERR_ARGUMENT, "up3d_tile_plan_host_array: null argument");
+        const PlanHost& H = h->H;
+        const std::string n(name);
+        const void* src = nullptr;
+        size_t bytes = 0;
+        auto pick = [&](const auto& v) {
+            src = v.data();
+            bytes = sizeof(v[0]) * v.size();
+        };
+        if (n == "perm") pick(H.perm);
+        else if (n == "iperm") pick(H.iperm);
+        else if (n == "eoff") pick(H.eoff);
+        else if (n == "noff") pick(H.noff);
+        else if (n == "uoff") pick(H.uoff);
+        else if (n == "tnode") pick(H.tnode);
+        else if (n == "lconn") pick(H.lconn);
+        else if (n == "nent_off") pick(H.nent_off);
+        else if (n == "nent") pick(H.nent);
+        else if (n == "ndst") pick(H.ndst);
+        else if (n == "uent_off") pick(H.uent_off);
+        else if (n == "uent") pick(H.uent);
+        else if (n == "udst") pick(H.udst);
+        else if (n == "cn_off") pick(H.cn_off);
+        else if (n == "cn_idx") pick(H.cn_idx);
+        else if (n == "cn_dst") pick(H.cn_dst);
+        else if (n == "ce_off") pick(H.ce_off);
+        else if (n == "ce_idx") pick(H.ce_idx);
+        else if (n == "ce_dst") pick(H.ce_dst);
+        else if (n == "fnbr") pick(H.fn_t);
+        else UP3D_REQUIRE(false, UP3D_ERR_VALUE, "up3d_tile_plan_host_array: unknown array " + n);
+        *nbytes = (int64_t)bytes;
+        if (dst && bytes) std::memcpy(dst, src, bytes);
+    });
+}
+
+int up3d_tile_plan_host_info(const up3d_tile_plan* h, up3d_tile_info* info) {
+    return guarded([&] {
+        UP3D_REQUIRE(h && info, UP3D_ERR_ARGUMENT, "up3d_tile_plan_host_info: null argument");
+        const PlanHost& H = h->H;
+        info->tile_elems = H.T;
+        info->max_nodes = H.max_nodes;
+        info->n_tiles = H.n_tiles;
+        info->n_tile_nodes = H.n_tile_nodes;
+        info->n_tile_edges = H.n_tile_edges;
+        info->n_partials = H.n_part;
+        info->n_combined_nodes = (int64_t)H.cn_dst.size();
+        info->n_combined_slots = (int64_t)H.ce_dst.size();
+        info->build_s = 0.0;
+    });
+}
+
+int up3d_tile_plan_host_destroy(up3d_tile_plan* h) {
+    return guarded([&] { delete h; });
 }
 
 }  // extern "C"
