@@ -232,12 +232,21 @@ int up3d_jacobian_nnz(up3d_mesh* mesh, const double* data, int64_t* newton_nnz,
  * and `branch_frozen` are non-NULL), sensitivities, residual R (n_nodes) and
  * the Newton Jacobian data on the P1 pattern (NULL skips the Jacobian).
  * Monitors (device, may be NULL).  rho_tilde_out / upstream_out (device,
- * may be NULL) receive the flux and the walk. */
+ * may be NULL) receive the flux and the walk.  Term 3 (kernels/jacobian.py:
+ * 184-229, :344-358): the merge is built symbolically (one warp per row)
+ * while the set of active elements or their upstream elements change; once
+ * the same pattern comes twice in a row its per-destination contributor
+ * lists are recorded, and while it repeats (the frozen finish, late Newton
+ * steps) Term 3 is a values-only sum per destination in the same order --
+ * the same bits. */
 int up3d_residual_jacobian(up3d_mesh* mesh, const double* phi, const up3d_flow* flow,
                            const int64_t* upstream_frozen, const int8_t* branch_frozen,
                            double* R, double* data, double* rho_tilde_out,
                            int32_t* upstream_out, up3d_monitors* monitors,
                            up3d_stream stream);
+/* Term-3 builds served by the values-only path on this mesh so far (no
+ * reference counterpart). */
+int up3d_mesh_term3_cache_hits(const up3d_mesh* mesh, int64_t* hits);
 
 /* ------------------------------------------------------ adjoint */
 

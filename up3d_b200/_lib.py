@@ -144,6 +144,7 @@ SIGNATURES = {
     "up3d_mesh_get_tuning": (_int, [_p, ctypes.POINTER(Tuning)]),
     "up3d_autotune": (_int, [_p, _p, ctypes.POINTER(Flow), _int, ctypes.POINTER(Tuning), _p]),
     "up3d_mesh_tile_info": (_int, [_p, _i32, ctypes.POINTER(TileInfo), _p]),
+    "up3d_mesh_term3_cache_hits": (_int, [_p, ctypes.POINTER(_i64)]),
     "up3d_tile_plan_host_create": (_int, [_p, _p, _p, _i64, _i64, _p, _p, _i32, ctypes.POINTER(_p)]),
     "up3d_tile_plan_host_info": (_int, [_p, ctypes.POINTER(TileInfo)]),
     "up3d_tile_plan_host_array": (_int, [_p, ctypes.c_char_p, _p, ctypes.POINTER(_i64)]),

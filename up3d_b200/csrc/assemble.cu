@@ -902,13 +902,19 @@ __global__ void __launch_bounds__(256)
 // each column's run is summed left to right and either added to the P1
 // slot (data) or, off the pattern, written to the row's extras scratch at
 // 4 ent_off[n] (at most 4 deg(n) columns), with the count in x_cnt[n].
-template <int WARPS>
+//
+// RECORD also writes, for the symbolic cache, every entry's code
+// (e << 4 | i << 2 | k) and destination at 4 ent_off[n] + position: the P1
+// slot, or -1 - (the extra's rank in its row); unused positions of the
+// row's region get INT32_MAX.
+template <int WARPS, bool RECORD>
 __global__ void __launch_bounds__(WARPS * 32)
     k_t3_rows(int64_t N, int cap, const int32_t* __restrict__ ent_off, const uint32_t* __restrict__ ent,
               const uint8_t* __restrict__ flag, const int32_t* __restrict__ up, const int4* __restrict__ conn,
               const double* __restrict__ t3v, const int32_t* __restrict__ indptr,
               const int32_t* __restrict__ indices, double* __restrict__ data, int32_t* __restrict__ xs_col,
-              double* __restrict__ xs_val, int32_t* __restrict__ x_cnt) {
+              double* __restrict__ xs_val, int32_t* __restrict__ x_cnt, uint32_t* __restrict__ rec_code,
+              int32_t* __restrict__ rec_key) {
     extern __shared__ __align__(16) unsigned char t3_smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* col0 = reinterpret_cast<int32_t*>(t3_smem) + (size_t)w * cap;
@@ -916,6 +922,11 @@ __global__ void __launch_bounds__(WARPS * 32)
     double* val0 = reinterpret_cast<double*>(t3_smem + (size_t)2 * WARPS * cap * sizeof(int32_t)) + (size_t)w * cap;
     double* val1 = reinterpret_cast<double*>(t3_smem + (size_t)2 * WARPS * cap * sizeof(int32_t)) +
                    (size_t)(WARPS + w) * cap;
+    // RECORD: each entry's distinct-column index and each distinct
+    // column's destination
+    unsigned char* rec_base = t3_smem + (size_t)2 * WARPS * cap * (sizeof(int32_t) + sizeof(double));
+    int16_t* eidx = reinterpret_cast<int16_t*>(rec_base) + (size_t)w * cap;
+    int32_t* dd = reinterpret_cast<int32_t*>(rec_base + (size_t)WARPS * cap * sizeof(int16_t)) + (size_t)w * cap;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -939,6 +950,11 @@ __global__ void __launch_bounds__(WARPS * 32)
                 const double* t = t3v + 8 * e;
                 const double ai = t[i];
                 const int pos = P + 4 * __popc(m & lt);
+                if (RECORD) {
+                    uint32_t* rc = rec_code + 4 * (int64_t)eb + pos;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) rc[k] = ((uint32_t)e << 4) | (uint32_t)(i << 2) | (uint32_t)k;
+                }
                 col0[pos] = cu.x;
                 col0[pos + 1] = cu.y;
                 col0[pos + 2] = cu.z;
@@ -952,6 +968,8 @@ __global__ void __launch_bounds__(WARPS * 32)
         }
         if (P == 0) {
             if (lane == 0) x_cnt[n] = 0;
+            if (RECORD)
+                for (int p = lane; p < 4 * deg; p += 32) rec_key[4 * (int64_t)eb + p] = INT32_MAX;
             continue;
         }
         __syncwarp();
@@ -984,6 +1002,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                     const int j = __ffs(gm) - 1;
                     gm &= gm - 1;
                     acc_c += val0[base + j];
+                    if (RECORD) eidx[base + j] = (int16_t)idx;
                 }
                 col1[idx] = c;
                 val1[idx] = acc_c;
@@ -1004,6 +1023,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             }
             const bool in_pattern = lo < L && indices[rb + lo] == c;
             if (in_pattern) data[rb + lo] += val1[d];
+            if (RECORD && in_pattern) dd[d] = rb + lo;
             col0[d] = in_pattern ? INT32_MAX : c;  // extra columns, for the ranks
         }
         __syncwarp();
@@ -1018,11 +1038,16 @@ __global__ void __launch_bounds__(WARPS * 32)
                 const int64_t o = 4 * (int64_t)eb + r;
                 xs_col[o] = c;
                 xs_val[o] = val1[d];
+                if (RECORD) dd[d] = -1 - r;
             }
             X += __popc(__ballot_sync(0xffffffffu, extra));
         }
         if (lane == 0) x_cnt[n] = X;
         __syncwarp();
+        if (RECORD) {
+            for (int p = lane; p < 4 * deg; p += 32) rec_key[4 * (int64_t)eb + p] = p < P ? dd[eidx[p]] : INT32_MAX;
+            __syncwarp();
+        }
     }
 }
 
@@ -1043,6 +1068,48 @@ __global__ void k_t3_compact(int64_t N, const int32_t* __restrict__ ent_off, con
             x_val[o + j] = xs_val[src + j];
         }
     }
+}
+
+// Symbolic cache of Term 3: extras' destinations made global (Z + the
+// extra's compacted position), then -- per destination, contributors in the
+// order the row kernel sums them -- the values-only rebuild.
+__global__ void k_t3_rec_fix(int64_t N, const int32_t* __restrict__ ent_off, const int32_t* __restrict__ x_ptr,
+                             int64_t Z, int32_t* __restrict__ rec_key) {
+    GRID_STRIDE(n, N) {
+        const int64_t b = 4 * (int64_t)ent_off[n], e = 4 * (int64_t)ent_off[n + 1];
+        for (int64_t p = b; p < e; ++p) {
+            const int32_t k = rec_key[p];
+            if (k < 0) rec_key[p] = (int32_t)(Z + x_ptr[n] + (-1 - k));
+        }
+    }
+}
+
+__global__ void k_t3_values(int64_t n_seg, const int32_t* __restrict__ seg, const int32_t* __restrict__ key,
+                            const uint32_t* __restrict__ code, const double* __restrict__ t3v, int64_t Z,
+                            double* __restrict__ data, double* __restrict__ x_val) {
+    GRID_STRIDE(d, n_seg) {
+        double v = 0.0;
+        const int32_t j1 = seg[d + 1];
+        for (int32_t j = seg[d]; j < j1; ++j) {
+            const uint32_t c = code[j];
+            const double* t = t3v + 8 * (int64_t)(c >> 4);
+            v += t[(c >> 2) & 3] * t[4 + (c & 3)];
+        }
+        const int32_t k = key[d];
+        if (k < Z) data[k] += v;
+        else x_val[k - Z] = v;
+    }
+}
+
+// Elements whose Term-3 activity or (active) upstream differ from the
+// recorded signature.
+__global__ void k_t3_sig_diff(int64_t E, const uint8_t* __restrict__ flag, const int32_t* __restrict__ up,
+                              const uint8_t* __restrict__ cflag, const int32_t* __restrict__ cup,
+                              unsigned long long* out) {
+    unsigned long long c = 0;
+    GRID_STRIDE(e, E) c += (flag[e] != cflag[e]) || (flag[e] && up[e] != cup[e]);
+    c = warp_sum_u64(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
 __global__ void k_count_flags(const uint8_t* __restrict__ f, int64_t n, unsigned long long* out) {
@@ -1147,7 +1214,7 @@ constexpr int T3_WARPS = 4;
 static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_active, int64_t& n_extra,
                         int64_t known_active = -1, const int32_t* upstream = nullptr) {
     if (!upstream) upstream = m->up32.get();
-    const int64_t E = m->E, N = m->N;
+    const int64_t E = m->E, N = m->N, Z = m->nnz;
     n_extra = 0;
     m->last_extra = 0;
     m->i64_ws.alloc(8);
@@ -1162,19 +1229,54 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
     n_active = known_active;
     m->last_active = n_active;
     if (n_active == 0) return;
+    // the symbolic cache: is the pattern the recorded one?
+    const bool cacheable = E < (1ll << 28) && Z + 16 * E < INT32_MAX;
+    bool same = false;
+    if (cacheable && m->t3c_state >= 1 && m->t3c_active == n_active) {
+        unsigned long long* c = reinterpret_cast<unsigned long long*>(m->i64_ws.get() + 3);
+        UP3D_CUDA(cudaMemsetAsync(c, 0, sizeof(unsigned long long), s));
+        k_t3_sig_diff<<<grid_for(E, 256), 256, 0, s>>>(E, m->t3_flag.get(), upstream, m->t3c_flag.get(),
+                                                      m->t3c_up.get(), c);
+        UP3D_CHECK_LAUNCH();
+        unsigned long long diff = 1;
+        UP3D_CUDA(cudaMemcpyAsync(&diff, c, sizeof(diff), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        same = diff == 0;
+    }
+    if (same && m->t3c_state == 2) {
+        // values only: the P1 slots and extras of the recorded pattern
+        if (m->t3c_nseg > 0) {
+            k_t3_values<<<grid_for(m->t3c_nseg, 256, (int64_t)m->n_sms * 16), 256, 0, s>>>(
+                m->t3c_nseg, m->t3c_seg.get(), m->t3c_key.get(), m->t3c_code.get(), m->t3v.get(), Z, data,
+                m->x_val_c.get());
+            UP3D_CHECK_LAUNCH();
+        }
+        n_extra = m->t3c_extra;
+        m->last_extra = n_extra;
+        m->t3c_hits += 1;
+        return;
+    }
+    // a pattern seen twice in a row is recorded for the calls that follow
+    const bool record = cacheable && same;
     const int cap = 4 * std::max<int32_t>(m->max_deg, 1);
-    const size_t smem = (size_t)T3_WARPS * cap * 2 * (sizeof(int32_t) + sizeof(double));
+    const size_t smem = (size_t)T3_WARPS * cap * 2 * (sizeof(int32_t) + sizeof(double)) +
+                        (size_t)T3_WARPS * cap * (sizeof(int16_t) + sizeof(int32_t));
     UP3D_REQUIRE(smem <= 227 * 1024, UP3D_ERR_VALUE, "Term 3: node degree too large for the row kernel");
-    if (smem > 48 * 1024)
-        UP3D_CUDA(cudaFuncSetAttribute(k_t3_rows<T3_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = record ? k_t3_rows<T3_WARPS, true> : k_t3_rows<T3_WARPS, false>;
+    if (smem > 48 * 1024) UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     m->x_col.alloc(16 * E);
     m->x_val.alloc(16 * E);
     m->extra_cnt.alloc(N + 1);
     m->x_ptr.alloc(N + 1);
+    if (record) {
+        m->t3c_code_tmp.alloc(16 * E);
+        m->t3c_key_tmp.alloc(16 * E);
+    }
     UP3D_CUDA(cudaMemsetAsync(m->extra_cnt.get() + N, 0, sizeof(int32_t), s));
-    k_t3_rows<T3_WARPS><<<grid_for(32 * N, T3_WARPS * 32, (int64_t)148 * 32), T3_WARPS * 32, smem, s>>>(
+    kern<<<grid_for(32 * N, T3_WARPS * 32, (int64_t)148 * 32), T3_WARPS * 32, smem, s>>>(
         N, cap, m->ent_off.get(), m->ent.get(), m->t3_flag.get(), upstream, m->conn.get(), m->t3v.get(),
-        m->indptr.get(), m->indices.get(), data, m->x_col.get(), m->x_val.get(), m->extra_cnt.get());
+        m->indptr.get(), m->indices.get(), data, m->x_col.get(), m->x_val.get(), m->extra_cnt.get(),
+        record ? m->t3c_code_tmp.get() : nullptr, record ? m->t3c_key_tmp.get() : nullptr);
     UP3D_CHECK_LAUNCH();
     scan(m, m->extra_cnt.get(), m->x_ptr.get(), N + 1, s);
     int32_t total = 0;
@@ -1191,6 +1293,54 @@ static void build_term3(up3d_mesh* m, double* data, cudaStream_t s, int64_t& n_a
                                                       m->x_val_c.get());
         UP3D_CHECK_LAUNCH();
     }
+    if (!cacheable) return;
+    if (record) {
+        // destinations made global, a stable sort by destination (row-major
+        // entry order kept within each), then the runs
+        k_t3_rec_fix<<<grid_for(N, 256), 256, 0, s>>>(N, m->ent_off.get(), m->x_ptr.get(), Z, m->t3c_key_tmp.get());
+        UP3D_CHECK_LAUNCH();
+        const int64_t n_items = 16 * E;
+        m->t3c_code.alloc(n_items);
+        m->t3c_key.alloc(n_items);
+        size_t bytes = 0;
+        UP3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, m->t3c_key_tmp.get(), m->t3c_key.get(),
+                                                  m->t3c_code_tmp.get(), m->t3c_code.get(), n_items, 0, 31, s));
+        m->cub_tmp.alloc(bytes);
+        UP3D_CUDA(cub::DeviceRadixSort::SortPairs(m->cub_tmp.get(), bytes, m->t3c_key_tmp.get(), m->t3c_key.get(),
+                                                  m->t3c_code_tmp.get(), m->t3c_code.get(), n_items, 0, 31, s));
+        // the valid entries (16 per active element) sort before the INT32_MAX fill
+        const int64_t n_valid = 16 * n_active;
+        m->t3c_cnt.alloc(n_valid + 1);
+        m->t3c_seg.alloc(n_valid + 1);
+        m->t3c_nruns.alloc(1);
+        // unique keys over the sorted prefix, written over the front of the
+        // tmp key array
+        bytes = 0;
+        UP3D_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, bytes, m->t3c_key.get(), m->t3c_key_tmp.get(),
+                                                     m->t3c_cnt.get(), m->t3c_nruns.get(), n_valid, s));
+        m->cub_tmp.alloc(bytes);
+        UP3D_CUDA(cub::DeviceRunLengthEncode::Encode(m->cub_tmp.get(), bytes, m->t3c_key.get(), m->t3c_key_tmp.get(),
+                                                     m->t3c_cnt.get(), m->t3c_nruns.get(), n_valid, s));
+        int64_t nruns = 0;
+        UP3D_CUDA(cudaMemcpyAsync(&nruns, m->t3c_nruns.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        UP3D_CUDA(cudaMemsetAsync(m->t3c_cnt.get() + nruns, 0, sizeof(int32_t), s));
+        scan(m, m->t3c_cnt.get(), m->t3c_seg.get(), nruns + 1, s);
+        // keep the run keys (destinations) where the values kernel reads them
+        UP3D_CUDA(cudaMemcpyAsync(m->t3c_key.get(), m->t3c_key_tmp.get(), sizeof(int32_t) * nruns,
+                                  cudaMemcpyDeviceToDevice, s));
+        UP3D_CUDA(cudaStreamSynchronize(s));
+        m->t3c_nseg = nruns;
+        m->t3c_state = 2;
+    } else {
+        m->t3c_flag.alloc(E);
+        m->t3c_up.alloc(E);
+        UP3D_CUDA(cudaMemcpyAsync(m->t3c_flag.get(), m->t3_flag.get(), E, cudaMemcpyDeviceToDevice, s));
+        UP3D_CUDA(cudaMemcpyAsync(m->t3c_up.get(), upstream, sizeof(int32_t) * E, cudaMemcpyDeviceToDevice, s));
+        m->t3c_state = 1;
+    }
+    m->t3c_active = n_active;
+    m->t3c_extra = n_extra;
 }
 
 static int64_t merged_nnz(up3d_mesh* m, const double* data, cudaStream_t s) {
@@ -1565,6 +1715,13 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
         UP3D_REQUIRE(t->tile_elems == 128 || t->tile_elems == 256, UP3D_ERR_VALUE,
                      "up3d_mesh_set_tuning: tile_elems must be 128 or 256");
         m->tune = *t;
+    });
+}
+
+int up3d_mesh_term3_cache_hits(const up3d_mesh* m, int64_t* hits) {
+    return guarded([&] {
+        UP3D_REQUIRE(m && hits, UP3D_ERR_ARGUMENT, "up3d_mesh_term3_cache_hits: null argument");
+        *hits = m->t3c_hits;
     });
 }
 

@@ -168,6 +168,18 @@ struct up3d_mesh {
     up3d::DBuf<int32_t> x_ptr;         // (N+1) extras row pointer
     up3d::DBuf<int32_t> x_row_c, x_col_c;  // extras, (row, col) order
     up3d::DBuf<double> x_val_c;
+    // Term-3 symbolic cache: while the active set and the active elements'
+    // upstream repeat, Term 3 is a values-only sum per destination
+    // (t3c_state 0: nothing recorded, 1: signature only, 2: cache valid)
+    int t3c_state = 0;
+    int64_t t3c_active = 0, t3c_extra = 0, t3c_nseg = 0;
+    int64_t t3c_hits = 0;                   // values-only rebuilds since creation
+    up3d::DBuf<uint8_t> t3c_flag;           // (E) recorded active flags
+    up3d::DBuf<int32_t> t3c_up;             // (E) recorded upstream
+    up3d::DBuf<uint32_t> t3c_code, t3c_code_tmp;  // (16E) contributor codes, by destination
+    up3d::DBuf<int32_t> t3c_key, t3c_key_tmp;     // (16E) destinations (sorted: run keys)
+    up3d::DBuf<int32_t> t3c_seg, t3c_cnt;   // segment offsets / lengths
+    up3d::DBuf<int64_t> t3c_nruns;
     // adjoint (residual vector-Jacobian products), grown on demand
     up3d::DBuf<double> adj_t, adj_a, adj_rt, adj_A;   // (E) each
     up3d::DBuf<double> adj_dx;                        // (E, 12) per-element node gradients

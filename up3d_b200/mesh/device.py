@@ -140,6 +140,12 @@ class DeviceMesh:
         t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, assembly, tile_elems, 0.0, 0.0)
         L.call("up3d_mesh_set_tuning", self.handle, ctypes.byref(t))
 
+    def term3_cache_hits(self) -> int:
+        """Term-3 builds served by the values-only path so far."""
+        h = ctypes.c_int64()
+        L.call("up3d_mesh_term3_cache_hits", self.handle, ctypes.byref(h))
+        return int(h.value)
+
     def tile_info(self, tile_elems: int | None = None) -> dict:
         """Sizes of the tiled assembly's plan (built here when missing)."""
         if tile_elems is None:
