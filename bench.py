@@ -771,6 +771,10 @@ def batched_timing(spec, seed=0):
         seq_ok.append(bool(r["converged"]))
     out["newton"] = {"batched_s": round(res_b["time_s"], 4), "sequential_s": round(float(sum(seq_s)), 4),
                      "batched_without_graphs_s": round(res_ng["time_s"], 4),
+                     "batched_phases_s": {k: round(v, 4) for k, v in res_b["timings"].items()},
+                     "batched_without_graphs_phases_s": {k: round(v, 4) for k, v in res_ng["timings"].items()},
+                     "batched_n_newton": [int(v) for v in res_b["n_newton"]],
+                     "batched_n_gmres": int(res_b["n_gmres_total"]),
                      "speedup": round(float(sum(seq_s)) / res_b["time_s"], 3),
                      "batched_converged": [bool(v) for v in res_b["converged"]],
                      "sequential_converged": seq_ok,

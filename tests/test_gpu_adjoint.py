@@ -1,8 +1,10 @@
 """Discrete adjoint: the hand-written residual vector-Jacobian product
 against central finite differences of the device residual, and the shape /
-Mach gradient of the lift-like wall integral against finite differences of
-re-converged solves and against a transpose solve with the reference's
-Jacobian (the oracle's)."""
+Mach gradient of the wall pressure force (the reference's surface-gradient
+Cp) against finite differences of re-converged solves and against a
+transpose solve with the reference's Jacobian (the oracle's) -- subsonic on
+a small mesh, and at the adjoint configuration itself (450 k tets, M0.80,
+frozen finish, Term 3 active)."""
 
 import numpy as np
 import pytest
@@ -159,3 +161,86 @@ def test_drag_gradient_matches_finite_differences():
         fd = (8.0 * (fk(h, k) - fk(-h, k)) - (fk(2 * h, k) - fk(-2 * h, k))) / (12.0 * h)
         ad = float(g["dF_dp"][k])
         assert abs(fd - ad) <= 1e-6 * max(abs(ad), abs(fd)), (k, fd, ad)
+
+
+def test_wall_objective_is_the_reference_wall_force():
+    """The adjoint's objective is post/surface.py's pressure-force
+    coefficient (surface-gradient Cp): equal to the device
+    wall_force_coefficients, which is pinned to the reference."""
+    import torch
+    from up3d_b200.adjoint import BumpShape, wall_faces_with_owners, wall_force_objective
+    from up3d_b200.mesh.kuhn import pocket_state
+    from up3d_b200.post.surface import wall_force_coefficients
+    shape = BumpShape(16, 6, 5, amplitude=0.05, seed=0)
+    mesh = shape.mesh()
+    phi = pocket_state(mesh, "mixed")
+    faces = wall_faces_with_owners(mesh)
+    ref = wall_force_coefficients(mesh.nodes, mesh.elements, faces[:, 1:4], phi, m_inf=0.8)
+    X = torch.from_numpy(mesh.nodes).cuda()
+    for axis in (0, 2):
+        F = float(wall_force_objective(X, torch.from_numpy(phi).cuda(), torch.from_numpy(faces).cuda(),
+                                       torch.tensor(0.8, dtype=torch.float64, device="cuda"), axis=axis))
+        assert abs(F - ref["cf"][axis]) <= 1e-12 * abs(ref["cf"]).max(), (axis, F, ref["cf"])
+
+
+@pytest.fixture(scope="module")
+def transonic_gradient():
+    """The adjoint configuration: 100 x 30 x 25 hexes (450 k tets), bump
+    0.05, M_inf 0.80 from M 0.70, the frozen finish, 16 shape modes."""
+    from up3d_b200.adjoint import BumpShape, adjoint_gradient
+    shape = BumpShape(100, 30, 25, amplitude=0.05, seed=0)
+    kw = {"tol_residual": 1e-13, "n_newton_max": 40}
+    g = adjoint_gradient(shape, 0.80, m_start=0.70, solve_kw=kw)
+    return shape, g
+
+
+def test_transonic_adjoint_matches_finite_differences(transonic_gradient):
+    """Central differences (step 1e-6) of the objective re-converged with the
+    state's frozen selection held fixed -- the discrete function the frozen
+    finish's Jacobian linearises -- for four shape modes and M_inf."""
+    from up3d_b200.adjoint import frozen_objective
+    shape, g = transonic_gradient
+    res = g["newton"]
+    assert res["converged"] and res["frozen_state"] is not None
+    assert g["n_term3_active"] > 0 and g["n_supersonic"] > 0
+    frozen, phi0 = res["frozen_state"], g["phi"]
+    h = 1e-6
+    for k in (0, 5, 10, 15):
+        e = np.zeros(shape.n_params)
+        e[k] = h
+        fp = frozen_objective(shape, 0.80, phi0, frozen, p=e)
+        fm = frozen_objective(shape, 0.80, phi0, frozen, p=-e)
+        fd = (fp - fm) / (2 * h)
+        ad = float(g["dF_dp"][k])
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3 * np.abs(g["dF_dp"]).max()), (k, fd, ad)
+    fp = frozen_objective(shape, 0.80 + h, phi0, frozen)
+    fm = frozen_objective(shape, 0.80 - h, phi0, frozen)
+    fd = (fp - fm) / (2 * h)
+    assert abs(fd - g["dF_dM"]) <= 1e-6 * abs(g["dF_dM"]), (fd, g["dF_dM"])
+
+
+def test_transonic_adjoint_solves_the_reference_jacobian_transpose(transonic_gradient):
+    """lam satisfies J_ff^T lam = dF/dphi_f with the oracle's (the
+    reference's) Newton Jacobian at the converged frozen state, to 1e-10."""
+    import scipy.sparse as sp
+    from oracle import oracle as O
+    shape, g = transonic_gradient
+    mesh = shape.mesh()
+    res = g["newton"]
+    up, br = (a.cpu().numpy() for a in res["frozen_state"])
+    phi = g["phi"].cpu().numpy()
+    op = O.PicardOperator(mesh.nodes, mesh.elements)
+    upw = O.UpwindOperator(mesh.nodes, mesh.elements)
+    grad, q2 = op.velocities(phi)
+    q2l = O.limit_q2_field(q2, 0.80, O.M_CAP)
+    rho = O.density_field(q2l, 0.80)
+    rt = upw.rho_tilde_frozen(q2l, rho, up, br, 0.80, O.UPWIND_C, O.M_CRIT).copy()
+    s_e, s_u = (a.copy() for a in upw.rho_tilde_frozen_sensitivities(q2l, rho, up, br, 0.80, O.UPWIND_C,
+                                                                       O.M_CRIT))
+    lim = q2l == q2
+    J = op.assemble_newton_jacobian(phi, rt, s_e, s_u, up, lim_mask=None if lim.all() else lim)
+    free = np.setdiff1d(np.arange(mesh.n_nodes), mesh.dirichlet_nodes)
+    Jff = sp.csr_matrix(J)[free][:, free]
+    lam = g["lambda"].cpu().numpy()[free]
+    rhs = g["dF_dphi"].cpu().numpy()[free]
+    assert np.abs(Jff.T @ lam - rhs).max() <= 1e-10 * np.abs(rhs).max()

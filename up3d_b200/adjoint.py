@@ -8,18 +8,25 @@ equations (the residual of kernels/jacobian.py and kernels/upwind.py):
   by the base Gaussian plus ``n_side x n_side`` Gaussian shape modes whose
   amplitudes are the design parameters (centres on a grid over the bump,
   jittered from a seed);
-* ``lift_objective`` -- F = -sum over lower-wall faces of Cp_e (S_f . e),
-  e = z (lift-like) or x (drag-like),
-  Cp_e the pressure coefficient of the face's element (physics/isentropic.py
-  pressure_coefficient at the element's limited speed) and S_f the outward
-  area vector, with its explicit partial derivatives (torch autograd);
+* ``wall_force_objective`` -- F = cf . e, e = z (lift-like) or x
+  (drag-like), with cf the reference's pressure-force coefficient of the
+  lower wall (post/surface.py:309-363 with alpha 0, S_ref 1, no smoothing):
+  per wall triangle the in-plane P1 gradient of phi (:80-118), the exact
+  isentropic Cp of its speed (physics/isentropic.py:122-143), the
+  body-outward normal taken from the owning tet (:192-230), cf = -sum Cp A
+  n_out -- written in torch so that autograd gives its explicit partials
+  with respect to phi, the node coordinates and M_inf;
+* ``lift_objective`` -- the earlier element-Cp integral (Cp of the face's
+  element at its limited speed), kept for comparison;
 * ``ResidualFunction`` -- R(phi, X, M_inf) as a torch.autograd.Function
   whose backward is the hand-written device product up3d_residual_vjp
   (node coordinates, Mach) plus J^T g (phi);
 * ``adjoint_gradient`` -- dF/dp and dF/dM_inf at a converged state:
   J^T lam = dF/dphi solved by GMRES + AMG on the free DOFs, then
-  dF/dX = dF/dX|explicit + sum w dq2/dX - lam^T dR/dX, chained through
-  dX/dp.
+  dF/dX = dF/dX|explicit - lam^T dR/dX, chained through dX/dp;
+* ``frozen_objective`` -- F after re-converging the discrete equations with
+  a given (upstream, branch) selection held fixed: the function whose
+  derivative the adjoint at a frozen finish is (for finite differences).
 """
 
 from __future__ import annotations
@@ -131,6 +138,53 @@ def lift_objective(X, q2n_elem, faces_dev, mach, interior_nodes_dev, gamma=GAMMA
     Sa = sign.detach() * S[:, axis]
     cp = _cp_torch(q2n_elem[e], mach, gamma)
     return -(cp * Sa).sum()
+
+
+def wall_force_objective(X, phi, faces_dev, mach, axis: int = 2, u_inf: float = 1.0, gamma=GAMMA):
+    """F = cf[axis] of post/surface.py's wall_force_coefficients (alpha 0,
+    S_ref 1, no smoothing) on the wall triangles faces_dev[:, 1:4], whose
+    owning tets' nodes are faces_dev[:, 4:8] (rows of
+    wall_faces_with_owners); X (N, 3) the node coordinates.  Torch tensors;
+    X, phi and mach may require grad.  See the module docstring."""
+    t = L.torch()
+    tri = faces_dev[:, 1:4]
+    p0, p1, p2 = X[tri[:, 0]], X[tri[:, 1]], X[tri[:, 2]]
+    edge1 = p1 - p0
+    edge2 = p2 - p0
+    area_vec = t.linalg.cross(edge1, edge2)
+    twice_area = t.linalg.norm(area_vec, dim=1)
+    n = area_vec / twice_area[:, None]
+    e1 = edge1 / t.linalg.norm(edge1, dim=1)[:, None]
+    e2 = t.linalg.cross(n, e1)
+    u1, v1 = (edge1 * e1).sum(dim=1), (edge1 * e2).sum(dim=1)
+    u2, v2 = (edge2 * e1).sum(dim=1), (edge2 * e2).sum(dim=1)
+    df1 = phi[tri[:, 1]] - phi[tri[:, 0]]
+    df2 = phi[tri[:, 2]] - phi[tri[:, 0]]
+    det = u1 * v2 - v1 * u2
+    du = (v2 * df1 - v1 * df2) / det
+    dv = (-u2 * df1 + u1 * df2) / det
+    grad = du[:, None] * e1 + dv[:, None] * e2
+    q2 = (grad * grad).sum(dim=1) / u_inf ** 2
+    hgm = 0.5 * (gamma - 1.0)
+    m2 = mach * mach
+    base = t.clamp(1.0 + hgm * m2 * (1.0 - q2), min=1e-10)
+    rho = base ** (1.0 / (gamma - 1.0))
+    cp = 2.0 / (gamma * m2) * (rho ** gamma - 1.0)
+    # body-outward (toward the owning tet, i.e. into the fluid): the sign is
+    # a discrete choice, not differentiated
+    owner_c = X[faces_dev[:, 4:8]].mean(dim=1)
+    face_c = (p0 + p1 + p2) / 3.0
+    flip = ((n * (owner_c - face_c)).sum(dim=1) < 0).detach()
+    n_out = t.where(flip[:, None], -n, n)
+    area = 0.5 * twice_area
+    return -(cp * area * n_out[:, axis]).sum()
+
+
+def wall_faces_with_owners(mesh) -> np.ndarray:
+    """(F, 8) int64 rows: owning element, the face's three nodes, the
+    owner's four nodes (lower wall of the channel)."""
+    faces = lower_wall_faces(mesh.elements, mesh.shape)
+    return np.column_stack([faces, mesh.elements[faces[:, 0]].astype(np.int64)])
 
 
 def transpose_csr(A):
@@ -254,29 +308,23 @@ def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[fl
     phi = res["phi"]
     flow = FlowParams(m_inf=mach, u_inf=ws.u_inf)
     actx = AdjointContext(ws, phi, flow, frozen=res.get("frozen_state"))
+    mon = ws.ev.read_monitors()  # of the Jacobian evaluation at the state
     # objective and its explicit partials
     X = t.from_numpy(mesh.nodes).cuda().requires_grad_(True)
-    _, q2 = ws.op.velocities(phi)
-    q2n = (q2.clone() / ws.u_inf ** 2).requires_grad_(True)
-    faces = lower_wall_faces(mesh.elements, mesh.shape)
-    opp = np.empty(len(faces), dtype=np.int64)
-    for r, (e, a, b, c) in enumerate(faces):
-        opp[r] = [v for v in mesh.elements[e] if v not in (a, b, c)][0]
-    faces_d = t.from_numpy(faces).cuda()
+    phi_g = phi.detach().clone().requires_grad_(True)
+    faces_d = t.from_numpy(wall_faces_with_owners(mesh)).cuda()
     M = t.tensor(float(mach), dtype=t.float64, device="cuda", requires_grad=True)
-    F = lift_objective(X, q2n, faces_d, M, t.from_numpy(opp).cuda(), axis=axis)
-    gX_exp, gq2, gM_exp = t.autograd.grad(F, (X, q2n, M))
-    w = gq2.contiguous()
-    # dF/dphi, then J^T lam = dF/dphi on the free DOFs
-    dphi, _, _ = actx.vjp(w_q2=w, want_dphi=True)
-    rhs = dphi.masked_fill(ws.mask.bool(), 0.0)
+    F = wall_force_objective(X, phi_g, faces_d, M, axis=axis, u_inf=ws.u_inf)
+    gX_exp, gphi, gM_exp = t.autograd.grad(F, (X, phi_g, M))
+    # J^T lam = dF/dphi on the free DOFs
+    rhs = gphi.detach().masked_fill(ws.mask.bool(), 0.0).contiguous()
     JTf = with_dirichlet(actx.JT, ws.mask)
     ws.amg = M_pre = amg_for(ws.picard_matrix(), getattr(ws, "amg", None))
     lam, n_it, info = solve_gmres(JTf, rhs, M=M_pre, rtol=tol_lambda, restart=100, maxiter=50,
                                   on_fail="return")
     lam = lam.masked_fill(ws.mask.bool(), 0.0)
-    # total derivatives: explicit + w path - lam^T dR
-    _, dX, dMr = actx.vjp(lam=(-lam).contiguous(), w_q2=w)
+    # total derivatives: explicit - lam^T dR
+    _, dX, dMr = actx.vjp(lam=(-lam).contiguous())
     dX_total = gX_exp.detach() + dX
     dz = t.from_numpy(shape.dz_dp()).cuda()
     dFdp = (dX_total[:, 2:3] * dz).sum(dim=0)  # the modes move z only
@@ -285,6 +333,7 @@ def adjoint_gradient(shape: BumpShape, mach: float, p=None, m_start: Optional[fl
     timings["adjoint_s"] = time.perf_counter() - c1
     return {"F": float(F.detach()), "dF_dp": dFdp.cpu().numpy(), "dF_dM": dFdM,
             "lambda": lam, "dF_dphi": rhs, "gmres_iterations": n_it, "gmres_info": info,
+            "n_term3_active": int(mon["n_term3_active"]), "n_supersonic": int(mon["n_supersonic"]),
             "phi": phi, "newton": res, "timings": timings, "context": actx}
 
 
@@ -299,11 +348,38 @@ def objective_value(shape: BumpShape, mach: float, p=None, m_start: Optional[flo
                                  **(solve_kw or {}))
     if not res["converged"]:
         raise RuntimeError("solve did not converge")
-    _, q2 = ws.op.velocities(res["phi"])
-    faces = lower_wall_faces(mesh.elements, mesh.shape)
-    opp = np.array([[v for v in mesh.elements[e] if v not in (a, b, c)][0]
-                    for e, a, b, c in faces], dtype=np.int64)
     X = t.from_numpy(mesh.nodes).cuda()
     M = t.tensor(float(mach), dtype=t.float64, device="cuda")
-    return float(lift_objective(X, q2 / ws.u_inf ** 2, t.from_numpy(faces).cuda(), M,
-                                t.from_numpy(opp).cuda(), axis=axis))
+    return float(wall_force_objective(X, res["phi"], t.from_numpy(wall_faces_with_owners(mesh)).cuda(), M,
+                                      axis=axis, u_inf=ws.u_inf))
+
+
+def frozen_objective(shape: BumpShape, mach: float, phi0, frozen, p=None, axis: int = 2,
+                     tol_residual: float = 1e-13, n_newton_max: int = 20) -> float:
+    """F after Newton on the discrete equations with the (upstream, branch)
+    selection `frozen` held fixed, from phi0 (a nearby converged state):
+    the function whose derivative a frozen-finish adjoint gives.  Exact
+    Jacobian (the frozen one), GMRES + AMG to 1e-12, full steps."""
+    t = L.require_cuda()
+    from .solve.fused import FlowParams
+    from .solve.linear import amg_for, solve_gmres, with_dirichlet
+    from .solve.newton import ChannelWorkspace
+    mesh = shape.mesh(p)
+    ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+    flow = FlowParams(m_inf=float(mach), u_inf=ws.u_inf)
+    phi = t.where(ws.free, L.to_device(phi0, t.float64), ws.phi_dir).clone()
+    for _ in range(n_newton_max):
+        R, _ = ws.residual(phi, flow, frozen=frozen, jacobian=True)
+        Rf = ws.r_free(R).clone()
+        if float(Rf.abs().max()) < tol_residual:
+            break
+        J = with_dirichlet(ws.ev.jacobian(), ws.mask)
+        ws.amg = M = amg_for(ws.picard_matrix(), getattr(ws, "amg", None))
+        dphi, _, _ = solve_gmres(J, -Rf, M=M, rtol=1e-12, restart=100, maxiter=50, on_fail="return")
+        phi = phi + dphi.masked_fill(ws.mask.bool(), 0.0)
+    else:
+        raise RuntimeError("frozen solve did not converge")
+    X = t.from_numpy(mesh.nodes).cuda()
+    M = t.tensor(float(mach), dtype=t.float64, device="cuda")
+    return float(wall_force_objective(X, phi, t.from_numpy(wall_faces_with_owners(mesh)).cuda(), M, axis=axis,
+                                      u_inf=ws.u_inf))

@@ -228,6 +228,8 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
         t.cuda.synchronize()
         return time.perf_counter()
 
+    timings = {"seed": 0.0, "residual": 0.0, "assembly": 0.0, "precond": 0.0, "linsolve": 0.0,
+               "line_search": 0.0}
     t0 = clock()
     levels = sorted(set(mach_schedule(float(machs.max()), min(m_start, float(machs.max())), dm)))
     converged_at = np.full(C, -1.0)
@@ -255,6 +257,7 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                            x0=t.where(ws.free, phi, t.zeros_like(phi)))
         phi = t.where(ws.free, x, ws.phi_dir)
     t_seed = clock() - t0
+    timings["seed"] = t_seed
 
     for lvl, m_lev in enumerate(levels):
         m_level = np.minimum(machs, m_lev)
@@ -268,6 +271,7 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
         history = []
         eta_prev = None
         for it in range(n_newton_max):
+            ta = clock()
             R = batch.evaluate(phi, m_level, jacobian=False)
             Rf = R.masked_fill(mask_b, 0.0)
             r_case = batch.per_case(Rf, "amax").cpu().numpy()
@@ -316,10 +320,16 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                 R = batch.evaluate(phi, m_level, jacobian=False)
                 Rf = R.masked_fill(mask_b, 0.0)
                 merit = batch.per_case(Rf, "sumsq")
+            tb = clock()
+            timings["residual"] += tb - ta
             batch.evaluate(phi, m_level, jacobian=True)
             J = with_dirichlet(ws.ev.jacobian(), ws.mask)
+            tc = clock()
+            timings["assembly"] += tc - tb
             if M_pre is None or it % amg_rebuild_every == 0:
                 ws.amg = M_pre = amg_for(ws.picard_matrix(), getattr(ws, "amg", None))
+            td = clock()
+            timings["precond"] += td - tc
             r_act = r_case[active]
             r_prev = history[-2][active] if len(history) > 1 else None
             etas = [_ew_forcing(float(a), None if r_prev is None else float(b), eta_prev)
@@ -335,6 +345,8 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
             y, n_it, _ = solve_gmres(J, rhs, M=M_pre, rtol=eta / np.sqrt(active.sum()),
                                      restart=gmres_restart, maxiter=gmres_maxiter, on_fail="return")
             dphi = y * scale[case_node]
+            te = clock()
+            timings["linsolve"] += te - td
             n_gmres_total += n_it
             n_newton[active] += 1
             dphi = dphi.masked_fill(mask_b | ~act_node, 0.0)
@@ -362,6 +374,7 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                 lam = np.where(accepted, lam, 0.5 * lam)
             lam = np.where(accepted, lam, best_lam)
             phi = phi + t.from_numpy(lam).cuda()[case_node] * dphi
+            timings["line_search"] += clock() - te
             if verbose:
                 print(f"  level M<={m_lev:.3f} it {it}: max|R| active = {r_act.max():.3e}")
         # a case still active at the end of a level failed it
@@ -369,4 +382,5 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
     t_total = clock() - t0
     return {"phi": phi, "converged": converged_at >= 0, "failed": failed, "n_newton": n_newton,
             "n_gmres_total": n_gmres_total, "levels": levels, "time_s": t_total, "seed_s": t_seed,
+            "timings": timings,
             "converged_s": converged_s, "froze": frozen}
