@@ -28,12 +28,24 @@ def sources():
     return sorted(CSRC.glob("*.cu"))
 
 
+STAMP = LIB_DIR / "libup3d.sources"
+
+
+def _source_digest() -> str:
+    """Digest of every source the library is built from (and the flags)."""
+    import hashlib
+    h = hashlib.sha256(" ".join(ARCH + FLAGS + LINK).encode())
+    deps = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "up3d.h"]
+    for p in deps:
+        h.update(p.name.encode())
+        h.update(p.read_bytes())
+    return h.hexdigest()
+
+
 def _stale() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not STAMP.exists():
         return True
-    t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "up3d.h"]
-    return any(p.stat().st_mtime > t for p in deps)
+    return STAMP.read_text().strip() != _source_digest()
 
 
 def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> Path:
@@ -61,10 +73,12 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
             print(text)
     if failed:
         raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
+    digest = _source_digest()
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), *LINK]
     subprocess.run(cmd, check=True)
     tmp.replace(LIB)
+    STAMP.write_text(digest + "\n")
     return LIB
 
 
