@@ -48,3 +48,14 @@ def test_unknown_ordering_raises():
     from up3d_b200.mesh.order import renumber
     with pytest.raises(ValueError):
         renumber(np.zeros((4, 3)), np.array([[0, 1, 2, 3]]), "rcm")
+
+
+def test_choking_mach_of_the_bump_channel():
+    """Quasi-1-D choking estimate: the configurations' bumps choke the
+    channel at M 0.7685 (bump 0.05) and M 0.7105 (bump 0.08); a vanishing
+    bump chokes only at M 1."""
+    from up3d_b200.mesh.kuhn import choking_mach
+    assert abs(choking_mach(0.05) - 0.76850) < 1e-4
+    assert abs(choking_mach(0.08) - 0.71049) < 1e-4
+    assert choking_mach(0.0) == 1.0
+    assert choking_mach(1e-4) > 0.98

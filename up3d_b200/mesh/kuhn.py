@@ -160,3 +160,34 @@ def pocket_state(mesh: BumpMesh, family: str, noise_seed: int = 42,
         raise ValueError(f"unknown pocket family {family!r}")
     rng = np.random.default_rng(noise_seed)
     return lx * f + noise * rng.standard_normal(len(s))
+
+
+def choking_mach(amplitude: float, height: float = 1.0, gamma: float = 1.4) -> float:
+    """Freestream Mach at which the bump channel chokes, by the quasi-1-D
+    isentropic estimate: the bump spans the channel's width, so its crest
+    leaves a throat of (height - amplitude) / height of the inflow area, and
+    the mass flux rho q that the Dirichlet inflow and outflow impose cannot
+    pass the throat once it exceeds the sonic flux rho* q* (local Mach 1,
+    q*^2 = (2 + (gamma - 1) M^2) / ((gamma + 1) M^2) in freestream units).
+    Above this Mach the channel has no steady isentropic full-potential
+    solution (the supersonic pocket reaches across the throat), so a Newton
+    continuation cannot converge there.  Bisection to 1e-12."""
+    throat = (height - amplitude) / height
+    if not 0.0 < throat <= 1.0:
+        raise ValueError("amplitude must lie in [0, height)")
+
+    def sonic_flux(m):
+        q2 = (2.0 + (gamma - 1.0) * m * m) / ((gamma + 1.0) * m * m)
+        rho = (1.0 + 0.5 * (gamma - 1.0) * m * m * (1.0 - q2)) ** (1.0 / (gamma - 1.0))
+        return rho * np.sqrt(q2)
+
+    if throat == 1.0:
+        return 1.0
+    lo, hi = 1e-3, 1.0
+    while hi - lo > 1e-12:
+        mid = 0.5 * (lo + hi)
+        if sonic_flux(mid) > 1.0 / throat:
+            lo = mid
+        else:
+            hi = mid
+    return lo
