@@ -72,6 +72,9 @@ def parse():
     p.add_argument("--naca", default="1", help="NACA0012 2.5D timings ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
+    p.add_argument("--c4", default="",
+                   help="mesh:bump:Mach of a one-run FP64 / mixed Newton comparison on the large mesh "
+                        "(the mixed-precision configuration is 320x96x80:0.05, below its choking Mach)")
     p.add_argument("--parity", type=int, default=1,
                    help="1: compare the timed states with the oracle after timing; 2: also the pocket states; "
                         "0: skip")
@@ -266,7 +269,7 @@ def read_traffic(kernel: str):
     return None
 
 
-def newton_timing(spec):
+def newton_timing(spec, reps=2):
     """Time-to-1e-10 of the device Newton solve (Picard seed, exact
     Jacobian, GMRES + AMG, line search, frozen finish) from the freestream
     potential, plain FP64 and mixed precision (FP32 Jacobian SpMV and FP32
@@ -279,13 +282,16 @@ def newton_timing(spec):
     shape = tuple(int(v) for v in shape_s.split("x"))
     amp, mach = float(amp_s), float(mach_s)
     mesh = bump_channel(*shape, amplitude=amp, seed=0)
+    from up3d_b200.mesh.kuhn import choking_mach
     out = {"case": f"bump channel {shape_s} Kuhn-split ({mesh.n_tets} tets), bump {amp}, "
                    f"M_inf {mach}, from freestream to |R_free|inf < 1e-10",
-           "n_tets": mesh.n_tets}
+           "n_tets": mesh.n_tets,
+           "choking_mach_quasi_1d": round(choking_mach(amp), 4),
+           "timed_runs": "second of two" if reps > 1 else "first (workspace and tile plan built before the clock)"}
     phis = {}
     for prec in ("fp64", "mixed"):
         res = None
-        for rep_ in range(2):
+        for rep_ in range(reps):
             ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -1075,6 +1081,7 @@ def run_ours(args):
                   "nu_max": [float(m["nu_max"]) for m in p_mon]}
 
     newton = newton_timing(args.newton) if args.newton else None
+    c4 = newton_timing(args.c4, reps=1) if args.c4 else None
     adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
     batched = batched_timing(args.batched) if args.batched else None
     weighted = weighted_timing(args.weighted) if args.weighted else None
@@ -1159,6 +1166,7 @@ def run_ours(args):
             "monitors": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in mon.items()},
             "pocket_states": pocket,
             "newton": newton,
+            "newton_large": c4,
             "adjoint": adjoint,
             "batched": batched,
             "weighted_upwind": weighted,

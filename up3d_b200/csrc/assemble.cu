@@ -1093,7 +1093,8 @@ __global__ void k_t3_values(int64_t n_seg, const int32_t* __restrict__ seg, cons
         for (int32_t j = seg[d]; j < j1; ++j) {
             const uint32_t c = code[j];
             const double* t = t3v + 8 * (int64_t)(c >> 4);
-            v += t[(c >> 2) & 3] * t[4 + (c & 3)];
+            // the row kernel rounds each product, then adds: no contraction
+            v = __dadd_rn(v, __dmul_rn(t[(c >> 2) & 3], t[4 + (c & 3)]));
         }
         const int32_t k = key[d];
         if (k < Z) data[k] += v;
