@@ -711,8 +711,12 @@ def batched_timing(spec, seed=0):
     rng = np.random.default_rng(seed)
     f = np.exp(rng.uniform(0.0, np.log(hi[0] / lo[0]), size=K))
     shapes = [tuple(int(round(v)) for v in lo * fi) for fi in f]
-    machs = rng.uniform(float(mlo_s), float(mhi_s), size=K)
+    machs_drawn = rng.uniform(float(mlo_s), float(mhi_s), size=K)
     amps = rng.uniform(0.02, 0.08, size=K)
+    # a case above its bump's choking Mach has no steady solution: cap it
+    # 0.02 below (mesh.kuhn.choking_mach)
+    from up3d_b200.mesh.kuhn import choking_mach
+    machs = np.minimum(machs_drawn, np.array([choking_mach(float(a)) - 0.02 for a in amps]))
     meshes = [bump_channel(*sh, amplitude=float(a), seed=c) for c, (sh, a) in enumerate(zip(shapes, amps))]
     # the ordering and launch shapes picked by the tuner (timed candidates)
     t_tune = time.perf_counter()
@@ -747,6 +751,8 @@ def batched_timing(spec, seed=0):
     ms_s = t_events(seq, 10)
     out = {"cases": K, "shapes": ["x".join(map(str, sh)) for sh in shapes],
            "machs": [round(float(m), 4) for m in machs], "amplitudes": [round(float(a), 4) for a in amps],
+           "machs_drawn": [round(float(m), 4) for m in machs_drawn],
+           "mach_cap": "each case at most 0.02 below its bump's choking Mach (quasi-1-D sonic-throat estimate)",
            "total_tets": int(E),
            "tuning": {"ordering": batch.ordering, "tuner_s": round(t_tune, 3),
                       "candidates_ms": {k: round(v["ms"], 4) for k, v in batch.tuning_report["candidates"].items()},
