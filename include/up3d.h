@@ -460,6 +460,12 @@ int up3d_residual_jacobian_batched(up3d_mesh* mesh, const double* phi, int n_cas
  *   tile_elems       elements per tile of the tiled form: 128 or 256 (the
  *                    plan is rebuilt when it changes; the summation order
  *                    depends on it)
+ *   tile_stretch     1, 2 or 4: the tiles' bisection counts extents along
+ *                    x divided by this factor, so tiles come out that many
+ *                    times longer along x -- the freestream direction of
+ *                    the channel cases, along which the upwind walk runs
+ *                    (fewer walks leave their tile); the summation order
+ *                    depends on it
  *   elem_us, row_us  autotune output: median time per launch of the
  *                    chosen shapes (0 when set by hand) */
 typedef struct {
@@ -469,12 +475,14 @@ typedef struct {
     int32_t row_plan8;
     int32_t assembly;
     int32_t tile_elems;
+    int32_t tile_stretch;
+    int32_t reserved;
     double elem_us;
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 512, 8, 0, 1, 256}.  UP3D_ERR_VALUE for a shape outside the
- * lists. */
+/* Default: {0, 512, 8, 0, 1, 256, 1}.  UP3D_ERR_VALUE for a shape outside
+ * the lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 
@@ -485,7 +493,9 @@ int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
  * another tile size; synchronises the stream. */
 typedef struct {
     int32_t tile_elems;
+    int32_t tile_stretch;       /* tiles this many times longer along x than across */
     int32_t max_nodes;          /* most distinct nodes of one tile */
+    int32_t max_edges;          /* most distinct element edges of one tile */
     int64_t n_tiles;
     int64_t n_tile_nodes;       /* sum over tiles of their distinct nodes */
     int64_t n_tile_edges;       /* sum over tiles of their distinct element edges */
@@ -507,7 +517,7 @@ int up3d_mesh_tile_info(up3d_mesh* mesh, int32_t tile_elems, up3d_tile_info* inf
 typedef struct up3d_tile_plan up3d_tile_plan; /* opaque host-side plan */
 int up3d_tile_plan_host_create(const int32_t* elements, const int32_t* face_neighbors, const double* centroids,
                                int64_t n_nodes, int64_t n_tets, const int32_t* indptr, const int32_t* indices,
-                               int32_t tile_elems, up3d_tile_plan** out);
+                               int32_t tile_elems, int32_t tile_stretch, up3d_tile_plan** out);
 int up3d_tile_plan_host_info(const up3d_tile_plan* plan, up3d_tile_info* info);
 int up3d_tile_plan_host_array(const up3d_tile_plan* plan, const char* name, void* dst, int64_t* nbytes);
 int up3d_tile_plan_host_destroy(up3d_tile_plan* plan);

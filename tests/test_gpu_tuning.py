@@ -66,8 +66,8 @@ def test_every_shape_gives_the_same_bits():
         assert torch.equal(ev.evaluate(phi, flow, jacobian=False), Rr0)
     # the tiled form at each tile size: its own fixed order, the same
     # discrete decisions, the same values to rounding
-    for T in (128, 256):
-        dm.set_tuning(assembly=1, tile_elems=T)
+    for T, stretch in ((128, 1), (256, 1), (256, 4)):
+        dm.set_tuning(assembly=1, tile_elems=T, tile_stretch=stretch)
         R, J, up, rt, mon = _outputs(ev, phi, flow)
         assert torch.equal(up, up0) and torch.equal(rt, rt0) and mon == mon0, T
         assert rel_err(R.cpu().numpy(), R0.cpu().numpy()) < 1e-13, T
@@ -78,7 +78,8 @@ def test_every_shape_gives_the_same_bits():
         Rf = ev.evaluate(phi, flow, jacobian=True, frozen=frozen)
         assert rel_err(Rf.cpu().numpy(), Rf0.cpu().numpy()) < 1e-13
         info = dm.tile_info(T)
-        assert info["tile_elems"] == T and info["n_tiles"] == -(-dm.n_tets // T)
+        assert info["tile_elems"] == T and info["tile_stretch"] == stretch
+        assert info["n_tiles"] == -(-dm.n_tets // T)
         assert info["n_combined_nodes"] <= dm.n_nodes and info["n_combined_slots"] <= dm.nnz
 
 
@@ -94,10 +95,10 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
     assert t == dm.tuning()
     assert (t["elem_persistent"], t["elem_threads_per_sm"]) in {(0, 512), (1, 512), (1, 640), (0, 768), (1, 768)}
     assert t["row_lanes"] in (4, 8, 16, 32) and t["row_plan8"] in (0, 1)
-    assert t["assembly"] in (0, 1) and t["tile_elems"] in (128, 256)
+    assert t["assembly"] in (0, 1) and t["tile_elems"] in (128, 256) and t["tile_stretch"] in (1, 2, 4)
     assert t["elem_us"] > 0 and (t["row_us"] > 0 or t["assembly"] == 1)
     R = ev.evaluate(phi, flow, jacobian=True).clone()
-    if t["assembly"] == 1 and t["tile_elems"] == 256:
+    if t["assembly"] == 1 and t["tile_elems"] == 256 and t["tile_stretch"] == 1:
         assert torch.equal(R, R0)
         assert (ev.jacobian().to_scipy() != J0).nnz == 0
     else:
@@ -110,7 +111,8 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
 def test_bad_shapes_are_refused():
     _, _, dm, _, _ = _setup()
     for bad in [(2, 512, 8), (-1, 512, 8), (0, 256, 8), (0, 1024, 8), (0, 512, 2), (0, 512, 12), (0, 512, 64),
-                (0, 512, 8, 2), (0, 512, 8, -1), (0, 512, 8, 0, 2), (0, 512, 8, 0, 1, 64), (0, 512, 8, 0, 1, 512)]:
+                (0, 512, 8, 2), (0, 512, 8, -1), (0, 512, 8, 0, 2), (0, 512, 8, 0, 1, 64), (0, 512, 8, 0, 1, 512),
+                (0, 512, 8, 0, 1, 256, 3)]:
         with pytest.raises(ValueError):
             dm.set_tuning(*bad)
     assert dm.tuning()["row_lanes"] == 8

@@ -30,7 +30,7 @@ def _pattern(elements, n):
     return P.indptr.astype(np.int32), P.indices.astype(np.int32)
 
 
-def _plan(nodes, elements, T):
+def _plan(nodes, elements, T, stretch=1):
     from oracle import oracle as O
     from up3d_b200 import _lib as L
     el = np.ascontiguousarray(elements, dtype=np.int32)
@@ -39,7 +39,7 @@ def _plan(nodes, elements, T):
     indptr, indices = _pattern(el, len(nodes))
     h = ctypes.c_void_p()
     L.call("up3d_tile_plan_host_create", el.ctypes.data, fn.ctypes.data, cen.ctypes.data, len(nodes), len(el),
-           indptr.ctypes.data, indices.ctypes.data, T, ctypes.byref(h))
+           indptr.ctypes.data, indices.ctypes.data, T, stretch, ctypes.byref(h))
     try:
         info = L.TileInfo()
         L.call("up3d_tile_plan_host_info", h, ctypes.byref(info))
@@ -71,11 +71,12 @@ def _meshes():
             ("union", nodes, elements, [len(a.elements), len(b.elements)])]
 
 
-@pytest.mark.parametrize("T", [128, 256])
+@pytest.mark.parametrize("T,stretch", [(128, 1), (256, 1), (256, 4)])
 @pytest.mark.parametrize("case", [0, 1])
-def test_plan_reproduces_a_direct_scatter(case, T):
+def test_plan_reproduces_a_direct_scatter(case, T, stretch):
     name, nodes, elements, comp_sizes = _meshes()[case]
-    P = _plan(nodes, elements, T)
+    P = _plan(nodes, elements, T, stretch)
+    assert P["info"]["tile_stretch"] == stretch
     E, N = len(elements), len(nodes)
     indptr, indices = P["indptr"], P["indices"]
     Z = len(indices)

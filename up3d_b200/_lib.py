@@ -49,8 +49,8 @@ class MeshInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """up3d_tuning: launch shapes of the fused evaluation's two passes."""
     _fields_ = [("elem_persistent", _i32), ("elem_threads_per_sm", _i32), ("row_lanes", _i32),
-                ("row_plan8", _i32), ("assembly", _i32), ("tile_elems", _i32), ("elem_us", _d),
-                ("row_us", _d)]
+                ("row_plan8", _i32), ("assembly", _i32), ("tile_elems", _i32), ("tile_stretch", _i32),
+                ("reserved", _i32), ("elem_us", _d), ("row_us", _d)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -58,7 +58,8 @@ class Tuning(ctypes.Structure):
 
 class TileInfo(ctypes.Structure):
     """up3d_tile_info: size of the tiled assembly's plan."""
-    _fields_ = [("tile_elems", _i32), ("max_nodes", _i32), ("n_tiles", _i64), ("n_tile_nodes", _i64),
+    _fields_ = [("tile_elems", _i32), ("tile_stretch", _i32), ("max_nodes", _i32), ("max_edges", _i32),
+                ("n_tiles", _i64), ("n_tile_nodes", _i64),
                 ("n_tile_edges", _i64), ("n_partials", _i64), ("n_combined_nodes", _i64),
                 ("n_combined_slots", _i64), ("build_s", _d)]
 
@@ -145,7 +146,7 @@ SIGNATURES = {
     "up3d_autotune": (_int, [_p, _p, ctypes.POINTER(Flow), _int, ctypes.POINTER(Tuning), _p]),
     "up3d_mesh_tile_info": (_int, [_p, _i32, ctypes.POINTER(TileInfo), _p]),
     "up3d_mesh_term3_cache_hits": (_int, [_p, ctypes.POINTER(_i64)]),
-    "up3d_tile_plan_host_create": (_int, [_p, _p, _p, _i64, _i64, _p, _p, _i32, ctypes.POINTER(_p)]),
+    "up3d_tile_plan_host_create": (_int, [_p, _p, _p, _i64, _i64, _p, _p, _i32, _i32, ctypes.POINTER(_p)]),
     "up3d_tile_plan_host_info": (_int, [_p, ctypes.POINTER(TileInfo)]),
     "up3d_tile_plan_host_array": (_int, [_p, ctypes.c_char_p, _p, ctypes.POINTER(_i64)]),
     "up3d_tile_plan_host_destroy": (_int, [_p]),

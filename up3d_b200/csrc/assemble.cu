@@ -501,6 +501,7 @@ struct TileArgs {
     const int32_t* noff;
     const int32_t* uoff;
     const int32_t* tnode;
+    const double4* txyz;
     const ushort4* lconn;
     const int32_t* nent_off;
     const uint16_t* nent;
@@ -523,20 +524,67 @@ struct TileArgs {
     const int32_t* case_of;
     int n_cases;
     int max_nodes;
+    int max_edges;
     int64_t E;
     int64_t n_tiles;
     Flow F0;
     double u2;
 };
 
-// Shared memory of one tile of NT elements: the tile's nodes (x, y, z,
-// phi), then per element its centroid, gradient, unlimited q^2 and density,
-// 14 local values (LOC layout), face neighbours, local connectivity and
-// limiter flag -- all structure-of-arrays.
+// Shared memory of one tile of NT elements (byte offsets, each region
+// 16-byte aligned): the tile's node positions (x, y, z, 0; copied
+// asynchronously from the plan's tile-ordered table) and potentials; per
+// element its centroid, gradient, unlimited q^2 and density, 14 local
+// values (LOC layout), face neighbours, local connectivity, limiter flag
+// and user id -- structure of arrays; then the tile's slice of the plan
+// (node-entry offsets, node destinations, node-entry codes, edge offsets,
+// edge destinations, edge codes), copied asynchronously in whole 16-byte
+// blocks while the elements are evaluated.
 constexpr int TS_DOUBLES = 8 + LOC_STRIDE;  // cx cy cz gx gy gz q2 rho + loc
-__host__ __device__ constexpr size_t tile_smem_bytes(int max_nodes, int nt) {
-    return (size_t)max_nodes * sizeof(double4) +
-           (size_t)nt * (TS_DOUBLES * sizeof(double) + sizeof(int4) + sizeof(ushort4) + 1);
+struct TileSmem {
+    size_t xs, phi, sd, fn, lc, lim, perm, noff, ndst, nent, uoff, udst, uent, total;
+    __host__ __device__ static constexpr size_t up16(size_t b) { return (b + 15) & ~size_t(15); }
+    __host__ __device__ TileSmem(int max_nodes, int max_edges, int nt) {
+        size_t o = 0;
+        xs = o;   o += up16((size_t)max_nodes * sizeof(double4));
+        phi = o;  o += up16((size_t)max_nodes * sizeof(double));
+        sd = o;   o += up16((size_t)nt * TS_DOUBLES * sizeof(double));
+        fn = o;   o += up16((size_t)nt * sizeof(int4));
+        lc = o;   o += up16((size_t)nt * sizeof(ushort4));
+        lim = o;  o += up16((size_t)nt);
+        perm = o; o += up16((size_t)nt * sizeof(int32_t));
+        // staged plan ranges: at most 15 bytes before the range plus 15 after
+        noff = o; o += up16((size_t)(max_nodes + 1) * sizeof(int32_t)) + 32;
+        ndst = o; o += up16((size_t)max_nodes * sizeof(int2)) + 32;
+        nent = o; o += up16((size_t)4 * nt * sizeof(uint16_t)) + 32;
+        uoff = o; o += up16((size_t)(max_edges + 1) * sizeof(int32_t)) + 32;
+        udst = o; o += up16((size_t)max_edges * sizeof(int2)) + 32;
+        uent = o; o += up16((size_t)6 * nt * sizeof(uint16_t)) + 32;
+        total = o;
+    }
+};
+
+// Asynchronous global -> shared copies (cp.async, 16-byte blocks).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// Copies the bytes [src, src + bytes) into shared memory at dst in whole
+// 16-byte blocks starting at the block that holds src (the plan's arrays
+// are padded by 16 bytes, so the last block stays inside the allocation);
+// returns the offset of src's first byte within dst.
+__device__ __forceinline__ int stage16(unsigned char* dst, const void* src, size_t bytes, int tid, int nt) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const unsigned char* base = reinterpret_cast<const unsigned char*>(a & ~uintptr_t(15));
+    const int delta = (int)(a & 15);
+    const int nblk = (int)((delta + bytes + 15) >> 4);
+    for (int b = tid; b < nblk; b += nt) cp_async16(dst + 16 * b, base + 16 * b);
+    return delta;
 }
 
 // Local values of one element into the tile's shared memory (the
@@ -581,8 +629,10 @@ __device__ __forceinline__ void store_local_s(double* __restrict__ sloc, int nt,
 template <bool FROZEN, bool JAC, bool BATCH, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ TileArgs a) {
     extern __shared__ __align__(16) unsigned char tsm[];
-    double4* xs = reinterpret_cast<double4*>(tsm);
-    double* sd = reinterpret_cast<double*>(xs + a.max_nodes);
+    const TileSmem L(a.max_nodes, a.max_edges, NT);
+    double4* xs = reinterpret_cast<double4*>(tsm + L.xs);
+    double* sphi = reinterpret_cast<double*>(tsm + L.phi);
+    double* sd = reinterpret_cast<double*>(tsm + L.sd);
     double* scx = sd;
     double* scy = sd + NT;
     double* scz = sd + 2 * NT;
@@ -592,22 +642,31 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
     double* sq2 = sd + 6 * NT;
     double* srho = sd + 7 * NT;
     double* sloc = sd + 8 * NT;
-    int4* sfn = reinterpret_cast<int4*>(sd + TS_DOUBLES * NT);
-    ushort4* slc = reinterpret_cast<ushort4*>(sfn + NT);
-    uint8_t* slim = reinterpret_cast<uint8_t*>(slc + NT);
+    int4* sfn = reinterpret_cast<int4*>(tsm + L.fn);
+    ushort4* slc = reinterpret_cast<ushort4*>(tsm + L.lc);
+    uint8_t* slim = tsm + L.lim;
+    int32_t* sperm = reinterpret_cast<int32_t*>(tsm + L.perm);
     const int tid = threadIdx.x;
     const int64_t E = a.E;
     MonAcc acc;
     for (int64_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const int32_t e0 = a.eoff[t], ne = a.eoff[t + 1] - e0;
         const int32_t n0 = a.noff[t], nn = a.noff[t + 1] - n0;
-        // ---- P0
-        for (int r = tid; r < nn; r += NT) {
-            const int32_t n = a.tnode[n0 + r];
-            double x, y, z, w;
-            ld4(reinterpret_cast<const double*>(a.X + n), x, y, z, w);
-            xs[r] = make_double4(x, y, z, a.phi[n]);
+        const int32_t u0 = a.uoff[t], nu = a.uoff[t + 1] - u0;
+        // ---- P0: positions (group 1), the plan slice (group 2), potentials
+        stage16(tsm + L.xs, a.txyz + n0, (size_t)nn * sizeof(double4), tid, NT);
+        cp_async_commit();
+        const int d_noff = stage16(tsm + L.noff, a.nent_off + n0, (size_t)(nn + 1) * sizeof(int32_t), tid, NT);
+        const int d_ndst = stage16(tsm + L.ndst, a.ndst + n0, (size_t)nn * sizeof(int2), tid, NT);
+        const int d_nent = stage16(tsm + L.nent, a.nent + 4 * (int64_t)e0, (size_t)4 * ne * sizeof(uint16_t), tid, NT);
+        int d_uoff = 0, d_udst = 0, d_uent = 0;
+        if (JAC) {
+            d_uoff = stage16(tsm + L.uoff, a.uent_off + u0, (size_t)(nu + 1) * sizeof(int32_t), tid, NT);
+            d_udst = stage16(tsm + L.udst, a.udst + u0, (size_t)nu * sizeof(int2), tid, NT);
+            d_uent = stage16(tsm + L.uent, a.uent + 6 * (int64_t)e0, (size_t)6 * ne * sizeof(uint16_t), tid, NT);
         }
+        cp_async_commit();
+        for (int r = tid; r < nn; r += NT) sphi[r] = a.phi[a.tnode[n0 + r]];
         const bool act = tid < ne;
         const int64_t xe = (int64_t)e0 + tid;
         int32_t user = 0;
@@ -617,7 +676,9 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
             slc[tid] = lc;
             sfn[tid] = a.fnbr[xe];
             user = a.perm[xe];
+            sperm[tid] = user;
         }
+        cp_async_wait<1>();  // this thread's position blocks are in
         __syncthreads();
         // ---- P1
         int ci = 0;
@@ -633,10 +694,11 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
             {
                 double bb[12];
                 geom_B_pts(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z, bb, Ve);
+                const double f0 = sphi[lc.x], f1 = sphi[lc.y], f2 = sphi[lc.z], f3 = sphi[lc.w];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    g[d] = radd(radd(radd(rmul(p0.w, bb[d]), rmul(p1.w, bb[3 + d])), rmul(p2.w, bb[6 + d])),
-                                rmul(p3.w, bb[9 + d]));
+                    g[d] = radd(radd(radd(rmul(f0, bb[d]), rmul(f1, bb[3 + d])), rmul(f2, bb[6 + d])),
+                                rmul(f3, bb[9 + d]));
             }
             const double q2n = __ddiv_rn(dot3r(g[0], g[1], g[2], g[0], g[1], g[2]), a.u2);
             q2l = q2n < F.q2cap ? q2n : F.q2cap;
@@ -810,22 +872,26 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
 #pragma unroll
                 for (int i = 0; i < 4; ++i) sloc[(2 * i) * NT + tid] = w1 * gB[i];
             }
-            a.up_out[user] = a.perm[u];
+            a.up_out[user] = u_in ? sperm[lu] : a.perm[u];
             if (a.rt_out) a.rt_out[user] = rt;
         }
+        cp_async_wait<0>();  // this thread's plan blocks are in
         __syncthreads();
-        // ---- P5: the tile's outputs
+        // ---- P5: the tile's outputs, the plan slice from shared memory
+        const int32_t* pnoff = reinterpret_cast<const int32_t*>(tsm + L.noff + d_noff);
+        const int2* pndst = reinterpret_cast<const int2*>(tsm + L.ndst + d_ndst);
+        const uint16_t* pnent = reinterpret_cast<const uint16_t*>(tsm + L.nent + d_nent);
+        const int32_t kbase = 4 * e0;
         for (int r = tid; r < nn; r += NT) {
-            const int32_t p = n0 + r;
-            const int32_t k1 = a.nent_off[p + 1];
+            const int32_t k1 = pnoff[r + 1] - kbase;
             double rs = 0.0, ds = 0.0;
-            for (int32_t k = a.nent_off[p]; k < k1; ++k) {
-                const uint32_t c = a.nent[k];
+            for (int32_t k = pnoff[r] - kbase; k < k1; ++k) {
+                const uint32_t c = pnent[k];
                 const int l = c >> 2, i = c & 3;
                 rs += sloc[(2 * i) * NT + l];
                 if (JAC) ds += sloc[(2 * i + 1) * NT + l];
             }
-            const int2 d = a.ndst[p];
+            const int2 d = pndst[r];
             if (d.x >= 0) {
                 a.R[d.x] = rs;
                 if (JAC) a.J[d.y] = ds;
@@ -836,15 +902,18 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
             }
         }
         if (JAC) {
-            const int32_t u1 = a.uoff[t + 1];
-            for (int32_t p = a.uoff[t] + tid; p < u1; p += NT) {
-                const int32_t k1 = a.uent_off[p + 1];
+            const int32_t* puoff = reinterpret_cast<const int32_t*>(tsm + L.uoff + d_uoff);
+            const int2* pudst = reinterpret_cast<const int2*>(tsm + L.udst + d_udst);
+            const uint16_t* puent = reinterpret_cast<const uint16_t*>(tsm + L.uent + d_uent);
+            const int32_t cbase = 6 * e0;
+            for (int p = tid; p < nu; p += NT) {
+                const int32_t k1 = puoff[p + 1] - cbase;
                 double v = 0.0;
-                for (int32_t k = a.uent_off[p]; k < k1; ++k) {
-                    const uint32_t c = a.uent[k];
+                for (int32_t k = puoff[p] - cbase; k < k1; ++k) {
+                    const uint32_t c = puent[k];
                     v += sloc[(8 + (c & 7)) * NT + (c >> 3)];
                 }
-                const int2 d = a.udst[p];
+                const int2 d = pudst[p];
                 if (d.x >= 0) {
                     a.J[d.x] = v;
                     a.J[d.y] = v;
@@ -1518,7 +1587,7 @@ template <bool FR, bool JA, bool BA, int NT, int MB>
 static void launch_tiles_nt(const up3d_mesh* m, const TileArgs& ta, cudaStream_t s) {
     auto kern = k_tile_eval<FR, JA, BA, NT, MB>;
     const TilePlan& P = *m->tiles;
-    const size_t smem = tile_smem_bytes(P.max_nodes, NT);
+    const size_t smem = TileSmem(P.max_nodes, P.max_edges, NT).total;
     UP3D_REQUIRE(smem <= 227 * 1024, UP3D_ERR_VALUE, "tiled assembly: a tile's shared memory exceeds 227 KB");
     if (smem > 48 * 1024)  // per device: set on every launch that needs it
         UP3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1541,7 +1610,7 @@ static void tiled_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
                            const int32_t* case_of, int n_cases, const int64_t* up_fz, const int8_t* br_fz,
                            double* R, double* data, double* rt_out, int32_t* up_dst, up3d_monitors* mo,
                            int8_t* br_out, cudaStream_t s) {
-    ensure_tiles(m, m->tune.tile_elems, s);
+    ensure_tiles(m, m->tune.tile_elems, m->tune.tile_stretch, s);
     const TilePlan& P = *m->tiles;
     TileArgs ta;
     ta.conn = P.conn.get();
@@ -1555,6 +1624,7 @@ static void tiled_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     ta.noff = P.noff.get();
     ta.uoff = P.uoff.get();
     ta.tnode = P.tnode.get();
+    ta.txyz = P.txyz.get();
     ta.lconn = P.lconn.get();
     ta.nent_off = P.nent_off.get();
     ta.nent = P.nent.get();
@@ -1577,6 +1647,7 @@ static void tiled_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     ta.case_of = case_of;
     ta.n_cases = n_cases;
     ta.max_nodes = P.max_nodes;
+    ta.max_edges = P.max_edges;
     ta.E = m->E;
     ta.n_tiles = P.n_tiles;
     ta.F0 = F;
@@ -1715,6 +1786,8 @@ int up3d_mesh_set_tuning(up3d_mesh* m, const up3d_tuning* t) {
                      "up3d_mesh_set_tuning: assembly must be 0 (two-pass) or 1 (tiled)");
         UP3D_REQUIRE(t->tile_elems == 128 || t->tile_elems == 256, UP3D_ERR_VALUE,
                      "up3d_mesh_set_tuning: tile_elems must be 128 or 256");
+        UP3D_REQUIRE(t->tile_stretch == 1 || t->tile_stretch == 2 || t->tile_stretch == 4, UP3D_ERR_VALUE,
+                     "up3d_mesh_set_tuning: tile_stretch must be 1, 2 or 4");
         m->tune = *t;
     });
 }
@@ -1818,26 +1891,28 @@ int up3d_autotune(up3d_mesh* m, const double* phi, const up3d_flow* flow, int re
             m->tune.row_us = best_r;
             // the tiled form, one plan per tile size: the whole evaluation
             // (tile kernel + combine) against the two passes
-            static const int tile_sizes[] = {128, 256};
+            static const int tile_shapes[][2] = {{256, 1}, {256, 4}, {128, 4}};
             double best_t = 0.0;
-            int best_T = 0;
-            for (int T : tile_sizes) {
-                m->tune.tile_elems = T;
+            int best_ts = -1;
+            for (int k = 0; k < (int)(sizeof(tile_shapes) / sizeof(tile_shapes[0])); ++k) {
+                m->tune.tile_elems = tile_shapes[k][0];
+                m->tune.tile_stretch = tile_shapes[k][1];
                 const double t = time_it([&] {
                     tiled_evaluate(m, phi, F, u2, no_flows, no_case, 0, no_up, no_br, R.get(), J.get(), no_rt,
                                    m->up32.get(), mo, no_brout, s);
                 });
-                if (best_T == 0 || t < best_t) {
+                if (best_ts < 0 || t < best_t) {
                     best_t = t;
-                    best_T = T;
+                    best_ts = k;
                 }
             }
-            m->tune.tile_elems = best_T;
+            m->tune.tile_elems = tile_shapes[best_ts][0];
+            m->tune.tile_stretch = tile_shapes[best_ts][1];
             if (best_t < best_e + best_r) {
                 m->tune.assembly = 1;
                 m->tune.elem_us = best_t;
                 m->tune.row_us = 0.0;
-                ensure_tiles(m, best_T, s);
+                ensure_tiles(m, m->tune.tile_elems, m->tune.tile_stretch, s);
             } else {
                 m->tune.assembly = 0;
             }

@@ -52,7 +52,7 @@ struct Dsu {
 
 // Recursive coordinate bisection of a[0, n) into runs of T (all full but
 // the last); a holds user element ids.
-void rcb(int32_t* a, int64_t n, int T, const std::vector<double4>& cen, int depth) {
+void rcb(int32_t* a, int64_t n, int T, const std::vector<double4>& cen, double stretch, int depth) {
     if (n <= T) {
         std::sort(a, a + n);
         return;
@@ -64,9 +64,12 @@ void rcb(int32_t* a, int64_t n, int T, const std::vector<double4>& cen, int dept
         lo[1] = std::min(lo[1], c.y); hi[1] = std::max(hi[1], c.y);
         lo[2] = std::min(lo[2], c.z); hi[2] = std::max(hi[2], c.z);
     }
+    // the longest extent, x counted 1/stretch: tiles `stretch` times longer
+    // along x than across
+    const double ext[3] = {(hi[0] - lo[0]) / stretch, hi[1] - lo[1], hi[2] - lo[2]};
     int ax = 0;
     for (int d = 1; d < 3; ++d)
-        if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+        if (ext[d] > ext[ax]) ax = d;
     const int64_t nt = (n + T - 1) / T;
     const int64_t k = (nt / 2) * T;
     auto coord = [&](int32_t e) {
@@ -79,13 +82,13 @@ void rcb(int32_t* a, int64_t n, int T, const std::vector<double4>& cen, int dept
     });
     if (depth < 6 && n > 65536) {
 #pragma omp task shared(cen)
-        rcb(a, k, T, cen, depth + 1);
+        rcb(a, k, T, cen, stretch, depth + 1);
 #pragma omp task shared(cen)
-        rcb(a + k, n - k, T, cen, depth + 1);
+        rcb(a + k, n - k, T, cen, stretch, depth + 1);
 #pragma omp taskwait
     } else {
-        rcb(a, k, T, cen, depth + 1);
-        rcb(a + k, n - k, T, cen, depth + 1);
+        rcb(a, k, T, cen, stretch, depth + 1);
+        rcb(a + k, n - k, T, cen, stretch, depth + 1);
     }
 }
 
@@ -105,7 +108,7 @@ constexpr int PAIR_J[6] = {1, 2, 3, 2, 3, 3};
 
 // The plan as host arrays (uploaded as they are into a TilePlan).
 struct PlanHost {
-    int32_t T = 0, max_nodes = 0;
+    int32_t T = 0, stretch = 1, max_nodes = 0, max_edges = 0;
     int64_t n_tiles = 0, n_tile_nodes = 0, n_tile_edges = 0, n_part = 0;
     std::vector<int32_t> perm, iperm, eoff, noff, uoff, tnode, nent_off, uent_off;
     std::vector<ushort4> lconn;
@@ -120,8 +123,10 @@ struct PlanHost {
 // neighbours, centroids and the P1 pattern (sorted rows).
 PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>& fn, const std::vector<double4>& cen,
                          int64_t N, const std::vector<int32_t>& indptr, const std::vector<int32_t>& indices,
-                         int T) {
+                         int T, int stretch) {
     UP3D_REQUIRE(T == 128 || T == 256, UP3D_ERR_VALUE, "tile plan: tile_elems must be 128 or 256");
+    UP3D_REQUIRE(stretch == 1 || stretch == 2 || stretch == 4, UP3D_ERR_VALUE,
+                 "tile plan: tile_stretch must be 1, 2 or 4");
     const int64_t E = (int64_t)conn.size(), Z = (int64_t)indices.size();
     // absolute diagonal slot of each row (-1 for an empty row) and the
     // transposed slot of every entry
@@ -167,7 +172,8 @@ PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>&
     // ---- 2. bisection per component; tiles of T within each component
 #pragma omp parallel
 #pragma omp single
-    for (int32_t c = 0; c < n_comp; ++c) rcb(order.data() + comp_off[c], comp_off[c + 1] - comp_off[c], T, cen, 0);
+    for (int32_t c = 0; c < n_comp; ++c)
+        rcb(order.data() + comp_off[c], comp_off[c + 1] - comp_off[c], T, cen, (double)stretch, 0);
     std::vector<int32_t> eoff(1, 0);
     for (int32_t c = 0; c < n_comp; ++c)
         for (int64_t b = comp_off[c]; b < comp_off[c + 1]; b += T)
@@ -276,12 +282,13 @@ PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>&
     std::vector<int2> ndst(n_tn), udst(n_te);
     std::vector<int32_t> node_pc(N + 1, 0), slot_pc(Z + 1, 0);  // partials per node / slot
     int64_t q = 0;
-    int32_t max_nodes = 0;
+    int32_t max_nodes = 0, max_edges = 0;
     {
         int64_t ne_run = 0, ue_run = 0;
         for (int64_t t = 0; t < n_tiles; ++t) {
             const TileHost& h = th[t];
             max_nodes = std::max<int32_t>(max_nodes, (int32_t)h.nodes.size());
+            max_edges = std::max<int32_t>(max_edges, (int32_t)h.eslot.size());
             for (size_t r = 0; r < h.nodes.size(); ++r) {
                 const int64_t p = noff[t] + (int64_t)r;
                 const int32_t n = h.nodes[r];
@@ -402,7 +409,9 @@ PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>&
 
     PlanHost H;
     H.T = T;
+    H.stretch = stretch;
     H.max_nodes = max_nodes;
+    H.max_edges = max_edges;
     H.n_tiles = n_tiles;
     H.n_tile_nodes = n_tn;
     H.n_tile_edges = n_te;
@@ -432,8 +441,18 @@ PlanHost build_plan_host(const std::vector<int4>& conn, const std::vector<int4>&
     return H;
 }
 
-void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
-    if (m->tiles && m->tiles->T == T) return;
+namespace {
+// tile-node positions in plan order (the kernel stages them with one
+// coalesced copy per tile)
+__global__ void k_tile_xyz(int64_t n, const int32_t* __restrict__ tnode, const double4* __restrict__ X,
+                           double4* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = X[tnode[i]];
+}
+}  // namespace
+
+void ensure_tiles(up3d_mesh* m, int T, int stretch, cudaStream_t s) {
+    if (m->tiles && m->tiles->T == T && m->tiles->stretch == stretch) return;
     UP3D_REQUIRE(T == 128 || T == 256, UP3D_ERR_VALUE, "tile plan: tile_elems must be 128 or 256");
     const auto t_start = std::chrono::steady_clock::now();
     const int64_t E = m->E, N = m->N, Z = m->nnz;
@@ -447,9 +466,11 @@ void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
     UP3D_CUDA(cudaMemcpyAsync(indptr.data(), m->indptr.get(), sizeof(int32_t) * (N + 1), cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaMemcpyAsync(indices.data(), m->indices.get(), sizeof(int32_t) * Z, cudaMemcpyDeviceToHost, s));
     UP3D_CUDA(cudaStreamSynchronize(s));
-    PlanHost H = build_plan_host(conn, fn, cen, N, indptr, indices, T);
+    PlanHost H = build_plan_host(conn, fn, cen, N, indptr, indices, T, stretch);
     auto P = std::make_shared<TilePlan>();
     P->T = T;
+    P->stretch = stretch;
+    P->max_edges = H.max_edges;
     P->n_tiles = H.n_tiles;
     P->max_nodes = H.max_nodes;
     P->n_tile_nodes = H.n_tile_nodes;
@@ -457,8 +478,10 @@ void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
     P->n_part = H.n_part;
     P->n_cnode = (int64_t)H.cn_dst.size();
     P->n_cedge = (int64_t)H.ce_dst.size();
+    // 16 bytes of padding after every array: the kernel stages a tile's
+    // ranges in whole 16-byte blocks
     auto up = [&](auto& buf, const auto& vec) {
-        buf.alloc(vec.size());
+        buf.alloc(vec.size() + 16 / sizeof(vec[0]) + 1);
         if (!vec.empty())
             UP3D_CUDA(cudaMemcpyAsync(buf.get(), vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice, s));
     };
@@ -479,6 +502,10 @@ void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s) {
     up(P->uent, H.uent);
     up(P->udst, H.udst);
     P->part.alloc(std::max<int64_t>(H.n_part, 1));
+    P->txyz.alloc(H.n_tile_nodes + 1);
+    k_tile_xyz<<<grid_for(H.n_tile_nodes, 256), 256, 0, s>>>(H.n_tile_nodes, P->tnode.get(), m->nodes4.get(),
+                                                            P->txyz.get());
+    UP3D_CHECK_LAUNCH();
     up(P->cn_off, H.cn_off);
     up(P->cn_idx, H.cn_idx);
     up(P->cn_dst, H.cn_dst);
@@ -499,10 +526,12 @@ extern "C" {
 int up3d_mesh_tile_info(up3d_mesh* m, int32_t tile_elems, up3d_tile_info* info, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(m && info, UP3D_ERR_ARGUMENT, "up3d_mesh_tile_info: null argument");
-        ensure_tiles(m, tile_elems, S(stream));
+        ensure_tiles(m, tile_elems, m->tune.tile_stretch, S(stream));
         const TilePlan& P = *m->tiles;
         info->tile_elems = P.T;
         info->max_nodes = P.max_nodes;
+        info->max_edges = P.max_edges;
+        info->tile_stretch = P.stretch;
         info->n_tiles = P.n_tiles;
         info->n_tile_nodes = P.n_tile_nodes;
         info->n_tile_edges = P.n_tile_edges;
@@ -520,7 +549,7 @@ struct up3d_tile_plan {
 
 int up3d_tile_plan_host_create(const int32_t* elements, const int32_t* face_neighbors, const double* centroids,
                                int64_t n_nodes, int64_t n_tets, const int32_t* indptr, const int32_t* indices,
-                               int32_t tile_elems, up3d_tile_plan** out) {
+                               int32_t tile_elems, int32_t tile_stretch, up3d_tile_plan** out) {
     return guarded([&] {
         UP3D_REQUIRE(elements && face_neighbors && centroids && indptr && indices && out, UP3D_ERR_ARGUMENT,
                      "up3d_tile_plan_host_create: null argument");
@@ -542,7 +571,7 @@ int up3d_tile_plan_host_create(const int32_t* elements, const int32_t* face_neig
         std::vector<int32_t> ip(indptr, indptr + n_nodes + 1), ix(indices, indices + Z);
         auto* h = new up3d_tile_plan();
         try {
-            h->H = build_plan_host(conn, fn, cen, n_nodes, ip, ix, tile_elems);
+            h->H = build_plan_host(conn, fn, cen, n_nodes, ip, ix, tile_elems, tile_stretch);
         } catch (...) {
             delete h;
             throw;
@@ -594,6 +623,8 @@ int up3d_tile_plan_host_info(const up3d_tile_plan* h, up3d_tile_info* info) {
         const PlanHost& H = h->H;
         info->tile_elems = H.T;
         info->max_nodes = H.max_nodes;
+        info->max_edges = H.max_edges;
+        info->tile_stretch = H.stretch;
         info->n_tiles = H.n_tiles;
         info->n_tile_nodes = H.n_tile_nodes;
         info->n_tile_edges = H.n_tile_edges;

@@ -26,6 +26,8 @@ namespace up3d {
 
 struct TilePlan {
     int32_t T = 0;              // most elements per tile
+    int32_t stretch = 1;        // tiles this many times longer along x than across
+    int32_t max_edges = 0;      // most distinct element edges of one tile
     int64_t n_tiles = 0;
     int32_t max_nodes = 0;      // most distinct nodes of one tile
     int64_t n_tile_nodes = 0;   // sum over tiles of their distinct nodes
@@ -44,6 +46,7 @@ struct TilePlan {
     DBuf<int32_t> noff;         // (n_tiles + 1) tile-node range of each tile
     DBuf<int32_t> uoff;         // (n_tiles + 1) tile-edge range of each tile
     DBuf<int32_t> tnode;        // (n_tile_nodes) global node of each tile-node, ascending per tile
+    DBuf<double4> txyz;         // (n_tile_nodes) its position (x, y, z, 0)
     DBuf<ushort4> lconn;        // (E) tile-local node indices of each element's vertices
     DBuf<int32_t> nent_off;     // (n_tile_nodes + 1)
     DBuf<uint16_t> nent;        // (4E) (local element << 2) | vertex, ascending local element
@@ -58,7 +61,8 @@ struct TilePlan {
     DBuf<int2> ce_dst;             // {slot, transposed slot}
 };
 
-// Builds (or rebuilds for another tile size) the mesh's tile plan.
-void ensure_tiles(up3d_mesh* m, int T, cudaStream_t s);
+// Builds (or rebuilds for another tile size or stretch) the mesh's tile
+// plan.  Every array is followed by 16 bytes of padding.
+void ensure_tiles(up3d_mesh* m, int T, int stretch, cudaStream_t s);
 
 }  // namespace up3d

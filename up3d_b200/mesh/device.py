@@ -133,11 +133,12 @@ class DeviceMesh:
         return t.as_dict()
 
     def set_tuning(self, elem_persistent: int = 0, elem_threads_per_sm: int = 512, row_lanes: int = 8,
-                   row_plan8: int = 0, assembly: int = 1, tile_elems: int = 256) -> None:
+                   row_plan8: int = 0, assembly: int = 1, tile_elems: int = 256, tile_stretch: int = 1) -> None:
         """Installs launch shapes by hand.  Within one assembly form (and,
-        for the tiled form, one tile size) every shape computes the same
-        bits; the forms agree to rounding."""
-        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, assembly, tile_elems, 0.0, 0.0)
+        for the tiled form, one tile size and stretch) every shape computes
+        the same bits; the forms agree to rounding."""
+        t = L.Tuning(elem_persistent, elem_threads_per_sm, row_lanes, row_plan8, assembly, tile_elems,
+                     tile_stretch, 0, 0.0, 0.0)
         L.call("up3d_mesh_set_tuning", self.handle, ctypes.byref(t))
 
     def term3_cache_hits(self) -> int:
