@@ -493,6 +493,7 @@ struct TileArgs {
     const int4* conn;        // (E) global node ids, internal order
     const int4* fnbr;        // (E) internal ids
     const double4* cen;      // (E) internal order
+    const double* disp;      // (E, 12) internal order
     const double4* X;        // (N) node positions
     const double* phi;       // (N)
     const int32_t* perm;     // internal -> user
@@ -739,42 +740,56 @@ __global__ void __launch_bounds__(NT, MB) k_tile_eval(const __grid_constant__ Ti
                     }
                 }
                 const double target = rmul(0.8, rsub(pmax, pmin));
-                double reach = 0.0, cx = ccx, cy = ccy, cz = ccz;
+                double reach = 0.0;
                 int64_t cur = xe;
                 for (int hops = 0; hops < 4 && reach < target; ++hops) {
                     const uint32_t lcur = (uint32_t)(cur - e0);
-                    const int4 f = lcur < (uint32_t)ne ? sfn[lcur] : a.fnbr[cur];
-                    const int nb[4] = {f.x, f.y, f.z, f.w};
+                    int nb[4];
+                    double d[4];
+                    if (lcur < (uint32_t)ne) {
+                        // inside the tile: cen(nbr) - cen(cur) from shared memory
+                        // (a neighbour outside the tile from the centroid table)
+                        const int4 f = sfn[lcur];
+                        nb[0] = f.x; nb[1] = f.y; nb[2] = f.z; nb[3] = f.w;
+                        const double cx = scx[lcur], cy = scy[lcur], cz = scz[lcur];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            d[k] = 0.0;
+                            if (nb[k] >= 0 && nb[k] < E) {
+                                const uint32_t ln = (uint32_t)(nb[k] - e0);
+                                double nx, ny, nz;
+                                if (ln < (uint32_t)ne) {
+                                    nx = scx[ln];
+                                    ny = scy[ln];
+                                    nz = scz[ln];
+                                } else {
+                                    double w;
+                                    ld4(reinterpret_cast<const double*>(a.cen + nb[k]), nx, ny, nz, w);
+                                }
+                                d[k] = dot3r(rsub(nx, cx), rsub(ny, cy), rsub(nz, cz), gx, gy, gz);
+                            }
+                        }
+                    } else {
+                        // outside: the precomputed displacement record (the
+                        // same rounded differences), one load next to fnbr
+                        const int4 f = a.fnbr[cur];
+                        nb[0] = f.x; nb[1] = f.y; nb[2] = f.z; nb[3] = f.w;
+                        double r[12];
+                        ld_B(a.disp + 12 * cur, r);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) d[k] = dot3r(r[3 * k], r[3 * k + 1], r[3 * k + 2], gx, gy, gz);
+                    }
                     int64_t best = -1;
-                    double best_disp = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+                    double best_disp = 0.0;
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        if (nb[k] >= 0 && nb[k] < E) {
-                            const uint32_t ln = (uint32_t)(nb[k] - e0);
-                            double nx, ny, nz;
-                            if (ln < (uint32_t)ne) {
-                                nx = scx[ln];
-                                ny = scy[ln];
-                                nz = scz[ln];
-                            } else {
-                                double w;
-                                ld4(reinterpret_cast<const double*>(a.cen + nb[k]), nx, ny, nz, w);
-                            }
-                            const double d = dot3r(rsub(nx, cx), rsub(ny, cy), rsub(nz, cz), gx, gy, gz);
-                            if (d < best_disp) {
-                                best_disp = d;
-                                best = nb[k];
-                                bx = nx;
-                                by = ny;
-                                bz = nz;
-                            }
+                        if (nb[k] >= 0 && nb[k] < E && d[k] < best_disp) {
+                            best_disp = d[k];
+                            best = nb[k];
                         }
                     }
                     if (best < 0) break;
                     cur = best;
-                    cx = bx;
-                    cy = by;
-                    cz = bz;
                     reach = radd(reach, -best_disp);
                 }
                 u = cur;
@@ -1616,6 +1631,7 @@ static void tiled_evaluate(up3d_mesh* m, const double* phi, const Flow& F, doubl
     ta.conn = P.conn.get();
     ta.fnbr = P.fnbr.get();
     ta.cen = P.cen.get();
+    ta.disp = P.disp.get();
     ta.X = m->nodes4.get();
     ta.phi = phi;
     ta.perm = P.perm.get();

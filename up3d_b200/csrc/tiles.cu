@@ -449,6 +449,13 @@ __global__ void k_tile_xyz(int64_t n, const int32_t* __restrict__ tnode, const d
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = X[tnode[i]];
 }
+// the mesh's face-displacement records in internal order
+__global__ void k_tile_disp(int64_t E, const int32_t* __restrict__ perm, const double* __restrict__ disp,
+                            double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 12 * E;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = disp[12 * (int64_t)perm[i / 12] + i % 12];
+}
 }  // namespace
 
 void ensure_tiles(up3d_mesh* m, int T, int stretch, cudaStream_t s) {
@@ -505,6 +512,9 @@ void ensure_tiles(up3d_mesh* m, int T, int stretch, cudaStream_t s) {
     P->txyz.alloc(H.n_tile_nodes + 1);
     k_tile_xyz<<<grid_for(H.n_tile_nodes, 256), 256, 0, s>>>(H.n_tile_nodes, P->tnode.get(), m->nodes4.get(),
                                                             P->txyz.get());
+    UP3D_CHECK_LAUNCH();
+    P->disp.alloc(12 * E);
+    k_tile_disp<<<grid_for(12 * E, 256), 256, 0, s>>>(E, P->perm.get(), m->disp.get(), P->disp.get());
     UP3D_CHECK_LAUNCH();
     up(P->cn_off, H.cn_off);
     up(P->cn_idx, H.cn_idx);

@@ -42,6 +42,7 @@ struct TilePlan {
     DBuf<int4> conn;            // (E) global node ids, internal order
     DBuf<int4> fnbr;            // (E) face neighbours as internal ids (-1 boundary)
     DBuf<double4> cen;          // (E) centroids, internal order
+    DBuf<double> disp;          // (E, 12) face displacements cen(nbr) - cen(e), internal order
     DBuf<int32_t> eoff;         // (n_tiles + 1) element range of each tile
     DBuf<int32_t> noff;         // (n_tiles + 1) tile-node range of each tile
     DBuf<int32_t> uoff;         // (n_tiles + 1) tile-edge range of each tile
