@@ -278,13 +278,17 @@ def newton_timing(spec, reps=2):
     import torch
     from up3d_b200.mesh.kuhn import bump_channel
     from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
-    shape_s, amp_s, mach_s = spec.split(":")
+    parts = spec.split(":")
+    shape_s, amp_s, mach_s = parts[:3]
     shape = tuple(int(v) for v in shape_s.split("x"))
     amp, mach = float(amp_s), float(mach_s)
+    m_start = float(parts[3]) if len(parts) > 3 else mach
+    dm_step = float(parts[4]) if len(parts) > 4 else 0.05
     mesh = bump_channel(*shape, amplitude=amp, seed=0)
     from up3d_b200.mesh.kuhn import choking_mach
     out = {"case": f"bump channel {shape_s} Kuhn-split ({mesh.n_tets} tets), bump {amp}, "
-                   f"M_inf {mach}, from freestream to |R_free|inf < 1e-10",
+                   f"M_inf {mach}" + (f" (Mach ramp from {m_start} by {dm_step})" if m_start < mach else "")
+                   + ", from freestream to |R_free|inf < 1e-10",
            "n_tets": mesh.n_tets,
            "choking_mach_quasi_1d": round(choking_mach(amp), 4),
            "timed_runs": "second of two" if reps > 1 else "first (workspace and tile plan built before the clock)"}
@@ -295,17 +299,18 @@ def newton_timing(spec, reps=2):
             ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            res = solve_newton_transonic(ws, mach, m_start=mach, dm=0.05, precision=prec)
+            res = solve_newton_transonic(ws, mach, m_start=m_start, dm=dm_step, precision=prec)
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
         phis[prec] = res["phi"]
         out[prec] = {"time_s": round(dt, 4), "converged": bool(res["converged"]),
                      "final_residual": float(res["residual_history"][-1]),
-                     "n_newton": int(res["level_history"][-1][1]),
-                     "n_gmres": int(res["level_history"][-1][3]),
+                     "n_newton": int(sum(lv[1] for lv in res["level_history"])),
+                     "n_gmres": int(sum(lv[3] for lv in res["level_history"])),
                      "n_refinements": int(res.get("n_refinements", 0)),
                      "n_supersonic": int(res["n_supersonic"]),
                      "phases_s": {k: round(v, 4) for k, v in res["timings"].items()}}
+        out[prec]["levels"] = [[round(float(lv[0]), 4), int(lv[1]), float(lv[2])] for lv in res["level_history"]]
     out["mixed_vs_fp64_max_dphi"] = float((phis["mixed"] - phis["fp64"]).abs().max())
     out["speedup_mixed"] = round(out["fp64"]["time_s"] / out["mixed"]["time_s"], 3)
     return out

@@ -702,6 +702,10 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
                            tol_rho: float = 1e-10, n_picard_max: int = 40, rtol: float = 1e-10,
                            maxiter: int = 3000, amg_rebuild_every: int = 4, forcing: float = 0.0,
                            upwind_c: float = 1.5, m_crit: float = 0.95, upwind_weighted: bool = False,
+                           upwind_mode: str = "kernel", upwind_p_weight: float = 3.0,
+                           upwind_reach_frac: float = 1.0, upwind_reach_gain_max: float = 4.0,
+                           upwind_nbr_depth: int = 3, upwind_sigma_s_frac: float = 0.35,
+                           upwind_sigma_p_frac: float = 0.35,
                            phi_init=None, gamma_init=None, kutta_per_outer: Optional[int] = None,
                            m_cap: float = 3.0, omega_rho: float = 1.0, pseudo_dt: Optional[float] = None,
                            pseudo_dt_growth: float = 1.1, pseudo_dt_max_ratio: float = 100.0,
@@ -723,8 +727,12 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
     numbers) and the convergence scalars on the host.  damping_theta adds
     theta diag(A_free) of each outer, pseudo_dt the lumped volumes over an
     adaptive dtau, to the matrix and D phi_k to the right-hand side (the
-    reference's pseudo-transient forms).  Not built: upwind_weighted
-    (NotImplementedError)."""
+    reference's pseudo-transient forms).  upwind_weighted takes rho~ from
+    the weighted upwind modes (UpwindOperator(weighted=True, mode=...),
+    kernels/upwind.py:176-454, with the reference's parameters) instead of
+    the walk, and the residual from PicardOperator.assemble_residual at
+    that rho~, as the reference's loop does (picard.py:592-603, :703-710,
+    :803-813)."""
     t = L.require_cuda()
     from ..physics.isentropic import mach_squared_field
     from .linear import solve_cg
@@ -732,8 +740,6 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         raise ValueError(f"solve_subsonic_lifting needs 0 <= M_inf < 1, got {m_inf}")
     if pseudo_dt is not None and damping_theta is not None:
         raise ValueError("pseudo_dt and damping_theta are mutually exclusive stabilizers -- pick one")
-    if upwind_weighted:
-        raise NotImplementedError("upwind_weighted is not built in the device lifting Picard")
     t_wall0 = time.perf_counter()
     ws = workspace
     if ws is None:
@@ -783,9 +789,30 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         v = phi_cut[probes].cpu().numpy()
         return np.bincount(wc.te_station, weights=v[:n_te] - v[n_te:], minlength=n_st) / counts
 
+    weighted = upwind_weighted and upwind_c > 0.0 and m_inf > 0.0
+    if weighted:
+        from ..kernels.upwind import UpwindOperator
+        from ..physics.isentropic import density_field, limit_q2_field
+        upw_w = UpwindOperator(t.as_tensor(np.asarray(ws.mesh.nodes)), t.as_tensor(np.asarray(ws.mesh.elements)),
+                               weighted=True, mode=upwind_mode, p_weight=upwind_p_weight,
+                               reach_frac=upwind_reach_frac, reach_gain_max=upwind_reach_gain_max,
+                               nbr_depth=upwind_nbr_depth, sigma_s_frac=upwind_sigma_s_frac,
+                               sigma_p_frac=upwind_sigma_p_frac)
+
     def evaluate(phi_cut):
-        ws.ev.evaluate(phi_cut, flow, jacobian=False, keep_state=True)
-        return ws.ev.rho_tilde.clone(), ws.ev.read_monitors()
+        """(rho~, monitors, R) at phi_cut: the fused evaluation (walk
+        flux), or the weighted modes' rho~ and the residual at it."""
+        if not weighted:
+            ws.ev.evaluate(phi_cut, flow, jacobian=False, keep_state=True)
+            return ws.ev.rho_tilde.clone(), ws.ev.read_monitors(), ws.ev.R
+        grad, q2 = ws.op.velocities(phi_cut)
+        q2l = limit_q2_field(q2 / u_inf ** 2, m_inf, m_cap, gamma_air)
+        rho = density_field(q2l, m_inf, gamma_air)
+        rt = upw_w.rho_tilde(grad, q2l, rho, m_inf, upwind_c, m_crit, gamma_air, rho_floor).clone()
+        R = ws.op.assemble_residual(phi_cut, rt).clone()
+        mon = {"nu_max": float(upw_w.nu_max), "n_supersonic": int(upw_w.n_supersonic),
+               "n_floored": int(upw_w.n_floored), "n_limited": int((q2l != q2 / u_inf ** 2).sum())}
+        return rt, mon, R
 
     if gamma_fixed is not None:
         gamma = np.broadcast_to(np.atleast_1d(np.asarray(gamma_fixed, dtype=np.float64)), (n_st,)).copy()
@@ -800,7 +827,7 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
     else:
         phi_cut = L.to_device(freestream_phi(np.asarray(mesh_cut.nodes), alpha_deg, u_inf), t.float64)
         phi_red = None
-    rho_t, mon = evaluate(phi_cut)
+    rho_t, mon, _ = evaluate(phi_cut)
     # pseudo-transient term D (picard.py:586-596, :736-745): the local
     # theta diag(A_free) of each outer, or the lumped volumes over dtau
     diag_pos = None
@@ -899,8 +926,8 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
         phi_red = phi_red_new if (omega == 1.0 or phi_red is None) else phi_red + omega * (phi_red_new - phi_red)
         phi_cut = ws.con.expand(phi_red, gamma)
         a = clock()
-        rho_t_new, mon = evaluate(phi_cut)
-        R = ws.ev.R if b_fold is None else ws.ev.R - b_cut
+        rho_t_new, mon, R_eval = evaluate(phi_cut)
+        R = R_eval if b_fold is None else R_eval - b_cut
         residual_history.append(float(fold(R).abs().max()))
         drho = float((rho_t_new - rho_t).abs().max())
         drho_history.append(drho)
