@@ -770,8 +770,9 @@ def batched_timing(spec, seed=0):
         b = BatchedChannels(meshes, ordering=batch.ordering)
         b.ws.ev.mesh.set_tuning(shapes_tuned["elem_persistent"], shapes_tuned["elem_threads_per_sm"],
                                 shapes_tuned["row_lanes"], shapes_tuned["row_plan8"], shapes_tuned["assembly"],
-                                shapes_tuned["tile_elems"])
-        b.ws.ev.mesh.tile_info()
+                                shapes_tuned["tile_elems"], shapes_tuned["tile_stretch"])
+        if shapes_tuned["assembly"] == 1:
+            b.ws.ev.mesh.tile_info()
         return b
     res_b = None
     for _ in range(2):

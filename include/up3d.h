@@ -481,8 +481,9 @@ typedef struct {
     double row_us;
 } up3d_tuning;
 
-/* Default: {0, 512, 8, 0, 1, 256, 1}.  UP3D_ERR_VALUE for a shape outside
- * the lists. */
+/* Default: {0, 512, 8, 0, 0, 256, 1} (the two-pass form, measured faster on
+ * the benchmark meshes; the autotuner times both).  UP3D_ERR_VALUE for a
+ * shape outside the lists. */
 int up3d_mesh_set_tuning(up3d_mesh* mesh, const up3d_tuning* tuning);
 int up3d_mesh_get_tuning(const up3d_mesh* mesh, up3d_tuning* tuning);
 

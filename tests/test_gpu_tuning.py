@@ -46,7 +46,7 @@ def test_every_shape_gives_the_same_bits():
     flow = FlowParams(m_inf=0.8)
     t0 = dm.tuning()
     assert t0["row_lanes"] == 8 and t0["elem_persistent"] == 0 and t0["elem_threads_per_sm"] == 512
-    assert t0["assembly"] == 1 and t0["tile_elems"] == 256
+    assert t0["assembly"] == 0 and t0["tile_elems"] == 256 and t0["tile_stretch"] == 1
     dm.set_tuning(*SHAPES[0], assembly=0)
     R0, J0, up0, rt0, mon0 = _outputs(ev, phi, flow)
     assert mon0["n_term3_active"] > 0
@@ -98,7 +98,7 @@ def test_autotune_installs_a_listed_shape_and_keeps_parity():
     assert t["assembly"] in (0, 1) and t["tile_elems"] in (128, 256) and t["tile_stretch"] in (1, 2, 4)
     assert t["elem_us"] > 0 and (t["row_us"] > 0 or t["assembly"] == 1)
     R = ev.evaluate(phi, flow, jacobian=True).clone()
-    if t["assembly"] == 1 and t["tile_elems"] == 256 and t["tile_stretch"] == 1:
+    if t["assembly"] == 0:
         assert torch.equal(R, R0)
         assert (ev.jacobian().to_scipy() != J0).nnz == 0
     else:

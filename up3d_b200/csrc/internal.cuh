@@ -116,7 +116,7 @@ struct up3d_mesh {
     int32_t max_row_len = 0, max_deg = 0;
     int32_t n_colors = -1;
     int32_t n_sms = 148;                       // multiprocessors of the mesh's device
-    up3d_tuning tune = {0, 512, 8, 0, 1, 256, 1, 0, 0.0, 0.0};  // launch shapes of the fused evaluation
+    up3d_tuning tune = {0, 512, 8, 0, 0, 256, 1, 0, 0.0, 0.0};  // launch shapes of the fused evaluation
     std::shared_ptr<up3d::TilePlan> tiles;     // tiled assembly plan (built on first use)
     int32_t batch_cases = 0;                   // cases of the flow table in flows_ws (0 = none)
     // face-hop neighbourhoods of the weighted "kernel" upwind mode (built on

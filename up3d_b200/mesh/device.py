@@ -133,7 +133,7 @@ class DeviceMesh:
         return t.as_dict()
 
     def set_tuning(self, elem_persistent: int = 0, elem_threads_per_sm: int = 512, row_lanes: int = 8,
-                   row_plan8: int = 0, assembly: int = 1, tile_elems: int = 256, tile_stretch: int = 1) -> None:
+                   row_plan8: int = 0, assembly: int = 0, tile_elems: int = 256, tile_stretch: int = 1) -> None:
         """Installs launch shapes by hand.  Within one assembly form (and,
         for the tiled form, one tile size and stretch) every shape computes
         the same bits; the forms agree to rounding."""

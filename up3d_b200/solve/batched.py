@@ -213,23 +213,40 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                          dm: float = 0.05, tol_residual: float = 1e-10, n_newton_max: int = 30,
                          n_picard_seed: int = 5, amg_rebuild_every: int = 2, gmres_restart: int = 60,
                          gmres_maxiter: int = 10, freeze_tol: float = 1e-6, freeze_refresh_max: int = 2,
-                         use_graphs: bool = True, verbose: bool = False) -> Dict[str, object]:
+                         use_graphs: bool = True, compact_fraction: float = 0.5,
+                         verbose: bool = False) -> Dict[str, object]:
     """Lockstep Newton of every case (module docstring); returns the union
     potential, per-case convergence, iteration counts and timings.  With
     use_graphs the line search's trial evaluations replay one captured CUDA
-    graph (step, batched residual, per-case merit)."""
+    graph (step, batched residual, per-case merit).
+
+    Compaction: every Krylov step, V-cycle and evaluation runs over the
+    whole union, so once the cases still being solved hold less than
+    `compact_fraction` of the union's elements (the others converged at
+    their target Mach, or failed), the solve continues on a new union of
+    those cases alone -- their potentials, frozen selections and per-case
+    state carried over, the AMG hierarchy rebuilt -- and the finished
+    cases' potentials are kept aside (0 disables it)."""
     t = L.require_cuda()
+    batch0 = batch
     ws = batch.ws
     machs = np.asarray(machs, dtype=np.float64)
     C = batch.n_cases
+    C0 = C
     mask_b = ws.mask.bool()
+    orig = np.arange(C)                                  # current case -> caller's case
+    tets = np.array([m.n_tets for m in batch.meshes], dtype=np.int64)
+    final = {"phi": [None] * C0, "converged_at": np.full(C0, -1.0), "converged_s": np.full(C0, np.nan),
+             "failed": np.zeros(C0, dtype=bool), "n_newton": np.zeros(C0, dtype=np.int64),
+             "froze": np.zeros(C0, dtype=bool)}
+    n_compactions = 0
 
     def clock():
         t.cuda.synchronize()
         return time.perf_counter()
 
     timings = {"seed": 0.0, "residual": 0.0, "assembly": 0.0, "precond": 0.0, "linsolve": 0.0,
-               "line_search": 0.0}
+               "line_search": 0.0, "compaction": 0.0}
     t0 = clock()
     levels = sorted(set(mach_schedule(float(machs.max()), min(m_start, float(machs.max())), dm)))
     converged_at = np.full(C, -1.0)
@@ -271,6 +288,29 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
         history = []
         eta_prev = None
         for it in range(n_newton_max):
+            finished = failed | (converged_at >= 0)
+            if (compact_fraction > 0.0 and finished.any() and not finished.all()
+                    and tets[~finished].sum() < compact_fraction * tets.sum()):
+                tq = clock()
+                keep = np.nonzero(~finished)[0]
+                for c in np.nonzero(finished)[0]:
+                    o = orig[c]
+                    final["phi"][o] = batch.case_phi(phi, c).clone()
+                    final["converged_at"][o], final["converged_s"][o] = converged_at[c], converged_s[c]
+                    final["failed"][o], final["n_newton"][o], final["froze"][o] = failed[c], n_newton[c], frozen[c]
+                batch, phi = _compacted(batch, phi, keep)
+                ws = batch.ws
+                mask_b = ws.mask.bool()
+                case_node = batch.case_of_node
+                M_pre = None
+                machs, m_level, active = machs[keep], m_level[keep], active[keep]
+                converged_at, converged_s, failed = converged_at[keep], converged_s[keep], failed[keep]
+                frozen, n_refresh, prev_live = frozen[keep], n_refresh[keep], prev_live[keep]
+                n_newton, orig, tets = n_newton[keep], orig[keep], tets[keep]
+                history = [h[keep] for h in history]
+                C = len(keep)
+                n_compactions += 1
+                timings["compaction"] += clock() - tq
             ta = clock()
             R = batch.evaluate(phi, m_level, jacobian=False)
             Rf = R.masked_fill(mask_b, 0.0)
@@ -380,7 +420,36 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
         # a case still active at the end of a level failed it
         failed |= active
     t_total = clock() - t0
-    return {"phi": phi, "converged": converged_at >= 0, "failed": failed, "n_newton": n_newton,
-            "n_gmres_total": n_gmres_total, "levels": levels, "time_s": t_total, "seed_s": t_seed,
-            "timings": timings,
-            "converged_s": converged_s, "froze": frozen}
+    for c in range(C):
+        o = orig[c]
+        final["phi"][o] = batch.case_phi(phi, c)
+        final["converged_at"][o], final["converged_s"][o] = converged_at[c], converged_s[c]
+        final["failed"][o], final["n_newton"][o], final["froze"][o] = failed[c], n_newton[c], frozen[c]
+    phi_union = phi if batch is batch0 else batch0.union_phi(final["phi"])
+    return {"phi": phi_union, "converged": final["converged_at"] >= 0, "failed": final["failed"],
+            "n_newton": final["n_newton"], "n_gmres_total": n_gmres_total, "levels": levels, "time_s": t_total,
+            "seed_s": t_seed, "timings": timings, "n_compactions": n_compactions,
+            "converged_s": final["converged_s"], "froze": final["froze"]}
+
+
+def _compacted(batch: BatchedChannels, phi, keep):
+    """A new union of the cases `keep` of `batch` (same ordering and launch
+    shapes), with their potentials and frozen selections carried over."""
+    t = L.torch()
+    new = BatchedChannels([batch.meshes[c] for c in keep], u_inf=batch.u_inf, ordering=batch.ordering,
+                          tune=False)
+    tu = batch.ws.ev.mesh.tuning()
+    new.ws.ev.mesh.set_tuning(tu["elem_persistent"], tu["elem_threads_per_sm"], tu["row_lanes"], tu["row_plan8"],
+                              tu["assembly"], tu["tile_elems"], tu["tile_stretch"])
+    if tu["assembly"] == 1:
+        new.ws.ev.mesh.tile_info()
+    phi_new = new.union_phi([batch.case_phi(phi, c) for c in keep])
+    if batch.up_fz is not None:
+        new.up_fz = t.zeros(new.n_tets, dtype=t.int64, device="cuda")
+        new.br_fz = t.full((new.n_tets,), -1, dtype=t.int8, device="cuda")
+        for k, c in enumerate(keep):
+            a, b = int(batch.elem_off[c]), int(batch.elem_off[c + 1])
+            na, nb = int(new.elem_off[k]), int(new.elem_off[k + 1])
+            new.up_fz[na:nb] = batch.up_fz[a:b] - a + na
+            new.br_fz[na:nb] = batch.br_fz[a:b]
+    return new, phi_new
