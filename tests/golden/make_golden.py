@@ -743,6 +743,94 @@ def make_lifting_picard(name):
 
 
 
+def make_lagged_lu(name):
+    """The reference's lagged-LU Newton (solve_newton_lifting(precond=
+    "direct", direct_refactor_every=1000), solve/newton.py:978-1008: one
+    sparse LU, the later steps GMRES on the fresh coupled operator with the
+    stale LU as preconditioner to direct_reuse_rtol) on both lifting
+    channels from the freestream: the converged state and the step, refactor
+    and GMRES counts."""
+    from types import SimpleNamespace
+    from pyfp3d.mesh.wake_cut import WakeCut as RefWakeCut
+    from pyfp3d.solve.newton import solve_newton_lifting
+    from up3d_b200.mesh.wake_cut import channel_vortex_center, cut_channel_sheet
+    arrays = {}
+    for case, (shape, m_inf, alpha, spanwise) in LIFTING_CASES.items():
+        cut = cut_channel_sheet(bump_channel(*shape, amplitude=0.08, seed=3), normal="y")
+        wc = RefWakeCut()
+        for k in ("n_nodes_orig", "master_nodes", "slave_nodes", "te_nodes", "station_z",
+                  "node_station", "te_station", "kutta_upper", "kutta_lower"):
+            setattr(wc, k, getattr(cut.wc, k))
+        mc = SimpleNamespace(nodes=cut.nodes, elements=cut.elements, boundary_faces=cut.boundary_faces)
+        vc = channel_vortex_center(cut)
+        res = solve_newton_lifting(mc, wc, m_inf, alpha_deg=alpha, vortex_center=vc,
+                                   farfield_spanwise_gamma=spanwise, n_picard_seed=0, precond="direct",
+                                   direct_refactor_every=1000)
+        assert res["converged"], case
+        pre = f"{case}/"
+        arrays.update({pre + "phi": res["phi"], pre + "gamma": res["gamma"],
+                       pre + "n_newton": np.int64(res["n_newton"]),
+                       pre + "n_refactor": np.int64(res["n_refactor"]),
+                       pre + "n_gmres_total": np.int64(res["n_gmres_total"]),
+                       pre + "residual_history": np.array(res["residual_history"])})
+        print("lagged LU", case, res["n_newton"], res["n_refactor"], res["n_gmres_total"])
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
+def make_weighted_picard(name):
+    """The reference's nested lifting Picard with the weighted upwind modes
+    (solve_subsonic_lifting(upwind_weighted=True), solve/picard.py:440-447,
+    :592-603; pyamg swapped for scipy spilu, as in make_picard) on the
+    transonic lifting channel (16 x 6 x 4, M0.8, alpha 2 deg, spanwise far
+    field), modes "kernel" and "blend", from the freestream."""
+    from types import SimpleNamespace
+    import scipy.sparse.linalg as spla
+    import pyfp3d.solve.linear as lin
+    from pyfp3d.mesh.wake_cut import WakeCut as RefWakeCut
+    from pyfp3d.solve.picard import solve_subsonic_lifting
+    from up3d_b200.mesh.wake_cut import channel_vortex_center, cut_channel_sheet
+
+    def _ilu_preconditioner(A):
+        ilu = spla.spilu(A.tocsc(), drop_tol=1e-5, fill_factor=20.0)
+        return None, spla.LinearOperator(A.shape, matvec=ilu.solve)
+
+    def ref_wc(wc):
+        r = RefWakeCut()
+        for k in ("n_nodes_orig", "master_nodes", "slave_nodes", "free_nodes", "te_nodes", "station_z",
+                  "node_station", "te_station", "kutta_upper", "kutta_lower"):
+            setattr(r, k, getattr(wc, k))
+        return r
+
+    saved = lin.build_amg_preconditioner
+    lin.build_amg_preconditioner = _ilu_preconditioner
+    arrays = {}
+    try:
+        shape, m_inf, alpha, spanwise = LIFTING_CASES["trans"]
+        cut = cut_channel_sheet(bump_channel(*shape, amplitude=0.08, seed=3), normal="y")
+        mc = SimpleNamespace(nodes=cut.nodes, elements=cut.elements, boundary_faces=cut.boundary_faces)
+        vc = channel_vortex_center(cut)
+        for mode in ("kernel", "blend"):
+            res = solve_subsonic_lifting(mc, ref_wc(cut.wc), m_inf, alpha_deg=alpha, vortex_center=vc,
+                                         upwind_weighted=True, upwind_mode=mode,
+                                         farfield_spanwise_gamma=spanwise, n_picard_max=200)
+            assert res["converged"], mode
+            pre = f"{mode}/"
+            arrays.update({pre + "phi": res["phi"], pre + "gamma": res["gamma"],
+                           pre + "n_picard": np.int64(res["n_picard"]),
+                           pre + "n_nu_active": np.int64(res["n_nu_active"]),
+                           pre + "drho_history": np.array(res["drho_history"])})
+            print("weighted picard", mode, res["n_picard"], res["n_nu_active"], res["gamma"][:2])
+        arrays.update({"m_inf": np.float64(m_inf), "alpha_deg": np.float64(alpha),
+                       "vortex_center": np.array(vc, dtype=np.float64)})
+    finally:
+        lin.build_amg_preconditioner = saved
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def make_te_pressure(name):
     """The pressure-equality Kutta estimator (constraints/te_pressure.py,
     TEControlVolumes) on the NACA0012 coarse cut: its control-volume
@@ -805,6 +893,14 @@ def main():
     if "--lifting-only" in sys.argv:
         make_lifting("lifting_newton")
         make_lifting_picard("lifting_picard")
+        make_weighted_picard("weighted_picard")
+        make_lagged_lu("lagged_lu")
+        return
+    if "--lagged-lu-only" in sys.argv:
+        make_lagged_lu("lagged_lu")
+        return
+    if "--weighted-picard-only" in sys.argv:
+        make_weighted_picard("weighted_picard")
         return
     if "--naca-only" in sys.argv:
         make_naca(ref_root, "naca_coarse")
@@ -838,6 +934,8 @@ def main():
     make_naca(ref_root, "naca_coarse")
     make_swept_cut("swept_cut")
     make_lifting_picard("lifting_picard")
+    make_weighted_picard("weighted_picard")
+    make_lagged_lu("lagged_lu")
     make_te_pressure("te_pressure")
 
 

@@ -336,6 +336,88 @@ class NewtonWorkspace:
         out[self._free_d] = z
         return out
 
+    def lagged_step(self, lu, Aop: CoupledOperator, rhs, rtol: float, restart: int, maxiter: int):
+        """The lagged-LU reuse step (newton.py:978-996): GMRES on the fresh
+        coupled operator J_ff + B K over the free unknowns, preconditioned
+        by a stale dense LU of J_ff, to rtol.  Right-preconditioned
+        restarted GMRES (modified Gram-Schmidt Arnoldi, Givens rotations),
+        converged when the true residual |rhs - A x| <= rtol |rhs|; at most
+        maxiter cycles of restart steps.  Returns (dphi reduced-size or
+        None when it did not converge, inner steps)."""
+        t = L.torch()
+        LU, piv, _ = lu
+        fr = self._free_d
+        b = rhs[fr]
+        n = b.numel()
+        full = t.zeros(self.n_red, dtype=t.float64, device="cuda")
+
+        def A(v):
+            full.zero_()
+            full[fr] = v
+            return Aop.matvec(full)[fr]
+
+        def Minv(v):
+            return t.linalg.lu_solve(LU, piv, v.unsqueeze(1)).squeeze(1)
+
+        b_norm = float(t.linalg.vector_norm(b))
+        x = t.zeros(n, dtype=t.float64, device="cuda")
+        if b_norm == 0.0:
+            out = t.zeros(self.n_red, dtype=t.float64, device="cuda")
+            return out, 0
+        tol = rtol * b_norm
+        m = max(1, min(int(restart), n))
+        n_it = 0
+        converged = False
+        for _ in range(int(maxiter)):
+            r = b - A(x)
+            beta = float(t.linalg.vector_norm(r))
+            if beta <= tol:
+                converged = True
+                break
+            V = t.empty((m + 1, n), dtype=t.float64, device="cuda")
+            V[0] = r / beta
+            H = np.zeros((m + 1, m))
+            cs, sn = np.zeros(m), np.zeros(m)
+            g = np.zeros(m + 1)
+            g[0] = beta
+            k_used = 0
+            for k in range(m):
+                w = A(Minv(V[k]))
+                h = V[:k + 1] @ w                     # classical projection, then one
+                w = w - V[:k + 1].T @ h               # re-orthogonalisation pass
+                h2 = V[:k + 1] @ w
+                w = w - V[:k + 1].T @ h2
+                hk = (h + h2).cpu().numpy()
+                hn = float(t.linalg.vector_norm(w))
+                H[:k + 1, k] = hk
+                H[k + 1, k] = hn
+                for i in range(k):
+                    a_, b_ = H[i, k], H[i + 1, k]
+                    H[i, k] = cs[i] * a_ + sn[i] * b_
+                    H[i + 1, k] = -sn[i] * a_ + cs[i] * b_
+                den = float(np.hypot(H[k, k], H[k + 1, k]))
+                cs[k], sn[k] = (1.0, 0.0) if den == 0.0 else (H[k, k] / den, H[k + 1, k] / den)
+                H[k, k] = den
+                H[k + 1, k] = 0.0
+                g[k + 1] = -sn[k] * g[k]
+                g[k] = cs[k] * g[k]
+                n_it += 1
+                k_used = k + 1
+                if hn != 0.0:
+                    V[k + 1] = w / hn
+                if abs(g[k + 1]) <= tol or hn == 0.0:
+                    break
+            y = np.linalg.solve(np.triu(H[:k_used, :k_used]), g[:k_used])
+            yd = t.from_numpy(y).cuda()
+            x = x + Minv(V[:k_used].T @ yd)
+        else:
+            converged = float(t.linalg.vector_norm(b - A(x))) <= tol
+        if not converged:
+            return None, n_it
+        out = t.zeros(self.n_red, dtype=t.float64, device="cuda")
+        out[fr] = x
+        return out, n_it
+
     def picard_block(self) -> DeviceCSR:
         """T^T A(rho_tilde) T with the far-field mask: the AMG source
         (newton.py:1013-1022), rho_tilde of the last evaluation."""
@@ -371,7 +453,7 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
                          tol_gamma: float = 1e-8, ew_eta0: float = 1e-2, ew_gamma: float = 0.9,
                          ew_eta_max: float = 1e-2, amg_rebuild_every: int = 2,
                          precond: str = "amg", direct_refactor_every: int = 1,
-                         gmres_restart: int = 60, gmres_maxiter: int = 10,
+                         direct_reuse_rtol: float = 1e-8, gmres_restart: int = 60, gmres_maxiter: int = 10,
                          line_search: bool = True, rtol_seed: float = 1e-7,
                          tol_residual_loose: Optional[float] = None,
                          tol_residual_rel: Optional[float] = None, accept_on_stall: bool = False,
@@ -398,8 +480,8 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     if precond not in ("amg", "direct"):
         raise NotImplementedError(f"precond={precond!r}: the device driver solves with AMG-GMRES or a "
                                   "dense direct factorisation")
-    if precond == "direct" and direct_refactor_every != 1:
-        raise NotImplementedError("direct_refactor_every != 1 (lagged-LU GMRES) is not built")
+    if direct_refactor_every < 1:
+        raise ValueError(f"direct_refactor_every must be >= 1, got {direct_refactor_every}")
     ws = workspace
     if ws is None:
         ws = NewtonWorkspace(mesh_cut, wc, alpha_deg, u_inf, gamma_air, vortex_center,
@@ -456,6 +538,7 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     r_level_best = np.inf
     n_term3_last = 0
     n_refactor = 0
+    lu, lu_age = None, 0
 
     a = clock()
     R, F, state = ws.eval_residual(phi_f, gamma, **res_kw)
@@ -555,12 +638,22 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
         rhs = -R - BF
         if precond == "direct":
             # exact step: dense LU of J_ff and the Woodbury update for the
-            # rank-n_stations coupling B K (newton.py:966-1011)
-            b2 = clock()
-            lu = ws.dense_lu(Aop)
-            timings["precond"] += clock() - b2
-            n_refactor += 1
-            dphi = ws.direct_step(lu, K_elim, rhs)
+            # rank-n_stations coupling B K (newton.py:966-1011); with
+            # direct_refactor_every > 1 the steps in between run GMRES on
+            # the fresh operator with the stale LU as preconditioner and
+            # refactor when that GMRES does not converge
+            dphi = None
+            if lu is not None and lu_age < direct_refactor_every:
+                dphi, n_it = ws.lagged_step(lu, Aop, rhs, direct_reuse_rtol, gmres_restart, 2)
+                n_gmres_total += n_it
+            if dphi is None:
+                b2 = clock()
+                lu = ws.dense_lu(Aop)
+                lu_age = 0
+                timings["precond"] += clock() - b2
+                n_refactor += 1
+                dphi = ws.direct_step(lu, K_elim, rhs)
+            lu_age += 1
             eta_history.append(0.0)
         else:
             eta = _ew_forcing(r_norm, residual_history[-2] if it > 0 else None, eta_prev, ew_eta0, ew_gamma,
