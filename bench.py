@@ -687,12 +687,22 @@ def wall_timing(spec):
     t0 = time.perf_counter()
     wall_force_coefficients(m.nodes, m.elements, wf, phi, m_inf=0.8, smooth_passes=2)
     api_ms = (time.perf_counter() - t0) * 1e3
+    # the same call with the mesh as device tensors: found by identity and
+    # in-place version, no digest (the first call digests them once)
+    nodes_d, elements_d = torch.from_numpy(m.nodes).cuda(), torch.from_numpy(m.elements).cuda()
+    wall_force_coefficients(nodes_d, elements_d, wf, phi, m_inf=0.8, smooth_passes=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        wall_force_coefficients(nodes_d, elements_d, wf, phi, m_inf=0.8, smooth_passes=2)
+    api_t_ms = (time.perf_counter() - t0) * 1e3 / 10
     t0 = time.perf_counter()
     ref = O.wall_force_coefficients(m.nodes, m.elements, wf, phi.cpu().numpy(), m_inf=0.8, smooth_passes=2)
     cpu_s = time.perf_counter() - t0
     return {"mesh": spec, "n_wall_triangles": int(len(wf)), "ms_per_evaluation": round(ms, 4),
-            "ms_per_api_call": round(api_ms, 2),
-            "api_note": "the API call also looks the mesh handle up by a digest of nodes and elements",
+            "ms_per_api_call": round(api_ms, 2), "ms_per_api_call_tensors": round(api_t_ms, 3),
+            "api_note": "with writeable numpy arrays the call looks the mesh handle up by a digest of nodes "
+                        "and elements; with tensors (or read-only arrays) seen before, by identity",
             "first_call_s": round(setup_s, 3), "cpu_oracle_s": round(cpu_s, 3),
             "cl": r["cl"], "max_abs_cf_diff_vs_oracle": float(np.abs(r["cf"] - ref["cf"]).max())}
 
@@ -706,7 +716,7 @@ def batched_timing(spec, seed=0):
     batched Newton against sequential plain solves."""
     import torch
     from up3d_b200.mesh.kuhn import bump_channel, seeded_state
-    from up3d_b200.solve.batched import BatchedChannels, solve_newton_batched
+    from up3d_b200.solve.batched import BatchedChannels, CaseSet, solve_newton_batched
     from up3d_b200.solve.fused import FlowParams
     from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
     k_s, lo_s, hi_s, mlo_s, mhi_s = spec.split(":")
@@ -778,7 +788,7 @@ def batched_timing(spec, seed=0):
     for _ in range(2):
         res_b = solve_newton_batched(fresh(), machs)
     res_ng = solve_newton_batched(fresh(), machs, use_graphs=False)
-    seq_s, seq_ok = [], []
+    seq_s, seq_ok, seq_phi = [], [], []
     for c, m in enumerate(meshes):
         ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
         torch.cuda.synchronize()
@@ -787,6 +797,7 @@ def batched_timing(spec, seed=0):
         torch.cuda.synchronize()
         seq_s.append(time.perf_counter() - t0)
         seq_ok.append(bool(r["converged"]))
+        seq_phi.append(r["phi"].cpu())
     out["newton"] = {"batched_s": round(res_b["time_s"], 4), "sequential_s": round(float(sum(seq_s)), 4),
                      "batched_without_graphs_s": round(res_ng["time_s"], 4),
                      "batched_phases_s": {k: round(v, 4) for k, v in res_b["timings"].items()},
@@ -799,6 +810,23 @@ def batched_timing(spec, seed=0):
                      "batched_case_s": [None if np.isnan(v) else round(float(v), 4)
                                         for v in res_b["converged_s"]],
                      "sequential_case_s": [round(v, 4) for v in seq_s]}
+    # the mixed schedule: the small cases in one lockstep union, the large
+    # ones alone (built before the clock, like the sequential workspaces)
+    for below in (100_000, 300_000):
+        cs = CaseSet(meshes, machs, batch_below=below)
+        res_cs = cs.solve()
+        out["newton"][f"mixed_schedule_{below // 1000}k"] = {
+            "batch_below_tets": below, "n_batched": res_cs["n_batched"], "n_plain": res_cs["n_plain"],
+            "batched_tets": int(sum(meshes[c].n_tets for c in cs.small)),
+            "time_s": round(res_cs["time_s"], 4),
+            "batched_s": None if "batched_s" not in res_cs else round(res_cs["batched_s"], 4),
+            "sequential_s_same_cases": {"batched": round(float(sum(seq_s[c] for c in cs.small)), 4),
+                                        "plain": round(float(sum(seq_s[c] for c in cs.large)), 4)},
+            "speedup_vs_sequential": round(float(sum(seq_s)) / res_cs["time_s"], 3),
+            "converged": bool(res_cs["converged"].all()),
+            "max_dphi_vs_sequential": float(max(float((res_cs["phi"][c].cpu() - seq_phi[c]).abs().max())
+                                                for c in range(len(meshes))))}
+        del cs
     return out
 
 

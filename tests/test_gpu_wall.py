@@ -76,3 +76,29 @@ def test_unowned_wall_face_raises():
     bad = np.array([[0, 1, 2]], dtype=np.int64)   # not a face of any tet
     with pytest.raises(ValueError, match="owned"):
         wall_force_coefficients(m.nodes, m.elements, bad, m.freestream())
+
+
+def test_mesh_handle_lookup_by_identity_sees_in_place_changes():
+    """get_mesh finds the handle of tensors (and read-only arrays) it has
+    seen by identity; an in-place change of a tensor (its version counter)
+    or a writeable array (its digest) gives the changed mesh's handle."""
+    import torch
+    from up3d_b200.mesh.device import get_mesh
+    from up3d_b200.mesh.kuhn import bump_channel
+    m = bump_channel(6, 3, 3, amplitude=0.05, seed=0)
+    nodes_d = torch.from_numpy(m.nodes.copy()).cuda()
+    elements_d = torch.from_numpy(m.elements.copy()).cuda()
+    a = get_mesh(nodes_d, elements_d)
+    assert get_mesh(nodes_d, elements_d) is a
+    assert get_mesh(m.nodes, m.elements) is a            # same contents, by digest
+    nodes_d[0, 0] += 0.25
+    b = get_mesh(nodes_d, elements_d)
+    assert b is not a and np.allclose(b.nodes[0, 0], m.nodes[0, 0] + 0.25)
+    ro_n, ro_e = m.nodes.copy(), m.elements.copy()
+    ro_n.flags.writeable = False
+    ro_e.flags.writeable = False
+    assert get_mesh(ro_n, ro_e) is a and get_mesh(ro_n, ro_e) is a
+    w = m.nodes.copy()
+    assert get_mesh(w, m.elements) is a
+    w[1, 1] += 0.5
+    assert get_mesh(w, m.elements) is not a

@@ -1,7 +1,8 @@
 """Device-resident mesh handle (owner of an ``up3d_mesh``) and a device CSR.
 
 One handle serves every operator built on the same (nodes, elements): the
-handles are cached by content digest, so ``PicardOperator`` and
+handles are cached by content digest (skipped for arrays that cannot have
+changed since they were last seen), so ``PicardOperator`` and
 ``UpwindOperator`` on one mesh share a single device copy of the geometry,
 adjacency and pattern, and the per-mesh setup runs once.
 """
@@ -172,37 +173,73 @@ class DeviceMesh:
 
 _CACHE: "OrderedDict[tuple, DeviceMesh]" = OrderedDict()
 _CACHE_SIZE = 4
+# (identity key) -> (weak references to the caller's two arrays, content key):
+# arrays that cannot have changed since they were digested skip the digest
+_SEEN: "OrderedDict[tuple, tuple]" = OrderedDict()
 
 
 def _digest(nodes: np.ndarray, elements: np.ndarray) -> str:
-    h = hashlib.blake2b(digest_size=20)
+    h = hashlib.sha256()
     h.update(np.asarray(nodes.shape, dtype=np.int64).tobytes())
-    h.update(nodes.tobytes())
+    h.update(memoryview(nodes).cast("B"))
     h.update(np.asarray(elements.shape, dtype=np.int64).tobytes())
-    h.update(elements.tobytes())
+    h.update(memoryview(elements).cast("B"))
     return h.hexdigest()
 
 
+def _identity(x):
+    """A key under which x cannot have changed while it is alive: a torch
+    tensor's storage, shape and in-place version counter, or a read-only
+    numpy array's buffer; None for anything else (a writeable array)."""
+    if L.is_torch(x):
+        return ("t", id(x), x.data_ptr(), tuple(x.shape), tuple(x.stride()), str(x.dtype), str(x.device),
+                x._version)
+    if isinstance(x, np.ndarray) and not x.flags.writeable and x.base is None:
+        return ("n", id(x), x.ctypes.data, x.shape, x.strides, x.dtype.str)
+    return None
+
+
 def get_mesh(nodes, elements, device: int | None = None) -> DeviceMesh:
-    """Shared DeviceMesh for (nodes, elements) on `device` (cached)."""
+    """Shared DeviceMesh for (nodes, elements) on `device`, cached by a
+    digest of their contents.  Torch tensors (tracked by their in-place
+    version counter) and read-only numpy arrays that were seen before skip
+    the digest; writeable numpy arrays are digested on every call, since
+    they may have been changed in place."""
+    import weakref
     t = L.require_cuda()
-    nodes = _as_numpy(nodes, np.float64)
-    elements = _as_numpy(elements, np.int32)
     dev = t.cuda.current_device() if device is None else int(device)
-    key = (_digest(nodes, elements), dev)
+    ident = None
+    a, b = _identity(nodes), _identity(elements)
+    if a is not None and b is not None:
+        ident = (a, b, dev)
+        seen = _SEEN.get(ident)
+        if seen is not None and seen[0]() is nodes and seen[1]() is elements and seen[2] in _CACHE:
+            _CACHE.move_to_end(seen[2])
+            return _CACHE[seen[2]]
+    nodes_h = _as_numpy(nodes, np.float64)
+    elements_h = _as_numpy(elements, np.int32)
+    key = (_digest(nodes_h, elements_h), dev)
     m = _CACHE.get(key)
     if m is None:
-        m = DeviceMesh(nodes, elements, dev)
+        m = DeviceMesh(nodes_h, elements_h, dev)
         _CACHE[key] = m
         while len(_CACHE) > _CACHE_SIZE:
             _CACHE.popitem(last=False)
     else:
         _CACHE.move_to_end(key)
+    if ident is not None:
+        try:
+            _SEEN[ident] = (weakref.ref(nodes), weakref.ref(elements), key)
+            while len(_SEEN) > 4 * _CACHE_SIZE:
+                _SEEN.popitem(last=False)
+        except TypeError:   # an object without weak references: no shortcut
+            pass
     return m
 
 
 def clear_cache():
     _CACHE.clear()
+    _SEEN.clear()
 
 
 class DeviceCSR:

@@ -340,9 +340,10 @@ class NewtonWorkspace:
         """The lagged-LU reuse step (newton.py:978-996): GMRES on the fresh
         coupled operator J_ff + B K over the free unknowns, preconditioned
         by a stale dense LU of J_ff, to rtol.  Right-preconditioned
-        restarted GMRES (modified Gram-Schmidt Arnoldi, Givens rotations),
-        converged when the true residual |rhs - A x| <= rtol |rhs|; at most
-        maxiter cycles of restart steps.  Returns (dphi reduced-size or
+        restarted GMRES (classical Gram-Schmidt Arnoldi with one
+        re-orthogonalisation pass, Givens rotations), converged when the
+        true residual |rhs - A x| <= rtol |rhs|; at most maxiter cycles of
+        restart steps.  Returns (dphi reduced-size or
         None when it did not converge, inner steps)."""
         t = L.torch()
         LU, piv, _ = lu
