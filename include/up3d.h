@@ -707,14 +707,18 @@ int up3d_gmres_coupled(const up3d_coupled* coupled, const up3d_csr* J, const up3
 /* Mixed-precision GMRES with FP64 iterative refinement (the mixed form of
  * the Newton linear solve the reference does with spla.gmres,
  * solve/newton.py:1029-1040).  The outer loop forms r = b - A x with A's
- * FP64 values and stops at ||r|| <= max(rtol ||b||, atol) or after
- * refine_max corrections; each correction solves A d = r by restarted
- * GMRES in FP32 -- A's FP32 values `data32` (and `extra32` for `extra`),
- * FP32 vectors, M applied in FP32 (an FP32 AMG hierarchy keeps its
- * coarsest solve in FP64) -- to max(inner_rtol, tol / ||r||) relative, and
- * is added to x in FP64; once a correction fails to halve the true
- * residual, FP64 GMRES finishes the solve from the current iterate.
- * inner = total Arnoldi steps, outer = corrections.  Synchronous. */
+ * FP64 values and tests up3d_gmres's criterion: with M, the preconditioned
+ * residual ||M r|| <= ||M b|| min(1, max(rtol, atol / ||b||)) (M applied in
+ * FP32); without, ||r|| <= max(rtol ||b||, atol).  It stops there, after
+ * refine_max corrections, or once the corrections have used restart x
+ * maxiter Arnoldi steps (the cap of one up3d_gmres call).  Each correction
+ * solves A d = r by restarted GMRES in FP32 -- A's FP32 values `data32`
+ * (and `extra32` for `extra`), FP32 vectors, M applied in FP32 (an FP32 AMG
+ * hierarchy keeps its coarsest solve in FP64) -- to max(inner_rtol,
+ * tol / ||M r||) relative, and is added to x in FP64; once a correction
+ * fails to halve the tested residual, FP64 GMRES finishes the solve from
+ * the current iterate within the remaining steps.  inner = total Arnoldi
+ * steps, outer = corrections, resid = ||b - A x||.  Synchronous. */
 int up3d_gmres_ir(const up3d_csr* A, const up3d_csr* extra, const float* data32,
                   const float* extra32, const double* b, double* x, double rtol, double atol,
                   int restart, int maxiter, int refine_max, double inner_rtol, up3d_precond* M,

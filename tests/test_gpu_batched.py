@@ -127,3 +127,43 @@ def test_tuned_batch_picks_an_ordering_and_converges():
     assert all(v["ms"] > 0 for v in rep["candidates"].values())
     res = solve_newton_batched(batch, machs)
     assert res["converged"].all()
+
+
+def test_compacted_batch_matches_plain_solves():
+    """Compaction onto the unfinished cases (as soon as one case has
+    finished) carries their potentials and frozen selections over: the
+    same converged potentials as the plain solves."""
+    from up3d_b200.solve.batched import BatchedChannels, solve_newton_batched
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    meshes = _cases()
+    machs = [0.6, 0.5, 0.7]
+    batch = BatchedChannels(meshes)
+    res = solve_newton_batched(batch, machs, compact_fraction=1.0)
+    assert res["converged"].all(), res
+    assert res["n_compactions"] >= 1
+    phi = res["phi"].cpu().numpy()
+    for c, (m, M) in enumerate(zip(meshes, machs)):
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        r = solve_newton_transonic(ws, M, m_start=min(0.70, M))
+        a, b = batch.node_off[c], batch.node_off[c + 1]
+        assert np.abs(phi[a:b] - r["phi"].cpu().numpy()).max() < 1e-8
+
+
+def test_case_set_batches_the_small_cases_and_runs_the_rest_alone():
+    from up3d_b200.mesh.kuhn import bump_channel
+    from up3d_b200.solve.batched import CaseSet
+    from up3d_b200.solve.newton import ChannelWorkspace, solve_newton_transonic
+    meshes = _cases() + [bump_channel(24, 8, 6, amplitude=0.04, seed=4)]
+    machs = [0.6, 0.5, 0.7, 0.65]
+    cs = CaseSet(meshes, machs, batch_below=1000)
+    assert sorted(cs.small.tolist()) == [0, 2] and sorted(cs.large.tolist()) == [1, 3]
+    res = cs.solve()
+    assert res["converged"].all() and res["n_batched"] == 2 and res["n_plain"] == 2
+    assert np.all(np.isfinite(res["case_s"])) and res["time_s"] >= np.nanmax(res["case_s"]) - 1e-9
+    for c, (m, M) in enumerate(zip(meshes, machs)):
+        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+        r = solve_newton_transonic(ws, M, m_start=min(0.70, M))
+        assert np.abs(res["phi"][c].cpu().numpy() - r["phi"].cpu().numpy()).max() < 1e-8
+    # one small case alone is not batched
+    one = CaseSet(meshes[:2], machs[:2], batch_below=1000)
+    assert one.batch is None and len(one.large) == 2

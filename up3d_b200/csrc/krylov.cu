@@ -567,14 +567,19 @@ template int gmres_solve<double>(const Operator&, const double*, double*, double
 template int gmres_solve<float>(const Operator&, const float*, float*, double, double, int, int, up3d_precond*,
                                  int64_t*, double*, cudaStream_t);
 
-// Mixed-precision GMRES with FP64 iterative refinement: the outer loop forms
-// the true residual r = b - A x with the FP64 values and stops at
-// ||r|| <= max(rtol ||b||, atol); each inner solve is restarted GMRES on the
-// FP32 operator (data32, extra32) and FP32 vectors with the preconditioner
-// applied in FP32, to max(inner_rtol, tol / ||r||) relative, and its
-// correction is added to x in FP64.  A correction that fails to halve the
-// true residual hands the rest of the solve to FP64 GMRES.  Returns 0 when
-// converged.
+// Mixed-precision GMRES with FP64 iterative refinement.  The outer loop
+// forms the true residual r = b - A x with the FP64 values and tests the
+// criterion of gmres_solve: with a preconditioner, the preconditioned
+// residual |M r| <= |M b| min(1, max(rtol, atol / |b|)) (M applied in FP32
+// to r rounded to FP32), without one |r| <= max(rtol |b|, atol).  Each
+// correction solves A d = r by restarted GMRES on the FP32 operator (data32,
+// extra32) with FP32 vectors and M applied in FP32, to max(inner_rtol,
+// tol / |M r|) relative, and is added to x in FP64.  A correction that fails
+// to halve the tested residual hands the rest of the solve to FP64 GMRES
+// from the current iterate.  The Arnoldi steps of all corrections (and of
+// that FP64 finish) share one budget of restart x maxiter, the cap of one
+// gmres_solve call, so a solve that cannot meet its tolerance costs what
+// the FP64 solve would.  Returns 0 when converged; resid = |r|.
 int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, double atol, int restart,
                    int maxiter, int refine_max, double inner_rtol, up3d_precond* M, int64_t* inner, int64_t* outer,
                    double* resid, cudaStream_t s) {
@@ -590,40 +595,60 @@ int gmres_ir_solve(const Operator& op, const double* b, double* x, double rtol, 
     tmp.alloc(n);
     r32.alloc(n);
     d32.alloc(n);
+    restart = (int)std::max<int64_t>(1, std::min<int64_t>(restart, n));
+    const int64_t budget = (int64_t)restart * maxiter;
+    // |v| of an FP64 vector in the tested norm: preconditioned (through the
+    // FP32 copy r32, which the correction then uses as its right-hand side)
+    // or plain
+    auto tested_norm = [&](const double* v) -> double {
+        k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(v, r32.get(), n);
+        UP3D_CHECK_LAUNCH();
+        if (!M) return bl.nrm2(v, n);
+        precond_apply(M, r32.get(), d32.get(), n, s);
+        return bl.nrm2(d32.get(), n);
+    };
     const double bnrm = bl.nrm2(b, n);
-    const double tol = eff_atol(atol, rtol, bnrm);
+    const double bt = tested_norm(b);
+    const double tol = M ? bt * std::min(1.0, eff_atol(atol, rtol, bnrm) / std::max(bnrm, 1e-300))
+                         : eff_atol(atol, rtol, bnrm);
     int64_t tot_inner = 0, it = 0;
-    double rn = 0.0, rn_prev = 0.0;
+    double rn = 0.0, rn_prev = 0.0, rtrue = 0.0;
     for (;; ++it) {
         op.apply(x, tmp.get(), s);
         k_sub<double><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
         UP3D_CHECK_LAUNCH();
-        rn = bl.nrm2(r.get(), n);
-        if (rn <= tol || !std::isfinite(rn) || it >= refine_max) break;
+        rn = tested_norm(r.get());
+        rtrue = M ? bl.nrm2(r.get(), n) : rn;
+        if (rn <= tol || !std::isfinite(rn) || it >= refine_max || tot_inner >= budget) break;
+        const int cycles_left = (int)std::max<int64_t>(1, (budget - tot_inner + restart - 1) / restart);
         if (it > 0 && rn > 0.5 * rn_prev) {
             // the FP32 corrections stopped paying (a system too ill-conditioned
             // for FP32): finish with FP64 GMRES from the current iterate
             int64_t inn = 0;
-            gmres_solve<double>(op, b, x, rtol, atol, restart, maxiter, M, &inn, &rn, s);
+            double r64 = 0.0;
+            gmres_solve<double>(op, b, x, rtol, atol, restart, cycles_left, M, &inn, &r64, s);
             tot_inner += inn;
             ++it;
+            op.apply(x, tmp.get(), s);
+            k_sub<double><<<grid_for(n, 256), 256, 0, s>>>(b, tmp.get(), r.get(), n);
+            UP3D_CHECK_LAUNCH();
+            rn = tested_norm(r.get());
+            rtrue = M ? bl.nrm2(r.get(), n) : rn;
             break;
         }
         rn_prev = rn;
-        k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(r.get(), r32.get(), n);
-        UP3D_CHECK_LAUNCH();
         UP3D_CUDA(cudaMemsetAsync(d32.get(), 0, sizeof(float) * n, s));
         int64_t inn = 0;
         double ires = 0.0;
-        gmres_solve<float>(op, r32.get(), d32.get(), std::max(inner_rtol, tol / rn), 0.0, restart, maxiter, M, &inn,
-                           &ires, s);
+        gmres_solve<float>(op, r32.get(), d32.get(), std::max(inner_rtol, tol / rn), 0.0, restart, cycles_left, M,
+                           &inn, &ires, s);
         tot_inner += inn;
         k_add_f32<<<grid_for(n, 256), 256, 0, s>>>(x, d32.get(), n);
         UP3D_CHECK_LAUNCH();
     }
     if (inner) *inner = tot_inner;
     if (outer) *outer = it;
-    if (resid) *resid = rn;
+    if (resid) *resid = rtrue;
     return rn <= tol ? 0 : maxiter;
 }
 

@@ -20,13 +20,18 @@ state once its residual is below ``freeze_tol`` (the plain driver's frozen
 finish; the other cases stay live in the same launches) and is accepted on
 frozen convergence -- the plain driver's refresh / revert of the frozen state
 is not repeated here.
+
+Lockstep pays for small cases, whose solve time is launches and host
+synchronisations, and costs for large ones, which fill the GPU alone and
+would be tied to the slowest case's iteration count.  ``CaseSet`` therefore
+puts the cases below a size into one union and runs the others one by one.
 """
 
 from __future__ import annotations
 
 import ctypes
 import time
-from typing import Dict, List, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -213,7 +218,7 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
                          dm: float = 0.05, tol_residual: float = 1e-10, n_newton_max: int = 30,
                          n_picard_seed: int = 5, amg_rebuild_every: int = 2, gmres_restart: int = 60,
                          gmres_maxiter: int = 10, freeze_tol: float = 1e-6, freeze_refresh_max: int = 2,
-                         use_graphs: bool = True, compact_fraction: float = 0.5,
+                         use_graphs: bool = True, compact_fraction: float = 0.0,
                          verbose: bool = False) -> Dict[str, object]:
     """Lockstep Newton of every case (module docstring); returns the union
     potential, per-case convergence, iteration counts and timings.  With
@@ -226,7 +231,9 @@ def solve_newton_batched(batch: BatchedChannels, machs: Sequence[float], m_start
     their target Mach, or failed), the solve continues on a new union of
     those cases alone -- their potentials, frozen selections and per-case
     state carried over, the AMG hierarchy rebuilt -- and the finished
-    cases' potentials are kept aside (0 disables it)."""
+    cases' potentials are kept aside (0, the default, disables it: on the
+    48-case set of 27 M tets rebuilding the union cost more than the
+    smaller union saved)."""
     t = L.require_cuda()
     batch0 = batch
     ws = batch.ws
@@ -453,3 +460,74 @@ def _compacted(batch: BatchedChannels, phi, keep):
             new.up_fz[na:nb] = batch.up_fz[a:b] - a + na
             new.br_fz[na:nb] = batch.br_fz[a:b]
     return new, phi_new
+
+
+class CaseSet:
+    """Independent channel cases solved on one device, each where it runs
+    fastest: the cases below ``batch_below`` tets share one lockstep union
+    (``BatchedChannels``: their launches, V-cycles and host synchronisations
+    are shared, which is where a small case spends its time), the larger
+    cases run one by one through the plain driver (a case of that size
+    fills the GPU alone, and lockstep would only tie it to the slowest
+    case's iteration count).  Everything the solves reuse -- the union, its
+    launch shapes, the per-case workspaces -- is built here, so ``solve``
+    times the solves alone."""
+
+    def __init__(self, meshes: Sequence[BumpMesh], machs: Sequence[float], batch_below: int = 300_000,
+                 u_inf: float = 1.0, tune_orderings: Sequence[str] = ("given",)):
+        L.require_cuda()
+        self.meshes = list(meshes)
+        self.machs = np.asarray(machs, dtype=np.float64)
+        if len(self.machs) != len(self.meshes):
+            raise ValueError(f"{len(self.meshes)} meshes but {len(self.machs)} Mach numbers")
+        tets = np.array([m.n_tets for m in self.meshes], dtype=np.int64)
+        small = np.nonzero(tets < batch_below)[0]
+        if len(small) < 2:
+            small = np.zeros(0, dtype=np.int64)
+        self.small = small
+        self.large = np.setdiff1d(np.arange(len(self.meshes)), small)
+        self.batch = None
+        self.batch_tuning = None
+        if len(small):
+            self.batch = BatchedChannels.tuned([self.meshes[c] for c in small], self.machs[small], u_inf=u_inf,
+                                               orderings=tune_orderings)
+            self.batch_tuning = self.batch.ws.ev.mesh.tuning()
+        self.wss = {int(c): ChannelWorkspace(self.meshes[c].nodes, self.meshes[c].elements,
+                                             self.meshes[c].dirichlet_nodes, u_inf=u_inf) for c in self.large}
+
+    def solve(self, m_start: float = 0.70, dm: float = 0.05, tol_residual: float = 1e-10,
+              batched_kw: Optional[dict] = None, plain_kw: Optional[dict] = None) -> Dict[str, object]:
+        """Every case to |R_free|_inf < tol_residual at its Mach number:
+        the union first, then the large cases.  Returns per-case potentials
+        (case numbering, device), convergence, Newton steps and the time at
+        which each case finished (seconds from the start), and the wall
+        time with the device synchronised."""
+        t = L.require_cuda()
+        from .newton import solve_newton_transonic
+        C = len(self.meshes)
+        out = {"phi": [None] * C, "converged": np.zeros(C, dtype=bool), "n_newton": np.zeros(C, dtype=np.int64),
+               "case_s": np.full(C, np.nan), "n_batched": int(len(self.small)), "n_plain": int(len(self.large))}
+        t.cuda.synchronize()
+        t0 = time.perf_counter()
+        if self.batch is not None:
+            res = solve_newton_batched(self.batch, self.machs[self.small], m_start=m_start, dm=dm,
+                                       tol_residual=tol_residual, compact_fraction=0.0, **(batched_kw or {}))
+            for k, c in enumerate(self.small):
+                out["phi"][c] = self.batch.case_phi(res["phi"], k)
+                out["converged"][c] = bool(res["converged"][k])
+                out["n_newton"][c] = int(res["n_newton"][k])
+                out["case_s"][c] = res["converged_s"][k]
+            out["batched_timings"] = res["timings"]
+            out["batched_s"] = res["time_s"]
+        for c in self.large:
+            M = float(self.machs[c])
+            r = solve_newton_transonic(self.wss[int(c)], M, m_start=min(m_start, M), dm=dm,
+                                       tol_residual=tol_residual, **(plain_kw or {}))
+            out["phi"][c] = r["phi"]
+            out["converged"][c] = bool(r["converged"])
+            out["n_newton"][c] = int(sum(lv[1] for lv in r["level_history"]))
+            t.cuda.synchronize()
+            out["case_s"][c] = time.perf_counter() - t0
+        t.cuda.synchronize()
+        out["time_s"] = time.perf_counter() - t0
+        return out

@@ -259,8 +259,9 @@ def solve_newton(ws: ChannelWorkspace, flow: FlowParams, phi_init=None, n_picard
         a = clock()
         rhs = -Rf
         if precision == "mixed":
-            # FP32 Jacobian values and FP32 AMG inside FP64-refined GMRES(50)
-            dphi, n_it, n_ref, info = solve_gmres_mixed(Jf, rhs, M=M_pre, rtol=eta, restart=50,
+            # FP32 Jacobian values and FP32 AMG inside FP64-refined GMRES,
+            # the FP64 solve's restart, criterion and step cap
+            dphi, n_it, n_ref, info = solve_gmres_mixed(Jf, rhs, M=M_pre, rtol=eta, restart=gmres_restart,
                                                         maxiter=gmres_maxiter, refine_max=10,
                                                         inner_rtol=1e-5)
             n_refine_total += n_ref
