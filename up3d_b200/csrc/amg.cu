@@ -32,6 +32,7 @@
 #include <numeric>
 #include <vector>
 
+#include "csr_rows.cuh"
 #include "internal.cuh"
 #include "krylov.cuh"
 
@@ -564,92 +565,57 @@ __global__ void k_jacobi_first(const T* __restrict__ dinv, const T* __restrict__
     GRID_STRIDE(i, n) x[i] = w * dinv[i] * b[i];
 }
 
-// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x); TPR lanes
-// per row, chosen per level from its mean row length.  The finest operator
-// is the embedded one (identity rows, no constrained columns): no mask.
-template <class T, bool RESID, int TPR>
-__global__ void __launch_bounds__(256)
+// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x); one warp
+// per 32 rows (csr_rows.cuh).  The finest operator is the embedded one
+// (identity rows, no constrained columns): no mask.
+template <class T, bool RESID>
+__global__ void __launch_bounds__(CSR_ROWS_BLOCK)
     k_jacobi_sweep(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
                    const T* __restrict__ Ax, const T* __restrict__ dinv, const T* __restrict__ b,
                    const T* __restrict__ x, T* __restrict__ out, T w) {
-    constexpr int RPW = 32 / TPR;
-    const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
+    __shared__ T sh[CSR_ROWS_BLOCK / 32][CSR_ROWS_CHUNK];
+    T* my = sh[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * RPW; base < n; base += n_warps * RPW) {
-        const int64_t r = base + group;
-        T acc = T(0);
-        if (r < n)
-            for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) acc += Ax[k] * x[Ai[k]];
-#pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
-        if (sub == 0 && r < n) {
+    for (int64_t r0 = warp * 32; r0 < n; r0 += n_warps * 32) {
+        const T acc = warp_row_sum<T>(Ap, r0, n, my, [&](int32_t k) { return Ax[k] * x[Ai[k]]; });
+        const int64_t r = r0 + lane;
+        if (r < n) {
             const T res = b[r] - acc;
             out[r] = RESID ? res : x[r] + w * dinv[r] * res;
         }
     }
 }
 
-// y (+)= A x, rectangular (restriction / prolongation), TPR lanes per row
-template <class T, bool ADD, int TPR>
-__global__ void __launch_bounds__(256)
+// y (+)= A x, rectangular (restriction / prolongation), one warp per 32 rows
+template <class T, bool ADD>
+__global__ void __launch_bounds__(CSR_ROWS_BLOCK)
     k_spmv_rect(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai, const T* __restrict__ Ax,
                 const T* __restrict__ x, T* __restrict__ y) {
-    constexpr int RPW = 32 / TPR;
-    const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
+    __shared__ T sh[CSR_ROWS_BLOCK / 32][CSR_ROWS_CHUNK];
+    T* my = sh[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * RPW; base < n; base += n_warps * RPW) {
-        const int64_t r = base + group;
-        T acc = T(0);
-        if (r < n)
-            for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) acc += Ax[k] * x[Ai[k]];
-#pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
-        if (sub == 0 && r < n) y[r] = ADD ? y[r] + acc : acc;
+    for (int64_t r0 = warp * 32; r0 < n; r0 += n_warps * 32) {
+        const T acc = warp_row_sum<T>(Ap, r0, n, my, [&](int32_t k) { return Ax[k] * x[Ai[k]]; });
+        const int64_t r = r0 + lane;
+        if (r < n) y[r] = ADD ? y[r] + acc : acc;
     }
 }
-
-// Lanes per row from the mean row length (thresholds tuned on B200).
-#ifndef UP3D_AMG_T4
-#define UP3D_AMG_T4 16
-#endif
-#ifndef UP3D_AMG_T8
-#define UP3D_AMG_T8 24
-#endif
-#ifndef UP3D_AMG_T16
-#define UP3D_AMG_T16 96
-#endif
-inline int lanes_per_row(int64_t nnz, int64_t n) {
-    const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
-    return avg <= UP3D_AMG_T4 ? 4 : avg <= UP3D_AMG_T8 ? 8 : avg <= UP3D_AMG_T16 ? 16 : 32;
-}
-inline unsigned rows_grid(int64_t n, int tpr) { return grid_for(n, 256 / tpr, (int64_t)148 * 64); }
 
 template <class T, bool RESID>
-void launch_sweep(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* dinv,
+void launch_sweep(int64_t n, int64_t, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* dinv,
                   const T* b, const T* x, T* out, T w, cudaStream_t s) {
-    switch (lanes_per_row(nnz, n)) {
-        case 4: k_jacobi_sweep<T, RESID, 4><<<rows_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
-        case 8: k_jacobi_sweep<T, RESID, 8><<<rows_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
-        case 16:
-            k_jacobi_sweep<T, RESID, 16><<<rows_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
-            break;
-        default:
-            k_jacobi_sweep<T, RESID, 32><<<rows_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
-    }
+    k_jacobi_sweep<T, RESID><<<csr_rows_grid(n), CSR_ROWS_BLOCK, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
     UP3D_CHECK_LAUNCH();
 }
 
 template <class T, bool ADD>
-void launch_rect(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* x, T* y,
+void launch_rect(int64_t n, int64_t, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* x, T* y,
                  cudaStream_t s) {
-    switch (lanes_per_row(nnz, n)) {
-        case 4: k_spmv_rect<T, ADD, 4><<<rows_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
-        case 8: k_spmv_rect<T, ADD, 8><<<rows_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
-        case 16: k_spmv_rect<T, ADD, 16><<<rows_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
-        default: k_spmv_rect<T, ADD, 32><<<rows_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, x, y);
-    }
+    k_spmv_rect<T, ADD><<<csr_rows_grid(n), CSR_ROWS_BLOCK, 0, s>>>(n, Ap, Ai, Ax, x, y);
     UP3D_CHECK_LAUNCH();
 }
 
