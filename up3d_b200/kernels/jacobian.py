@@ -31,9 +31,12 @@ class PicardOperator:
         R = op.assemble_residual(phi, rho)
     """
 
-    def __init__(self, nodes, elements):
+    def __init__(self, nodes, elements, *, mesh=None):
+        """`mesh` (keyword only, not in the reference's signature): a
+        DeviceMesh of these nodes and elements to work on instead of the
+        shared handle looked up from the arrays."""
         t = L.require_cuda()
-        self._mesh = get_mesh(nodes, elements)
+        self._mesh = mesh if mesh is not None else get_mesh(nodes, elements)
         m = self._mesh
         self.n_nodes = m.n_nodes
         self.n_tets = m.n_tets

@@ -59,9 +59,11 @@ class UpwindOperator:
 
     def __init__(self, nodes, elements, weighted: bool = False, mode: str = "kernel",
                  p_weight: float = 3.0, reach_frac: float = 1.0, reach_gain_max: float = 4.0,
-                 nbr_depth: int = 3, sigma_s_frac: float = 0.35, sigma_p_frac: float = 0.35):
+                 nbr_depth: int = 3, sigma_s_frac: float = 0.35, sigma_p_frac: float = 0.35, *, mesh=None):
+        # mesh (keyword only, not in the reference's signature): a DeviceMesh
+        # of these nodes and elements instead of the shared handle
         t = L.require_cuda()
-        self._mesh = get_mesh(nodes, elements)
+        self._mesh = mesh if mesh is not None else get_mesh(nodes, elements)
         self._host = not L.is_torch(nodes)
         self.weighted = bool(weighted)
         self.mode = mode

@@ -115,7 +115,7 @@ class NewtonWorkspace:
         self.mesh = get_mesh(nodes, mesh_cut.elements)
         self.ev = ResidualJacobian(self.mesh)
         from ..kernels.jacobian import PicardOperator
-        self.op = PicardOperator(t.as_tensor(nodes), t.as_tensor(np.asarray(self.mesh.elements)))
+        self.op = PicardOperator(t.as_tensor(nodes), t.as_tensor(np.asarray(self.mesh.elements)), mesh=self.mesh)
         self.external_rhs = None
         if external_rhs is not None:
             b = np.asarray(external_rhs, dtype=np.float64)
@@ -439,7 +439,7 @@ class NewtonWorkspace:
         rho = density_field(q2l, fl.m_inf, fl.gamma)
         if not hasattr(self, "_upw"):
             self._upw = UpwindOperator(t.as_tensor(np.asarray(self.mesh.nodes)),
-                                       t.as_tensor(np.asarray(self.mesh.elements)))
+                                       t.as_tensor(np.asarray(self.mesh.elements)), mesh=self.mesh)
         up, br = self._upw.freeze_upwind_state(grad, q2l, rho, fl.m_inf, fl.upwind_c, fl.m_crit,
                                                fl.gamma, fl.rho_floor)
         return up.clone(), br.clone()
@@ -891,7 +891,7 @@ def solve_subsonic_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u
                                weighted=True, mode=upwind_mode, p_weight=upwind_p_weight,
                                reach_frac=upwind_reach_frac, reach_gain_max=upwind_reach_gain_max,
                                nbr_depth=upwind_nbr_depth, sigma_s_frac=upwind_sigma_s_frac,
-                               sigma_p_frac=upwind_sigma_p_frac)
+                               sigma_p_frac=upwind_sigma_p_frac, mesh=ws.mesh)
 
     def evaluate(phi_cut):
         """(rho~, monitors, R) at phi_cut: the fused evaluation (walk

@@ -65,7 +65,7 @@ class ChannelWorkspace:
         self.mesh = mesh if mesh is not None else get_mesh(nodes, elements)
         from ..kernels.jacobian import PicardOperator
         self.op = PicardOperator(t.as_tensor(np.asarray(self.mesh.nodes)),
-                                 t.as_tensor(np.asarray(self.mesh.elements)))
+                                 t.as_tensor(np.asarray(self.mesh.elements)), mesh=self.mesh)
         self.ev = ResidualJacobian(self.mesh)
         n = self.mesh.n_nodes
         self.u_inf = float(u_inf)
@@ -103,7 +103,7 @@ class ChannelWorkspace:
         rho = density_field(q2l, flow.m_inf, flow.gamma)
         if not hasattr(self, "_upw"):
             self._upw = UpwindOperator(t.as_tensor(np.asarray(self.mesh.nodes)),
-                                       t.as_tensor(np.asarray(self.mesh.elements)))
+                                       t.as_tensor(np.asarray(self.mesh.elements)), mesh=self.mesh)
         up, br = self._upw.freeze_upwind_state(grad, q2l, rho, flow.m_inf, flow.upwind_c,
                                                flow.m_crit, flow.gamma, flow.rho_floor)
         return up.clone(), br.clone()
