@@ -72,10 +72,11 @@ def parse():
     p.add_argument("--naca", default="1", help="NACA0012 2.5D timings ('' to skip)")
     p.add_argument("--newton", default="200x60x50:0.08:0.70",
                    help="mesh:bump:Mach of the time-to-1e-10 Newton solves ('' to skip)")
-    p.add_argument("--c4", default="",
-                   help="mesh:bump:Mach of a one-run FP64 / mixed Newton comparison on the large mesh "
-                        "(the mixed-precision configuration is 320x96x80:0.05, below its choking Mach)")
-    p.add_argument("--parity", type=int, default=1,
+    p.add_argument("--c4", default="320x96x80:0.05:0.75:0.70:0.025",
+                   help="mesh:bump:Mach[:m_start[:dm]] of a one-run FP64 / mixed Newton comparison on the "
+                        "large mesh (14.7 M tets, bump 0.05: M0.75 is below its choking Mach 0.7685) "
+                        "('' to skip)")
+    p.add_argument("--parity", type=int, default=2,
                    help="1: compare the timed states with the oracle after timing; 2: also the pocket states; "
                         "0: skip")
     p.add_argument("--linear", type=int, default=1,
@@ -1143,18 +1144,21 @@ def run_ours(args):
                   "n_term3_extra": [int(m["n_term3_extra"]) for m in p_mon],
                   "nu_max": [float(m["nu_max"]) for m in p_mon]}
 
-    newton = newton_timing(args.newton) if args.newton else None
-    c4 = newton_timing(args.c4, reps=1) if args.c4 else None
-    adjoint = adjoint_timing(args.adjoint) if args.adjoint else None
-    batched = batched_timing(args.batched) if args.batched else None
-    weighted = weighted_timing(args.weighted) if args.weighted else None
-    wake = wake_timing(args.wake) if args.wake else None
-    wall = wall_timing(args.wall) if args.wall else None
-    lifting = lifting_timing(args.lifting) if args.lifting else None
-    naca = naca_timing() if args.naca else None
+    # the solver-level timings run on one GPU only: a scaling run (N > 1)
+    # measures the replicated step alone
+    solo = world == 1
+    newton = newton_timing(args.newton) if args.newton and solo else None
+    c4 = newton_timing(args.c4, reps=1) if args.c4 and solo else None
+    adjoint = adjoint_timing(args.adjoint) if args.adjoint and solo else None
+    batched = batched_timing(args.batched) if args.batched and solo else None
+    weighted = weighted_timing(args.weighted) if args.weighted and solo else None
+    wake = wake_timing(args.wake) if args.wake and solo else None
+    wall = wall_timing(args.wall) if args.wall and solo else None
+    lifting = lifting_timing(args.lifting) if args.lifting and solo else None
+    naca = naca_timing() if args.naca and solo else None
 
-    parity = bench_parity(mesh, order, ev, flow, d_phis, phis, args.parity >= 2) if args.parity else None
-    linear = linear_timing(ev, dmesh, mesh, order, d_phis[0], flow) if args.linear else None
+    parity = bench_parity(mesh, order, ev, flow, d_phis, phis, args.parity >= 2) if args.parity and solo else None
+    linear = linear_timing(ev, dmesh, mesh, order, d_phis[0], flow) if args.linear and solo else None
 
     ms, e2e_ms, sus_ms = max_over_ranks([ms, e2e_ms, sus_ms], device="cuda")
     value = dmesh.n_tets * args.steps * world / (ms * 1e-3) / 1e6
