@@ -565,57 +565,90 @@ __global__ void k_jacobi_first(const T* __restrict__ dinv, const T* __restrict__
     GRID_STRIDE(i, n) x[i] = w * dinv[i] * b[i];
 }
 
-// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x); one warp
-// per 32 rows (csr_rows.cuh).  The finest operator is the embedded one
-// (identity rows, no constrained columns): no mask.
-template <class T, bool RESID>
-__global__ void __launch_bounds__(CSR_ROWS_BLOCK)
-    k_jacobi_sweep(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
-                   const T* __restrict__ Ax, const T* __restrict__ dinv, const T* __restrict__ b,
-                   const T* __restrict__ x, T* __restrict__ out, T w) {
-    __shared__ T sh[CSR_ROWS_BLOCK / 32][CSR_ROWS_CHUNK];
-    T* my = sh[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
+// Row loop shared by the CSR kernels below: TPR = 0 is one warp per 32
+// rows (csr_rows.cuh warp_row_sum), else TPR lanes per row; epi(r, acc)
+// writes row r (called once per row, by one lane).
+template <class T, int TPR, class Prod, class Epi>
+__device__ __forceinline__ void csr_rows_loop(int64_t n, const int32_t* __restrict__ Ap, T* sh, Prod prod, Epi epi) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r0 = warp * 32; r0 < n; r0 += n_warps * 32) {
-        const T acc = warp_row_sum<T>(Ap, r0, n, my, [&](int32_t k) { return Ax[k] * x[Ai[k]]; });
-        const int64_t r = r0 + lane;
-        if (r < n) {
-            const T res = b[r] - acc;
-            out[r] = RESID ? res : x[r] + w * dinv[r] * res;
+    if constexpr (TPR == 0) {
+        const int lane = threadIdx.x & 31;
+        for (int64_t r0 = warp * 32; r0 < n; r0 += n_warps * 32) {   // warp-uniform
+            const T acc = warp_row_sum<T>(Ap, r0, n, sh, prod);
+            if (r0 + lane < n) epi(r0 + lane, acc);
+        }
+    } else {
+        constexpr int RPW = 32 / TPR;
+        const int sub = threadIdx.x % TPR, group = (threadIdx.x & 31) / TPR;
+        for (int64_t base = warp * RPW; base < n; base += n_warps * RPW) {   // warp-uniform
+            const int64_t r = base + group;
+            const T acc = lanes_row_sum<T, TPR>(Ap, r, n, prod);
+            if (sub == 0 && r < n) epi(r, acc);
         }
     }
 }
 
-// y (+)= A x, rectangular (restriction / prolongation), one warp per 32 rows
-template <class T, bool ADD>
-__global__ void __launch_bounds__(CSR_ROWS_BLOCK)
+// out = x + w D^-1 (b - A x)   (or, with RESID, out = b - A x).  The finest
+// operator is the embedded one (identity rows, no constrained columns): no
+// mask.
+template <class T, bool RESID, int TPR>
+__global__ void __launch_bounds__(256)
+    k_jacobi_sweep(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai,
+                   const T* __restrict__ Ax, const T* __restrict__ dinv, const T* __restrict__ b,
+                   const T* __restrict__ x, T* __restrict__ out, T w) {
+    __shared__ T sh[TPR == 0 ? 256 / 32 : 1][TPR == 0 ? CSR_ROWS_CHUNK : 1];
+    csr_rows_loop<T, TPR>(
+        n, Ap, sh[TPR == 0 ? threadIdx.x >> 5 : 0], [&](int32_t k) { return Ax[k] * x[Ai[k]]; },
+        [&](int64_t r, T acc) {
+            const T res = b[r] - acc;
+            out[r] = RESID ? res : x[r] + w * dinv[r] * res;
+        });
+}
+
+// y (+)= A x, rectangular (restriction / prolongation)
+template <class T, bool ADD, int TPR>
+__global__ void __launch_bounds__(256)
     k_spmv_rect(int64_t n, const int32_t* __restrict__ Ap, const int32_t* __restrict__ Ai, const T* __restrict__ Ax,
                 const T* __restrict__ x, T* __restrict__ y) {
-    __shared__ T sh[CSR_ROWS_BLOCK / 32][CSR_ROWS_CHUNK];
-    T* my = sh[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r0 = warp * 32; r0 < n; r0 += n_warps * 32) {
-        const T acc = warp_row_sum<T>(Ap, r0, n, my, [&](int32_t k) { return Ax[k] * x[Ai[k]]; });
-        const int64_t r = r0 + lane;
-        if (r < n) y[r] = ADD ? y[r] + acc : acc;
-    }
+    __shared__ T sh[TPR == 0 ? 256 / 32 : 1][TPR == 0 ? CSR_ROWS_CHUNK : 1];
+    csr_rows_loop<T, TPR>(
+        n, Ap, sh[TPR == 0 ? threadIdx.x >> 5 : 0], [&](int32_t k) { return Ax[k] * x[Ai[k]]; },
+        [&](int64_t r, T acc) { y[r] = ADD ? y[r] + acc : acc; });
 }
 
 template <class T, bool RESID>
-void launch_sweep(int64_t n, int64_t, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* dinv,
+void launch_sweep(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* dinv,
                   const T* b, const T* x, T* out, T w, cudaStream_t s) {
-    k_jacobi_sweep<T, RESID><<<csr_rows_grid(n), CSR_ROWS_BLOCK, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+    if (use_warp_rows(n, nnz)) {
+        k_jacobi_sweep<T, RESID, 0><<<csr_rows_grid(n), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+    } else {
+        switch (lanes_per_row(nnz, n)) {
+            case 4: k_jacobi_sweep<T, RESID, 4><<<lanes_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
+            case 8: k_jacobi_sweep<T, RESID, 8><<<lanes_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w); break;
+            case 16:
+                k_jacobi_sweep<T, RESID, 16><<<lanes_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+                break;
+            default:
+                k_jacobi_sweep<T, RESID, 32><<<lanes_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, dinv, b, x, out, w);
+        }
+    }
     UP3D_CHECK_LAUNCH();
 }
 
 template <class T, bool ADD>
-void launch_rect(int64_t n, int64_t, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* x, T* y,
+void launch_rect(int64_t n, int64_t nnz, const int32_t* Ap, const int32_t* Ai, const T* Ax, const T* x, T* y,
                  cudaStream_t s) {
-    k_spmv_rect<T, ADD><<<csr_rows_grid(n), CSR_ROWS_BLOCK, 0, s>>>(n, Ap, Ai, Ax, x, y);
+    if (use_warp_rows(n, nnz)) {
+        k_spmv_rect<T, ADD, 0><<<csr_rows_grid(n), 256, 0, s>>>(n, Ap, Ai, Ax, x, y);
+    } else {
+        switch (lanes_per_row(nnz, n)) {
+            case 4: k_spmv_rect<T, ADD, 4><<<lanes_grid(n, 4), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+            case 8: k_spmv_rect<T, ADD, 8><<<lanes_grid(n, 8), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+            case 16: k_spmv_rect<T, ADD, 16><<<lanes_grid(n, 16), 256, 0, s>>>(n, Ap, Ai, Ax, x, y); break;
+            default: k_spmv_rect<T, ADD, 32><<<lanes_grid(n, 32), 256, 0, s>>>(n, Ap, Ai, Ax, x, y);
+        }
+    }
     UP3D_CHECK_LAUNCH();
 }
 

@@ -50,6 +50,35 @@ __device__ __forceinline__ T warp_row_sum(const int32_t* __restrict__ Ap, int64_
     return acc;
 }
 
+// Sum over row r of prod(k) by TPR lanes striding the row's entries,
+// reduced by a fixed shuffle tree; every lane of the warp must call (rows
+// past n contribute 0).  For short matrices (few rows: the warp-rows form
+// would leave most SMs idle) and long rows (AMG coarse levels, restriction).
+template <class T, int TPR, class Prod>
+__device__ __forceinline__ T lanes_row_sum(const int32_t* __restrict__ Ap, int64_t r, int64_t n, Prod prod) {
+    const int sub = threadIdx.x % TPR;
+    T acc = T(0);
+    if (r < n)
+        for (int32_t k = Ap[r] + sub; k < Ap[r + 1]; k += TPR) acc += prod(k);
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+    return acc;
+}
+
+// The warp-rows form pays once a matrix has rows enough to give every SM
+// a few warps of 32 rows and its rows are short (measured on B200: the
+// 625 k-row P1 Jacobian 0.045 -> 0.034 ms; a 24 k-row AMG level with 26
+// entries per row 2x slower than 16 lanes per row).
+constexpr int64_t CSR_ROWS_MIN_ROWS = 148 * 16 * 32;
+inline bool use_warp_rows(int64_t n, int64_t nnz) { return n >= CSR_ROWS_MIN_ROWS && nnz <= 24 * n; }
+
+// Lanes per row from the mean row length (thresholds tuned on B200).
+inline int lanes_per_row(int64_t nnz, int64_t n) {
+    const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
+    return avg <= 16 ? 4 : avg <= 24 ? 8 : avg <= 96 ? 16 : 32;
+}
+inline unsigned lanes_grid(int64_t n, int tpr) { return grid_for(n, 256 / tpr, (int64_t)148 * 64); }
+
 // Blocks for n rows at 32 rows per warp, capped at a persistent wave.
 inline unsigned csr_rows_grid(int64_t n) {
     const int64_t groups = (n + 31) / 32;

@@ -28,10 +28,11 @@ constexpr int RGRID = 592;   // fixed partial count (4 x 148 SMs): reproducible 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-// partial[b*K + k] = sum over this block's slice of x_k . y (K vectors of
-// V), MD_KT dot products per pass: y is read once per MD_KT vectors and one
-// block reduction serves them all.  Products and sums in FP64 whatever the
-// vector type.
+// partial[b*K + k] = sum over block column b's slice of x_k . y (K vectors
+// of V), MD_KT dot products per block: blockIdx.y picks the group of MD_KT
+// vectors, so the groups run side by side instead of one after another in
+// each block (y, read once per group, stays in L2).  Products and sums in
+// FP64 whatever the vector type.
 constexpr int MD_KT = 8;
 template <class T>
 __global__ void __launch_bounds__(RB)
@@ -39,30 +40,28 @@ __global__ void __launch_bounds__(RB)
                double* __restrict__ partial) {
     __shared__ double sh[MD_KT][RB / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int k0 = 0; k0 < K; k0 += MD_KT) {
-        const int kt = min(MD_KT, K - k0);
-        double acc[MD_KT];
+    const int k0 = blockIdx.y * MD_KT;
+    const int kt = min(MD_KT, K - k0);
+    double acc[MD_KT];
 #pragma unroll
-        for (int j = 0; j < MD_KT; ++j) acc[j] = 0.0;
-        GRID_STRIDE(i, n) {
-            const double yi = (double)y[i];
+    for (int j = 0; j < MD_KT; ++j) acc[j] = 0.0;
+    GRID_STRIDE(i, n) {
+        const double yi = (double)y[i];
 #pragma unroll
-            for (int j = 0; j < MD_KT; ++j)
-                if (j < kt) acc[j] += (double)V[(int64_t)(k0 + j) * ldv + i] * yi;
-        }
+        for (int j = 0; j < MD_KT; ++j)
+            if (j < kt) acc[j] += (double)V[(int64_t)(k0 + j) * ldv + i] * yi;
+    }
 #pragma unroll
-        for (int j = 0; j < MD_KT; ++j) {
-            const double v = warp_sum(acc[j]);
-            if (lane == 0) sh[j][w] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x < kt) {
-            double t = 0.0;
+    for (int j = 0; j < MD_KT; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) sh[j][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kt) {
+        double t = 0.0;
 #pragma unroll
-            for (int q = 0; q < RB / 32; ++q) t += sh[threadIdx.x][q];
-            partial[(int64_t)blockIdx.x * K + k0 + threadIdx.x] = t;
-        }
-        __syncthreads();
+        for (int q = 0; q < RB / 32; ++q) t += sh[threadIdx.x][q];
+        partial[(int64_t)blockIdx.x * K + k0 + threadIdx.x] = t;
     }
 }
 
@@ -77,14 +76,25 @@ __global__ void k_finish(const double* __restrict__ partial, int nb, int K, doub
     }
 }
 
-// y -= sum_k h[k] V_k  (h on the device)
+// y -= sum_k h[k] V_k  (h on the device, staged in shared memory 64 at a
+// time; k ascending for every element)
 template <class T>
-__global__ void k_multiaxpy(const T* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h,
-                            T* __restrict__ y, int64_t n) {
-    GRID_STRIDE(i, n) {
-        double acc = (double)y[i];
-        for (int k = 0; k < K; ++k) acc -= h[k] * (double)V[k * ldv + i];
-        y[i] = (T)acc;
+__global__ void __launch_bounds__(256)
+    k_multiaxpy(const T* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h, T* __restrict__ y,
+                int64_t n) {
+    __shared__ double hs[64];
+    for (int c0 = 0; c0 < K; c0 += 64) {
+        const int kc = min(64, K - c0);
+        __syncthreads();
+        if (threadIdx.x < kc) hs[threadIdx.x] = h[c0 + threadIdx.x];
+        __syncthreads();
+        GRID_STRIDE(i, n) {
+            double acc = (double)y[i];
+            const T* v = V + (int64_t)c0 * ldv + i;
+#pragma unroll 8
+            for (int k = 0; k < kc; ++k) acc -= hs[k] * (double)v[(int64_t)k * ldv];
+            y[i] = (T)acc;
+        }
     }
 }
 
@@ -175,7 +185,8 @@ template <class T>
 void Blas::multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev) {
     for (int k0 = 0; k0 < K; k0 += 64) {
         int kk = std::min(64, K - k0);
-        k_multidot<T><<<RGRID, RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n, partial.get());
+        k_multidot<T><<<dim3(RGRID, (kk + MD_KT - 1) / MD_KT), RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n,
+                                                                          partial.get());
         UP3D_CHECK_LAUNCH();
         k_finish<<<1, 1024, 0, s>>>(partial.get(), RGRID, kk, out_dev + k0);
         UP3D_CHECK_LAUNCH();
