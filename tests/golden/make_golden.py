@@ -743,6 +743,98 @@ def make_lifting_picard(name):
 
 
 
+MV_SHEET = {"shape": (16, 6, 5), "amplitude": 0.08, "seed": 3, "te_x": 2.5, "sheet_z": 0.55,
+            "m_inf": 0.8, "jump": 0.05}
+
+
+def mv_case():
+    """The level-set case: the bump channel cut by the horizontal half-plane
+    z = sheet_z downstream of x = te_x (TE line across the span, y from 1
+    to 0 so that "+" is +z), a transonic pocket state on the main DOFs and a
+    jump on the aux DOFs."""
+    c = MV_SHEET
+    mesh = bump_channel(*c["shape"], amplitude=c["amplitude"], seed=c["seed"])
+    te = np.array([[c["te_x"], 1.0, c["sheet_z"]], [c["te_x"], 0.0, c["sheet_z"]]])
+    return mesh, te, np.array([1.0, 0.0, 0.0])
+
+
+def mv_state(mesh, node_side, ext_dof_of_node):
+    phi_main = pocket_state(mesh, "mixed")
+    cut_nodes = np.flatnonzero(ext_dof_of_node >= 0)
+    gam = MV_SHEET["jump"] * (1.0 + 0.3 * mesh.nodes[cut_nodes, 0])
+    aux = phi_main[cut_nodes] - node_side[cut_nodes] * gam
+    return np.concatenate([phi_main, aux])
+
+
+def make_multivalued(name):
+    """The reference's level-set path -- WakeLevelSet (wake/levelset.py),
+    CutElementMap (wake/cut_elements.py), MultivaluedOperator
+    (wake/multivalued.py) with the cut-element assembly of
+    kernels/cut_assembly.py -- on the bump channel cut by a half-plane sheet
+    (mv_case): the level set at the nodes, the cut census and extended DOF
+    numbering, the extended matrix with the continuity closure and with the
+    wake least-squares closure (mass-conservation TE rows, no TE nodes on
+    this sheet), the per-side upwinded densities and monitors, the per-side
+    Newton records, live and frozen, at M0.8 with a jump on the aux DOFs."""
+    from pyfp3d.physics.isentropic import density_field
+    from pyfp3d.wake.cut_elements import CutElementMap
+    from pyfp3d.wake.levelset import WakeLevelSet
+    from pyfp3d.wake.multivalued import MultivaluedOperator
+    mesh, te, direction = mv_case()
+    ls = WakeLevelSet(te, direction)
+    s_, d_, q_ = ls.evaluate(mesh.nodes)
+    cm = CutElementMap(mesh.nodes, mesh.elements, ls)
+    mv = MultivaluedOperator(mesh.nodes, mesh.elements, cm, levelset=ls)
+    m_inf = MV_SHEET["m_inf"]
+    phi_ext = mv_state(mesh, cm.node_side, cm.ext_dof_of_node)
+    arrays = {"te_points": te, "direction": direction, "s": s_, "d": d_, "q": q_,
+              "normals_cut": ls.surface_normals(mesh.nodes[mesh.elements[cm.cut_elems]].mean(axis=1)),
+              "phi_ext": phi_ext, "node_side": cm.node_side, "te_nodes": cm.te_nodes,
+              "cut_elems": cm.cut_elems, "te_lower_elems": cm.te_lower_elems,
+              "beyond_tip_elems": cm.beyond_tip_elems, "shifted_nodes": cm.shifted_nodes,
+              "ext_dof_of_node": cm.ext_dof_of_node, "dofs_upper": cm.dofs_upper, "dofs_lower": cm.dofs_lower,
+              "n_total": np.int64(cm.n_total_dofs)}
+    _, q2 = mv.op.velocities(phi_ext[:mv.n_main])
+    rho = density_field(q2, m_inf).copy()
+    arrays["rho_main"] = rho
+
+    def put(tag, A):
+        A = A.tocsr()
+        A.sort_indices()
+        arrays.update({tag + "/indptr": A.indptr.astype(np.int64), tag + "/indices": A.indices.astype(np.int64),
+                       tag + "/data": A.data})
+
+    put("A_laplace", mv.assemble_matrix(None))
+    put("A_continuity", mv.assemble_matrix(rho))
+    rho_up, rho_lo = mv.element_densities(phi_ext, m_inf)
+    arrays.update({"rho_up": rho_up, "rho_lo": rho_lo})
+    put("A_wake_ls", mv.assemble_matrix((rho_up, rho_lo), closure="wake_ls", te_kutta="mass"))
+    rt_u, rt_l = mv.element_rho_tilde(phi_ext, m_inf, UPWIND_C, M_CRIT)
+    arrays.update({"rt_up": rt_u.copy(), "rt_lo": rt_l.copy(), "mon": np.array(
+        [mv.nu_max, mv.n_nu_active, mv.n_floored, mv.n_limited], dtype=np.float64),
+        "nu_active_elements": mv.nu_active_elements()})
+    up, lo = mv.side_potentials(phi_ext)
+    arrays.update({"phi_up": up, "phi_lo": lo,
+                   "node_jump": mv.node_jump(phi_ext, np.flatnonzero(cm.ext_dof_of_node >= 0)),
+                   "mach2": mv.element_mach2(phi_ext, m_inf)})
+    for tag, fz in (("live", None), ("frozen", mv.freeze_side_state(phi_ext, m_inf, UPWIND_C, M_CRIT))):
+        if fz is not None:
+            for k, side in enumerate(("upper", "lower")):
+                arrays[f"freeze/{side}/upstream"] = fz[k][0].copy()
+                arrays[f"freeze/{side}/branch"] = fz[k][1].copy()
+        sides = mv.newton_side_data(phi_ext, m_inf, UPWIND_C, M_CRIT, frozen=fz)
+        for side, rec in zip(("upper", "lower"), sides):
+            for key in ("rho_tilde", "s_e", "s_u", "upstream", "grad", "lim_mask", "keep", "dofvec", "readvec",
+                        "grad_row"):
+                arrays[f"{tag}/{side}/{key}"] = np.asarray(rec[key]).copy()
+        arrays[f"{tag}/mon"] = np.array([mv.nu_max, mv.n_nu_active, mv.n_floored, mv.n_limited], dtype=np.float64)
+    print("multivalued: cut", len(cm.cut_elems), "aux", cm.n_ext_dofs, "nu_active", mv.n_nu_active,
+          "mixed plain", int(mv._mixed_plain_mask().sum()))
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({path.stat().st_size / 1e6:.2f} MB)")
+
+
 def make_lagged_lu(name):
     """The reference's lagged-LU Newton (solve_newton_lifting(precond=
     "direct", direct_refactor_every=1000), solve/newton.py:978-1008: one
@@ -896,6 +988,9 @@ def main():
         make_weighted_picard("weighted_picard")
         make_lagged_lu("lagged_lu")
         return
+    if "--multivalued-only" in sys.argv:
+        make_multivalued("multivalued")
+        return
     if "--lagged-lu-only" in sys.argv:
         make_lagged_lu("lagged_lu")
         return
@@ -936,6 +1031,7 @@ def main():
     make_lifting_picard("lifting_picard")
     make_weighted_picard("weighted_picard")
     make_lagged_lu("lagged_lu")
+    make_multivalued("multivalued")
     make_te_pressure("te_pressure")
 
 
