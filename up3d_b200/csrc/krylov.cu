@@ -98,6 +98,71 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// The second and third passes of a CGS2 Arnoldi step, each one sweep over
+// the basis: y -= sum_k h[k] V_k (K <= 64 vectors) tile by tile (one row
+// per thread, 256-row tiles), then over the same tile, whose V values the
+// update has just brought into cache, the partial dots V_k . y (DOTS) or
+// y . y (NORM) of the new y: partial[b * P + k] with P = K (DOTS) or 1,
+// one block's tiles in ascending order (reproducible sums).
+constexpr int CG_TILE = 256;
+template <class T, bool DOTS>
+__global__ void __launch_bounds__(CG_TILE)
+    k_axpy_dots(const T* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h, T* __restrict__ y,
+                int64_t n, double* __restrict__ partial) {
+    __shared__ double hs[64];
+    __shared__ double ys[CG_TILE];
+    __shared__ double acc_blk[64];
+    __shared__ double wsum[CG_TILE / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < K) hs[threadIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < 64) acc_blk[threadIdx.x] = 0.0;
+    __syncthreads();
+    for (int64_t tile = blockIdx.x; tile * CG_TILE < n; tile += gridDim.x) {
+        const int64_t i0 = tile * CG_TILE;
+        const int64_t i = i0 + threadIdx.x;
+        double yi = 0.0;
+        if (i < n) {
+            double a = (double)y[i];
+            const T* v = V + i;
+#pragma unroll 8
+            for (int k = 0; k < K; ++k) a -= hs[k] * (double)v[(int64_t)k * ldv];
+            const T r = (T)a;
+            y[i] = r;
+            yi = (double)r;
+        }
+        if (DOTS) {
+            ys[threadIdx.x] = yi;
+            __syncthreads();
+            const int rows = n - i0 < CG_TILE ? (int)(n - i0) : CG_TILE;
+            for (int k = warp; k < K; k += CG_TILE / 32) {
+                const T* v = V + (int64_t)k * ldv + i0;
+                double d = 0.0;
+#pragma unroll
+                for (int m = 0; m < CG_TILE / 32; ++m) {
+                    const int r = lane + 32 * m;
+                    if (r < rows) d += (double)v[r] * ys[r];
+                }
+                d = warp_sum(d);
+                if (lane == 0) acc_blk[k] += d;
+            }
+            __syncthreads();
+        } else {
+            const double d = warp_sum(yi * yi);
+            if (lane == 0) wsum[warp] = d;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < CG_TILE / 32; ++q) t += wsum[q];
+                acc_blk[0] += t;
+            }
+            __syncthreads();
+        }
+    }
+    const int P = DOTS ? K : 1;
+    if (threadIdx.x < P) partial[(int64_t)blockIdx.x * P + threadIdx.x] = acc_blk[threadIdx.x];
+}
+
 __global__ void k_axpby(double a, const double* __restrict__ x, double b, double* __restrict__ y, int64_t n) {
     GRID_STRIDE(i, n) y[i] = a * x[i] + b * y[i];
 }
@@ -173,7 +238,7 @@ __global__ void k_copy_scalar(const double* __restrict__ src, double* __restrict
 // ------------------------------------------------------------ Vec helper
 
 Blas::Blas(cudaStream_t s) : s(s) {
-    partial.alloc((size_t)RGRID * 64);
+    partial.alloc((size_t)std::max(RGRID, 148 * 8) * 64);
     scal.alloc(128);
     UP3D_CUDA(cudaMallocHost(&host, 128 * sizeof(double)));
 }
@@ -223,12 +288,27 @@ void Blas::multiaxpy(const T* V, int64_t ldv, int K, const double* h_dev, T* y, 
     UP3D_CHECK_LAUNCH();
 }
 
+template <class T>
+void Blas::axpy_dots(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n, bool dots,
+                     double* out_dev) {
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + CG_TILE - 1) / CG_TILE, 148 * 8));
+    const int P = dots ? K : 1;
+    if (dots)
+        k_axpy_dots<T, true><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get());
+    else
+        k_axpy_dots<T, false><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get());
+    UP3D_CHECK_LAUNCH();
+    k_finish<<<1, 1024, 0, s>>>(partial.get(), (int)grid, P, out_dev);
+    UP3D_CHECK_LAUNCH();
+}
+
 #define UP3D_BLAS_INST(T)                                                                 \
     template void Blas::multidot<T>(const T*, int64_t, int, const T*, int64_t, double*); \
     template double Blas::dot<T>(const T*, const T*, int64_t);                           \
     template double Blas::nrm2<T>(const T*, int64_t);                                    \
     template void Blas::scale<T>(T*, double, int64_t);                                   \
-    template void Blas::multiaxpy<T>(const T*, int64_t, int, const double*, T*, int64_t);
+    template void Blas::multiaxpy<T>(const T*, int64_t, int, const double*, T*, int64_t); \
+    template void Blas::axpy_dots<T>(const T*, int64_t, int, const double*, T*, int64_t, bool, double*);
 UP3D_BLAS_INST(double)
 UP3D_BLAS_INST(float)
 #undef UP3D_BLAS_INST
@@ -447,15 +527,13 @@ int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, 
     restart = (int)std::min<int64_t>(restart, n);
     DBuf<T>* B = W.bufs<T>();
     DBuf<T>& V = B[0];
-    DBuf<T>& w = B[1];
     DBuf<T>& r = B[2];
     DBuf<T>& tmp = B[3];
     DBuf<double>& hdev = W.d[5];
     V.alloc((size_t)(restart + 1) * n);
-    w.alloc(n);
     r.alloc(n);
     tmp.alloc(n);
-    hdev.alloc(2 * (restart + 1) + 2);
+    hdev.alloc(2 * restart + 6);
     double* hbuf = W.pinned(restart + 3);
     std::vector<double> H((size_t)restart * (restart + 1), 0.0), gc(restart), gs(restart), S(restart + 1);
     const double bnrm = bl.nrm2(b, n);
@@ -497,25 +575,32 @@ int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, 
             // one Arnoldi step on the device, one readback: the column
             // [h_0 .. h_col] (CGS2: two projections onto V_0..V_col, summed),
             // |w| before and after the projections
-            double* hsum = hdev.get();
-            double* hpass = hdev.get() + (restart + 1);
-            double* hn = hdev.get() + 2 * (restart + 1);
+            // the new vector is formed in place in V[col + 1]: pass 1 takes
+            // V_0..V_col and the vector itself in one multidot (h and
+            // |w|^2), passes 2 and 3 are one sweep each (update + the next
+            // pass's dots, update + |w|^2)
+            double* hsum = hdev.get();                  // h_0..h_col, |w|^2 before, |w|^2 after
+            double* hpass = hdev.get() + (restart + 3);
+            double* hn = hsum + col + 1;
+            T* wv = V.get() + (size_t)(col + 1) * n;
             op.apply(V.get() + (size_t)col * n, tmp.get(), s);
-            precond_apply(M, tmp.get(), w.get(), n, s);
-            bl.multidot(w.get(), 0, 1, w.get(), n, hn);
-            bl.multidot(V.get(), n, col + 1, w.get(), n, hsum);
-            bl.multiaxpy(V.get(), n, col + 1, hsum, w.get(), n);
-            bl.multidot(V.get(), n, col + 1, w.get(), n, hpass);
-            bl.multiaxpy(V.get(), n, col + 1, hpass, w.get(), n);
+            precond_apply(M, tmp.get(), wv, n, s);
+            if (col + 1 <= 64) {
+                bl.multidot(V.get(), n, col + 2, wv, n, hsum);
+                bl.axpy_dots(V.get(), n, col + 1, hsum, wv, n, true, hpass);
+                bl.axpy_dots(V.get(), n, col + 1, hpass, wv, n, false, hn + 1);
+            } else {
+                bl.multidot(V.get(), n, col + 2, wv, n, hsum);
+                bl.multiaxpy(V.get(), n, col + 1, hsum, wv, n);
+                bl.multidot(V.get(), n, col + 1, wv, n, hpass);
+                bl.multiaxpy(V.get(), n, col + 1, hpass, wv, n);
+                bl.multidot(wv, 0, 1, wv, n, hn + 1);
+            }
             k_accumulate<double><<<1, 64, 0, s>>>(hsum, hpass, col + 1);
             UP3D_CHECK_LAUNCH();
-            bl.multidot(w.get(), 0, 1, w.get(), n, hn + 1);
-            UP3D_CUDA(cudaMemcpyAsync(V.get() + (size_t)(col + 1) * n, w.get(), sizeof(T) * n,
-                                      cudaMemcpyDeviceToDevice, s));
-            k_scale_unless_breakdown<T><<<grid_for(n, 256), 256, 0, s>>>(V.get() + (size_t)(col + 1) * n, hn, eps, n);
+            k_scale_unless_breakdown<T><<<grid_for(n, 256), 256, 0, s>>>(wv, hn, eps, n);
             UP3D_CHECK_LAUNCH();
-            UP3D_CUDA(cudaMemcpyAsync(hbuf, hsum, sizeof(double) * (col + 1), cudaMemcpyDeviceToHost, s));
-            UP3D_CUDA(cudaMemcpyAsync(hbuf + col + 1, hn, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+            UP3D_CUDA(cudaMemcpyAsync(hbuf, hsum, sizeof(double) * (col + 3), cudaMemcpyDeviceToHost, s));
             UP3D_CUDA(cudaStreamSynchronize(s));
             for (int k = 0; k <= col; ++k) Hat(col, k) = hbuf[k];
             const double h0 = std::sqrt(hbuf[col + 1]);

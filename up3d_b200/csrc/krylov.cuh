@@ -40,6 +40,11 @@ struct Blas {
     void scale(T* x, double a, int64_t n);
     template <class T>
     void multiaxpy(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n);
+    // y -= V h (K <= 64) in one sweep that also forms V^T y (dots) or y.y
+    // (!dots) of the new y into out_dev
+    template <class T>
+    void axpy_dots(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n, bool dots,
+                   double* out_dev);
 };
 
 // y = A x (+ extra x): the P1-pattern matrix plus, for the Newton Jacobian,
