@@ -258,15 +258,15 @@ def read_peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic(kernel: str):
-    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+def read_traffic(kernel: str, n_tets: int):
+    """DRAM bytes per launch at n_tets from a committed ncu summary (its
+    measured bytes per element times the element count), if one exists."""
+    import re
     for f in sorted((REPO / "profiles").glob(f"{kernel}*.md")):
         for line in f.read_text().splitlines():
             if line.startswith("dram_bytes_per_launch_full_size:"):
-                try:
-                    return float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    return None
+                m = re.search(r"\(([0-9.]+) B/elem", line)
+                return None if m is None else round(float(m.group(1)) * n_tets)
     return None
 
 
@@ -1176,13 +1176,13 @@ def run_ours(args):
         per_launch_ms = (prof["elem_sweep"]["ms"] + prof["row_gather"]["ms"]) / calls
         dom_bytes = bm["elem_sweep"] + bm["row_gather"]
         design_bytes = bm["design"]["tile_eval"]
-        traffic = read_traffic("tile_eval")
+        traffic = read_traffic("tile_eval", dmesh.n_tets)
     else:
         dom = max(("elem_sweep", "row_gather"), key=lambda s: prof[s]["ms"])
         per_launch_ms = prof[dom]["ms"] / max(prof[dom]["calls"], 1)
         dom_bytes = bm[dom]
         design_bytes = bm["design"][dom]
-        traffic = read_traffic(dom)
+        traffic = read_traffic(dom, dmesh.n_tets)
     achieved = dom_bytes / (per_launch_ms * 1e-3) / 1e9
     step_bytes = bm["fused"]
     phase_names = {"elem_sweep": "tile_eval", "row_gather": "combine"} if tiled else {}
