@@ -611,6 +611,22 @@ int up3d_amg_get_info(const up3d_precond* M, up3d_amg_info* info);
 int up3d_amg_refresh(up3d_precond* M, const up3d_csr* A, up3d_stream stream);
 
 /* Point-Jacobi preconditioner z = D^{-1} r (constrained rows: identity). */
+/* ILU(0) preconditioner on A's own pattern (replaces solve/linear.py:84-131
+ * build_ilu_preconditioner; the reference's threshold ILU is scipy's serial
+ * spilu): the fixed-point form of ILU(0) (Chow and Patel, SIAM J. Sci.
+ * Comput. 37, 2015), `sweeps` sweeps from L = strict lower part of A over
+ * its diagonal and U = upper part; applied as U^-1 L^-1 r with
+ * `tri_sweeps` Jacobi sweeps per triangle.  Honours A->dirichlet (identity
+ * rows, dropped columns).  Every row needs its diagonal in the pattern
+ * (UP3D_ERR_VALUE otherwise); a non-finite factorisation is redone on
+ * A + 1e-3 mean|a_ii| I, and UP3D_ERR_RUNTIME if that fails too.  FP64
+ * vectors only (up3d_gmres_ir refuses it).  sweeps, tri_sweeps in [1, 100]
+ * (UP3D_ERR_VALUE otherwise). */
+int up3d_precond_ilu0(const up3d_csr* A, int sweeps, int tri_sweeps, up3d_precond** out, up3d_stream stream);
+/* The ILU(0) factors (nnz values on A's pattern: L strictly below the
+ * diagonal, unit diagonal implied; U on and above) into `lu` (device), and
+ * the diagonal shift the factorisation used into *shift (host). */
+int up3d_precond_ilu0_factors(const up3d_precond* M, double* lu, double* shift, up3d_stream stream);
 int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream);
 /* z = M r */
 int up3d_precond_apply(up3d_precond* M, const double* r, double* z, up3d_stream stream);

@@ -129,8 +129,8 @@ def test_gpu_lifting_rejects_unbuilt_options(gold):
         NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="nope")
     with pytest.raises(ValueError):                 # the channel cut has no wall group
         NewtonWorkspace(cut, cut.wc, 3.0, vortex_center=vc, kutta_estimator="pressure")
-    with pytest.raises(NotImplementedError):
-        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="ilu")
+    with pytest.raises(ValueError):
+        solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="nope")
     with pytest.raises(ValueError):
         solve_newton_lifting(cut, cut.wc, 0.5, vortex_center=vc, precond="direct", direct_refactor_every=0)
     from up3d_b200.solve.lifting import solve_subsonic_lifting
@@ -267,6 +267,24 @@ def test_gpu_lifting_direct_steps_match_reference(gold, name):
     assert np.allclose(hist[big], ref[big], rtol=1e-6)
     assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-10
     assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_lifting_ilu_reaches_reference_solution(gold, name):
+    """precond="ilu" (device ILU(0) of the reduced J_ff every step, in place
+    of the reference's host threshold ILU): the reference's converged state
+    (the exact-step fixture) to 1e-9."""
+    from up3d_b200.mesh.wake_cut import channel_vortex_center
+    from up3d_b200.solve.lifting import solve_newton_lifting
+    g, cut = _case(gold, name)
+    res = solve_newton_lifting(cut, cut.wc, float(g["m_inf"]), alpha_deg=float(g["alpha_deg"]),
+                               vortex_center=channel_vortex_center(cut),
+                               farfield_spanwise_gamma=bool(g["spanwise"]), n_picard_seed=0, precond="ilu")
+    assert res["converged"]
+    assert res["n_newton"] <= int(g["sol_n_newton"]) + 3
+    assert np.max(np.abs(res["phi"].cpu().numpy() - g["sol_phi"])) <= 1e-9
+    assert np.max(np.abs(res["gamma"].cpu().numpy() - g["sol_gamma"])) <= 1e-9
+    print(name, "ilu n_newton", res["n_newton"], "n_gmres", res["n_gmres_total"])
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -159,6 +159,8 @@ SIGNATURES = {
     "up3d_amg_get_info": (_int, [_p, _p]),
     "up3d_amg_refresh": (_int, [_p, _p, _p]),
     "up3d_precond_jacobi": (_int, [_p, ctypes.POINTER(_p), _p]),
+    "up3d_precond_ilu0": (_int, [_p, _int, _int, ctypes.POINTER(_p), _p]),
+    "up3d_precond_ilu0_factors": (_int, [_p, _p, ctypes.POINTER(_d), _p]),
     "up3d_precond_apply": (_int, [_p, _p, _p, _p]),
     "up3d_amg_vcycle": (_int, [_p, _p, _p, _p]),
     "up3d_amg_vcycle_f32": (_int, [_p, _p, _p, _p]),

@@ -394,6 +394,8 @@ void up3d_precond::apply(const double* r, double* z, cudaStream_t s) {
         UP3D_CHECK_LAUNCH();
     } else if (kind == 2) {
         amg_apply(amg, r, z, s);
+    } else if (kind == 3) {
+        ilu0_apply(ilu, r, z, s);
     } else {
         UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
@@ -406,6 +408,8 @@ void up3d_precond::apply(const float* r, float* z, cudaStream_t s) {
         UP3D_CHECK_LAUNCH();
     } else if (kind == 2) {
         amg_apply_f32(amg, r, z, s);
+    } else if (kind == 3) {
+        UP3D_REQUIRE(false, UP3D_ERR_NOT_IMPLEMENTED, "the ILU(0) preconditioner applies to FP64 vectors only");
     } else {
         UP3D_CUDA(cudaMemcpyAsync(z, r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
     }
@@ -764,6 +768,29 @@ void make_op(Operator& op, const up3d_csr* A, const up3d_csr* extra) {
 }  // namespace
 
 extern "C" {
+
+int up3d_precond_ilu0(const up3d_csr* A, int sweeps, int tri_sweeps, up3d_precond** out, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(A && out, UP3D_ERR_ARGUMENT, "up3d_precond_ilu0: null argument");
+        auto* M = new up3d_precond();
+        M->kind = 3;
+        M->n = A->n;
+        try {
+            M->ilu = ilu0_create(A, sweeps, tri_sweeps, S(stream));
+        } catch (...) {
+            delete M;
+            throw;
+        }
+        *out = M;
+    });
+}
+
+int up3d_precond_ilu0_factors(const up3d_precond* M, double* lu, double* shift, up3d_stream stream) {
+    return guarded([&] {
+        UP3D_REQUIRE(M && M->kind == 3 && M->ilu, UP3D_ERR_ARGUMENT, "up3d_precond_ilu0_factors: not an ILU(0) handle");
+        ilu0_factors(M->ilu, lu, shift, S(stream));
+    });
+}
 
 int up3d_precond_jacobi(const up3d_csr* A, up3d_precond** out, up3d_stream stream) {
     return guarded([&] {

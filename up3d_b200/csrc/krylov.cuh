@@ -68,18 +68,24 @@ void amg_destroy(void* amg);
 void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s);
 void amg_refresh(void* amg, const up3d_csr& A, cudaStream_t s);
 const up3d_amg_info* amg_info(void* amg);
+void* ilu0_create(const up3d_csr* A, int sweeps, int tri_sweeps, cudaStream_t s);
+void ilu0_apply(void* ilu, const double* r, double* z, cudaStream_t s);
+void ilu0_destroy(void* ilu);
+void ilu0_factors(const void* ilu, double* out, double* shift, cudaStream_t s);
 
 }  // namespace up3d
 
 // Preconditioner handle: identity, point Jacobi or an AMG hierarchy.
 struct up3d_precond {
-    int kind = 0;  // 0 identity, 1 Jacobi, 2 AMG
+    int kind = 0;  // 0 identity, 1 Jacobi, 2 AMG, 3 ILU(0)
     int64_t n = 0;
     up3d::DBuf<double> dinv;
     void* amg = nullptr;
+    void* ilu = nullptr;
     up3d_precond() = default;
     ~up3d_precond() {
         if (amg) up3d::amg_destroy(amg);
+        if (ilu) up3d::ilu0_destroy(ilu);
     }
     void apply(const double* r, double* z, cudaStream_t s);
     void apply(const float* r, float* z, cudaStream_t s);

@@ -28,7 +28,10 @@ its state-dependent eliminated row -D^-1 K_p is rebuilt on the host per
 Newton step (n_stations rows over the TE fans' nodes) and uploaded to the
 coupled handle.  precond="direct" takes exact steps (dense LU of the
 reduced J_ff on the device with the Woodbury update for the Kutta
-coupling); precond="ilu" (the reference's host incomplete LU) is not built.
+coupling), with direct_refactor_every > 1 GMRES steps on a stale LU in
+between; precond="ilu" preconditions GMRES with a device ILU(0) of the
+reduced J_ff, rebuilt every step (the reference's host threshold ILU has no
+device form; see solve.linear.build_ilu_preconditioner).
 """
 
 from __future__ import annotations
@@ -44,7 +47,7 @@ from ..constraints.dirichlet import FarfieldBasis, freestream_phi, kutta_row
 from ..constraints.wake import WakeConstraint
 from ..mesh.device import DeviceCSR, device_view, get_mesh
 from .fused import FlowParams, ResidualJacobian
-from .linear import _csr_struct, amg_for
+from .linear import _csr_struct, amg_for, build_ilu_preconditioner
 from .newton import _ew_forcing
 
 
@@ -298,12 +301,11 @@ class NewtonWorkspace:
         if self.n_free > self.DIRECT_MAX_FREE:
             raise ValueError(f"precond='direct' is for small cases: {self.n_free} free unknowns "
                              f"(limit {self.DIRECT_MAX_FREE}); use precond='amg'")
-        if not hasattr(self, "_con_direct"):
-            self._con_direct = WakeConstraint(Aop.J, self.wc)   # plans of the merged Jacobian patterns
+        J_red = self.jacobian_block(Aop)
+        if not hasattr(self, "_free_pos"):
             self._free_pos = t.full((self.n_red,), -1, dtype=t.int64, device="cuda")
             self._free_pos[L.to_device(self.free, t.int64)] = t.arange(self.n_free, device="cuda")
             self._free_d = L.to_device(self.free, t.int64)
-        J_red, _ = self._con_direct.reduce_operator(Aop.J)
         ip = J_red.indptr.to(t.int64)
         rows = t.repeat_interleave(t.arange(self.n_red, device="cuda"), ip[1:] - ip[:-1])
         cols = J_red.indices.to(t.int64)
@@ -320,6 +322,17 @@ class NewtonWorkspace:
         B = t.stack(cols_b, dim=1) if cols_b else t.zeros((self.n_free, 0), dtype=t.float64, device="cuda")
         LU, piv = t.linalg.lu_factor(D)
         return LU, piv, B
+
+    def jacobian_block(self, Aop: CoupledOperator) -> DeviceCSR:
+        """T^T J T of this step's cut-mesh Jacobian (Term-3 entries merged),
+        with the far-field mask: J_ff embedded in the reduced numbering, the
+        matrix the direct and ILU preconditioners factor."""
+        if not hasattr(self, "_con_direct"):
+            self._con_direct = WakeConstraint(Aop.J, self.wc)   # plans of the merged Jacobian patterns
+        J_red, _ = self._con_direct.reduce_operator(Aop.J)
+        J_red.dirichlet = self.mask
+        J_red.extra = None
+        return J_red
 
     def direct_step(self, lu, K, rhs):
         """dphi = z - JB S^-1 K z with z = J_ff^-1 rhs, JB = J_ff^-1 B,
@@ -478,9 +491,8 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
     if m_inf > 0.0 and upwind_c <= 0.0:
         raise ValueError("the Newton driver runs with the walk upwind machinery active for m_inf > 0; "
                          "pass upwind_c > 0")
-    if precond not in ("amg", "direct"):
-        raise NotImplementedError(f"precond={precond!r}: the device driver solves with AMG-GMRES or a "
-                                  "dense direct factorisation")
+    if precond not in ("amg", "direct", "ilu"):
+        raise ValueError(f"unknown precond {precond!r}")
     if direct_refactor_every < 1:
         raise ValueError(f"direct_refactor_every must be >= 1, got {direct_refactor_every}")
     ws = workspace
@@ -630,6 +642,9 @@ def solve_newton_lifting(mesh_cut, wc, m_inf: float, alpha_deg: float = 0.0, u_i
         a = clock()
         if precond == "amg" and (M_pre is None or it % amg_rebuild_every == 0):
             ws.amg = M_pre = amg_for(ws.picard_block(), ws.amg)
+        elif precond == "ilu":
+            # ILU of J_ff itself, every step (newton.py:1023-1024)
+            M_pre = build_ilu_preconditioner(ws.jacobian_block(Aop))
         timings["precond"] += clock() - a
         # rhs = -R_f - B F_elim  (B F_elim = the coupled operator at x = 0)
         a = clock()

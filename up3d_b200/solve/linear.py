@@ -182,10 +182,30 @@ def build_jacobi_preconditioner(A, dirichlet=None) -> DevicePreconditioner:
     return DevicePreconditioner(h.value, Ad.shape[0], "jacobi")
 
 
-def build_ilu_preconditioner(A, drop_tol: float = 1e-4, fill_factor: float = 10.0):
-    """solve/linear.py:84-131 -- incomplete LU is not part of the B200 path
-    (its triangular solves serialise); the device drivers use AMG."""
-    raise NotImplementedError("build_ilu_preconditioner: use build_amg_preconditioner on the device")
+def build_ilu_preconditioner(A, drop_tol: float = 1e-4, fill_factor: float = 10.0, dirichlet=None,
+                             sweeps: int = 5, tri_sweeps: int = 3) -> DevicePreconditioner:
+    """Incomplete-LU preconditioner (solve/linear.py:84-131) on the device:
+    ILU(0) on A's own pattern by fixed-point sweeps, applied with Jacobi
+    sweeps on each triangle (up3d_precond_ilu0).  The reference's threshold
+    ILU (scipy spilu with drop_tol and fill_factor, a serial host
+    factorisation) has no device form; drop_tol and fill_factor are
+    accepted and not used: ILU(0) keeps no fill and drops nothing.  A
+    non-finite factorisation is redone shifted by 1e-3 mean|a_ii| (the
+    reference's last fallback).  Returns a DevicePreconditioner (FP64)."""
+    Ad = as_device_csr(A)
+    h = ctypes.c_void_p()
+    L.call("up3d_precond_ilu0", ctypes.byref(_csr_struct(Ad, dirichlet)), int(sweeps), int(tri_sweeps),
+           ctypes.byref(h), L.stream_ptr())
+    return DevicePreconditioner(h.value, Ad.shape[0], "ilu0")
+
+
+def ilu_factors(M: DevicePreconditioner, nnz: int):
+    """(values on A's pattern, diagonal shift) of an ILU(0) preconditioner."""
+    t = L.torch()
+    lu = t.empty(nnz, dtype=t.float64, device="cuda")
+    shift = ctypes.c_double()
+    L.call("up3d_precond_ilu0_factors", M.handle, lu.data_ptr(), ctypes.byref(shift), L.stream_ptr())
+    return lu, float(shift.value)
 
 
 # ------------------------------------------------------------------ solvers
