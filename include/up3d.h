@@ -281,9 +281,9 @@ int up3d_face_normals(const up3d_mesh* mesh, double* out, up3d_stream stream);
  * built once per depth and kept on the mesh (rebuilt after
  * up3d_mesh_set_face_neighbors).  Device views of the CSR (offsets int64
  * n_tets + 1, indices int32) and the total; any output may be NULL.
- * UP3D_ERR_VALUE for depth outside [1, 4] (the reference takes any depth;
- * 4 hops reach up to 160 elements).  Synchronises the stream when it
- * builds. */
+ * Depths up to 4 (at most 160 elements) are built on the device, deeper
+ * ones on the host (OpenMP breadth-first search) and uploaded.
+ * UP3D_ERR_VALUE for depth < 1.  Synchronises the stream when it builds. */
 int up3d_mesh_neighborhoods(up3d_mesh* mesh, int depth, const int64_t** offsets,
                             const int32_t** indices, int64_t* total, up3d_stream stream);
 

@@ -75,7 +75,7 @@ def test_weighted_rho_tilde_matches_reference(gold, pname, mode):
         assert abs(upw.nu_max - float(gold[f"{key}/nu_max"])) <= 1e-12 * max(1.0, upw.nu_max), key
 
 
-@pytest.mark.parametrize("depth", [1, 2, 3, 4])
+@pytest.mark.parametrize("depth", [1, 2, 3, 4, 5, 7])
 def test_neighborhoods_match_oracle_on_a_larger_mesh(depth):
     from oracle import oracle as O
     from up3d_b200.kernels.upwind import build_upstream_neighborhoods
@@ -163,7 +163,24 @@ def test_weighted_mode_offers_rho_tilde_only_and_walk_mode_is_unchanged():
     ref = O.UpwindOperator(nodes, elements).rho_tilde(grad, q2, rho, 0.82, UPWIND_C, M_CRIT)
     assert rel_err(walk, ref) < REL_TOL
     with pytest.raises(ValueError, match="depth"):
-        UpwindOperator(nodes, elements, weighted=True, mode="kernel", nbr_depth=5)
+        UpwindOperator(nodes, elements, weighted=True, mode="kernel", nbr_depth=0)
+
+
+def test_kernel_mode_deeper_than_four_hops_matches_oracle():
+    """Neighbourhoods past four hops (built on the host) feed the same
+    kernel-mode sweep: the oracle's rho~ at nbr_depth 5 and 6."""
+    from oracle import oracle as O
+    from up3d_b200.kernels.upwind import UpwindOperator
+    from up3d_b200.mesh.kuhn import bump_channel, pocket_state
+    m = bump_channel(16, 6, 5, amplitude=0.08, seed=2)
+    grad, q2l, rho = _inputs(m.nodes, m.elements, pocket_state(m, "mixed"), 0.8)
+    for depth in (5, 6):
+        ref = O.UpwindOperator(m.nodes, m.elements, weighted=True, mode="kernel", nbr_depth=depth)
+        upw = UpwindOperator(m.nodes, m.elements, weighted=True, mode="kernel", nbr_depth=depth)
+        r = ref.rho_tilde(grad, q2l, rho, 0.8, UPWIND_C, M_CRIT).copy()
+        d = upw.rho_tilde(grad, q2l, rho, 0.8, UPWIND_C, M_CRIT)
+        assert rel_err(d, r) < REL_TOL, depth
+        assert upw.n_supersonic == ref.n_supersonic, depth
 
 
 def test_masked_face_neighbors_rebuild_the_neighborhoods():

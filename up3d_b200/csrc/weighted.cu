@@ -9,6 +9,9 @@
 // neighbourhood ascending, faces 0..3) with IEEE-rounded products and sums
 // (no contraction), like the oracle.
 
+#include <algorithm>
+#include <vector>
+
 #include <cub/cub.cuh>
 
 #include "elem.cuh"
@@ -264,6 +267,61 @@ __global__ void k_rho_tilde_blend(const int4* __restrict__ conn, const double4* 
 
 }  // namespace
 
+// Neighbourhoods deeper than NB_MAX_DEPTH hops grow past what one
+// thread's list holds; they are built on the host from a copy of the face
+// table (OpenMP over elements; one mark array per thread makes each BFS
+// linear in the neighbourhood's size) and uploaded.  Same lists: the
+// elements within `depth` hops, the element excluded, ascending.
+// Synchronises the stream.
+static int64_t neighborhoods_host(const int4* fn_dev, int64_t E, int depth, int64_t* off_dev, DBuf<int32_t>* idx_out,
+                                  int32_t* idx_dev, cudaStream_t s) {
+    std::vector<int4> fn(E);
+    if (E) UP3D_CUDA(cudaMemcpyAsync(fn.data(), fn_dev, sizeof(int4) * E, cudaMemcpyDeviceToHost, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    std::vector<std::vector<int32_t>> lists(E);
+#pragma omp parallel
+    {
+        std::vector<int64_t> mark(E, -1);
+        std::vector<int32_t> seen;
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t e = 0; e < E; ++e) {
+            seen.clear();
+            seen.push_back((int32_t)e);
+            mark[e] = e;
+            size_t lo = 0, hi = 1;
+            for (int d = 0; d < depth && lo < hi; ++d) {
+                for (size_t i = lo; i < hi; ++i) {
+                    const int4 f = fn[seen[i]];
+                    const int32_t nb[4] = {f.x, f.y, f.z, f.w};
+                    for (int k = 0; k < 4; ++k) {
+                        if (nb[k] < 0 || nb[k] >= E || mark[nb[k]] == e) continue;
+                        mark[nb[k]] = e;
+                        seen.push_back(nb[k]);
+                    }
+                }
+                lo = hi;
+                hi = seen.size();
+            }
+            lists[e].assign(seen.begin() + 1, seen.end());
+            std::sort(lists[e].begin(), lists[e].end());
+        }
+    }
+    std::vector<int64_t> off(E + 1, 0);
+    for (int64_t e = 0; e < E; ++e) off[e + 1] = off[e] + (int64_t)lists[e].size();
+    const int64_t total = off[E];
+    std::vector<int32_t> idx(total > 0 ? total : 1);
+    for (int64_t e = 0; e < E; ++e) std::copy(lists[e].begin(), lists[e].end(), idx.begin() + off[e]);
+    UP3D_CUDA(cudaMemcpyAsync(off_dev, off.data(), sizeof(int64_t) * (E + 1), cudaMemcpyHostToDevice, s));
+    int32_t* dst = idx_dev;
+    if (idx_out) {
+        idx_out->alloc(total > 0 ? total : 1);
+        dst = idx_out->get();
+    }
+    if (dst && total) UP3D_CUDA(cudaMemcpyAsync(dst, idx.data(), sizeof(int32_t) * total, cudaMemcpyHostToDevice, s));
+    UP3D_CUDA(cudaStreamSynchronize(s));
+    return total;
+}
+
 // Offsets (n + 1) of the depth-hop neighbourhoods of the face-neighbour
 // table fn; returns the total.  Synchronises the stream.
 static int64_t neighborhood_offsets(const int4* fn, int64_t E, int depth, int64_t* off, DBuf<unsigned char>& tmp,
@@ -290,6 +348,11 @@ void ensure_neighborhoods(up3d_mesh* m, int depth, cudaStream_t s) {
     const int64_t E = m->E;
     m->nb_depth = 0;
     m->nb_off.alloc(E + 1);
+    if (depth > NB_MAX_DEPTH) {
+        m->nb_total = neighborhoods_host(m->fnbr.get(), E, depth, m->nb_off.get(), &m->nb_idx, nullptr, s);
+        m->nb_depth = depth;
+        return;
+    }
     DBuf<unsigned char> tmp;
     const int64_t total = neighborhood_offsets(m->fnbr.get(), E, depth, m->nb_off.get(), tmp, s);
     m->nb_idx.alloc(total > 0 ? total : 1);
@@ -318,8 +381,7 @@ int up3d_mesh_neighborhoods(up3d_mesh* m, int depth, const int64_t** offsets, co
                             int64_t* total, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(m, UP3D_ERR_ARGUMENT, "up3d_mesh_neighborhoods: null argument");
-        UP3D_REQUIRE(depth >= 1 && depth <= NB_MAX_DEPTH, UP3D_ERR_VALUE,
-                     "up3d_mesh_neighborhoods: depth must be in [1, 4]");
+        UP3D_REQUIRE(depth >= 1, UP3D_ERR_VALUE, "up3d_mesh_neighborhoods: depth must be >= 1");
         ensure_neighborhoods(m, depth, S(stream));
         if (offsets) *offsets = m->nb_off.get();
         if (indices) *indices = m->nb_idx.get();
@@ -331,8 +393,7 @@ int up3d_face_neighborhoods(const int32_t* fn, int64_t n, int depth, int64_t* of
                             int64_t* total, up3d_stream stream) {
     return guarded([&] {
         UP3D_REQUIRE(fn && offsets && n >= 0, UP3D_ERR_ARGUMENT, "up3d_face_neighborhoods: null argument");
-        UP3D_REQUIRE(depth >= 1 && depth <= NB_MAX_DEPTH, UP3D_ERR_VALUE,
-                     "up3d_face_neighborhoods: depth must be in [1, 4]");
+        UP3D_REQUIRE(depth >= 1, UP3D_ERR_VALUE, "up3d_face_neighborhoods: depth must be >= 1");
         cudaStream_t s = S(stream);
         const int4* f4 = reinterpret_cast<const int4*>(fn);
         if (!indices) {
@@ -342,11 +403,19 @@ int up3d_face_neighborhoods(const int32_t* fn, int64_t n, int depth, int64_t* of
                 *total = 0;
                 return;
             }
+            if (depth > NB_MAX_DEPTH) {
+                *total = neighborhoods_host(f4, n, depth, offsets, nullptr, nullptr, s);
+                return;
+            }
             DBuf<unsigned char> tmp;
             *total = neighborhood_offsets(f4, n, depth, offsets, tmp, s);
             return;
         }
         if (n == 0) return;
+        if (depth > NB_MAX_DEPTH) {
+            neighborhoods_host(f4, n, depth, offsets, nullptr, indices, s);
+            return;
+        }
         k_neighborhoods<true><<<grid_for(n, 128), 128, 0, s>>>(f4, n, depth, nullptr, offsets, indices);
         UP3D_CHECK_LAUNCH();
     });
@@ -359,8 +428,7 @@ int up3d_rho_tilde_kernel(up3d_mesh* m, const double* grad, const double* q2, co
     return guarded([&] {
         UP3D_REQUIRE(m && grad && q2 && rho && flow && nu && rho_tilde, UP3D_ERR_ARGUMENT,
                      "up3d_rho_tilde_kernel: null argument");
-        UP3D_REQUIRE(depth >= 1 && depth <= NB_MAX_DEPTH, UP3D_ERR_VALUE,
-                     "up3d_rho_tilde_kernel: depth must be in [1, 4]");
+        UP3D_REQUIRE(depth >= 1, UP3D_ERR_VALUE, "up3d_rho_tilde_kernel: depth must be >= 1");
         cudaStream_t s = S(stream);
         ensure_neighborhoods(m, depth, s);
         if (mon) UP3D_CUDA(cudaMemsetAsync(mon, 0, sizeof(up3d_monitors), s));

@@ -34,7 +34,7 @@ def compute_face_normals(nodes, elements, out) -> None:
 def build_upstream_neighborhoods(face_neighbors, depth: int = 3):
     """The elements within `depth` face hops of each element, itself
     excluded, ascending, as CSR (offsets, indices) int64
-    (kernels/upwind.py:313-341).  depth in [1, 4] on the device."""
+    (kernels/upwind.py:313-341).  Any depth >= 1 (deeper than 4 hops built on the host)."""
     t = L.torch()
     fn = L.to_device(face_neighbors, t.int32)
     n = int(fn.shape[0])
