@@ -28,6 +28,30 @@ constexpr int RGRID = 592;   // fixed partial count (4 x 148 SMs): reproducible 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
+// Called by every thread of every block after the block has written its
+// partials: the last block to arrive sums partial[b * K + k] over b for
+// each k into out (lanes stride b, then a warp sum: a fixed order)
+// and re-arms the counter for the next launch on the stream.
+__device__ __forceinline__ void last_block_finish(const double* partial, int nb, int K, double* out,
+                                                  unsigned int* counter) {
+    __shared__ bool last;
+    const unsigned int blocks = gridDim.x * gridDim.y;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == blocks - 1u;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = w; k < K; k += nw) {
+        double acc = 0.0;
+        for (int b = lane; b < nb; b += 32) acc += __ldcg(partial + (int64_t)b * K + k);
+        acc = warp_sum(acc);
+        if (lane == 0) out[k] = acc;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
 // partial[b*K + k] = sum over block column b's slice of x_k . y (K vectors
 // of V), MD_KT dot products per block: blockIdx.y picks the group of MD_KT
 // vectors, so the groups run side by side instead of one after another in
@@ -37,7 +61,7 @@ constexpr int MD_KT = 8;
 template <class T>
 __global__ void __launch_bounds__(RB)
     k_multidot(const T* __restrict__ V, int64_t ldv, int K, const T* __restrict__ y, int64_t n,
-               double* __restrict__ partial) {
+               double* __restrict__ partial, double* __restrict__ out, unsigned int* __restrict__ counter) {
     __shared__ double sh[MD_KT][RB / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int k0 = blockIdx.y * MD_KT;
@@ -63,18 +87,9 @@ __global__ void __launch_bounds__(RB)
         for (int q = 0; q < RB / 32; ++q) t += sh[threadIdx.x][q];
         partial[(int64_t)blockIdx.x * K + k0 + threadIdx.x] = t;
     }
+    last_block_finish(partial, (int)gridDim.x, K, out, counter);
 }
 
-// out[k] = sum_b partial[b*K + k], fixed order: one warp per k.
-__global__ void k_finish(const double* __restrict__ partial, int nb, int K, double* __restrict__ out) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int k = w; k < K; k += nw) {
-        double acc = 0.0;
-        for (int b = lane; b < nb; b += 32) acc += partial[(int64_t)b * K + k];
-        acc = warp_sum(acc);
-        if (lane == 0) out[k] = acc;
-    }
-}
 
 // y -= sum_k h[k] V_k  (h on the device, staged in shared memory 64 at a
 // time; k ascending for every element)
@@ -108,7 +123,7 @@ constexpr int CG_TILE = 256;
 template <class T, bool DOTS>
 __global__ void __launch_bounds__(CG_TILE)
     k_axpy_dots(const T* __restrict__ V, int64_t ldv, int K, const double* __restrict__ h, T* __restrict__ y,
-                int64_t n, double* __restrict__ partial) {
+                int64_t n, double* __restrict__ partial, double* __restrict__ out, unsigned int* __restrict__ counter) {
     __shared__ double hs[64];
     __shared__ double ys[CG_TILE];
     __shared__ double acc_blk[64];
@@ -161,6 +176,7 @@ __global__ void __launch_bounds__(CG_TILE)
     }
     const int P = DOTS ? K : 1;
     if (threadIdx.x < P) partial[(int64_t)blockIdx.x * P + threadIdx.x] = acc_blk[threadIdx.x];
+    last_block_finish(partial, (int)gridDim.x, P, out, counter);
 }
 
 __global__ void k_axpby(double a, const double* __restrict__ x, double b, double* __restrict__ y, int64_t n) {
@@ -240,6 +256,8 @@ __global__ void k_copy_scalar(const double* __restrict__ src, double* __restrict
 Blas::Blas(cudaStream_t s) : s(s) {
     partial.alloc((size_t)std::max(RGRID, 148 * 8) * 64);
     scal.alloc(128);
+    counter.alloc(1);
+    UP3D_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned int), s));
     UP3D_CUDA(cudaMallocHost(&host, 128 * sizeof(double)));
 }
 Blas::~Blas() {
@@ -251,9 +269,8 @@ void Blas::multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, doubl
     for (int k0 = 0; k0 < K; k0 += 64) {
         int kk = std::min(64, K - k0);
         k_multidot<T><<<dim3(RGRID, (kk + MD_KT - 1) / MD_KT), RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n,
-                                                                          partial.get());
-        UP3D_CHECK_LAUNCH();
-        k_finish<<<1, 1024, 0, s>>>(partial.get(), RGRID, kk, out_dev + k0);
+                                                                          partial.get(), out_dev + k0,
+                                                                          counter.get());
         UP3D_CHECK_LAUNCH();
     }
 }
@@ -292,13 +309,10 @@ template <class T>
 void Blas::axpy_dots(const T* V, int64_t ldv, int K, const double* h_dev, T* y, int64_t n, bool dots,
                      double* out_dev) {
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + CG_TILE - 1) / CG_TILE, 148 * 8));
-    const int P = dots ? K : 1;
     if (dots)
-        k_axpy_dots<T, true><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get());
+        k_axpy_dots<T, true><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get(), out_dev, counter.get());
     else
-        k_axpy_dots<T, false><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get());
-    UP3D_CHECK_LAUNCH();
-    k_finish<<<1, 1024, 0, s>>>(partial.get(), (int)grid, P, out_dev);
+        k_axpy_dots<T, false><<<grid, CG_TILE, 0, s>>>(V, ldv, K, h_dev, y, n, partial.get(), out_dev, counter.get());
     UP3D_CHECK_LAUNCH();
 }
 

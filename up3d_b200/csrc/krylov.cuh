@@ -26,6 +26,7 @@ void coupled_apply(const up3d_coupled* c, const up3d_csr& J, const up3d_csr& ext
 struct Blas {
     cudaStream_t s;
     DBuf<double> partial, scal;
+    DBuf<unsigned int> counter;   // blocks arrived, for the last-block reductions (re-armed by it)
     double* host = nullptr;  // pinned scalar readback
     explicit Blas(cudaStream_t s);
     ~Blas();
