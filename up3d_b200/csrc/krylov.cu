@@ -60,7 +60,7 @@ __device__ __forceinline__ void last_block_finish(const double* partial, int nb,
 constexpr int MD_KT = 8;
 template <class T>
 __global__ void __launch_bounds__(RB)
-    k_multidot(const T* __restrict__ V, int64_t ldv, int K, const T* __restrict__ y, int64_t n,
+    k_multidot(const T* __restrict__ V, int64_t ldv, int Kv, int K, const T* __restrict__ y, int64_t n,
                double* __restrict__ partial, double* __restrict__ out, unsigned int* __restrict__ counter) {
     __shared__ double sh[MD_KT][RB / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -73,7 +73,10 @@ __global__ void __launch_bounds__(RB)
         const double yi = (double)y[i];
 #pragma unroll
         for (int j = 0; j < MD_KT; ++j)
-            if (j < kt) acc[j] += (double)V[(int64_t)(k0 + j) * ldv + i] * yi;
+            if (j < kt) {
+                const T* v = (k0 + j < Kv) ? V + (int64_t)(k0 + j) * ldv : y;
+                acc[j] += (double)v[i] * yi;
+            }
     }
 #pragma unroll
     for (int j = 0; j < MD_KT; ++j) {
@@ -265,11 +268,12 @@ Blas::~Blas() {
 }
 
 template <class T>
-void Blas::multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev) {
-    for (int k0 = 0; k0 < K; k0 += 64) {
-        int kk = std::min(64, K - k0);
-        k_multidot<T><<<dim3(RGRID, (kk + MD_KT - 1) / MD_KT), RB, 0, s>>>(V + k0 * ldv, ldv, kk, y, n,
-                                                                          partial.get(), out_dev + k0,
+void Blas::multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev, bool self_dot) {
+    const int Ktot = K + (self_dot ? 1 : 0);
+    for (int k0 = 0; k0 < Ktot; k0 += 64) {
+        int kk = std::min(64, Ktot - k0);
+        k_multidot<T><<<dim3(RGRID, (kk + MD_KT - 1) / MD_KT), RB, 0, s>>>(V + (int64_t)k0 * ldv, ldv, K - k0, kk, y,
+                                                                          n, partial.get(), out_dev + k0,
                                                                           counter.get());
         UP3D_CHECK_LAUNCH();
     }
@@ -317,7 +321,7 @@ void Blas::axpy_dots(const T* V, int64_t ldv, int K, const double* h_dev, T* y, 
 }
 
 #define UP3D_BLAS_INST(T)                                                                 \
-    template void Blas::multidot<T>(const T*, int64_t, int, const T*, int64_t, double*); \
+    template void Blas::multidot<T>(const T*, int64_t, int, const T*, int64_t, double*, bool); \
     template double Blas::dot<T>(const T*, const T*, int64_t);                           \
     template double Blas::nrm2<T>(const T*, int64_t);                                    \
     template void Blas::scale<T>(T*, double, int64_t);                                   \
@@ -504,12 +508,13 @@ int cg_solve(const Operator& op, const double* b, double* x, double rtol, double
 // V_{col+1} *= 1 / |w| unless |w| <= eps |w_before| (Arnoldi breakdown);
 // hn = (|w_before|^2, |w|^2)
 template <class T>
-__global__ void k_scale_unless_breakdown(T* __restrict__ v, const double* __restrict__ hn, double eps, int64_t n) {
+__global__ void k_scale_unless_breakdown(const T* __restrict__ w, T* __restrict__ v, const double* __restrict__ hn,
+                                         double eps, int64_t n) {
     const double h0 = sqrt(hn[0]), h1 = sqrt(hn[1]);
-    if (h1 <= eps * h0) return;
-    const double f = 1.0 / h1;
+    const bool keep = h1 <= eps * h0;   // breakdown: the vector is copied unscaled
+    const double f = keep ? 1.0 : 1.0 / h1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[i] = (T)((double)v[i] * f);
+        v[i] = keep ? w[i] : (T)((double)w[i] * f);
 }
 
 // Givens rotation as LAPACK xLARTG: c*f + s*g = r, -s*f + c*g = 0.
@@ -545,10 +550,12 @@ int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, 
     restart = (int)std::min<int64_t>(restart, n);
     DBuf<T>* B = W.bufs<T>();
     DBuf<T>& V = B[0];
+    DBuf<T>& w = B[1];
     DBuf<T>& r = B[2];
     DBuf<T>& tmp = B[3];
     DBuf<double>& hdev = W.d[5];
     V.alloc((size_t)(restart + 1) * n);
+    w.alloc(n);
     r.alloc(n);
     tmp.alloc(n);
     hdev.alloc(2 * restart + 6);
@@ -593,30 +600,31 @@ int gmres_solve(const Operator& op, const T* b, T* x, double rtol, double atol, 
             // one Arnoldi step on the device, one readback: the column
             // [h_0 .. h_col] (CGS2: two projections onto V_0..V_col, summed),
             // |w| before and after the projections
-            // the new vector is formed in place in V[col + 1]: pass 1 takes
-            // V_0..V_col and the vector itself in one multidot (h and
-            // |w|^2), passes 2 and 3 are one sweep each (update + the next
-            // pass's dots, update + |w|^2)
+            // pass 1 takes V_0..V_col and the new vector itself in one
+            // multidot (h and |w|^2), passes 2 and 3 are one sweep each
+            // (update + the next pass's dots, update + |w|^2), and the
+            // normalisation writes the vector into V[col + 1].  The
+            // preconditioner's output stays the one buffer w, so its
+            // captured V-cycle graph is replayed, not captured per column.
             double* hsum = hdev.get();                  // h_0..h_col, |w|^2 before, |w|^2 after
             double* hpass = hdev.get() + (restart + 3);
             double* hn = hsum + col + 1;
-            T* wv = V.get() + (size_t)(col + 1) * n;
+            T* wv = w.get();
             op.apply(V.get() + (size_t)col * n, tmp.get(), s);
             precond_apply(M, tmp.get(), wv, n, s);
+            bl.multidot(V.get(), n, col + 1, wv, n, hsum, true);
             if (col + 1 <= 64) {
-                bl.multidot(V.get(), n, col + 2, wv, n, hsum);
                 bl.axpy_dots(V.get(), n, col + 1, hsum, wv, n, true, hpass);
                 bl.axpy_dots(V.get(), n, col + 1, hpass, wv, n, false, hn + 1);
             } else {
-                bl.multidot(V.get(), n, col + 2, wv, n, hsum);
                 bl.multiaxpy(V.get(), n, col + 1, hsum, wv, n);
                 bl.multidot(V.get(), n, col + 1, wv, n, hpass);
                 bl.multiaxpy(V.get(), n, col + 1, hpass, wv, n);
-                bl.multidot(wv, 0, 1, wv, n, hn + 1);
+                bl.multidot(wv, 0, 0, wv, n, hn + 1, true);
             }
             k_accumulate<double><<<1, 64, 0, s>>>(hsum, hpass, col + 1);
             UP3D_CHECK_LAUNCH();
-            k_scale_unless_breakdown<T><<<grid_for(n, 256), 256, 0, s>>>(wv, hn, eps, n);
+            k_scale_unless_breakdown<T><<<grid_for(n, 256), 256, 0, s>>>(wv, V.get() + (size_t)(col + 1) * n, hn, eps, n);
             UP3D_CHECK_LAUNCH();
             UP3D_CUDA(cudaMemcpyAsync(hbuf, hsum, sizeof(double) * (col + 3), cudaMemcpyDeviceToHost, s));
             UP3D_CUDA(cudaStreamSynchronize(s));

@@ -30,8 +30,9 @@ struct Blas {
     double* host = nullptr;  // pinned scalar readback
     explicit Blas(cudaStream_t s);
     ~Blas();
+    // out[k] = V_k . y for k < K, then y . y at out[K] when self_dot
     template <class T>
-    void multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev);
+    void multidot(const T* V, int64_t ldv, int K, const T* y, int64_t n, double* out_dev, bool self_dot = false);
     template <class T>
     double dot(const T* x, const T* y, int64_t n);
     template <class T>
