@@ -21,6 +21,8 @@ Numba kernels) on all host cores, same workload, rank 0 only.
 from __future__ import annotations
 
 import argparse
+import contextlib
+import gc
 import json
 import os
 import subprocess
@@ -278,6 +280,21 @@ def read_traffic(kernel: str, n_tets: int):
     return None
 
 
+@contextlib.contextmanager
+def settled_gc():
+    """Wall-clock solve timings: the cyclic garbage of earlier runs (device
+    buffers of dropped workspaces among it) is collected before the clock
+    starts and the cyclic collector stays off until it stops, so that no
+    collection, and no implicit device synchronisation of the buffers it
+    frees, lands inside a timed solve."""
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        gc.enable()
+
+
 def newton_timing(spec, reps=4):
     """Time-to-1e-10 of the device Newton solve (Picard seed, exact
     Jacobian, GMRES + AMG, line search, frozen finish) from the freestream
@@ -306,13 +323,16 @@ def newton_timing(spec, reps=4):
     for prec in ("fp64", "mixed"):
         runs = []
         for rep_ in range(reps):
-            ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            r = solve_newton_transonic(ws, mach, m_start=m_start, dm=dm_step, precision=prec)
-            torch.cuda.synchronize()
+            ws = None
+            with settled_gc():
+                ws = ChannelWorkspace(mesh.nodes, mesh.elements, mesh.dirichlet_nodes)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r = solve_newton_transonic(ws, mach, m_start=m_start, dm=dm_step, precision=prec)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
             if reps == 1 or rep_ > 0:
-                runs.append((time.perf_counter() - t0, r))
+                runs.append((dt, r))
         runs.sort(key=lambda x: x[0])
         dt, res = runs[len(runs) // 2]
         phis[prec] = res["phi"]
@@ -343,7 +363,8 @@ def adjoint_timing(spec):
     mach = float(mach_s)
     g = None
     for _ in range(2):
-        g = adjoint_gradient(shape, mach, m_start=min(0.70, mach))
+        with settled_gc():
+            g = adjoint_gradient(shape, mach, m_start=min(0.70, mach))
     torch.cuda.synchronize()
     return {"case": f"bump channel {shape_s} ({len(shape.elements)} tets), bump {amp_s}, M_inf {mach}, "
                     f"{shape.n_params} shape modes + Mach",
@@ -502,7 +523,8 @@ def lifting_timing(spec):
 
     cut, vc = case(shape)
     device_solve(cut, vc, 1e-6)                # warm-up (library, mesh caches)
-    ws, res, setup = device_solve(cut, vc, 1e-6)
+    with settled_gc():
+        ws, res, setup = device_solve(cut, vc, 1e-6)
     out = {"case": f"bump channel {parts[0]} Kuhn-split, y-normal wake sheet from x = {vc[0]:.2f}, "
                    f"M_inf {m_inf}, alpha {alpha} deg, from the freestream",
            "n_tets": int(len(cut.elements)), "n_red": int(ws.n_red), "n_stations": int(ws.n_st),
@@ -512,11 +534,13 @@ def lifting_timing(spec):
            "final_residual": res["residual_history"][-1], "final_F": res["F_history"][-1],
            "n_supersonic": int(res["n_nu_active"]), "n_term3_active": int(res["n_term3_active"]),
            "phases_s": {k: round(v, 4) for k, v in res["timings"].items()}}
-    t0 = time.perf_counter()
-    cont = solve_newton_transonic(cut, cut.wc, m_inf + 0.05, alpha, m_start=m_inf - 0.1,
-                                  newton_kw={"vortex_center": vc})
+    with settled_gc():
+        t0 = time.perf_counter()
+        cont = solve_newton_transonic(cut, cut.wc, m_inf + 0.05, alpha, m_start=m_inf - 0.1,
+                                      newton_kw={"vortex_center": vc})
+        cont_s = time.perf_counter() - t0
     out["continuation"] = {"mach": [round(m_inf - 0.1, 3), round(m_inf + 0.05, 3)],
-                           "time_s": round(time.perf_counter() - t0, 3), "converged": bool(cont["converged"]),
+                           "time_s": round(cont_s, 3), "converged": bool(cont["converged"]),
                            "levels": [[round(m, 4), n, r] for m, n, r in cont["level_history"]],
                            "n_supersonic": int(cont["n_nu_active"])}
     if len(parts) > 3 and parts[3]:
@@ -800,16 +824,20 @@ def batched_timing(spec, seed=0):
         return b
     res_b = None
     for _ in range(2):
-        res_b = solve_newton_batched(fresh(), machs)
-    res_ng = solve_newton_batched(fresh(), machs, use_graphs=False)
+        with settled_gc():
+            res_b = solve_newton_batched(fresh(), machs)
+    with settled_gc():
+        res_ng = solve_newton_batched(fresh(), machs, use_graphs=False)
     seq_s, seq_ok, seq_phi = [], [], []
     for c, m in enumerate(meshes):
-        ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = solve_newton_transonic(ws, float(machs[c]), m_start=min(0.70, float(machs[c])))
-        torch.cuda.synchronize()
-        seq_s.append(time.perf_counter() - t0)
+        ws = None
+        with settled_gc():
+            ws = ChannelWorkspace(m.nodes, m.elements, m.dirichlet_nodes)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = solve_newton_transonic(ws, float(machs[c]), m_start=min(0.70, float(machs[c])))
+            torch.cuda.synchronize()
+            seq_s.append(time.perf_counter() - t0)
         seq_ok.append(bool(r["converged"]))
         seq_phi.append(r["phi"].cpu())
     out["newton"] = {"batched_s": round(res_b["time_s"], 4), "sequential_s": round(float(sum(seq_s)), 4),
@@ -827,8 +855,11 @@ def batched_timing(spec, seed=0):
     # the mixed schedule: the small cases in one lockstep union, the large
     # ones alone (built before the clock, like the sequential workspaces)
     for below in (100_000, 300_000):
+        cs = None
+        gc.collect()
         cs = CaseSet(meshes, machs, batch_below=below)
-        res_cs = cs.solve()
+        with settled_gc():
+            res_cs = cs.solve()
         out["newton"][f"mixed_schedule_{below // 1000}k"] = {
             "batch_below_tets": below, "n_batched": res_cs["n_batched"], "n_plain": res_cs["n_plain"],
             "batched_tets": int(sum(meshes[c].n_tets for c in cs.small)),
