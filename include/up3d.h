@@ -539,6 +539,23 @@ int up3d_autotune(up3d_mesh* mesh, const double* phi, const up3d_flow* flow, int
 /* Number of library kernel launches since the library was loaded (the
  * reference has no counterpart; used to report device launches per step). */
 int up3d_launch_count(int64_t* out);
+
+/* The library's device memory (no reference counterpart: numpy / scipy
+ * allocate on the host).  Every device buffer of the library comes from a
+ * per-device cache of cudaMalloc'd blocks: a freed block is kept, once the
+ * device has finished the work in flight (the synchronisation cudaFree
+ * implies), and handed to a later request of the same size or at most a
+ * quarter smaller, so repeated set-ups of a problem (a fresh workspace per
+ * solve) make no driver allocation.  The cache holds at most
+ * UP3D_POOL_CACHE_MB MiB (read at the first allocation; default 4096, 0
+ * turns caching off); when cudaMalloc runs out of memory the device's
+ * cached blocks are released and the allocation retried once.
+ * up3d_pool_stats: bytes cached and handed out, and the requests served
+ * from the cache (hits) or by cudaMalloc (misses) since the library was
+ * loaded.  up3d_pool_release: cudaFree of every cached block (for a caller
+ * that needs the memory elsewhere); released_bytes may be NULL. */
+int up3d_pool_stats(int64_t* cached_bytes, int64_t* live_bytes, int64_t* hits, int64_t* misses);
+int up3d_pool_release(int64_t* released_bytes);
 /* Enable (1) / disable (0) per-phase CUDA-event timing and reset it. */
 int up3d_profile(int enable);
 /* Per phase slot (0 element sweep, 1 row gather, 2 Term-3 build, 3 SpMV,

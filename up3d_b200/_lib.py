@@ -151,6 +151,9 @@ SIGNATURES = {
     "up3d_tile_plan_host_array": (_int, [_p, ctypes.c_char_p, _p, ctypes.POINTER(_i64)]),
     "up3d_tile_plan_host_destroy": (_int, [_p]),
     "up3d_launch_count": (_int, [ctypes.POINTER(_i64)]),
+    "up3d_pool_stats": (_int, [ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                               ctypes.POINTER(_i64)]),
+    "up3d_pool_release": (_int, [ctypes.POINTER(_i64)]),
     "up3d_profile": (_int, [_int]),
     "up3d_profile_read": (_int, [_p, _p, _p, _int]),
     "up3d_spmv": (_int, [_i64, _p, _p, _p, _p, _p, _p, _p]),
@@ -307,6 +310,21 @@ PROF_SLOTS = ("elem_sweep", "row_gather", "term3", "spmv", "krylov")
 def launch_count() -> int:
     out = ctypes.c_int64()
     call("up3d_launch_count", ctypes.byref(out))
+    return int(out.value)
+
+
+def pool_stats() -> dict:
+    """The device block cache: bytes cached and handed out, cache hits and
+    misses (up3d_pool_stats)."""
+    v = [ctypes.c_int64() for _ in range(4)]
+    call("up3d_pool_stats", *(ctypes.byref(x) for x in v))
+    return dict(zip(("cached_bytes", "live_bytes", "hits", "misses"), (int(x.value) for x in v)))
+
+
+def pool_release() -> int:
+    """Frees every cached device block; returns the bytes released."""
+    out = ctypes.c_int64()
+    call("up3d_pool_release", ctypes.byref(out))
     return int(out.value)
 
 

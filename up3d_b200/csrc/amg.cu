@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -792,6 +793,9 @@ struct Amg {
     std::vector<Graph> graphs;
     cudaStream_t capture_stream = nullptr;
     int device = 0;
+    // the numeric phase's vector kernels (kept: set-up and every refresh
+    // would otherwise allocate and free its scratch and pinned readback)
+    std::unique_ptr<Blas> blas;
     void drop_graphs() {
         for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
         graphs.clear();
@@ -860,7 +864,9 @@ std::vector<int32_t> diag_slots(const HostCSR& A) {
 // operator, then the coarsest inverse; fills the cycle's levels.
 void numeric(Amg& a, cudaStream_t s) {
     const size_t L = a.sym.size();
-    Blas blas(s);
+    if (!a.blas) a.blas.reset(new Blas(s));
+    Blas& blas = *a.blas;
+    blas.s = s;
     double* dots = a.pw_scal.get();       // x.y, y.y, x.x, |y|
     double* lam = a.pw_scal.get() + 4;
     int* done = a.flags.get();

@@ -69,6 +69,12 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 32) {
 
 // ------------------------------------------------------------ device buffer
 
+// Device blocks of the library's buffers (pool.cu): cudaMalloc'd, cached
+// per device once freed (after the device has finished with them) and
+// reused by later requests of nearly the same size.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -78,7 +84,7 @@ struct DBuf {
     DBuf& operator=(const DBuf&) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }
@@ -86,7 +92,7 @@ struct DBuf {
         if (count <= n && p) return;
         release();
         if (count == 0) count = 1;
-        UP3D_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        p = static_cast<T*>(dev_alloc(count * sizeof(T)));
         n = count;
     }
     T* get() const { return p; }
