@@ -295,6 +295,15 @@ def settled_gc():
         gc.enable()
 
 
+def empty_pool():
+    """Each solver leg starts from an empty device block cache: the blocks
+    that earlier legs left cached are released here, outside any clock,
+    instead of being evicted (deferred cudaFree calls) inside a timed solve."""
+    from up3d_b200 import _lib as L
+    gc.collect()
+    L.pool_release()
+
+
 def newton_timing(spec, reps=4):
     """Time-to-1e-10 of the device Newton solve (Picard seed, exact
     Jacobian, GMRES + AMG, line search, frozen finish) from the freestream
@@ -321,6 +330,7 @@ def newton_timing(spec, reps=4):
                           else "first (workspace and tile plan built before the clock)")}
     phis = {}
     for prec in ("fp64", "mixed"):
+        empty_pool()
         runs = []
         for rep_ in range(reps):
             ws = None
@@ -362,6 +372,7 @@ def adjoint_timing(spec):
     shape = BumpShape(nx, ny, nz, amplitude=float(amp_s), seed=0)
     mach = float(mach_s)
     g = None
+    empty_pool()
     for _ in range(2):
         with settled_gc():
             g = adjoint_gradient(shape, mach, m_start=min(0.70, mach))
@@ -522,6 +533,7 @@ def lifting_timing(spec):
         return ws, res, setup
 
     cut, vc = case(shape)
+    empty_pool()
     device_solve(cut, vc, 1e-6)                # warm-up (library, mesh caches)
     with settled_gc():
         ws, res, setup = device_solve(cut, vc, 1e-6)
@@ -823,12 +835,14 @@ def batched_timing(spec, seed=0):
             b.ws.ev.mesh.tile_info()
         return b
     res_b = None
+    empty_pool()
     for _ in range(2):
         with settled_gc():
             res_b = solve_newton_batched(fresh(), machs)
     with settled_gc():
         res_ng = solve_newton_batched(fresh(), machs, use_graphs=False)
     seq_s, seq_ok, seq_phi = [], [], []
+    empty_pool()
     for c, m in enumerate(meshes):
         ws = None
         with settled_gc():
@@ -856,7 +870,7 @@ def batched_timing(spec, seed=0):
     # ones alone (built before the clock, like the sequential workspaces)
     for below in (100_000, 300_000):
         cs = None
-        gc.collect()
+        empty_pool()
         cs = CaseSet(meshes, machs, batch_below=below)
         with settled_gc():
             res_cs = cs.solve()

@@ -548,7 +548,8 @@ int up3d_launch_count(int64_t* out);
  * quarter smaller, so repeated set-ups of a problem (a fresh workspace per
  * solve) make no driver allocation.  The cache holds at most
  * UP3D_POOL_CACHE_MB MiB (read at the first allocation; default 4096, 0
- * turns caching off); when cudaMalloc runs out of memory the device's
+ * turns caching off; past it the least recently freed blocks are released
+ * down to three quarters of it); when cudaMalloc runs out of memory the device's
  * cached blocks are released and the allocation retried once.
  * up3d_pool_stats: bytes cached and handed out, and the requests served
  * from the cache (hits) or by cudaMalloc (misses) since the library was

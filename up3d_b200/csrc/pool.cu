@@ -12,9 +12,12 @@
 // stream, so dev_free waits for the device before it caches the block --
 // the same synchronisation cudaFree implies.  The cache holds at most
 // cap bytes per process (UP3D_POOL_CACHE_MB, default 4096; 0 turns caching
-// off); beyond that the largest cached blocks are released.  When
+// off); past the cap the least recently freed blocks are released until
+// three quarters of it remain (so that eviction, which costs what the
+// deferred cudaFree calls cost, comes in few batches).  When
 // cudaMalloc runs out of memory the device's cached blocks are released
 // and the allocation is retried once.
+#include <cstdint>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -30,12 +33,18 @@ struct Block {
     size_t size;
 };
 
+struct Cached {
+    void* p;
+    uint64_t seq;  // order of the frees (eviction takes the oldest first)
+};
+
 struct Pool {
     std::mutex mu;
-    std::unordered_map<void*, Block> live;                  // handed out
-    std::multimap<std::pair<int, size_t>, void*> cached;    // (device, size) -> free block
+    std::unordered_map<void*, Block> live;                   // handed out
+    std::multimap<std::pair<int, size_t>, Cached> cached;    // (device, size) -> free block
     size_t cached_bytes = 0, live_bytes = 0;
     int64_t hits = 0, misses = 0;
+    uint64_t seq = 0;
     size_t cap = size_t(4096) << 20;
     Pool() {
         if (const char* v = std::getenv("UP3D_POOL_CACHE_MB")) {
@@ -72,7 +81,7 @@ size_t release_locked(Pool& P, int device) {
             continue;
         }
         if (it->first.first != prev) cudaSetDevice(it->first.first);
-        cudaFree(it->second);
+        cudaFree(it->second.p);
         freed += it->first.second;
         P.cached_bytes -= it->first.second;
         it = P.cached.erase(it);
@@ -94,7 +103,7 @@ void* dev_alloc(size_t bytes) {
         // most a quarter larger than asked
         auto it = P.cached.lower_bound({dev, sz});
         if (it != P.cached.end() && it->first.first == dev && it->first.second - sz <= sz / 4) {
-            void* p = it->second;
+            void* p = it->second.p;
             const size_t bsz = it->first.second;
             P.cached.erase(it);
             P.cached_bytes -= bsz;
@@ -147,18 +156,22 @@ void dev_free(void* p) {
         cudaGetLastError();
     } else {
         std::lock_guard<std::mutex> g(P.mu);
-        P.cached.insert({{b.device, b.size}, p});
+        P.cached.insert({{b.device, b.size}, Cached{p, P.seq++}});
         P.cached_bytes += b.size;
-        // over the cap: release the largest cached blocks
-        while (P.cached_bytes > P.cap && !P.cached.empty()) {
-            auto big = P.cached.begin();
-            for (auto it = P.cached.begin(); it != P.cached.end(); ++it)
-                if (it->first.second > big->first.second) big = it;
-            if (big->first.first != b.device) cudaSetDevice(big->first.first);
-            cudaFree(big->second);
-            if (big->first.first != b.device) cudaSetDevice(b.device);
-            P.cached_bytes -= big->first.second;
-            P.cached.erase(big);
+        // over the cap: release the least recently freed blocks down to
+        // three quarters of it
+        if (P.cached_bytes > P.cap) {
+            const size_t low = P.cap - P.cap / 4;
+            while (P.cached_bytes > low && !P.cached.empty()) {
+                auto old = P.cached.begin();
+                for (auto it = P.cached.begin(); it != P.cached.end(); ++it)
+                    if (it->second.seq < old->second.seq) old = it;
+                if (old->first.first != b.device) cudaSetDevice(old->first.first);
+                cudaFree(old->second.p);
+                if (old->first.first != b.device) cudaSetDevice(b.device);
+                P.cached_bytes -= old->first.second;
+                P.cached.erase(old);
+            }
         }
     }
     if (prev >= 0 && prev != b.device) cudaSetDevice(prev);
