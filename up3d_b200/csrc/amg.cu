@@ -70,13 +70,24 @@ unsigned char* stage_buffer(Stage& st) {
     }
     return st.p;
 }
+// host memcpy spread over the OpenMP threads (1 MiB pieces): a single
+// thread copies pageable memory at a fraction of the link's rate
+void par_memcpy(unsigned char* dst, const unsigned char* src, size_t bytes) {
+    constexpr size_t PIECE = size_t(1) << 20;
+    const int64_t pieces = (int64_t)((bytes + PIECE - 1) / PIECE);
+#pragma omp parallel for schedule(static) if (pieces > 1)
+    for (int64_t k = 0; k < pieces; ++k) {
+        const size_t o = (size_t)k * PIECE;
+        std::memcpy(dst + o, src + o, std::min(PIECE, bytes - o));
+    }
+}
 void h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     Stage& st = stage();
     std::lock_guard<std::mutex> g(st.mu);
     unsigned char* buf = stage_buffer(st);
     for (size_t o = 0; o < bytes; o += STAGE_CHUNK) {
         const size_t b = std::min(STAGE_CHUNK, bytes - o);
-        std::memcpy(buf, static_cast<const unsigned char*>(src) + o, b);
+        par_memcpy(buf, static_cast<const unsigned char*>(src) + o, b);
         UP3D_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + o, buf, b, cudaMemcpyHostToDevice, s));
         UP3D_CUDA(cudaStreamSynchronize(s));
     }
@@ -89,7 +100,7 @@ void d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
         const size_t b = std::min(STAGE_CHUNK, bytes - o);
         UP3D_CUDA(cudaMemcpyAsync(buf, static_cast<const unsigned char*>(src) + o, b, cudaMemcpyDeviceToHost, s));
         UP3D_CUDA(cudaStreamSynchronize(s));
-        std::memcpy(static_cast<unsigned char*>(dst) + o, buf, b);
+        par_memcpy(static_cast<unsigned char*>(dst) + o, buf, b);
     }
 }
 
@@ -220,24 +231,50 @@ HostCSR prolongator_pattern(const HostCSR& A, const std::vector<int32_t>& agg, i
     return P;
 }
 
-// R = P^T pattern; R entry t takes the value of P entry tperm[t].
+// R = P^T pattern; R entry t takes the value of P entry tperm[t].  Each
+// R row lists its P rows in ascending order: the P rows are cut into one
+// contiguous range per thread, each thread counts its range's entries per
+// column, and the column-major prefix over (column, thread) gives every
+// thread its own slots, filled in row order.
 HostCSR transpose_pattern(const HostCSR& P, std::vector<int32_t>& tperm) {
     HostCSR R;
     R.n = P.m;
     R.m = P.n;
     R.p.assign(R.n + 1, 0);
-    for (int32_t c : P.i) R.p[c + 1]++;
-    for (int64_t r = 0; r < R.n; ++r) R.p[r + 1] += R.p[r];
     R.i.resize(P.i.size());
     tperm.resize(P.i.size());
-    std::vector<int32_t> cur(R.p.begin(), R.p.end() - 1);
-    for (int64_t r = 0; r < P.n; ++r)
-        for (int32_t k = P.p[r]; k < P.p[r + 1]; ++k) {
-            const int32_t c = P.i[k];
-            R.i[cur[c]] = (int32_t)r;
-            tperm[cur[c]] = k;
-            ++cur[c];
+    const int T = std::max(1, std::min(omp_get_max_threads(), 64));
+    const int64_t nc = R.n;
+    std::vector<int64_t> cnt((size_t)T * (nc + 1), 0);  // (thread, column) counts, then offsets
+    auto lo = [&](int t) { return P.n * t / T; };
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (int t = 0; t < T; ++t) {
+        int64_t* c_t = cnt.data() + (size_t)t * (nc + 1);
+        for (int64_t r = lo(t); r < lo(t + 1); ++r)
+            for (int32_t k = P.p[r]; k < P.p[r + 1]; ++k) c_t[P.i[k]]++;
+    }
+    int64_t run = 0;
+    for (int64_t c = 0; c < nc; ++c) {
+        R.p[c] = (int32_t)run;
+        for (int t = 0; t < T; ++t) {
+            int64_t& v = cnt[(size_t)t * (nc + 1) + c];
+            const int64_t n_tc = v;
+            v = run;
+            run += n_tc;
         }
+    }
+    R.p[nc] = (int32_t)run;
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (int t = 0; t < T; ++t) {
+        int64_t* c_t = cnt.data() + (size_t)t * (nc + 1);
+        for (int64_t r = lo(t); r < lo(t + 1); ++r)
+            for (int32_t k = P.p[r]; k < P.p[r + 1]; ++k) {
+                const int32_t c = P.i[k];
+                const int64_t o = c_t[c]++;
+                R.i[o] = (int32_t)r;
+                tperm[o] = k;
+            }
+    }
     return R;
 }
 
@@ -1153,8 +1190,7 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         HostCSR h;
         h.n = h.m = n;
         h.p.resize(n + 1);
-        UP3D_CUDA(cudaMemcpyAsync(h.p.data(), A.indptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-        UP3D_CUDA(cudaStreamSynchronize(s));
+        d2h(h.p.data(), A.indptr, sizeof(int32_t) * (n + 1), s);
         const int64_t nnz = h.p[n];
         h.i.resize(nnz);
         d2h(h.i.data(), A.indices, sizeof(int32_t) * nnz, s);
@@ -1167,8 +1203,11 @@ void* amg_setup(const up3d_csr& A, const up3d_amg_options& opt, cudaStream_t s) 
         a->n_in = n;
         a->nnz_in = nnz;
         a->has_dir = A.dirichlet != nullptr;
-        upload(a->in_p, h.p, s);
-        upload(a->in_i, h.i, s);
+        a->in_p.alloc(n + 1);
+        a->in_i.alloc(std::max<int64_t>(nnz, 1));
+        UP3D_CUDA(cudaMemcpyAsync(a->in_p.get(), A.indptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice, s));
+        if (nnz)
+            UP3D_CUDA(cudaMemcpyAsync(a->in_i.get(), A.indices, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, s));
         if (a->has_dir) upload(a->in_dir, skip, s);
         // finest operator as the embedded free-DOF system: identity rows,
         // constrained columns dropped; src = caller entry (-1: identity)
