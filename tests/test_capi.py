@@ -48,3 +48,15 @@ def test_no_device_raises_cleanly():
     import numpy as np
     with pytest.raises(RuntimeError, match="CUDA device"):
         PicardOperator(np.zeros((4, 3)), np.array([[0, 1, 2, 3]], dtype=np.int32))
+
+
+def test_pool_accounting_without_a_device():
+    """The device block cache's accounting entry points are host-only: with
+    nothing allocated they report an empty cache, a release frees nothing,
+    and a null argument is refused."""
+    s = L.pool_stats()
+    if s["live_bytes"] == 0 and s["misses"] == 0:  # no device buffer made in this process
+        assert s == {"cached_bytes": 0, "live_bytes": 0, "hits": 0, "misses": 0}
+        assert L.pool_release() == 0
+    with pytest.raises(TypeError):
+        L.call("up3d_pool_stats", None, None, None, None)
