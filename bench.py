@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mesh", default="x".join(map(str, MESH)))
     p.add_argument("--e2e-steps", type=int, default=100)
-    p.add_argument("--cpu-states", type=int, default=5)
+    p.add_argument("--cpu-states", type=int, default=40)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pocket-steps", type=int, default=300)
     p.add_argument("--order", default="given", choices=["given", "morton", "hilbert"],
